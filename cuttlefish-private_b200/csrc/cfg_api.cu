@@ -1,0 +1,484 @@
+// cfg_api.cu -- the C ABI (include/cuttlefish_gpu.h): context, device buffers and
+// the launch sequence partition -> bucket scatter -> subgraph construct+walk.
+#include "cuttlefish_gpu.h"
+#include "cfg_device.cuh"
+#include "cfg_internal.h"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace cfg;
+
+namespace {
+
+// seed ^= wymix(seed ^ s0, s1) for seed 0 (include/wyhash/wyhash.h:118), on the host.
+uint64_t wy_seed0() {
+    const __uint128_t r = (__uint128_t)WY_S0 * WY_S1;
+    return (uint64_t)r ^ (uint64_t)(r >> 64);
+}
+
+}  // namespace
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    bool ensure(size_t need) {
+        if (need <= bytes) return true;
+        if (p) cudaFree(p);
+        p = nullptr; bytes = 0;
+        size_t want = need + need / 4 + 4096;
+        if (cudaMalloc(&p, want) != cudaSuccess) { cudaGetLastError(); return false; }
+        bytes = want;
+        return true;
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
+    template <typename T> T* as() const { return (T*)p; }
+};
+
+struct cfg_ctx {
+    int device = 0;
+    cfg_params p{};
+    uint32_t G = 16384;
+    int words = 1;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[5] = {};
+    float times[4] = {0, 0, 0, 0};
+    std::string err;
+
+    // input
+    DevBuf packed, frag_off, frag_len;
+    const uint64_t* d_packed = nullptr; const uint64_t* d_frag_off = nullptr; const uint32_t* d_frag_len = nullptr;
+    uint64_t n_bases = 0, n_frags = 0;
+    bool have_input = false, have_run = false;
+
+    // partition
+    DevBuf flat, hist, misc, bucket_off, inst, fill, recs;
+    // plan
+    DevBuf list, tab_off, tab_cap, arena;
+    // outputs
+    DevBuf fasta, lm_text, lm, dump, retry, counters;
+    uint64_t fasta_cap = 0, lm_text_cap = 0, lm_cap = 0, dump_cap = 0;
+
+    // host results
+    std::vector<char> h_fasta, h_lm_text;
+    std::vector<cfg_lmtig> h_lm;
+    std::vector<cfg_state> h_states;
+    std::vector<cfg_record> h_records;
+    cfg_counts counts{};
+    uint64_t n_records = 0, n_instances = 0, dump_n = 0;
+};
+
+namespace {
+
+int fail(cfg_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(cfg_ctx* c, cudaError_t e, const char* what) {
+    return fail(c, CFG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                                   \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return cuda_fail(c, e_, #call);     \
+    } while (0)
+
+uint32_t next_pow2(uint64_t v) {
+    uint64_t p = 64;
+    while (p < v) p <<= 1;
+    return (uint32_t)std::min<uint64_t>(p, 1ull << 31);
+}
+
+struct MiscWords {   // small device-side words, one allocation
+    unsigned long long rec_cursor;
+    uint32_t err;
+    uint32_t pad;
+};
+
+int check_err_word(cfg_ctx* c, uint32_t e) {
+    if (e & DERR_MISSING_KEY) return fail(c, CFG_ERR_WALK_LIMIT, "neighbour k-mer missing from its subgraph table");
+    if (e & DERR_WALK_LIMIT) return fail(c, CFG_ERR_WALK_LIMIT, "unitig walk exceeded its step bound");
+    if (e & DERR_CAS_LIMIT) return fail(c, CFG_ERR_WALK_LIMIT, "edge-count CAS loop exceeded its bound");
+    return CFG_OK;
+}
+
+// Partition + bucket scatter.  Leaves bucketed records in c->recs and per-subgraph
+// instance counts in `inst_h`.
+int run_partition(cfg_ctx* c, std::vector<uint32_t>& inst_h, std::vector<uint32_t>& off_h) {
+    const uint32_t G = c->G;
+    if (!c->hist.ensure(sizeof(unsigned long long) * G)) return fail(c, CFG_ERR_OOM, "hist");
+    if (!c->misc.ensure(sizeof(MiscWords))) return fail(c, CFG_ERR_OOM, "misc");
+    uint64_t cap = std::max<uint64_t>(c->n_bases / 4 + 1024, 1u << 16);
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        if (!c->flat.ensure(cap * 8)) return fail(c, CFG_ERR_OOM, "flat records");
+        cap = c->flat.bytes / 8;
+        CK(cudaMemsetAsync(c->hist.p, 0, sizeof(unsigned long long) * G, c->stream));
+        CK(cudaMemsetAsync(c->misc.p, 0, sizeof(MiscWords), c->stream));
+        PartitionArgs a{};
+        a.packed = c->d_packed; a.frag_off = c->d_frag_off; a.frag_len = c->d_frag_len;
+        a.n_frags = c->n_frags; a.n_bases = c->n_bases;
+        a.k = c->p.k; a.l = c->p.l; a.w = c->p.k - c->p.l;
+        a.gmask = G - 1; a.seed0 = wy_seed0(); a.seg = 2048;
+        a.recs = c->flat.as<uint64_t>(); a.rec_cap = cap;
+        a.rec_cursor = &c->misc.as<MiscWords>()->rec_cursor;
+        a.hist = c->hist.as<unsigned long long>();
+        a.err = &c->misc.as<MiscWords>()->err;
+        launch_partition(a, c->stream);
+        CK(cudaGetLastError());
+        MiscWords m{};
+        CK(cudaMemcpyAsync(&m, c->misc.p, sizeof(m), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (m.rec_cursor <= cap && !(m.err & DERR_REC_OVERFLOW)) { c->n_records = m.rec_cursor; break; }
+        cap = m.rec_cursor + 1024;
+        if (attempt == 2) return fail(c, CFG_ERR_OOM, "record buffer kept overflowing");
+    }
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    if (!c->bucket_off.ensure(4ull * (G + 1)) || !c->inst.ensure(4ull * G) || !c->fill.ensure(4ull * G))
+        return fail(c, CFG_ERR_OOM, "bucket arrays");
+    if (!c->recs.ensure(8 * std::max<uint64_t>(c->n_records, 1))) return fail(c, CFG_ERR_OOM, "bucketed records");
+    launch_bucket_scan(c->hist.as<unsigned long long>(), G, c->bucket_off.as<uint32_t>(), c->inst.as<uint32_t>(),
+                       c->fill.as<uint32_t>(), c->stream);
+    ScatterArgs s{};
+    s.flat = c->flat.as<uint64_t>(); s.n = c->n_records;
+    s.bucket_off = c->bucket_off.as<uint32_t>(); s.bucket_fill = c->fill.as<uint32_t>();
+    s.recs = c->recs.as<uint64_t>();
+    launch_scatter(s, c->stream);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ev[2], c->stream));
+    inst_h.resize(G); off_h.resize(G + 1);
+    CK(cudaMemcpyAsync(inst_h.data(), c->inst.p, 4ull * G, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(off_h.data(), c->bucket_off.p, 4ull * (G + 1), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->n_instances = 0;
+    for (uint32_t g = 0; g < G; ++g) c->n_instances += inst_h[g];
+    return CFG_OK;
+}
+
+struct Launch { std::vector<uint32_t> list; std::vector<uint64_t> off; std::vector<uint32_t> cap; uint32_t smem_cap = 0; bool smem = false; };
+
+int launch_plan(cfg_ctx* c, const std::vector<Launch>& plan, uint64_t arena_slots) {
+    const int W = c->words;
+    if (arena_slots && !c->arena.ensure(arena_slots * slot_bytes(W))) return fail(c, CFG_ERR_OOM, "table arena");
+    size_t n_total = 0;
+    for (const Launch& L : plan) n_total += L.list.size();
+    if (!c->list.ensure(4 * std::max<size_t>(n_total, 1)) || !c->tab_off.ensure(8 * std::max<size_t>(n_total, 1)) ||
+        !c->tab_cap.ensure(4 * std::max<size_t>(n_total, 1)))
+        return fail(c, CFG_ERR_OOM, "plan arrays");
+    size_t at = 0;
+    for (const Launch& L : plan) {
+        if (L.list.empty()) continue;
+        uint32_t* d_list = c->list.as<uint32_t>() + at;
+        uint64_t* d_off = c->tab_off.as<uint64_t>() + at;
+        uint32_t* d_cap = c->tab_cap.as<uint32_t>() + at;
+        CK(cudaMemcpyAsync(d_list, L.list.data(), 4 * L.list.size(), cudaMemcpyHostToDevice, c->stream));
+        if (!L.smem) {
+            CK(cudaMemcpyAsync(d_off, L.off.data(), 8 * L.off.size(), cudaMemcpyHostToDevice, c->stream));
+            CK(cudaMemcpyAsync(d_cap, L.cap.data(), 4 * L.cap.size(), cudaMemcpyHostToDevice, c->stream));
+        }
+        SubgraphArgs a{};
+        a.packed = c->d_packed; a.recs = c->recs.as<uint64_t>(); a.bucket_off = c->bucket_off.as<uint32_t>();
+        a.list = d_list; a.n_list = (uint32_t)L.list.size();
+        a.tab_off = d_off; a.tab_cap = d_cap; a.smem_cap = L.smem_cap; a.arena = c->arena.as<unsigned char>();
+        a.k = c->p.k; a.fth = c->p.cutoff; a.load_limit_pct = 90;
+        a.fasta = c->fasta.as<char>(); a.fasta_cap = c->fasta_cap;
+        a.lm_text = c->lm_text.as<char>(); a.lm_text_cap = c->lm_text_cap;
+        a.lm = c->lm.as<LmtigOut>(); a.lm_cap = c->lm_cap;
+        a.dump = (c->p.flags & CFG_FLAG_DUMP_STATES) ? c->dump.as<StateOut>() : nullptr; a.dump_cap = c->dump_cap;
+        a.retry = c->retry.as<uint32_t>(); a.cnt = c->counters.as<Counters>();
+        a.err = &c->misc.as<MiscWords>()->err;
+        const uint32_t threads = L.smem ? std::min<uint32_t>(256, std::max<uint32_t>(64, L.smem_cap / 4)) : 512;
+        launch_subgraphs(a, W, L.smem, threads, c->stream);
+        CK(cudaGetLastError());
+        at += L.list.size();
+    }
+    return CFG_OK;
+}
+
+int ensure_outputs(cfg_ctx* c, uint64_t fasta_need, uint64_t lm_text_need, uint64_t lm_need) {
+    if (!c->fasta.ensure(fasta_need)) return fail(c, CFG_ERR_OOM, "fasta arena");
+    c->fasta_cap = c->fasta.bytes;
+    if (!c->lm_text.ensure(lm_text_need)) return fail(c, CFG_ERR_OOM, "lm-tig arena");
+    c->lm_text_cap = c->lm_text.bytes;
+    if (!c->lm.ensure(lm_need * sizeof(LmtigOut))) return fail(c, CFG_ERR_OOM, "lm-tig records");
+    c->lm_cap = c->lm.bytes / sizeof(LmtigOut);
+    if (!c->retry.ensure(4ull * c->G)) return fail(c, CFG_ERR_OOM, "retry list");
+    if (!c->counters.ensure(sizeof(Counters))) return fail(c, CFG_ERR_OOM, "counters");
+    if (c->p.flags & CFG_FLAG_DUMP_STATES) {
+        if (!c->dump.ensure(sizeof(StateOut) * std::max<uint64_t>(c->n_instances, 1))) return fail(c, CFG_ERR_OOM, "state dump");
+        c->dump_cap = c->dump.bytes / sizeof(StateOut);
+    }
+    return CFG_OK;
+}
+
+int run_subgraphs(cfg_ctx* c, const std::vector<uint32_t>& inst_h) {
+    const uint32_t G = c->G;
+    const int W = c->words;
+    const uint32_t load = c->p.table_load_pct ? c->p.table_load_pct : 125;
+    const uint32_t smem_max = (uint32_t)subgraph_max_smem_cap(W);
+    std::vector<uint32_t> caps(G, 0);
+    for (uint32_t g = 0; g < G; ++g)
+        if (inst_h[g]) caps[g] = next_pow2(((uint64_t)inst_h[g] * load + 99) / 100);
+
+    uint64_t fasta_need = c->n_bases + (c->n_records + 1024) * 8 + (1u << 20);
+    uint64_t lm_text_need = c->n_bases / 2 + (c->n_records + 1024) * (c->p.k + 2);
+    uint64_t lm_need = c->n_records + 1024;
+    std::vector<uint32_t> todo;
+    for (uint32_t g = 0; g < G; ++g) if (inst_h[g]) todo.push_back(g);
+    // larger subgraphs first (src/Subgraphs_Manager.cpp:222-231)
+    std::stable_sort(todo.begin(), todo.end(), [&](uint32_t a, uint32_t b) { return inst_h[a] > inst_h[b]; });
+
+    for (int round = 0; round < 3; ++round) {   // output-arena overflow: regrow, rerun all
+        int rc = ensure_outputs(c, fasta_need, lm_text_need, lm_need);
+        if (rc) return rc;
+        CK(cudaMemsetAsync(c->counters.p, 0, sizeof(Counters), c->stream));
+        std::vector<uint32_t> work = todo;
+        std::vector<uint32_t> cur_caps = caps;
+        uint64_t retries = 0;
+        bool overflow = false;
+        for (int pass = 0; pass < 12 && !work.empty(); ++pass) {
+            std::vector<Launch> plan;
+            std::vector<uint32_t> cls;   // shared-memory classes by capacity
+            Launch glob; glob.smem = false;
+            uint64_t arena_slots = 0;
+            for (uint32_t g : work) {
+                const uint32_t cap = cur_caps[g];
+                if (cap <= smem_max) {
+                    size_t i = 0;
+                    while (i < plan.size() && plan[i].smem_cap != cap) ++i;
+                    if (i == plan.size()) { plan.emplace_back(); plan.back().smem = true; plan.back().smem_cap = cap; }
+                    plan[i].list.push_back(g);
+                } else {
+                    glob.list.push_back(g); glob.off.push_back(arena_slots); glob.cap.push_back(cap);
+                    arena_slots += cap;
+                }
+            }
+            plan.push_back(glob);
+            CK(cudaMemsetAsync(&c->counters.as<Counters>()->retry_count, 0, sizeof(unsigned long long), c->stream));
+            rc = launch_plan(c, plan, arena_slots);
+            if (rc) return rc;
+            Counters h{};
+            MiscWords m{};
+            CK(cudaMemcpyAsync(&h, c->counters.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaMemcpyAsync(&m, c->misc.p, sizeof(m), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            rc = check_err_word(c, m.err);
+            if (rc) return rc;
+            if (m.err & (DERR_OUT_OVERFLOW | DERR_DUMP_OVERFLOW)) {
+                fasta_need = std::max<uint64_t>(fasta_need, h.fasta_bytes) * 2;
+                lm_text_need = std::max<uint64_t>(lm_text_need, h.lm_bytes) * 2;
+                lm_need = std::max<uint64_t>(lm_need, h.lm_count) * 2;
+                CK(cudaMemsetAsync(&c->misc.as<MiscWords>()->err, 0, sizeof(uint32_t), c->stream));
+                overflow = true;
+                break;
+            }
+            work.clear();
+            if (h.retry_count) {
+                work.resize(h.retry_count);
+                CK(cudaMemcpyAsync(work.data(), c->retry.p, 4 * h.retry_count, cudaMemcpyDeviceToHost, c->stream));
+                CK(cudaStreamSynchronize(c->stream));
+                retries += h.retry_count;
+                for (uint32_t g : work) {
+                    if (cur_caps[g] >= (1u << 30)) return fail(c, CFG_ERR_TABLE_FULL, "subgraph table exceeded 2^30 slots");
+                    cur_caps[g] = std::max<uint32_t>(cur_caps[g] * 4, smem_max * 2);
+                }
+            }
+        }
+        if (overflow) continue;
+        if (!work.empty()) return fail(c, CFG_ERR_TABLE_FULL, "subgraph tables kept overflowing");
+        Counters h{};
+        CK(cudaMemcpyAsync(&h, c->counters.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        cfg_counts& o = c->counts;
+        o.n_bases = c->n_bases; o.n_records = c->n_records; o.n_instances = c->n_instances;
+        o.n_vertices = h.vertices; o.n_isolated = h.isolated; o.n_phantom = h.phantom;
+        o.n_trivial = h.trivial; o.n_icc = h.icc; o.n_lmtig = h.lm_count;
+        o.fasta_bytes = h.fasta_bytes; o.lmtig_bytes = h.lm_bytes; o.n_retries = retries;
+        c->dump_n = h.dump_count;
+        return CFG_OK;
+    }
+    return fail(c, CFG_ERR_OOM, "output arenas kept overflowing");
+}
+
+}  // namespace
+
+extern "C" {
+
+int cfg_create(int device, const cfg_params* params, cfg_ctx** out) {
+    if (!out) return CFG_ERR_BAD_INPUT;
+    *out = nullptr;
+    if (!params) return CFG_ERR_BAD_INPUT;
+    const cfg_params& p = *params;
+    if (p.k < 3 || p.k > 63 || (p.k % 2) == 0) return CFG_ERR_BAD_INPUT;
+    if (p.l < 1 || p.l > 32 || p.l > p.k - 1) return CFG_ERR_BAD_INPUT;
+    if (p.cutoff < 1 || p.cutoff > 15) return CFG_ERR_BAD_INPUT;
+    if (p.graph_count == 0 || p.graph_count > 65536 || (p.graph_count & (p.graph_count - 1))) return CFG_ERR_BAD_INPUT;
+    int n_dev = 0;
+    if (cudaGetDeviceCount(&n_dev) != cudaSuccess || device < 0 || device >= n_dev) { cudaGetLastError(); return CFG_ERR_CUDA; }
+    if (cudaSetDevice(device) != cudaSuccess) return CFG_ERR_CUDA;
+    cfg_ctx* c = new (std::nothrow) cfg_ctx();
+    if (!c) return CFG_ERR_OOM;
+    c->device = device; c->p = p; c->G = p.graph_count; c->words = p.k <= 31 ? 1 : 2;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return CFG_ERR_CUDA; }
+    for (auto& e : c->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) { cfg_destroy(c); return CFG_ERR_CUDA; }
+    *out = c;
+    return CFG_OK;
+}
+
+static int check_frags(cfg_ctx* c, uint64_t n_bases, const uint64_t* frag_off, const uint32_t* frag_len, uint64_t n_frags) {
+    if (n_bases >= (1ull << 32)) return fail(c, CFG_ERR_BAD_INPUT, "a job must hold fewer than 2^32 bases");
+    uint64_t at = 0;
+    for (uint64_t i = 0; i < n_frags; ++i) {
+        if (frag_off[i] != at) return fail(c, CFG_ERR_BAD_INPUT, "fragments must be back-to-back in input order");
+        if (frag_len[i] < c->p.k + 1) return fail(c, CFG_ERR_BAD_INPUT, "fragments must hold at least k+1 bases");
+        at += frag_len[i];
+    }
+    if (at != n_bases) return fail(c, CFG_ERR_BAD_INPUT, "fragment lengths do not sum to n_bases");
+    return CFG_OK;
+}
+
+int cfg_submit_packed(cfg_ctx* c, const uint64_t* packed, uint64_t n_bases, const uint64_t* frag_off,
+                      const uint32_t* frag_len, uint64_t n_frags) {
+    if (!c || (n_bases && !packed) || (n_frags && (!frag_off || !frag_len))) return fail(c, CFG_ERR_BAD_INPUT, "null input");
+    int rc = check_frags(c, n_bases, frag_off, frag_len, n_frags);
+    if (rc) return rc;
+    CK(cudaSetDevice(c->device));
+    const uint64_t words = (n_bases + 31) / 32;
+    if (!c->packed.ensure(8 * (words + 4)) || !c->frag_off.ensure(8 * (n_frags + 1)) || !c->frag_len.ensure(4 * (n_frags + 1)))
+        return fail(c, CFG_ERR_OOM, "input buffers");
+    CK(cudaMemsetAsync(c->packed.p, 0, 8 * (words + 4), c->stream));
+    if (words) CK(cudaMemcpyAsync(c->packed.p, packed, 8 * words, cudaMemcpyHostToDevice, c->stream));
+    if (n_frags) {
+        CK(cudaMemcpyAsync(c->frag_off.p, frag_off, 8 * n_frags, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->frag_len.p, frag_len, 4 * n_frags, cudaMemcpyHostToDevice, c->stream));
+    }
+    c->d_packed = c->packed.as<uint64_t>(); c->d_frag_off = c->frag_off.as<uint64_t>(); c->d_frag_len = c->frag_len.as<uint32_t>();
+    c->n_bases = n_bases; c->n_frags = n_frags;
+    c->have_input = true; c->have_run = false;
+    return CFG_OK;
+}
+
+int cfg_submit_packed_device(cfg_ctx* c, const uint64_t* d_packed, uint64_t n_bases, const uint64_t* d_frag_off,
+                             const uint32_t* d_frag_len, uint64_t n_frags) {
+    if (!c || (n_bases && !d_packed) || (n_frags && (!d_frag_off || !d_frag_len))) return fail(c, CFG_ERR_BAD_INPUT, "null input");
+    if (n_bases >= (1ull << 32)) return fail(c, CFG_ERR_BAD_INPUT, "a job must hold fewer than 2^32 bases");
+    c->d_packed = d_packed; c->d_frag_off = d_frag_off; c->d_frag_len = d_frag_len;
+    c->n_bases = n_bases; c->n_frags = n_frags;
+    c->have_input = true; c->have_run = false;
+    return CFG_OK;
+}
+
+int cfg_run(cfg_ctx* c) {
+    if (!c) return CFG_ERR_BAD_INPUT;
+    if (!c->have_input) return fail(c, CFG_ERR_STATE, "cfg_run before cfg_submit_packed");
+    CK(cudaSetDevice(c->device));
+    c->err.clear();
+    c->have_run = false;
+    c->counts = cfg_counts{};
+    CK(cudaEventRecord(c->ev[0], c->stream));
+    std::vector<uint32_t> inst_h, off_h;
+    int rc = run_partition(c, inst_h, off_h);
+    if (rc) return rc;
+    rc = run_subgraphs(c, inst_h);
+    if (rc) return rc;
+    CK(cudaEventRecord(c->ev[3], c->stream));
+    CK(cudaEventSynchronize(c->ev[3]));
+    float t01 = 0, t12 = 0, t23 = 0, t03 = 0;
+    cudaEventElapsedTime(&t01, c->ev[0], c->ev[1]);
+    cudaEventElapsedTime(&t12, c->ev[1], c->ev[2]);
+    cudaEventElapsedTime(&t23, c->ev[2], c->ev[3]);
+    cudaEventElapsedTime(&t03, c->ev[0], c->ev[3]);
+    c->times[0] = t01; c->times[1] = t12; c->times[2] = t23; c->times[3] = t03;
+    c->have_run = true;
+    return CFG_OK;
+}
+
+int cfg_fetch_counts(cfg_ctx* c, cfg_counts* out) {
+    if (!c || !out) return CFG_ERR_BAD_INPUT;
+    if (!c->have_run) return fail(c, CFG_ERR_STATE, "no completed run");
+    *out = c->counts;
+    return CFG_OK;
+}
+
+int cfg_fetch(cfg_ctx* c, cfg_results* out) {
+    if (!c || !out) return CFG_ERR_BAD_INPUT;
+    if (!c->have_run) return fail(c, CFG_ERR_STATE, "no completed run");
+    CK(cudaSetDevice(c->device));
+    const cfg_counts& n = c->counts;
+    c->h_fasta.resize(n.fasta_bytes);
+    c->h_lm_text.resize(n.lmtig_bytes);
+    c->h_lm.resize(n.n_lmtig);
+    if (n.fasta_bytes) CK(cudaMemcpyAsync(c->h_fasta.data(), c->fasta.p, n.fasta_bytes, cudaMemcpyDeviceToHost, c->stream));
+    if (n.lmtig_bytes) CK(cudaMemcpyAsync(c->h_lm_text.data(), c->lm_text.p, n.lmtig_bytes, cudaMemcpyDeviceToHost, c->stream));
+    static_assert(sizeof(cfg_lmtig) == sizeof(LmtigOut), "lm-tig record layout");
+    if (n.n_lmtig) CK(cudaMemcpyAsync(c->h_lm.data(), c->lm.p, n.n_lmtig * sizeof(cfg_lmtig), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    out->counts = n;
+    out->fasta = c->h_fasta.data();
+    out->lmtig_text = c->h_lm_text.data();
+    out->lmtigs = c->h_lm.data();
+    return CFG_OK;
+}
+
+int cfg_dump_states(cfg_ctx* c, cfg_state_dump* out) {
+    if (!c || !out) return CFG_ERR_BAD_INPUT;
+    if (!c->have_run) return fail(c, CFG_ERR_STATE, "no completed run");
+    if (!(c->p.flags & CFG_FLAG_DUMP_STATES)) return fail(c, CFG_ERR_STATE, "context created without CFG_FLAG_DUMP_STATES");
+    static_assert(sizeof(cfg_state) == sizeof(StateOut), "state layout");
+    c->h_states.resize(c->dump_n);
+    if (c->dump_n) {
+        CK(cudaMemcpyAsync(c->h_states.data(), c->dump.p, c->dump_n * sizeof(cfg_state), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    out->n = c->dump_n;
+    out->states = c->h_states.data();
+    return CFG_OK;
+}
+
+int cfg_dump_records(cfg_ctx* c, cfg_record_dump* out) {
+    if (!c || !out) return CFG_ERR_BAD_INPUT;
+    if (!c->have_run) return fail(c, CFG_ERR_STATE, "no completed run");
+    if (!(c->p.flags & CFG_FLAG_DUMP_RECORDS)) return fail(c, CFG_ERR_STATE, "context created without CFG_FLAG_DUMP_RECORDS");
+    std::vector<uint64_t> raw(c->n_records);
+    if (c->n_records) {
+        CK(cudaMemcpyAsync(raw.data(), c->recs.p, 8 * c->n_records, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    c->h_records.resize(c->n_records);
+    for (uint64_t i = 0; i < c->n_records; ++i) {
+        const uint64_t r = raw[i];
+        c->h_records[i] = cfg_record{rec_pos(r), (uint8_t)rec_len(r), (uint8_t)(rec_ld(r) | (rec_rd(r) << 1)), (uint16_t)rec_g(r)};
+    }
+    out->n = c->n_records;
+    out->records = c->h_records.data();
+    return CFG_OK;
+}
+
+int cfg_last_timings(cfg_ctx* c, float out_ms[4]) {
+    if (!c || !out_ms) return CFG_ERR_BAD_INPUT;
+    if (!c->have_run) return fail(c, CFG_ERR_STATE, "no completed run");
+    for (int i = 0; i < 4; ++i) out_ms[i] = c->times[i];
+    return CFG_OK;
+}
+
+const char* cfg_last_error_string(cfg_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+void cfg_destroy(cfg_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    DevBuf* bufs[] = {&c->packed, &c->frag_off, &c->frag_len, &c->flat, &c->hist, &c->misc, &c->bucket_off, &c->inst,
+                      &c->fill, &c->recs, &c->list, &c->tab_off, &c->tab_cap, &c->arena, &c->fasta, &c->lm_text,
+                      &c->lm, &c->dump, &c->retry, &c->counters};
+    for (DevBuf* b : bufs) b->release();
+    for (auto& e : c->ev) if (e) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+}  // extern "C"

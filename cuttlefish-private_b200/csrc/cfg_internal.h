@@ -1,0 +1,108 @@
+// cfg_internal.h -- launch interface between the C ABI (cfg_api.cu) and the kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cfg {
+
+// A weak super k-mer packed in 64 bits: start in the packed stream (bits 0-31),
+// length in bases (32-39), l_disc (40), r_disc (41), subgraph (48-63).  It is the
+// reference's Super_Kmer_Attributes<false> (include/Super_Kmer_Attributes.hpp:25-61)
+// with the label replaced by its position in the resident 2-bit input.
+__host__ __device__ inline uint64_t rec_pack(uint32_t pos, uint32_t len, uint32_t ld, uint32_t rd, uint32_t g) {
+    return (uint64_t)pos | ((uint64_t)len << 32) | ((uint64_t)ld << 40) | ((uint64_t)rd << 41) | ((uint64_t)g << 48);
+}
+__host__ __device__ inline uint32_t rec_pos(uint64_t r) { return (uint32_t)r; }
+__host__ __device__ inline uint32_t rec_len(uint64_t r) { return (uint32_t)(r >> 32) & 0xFF; }
+__host__ __device__ inline uint32_t rec_ld(uint64_t r) { return (uint32_t)(r >> 40) & 1; }
+__host__ __device__ inline uint32_t rec_rd(uint64_t r) { return (uint32_t)(r >> 41) & 1; }
+__host__ __device__ inline uint32_t rec_g(uint64_t r) { return (uint32_t)(r >> 48); }
+
+// Device error word bits.
+enum : uint32_t {
+    DERR_REC_OVERFLOW = 1u,    // flat record buffer too small (recoverable: regrow + rerun)
+    DERR_OUT_OVERFLOW = 2u,    // output arenas too small (recoverable)
+    DERR_MISSING_KEY = 4u,     // a neighbour k-mer was not in its subgraph's table (bug guard)
+    DERR_WALK_LIMIT = 8u,      // a walk exceeded its step bound (bug guard)
+    DERR_CAS_LIMIT = 16u,      // a CAS retry loop exceeded its bound (bug guard)
+    DERR_DUMP_OVERFLOW = 32u,  // state dump buffer too small (recoverable)
+};
+
+struct PartitionArgs {
+    const uint64_t* packed;
+    const uint64_t* frag_off;
+    const uint32_t* frag_len;
+    uint64_t n_frags;
+    uint64_t n_bases;
+    uint32_t k, l, w;           // w = k - l
+    uint32_t gmask;
+    uint64_t seed0;             // wyhash seed after its first mix
+    uint32_t seg;               // stream bases per warp segment
+    uint64_t* recs;             // flat records
+    uint64_t rec_cap;
+    unsigned long long* rec_cursor;
+    unsigned long long* hist;   // per subgraph: records (low 32) | instances (high 32)
+    uint32_t* err;
+};
+
+struct ScatterArgs {
+    const uint64_t* flat;
+    uint64_t n;
+    const uint32_t* bucket_off;  // G + 1 offsets
+    uint32_t* bucket_fill;       // G counters, zeroed
+    uint64_t* recs;              // bucketed
+};
+
+struct LmtigOut {                // mirrors cfg_lmtig
+    uint64_t u[2], v[2];
+    uint64_t label_off;
+    uint32_t label_len;
+    uint16_t g;
+    uint8_t flags, pad;
+};
+
+struct StateOut {                // mirrors cfg_state
+    uint64_t key[2];
+    uint32_t ef;
+    uint16_t g;
+    uint8_t status, pad;
+};
+
+struct Counters {                // device-side counters of the subgraph phase
+    unsigned long long vertices, isolated, phantom, trivial, icc, lmtig;
+    unsigned long long fasta_bytes, lm_bytes, lm_count, dump_count, retry_count;
+};
+
+struct SubgraphArgs {
+    const uint64_t* packed;
+    const uint64_t* recs;        // bucketed records
+    const uint32_t* bucket_off;  // G + 1
+    const uint32_t* list;        // subgraphs of this launch
+    uint32_t n_list;
+    const uint64_t* tab_off;     // global path: per-list-entry table offset (slots) into the arena
+    const uint32_t* tab_cap;     // global path: per-list-entry capacity (power of two)
+    uint32_t smem_cap;           // shared path: capacity of every table of this launch
+    unsigned char* arena;        // global path tables
+    uint32_t k, fth;
+    uint32_t load_limit_pct;     // a table fuller than this is abandoned and retried larger
+    char* fasta; uint64_t fasta_cap;
+    char* lm_text; uint64_t lm_text_cap;
+    LmtigOut* lm; uint64_t lm_cap;
+    StateOut* dump; uint64_t dump_cap;
+    uint32_t* retry;             // subgraphs whose table overflowed
+    Counters* cnt;
+    uint32_t* err;
+};
+
+// bytes per table slot
+__host__ __device__ inline uint32_t slot_bytes(int words) { return words == 1 ? 28u : 36u; }
+
+void launch_partition(const PartitionArgs& a, cudaStream_t s);
+void launch_bucket_scan(const unsigned long long* hist, uint32_t G, uint32_t* bucket_off, uint32_t* inst,
+                        uint32_t* fill, cudaStream_t s);
+void launch_scatter(const ScatterArgs& a, cudaStream_t s);
+void launch_subgraphs(const SubgraphArgs& a, int words, bool smem, uint32_t threads, cudaStream_t s);
+int subgraph_max_smem_cap(int words);
+
+}  // namespace cfg

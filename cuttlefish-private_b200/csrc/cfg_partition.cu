@@ -1,0 +1,234 @@
+// cfg_partition.cu -- K1: weak super k-mer partitioning and bucket scatter.
+//
+// Restates Graph_Partitioner::process_chunk (src/Graph_Partitioner.cpp:505-597)
+// with Min_Iterator<k-1> (include/Minimizer_Iterator.hpp:306-378) as a
+// data-parallel sweep.  For every (k-1)-mer j of a fragment the subgraph is
+// g_j = (min over its k-l l-mers of min(wyhash(l-mer), wyhash(rc(l-mer)))) & (G-1).
+// The sequential cut rule (cut where g changes, or where the super (k-1)-mer
+// reaches 2(k-1)-l bases) is equivalent to: pieces start at every g change and
+// then every k-l (k-1)-mers inside a run of equal g.  So a run's pieces depend
+// only on where the run starts, and a warp can own every run that starts in its
+// stream segment, continuing past the segment's end until that run ends.
+#include "cfg_device.cuh"
+#include "cfg_internal.h"
+
+namespace cfg {
+
+namespace {
+
+constexpr int RING = 128;             // per-warp ring of l-mer hashes (w <= 62)
+constexpr int WARPS_PER_BLOCK = 8;
+
+__device__ __forceinline__ uint32_t lanemask_lt() { uint32_t m; asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m)); return m; }
+
+__device__ __forceinline__ uint64_t lmer_at(const uint64_t* __restrict__ s, uint64_t p, uint32_t l) {
+    return window64(s, p) >> (64 - 2 * l);
+}
+
+// Processes the (k-1)-mer positions [j0, j1) of one fragment: emits every weak
+// super k-mer whose run starts there.
+__device__ void sweep_fragment(const PartitionArgs& a, uint64_t* ring, uint64_t F0, uint32_t FL, uint32_t j0, uint32_t j1) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t k = a.k, l = a.l, w = a.w;
+    const uint32_t M = FL - k + 2;                 // (k-1)-mers in the fragment
+    const uint32_t n_lmers = FL - l + 1;
+    const uint32_t start = j0 == 0 ? 0 : j0 - 1;   // position j0-1 only primes the change test
+
+    // l-mers [start, start + w - 1) before the first chunk
+    for (uint32_t q = start + lane; q < start + w - 1; q += 32)
+        if (q < n_lmers) ring[q & (RING - 1)] = lmer_hash(lmer_at(a.packed, F0 + q, l), l, a.seed0);
+
+    bool active = false;
+    uint32_t r0 = 0, run_start = 0, last_cut = 0, last_cut_g = 0, last_cut_chg = 0, carry_g = 0;
+
+    for (uint32_t base = start;; base += 32) {
+        __syncwarp();
+        {
+            const uint32_t q = base + w - 1 + lane;
+            if (q < n_lmers) ring[q & (RING - 1)] = lmer_hash(lmer_at(a.packed, F0 + q, l), l, a.seed0);
+        }
+        __syncwarp();
+        const uint32_t j = base + lane;
+        const bool valid = j < M;
+        uint32_t g = 0;
+        if (valid) {
+            uint64_t m = ~0ull;
+            for (uint32_t t = 0; t < w; ++t) {
+                const uint64_t h = ring[(j + t) & (RING - 1)];
+                m = h < m ? h : m;
+            }
+            g = (uint32_t)m & a.gmask;
+        }
+        uint32_t gprev = __shfl_up_sync(0xffffffffu, g, 1);
+        if (lane == 0) gprev = carry_g;
+        const bool is_chg = valid && j >= j0 && (j == 0 || gprev != g);
+        const uint32_t chg = __ballot_sync(0xffffffffu, is_chg);
+
+        bool just_activated = false;
+        uint32_t r0_lane = 0;
+        if (!active) {
+            if (chg == 0) {
+                if (base + 32 >= j1 || base + 32 >= M) return;   // no run starts in [j0, j1)
+                carry_g = __shfl_sync(0xffffffffu, g, 31);
+                continue;
+            }
+            r0_lane = __ffs(chg) - 1;
+            r0 = base + r0_lane;
+            if (r0 >= j1) return;
+            active = true; just_activated = true;
+            run_start = r0; last_cut = r0;
+            last_cut_g = __shfl_sync(0xffffffffu, g, r0_lane);
+            last_cut_chg = 1;
+        }
+        const uint32_t act_mask = just_activated ? (0xffffffffu << r0_lane) : 0xffffffffu;
+
+        // run start of each position: highest change at or below it, else the carried one
+        const uint32_t le = chg & (lanemask_lt() | (1u << lane));
+        const uint32_t rs = le ? base + (31 - __clz(le)) : run_start;
+        const bool is_cut = valid && ((act_mask >> lane) & 1) && (is_chg || ((j - rs) % w) == 0);
+        uint32_t cut = __ballot_sync(0xffffffffu, is_cut);
+
+        // stop at the first change at or past j1: the run it starts belongs to the next segment
+        bool stopping = false;
+        {
+            const uint32_t past = __ballot_sync(0xffffffffu, valid && j >= j1);
+            const uint32_t stop = chg & past;
+            if (stop) {
+                const uint32_t sl = __ffs(stop) - 1;
+                cut &= (sl == 31) ? 0xffffffffu : ((2u << sl) - 1);
+                stopping = true;
+            }
+        }
+        uint32_t emit = cut;
+        if (just_activated) emit &= ~(1u << r0_lane);
+
+        // piece [c, c') ends at every emitting lane c' = j
+        const uint32_t below = cut & lanemask_lt();
+        const uint32_t pl = below ? (31 - __clz(below)) : 0;
+        const uint32_t pg = __shfl_sync(0xffffffffu, g, pl);
+        const uint32_t pchg = __shfl_sync(0xffffffffu, (uint32_t)is_chg, pl);
+        const bool fin = !stopping && (base + 32 >= M);      // the fragment's last (k-1)-mer is in this chunk
+        const uint32_t n_emit = __popc(emit) + (fin ? 1 : 0);
+        unsigned long long slot0 = 0;
+        if (n_emit) {
+            if (lane == 0) slot0 = atomicAdd(a.rec_cursor, (unsigned long long)n_emit);
+            slot0 = __shfl_sync(0xffffffffu, slot0, 0);
+        }
+        if ((emit >> lane) & 1) {
+            const uint32_t c = below ? base + pl : last_cut;
+            const uint32_t cg = below ? pg : last_cut_g;
+            const uint32_t cchg = below ? pchg : last_cut_chg;
+            const uint32_t lj = c > 0;
+            const uint32_t len = lj + (j - c + k - 2) + 1;
+            const uint64_t r = rec_pack((uint32_t)(F0 + c - lj), len, lj & cchg, is_chg ? 1u : 0u, cg);
+            const unsigned long long idx = slot0 + __popc(emit & lanemask_lt());
+            if (idx < a.rec_cap) a.recs[idx] = r; else atomicOr(a.err, DERR_REC_OVERFLOW);
+            atomicAdd(a.hist + cg, 1ull | ((unsigned long long)(len - k + 1) << 32));
+        }
+        // carries: last cut / run start of this chunk
+        if (cut) {
+            const uint32_t hl = 31 - __clz(cut);
+            last_cut = base + hl;
+            last_cut_g = __shfl_sync(0xffffffffu, g, hl);
+            last_cut_chg = __shfl_sync(0xffffffffu, (uint32_t)is_chg, hl);
+        }
+        if (chg) run_start = base + (31 - __clz(chg));
+        carry_g = __shfl_sync(0xffffffffu, g, 31);
+        if (fin && lane == 0) {   // final piece [last_cut, M): not joined on the right
+            const uint32_t c = last_cut, lj = c > 0;
+            const uint32_t len = lj + (FL - c);
+            const uint64_t r = rec_pack((uint32_t)(F0 + c - lj), len, lj & last_cut_chg, 0, last_cut_g);
+            const unsigned long long idx = slot0 + __popc(emit);
+            if (idx < a.rec_cap) a.recs[idx] = r; else atomicOr(a.err, DERR_REC_OVERFLOW);
+            atomicAdd(a.hist + last_cut_g, 1ull | ((unsigned long long)(len - k + 1) << 32));
+        }
+        if (stopping || fin) return;
+    }
+}
+
+__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_partition(const PartitionArgs a) {
+    __shared__ uint64_t rings[WARPS_PER_BLOCK][RING];
+    uint64_t* ring = rings[threadIdx.x >> 5];
+    const uint64_t n_seg = (a.n_bases + a.seg - 1) / a.seg;
+    const uint64_t warp0 = (uint64_t)blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5);
+    const uint64_t n_warps = (uint64_t)gridDim.x * WARPS_PER_BLOCK;
+    for (uint64_t sgi = warp0; sgi < n_seg; sgi += n_warps) {
+        const uint64_t s0 = sgi * a.seg, s1 = min(s0 + a.seg, a.n_bases);
+        // last fragment starting at or before s0
+        uint64_t lo = 0, hi = a.n_frags;
+        while (hi - lo > 1) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (a.frag_off[mid] <= s0) lo = mid; else hi = mid;
+        }
+        for (uint64_t f = lo; f < a.n_frags; ++f) {
+            const uint64_t F0 = a.frag_off[f];
+            if (F0 >= s1) break;
+            const uint32_t FL = a.frag_len[f];
+            const uint32_t M = FL - a.k + 2;
+            const uint32_t j0 = s0 > F0 ? (uint32_t)(s0 - F0) : 0;
+            const uint64_t e = s1 - F0;
+            const uint32_t j1 = e < M ? (uint32_t)e : M;
+            if (j0 < j1) sweep_fragment(a, ring, F0, FL, j0, j1);
+        }
+    }
+}
+
+// Exclusive scan of the per-subgraph record counts (one block).
+__global__ void __launch_bounds__(1024) k_bucket_scan(const unsigned long long* __restrict__ hist, uint32_t G,
+                                                      uint32_t* bucket_off, uint32_t* inst, uint32_t* fill) {
+    __shared__ uint32_t part[1024];
+    const uint32_t t = threadIdx.x;
+    const uint32_t per = (G + 1023) / 1024;
+    const uint32_t b0 = t * per, b1 = min(b0 + per, G);
+    uint32_t sum = 0;
+    for (uint32_t b = b0; b < b1; ++b) sum += (uint32_t)hist[b];
+    part[t] = sum;
+    __syncthreads();
+    for (uint32_t d = 1; d < 1024; d <<= 1) {
+        const uint32_t v = t >= d ? part[t - d] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    uint32_t run = part[t] - sum;
+    for (uint32_t b = b0; b < b1; ++b) {
+        bucket_off[b] = run;
+        run += (uint32_t)hist[b];
+        inst[b] = (uint32_t)(hist[b] >> 32);
+        fill[b] = 0;
+    }
+    if (t == 1023) bucket_off[G] = part[1023];
+}
+
+__global__ void k_scatter(const ScatterArgs a) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t r = a.flat[i];
+        const uint32_t g = rec_g(r);
+        const uint32_t slot = atomicAdd(a.bucket_fill + g, 1u);
+        a.recs[a.bucket_off[g] + slot] = r;
+    }
+}
+
+}  // namespace
+
+void launch_partition(const PartitionArgs& a, cudaStream_t s) {
+    const uint64_t n_seg = (a.n_bases + a.seg - 1) / a.seg;
+    uint64_t blocks = (n_seg + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
+    if (blocks > (1u << 20)) blocks = 1u << 20;
+    if (blocks == 0) return;
+    k_partition<<<(unsigned)blocks, WARPS_PER_BLOCK * 32, 0, s>>>(a);
+}
+
+void launch_bucket_scan(const unsigned long long* hist, uint32_t G, uint32_t* bucket_off, uint32_t* inst,
+                        uint32_t* fill, cudaStream_t s) {
+    k_bucket_scan<<<1, 1024, 0, s>>>(hist, G, bucket_off, inst, fill);
+}
+
+void launch_scatter(const ScatterArgs& a, cudaStream_t s) {
+    if (a.n == 0) return;
+    uint64_t blocks = (a.n + 255) / 256;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    k_scatter<<<(unsigned)blocks, 256, 0, s>>>(a);
+}
+
+}  // namespace cfg

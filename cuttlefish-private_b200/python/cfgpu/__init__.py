@@ -1,0 +1,251 @@
+"""ctypes binding of the B200 compaction library (``include/cuttlefish_gpu.h``).
+
+The library is ``cuttlefish-private_b200/lib/libcfgpu.so`` built by the package
+Makefile.  Loading fails loudly when it is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "libcfgpu.so")
+
+CFG_FLAG_DUMP_STATES = 0x1
+CFG_FLAG_DUMP_RECORDS = 0x2
+
+ERRORS = {0: "OK", 1: "BAD_INPUT", 2: "OOM", 3: "TABLE_FULL", 4: "WALK_LIMIT", 5: "CUDA", 6: "STATE"}
+
+U64P = ctypes.POINTER(ctypes.c_uint64)
+U32P = ctypes.POINTER(ctypes.c_uint32)
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("k", ctypes.c_uint32), ("l", ctypes.c_uint32), ("cutoff", ctypes.c_uint32),
+                ("graph_count", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+                ("table_load_pct", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 2)]
+
+
+class Counts(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in (
+        "n_bases", "n_records", "n_instances", "n_vertices", "n_isolated", "n_phantom", "n_trivial",
+        "n_icc", "n_lmtig", "fasta_bytes", "lmtig_bytes", "n_retries")]
+
+
+class Lmtig(ctypes.Structure):
+    _fields_ = [("u", ctypes.c_uint64 * 2), ("v", ctypes.c_uint64 * 2), ("label_off", ctypes.c_uint64),
+                ("label_len", ctypes.c_uint32), ("g", ctypes.c_uint16), ("flags", ctypes.c_uint8),
+                ("pad", ctypes.c_uint8)]
+
+
+class Results(ctypes.Structure):
+    _fields_ = [("counts", Counts), ("fasta", ctypes.c_void_p), ("lmtig_text", ctypes.c_void_p),
+                ("lmtigs", ctypes.POINTER(Lmtig))]
+
+
+class State(ctypes.Structure):
+    _fields_ = [("key", ctypes.c_uint64 * 2), ("ef", ctypes.c_uint32), ("g", ctypes.c_uint16),
+                ("status", ctypes.c_uint8), ("pad", ctypes.c_uint8)]
+
+
+class StateDump(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint64), ("states", ctypes.POINTER(State))]
+
+
+class Record(ctypes.Structure):
+    _fields_ = [("pos", ctypes.c_uint32), ("len", ctypes.c_uint8), ("flags", ctypes.c_uint8), ("g", ctypes.c_uint16)]
+
+
+class RecordDump(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint64), ("records", ctypes.POINTER(Record))]
+
+
+class Packed(ctypes.Structure):
+    _fields_ = [("n_bases", ctypes.c_uint64), ("n_frags", ctypes.c_uint64), ("words", U64P),
+                ("frag_off", U64P), ("frag_len", U32P), ("pinned", ctypes.c_int)]
+
+
+# every exported entry point with its ctypes signature
+SIGNATURES = {
+    "cfg_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(Params), ctypes.POINTER(ctypes.c_void_p)]),
+    "cfg_submit_packed": (ctypes.c_int, [ctypes.c_void_p, U64P, ctypes.c_uint64, U64P, U32P, ctypes.c_uint64]),
+    "cfg_submit_packed_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                                ctypes.c_void_p, ctypes.c_uint64]),
+    "cfg_run": (ctypes.c_int, [ctypes.c_void_p]),
+    "cfg_fetch": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Results)]),
+    "cfg_fetch_counts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Counts)]),
+    "cfg_dump_states": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(StateDump)]),
+    "cfg_dump_records": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(RecordDump)]),
+    "cfg_last_timings": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
+    "cfg_last_error_string": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "cfg_destroy": (None, [ctypes.c_void_p]),
+    "cfg_pack_records": (ctypes.c_int, [ctypes.c_char_p, U64P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int,
+                                        ctypes.POINTER(Packed)]),
+    "cfg_packed_free": (None, [ctypes.POINTER(Packed)]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads libcfgpu.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `make -C cuttlefish-private_b200` "
+                           "(there is no CPU fallback)")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class CfgError(RuntimeError):
+    pass
+
+
+def _check(lib, ctx, rc, what):
+    if rc != 0:
+        msg = lib.cfg_last_error_string(ctx) if ctx else b""
+        raise CfgError(f"{what}: {ERRORS.get(rc, rc)} {msg.decode(errors='replace') if msg else ''}")
+
+
+def concat_records(records):
+    """records: iterable of str/bytes -> (bytes, offsets array)."""
+    bs = [r.encode() if isinstance(r, str) else bytes(r) for r in records]
+    data = b"".join(bs)
+    offs = [0]
+    for b in bs:
+        offs.append(offs[-1] + len(b))
+    return data, (ctypes.c_uint64 * len(offs))(*offs), len(bs)
+
+
+class PackedInput:
+    """Fragments of a set of records, packed 2 bits per base (cfg_pack_records)."""
+
+    def __init__(self, records, k: int, pinned: bool = False, data_offsets=None):
+        self.lib = load()
+        self.p = Packed()
+        if data_offsets is None:
+            data, offs, n = concat_records(records)
+        else:
+            data, offs, n = data_offsets
+        rc = self.lib.cfg_pack_records(data, offs, n, k, 1 if pinned else 0, ctypes.byref(self.p))
+        _check(self.lib, None, rc, "cfg_pack_records")
+
+    @property
+    def n_bases(self):
+        return self.p.n_bases
+
+    def close(self):
+        if self.p.words:
+            self.lib.cfg_packed_free(ctypes.byref(self.p))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class LmtigRec:
+    u: tuple
+    v: tuple
+    label: str
+    g: int
+    flags: int
+
+
+class Compactor:
+    """One GPU context (cfg_ctx): submit -> run -> fetch."""
+
+    def __init__(self, k: int, l: int = 20, cutoff: int = 1, graph_count: int = 16384, device: int = 0,
+                 flags: int = 0, table_load_pct: int = 0):
+        self.lib = load()
+        self.k = k
+        self.params = Params(k, l, cutoff, graph_count, flags, table_load_pct)
+        ctx = ctypes.c_void_p()
+        rc = self.lib.cfg_create(device, ctypes.byref(self.params), ctypes.byref(ctx))
+        _check(self.lib, None, rc, "cfg_create")
+        self.ctx = ctx
+
+    def close(self):
+        if self.ctx:
+            self.lib.cfg_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def submit(self, packed: PackedInput):
+        p = packed.p
+        rc = self.lib.cfg_submit_packed(self.ctx, p.words, p.n_bases, p.frag_off, p.frag_len, p.n_frags)
+        _check(self.lib, self.ctx, rc, "cfg_submit_packed")
+
+    def submit_device(self, d_words: int, n_bases: int, d_frag_off: int, d_frag_len: int, n_frags: int):
+        rc = self.lib.cfg_submit_packed_device(self.ctx, d_words, n_bases, d_frag_off, d_frag_len, n_frags)
+        _check(self.lib, self.ctx, rc, "cfg_submit_packed_device")
+
+    def run(self):
+        _check(self.lib, self.ctx, self.lib.cfg_run(self.ctx), "cfg_run")
+
+    def counts(self) -> Counts:
+        c = Counts()
+        _check(self.lib, self.ctx, self.lib.cfg_fetch_counts(self.ctx, ctypes.byref(c)), "cfg_fetch_counts")
+        return c
+
+    def timings(self):
+        t = (ctypes.c_float * 4)()
+        _check(self.lib, self.ctx, self.lib.cfg_last_timings(self.ctx, t), "cfg_last_timings")
+        return list(t)
+
+    def fetch(self):
+        r = Results()
+        _check(self.lib, self.ctx, self.lib.cfg_fetch(self.ctx, ctypes.byref(r)), "cfg_fetch")
+        fasta = ctypes.string_at(r.fasta, r.counts.fasta_bytes) if r.counts.fasta_bytes else b""
+        text = ctypes.string_at(r.lmtig_text, r.counts.lmtig_bytes) if r.counts.lmtig_bytes else b""
+        lms = []
+        for i in range(r.counts.n_lmtig):
+            m = r.lmtigs[i]
+            lab = text[m.label_off:m.label_off + m.label_len].decode()
+            lms.append(LmtigRec((m.u[0], m.u[1]), (m.v[0], m.v[1]), lab, m.g, m.flags))
+        return r.counts, fasta, lms
+
+    def states(self):
+        d = StateDump()
+        _check(self.lib, self.ctx, self.lib.cfg_dump_states(self.ctx, ctypes.byref(d)), "cfg_dump_states")
+        return [(d.states[i].g, (d.states[i].key[0], d.states[i].key[1]), d.states[i].ef, d.states[i].status)
+                for i in range(d.n)]
+
+    def records(self):
+        d = RecordDump()
+        _check(self.lib, self.ctx, self.lib.cfg_dump_records(self.ctx, ctypes.byref(d)), "cfg_dump_records")
+        return [(d.records[i].pos, d.records[i].len, d.records[i].flags, d.records[i].g) for i in range(d.n)]
+
+
+def kmer_label(key, k):
+    """(low, high) words of a k-mer -> ACGT string."""
+    lo, hi = key
+    out = []
+    for i in range(k):
+        bp = 2 * (k - 1 - i)
+        b = (hi >> (bp - 64)) & 3 if bp >= 64 else (lo >> bp) & 3
+        out.append("ACGT"[b])
+    return "".join(out)
+
+
+def unpack_bases(packed: PackedInput, start: int, n: int) -> str:
+    w = packed.p.words
+    out = []
+    for i in range(start, start + n):
+        out.append("ACGT"[(w[i >> 5] >> (62 - 2 * (i & 31))) & 3])
+    return "".join(out)

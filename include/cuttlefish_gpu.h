@@ -1,0 +1,179 @@
+/*
+ * cuttlefish_gpu.h -- C ABI of the B200 compaction hot path.
+ *
+ * One context drives one job on one GPU: partition the input into weak super
+ * k-mers bucketed into subgraphs, build each subgraph's vertex table with the
+ * per-side edge frequencies and discontinuity flags, and walk every subgraph's
+ * locally maximal unitigs.  The results are what the reference's
+ * Subgraphs_Manager hands to its sinks:
+ *   - trivial maximal unitigs as FASTA text ">0\nSEQ\n"  (the op_buf sink,
+ *     include/Maximal_Unitig_Scratch.hpp:253-260, include/Character_Buffer.hpp:149-175);
+ *   - lm-tigs with their discontinuity edges (Discontinuity_Graph::add_edge,
+ *     include/Discontinuity_Graph.hpp:95,143-151);
+ *   - the potential-phantom-edge count (Discontinuity_Graph::inc_potential_phantom_edge,
+ *     include/Discontinuity_Graph.hpp:119);
+ *   - the trivial-unitig and cycle counts (Subgraphs_Manager::trivial_mtig_count /
+ *     icc_count, include/Subgraphs_Manager.hpp:80-134).
+ *
+ * Conventions: every call returns CFG_OK (0) or a CFG_ERR_* code; no C++
+ * exception and no device trap crosses this boundary.  Input buffers belong to
+ * the caller; result buffers belong to the context and stay valid until the
+ * next cfg_run / cfg_destroy.  A context is not re-entrant: use one per host
+ * thread (several contexts may share a device; each owns a stream).
+ */
+#ifndef CUTTLEFISH_GPU_H
+#define CUTTLEFISH_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    CFG_OK = 0,
+    CFG_ERR_BAD_INPUT = 1,   /* invalid parameters or input layout */
+    CFG_ERR_OOM = 2,         /* device or host allocation failed */
+    CFG_ERR_TABLE_FULL = 3,  /* a subgraph table overflowed its maximum capacity */
+    CFG_ERR_WALK_LIMIT = 4,  /* a walk exceeded its step bound (inconsistent table) */
+    CFG_ERR_CUDA = 5,        /* a CUDA runtime call failed */
+    CFG_ERR_STATE = 6        /* call out of order (e.g. fetch before run) */
+};
+
+/* cfg_params.flags */
+#define CFG_FLAG_DUMP_STATES   0x1u  /* keep every vertex state for cfg_dump_states */
+#define CFG_FLAG_DUMP_RECORDS  0x2u  /* keep the bucketed weak super k-mers for cfg_dump_records */
+
+typedef struct cfg_params {
+    uint32_t k;            /* odd, 3..63                                       (Build_Params::k) */
+    uint32_t l;            /* minimizer length, 1..min(k-1, 32)                 (--min-len)      */
+    uint32_t cutoff;       /* edge-frequency threshold, 1..15                   (-c)             */
+    uint32_t graph_count;  /* power of two <= 65536; the reference uses 16384 (include/Atlas.hpp:33-35) */
+    uint32_t flags;        /* CFG_FLAG_* */
+    uint32_t table_load_pct;  /* expected distinct/instances ratio in percent used to size tables;
+                                 0 = default (125 for references, pass ~50 for deep read sets) */
+    uint32_t reserved[2];
+} cfg_params;
+
+typedef struct cfg_ctx cfg_ctx;
+
+/* Counters of one run. */
+typedef struct cfg_counts {
+    uint64_t n_bases;       /* bases in the packed input */
+    uint64_t n_records;     /* weak super k-mers */
+    uint64_t n_instances;   /* k-mer instances over all weak super k-mers */
+    uint64_t n_vertices;    /* distinct (subgraph, canonical k-mer) vertices */
+    uint64_t n_isolated;
+    uint64_t n_phantom;
+    uint64_t n_trivial;     /* trivial maximal unitigs, cycles included */
+    uint64_t n_icc;         /* trivial maximal unitigs that are cycles */
+    uint64_t n_lmtig;       /* lm-tigs == discontinuity edges */
+    uint64_t fasta_bytes;   /* bytes of trivial-unitig FASTA text */
+    uint64_t lmtig_bytes;   /* bytes of lm-tig labels */
+    uint64_t n_retries;     /* subgraph-phase relaunches after table/arena overflow */
+} cfg_counts;
+
+/* One discontinuity edge with its lm-tig (Discontinuity_Graph::add_edge arguments). */
+typedef struct cfg_lmtig {
+    uint64_t u[2];          /* canonical k-mer of u, [0]=low word (last 32 bases), [1]=high word */
+    uint64_t v[2];
+    uint64_t label_off;     /* offset of the label in cfg_results.lmtig_text */
+    uint32_t label_len;
+    uint16_t g;             /* subgraph */
+    uint8_t  flags;         /* bit0 s_u==back, bit1 s_v==back, bit2 u_is_phi, bit3 v_is_phi */
+    uint8_t  pad;
+} cfg_lmtig;
+
+typedef struct cfg_results {
+    cfg_counts counts;
+    const char*      fasta;        /* counts.fasta_bytes bytes */
+    const char*      lmtig_text;   /* counts.lmtig_bytes bytes */
+    const cfg_lmtig* lmtigs;       /* counts.n_lmtig entries */
+} cfg_results;
+
+/* One vertex state (debug / parity). */
+typedef struct cfg_state {
+    uint64_t key[2];        /* canonical k-mer, [0]=low word */
+    uint32_t ef;            /* packed 4-bit edge frequencies (front nibbles 0-3, back 4-7), saturated at 15 */
+    uint16_t g;
+    uint8_t  status;        /* bit0 visited, bit1 disc front, bit2 disc back */
+    uint8_t  pad;
+} cfg_state;
+
+typedef struct cfg_state_dump { uint64_t n; const cfg_state* states; } cfg_state_dump;
+
+/* A weak super k-mer: start in the packed stream, length, flags, subgraph. */
+typedef struct cfg_record { uint32_t pos; uint8_t len; uint8_t flags; uint16_t g; } cfg_record;
+typedef struct cfg_record_dump { uint64_t n; const cfg_record* records; } cfg_record_dump;
+
+/* Creates a context on `device`.  Replaces the construction of
+ * Subgraphs_Manager<k,false> (include/Subgraphs_Manager.hpp:80-95,
+ * src/Subgraphs_Manager.cpp:26-52) plus Edge_Frequency::set_edge_threshold
+ * (src/dBG_Contractor.cpp:24). */
+int cfg_create(int device, const cfg_params* params, cfg_ctx** out);
+
+/* Supplies one job's input as 2-bit bases (A0 C1 G2 T3), 32 per 64-bit word,
+ * base i of the stream in bits [63-2(i%32) .. 62-2(i%32)] of word i/32, and the
+ * fragments: maximal ACGT runs of at least k+1 bases, frag_off[i] their first
+ * base in the stream, frag_len[i] their length, in input order and
+ * back-to-back (frag_off[i+1] == frag_off[i] + frag_len[i]).  The stream must
+ * hold fewer than 2^32 bases.  Copies to the device on the context's stream.
+ * Replaces the input side of Graph_Partitioner::partition
+ * (src/Graph_Partitioner.cpp:120-185,461-501). */
+int cfg_submit_packed(cfg_ctx* ctx, const uint64_t* packed, uint64_t n_bases,
+                      const uint64_t* frag_off, const uint32_t* frag_len, uint64_t n_frags);
+
+/* Same, with the three arrays already in device memory (no copy). */
+int cfg_submit_packed_device(cfg_ctx* ctx, const uint64_t* d_packed, uint64_t n_bases,
+                             const uint64_t* d_frag_off, const uint32_t* d_frag_len, uint64_t n_frags);
+
+/* Partition -> subgraph construct -> local walk, all on the device.  Replaces
+ * Graph_Partitioner::process_chunk (src/Graph_Partitioner.cpp:424-614),
+ * Subgraphs_Manager::finalize/process (src/Subgraphs_Manager.cpp:84-255),
+ * Subgraph::construct (src/Subgraph.cpp:43-108) and Subgraph::contract
+ * (src/Subgraph.cpp:183-271).  Results stay on the device. */
+int cfg_run(cfg_ctx* ctx);
+
+/* Copies the results to host memory owned by the context. */
+int cfg_fetch(cfg_ctx* ctx, cfg_results* out);
+
+/* Counters only (small copy). */
+int cfg_fetch_counts(cfg_ctx* ctx, cfg_counts* out);
+
+/* Vertex states of the last run (needs CFG_FLAG_DUMP_STATES). */
+int cfg_dump_states(cfg_ctx* ctx, cfg_state_dump* out);
+
+/* Bucketed weak super k-mers of the last run (needs CFG_FLAG_DUMP_RECORDS). */
+int cfg_dump_records(cfg_ctx* ctx, cfg_record_dump* out);
+
+/* Device time of the last cfg_run's kernels, in milliseconds:
+ * [0] partition, [1] bucket scatter, [2] subgraph construct+walk, [3] whole run. */
+int cfg_last_timings(cfg_ctx* ctx, float out_ms[4]);
+
+const char* cfg_last_error_string(cfg_ctx* ctx);
+
+/* Host-side input preparation.  Splits each record seq[rec_off[i] .. rec_off[i+1])
+ * into fragments -- maximal runs of A/C/G/T (either case) holding at least k+1
+ * bases, which is the fragment rule of Graph_Partitioner::process_chunk
+ * (src/Graph_Partitioner.cpp:461-501) -- and packs them into the layout
+ * cfg_submit_packed takes.  With `pinned` the buffers are page-locked (faster
+ * copies to the device).  Free with cfg_packed_free. */
+typedef struct cfg_packed {
+    uint64_t n_bases;
+    uint64_t n_frags;
+    uint64_t* words;       /* (n_bases + 31) / 32 words */
+    uint64_t* frag_off;
+    uint32_t* frag_len;
+    int pinned;
+} cfg_packed;
+
+int cfg_pack_records(const char* seq, const uint64_t* rec_off, uint64_t n_rec, uint32_t k, int pinned, cfg_packed* out);
+void cfg_packed_free(cfg_packed* p);
+
+void cfg_destroy(cfg_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,159 @@
+"""ctypes binding of the CPU oracle (oracle/_build/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU legs of bench.py as the checker; never by the product.
+"""
+from __future__ import annotations
+
+import collections
+import ctypes
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+REF_DRIVER = os.path.join(HERE, "_ref", "ref_driver")
+
+U64P = ctypes.POINTER(ctypes.c_uint64)
+U32P = ctypes.POINTER(ctypes.c_uint32)
+U8P = ctypes.POINTER(ctypes.c_uint8)
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("k", ctypes.c_uint32), ("l", ctypes.c_uint32), ("cutoff", ctypes.c_uint32),
+                ("graph_count", ctypes.c_uint32)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in (
+        "n_records", "n_instances", "n_vertices", "n_isolated", "n_phantom", "n_trivial", "n_icc",
+        "n_lmtig", "n_edges")] + [
+        ("rec_g", U32P), ("rec_len", U8P), ("rec_flags", U8P), ("rec_src", U64P),
+        ("vtx_g", U32P), ("vtx_key", U64P), ("vtx_ef", U32P), ("vtx_status", U8P),
+        ("fasta_bytes", ctypes.c_uint64), ("fasta", ctypes.c_void_p),
+        ("lm_text", ctypes.c_void_p), ("lm_off", U64P), ("lm_u", U64P), ("lm_v", U64P),
+        ("lm_flags", U8P), ("lm_g", U32P)]
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        lib = ctypes.CDLL(LIB)
+        lib.orc_create.restype = ctypes.c_void_p
+        lib.orc_create.argtypes = [ctypes.POINTER(Params)]
+        lib.orc_run.argtypes = [ctypes.c_void_p, ctypes.c_char_p, U64P, ctypes.c_uint64, ctypes.c_int]
+        lib.orc_partition_only.argtypes = [ctypes.c_void_p, ctypes.c_char_p, U64P, ctypes.c_uint64]
+        lib.orc_get.argtypes = [ctypes.c_void_p, ctypes.POINTER(Result)]
+        lib.orc_destroy.argtypes = [ctypes.c_void_p]
+        lib.orc_wyhash8.restype = ctypes.c_uint64
+        lib.orc_wyhash8.argtypes = [ctypes.c_uint64]
+        lib.orc_km1_min_hashes.argtypes = [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, U64P]
+        lib.orc_state_update.argtypes = [U32P, U8P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        lib.orc_edge_at.argtypes = [ctypes.c_uint32, ctypes.c_int, ctypes.c_uint32]
+        _lib = lib
+    return _lib
+
+
+def key_label(hi, lo, k):
+    out = []
+    for i in range(k):
+        bp = 2 * (k - 1 - i)
+        b = (hi >> (bp - 64)) & 3 if bp >= 64 else (lo >> bp) & 3
+        out.append("ACGT"[b])
+    return "".join(out)
+
+
+class OracleRun:
+    """Result of one oracle run, converted to Python collections."""
+
+    def __init__(self, records, k, l, cutoff, graph_count=16384, threads=1, partition_only=False, data_offsets=None):
+        lib = load()
+        p = Params(k, l, cutoff, graph_count)
+        ctx = lib.orc_create(ctypes.byref(p))
+        if not ctx:
+            raise ValueError("invalid oracle parameters")
+        if data_offsets is None:
+            bs = [r.encode() if isinstance(r, str) else bytes(r) for r in records]
+            data = b"".join(bs)
+            offs = [0]
+            for b in bs:
+                offs.append(offs[-1] + len(b))
+            arr = (ctypes.c_uint64 * len(offs))(*offs)
+            n = len(bs)
+        else:
+            data, arr, n = data_offsets
+        try:
+            if partition_only:
+                rc = lib.orc_partition_only(ctx, data, arr, n)
+            else:
+                rc = lib.orc_run(ctx, data, arr, n, threads)
+            assert rc == 0
+            r = Result()
+            lib.orc_get(ctx, ctypes.byref(r))
+            self.k = k
+            self.counts = {n: getattr(r, n) for n, _ in Result._fields_[:9]}
+            self.records = collections.Counter()
+            for i in range(r.n_records):
+                s, ln = r.rec_src[i], r.rec_len[i]
+                lab = data[s:s + ln].decode().upper()
+                self.records[(r.rec_g[i], ln, r.rec_flags[i], lab)] += 1
+            if partition_only:
+                return
+            self.states = {}
+            for i in range(r.n_vertices):
+                lab = key_label(r.vtx_key[2 * i], r.vtx_key[2 * i + 1], k)
+                self.states[(r.vtx_g[i], lab)] = (r.vtx_ef[i], r.vtx_status[i])
+            self.fasta = ctypes.string_at(r.fasta, r.fasta_bytes) if r.fasta_bytes else b""
+            self.lmtigs = collections.Counter()
+            if r.n_lmtig:
+                txt = ctypes.string_at(r.lm_text, r.lm_off[r.n_lmtig]).decode()
+                for i in range(r.n_lmtig):
+                    u = key_label(r.lm_u[2 * i], r.lm_u[2 * i + 1], k)
+                    v = key_label(r.lm_v[2 * i], r.lm_v[2 * i + 1], k)
+                    self.lmtigs[(r.lm_g[i], txt[r.lm_off[i]:r.lm_off[i + 1]], u, v, r.lm_flags[i])] += 1
+        finally:
+            lib.orc_destroy(ctx)
+
+    def fasta_records(self):
+        return fasta_multiset(self.fasta)
+
+
+def fasta_multiset(fasta: bytes):
+    """FASTA text '>0\\nSEQ\\n...' -> Counter of (header, seq)."""
+    out = collections.Counter()
+    lines = fasta.decode().split("\n")
+    assert lines[-1] == "" or not fasta
+    for i in range(0, len(lines) - 1, 2):
+        out[(lines[i], lines[i + 1])] += 1
+    return out
+
+
+def wyhash8(x):
+    return load().orc_wyhash8(x)
+
+
+def km1_min_hashes(seq: str, k: int, l: int):
+    n = len(seq) - (k - 1) + 1
+    out = (ctypes.c_uint64 * max(n, 1))()
+    assert load().orc_km1_min_hashes(seq.encode(), len(seq), k, l, out) == 0
+    return list(out[:n])
+
+
+def state_update(ef, status, front, back, s0, s1):
+    e = ctypes.c_uint32(ef)
+    s = ctypes.c_uint8(status)
+    load().orc_state_update(ctypes.byref(e), ctypes.byref(s), front, back, s0, s1)
+    return e.value, s.value
+
+
+def edge_at(ef, side, fth):
+    return load().orc_edge_at(ef, side, fth)

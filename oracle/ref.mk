@@ -7,7 +7,7 @@
 REF      ?= /root/reference
 CXX      ?= g++
 OUT      := _ref
-KS       := 5 9 15 23 31 63
+KS       := 3 5 7 9 15 23 31 63
 BASE     := -std=c++17 -O2 -w -DL1_CACHE_LINE_SIZE=64 -DFMT_HEADER_ONLY -Iref_shim -I$(REF)/include
 MUS_OBJ  := $(foreach k,$(KS),$(OUT)/mus_$(k).o)
 

@@ -266,6 +266,7 @@ int main(int argc, char** argv) {
     if (m == "min") {
         const int k = std::atoi(argv[2]); const uint16_t l = (uint16_t)std::atoi(argv[3]);
         switch (k) {
+            case 3: mode_min<2>(l); break;   case 7: mode_min<6>(l); break;
             case 5: mode_min<4>(l); break;   case 9: mode_min<8>(l); break;
             case 15: mode_min<14>(l); break; case 23: mode_min<22>(l); break;
             case 31: mode_min<30>(l); break; case 63: mode_min<62>(l); break;
@@ -275,6 +276,7 @@ int main(int argc, char** argv) {
     }
     if (m == "run" && argc >= 8) {   // run K L C G fasta_out lmtig_out  < records (one per line)
         switch (std::atoi(argv[2])) {
+            case 3: return run_k<3>(argc, argv);   case 7: return run_k<7>(argc, argv);
             case 5: return run_k<5>(argc, argv);   case 9: return run_k<9>(argc, argv);
             case 15: return run_k<15>(argc, argv); case 23: return run_k<23>(argc, argv);
             case 31: return run_k<31>(argc, argv); case 63: return run_k<63>(argc, argv);

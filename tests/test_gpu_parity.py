@@ -1,0 +1,108 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle.
+
+Every comparison is exact (integer/byte work): the multiset of weak super
+k-mer records per subgraph, every vertex's edge-frequency word and status
+bits, the trivial maximal unitigs as FASTA text, and the lm-tigs with their
+discontinuity edges (label orientation included).
+"""
+import collections
+
+import numpy as np
+import pytest
+
+import cfgpu
+import orc
+import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_run(records, k, l, c, G, load_pct=0):
+    packed = cfgpu.PackedInput(records, k)
+    flags = cfgpu.CFG_FLAG_DUMP_STATES | cfgpu.CFG_FLAG_DUMP_RECORDS
+    with cfgpu.Compactor(k, l, c, G, flags=flags, table_load_pct=load_pct) as cx:
+        cx.submit(packed)
+        cx.run()
+        counts, fasta, lms = cx.fetch()
+        states = cx.states()
+        recs = cx.records()
+    rec_ms = collections.Counter()
+    for pos, ln, fl, g in recs:
+        rec_ms[(g, ln, fl, cfgpu.unpack_bases(packed, pos, ln))] += 1
+    st = {(g, cfgpu.kmer_label(key, k)): (ef, status) for g, key, ef, status in states}
+    lm = collections.Counter()
+    for m in lms:
+        lm[(m.g, m.label, cfgpu.kmer_label(m.u, k), cfgpu.kmer_label(m.v, k), m.flags)] += 1
+    packed.close()
+    return counts, rec_ms, st, orc.fasta_multiset(fasta), lm
+
+
+def compare(records, k, l, c, G, load_pct=0):
+    o = orc.OracleRun(records, k, l, c, G)
+    counts, rec_ms, st, fa, lm = gpu_run(records, k, l, c, G, load_pct)
+    assert counts.n_records == o.counts["n_records"]
+    assert counts.n_instances == o.counts["n_instances"]
+    assert rec_ms == o.records, "weak super k-mer records differ"
+    assert counts.n_vertices == o.counts["n_vertices"]
+    assert st == o.states, "vertex states differ"
+    assert fa == o.fasta_records(), "trivial maximal unitigs differ"
+    assert lm == o.lmtigs, "lm-tigs differ"
+    for name in ("n_isolated", "n_phantom", "n_trivial", "n_icc", "n_lmtig"):
+        assert getattr(counts, name) == o.counts[name], name
+    return counts
+
+
+CASES = [  # k, l, cutoff, G, n, seed
+    (31, 20, 1, 16384, 40_000, 1),
+    (31, 20, 2, 16384, 40_000, 2),
+    (31, 20, 1, 64, 20_000, 3),
+    (31, 20, 1, 1, 8_000, 4),
+    (63, 20, 1, 16384, 40_000, 5),
+    (63, 20, 1, 4, 12_000, 6),
+    (5, 3, 1, 16384, 3_000, 7),
+    (9, 4, 2, 64, 6_000, 8),
+    (15, 7, 1, 16384, 10_000, 9),
+    (23, 11, 3, 256, 10_000, 10),
+    (33, 15, 1, 1024, 10_000, 11),
+    (31, 30, 1, 16384, 10_000, 12),
+    (31, 1, 1, 16384, 10_000, 13),
+]
+
+
+@pytest.mark.parametrize("k,l,c,G,n,seed", CASES)
+def test_adversarial(k, l, c, G, n, seed):
+    rng = np.random.default_rng(seed)
+    recs = [synth.adversarial(rng, int(rng.integers(k + 1, n)), k) for _ in range(3)]
+    recs.append(synth.adversarial(rng, k + 1, k))          # shortest possible fragment
+    recs.append("N" * 50 + synth.random_seq(rng, k) + "N")  # too short: dropped
+    compare(recs, k, l, c, G)
+
+
+def test_reference_like_genome():
+    rng = np.random.default_rng(21)
+    g = synth.genome_with_repeats(rng, 300_000, n_copies=30, n_pal=20)
+    counts = compare([g], 31, 20, 1, 16384)
+    assert counts.n_lmtig > 0 and counts.n_trivial > 0
+
+
+def test_reads_cutoff2():
+    rng = np.random.default_rng(22)
+    g = synth.genome_with_repeats(rng, 20_000, n_copies=5, n_pal=3)
+    rd = synth.reads(rng, g, 3_000)
+    compare(rd, 31, 20, 2, 16384, load_pct=60)
+
+
+def test_homopolymer_and_cycles():
+    recs = ["A" * 200, "C" * 40 + "G" * 40, "ACGT" * 30, "AACAC" * 20, "TAGATAG" * 15,
+            "GATTACA" + "A" * 70 + "GATTACA", "T" * 33 + "C" + "A" * 33]
+    for k, l in ((5, 3), (9, 4), (31, 20)):
+        for G in (1, 16, 16384):
+            compare(recs, k, l, 1, G)
+
+
+def test_small_table_retry():
+    # force tiny shared-memory tables so subgraphs overflow and are retried larger
+    rng = np.random.default_rng(23)
+    g = synth.random_seq(rng, 60_000)
+    counts = compare([g], 31, 20, 1, 64, load_pct=10)
+    assert counts.n_retries > 0
