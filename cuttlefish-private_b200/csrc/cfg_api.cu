@@ -38,13 +38,30 @@ struct DevBuf {
     template <typename T> T* as() const { return (T*)p; }
 };
 
+struct HostBuf {   // page-locked host memory for device->host result copies
+    void* p = nullptr;
+    size_t bytes = 0;
+    bool ensure(size_t need) {
+        if (need <= bytes) return true;
+        if (p) cudaFreeHost(p);
+        p = nullptr; bytes = 0;
+        const size_t want = need + need / 4 + 4096;
+        if (cudaMallocHost(&p, want) != cudaSuccess) { cudaGetLastError(); return false; }
+        bytes = want;
+        return true;
+    }
+    void release() { if (p) cudaFreeHost(p); p = nullptr; bytes = 0; }
+};
+
 struct cfg_ctx {
     int device = 0;
     cfg_params p{};
     uint32_t G = 16384;
     int words = 1;
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev[5] = {};
+    cudaEvent_t ev[8] = {};
+    float sub_ms = 0;
+    uint64_t launches = 0;
     float times[4] = {0, 0, 0, 0};
     std::string err;
 
@@ -63,12 +80,12 @@ struct cfg_ctx {
     uint64_t fasta_cap = 0, lm_text_cap = 0, lm_cap = 0, dump_cap = 0;
 
     // host results
-    std::vector<char> h_fasta, h_lm_text;
-    std::vector<cfg_lmtig> h_lm;
+    HostBuf h_fasta, h_lm_text, h_lm;
     std::vector<cfg_state> h_states;
     std::vector<cfg_record> h_records;
     cfg_counts counts{};
     uint64_t n_records = 0, n_instances = 0, dump_n = 0;
+    uint64_t phase_cycles[5] = {0, 0, 0, 0, 0};
 };
 
 namespace {
@@ -128,8 +145,11 @@ int run_partition(cfg_ctx* c, std::vector<uint32_t>& inst_h, std::vector<uint32_
         a.rec_cursor = &c->misc.as<MiscWords>()->rec_cursor;
         a.hist = c->hist.as<unsigned long long>();
         a.err = &c->misc.as<MiscWords>()->err;
+        CK(cudaEventRecord(c->ev[1], c->stream));
         launch_partition(a, c->stream);
         CK(cudaGetLastError());
+        CK(cudaEventRecord(c->ev[2], c->stream));
+        c->launches += 1;
         MiscWords m{};
         CK(cudaMemcpyAsync(&m, c->misc.p, sizeof(m), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
@@ -137,7 +157,7 @@ int run_partition(cfg_ctx* c, std::vector<uint32_t>& inst_h, std::vector<uint32_
         cap = m.rec_cursor + 1024;
         if (attempt == 2) return fail(c, CFG_ERR_OOM, "record buffer kept overflowing");
     }
-    CK(cudaEventRecord(c->ev[1], c->stream));
+    CK(cudaEventRecord(c->ev[3], c->stream));
     if (!c->bucket_off.ensure(4ull * (G + 1)) || !c->inst.ensure(4ull * G) || !c->fill.ensure(4ull * G))
         return fail(c, CFG_ERR_OOM, "bucket arrays");
     if (!c->recs.ensure(8 * std::max<uint64_t>(c->n_records, 1))) return fail(c, CFG_ERR_OOM, "bucketed records");
@@ -149,7 +169,8 @@ int run_partition(cfg_ctx* c, std::vector<uint32_t>& inst_h, std::vector<uint32_
     s.recs = c->recs.as<uint64_t>();
     launch_scatter(s, c->stream);
     CK(cudaGetLastError());
-    CK(cudaEventRecord(c->ev[2], c->stream));
+    CK(cudaEventRecord(c->ev[4], c->stream));
+    c->launches += 1 + (c->n_records ? 1 : 0);
     inst_h.resize(G); off_h.resize(G + 1);
     CK(cudaMemcpyAsync(inst_h.data(), c->inst.p, 4ull * G, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpyAsync(off_h.data(), c->bucket_off.p, 4ull * (G + 1), cudaMemcpyDeviceToHost, c->stream));
@@ -159,7 +180,9 @@ int run_partition(cfg_ctx* c, std::vector<uint32_t>& inst_h, std::vector<uint32_
     return CFG_OK;
 }
 
-struct Launch { std::vector<uint32_t> list; std::vector<uint64_t> off; std::vector<uint32_t> cap; uint32_t smem_cap = 0; bool smem = false; };
+// One launch: subgraphs sharing a table shape.  cluster 0 = global arena tables
+// (per-entry offset/capacity), else `cluster` CTAs with `per` slots each.
+struct Launch { std::vector<uint32_t> list; std::vector<uint64_t> off; std::vector<uint32_t> cap; uint32_t per = 0; uint32_t cluster = 0; };
 
 int launch_plan(cfg_ctx* c, const std::vector<Launch>& plan, uint64_t arena_slots) {
     const int W = c->words;
@@ -176,14 +199,14 @@ int launch_plan(cfg_ctx* c, const std::vector<Launch>& plan, uint64_t arena_slot
         uint64_t* d_off = c->tab_off.as<uint64_t>() + at;
         uint32_t* d_cap = c->tab_cap.as<uint32_t>() + at;
         CK(cudaMemcpyAsync(d_list, L.list.data(), 4 * L.list.size(), cudaMemcpyHostToDevice, c->stream));
-        if (!L.smem) {
+        if (L.cluster == 0) {
             CK(cudaMemcpyAsync(d_off, L.off.data(), 8 * L.off.size(), cudaMemcpyHostToDevice, c->stream));
             CK(cudaMemcpyAsync(d_cap, L.cap.data(), 4 * L.cap.size(), cudaMemcpyHostToDevice, c->stream));
         }
         SubgraphArgs a{};
         a.packed = c->d_packed; a.recs = c->recs.as<uint64_t>(); a.bucket_off = c->bucket_off.as<uint32_t>();
         a.list = d_list; a.n_list = (uint32_t)L.list.size();
-        a.tab_off = d_off; a.tab_cap = d_cap; a.smem_cap = L.smem_cap; a.arena = c->arena.as<unsigned char>();
+        a.tab_off = d_off; a.tab_cap = d_cap; a.smem_cap = L.per; a.arena = c->arena.as<unsigned char>();
         a.k = c->p.k; a.fth = c->p.cutoff; a.load_limit_pct = 90;
         a.fasta = c->fasta.as<char>(); a.fasta_cap = c->fasta_cap;
         a.lm_text = c->lm_text.as<char>(); a.lm_text_cap = c->lm_text_cap;
@@ -191,9 +214,9 @@ int launch_plan(cfg_ctx* c, const std::vector<Launch>& plan, uint64_t arena_slot
         a.dump = (c->p.flags & CFG_FLAG_DUMP_STATES) ? c->dump.as<StateOut>() : nullptr; a.dump_cap = c->dump_cap;
         a.retry = c->retry.as<uint32_t>(); a.cnt = c->counters.as<Counters>();
         a.err = &c->misc.as<MiscWords>()->err;
-        const uint32_t threads = L.smem ? std::min<uint32_t>(256, std::max<uint32_t>(64, L.smem_cap / 4)) : 512;
-        launch_subgraphs(a, W, L.smem, threads, c->stream);
-        CK(cudaGetLastError());
+        const uint32_t threads = L.cluster == 0 ? 512 : std::min<uint32_t>(512, std::max<uint32_t>(64, L.per / 4));
+        CK(launch_subgraphs(a, W, L.cluster, threads, c->stream));
+        c->launches += 1;
         at += L.list.size();
     }
     return CFG_OK;
@@ -218,12 +241,15 @@ int ensure_outputs(cfg_ctx* c, uint64_t fasta_need, uint64_t lm_text_need, uint6
 int run_subgraphs(cfg_ctx* c, const std::vector<uint32_t>& inst_h) {
     const uint32_t G = c->G;
     const int W = c->words;
-    const uint32_t load = c->p.table_load_pct ? c->p.table_load_pct : 125;
-    const uint32_t smem_max = (uint32_t)subgraph_max_smem_cap(W);
-    std::vector<uint32_t> caps(G, 0);
+    // expected distinct vertices per k-mer instance, in percent; tables are sized for
+    // a load factor near one half of that estimate
+    const uint32_t load = c->p.table_load_pct ? c->p.table_load_pct : 100;
+    const uint32_t per_max = subgraph_max_per_cta(W);   // one CTA's table
+    const uint32_t per_cl = subgraph_cluster_per_cta(W);   // each CTA of a cluster
+    const uint32_t max_cluster = 8;
+    std::vector<uint64_t> want(G, 0);                      // slots wanted per subgraph
     for (uint32_t g = 0; g < G; ++g)
-        if (inst_h[g]) caps[g] = next_pow2(((uint64_t)inst_h[g] * load + 99) / 100);
-
+        if (inst_h[g]) want[g] = std::max<uint64_t>(64, ((uint64_t)inst_h[g] * load * 2 + 99) / 100);
     uint64_t fasta_need = c->n_bases + (c->n_records + 1024) * 8 + (1u << 20);
     uint64_t lm_text_need = c->n_bases / 2 + (c->n_records + 1024) * (c->p.k + 2);
     uint64_t lm_need = c->n_records + 1024;
@@ -237,35 +263,45 @@ int run_subgraphs(cfg_ctx* c, const std::vector<uint32_t>& inst_h) {
         if (rc) return rc;
         CK(cudaMemsetAsync(c->counters.p, 0, sizeof(Counters), c->stream));
         std::vector<uint32_t> work = todo;
-        std::vector<uint32_t> cur_caps = caps;
+        std::vector<uint64_t> cur_want = want;
         uint64_t retries = 0;
         bool overflow = false;
         for (int pass = 0; pass < 12 && !work.empty(); ++pass) {
             std::vector<Launch> plan;
-            std::vector<uint32_t> cls;   // shared-memory classes by capacity
-            Launch glob; glob.smem = false;
+            Launch glob; glob.cluster = 0;
             uint64_t arena_slots = 0;
             for (uint32_t g : work) {
-                const uint32_t cap = cur_caps[g];
-                if (cap <= smem_max) {
-                    size_t i = 0;
-                    while (i < plan.size() && plan[i].smem_cap != cap) ++i;
-                    if (i == plan.size()) { plan.emplace_back(); plan.back().smem = true; plan.back().smem_cap = cap; }
-                    plan[i].list.push_back(g);
-                } else {
+                const uint64_t w = cur_want[g];
+                uint32_t cl, per;
+                if (w <= per_max) { cl = 1; per = next_pow2(w); }
+                else if (w <= (uint64_t)per_cl * max_cluster) { cl = (uint32_t)((w + per_cl - 1) / per_cl); per = per_cl; }
+                else {
+                    const uint32_t cap = next_pow2(w);
                     glob.list.push_back(g); glob.off.push_back(arena_slots); glob.cap.push_back(cap);
                     arena_slots += cap;
+                    continue;
                 }
+                size_t i = 0;
+                while (i < plan.size() && !(plan[i].per == per && plan[i].cluster == cl)) ++i;
+                if (i == plan.size()) { plan.emplace_back(); plan.back().per = per; plan.back().cluster = cl; }
+                plan[i].list.push_back(g);
             }
             plan.push_back(glob);
             CK(cudaMemsetAsync(&c->counters.as<Counters>()->retry_count, 0, sizeof(unsigned long long), c->stream));
+            CK(cudaEventRecord(c->ev[5], c->stream));
             rc = launch_plan(c, plan, arena_slots);
             if (rc) return rc;
+            CK(cudaEventRecord(c->ev[6], c->stream));
             Counters h{};
             MiscWords m{};
             CK(cudaMemcpyAsync(&h, c->counters.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
             CK(cudaMemcpyAsync(&m, c->misc.p, sizeof(m), cudaMemcpyDeviceToHost, c->stream));
             CK(cudaStreamSynchronize(c->stream));
+            {
+                float ms = 0;
+                cudaEventElapsedTime(&ms, c->ev[5], c->ev[6]);
+                c->sub_ms += ms;
+            }
             rc = check_err_word(c, m.err);
             if (rc) return rc;
             if (m.err & (DERR_OUT_OVERFLOW | DERR_DUMP_OVERFLOW)) {
@@ -283,8 +319,8 @@ int run_subgraphs(cfg_ctx* c, const std::vector<uint32_t>& inst_h) {
                 CK(cudaStreamSynchronize(c->stream));
                 retries += h.retry_count;
                 for (uint32_t g : work) {
-                    if (cur_caps[g] >= (1u << 30)) return fail(c, CFG_ERR_TABLE_FULL, "subgraph table exceeded 2^30 slots");
-                    cur_caps[g] = std::max<uint32_t>(cur_caps[g] * 4, smem_max * 2);
+                    if (cur_want[g] >= (1ull << 30)) return fail(c, CFG_ERR_TABLE_FULL, "subgraph table exceeded 2^30 slots");
+                    cur_want[g] *= 4;
                 }
             }
         }
@@ -298,7 +334,9 @@ int run_subgraphs(cfg_ctx* c, const std::vector<uint32_t>& inst_h) {
         o.n_vertices = h.vertices; o.n_isolated = h.isolated; o.n_phantom = h.phantom;
         o.n_trivial = h.trivial; o.n_icc = h.icc; o.n_lmtig = h.lm_count;
         o.fasta_bytes = h.fasta_bytes; o.lmtig_bytes = h.lm_bytes; o.n_retries = retries;
+        o.n_launches = c->launches;
         c->dump_n = h.dump_count;
+        for (int i = 0; i < 5; ++i) c->phase_cycles[i] = h.phase_cycles[i];
         return CFG_OK;
     }
     return fail(c, CFG_ERR_OOM, "output arenas kept overflowing");
@@ -380,20 +418,21 @@ int cfg_run(cfg_ctx* c) {
     c->err.clear();
     c->have_run = false;
     c->counts = cfg_counts{};
+    c->sub_ms = 0;
+    c->launches = 0;
     CK(cudaEventRecord(c->ev[0], c->stream));
     std::vector<uint32_t> inst_h, off_h;
     int rc = run_partition(c, inst_h, off_h);
     if (rc) return rc;
     rc = run_subgraphs(c, inst_h);
     if (rc) return rc;
-    CK(cudaEventRecord(c->ev[3], c->stream));
-    CK(cudaEventSynchronize(c->ev[3]));
-    float t01 = 0, t12 = 0, t23 = 0, t03 = 0;
-    cudaEventElapsedTime(&t01, c->ev[0], c->ev[1]);
-    cudaEventElapsedTime(&t12, c->ev[1], c->ev[2]);
-    cudaEventElapsedTime(&t23, c->ev[2], c->ev[3]);
-    cudaEventElapsedTime(&t03, c->ev[0], c->ev[3]);
-    c->times[0] = t01; c->times[1] = t12; c->times[2] = t23; c->times[3] = t03;
+    CK(cudaEventRecord(c->ev[7], c->stream));
+    CK(cudaEventSynchronize(c->ev[7]));
+    float tp = 0, ts = 0, tt = 0;
+    cudaEventElapsedTime(&tp, c->ev[1], c->ev[2]);
+    cudaEventElapsedTime(&ts, c->ev[3], c->ev[4]);
+    cudaEventElapsedTime(&tt, c->ev[0], c->ev[7]);
+    c->times[0] = tp; c->times[1] = ts; c->times[2] = c->sub_ms; c->times[3] = tt;
     c->have_run = true;
     return CFG_OK;
 }
@@ -410,18 +449,18 @@ int cfg_fetch(cfg_ctx* c, cfg_results* out) {
     if (!c->have_run) return fail(c, CFG_ERR_STATE, "no completed run");
     CK(cudaSetDevice(c->device));
     const cfg_counts& n = c->counts;
-    c->h_fasta.resize(n.fasta_bytes);
-    c->h_lm_text.resize(n.lmtig_bytes);
-    c->h_lm.resize(n.n_lmtig);
-    if (n.fasta_bytes) CK(cudaMemcpyAsync(c->h_fasta.data(), c->fasta.p, n.fasta_bytes, cudaMemcpyDeviceToHost, c->stream));
-    if (n.lmtig_bytes) CK(cudaMemcpyAsync(c->h_lm_text.data(), c->lm_text.p, n.lmtig_bytes, cudaMemcpyDeviceToHost, c->stream));
     static_assert(sizeof(cfg_lmtig) == sizeof(LmtigOut), "lm-tig record layout");
-    if (n.n_lmtig) CK(cudaMemcpyAsync(c->h_lm.data(), c->lm.p, n.n_lmtig * sizeof(cfg_lmtig), cudaMemcpyDeviceToHost, c->stream));
+    if (!c->h_fasta.ensure(n.fasta_bytes + 1) || !c->h_lm_text.ensure(n.lmtig_bytes + 1) ||
+        !c->h_lm.ensure(n.n_lmtig * sizeof(cfg_lmtig) + 1))
+        return fail(c, CFG_ERR_OOM, "pinned result buffers");
+    if (n.fasta_bytes) CK(cudaMemcpyAsync(c->h_fasta.p, c->fasta.p, n.fasta_bytes, cudaMemcpyDeviceToHost, c->stream));
+    if (n.lmtig_bytes) CK(cudaMemcpyAsync(c->h_lm_text.p, c->lm_text.p, n.lmtig_bytes, cudaMemcpyDeviceToHost, c->stream));
+    if (n.n_lmtig) CK(cudaMemcpyAsync(c->h_lm.p, c->lm.p, n.n_lmtig * sizeof(cfg_lmtig), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     out->counts = n;
-    out->fasta = c->h_fasta.data();
-    out->lmtig_text = c->h_lm_text.data();
-    out->lmtigs = c->h_lm.data();
+    out->fasta = (const char*)c->h_fasta.p;
+    out->lmtig_text = (const char*)c->h_lm_text.p;
+    out->lmtigs = (const cfg_lmtig*)c->h_lm.p;
     return CFG_OK;
 }
 
@@ -466,6 +505,13 @@ int cfg_last_timings(cfg_ctx* c, float out_ms[4]) {
     return CFG_OK;
 }
 
+int cfg_last_phase_cycles(cfg_ctx* c, uint64_t out[5]) {
+    if (!c || !out) return CFG_ERR_BAD_INPUT;
+    if (!c->have_run) return fail(c, CFG_ERR_STATE, "no completed run");
+    for (int i = 0; i < 5; ++i) out[i] = c->phase_cycles[i];
+    return CFG_OK;
+}
+
 const char* cfg_last_error_string(cfg_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
 void cfg_destroy(cfg_ctx* c) {
@@ -476,6 +522,7 @@ void cfg_destroy(cfg_ctx* c) {
                       &c->fill, &c->recs, &c->list, &c->tab_off, &c->tab_cap, &c->arena, &c->fasta, &c->lm_text,
                       &c->lm, &c->dump, &c->retry, &c->counters};
     for (DevBuf* b : bufs) b->release();
+    c->h_fasta.release(); c->h_lm_text.release(); c->h_lm.release();
     for (auto& e : c->ev) if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;

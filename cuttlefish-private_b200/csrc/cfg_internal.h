@@ -72,6 +72,7 @@ struct StateOut {                // mirrors cfg_state
 struct Counters {                // device-side counters of the subgraph phase
     unsigned long long vertices, isolated, phantom, trivial, icc, lmtig;
     unsigned long long fasta_bytes, lm_bytes, lm_count, dump_count, retry_count;
+    unsigned long long phase_cycles[5];   // SM cycles summed over CTAs: build, W1, W2, W3, tail
 };
 
 struct SubgraphArgs {
@@ -82,7 +83,7 @@ struct SubgraphArgs {
     uint32_t n_list;
     const uint64_t* tab_off;     // global path: per-list-entry table offset (slots) into the arena
     const uint32_t* tab_cap;     // global path: per-list-entry capacity (power of two)
-    uint32_t smem_cap;           // shared path: capacity of every table of this launch
+    uint32_t smem_cap;           // shared path: slots held by each CTA of this launch
     unsigned char* arena;        // global path tables
     uint32_t k, fth;
     uint32_t load_limit_pct;     // a table fuller than this is abandoned and retried larger
@@ -95,14 +96,16 @@ struct SubgraphArgs {
     uint32_t* err;
 };
 
-// bytes per table slot
-__host__ __device__ inline uint32_t slot_bytes(int words) { return words == 1 ? 28u : 36u; }
+// bytes per table slot: k-mer (8 per word) + state word (8) + meta (4) + work-list entry (4)
+__host__ __device__ inline uint32_t slot_bytes(int words) { return words == 1 ? 24u : 32u; }
 
 void launch_partition(const PartitionArgs& a, cudaStream_t s);
 void launch_bucket_scan(const unsigned long long* hist, uint32_t G, uint32_t* bucket_off, uint32_t* inst,
                         uint32_t* fill, cudaStream_t s);
 void launch_scatter(const ScatterArgs& a, cudaStream_t s);
-void launch_subgraphs(const SubgraphArgs& a, int words, bool smem, uint32_t threads, cudaStream_t s);
-int subgraph_max_smem_cap(int words);
+// cluster == 0: tables in the global arena; 1: one CTA's shared memory; >1: a cluster's.
+cudaError_t launch_subgraphs(const SubgraphArgs& a, int words, uint32_t cluster, uint32_t threads, cudaStream_t s);
+uint32_t subgraph_max_per_cta(int words);      // one CTA owning a whole table
+uint32_t subgraph_cluster_per_cta(int words);  // each CTA of a cluster
 
 }  // namespace cfg

@@ -27,7 +27,9 @@ __device__ __forceinline__ uint64_t lmer_at(const uint64_t* __restrict__ s, uint
 
 // Processes the (k-1)-mer positions [j0, j1) of one fragment: emits every weak
 // super k-mer whose run starts there.
-__device__ void sweep_fragment(const PartitionArgs& a, uint64_t* ring, uint64_t F0, uint32_t FL, uint32_t j0, uint32_t j1) {
+// mod_w[x] = x % w for x < 128 (w <= 62): the cap-cut test without a division.
+__device__ void sweep_fragment(const PartitionArgs& a, uint64_t* ring, const uint8_t* mod_w, uint64_t F0, uint32_t FL,
+                               uint32_t j0, uint32_t j1) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t k = a.k, l = a.l, w = a.w;
     const uint32_t M = FL - k + 2;                 // (k-1)-mers in the fragment
@@ -39,7 +41,8 @@ __device__ void sweep_fragment(const PartitionArgs& a, uint64_t* ring, uint64_t 
         if (q < n_lmers) ring[q & (RING - 1)] = lmer_hash(lmer_at(a.packed, F0 + q, l), l, a.seed0);
 
     bool active = false;
-    uint32_t r0 = 0, run_start = 0, last_cut = 0, last_cut_g = 0, last_cut_chg = 0, carry_g = 0;
+    uint32_t r0 = 0, last_cut = 0, last_cut_g = 0, last_cut_chg = 0, carry_g = 0;
+    uint32_t carry_rem = 0;   // (base - start of the run in progress) % w
 
     for (uint32_t base = start;; base += 32) {
         __syncwarp();
@@ -76,7 +79,7 @@ __device__ void sweep_fragment(const PartitionArgs& a, uint64_t* ring, uint64_t 
             r0 = base + r0_lane;
             if (r0 >= j1) return;
             active = true; just_activated = true;
-            run_start = r0; last_cut = r0;
+            last_cut = r0;
             last_cut_g = __shfl_sync(0xffffffffu, g, r0_lane);
             last_cut_chg = 1;
         }
@@ -84,8 +87,8 @@ __device__ void sweep_fragment(const PartitionArgs& a, uint64_t* ring, uint64_t 
 
         // run start of each position: highest change at or below it, else the carried one
         const uint32_t le = chg & (lanemask_lt() | (1u << lane));
-        const uint32_t rs = le ? base + (31 - __clz(le)) : run_start;
-        const bool is_cut = valid && ((act_mask >> lane) & 1) && (is_chg || ((j - rs) % w) == 0);
+        const uint32_t rem = le ? mod_w[lane - (31 - __clz(le))] : mod_w[carry_rem + lane];
+        const bool is_cut = valid && ((act_mask >> lane) & 1) && (is_chg || rem == 0);
         uint32_t cut = __ballot_sync(0xffffffffu, is_cut);
 
         // stop at the first change at or past j1: the run it starts belongs to the next segment
@@ -132,7 +135,7 @@ __device__ void sweep_fragment(const PartitionArgs& a, uint64_t* ring, uint64_t 
             last_cut_g = __shfl_sync(0xffffffffu, g, hl);
             last_cut_chg = __shfl_sync(0xffffffffu, (uint32_t)is_chg, hl);
         }
-        if (chg) run_start = base + (31 - __clz(chg));
+        carry_rem = chg ? mod_w[32 - (31 - __clz(chg))] : mod_w[carry_rem + 32];
         carry_g = __shfl_sync(0xffffffffu, g, 31);
         if (fin && lane == 0) {   // final piece [last_cut, M): not joined on the right
             const uint32_t c = last_cut, lj = c > 0;
@@ -148,6 +151,9 @@ __device__ void sweep_fragment(const PartitionArgs& a, uint64_t* ring, uint64_t 
 
 __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_partition(const PartitionArgs a) {
     __shared__ uint64_t rings[WARPS_PER_BLOCK][RING];
+    __shared__ uint8_t mod_w[128];
+    if (threadIdx.x < 128) mod_w[threadIdx.x] = (uint8_t)(threadIdx.x % a.w);
+    __syncthreads();
     uint64_t* ring = rings[threadIdx.x >> 5];
     const uint64_t n_seg = (a.n_bases + a.seg - 1) / a.seg;
     const uint64_t warp0 = (uint64_t)blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5);
@@ -168,7 +174,7 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_partition(const Partit
             const uint32_t j0 = s0 > F0 ? (uint32_t)(s0 - F0) : 0;
             const uint64_t e = s1 - F0;
             const uint32_t j1 = e < M ? (uint32_t)e : M;
-            if (j0 < j1) sweep_fragment(a, ring, F0, FL, j0, j1);
+            if (j0 < j1) sweep_fragment(a, ring, mod_w, F0, FL, j0, j1);
         }
     }
 }

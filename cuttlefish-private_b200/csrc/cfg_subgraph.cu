@@ -1,21 +1,26 @@
 // cfg_subgraph.cu -- K2 + K3: per-subgraph vertex table and local unitig walk.
 //
-// One CTA owns one subgraph.  Its open-addressing table lives in shared memory
-// when it fits (global-memory arena otherwise) and holds per vertex: the
-// canonical k-mer, the packed 4-bit edge frequencies and discontinuity flags of
-// State_Config<false> (include/State_Config.hpp:24-268), and the stream position
-// of the vertex's first occurrence.
+// One subgraph is owned by one CTA, or by a thread-block cluster of up to 8
+// CTAs whose shared memories together hold the subgraph's open-addressing
+// table (slot s lives in CTA s / per, reached through distributed shared
+// memory).  Subgraphs too large for a cluster use a global-memory arena with
+// the same code.  Per vertex the table holds the canonical k-mer, one 64-bit
+// state word -- the packed 4-bit edge frequencies of State_Config<false>
+// (include/State_Config.hpp:24-268) in the low half and the stream position of
+// the vertex's first occurrence in the high half -- and a meta word
+// (discontinuity flags, then the walk's bookkeeping).
 //
-// Build (Subgraph::construct, src/Subgraph.cpp:43-108): a thread per weak super
-// k-mer rolls its k-mers and applies HT_Router::update (include/Subgraph.hpp:546-560)
-// with CAS-updated saturating counters; the self-loop rule (:82-83) needs only the
-// previous k-mer of the same super k-mer.
+// Build (Subgraph::construct, src/Subgraph.cpp:43-108): every thread of the
+// CTA/cluster takes weak super k-mers, rolls their k-mers and applies
+// HT_Router::update (include/Subgraph.hpp:546-560) as one CAS on the state word
+// (saturated counts and an unchanged first occurrence need no CAS).  The
+// self-loop rule (:82-83) needs only the previous k-mer of the same super k-mer.
 //
 // Walk (Subgraph::contract / extract_maximal_unitig / walk_unitig,
 // src/Subgraph.cpp:183-271, include/Subgraph.hpp:414-543): a step v -(side s)-> u
 // is taken iff s holds one passing edge, u != v, and u's entrance side holds at
 // most one.  That relation is symmetric, so the reference's sequential walk from
-// any seed returns the whole maximal path, whatever the seed order, except in one
+// any seed returns the whole maximal path whatever the seed order, except in one
 // case: a homopolymer vertex b^k whose back side holds only its own self-loop and
 // whose front side holds at most one edge.  Seeded directly, the reference
 // records it as a one-vertex cycle; reached from its predecessor, it ends that
@@ -23,8 +28,12 @@
 // occurrence), so the kernel compares first-occurrence positions to decide, and
 // orients each lm-tig by its first-inserted vertex exactly as the reference does.
 // Paths are walked from both ends in parallel; the end with the smaller slot emits.
+#include <cooperative_groups.h>
+
 #include "cfg_device.cuh"
 #include "cfg_internal.h"
+
+namespace cg = cooperative_groups;
 
 namespace cfg {
 
@@ -32,76 +41,206 @@ namespace {
 
 constexpr uint32_t NONE = 0xffffffffu;
 constexpr uint64_t EMPTY = ~0ull;
+constexpr uint64_t BUSY = ~1ull;   // a two-word key's high word while its low word is written
 // walk termination kinds (Walk_Termination, include/Subgraph.hpp:362-369)
 constexpr uint32_t T_OK = 0, T_BRANCHED = 1, T_CROSSED = 2, T_DEAD = 3, T_EXIT = 4;
 // meta layout: bits 0-2 visited / disc front / disc back; 3 Q (self-looped homopolymer);
 // 4 isolated; 8-10 front termination; 11-13 back termination
 constexpr uint32_t M_Q = 8u, M_ISO = 16u;
+enum { LOCAL = 0, CLUSTER = 1, GLOBAL = 2 };
 
 __device__ __forceinline__ uint32_t term_of(uint32_t meta, int side) { return (meta >> (side == FRONT ? 8 : 11)) & 7; }
 __device__ __forceinline__ uint32_t compb(uint32_t b) { return b < 4 ? 3 - b : b; }
+__device__ __forceinline__ uint32_t st_ef(uint64_t st) { return (uint32_t)st; }
+__device__ __forceinline__ uint32_t st_ins(uint64_t st) { return (uint32_t)(st >> 32); }
 
-template <int W, bool SM>
+// Memory-space accessors.  LOCAL and CLUSTER address a slot by a 32-bit shared
+// address (CLUSTER: mapped into the owning CTA with mapa); GLOBAL by a pointer.
+// Explicit state spaces keep table traffic on the shared-memory pipes.
+template <int MODE> struct Mem;
+template <> struct Mem<LOCAL> {
+    typedef uint32_t A;
+    // volatile: these loads also serve waits on other threads' stores (a weak load may be hoisted)
+    static __device__ __forceinline__ uint64_t ld64(A a) { uint64_t v; asm volatile("ld.volatile.shared.u64 %0, [%1];" : "=l"(v) : "r"(a) : "memory"); return v; }
+    static __device__ __forceinline__ uint32_t ld32(A a) { uint32_t v; asm volatile("ld.volatile.shared.u32 %0, [%1];" : "=r"(v) : "r"(a) : "memory"); return v; }
+    static __device__ __forceinline__ void st64(A a, uint64_t v) { asm volatile("st.volatile.shared.u64 [%0], %1;" :: "r"(a), "l"(v) : "memory"); }
+    static __device__ __forceinline__ void st32(A a, uint32_t v) { asm volatile("st.volatile.shared.u32 [%0], %1;" :: "r"(a), "r"(v) : "memory"); }
+    static __device__ __forceinline__ uint64_t cas64(A a, uint64_t c, uint64_t v) { uint64_t o; asm volatile("atom.shared.cas.b64 %0, [%1], %2, %3;" : "=l"(o) : "r"(a), "l"(c), "l"(v) : "memory"); return o; }
+    static __device__ __forceinline__ uint64_t exch64(A a, uint64_t v) { uint64_t o; asm volatile("atom.shared.exch.b64 %0, [%1], %2;" : "=l"(o) : "r"(a), "l"(v) : "memory"); return o; }
+    static __device__ __forceinline__ void or32(A a, uint32_t v) { asm volatile("red.shared.or.b32 [%0], %1;" :: "r"(a), "r"(v) : "memory"); }
+    static __device__ __forceinline__ void fence() { __threadfence_block(); }
+};
+template <> struct Mem<CLUSTER> {
+    typedef uint32_t A;
+    static __device__ __forceinline__ uint64_t ld64(A a) { uint64_t v; asm volatile("ld.relaxed.cluster.shared::cluster.u64 %0, [%1];" : "=l"(v) : "r"(a) : "memory"); return v; }
+    static __device__ __forceinline__ uint32_t ld32(A a) { uint32_t v; asm volatile("ld.relaxed.cluster.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(a) : "memory"); return v; }
+    static __device__ __forceinline__ void st64(A a, uint64_t v) { asm volatile("st.relaxed.cluster.shared::cluster.u64 [%0], %1;" :: "r"(a), "l"(v) : "memory"); }
+    static __device__ __forceinline__ void st32(A a, uint32_t v) { asm volatile("st.relaxed.cluster.shared::cluster.u32 [%0], %1;" :: "r"(a), "r"(v) : "memory"); }
+    static __device__ __forceinline__ uint64_t cas64(A a, uint64_t c, uint64_t v) { uint64_t o; asm volatile("atom.relaxed.cluster.shared::cluster.cas.b64 %0, [%1], %2, %3;" : "=l"(o) : "r"(a), "l"(c), "l"(v) : "memory"); return o; }
+    static __device__ __forceinline__ uint64_t exch64(A a, uint64_t v) { uint64_t o; asm volatile("atom.relaxed.cluster.shared::cluster.exch.b64 %0, [%1], %2;" : "=l"(o) : "r"(a), "l"(v) : "memory"); return o; }
+    static __device__ __forceinline__ void or32(A a, uint32_t v) { asm volatile("red.relaxed.cluster.shared::cluster.or.b32 [%0], %1;" :: "r"(a), "r"(v) : "memory"); }
+    static __device__ __forceinline__ void fence() { asm volatile("fence.acq_rel.cluster;" ::: "memory"); }
+};
+template <> struct Mem<GLOBAL> {
+    typedef uint64_t A;   // generic address of global memory
+    static __device__ __forceinline__ uint64_t ld64(A a) { return *(const volatile unsigned long long*)a; }
+    static __device__ __forceinline__ uint32_t ld32(A a) { return *(const volatile unsigned int*)a; }
+    static __device__ __forceinline__ void st64(A a, uint64_t v) { *(volatile unsigned long long*)a = v; }
+    static __device__ __forceinline__ void st32(A a, uint32_t v) { *(volatile unsigned int*)a = v; }
+    static __device__ __forceinline__ uint64_t cas64(A a, uint64_t c, uint64_t v) { return atomicCAS((unsigned long long*)a, (unsigned long long)c, (unsigned long long)v); }
+    static __device__ __forceinline__ uint64_t exch64(A a, uint64_t v) { return atomicExch((unsigned long long*)a, (unsigned long long)v); }
+    static __device__ __forceinline__ void or32(A a, uint32_t v) { atomicOr((unsigned int*)a, v); }
+    static __device__ __forceinline__ void fence() { __threadfence(); }
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ uint32_t mapa_cluster(uint32_t a, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+    return r;
+}
+
+// The table of one subgraph: nranks sub-tables of `per` slots, one per CTA of the
+// cluster (one in LOCAL and GLOBAL mode).  A k-mer's sub-table (its owner) and its
+// home slot there come from two independent halves of its hash; probing wraps
+// inside the sub-table.  The CTAs of a cluster share out the subgraph's weak super
+// k-mers and update other CTAs' sub-tables with atomics through DSMEM.
+template <int W, int MODE>
 struct Tab {
-    unsigned long long* keys;   // W words per slot
-    uint32_t* ef;
-    uint32_t* meta;
-    uint32_t* ins;
-    uint32_t* nbr;              // 2 per slot: (slot << 1 | entrance side) or NONE
-    uint32_t mask;
+    typedef Mem<MODE> M;
+    typedef typename M::A A;
+    A keys, st, meta;           // this CTA's base addresses (W key words per slot, ef | ins << 32, meta)
+    uint32_t per, shift, pmask; // slots per sub-table; slot s lives in rank s >> shift at index s & pmask
+    uint32_t nranks, rank;
+    uint32_t* err_flag;         // set when a wait on a key being written exceeds its bound
 
-    template <typename T> __device__ __forceinline__ T ld(const T* p) const {
-        if constexpr (SM) return *(const volatile T*)p;
-        else return __ldcg(p);
+    __device__ __forceinline__ A addr(A base, uint32_t s, uint32_t bytes) const {
+        if constexpr (MODE == CLUSTER) return mapa_cluster(base + (s & pmask) * bytes, s >> shift);
+        else return base + (A)s * bytes;
     }
+    __device__ __forceinline__ A ka(uint32_t s) const { return addr(keys, s, 8 * W); }
+    __device__ __forceinline__ A sa(uint32_t s) const { return addr(st, s, 8); }
+    __device__ __forceinline__ A ma(uint32_t s) const { return addr(meta, s, 4); }
+
+    __device__ __forceinline__ uint64_t ld_st(uint32_t s) const { return M::ld64(sa(s)); }
+    __device__ __forceinline__ uint32_t ld_meta(uint32_t s) const { return M::ld32(ma(s)); }
+    __device__ __forceinline__ void or_meta(uint32_t s, uint32_t v) const { M::or32(ma(s), v); }
+
     __device__ __forceinline__ Kmer<W> key(uint32_t s) const {
-        if constexpr (W == 1) return Kmer<1>{ld(keys + s)};
-        else return Kmer<2>{ld(keys + 2 * s), ld(keys + 2 * s + 1)};
+        const A a = ka(s);
+        if constexpr (W == 1) return Kmer<1>{M::ld64(a)};
+        else return Kmer<2>{M::ld64(a), M::ld64(a + 8)};
     }
-    __device__ __forceinline__ bool empty(uint32_t s) const {
-        if constexpr (W == 1) return ld(keys + s) == EMPTY;
-        else return ld(keys + 2 * s + 1) == EMPTY;
+    // owner rank and home index inside the owner's sub-table
+    __device__ __forceinline__ void place(const Kmer<W>& x, uint32_t& r, uint32_t& h) const {
+        const uint64_t z = key_hash(x);
+        r = (uint32_t)(((uint64_t)(uint32_t)z * nranks) >> 32);
+        h = (uint32_t)(((z >> 32) * per) >> 32);
     }
-    __device__ uint32_t find(const Kmer<W>& x) const {   // read-only phase
-        uint32_t h = (uint32_t)key_hash(x) & mask;
-        for (uint32_t p = 0; p <= mask; ++p) {
-            if (empty(h)) return NONE;
-            if (key(h) == x) return h;
-            h = (h + 1) & mask;
+    __device__ uint32_t find(const Kmer<W>& x) const {   // read-only phase, any CTA
+        uint32_t r, h;
+        place(x, r, h);
+        const uint32_t b = r * per;
+        for (uint32_t p = 0; p < per; ++p) {
+            const A a = ka(b + h);
+            const uint64_t top = M::ld64(a + 8 * (W - 1));
+            if (top == EMPTY) return NONE;
+            if constexpr (W == 1) { if (top == x.lo) return b + h; }
+            else { if (top == x.hi && M::ld64(a) == x.lo) return b + h; }
+            if (++h == per) h = 0;
         }
         return NONE;
     }
-    __device__ uint32_t find_or_insert(const Kmer<W>& x, bool& fresh) {
-        uint32_t h = (uint32_t)key_hash(x) & mask;
+    // build phase: find or insert x in sub-table `owner` starting at its home index h;
+    // returns the global slot or NONE.  Other ranks' sub-tables are reached through DSMEM.
+    __device__ uint32_t find_or_insert(const Kmer<W>& x, uint32_t owner, uint32_t h, bool& fresh) const {
         fresh = false;
-        for (uint32_t p = 0; p <= mask; ++p) {
+        const uint32_t b = owner * per;
+        for (uint32_t p = 0; p < per; ++p) {
+            const A a = ka(b + h);
             if constexpr (W == 1) {
-                const unsigned long long cur = ld(keys + h);
-                if (cur == x.lo) return h;
+                const uint64_t cur = M::ld64(a);
+                if (cur == x.lo) return b + h;
                 if (cur == EMPTY) {
-                    const unsigned long long old = atomicCAS(keys + h, EMPTY, (unsigned long long)x.lo);
-                    if (old == EMPTY) { fresh = true; return h; }
-                    if (old == x.lo) return h;
+                    const uint64_t old = M::cas64(a, EMPTY, x.lo);
+                    if (old == EMPTY) { fresh = true; return b + h; }
+                    if (old == x.lo) return b + h;
                 }
             } else {
-                const unsigned long long hi = ld(keys + 2 * h + 1);
-                if (hi == EMPTY || hi == x.hi) {
-                    uint64_t olo, ohi;
-                    cas128(keys + 2 * h, EMPTY, EMPTY, x.lo, x.hi, olo, ohi);
-                    if (olo == EMPTY && ohi == EMPTY) { fresh = true; return h; }
-                    if (olo == x.lo && ohi == x.hi) return h;
+                // two-word key: claim the high word with a 64-bit CAS (EMPTY -> BUSY), write
+                // the low word, then publish the high word; readers wait (bounded) on BUSY
+                uint64_t hi = M::ld64(a + 8);
+                if (hi == EMPTY) {
+                    hi = M::cas64(a + 8, EMPTY, BUSY);
+                    if (hi == EMPTY) {
+                        M::st64(a, x.lo);
+                        M::fence();
+                        M::exch64(a + 8, x.hi);
+                        fresh = true;
+                        return b + h;
+                    }
+                }
+                for (uint32_t spin = 0; hi == BUSY; ++spin) {
+                    if (spin > (1u << 24)) { atomicOr(err_flag, DERR_CAS_LIMIT); return NONE; }
+                    hi = M::ld64(a + 8);
+                }
+                if (hi == x.hi) {
+                    M::fence();
+                    if (M::ld64(a) == x.lo) return b + h;
                 }
             }
-            h = (h + 1) & mask;
+            if (++h == per) h = 0;
         }
         return NONE;
     }
+    // state word update: ef gets the edges, ins the earliest position (one CAS unless unchanged)
+    __device__ __forceinline__ void update_state(uint32_t s, uint32_t front, uint32_t back, uint32_t pos) const {
+        const A a = sa(s);
+        uint64_t cur = M::ld64(a);
+        for (uint32_t it = 0;; ++it) {
+            const uint32_t ef = ef_add((uint32_t)cur, front, back);
+            const uint32_t in = min((uint32_t)(cur >> 32), pos);
+            const uint64_t nv = (uint64_t)ef | ((uint64_t)in << 32);
+            if (nv == cur) return;
+            const uint64_t old = M::cas64(a, cur, nv);
+            if (old == cur) return;
+            cur = old;
+            if (it > (1u << 22)) { atomicOr(err_flag, DERR_CAS_LIMIT); return; }
+        }
+    }
+    __device__ __forceinline__ void mark_disc(uint32_t s, uint32_t disc) const {
+        const A a = ma(s);
+        if ((M::ld32(a) & disc) != disc) M::or32(a, disc);
+    }
 };
 
-struct Block {   // per-CTA shared bookkeeping
-    uint32_t inserted, overflow;
+struct Block {   // per-CTA shared bookkeeping (in CLUSTER mode the flags of rank 0 are the cluster's)
+    uint32_t inserted, overflow, wl_n, pad;
     unsigned long long vertices, isolated, phantom, trivial, icc, lmtig;
 };
+
+__device__ __forceinline__ uint32_t lane_lt() { uint32_t m; asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m)); return m; }
+
+// Appends every local slot ls < per with pred(ls) to the shared work list wl (order
+// unspecified).  All threads of the CTA must call it; blockDim is a multiple of 32.
+template <typename Pred>
+__device__ __forceinline__ void compact(uint32_t per, uint32_t* wl, uint32_t* n, Pred pred) {
+    const uint32_t nt = blockDim.x;
+    for (uint32_t base = 0; base < per; base += nt) {
+        const uint32_t ls = base + threadIdx.x;
+        const bool p = ls < per && pred(ls);
+        const uint32_t m = __ballot_sync(0xffffffffu, p);
+        uint32_t at = 0;
+        if ((threadIdx.x & 31) == 0 && m) at = atomicAdd(n, (uint32_t)__popc(m));
+        at = __shfl_sync(0xffffffffu, at, 0);
+        if (p) wl[at + __popc(m & lane_lt())] = ls;
+    }
+}
+
+template <int MODE> __device__ __forceinline__ void tsync() {
+    if constexpr (MODE == CLUSTER) cg::this_cluster().sync();
+    else __syncthreads();
+}
 
 template <int W>
 __device__ __forceinline__ Kmer<W> phi_kmer(const KOps<W>& ops) {   // all-T k-mer, include/Discontinuity_Graph.hpp:44-49
@@ -112,31 +251,46 @@ __device__ __forceinline__ Kmer<W> phi_kmer(const KOps<W>& ops) {   // all-T k-m
 }
 
 template <int W>
-__device__ __forceinline__ void put_key(uint64_t out[2], const Kmer<W>& x) {
-    out[0] = x.lo;
-    out[1] = x.hi_word();
+__device__ __forceinline__ void put_key(uint64_t out[2], const Kmer<W>& x) { out[0] = x.lo; out[1] = x.hi_word(); }
+
+// A vertex in walk direction: its directed k-mer, the reverse complement, and its slot.
+template <int W> struct DV { Kmer<W> d, r; uint32_t slot; };
+
+// Oriented vertex leaving slot s through `side`: the directed form is the canonical
+// k-mer when leaving through the back side (Directed_Vertex exit_side, :295-299).
+template <int W, int MODE>
+__device__ __forceinline__ DV<W> dv_at(const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t s, int side) {
+    const Kmer<W> x = T.key(s), xr = ops.rc(x);
+    return side == BACK ? DV<W>{x, xr, s} : DV<W>{xr, x, s};
 }
 
-// Writes the label of the path that starts at (slot, exit side) and has n vertices.
-template <int W, bool SM>
-__device__ void write_path(const Tab<W, SM>& T, const KOps<W>& ops, uint32_t s0, int side0, uint32_t n, char* dst, bool rev) {
-    const uint32_t k = ops.k;
-    const uint32_t L = n + k - 1;
-    const Kmer<W> x = T.key(s0);
-    const Kmer<W> d = side0 == BACK ? x : ops.rc(x);
-    auto put = [&](uint32_t i, uint32_t b) {
-        if (!rev) dst[i] = "ACGT"[b];
-        else dst[L - 1 - i] = "ACGT"[3 - b];
-    };
-    for (uint32_t i = 0; i < k; ++i) put(i, ops.base(d, i));
-    uint32_t cur = s0; int side = side0;
-    for (uint32_t t = 1; t < n; ++t) {
-        const uint32_t nb = T.ld(T.nbr + 2 * cur + side);
-        const uint32_t u = nb >> 1; const int s_in = (int)(nb & 1);
-        const Kmer<W> ku = T.key(u);
-        put(k - 1 + t, s_in == FRONT ? ops.last_base(ku) : 3 - ops.first_base(ku));
-        cur = u; side = 1 - s_in;
-    }
+// One walk step out of v through `side` (which must hold a single passing edge):
+// the next vertex and the side it is entered by.
+template <int W, int MODE>
+__device__ __forceinline__ bool step_inline(const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t fth, DV<W>& v, int side, int& s_in) {
+    const uint32_t e = ef_edge_at(st_ef(T.ld_st(v.slot)), side, fth);
+    const uint32_t b = side == BACK ? e : 3 - e;
+    ops.push_back(v.d, b);
+    ops.push_front(v.r, 3 - b);
+    const bool c = v.d < v.r;
+    const uint32_t u = T.find(c ? v.d : v.r);
+    if (u == NONE) return false;
+    v.slot = u;
+    s_in = c ? FRONT : BACK;
+    return true;
+}
+
+// Two-word (k > 32) walks take the step out of line: inlined into the path walk at
+// ptxas -O2/-O3 they failed lookups that the same source finds at -O1 or out of line.
+template <int W, int MODE>
+__device__ __noinline__ bool step_outline(const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t fth, DV<W>& v, int side,
+                                          int& s_in) {
+    return step_inline(T, ops, fth, v, side, s_in);
+}
+template <int W, int MODE>
+__device__ __forceinline__ bool step(const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t fth, DV<W>& v, int side, int& s_in) {
+    if constexpr (W == 1) return step_inline(T, ops, fth, v, side, s_in);
+    else return step_outline(T, ops, fth, v, side, s_in);
 }
 
 template <int W>
@@ -148,29 +302,81 @@ __device__ __forceinline__ char* reserve_fasta(const SubgraphArgs& a, uint32_t L
     return p + 3;
 }
 
-template <int W, bool SM>
-__device__ void emit_kmer_cycle(const SubgraphArgs& a, const Tab<W, SM>& T, const KOps<W>& ops, uint32_t s, Block& B) {
+// Writes the label of the path of n vertices that starts at v (in walk direction).
+template <int W, int MODE>
+__device__ void write_path(const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t fth, DV<W> v, int side, uint32_t n,
+                           char* dst, bool rev, bool mark) {
+    const uint32_t k = ops.k, L = n + k - 1;
+    auto put = [&](uint32_t i, uint32_t b) {
+        if (!rev) dst[i] = "ACGT"[b];
+        else dst[L - 1 - i] = "ACGT"[3 - b];
+    };
+    if (dst) for (uint32_t i = 0; i < k; ++i) put(i, ops.base(v.d, i));
+    if (mark) T.or_meta(v.slot, M_VISITED);
+    for (uint32_t t = 1; t < n; ++t) {
+        int s_in;
+        if (!step(T, ops, fth, v, side, s_in)) return;
+        if (dst) put(k - 1 + t, ops.last_base(v.d));
+        if (mark) T.or_meta(v.slot, M_VISITED);
+        side = 1 - s_in;
+    }
+}
+
+template <int W, int MODE>
+__device__ void emit_kmer_cycle(const SubgraphArgs& a, const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t s, Block& B) {
     char* p = reserve_fasta<W>(a, ops.k);
     if (p) { const Kmer<W> x = T.key(s); for (uint32_t i = 0; i < ops.k; ++i) p[i] = "ACGT"[ops.base(x, i)]; }
     atomicAdd(&B.trivial, 1ull); atomicAdd(&B.icc, 1ull);
 }
 
-struct EndInfo { uint32_t slot; uint32_t term; bool canon; };   // an end of a path in walk direction
+template <int W>
+__device__ __forceinline__ bool local_empty(const unsigned long long* lkeys, uint32_t ls) {
+    return lkeys[(size_t)ls * W + (W - 1)] == EMPTY;
+}
 
-template <int W, bool SM>
-__device__ void emit_path(const SubgraphArgs& a, const Tab<W, SM>& T, const KOps<W>& ops, uint32_t g,
-                          uint32_t s0, int side0, uint32_t n, EndInfo st, EndInfo en, bool seed_canon, Block& B) {
-    const uint32_t k = ops.k;
+struct EndInfo { uint32_t slot; uint32_t term; bool canon; };   // a path end in walk direction
+
+// The bases of one weak super k-mer (<= 128 of them), loaded once as four 64-bit
+// windows: the words are read up front, so the k-mer loop makes no memory access
+// for its predecessor/successor bases.  The packed stream carries 4 words of padding.
+struct RecBases {
+    uint64_t w0, w1, w2, w3;
+    __device__ __forceinline__ RecBases(const uint64_t* __restrict__ s, uint32_t pos, uint32_t len) {
+        const uint64_t q = pos >> 5;
+        const uint32_t sh = 2 * (pos & 31);
+        const uint64_t a0 = __ldg(s + q), a1 = __ldg(s + q + 1), a2 = len > 32 ? __ldg(s + q + 2) : 0;
+        const uint64_t a3 = len > 64 ? __ldg(s + q + 3) : 0, a4 = len > 96 ? __ldg(s + q + 4) : 0;
+        if (sh == 0) { w0 = a0; w1 = a1; w2 = a2; w3 = a3; }
+        else {
+            w0 = (a0 << sh) | (a1 >> (64 - sh)); w1 = (a1 << sh) | (a2 >> (64 - sh));
+            w2 = (a2 << sh) | (a3 >> (64 - sh)); w3 = (a3 << sh) | (a4 >> (64 - sh));
+        }
+    }
+    __device__ __forceinline__ uint32_t base(uint32_t i) const {
+        const uint32_t j = i >> 5;
+        const uint64_t w = j == 0 ? w0 : j == 1 ? w1 : j == 2 ? w2 : w3;
+        return (uint32_t)(w >> (62 - 2 * (i & 31))) & 3;
+    }
+    template <int W> __device__ __forceinline__ Kmer<W> first_kmer(uint32_t k) const {
+        if constexpr (W == 1) return Kmer<1>{w0 >> (64 - 2 * k)};
+        else {
+            const uint32_t nh = k - 32;   // bases in the high word
+            return Kmer<2>{(w0 << (2 * nh)) | (w1 >> (64 - 2 * nh)), w0 >> (64 - 2 * nh)};
+        }
+    }
+};
+
+template <int W, int MODE>
+__device__ void emit_path(const SubgraphArgs& a, const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t g, const DV<W>& v0,
+                          int side0, uint32_t n, const DV<W>& vlast, EndInfo st, EndInfo en, bool seed_canon, Block& B) {
+    const uint32_t k = ops.k, fth = a.fth;
     const uint32_t L = n + k - 1;
     const bool lm = st.term == T_EXIT || en.term == T_EXIT;
     if (!lm) {
         // trivial maximal unitig in canonical orientation (Maximal_Unitig_Scratch::finalize, :200-222)
-        const Kmer<W> xs = T.key(st.slot), xe = T.key(en.slot);
-        const Kmer<W> first = st.canon ? xs : ops.rc(xs);
-        const Kmer<W> last_rc = en.canon ? ops.rc(xe) : xe;
-        const bool rev = last_rc < first;
+        const bool rev = vlast.r < v0.d;   // rc(last k-mer) < first k-mer
         char* p = reserve_fasta<W>(a, L);
-        if (p) write_path(T, ops, s0, side0, n, p, rev);
+        write_path(T, ops, fth, v0, side0, n, p, rev, true);
         atomicAdd(&B.trivial, 1ull);
         return;
     }
@@ -182,8 +388,10 @@ __device__ void emit_path(const SubgraphArgs& a, const Tab<W, SM>& T, const KOps
     const unsigned long long idx = atomicAdd(&a.cnt->lm_count, 1ull);
     const unsigned long long off = atomicAdd(&a.cnt->lm_bytes, (unsigned long long)L);
     atomicAdd(&B.lmtig, 1ull);
-    if (idx >= a.lm_cap || off + L > a.lm_text_cap) { atomicOr(a.err, DERR_OUT_OVERFLOW); return; }
-    write_path(T, ops, s0, side0, n, a.lm_text + off, rev);
+    const bool fits = idx < a.lm_cap && off + L <= a.lm_text_cap;
+    if (!fits) atomicOr(a.err, DERR_OUT_OVERFLOW);
+    write_path(T, ops, fth, v0, side0, n, fits ? a.lm_text + off : nullptr, rev, true);
+    if (!fits) return;
     LmtigOut o;
     const Kmer<W> phi = phi_kmer(ops);
     const bool u_exit = eu.term == T_EXIT, v_exit = ev.term == T_EXIT;
@@ -197,90 +405,100 @@ __device__ void emit_path(const SubgraphArgs& a, const Tab<W, SM>& T, const KOps
     a.lm[idx] = o;
 }
 
-template <int W, bool SM>
-__device__ void run_subgraph(const SubgraphArgs& a, Tab<W, SM> T, uint32_t g, uint32_t cap, Block& B) {
+// rank/nranks: this CTA's position in its cluster; per: slots owned by one CTA.
+template <int W, int MODE>
+__device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block& B, Block* Bc,
+                             uint32_t g, uint32_t rank, uint32_t nranks, uint32_t per,
+                             unsigned long long* lkeys, unsigned long long* lst, uint32_t* lmeta, uint32_t* wl) {
+    long long clk[6];
+    clk[0] = clock64();
     const KOps<W> ops(a.k);
     const uint32_t k = a.k, fth = a.fth;
     const uint32_t tid = threadIdx.x, nt = blockDim.x;
+    const uint32_t base_slot = rank * per;
 
-    for (uint32_t s = tid; s < cap; s += nt) {
-        if constexpr (W == 1) T.keys[s] = EMPTY; else { T.keys[2 * s] = EMPTY; T.keys[2 * s + 1] = EMPTY; }
-        T.ef[s] = 0; T.meta[s] = 0; T.ins[s] = 0xffffffffu;
+    for (uint32_t s = tid; s < per; s += nt) {
+        if constexpr (W == 1) lkeys[s] = EMPTY; else { lkeys[2 * s] = EMPTY; lkeys[2 * s + 1] = EMPTY; }
+        lst[s] = 0xffffffff00000000ull;   // ef 0, first occurrence "none"
+        lmeta[s] = 0;
     }
-    if (tid == 0) { B.inserted = 0; B.overflow = 0; B.vertices = B.isolated = B.phantom = B.trivial = B.icc = B.lmtig = 0; }
-    __syncthreads();
+    if (tid == 0) { B.inserted = 0; B.overflow = 0; B.wl_n = 0; B.vertices = B.isolated = B.phantom = B.trivial = B.icc = B.lmtig = 0; }
+    tsync<MODE>();
 
     // ---------------- build ----------------
-    const uint32_t limit = (uint32_t)(((uint64_t)cap * a.load_limit_pct) / 100);
+    const uint32_t limit = (uint32_t)(((uint64_t)per * a.load_limit_pct) / 100);
     const uint32_t r0 = a.bucket_off[g], r1 = a.bucket_off[g + 1];
-    for (uint32_t r = r0 + tid; r < r1; r += nt) {
+    for (uint32_t r = r0 + rank * nt + tid; r < r1; r += nranks * nt) {
         if (*(volatile uint32_t*)&B.overflow) break;
         const uint64_t rec = a.recs[r];
         const uint32_t pos = rec_pos(rec), len = rec_len(rec), ld = rec_ld(rec), rd = rec_rd(rec);
-        Kmer<W> fw = ops.load(a.packed, pos);
+        const RecBases rb(a.packed, pos, len);   // the whole record in registers (<= 128 bases)
+        Kmer<W> fw = rb.first_kmer<W>(k);
         Kmer<W> rc = ops.rc(fw);
         Kmer<W> pred_can = fw;
         for (uint32_t idx = 0;; ++idx) {
             const bool canon = fw < rc;
             const Kmer<W> can = canon ? fw : rc;
-            const uint32_t pred = idx == 0 ? BASE_E : base_at(a.packed, pos + idx - 1);
-            const uint32_t succ = idx + k == len ? BASE_E : base_at(a.packed, pos + idx + k);
+            const uint32_t pred = idx == 0 ? BASE_E : rb.base(idx - 1);
+            const uint32_t succ = idx + k == len ? BASE_E : rb.base(idx + k);
             uint32_t front = canon ? pred : compb(succ);
             uint32_t back = canon ? succ : compb(pred);
             if (idx > 0 && can == pred_can) { if (canon) front = BASE_E; else back = BASE_E; }
+            uint32_t owner, h;
+            T.place(can, owner, h);
             bool fresh;
-            const uint32_t s = T.find_or_insert(can, fresh);
+            const uint32_t s = T.find_or_insert(can, owner, h, fresh);
             if (s == NONE) { atomicOr(&B.overflow, 1u); break; }
+            // fresh vertices are counted per inserting CTA (records, hence inserts, are spread
+            // evenly, so one CTA's count stands for one sub-table's load)
             if (fresh && atomicAdd(&B.inserted, 1u) + 1 > limit) { atomicOr(&B.overflow, 1u); break; }
-            uint32_t cur = T.ld(T.ef + s);
-            for (uint32_t it = 0;; ++it) {
-                const uint32_t nv = ef_add(cur, front, back);
-                if (nv == cur) break;
-                const uint32_t old = atomicCAS(T.ef + s, cur, nv);
-                if (old == cur) break;
-                cur = old;
-                if (it > (1u << 22)) { atomicOr(a.err, DERR_CAS_LIMIT); break; }
-            }
-            const uint32_t p = pos + idx;
-            if (p < T.ld(T.ins + s)) atomicMin(T.ins + s, p);
+            T.update_state(s, front, back, pos + idx);
             uint32_t disc = 0;
             if (idx == 0 && ld) disc |= canon ? M_DISC_F : M_DISC_B;            // entrance side
             if (idx + k == len && rd) disc |= canon ? M_DISC_B : M_DISC_F;      // exit side
-            if (disc && (T.ld(T.meta + s) & disc) != disc) atomicOr(T.meta + s, disc);
+            if (disc) T.mark_disc(s, disc);
             if (idx + k == len) break;
             pred_can = can;
             ops.push_back(fw, succ);
             ops.push_front(rc, 3 - succ);
         }
     }
+    // one CTA's overflow is the whole cluster's
     __syncthreads();
-    if (B.overflow) {
-        if (tid == 0) {
+    if (tid == 0 && B.overflow && Bc != &B) atomicOr(&Bc->overflow, 1u);
+    tsync<MODE>();
+    const bool overflow = *(volatile uint32_t*)&Bc->overflow;
+    if (overflow) {
+        if (rank == 0 && tid == 0) {
             const unsigned long long i = atomicAdd(&a.cnt->retry_count, 1ull);
             a.retry[i] = g;
         }
+        tsync<MODE>();   // no CTA leaves while another may still read its shared memory
         return;
     }
 
-    // ---------------- W1: neighbour links ----------------
-    for (uint32_t s = tid; s < cap; s += nt) {
-        if (T.empty(s)) continue;
-        const uint32_t ef = T.ef[s];
-        uint32_t meta = T.meta[s];
+    clk[1] = clock64();
+    // ---------------- W1: termination of every side ----------------
+    compact(per, wl, &B.wl_n, [&](uint32_t ls) { return !local_empty<W>(lkeys, ls); });
+    __syncthreads();
+    for (uint32_t i = tid, nw = B.wl_n; i < nw; i += nt) {
+        const uint32_t ls = wl[i];
+        const uint32_t s = base_slot + ls;
+        const uint32_t ef = st_ef(lst[ls]);
+        uint32_t meta = lmeta[ls];
         const uint32_t cf = ef_count(ef, FRONT, fth), cb = ef_count(ef, BACK, fth);
         atomicAdd(&B.vertices, 1ull);
         if (cf == 0 && cb == 0) {
             atomicAdd(&B.isolated, 1ull);
             if (meta & (M_DISC_F | M_DISC_B)) atomicAdd(&B.phantom, 1ull);
-            T.meta[s] = meta | M_ISO;
-            T.nbr[2 * s] = NONE; T.nbr[2 * s + 1] = NONE;
+            lmeta[ls] = meta | M_ISO;
             continue;
         }
         const Kmer<W> x = T.key(s);
         const Kmer<W> xr = ops.rc(x);
         for (int side = 0; side < 2; ++side) {
             const uint32_t e = ef_edge_at(ef, side, fth);
-            uint32_t term = T_OK, link = NONE;
+            uint32_t term = T_OK;
             if (e == BASE_N) term = T_BRANCHED;
             else if (e == BASE_E) term = (meta & (side == FRONT ? M_DISC_F : M_DISC_B)) ? T_EXIT : T_DEAD;
             else {
@@ -291,61 +509,72 @@ __device__ void run_subgraph(const SubgraphArgs& a, Tab<W, SM> T, uint32_t g, ui
                 const uint32_t u = T.find(yc ? y : yr);
                 const int s_in = yc ? FRONT : BACK;
                 if (u == NONE) { atomicOr(a.err, DERR_MISSING_KEY); term = T_CROSSED; }
-                else if (u == s) term = T_CROSSED;                               // self-loop
-                else if (ef_count(T.ef[u], s_in, fth) > 1) term = T_CROSSED;     // branching entrance
-                else link = (u << 1) | (uint32_t)s_in;
+                else if (u == s) term = T_CROSSED;                                        // self-loop
+                else if (ef_count(st_ef(T.ld_st(u)), s_in, fth) > 1) term = T_CROSSED;    // branching entrance
             }
-            T.nbr[2 * s + side] = link;
             meta |= term << (side == FRONT ? 8 : 11);
         }
         // homopolymer b^k (b in {A, C}) whose back side holds only its self-loop
         const uint32_t eb = ef_edge_at(ef, BACK, fth);
         if (eb < 2 && cf <= 1 && ops.is_homopolymer(x, eb)) meta |= M_Q;
-        T.meta[s] = meta;
+        lmeta[ls] = meta;
     }
-    __syncthreads();
+    tsync<MODE>();
 
+    clk[2] = clock64();
     // ---------------- W2: paths, walked from their ends ----------------
-    for (uint32_t s = tid; s < cap; s += nt) {
-        if (T.empty(s)) continue;
-        const uint32_t meta = T.meta[s];
-        if (meta & M_ISO) continue;
-        const uint32_t nf = T.nbr[2 * s], nb = T.nbr[2 * s + 1];
-        if (nf != NONE && nb != NONE) continue;   // interior (or cycle) vertex
-        if (nf == NONE && nb == NONE) {           // one-vertex path
+    if (tid == 0) B.wl_n = 0;
+    __syncthreads();
+    compact(per, wl, &B.wl_n, [&](uint32_t ls) {
+        if (local_empty<W>(lkeys, ls)) return false;
+        const uint32_t m = lmeta[ls];
+        return !(m & M_ISO) && (term_of(m, FRONT) != T_OK || term_of(m, BACK) != T_OK);
+    });
+    __syncthreads();
+    for (uint32_t i = tid, nw = B.wl_n; i < nw; i += nt) {
+        const uint32_t ls = wl[i];
+        const uint32_t s = base_slot + ls;
+        const uint32_t meta = lmeta[ls];
+        const bool okf = term_of(meta, FRONT) == T_OK, okb = term_of(meta, BACK) == T_OK;
+        if (!okf && !okb) {         // one-vertex path
             if (meta & M_Q) emit_kmer_cycle(a, T, ops, s, B);
             else {
+                const DV<W> v = dv_at(T, ops, s, BACK);
                 const EndInfo st{s, term_of(meta, FRONT), true}, en{s, term_of(meta, BACK), true};
-                emit_path(a, T, ops, g, s, BACK, 1, st, en, true, B);
+                emit_path(a, T, ops, g, v, BACK, 1, v, st, en, true, B);
             }
-            T.meta[s] = meta | M_VISITED;
+            lmeta[ls] = lmeta[ls] | M_VISITED;
             continue;
         }
-        const int side0 = nf != NONE ? FRONT : BACK;   // walk through the linked side
-        // pass 1: find the other end, first-occurrence minima
-        uint32_t cur = s; int side = side0;
+        const int side0 = okf ? FRONT : BACK;   // walk through the linked side
+        const uint32_t ins0 = st_ins(lst[ls]);
+        const DV<W> v0 = dv_at(T, ops, s, side0);
+        // pass 1: the other end, first-occurrence minima
+        DV<W> v = v0; int side = side0;
         uint32_t n = 1;
-        uint32_t p1 = NONE; int p1_side = 0;          // second vertex
-        uint32_t prev = NONE; int prev_side = 0;      // vertex before the current one
+        uint32_t v1_slot = s; int v1_side = side0;     // second vertex
+        uint32_t vp_slot = s; int vp_side = side0;     // vertex before the current one
         uint32_t m_int = 0xffffffffu; bool m_int_canon = true;
+        uint32_t cur_meta = meta;
         bool ok = true;
-        while (true) {
-            const uint32_t lnk = T.nbr[2 * cur + side];
-            if (lnk == NONE) break;
-            if (cur != s) {   // cur is interior
-                const uint32_t ic = T.ins[cur];
+        while (term_of(cur_meta, side) == T_OK) {
+            if (n > 1) {   // v is interior
+                const uint32_t ic = st_ins(T.ld_st(v.slot));
                 if (ic < m_int) { m_int = ic; m_int_canon = side == BACK; }
             }
-            prev = cur; prev_side = side;
-            cur = lnk >> 1; side = 1 - (int)(lnk & 1);
-            if (n == 1) { p1 = cur; p1_side = side; }
-            if (++n > cap + 1) { atomicOr(a.err, DERR_WALK_LIMIT); ok = false; break; }
+            vp_slot = v.slot; vp_side = side;
+            int s_in;
+            if (!step(T, ops, fth, v, side, s_in)) { atomicOr(a.err, DERR_MISSING_KEY); ok = false; break; }
+            side = 1 - s_in;
+            cur_meta = T.ld_meta(v.slot);
+            if (n == 1) { v1_slot = v.slot; v1_side = side; }
+            if (++n > T.per * T.nranks + 1) { atomicOr(a.err, DERR_WALK_LIMIT); ok = false; break; }
         }
         if (!ok) continue;
-        const uint32_t e = cur; const int e_side = side;   // other end, walk stops at its side e_side
-        if (e < s) continue;                                // the smaller end emits
-        const uint32_t meta_e = T.meta[e];
-        const uint32_t ins0 = T.ins[s], ins1 = T.ins[e];
+        const uint32_t e = v.slot; const int e_side = side;   // other end; the walk stops at its side e_side
+        if (e < s) continue;                                   // the smaller end emits
+        const uint32_t meta_e = cur_meta;
+        const uint32_t ins1 = st_ins(T.ld_st(e));
         const bool q0 = meta & M_Q, q1 = meta_e & M_Q;
         uint32_t m = m_int;
         if (!q0 && ins0 < m) m = ins0;
@@ -356,134 +585,158 @@ __device__ void run_subgraph(const SubgraphArgs& a, Tab<W, SM> T, uint32_t g, ui
         const uint32_t n2 = n - fake0 - fake1;
         if (n2 > 0) {
             EndInfo st, en;
-            uint32_t s0; int sd0;
-            if (!fake0) { st = EndInfo{s, term_of(meta, 1 - side0), side0 == BACK}; s0 = s; sd0 = side0; }
-            else { st = EndInfo{p1, T_CROSSED, p1_side == BACK}; s0 = p1; sd0 = p1_side; }
-            if (!fake1) en = EndInfo{e, term_of(meta_e, e_side), e_side == BACK};
-            else en = EndInfo{prev, T_CROSSED, prev_side == BACK};
+            DV<W> vs; int sd0;
+            if (!fake0) { st = EndInfo{s, term_of(meta, 1 - side0), side0 == BACK}; vs = v0; sd0 = side0; }
+            else { st = EndInfo{v1_slot, T_CROSSED, v1_side == BACK}; vs = dv_at(T, ops, v1_slot, v1_side); sd0 = v1_side; }
+            DV<W> ve;
+            if (!fake1) { en = EndInfo{e, term_of(meta_e, e_side), e_side == BACK}; ve = v; }
+            else { en = EndInfo{vp_slot, T_CROSSED, vp_side == BACK}; ve = dv_at(T, ops, vp_slot, vp_side); }
             // first-inserted vertex of the emitted path and its orientation along the walk
             uint32_t best = m_int; bool best_canon = m_int_canon;
             if (!fake0 && ins0 < best) { best = ins0; best_canon = side0 == BACK; }
             if (!fake1 && ins1 < best) { best = ins1; best_canon = e_side == BACK; }
-            emit_path(a, T, ops, g, s0, sd0, n2, st, en, best_canon, B);
+            emit_path(a, T, ops, g, vs, sd0, n2, ve, st, en, best_canon, B);
         }
-        // mark the whole path visited
-        cur = s; side = side0;
-        T.meta[cur] |= M_VISITED;
-        for (uint32_t t = 1; t < n; ++t) {
-            const uint32_t lnk = T.nbr[2 * cur + side];
-            cur = lnk >> 1; side = 1 - (int)(lnk & 1);
-            T.meta[cur] |= M_VISITED;
-        }
+        if (fake0) T.or_meta(s, M_VISITED);
+        if (fake1) T.or_meta(e, M_VISITED);
     }
-    __syncthreads();
+    tsync<MODE>();
 
+    clk[3] = clock64();
     // ---------------- W3: isolated cycles ----------------
-    for (uint32_t s = tid; s < cap; s += nt) {
-        if (T.empty(s)) continue;
-        const uint32_t meta = T.ld(T.meta + s);
-        if (meta & (M_ISO | M_VISITED)) continue;
+    if (tid == 0) B.wl_n = 0;
+    __syncthreads();
+    compact(per, wl, &B.wl_n, [&](uint32_t ls) {
+        return !local_empty<W>(lkeys, ls) && !(lmeta[ls] & (M_ISO | M_VISITED));
+    });
+    __syncthreads();
+    for (uint32_t i = tid, nw = B.wl_n; i < nw; i += nt) {
+        const uint32_t ls = wl[i];
+        const uint32_t s = base_slot + ls;
+        if (*(volatile uint32_t*)(lmeta + ls) & M_VISITED) continue;
         // every vertex left has both sides linked: walk the cycle from s out of its back side
-        const Kmer<W> xs = T.key(s);
-        uint32_t cur = s; int side = BACK; uint32_t n = 0;
+        const DV<W> v0 = dv_at(T, ops, s, BACK);
+        DV<W> v = v0; int side = BACK; uint32_t n = 0;
         bool is_min = true, ok = true;
         do {
-            const uint32_t lnk = T.nbr[2 * cur + side];
-            if (lnk == NONE || ++n > cap) { atomicOr(a.err, DERR_WALK_LIMIT); ok = false; break; }
-            cur = lnk >> 1; side = 1 - (int)(lnk & 1);
-            if (cur != s && T.key(cur) < xs) is_min = false;
-        } while (cur != s);
+            int s_in;
+            if (!step(T, ops, fth, v, side, s_in) || ++n > T.per * T.nranks) { atomicOr(a.err, DERR_WALK_LIMIT); ok = false; break; }
+            side = 1 - s_in;
+            if (v.slot != s && (v.d < v.r ? v.d : v.r) < v0.d) is_min = false;
+        } while (v.slot != s);
         if (!ok || !is_min) continue;
         // Character_Buffer::rotate_append_cycle (include/Character_Buffer.hpp:166-175): start at the
         // minimum vertex in its canonical orientation
         char* p = reserve_fasta<W>(a, n + k - 1);
-        if (p) write_path(T, ops, s, BACK, n, p, false);
+        write_path(T, ops, fth, v0, BACK, n, p, false, true);
         atomicAdd(&B.trivial, 1ull); atomicAdd(&B.icc, 1ull);
-        cur = s; side = BACK;
-        for (uint32_t t = 0; t < n; ++t) {
-            T.meta[cur] |= M_VISITED;
-            const uint32_t lnk = T.nbr[2 * cur + side];
-            cur = lnk >> 1; side = 1 - (int)(lnk & 1);
-        }
     }
-    __syncthreads();
+    tsync<MODE>();
+    clk[4] = clock64();
 
     if (a.dump) {
-        for (uint32_t s = tid; s < cap; s += nt) {
-            if (T.empty(s)) continue;
+        for (uint32_t ls = tid; ls < per; ls += nt) {
+            const uint32_t s = base_slot + ls;
+            if (local_empty<W>(lkeys, ls)) continue;
             const unsigned long long i = atomicAdd(&a.cnt->dump_count, 1ull);
             if (i >= a.dump_cap) { atomicOr(a.err, DERR_DUMP_OVERFLOW); continue; }
             StateOut o;
             put_key(o.key, T.key(s));
-            o.ef = T.ef[s]; o.g = (uint16_t)g; o.status = (uint8_t)(T.meta[s] & 7); o.pad = 0;
+            o.ef = st_ef(lst[ls]); o.g = (uint16_t)g; o.status = (uint8_t)(lmeta[ls] & 7); o.pad = 0;
             a.dump[i] = o;
         }
     }
+    __syncthreads();
     if (tid == 0) {
+        clk[5] = clock64();
+        for (int i = 0; i < 5; ++i) atomicAdd(&a.cnt->phase_cycles[i], (unsigned long long)(clk[i + 1] - clk[i]));
         atomicAdd(&a.cnt->vertices, B.vertices); atomicAdd(&a.cnt->isolated, B.isolated);
         atomicAdd(&a.cnt->phantom, B.phantom); atomicAdd(&a.cnt->trivial, B.trivial);
         atomicAdd(&a.cnt->icc, B.icc); atomicAdd(&a.cnt->lmtig, B.lmtig);
     }
+    tsync<MODE>();   // no CTA leaves while another may still read its shared memory
 }
 
 template <int W>
-__global__ void __launch_bounds__(256) k_subgraph_smem(const SubgraphArgs a) {
+__device__ __forceinline__ void carve(unsigned char* base, uint32_t per, unsigned long long*& keys, unsigned long long*& st,
+                                      uint32_t*& meta, uint32_t*& wl) {
+    keys = (unsigned long long*)base;
+    st = (unsigned long long*)(base + (size_t)per * 8 * W);
+    meta = (uint32_t*)(base + (size_t)per * (8 * W + 8));
+    wl = meta + per;
+}
+
+// One subgraph per CTA (per = the table's whole capacity) or per cluster.
+template <int W, int MODE>
+__global__ void __launch_bounds__(512) k_subgraph_shared(const SubgraphArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ Block B;
-    const uint32_t cap = a.smem_cap;
-    Tab<W, true> T;
-    T.keys = (unsigned long long*)smem;
-    T.ef = (uint32_t*)(smem + (size_t)cap * 8 * W);
-    T.meta = T.ef + cap;
-    T.ins = T.meta + cap;
-    T.nbr = T.ins + cap;
-    T.mask = cap - 1;
-    for (uint32_t i = blockIdx.x; i < a.n_list; i += gridDim.x) {
-        const uint32_t g = a.list[i];
-        run_subgraph<W, true>(a, T, g, cap, B);
-        __syncthreads();
-    }
+    uint32_t rank = 0, nranks = 1;
+    if constexpr (MODE == CLUSTER) { rank = cg::this_cluster().block_rank(); nranks = cg::this_cluster().num_blocks(); }
+    const uint32_t per = a.smem_cap;
+    Tab<W, MODE> T;
+    unsigned long long *lk, *ls; uint32_t *lm, *wl;
+    carve<W>(smem, per, lk, ls, lm, wl);
+    T.keys = smem_addr(lk); T.st = smem_addr(ls); T.meta = smem_addr(lm); T.err_flag = a.err;
+    T.per = per; T.nranks = nranks; T.rank = rank;
+    T.shift = 31 - __clz(per); T.pmask = per - 1;
+    Block* Bc = &B;
+    if constexpr (MODE == CLUSTER) Bc = cg::this_cluster().map_shared_rank(&B, 0);
+    const uint32_t i = blockIdx.x / nranks;
+    if (i < a.n_list) run_subgraph<W, MODE>(a, T, B, Bc, a.list[i], rank, nranks, per, lk, ls, lm, wl);
 }
 
 template <int W>
 __global__ void __launch_bounds__(512) k_subgraph_global(const SubgraphArgs a) {
     __shared__ Block B;
     for (uint32_t i = blockIdx.x; i < a.n_list; i += gridDim.x) {
-        const uint32_t g = a.list[i];
         const uint32_t cap = a.tab_cap[i];
         unsigned char* base = a.arena + a.tab_off[i] * (uint64_t)slot_bytes(W);
-        Tab<W, false> T;
-        T.keys = (unsigned long long*)base;
-        T.ef = (uint32_t*)(base + (size_t)cap * 8 * W);
-        T.meta = T.ef + cap;
-        T.ins = T.meta + cap;
-        T.nbr = T.ins + cap;
-        T.mask = cap - 1;
-        run_subgraph<W, false>(a, T, g, cap, B);
+        Tab<W, GLOBAL> T;
+        unsigned long long *lk, *ls; uint32_t *lm, *wl;
+        carve<W>(base, cap, lk, ls, lm, wl);
+        T.keys = (uint64_t)lk; T.st = (uint64_t)ls; T.meta = (uint64_t)lm;
+        T.per = cap; T.nranks = 1; T.rank = 0; T.shift = 31; T.pmask = 0xffffffffu; T.err_flag = a.err;
+        run_subgraph<W, GLOBAL>(a, T, B, &B, a.list[i], 0, 1, cap, lk, ls, lm, wl);
         __syncthreads();
     }
 }
 
+template <typename K>
+cudaError_t launch_shared(K kernel, const SubgraphArgs& a, uint32_t cluster, uint32_t threads, size_t bytes, cudaStream_t s) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(a.n_list * cluster);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = bytes;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster; attr[0].val.clusterDim.y = 1; attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = cluster > 1 ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, a);
+}
+
 }  // namespace
 
-int subgraph_max_smem_cap(int words) { return words == 1 ? 4096 : 4096; }
+uint32_t subgraph_max_per_cta(int words) { return words == 1 ? 4096 : 2048; }
+uint32_t subgraph_cluster_per_cta(int words) { return words == 1 ? 4096 : 2048; }
 
-void launch_subgraphs(const SubgraphArgs& a, int words, bool smem, uint32_t threads, cudaStream_t s) {
-    if (a.n_list == 0) return;
-    const unsigned grid = a.n_list;
-    if (smem) {
-        const size_t bytes = (size_t)a.smem_cap * slot_bytes(words);
-        if (words == 1) {
-            cudaFuncSetAttribute(k_subgraph_smem<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-            k_subgraph_smem<1><<<grid, threads, bytes, s>>>(a);
-        } else {
-            cudaFuncSetAttribute(k_subgraph_smem<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-            k_subgraph_smem<2><<<grid, threads, bytes, s>>>(a);
-        }
-    } else {
-        if (words == 1) k_subgraph_global<1><<<grid, threads, 0, s>>>(a);
-        else k_subgraph_global<2><<<grid, threads, 0, s>>>(a);
+cudaError_t launch_subgraphs(const SubgraphArgs& a, int words, uint32_t cluster, uint32_t threads, cudaStream_t s) {
+    if (a.n_list == 0) return cudaSuccess;
+    if (cluster == 0) {   // global-memory tables
+        if (words == 1) k_subgraph_global<1><<<a.n_list, threads, 0, s>>>(a);
+        else k_subgraph_global<2><<<a.n_list, threads, 0, s>>>(a);
+        return cudaGetLastError();
     }
+    const size_t bytes = (size_t)a.smem_cap * slot_bytes(words);
+    if (cluster == 1)
+        return words == 1 ? launch_shared(k_subgraph_shared<1, LOCAL>, a, 1, threads, bytes, s)
+                          : launch_shared(k_subgraph_shared<2, LOCAL>, a, 1, threads, bytes, s);
+    return words == 1 ? launch_shared(k_subgraph_shared<1, CLUSTER>, a, cluster, threads, bytes, s)
+                      : launch_shared(k_subgraph_shared<2, CLUSTER>, a, cluster, threads, bytes, s);
 }
 
 }  // namespace cfg

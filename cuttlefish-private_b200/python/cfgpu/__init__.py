@@ -30,7 +30,7 @@ class Params(ctypes.Structure):
 class Counts(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in (
         "n_bases", "n_records", "n_instances", "n_vertices", "n_isolated", "n_phantom", "n_trivial",
-        "n_icc", "n_lmtig", "fasta_bytes", "lmtig_bytes", "n_retries")]
+        "n_icc", "n_lmtig", "fasta_bytes", "lmtig_bytes", "n_retries", "n_launches")]
 
 
 class Lmtig(ctypes.Structure):
@@ -78,6 +78,7 @@ SIGNATURES = {
     "cfg_dump_states": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(StateDump)]),
     "cfg_dump_records": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(RecordDump)]),
     "cfg_last_timings": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
+    "cfg_last_phase_cycles": (ctypes.c_int, [ctypes.c_void_p, U64P]),
     "cfg_last_error_string": (ctypes.c_char_p, [ctypes.c_void_p]),
     "cfg_destroy": (None, [ctypes.c_void_p]),
     "cfg_pack_records": (ctypes.c_int, [ctypes.c_char_p, U64P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int,
@@ -207,6 +208,17 @@ class Compactor:
         t = (ctypes.c_float * 4)()
         _check(self.lib, self.ctx, self.lib.cfg_last_timings(self.ctx, t), "cfg_last_timings")
         return list(t)
+
+    def phase_cycles(self):
+        t = (ctypes.c_uint64 * 5)()
+        _check(self.lib, self.ctx, self.lib.cfg_last_phase_cycles(self.ctx, t), "cfg_last_phase_cycles")
+        return list(t)
+
+    def fetch_raw(self) -> Results:
+        """cfg_fetch only: the outputs land in the context's page-locked host buffers."""
+        r = Results()
+        _check(self.lib, self.ctx, self.lib.cfg_fetch(self.ctx, ctypes.byref(r)), "cfg_fetch")
+        return r
 
     def fetch(self):
         r = Results()

@@ -50,8 +50,10 @@ typedef struct cfg_params {
     uint32_t cutoff;       /* edge-frequency threshold, 1..15                   (-c)             */
     uint32_t graph_count;  /* power of two <= 65536; the reference uses 16384 (include/Atlas.hpp:33-35) */
     uint32_t flags;        /* CFG_FLAG_* */
-    uint32_t table_load_pct;  /* expected distinct/instances ratio in percent used to size tables;
-                                 0 = default (125 for references, pass ~50 for deep read sets) */
+    uint32_t table_load_pct;  /* expected distinct vertices per k-mer instance, in percent, used to
+                                 size subgraph tables (at about half load); 0 = default 100 (one
+                                 genome); deep read sets need ~20.  A wrong guess costs only a
+                                 rebuild of the tables that overflow. */
     uint32_t reserved[2];
 } cfg_params;
 
@@ -70,7 +72,8 @@ typedef struct cfg_counts {
     uint64_t n_lmtig;       /* lm-tigs == discontinuity edges */
     uint64_t fasta_bytes;   /* bytes of trivial-unitig FASTA text */
     uint64_t lmtig_bytes;   /* bytes of lm-tig labels */
-    uint64_t n_retries;     /* subgraph-phase relaunches after table/arena overflow */
+    uint64_t n_retries;     /* subgraph tables abandoned for overflow and rebuilt larger */
+    uint64_t n_launches;    /* kernels launched by the run */
 } cfg_counts;
 
 /* One discontinuity edge with its lm-tig (Discontinuity_Graph::add_edge arguments). */
@@ -146,9 +149,16 @@ int cfg_dump_states(cfg_ctx* ctx, cfg_state_dump* out);
 /* Bucketed weak super k-mers of the last run (needs CFG_FLAG_DUMP_RECORDS). */
 int cfg_dump_records(cfg_ctx* ctx, cfg_record_dump* out);
 
-/* Device time of the last cfg_run's kernels, in milliseconds:
- * [0] partition, [1] bucket scatter, [2] subgraph construct+walk, [3] whole run. */
+/* Device time of the last cfg_run, in milliseconds, from CUDA events on the
+ * context's stream: [0] partition kernel, [1] bucket scan + scatter kernels,
+ * [2] subgraph construct+walk kernels (all launches), [3] the whole run
+ * including the host-side planning between phases. */
 int cfg_last_timings(cfg_ctx* ctx, float out_ms[4]);
+
+/* Profiling aid: SM clock cycles of the last run's subgraph kernels, summed over
+ * CTAs, per phase: [0] table build, [1] side terminations, [2] path walks,
+ * [3] cycle walks, [4] state dump and counters. */
+int cfg_last_phase_cycles(cfg_ctx* ctx, uint64_t out[5]);
 
 const char* cfg_last_error_string(cfg_ctx* ctx);
 

@@ -127,6 +127,22 @@ class OracleRun:
         return fasta_multiset(self.fasta)
 
 
+def timed_run(data, offsets, n_rec, k, l, cutoff, graph_count=16384, threads=1):
+    """Runs the oracle once and returns its wall time in seconds (no Python-side conversion)."""
+    import time
+    lib = load()
+    p = Params(k, l, cutoff, graph_count)
+    ctx = lib.orc_create(ctypes.byref(p))
+    if not ctx:
+        raise ValueError("invalid oracle parameters")
+    try:
+        t0 = time.perf_counter()
+        assert lib.orc_run(ctx, data, offsets, n_rec, threads) == 0
+        return time.perf_counter() - t0
+    finally:
+        lib.orc_destroy(ctx)
+
+
 def fasta_multiset(fasta: bytes):
     """FASTA text '>0\\nSEQ\\n...' -> Counter of (header, seq)."""
     out = collections.Counter()

@@ -89,7 +89,7 @@ def test_reads_cutoff2():
     rng = np.random.default_rng(22)
     g = synth.genome_with_repeats(rng, 20_000, n_copies=5, n_pal=3)
     rd = synth.reads(rng, g, 3_000)
-    compare(rd, 31, 20, 2, 16384, load_pct=60)
+    compare(rd, 31, 20, 2, 16384, load_pct=30)
 
 
 def test_homopolymer_and_cycles():
@@ -98,6 +98,15 @@ def test_homopolymer_and_cycles():
     for k, l in ((5, 3), (9, 4), (31, 20)):
         for G in (1, 16, 16384):
             compare(recs, k, l, 1, G)
+
+
+@pytest.mark.parametrize("k", [31, 63])
+@pytest.mark.parametrize("load_pct", [1500, 4500, 40000])
+def test_table_modes(k, load_pct):
+    """Oversized table requests route subgraphs to one-CTA, cluster (DSMEM) and global-arena tables."""
+    rng = np.random.default_rng(24 + load_pct)
+    recs = [synth.adversarial(rng, 20_000, k) for _ in range(2)]
+    compare(recs, k, 20, 1, 64, load_pct=load_pct)
 
 
 def test_small_table_retry():
