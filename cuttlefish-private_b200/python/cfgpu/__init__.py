@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(PKG_DIR, "lib", "libcfgpu.so")
 
 CFG_FLAG_DUMP_STATES = 0x1
 CFG_FLAG_DUMP_RECORDS = 0x2
+CFG_NOALLOC_MAX_BASES = 917472
 
 ERRORS = {0: "OK", 1: "BAD_INPUT", 2: "OOM", 3: "TABLE_FULL", 4: "WALK_LIMIT", 5: "CUDA", 6: "STATE"}
 
@@ -81,6 +82,9 @@ SIGNATURES = {
     "cfg_last_phase_cycles": (ctypes.c_int, [ctypes.c_void_p, U64P]),
     "cfg_last_error_string": (ctypes.c_char_p, [ctypes.c_void_p]),
     "cfg_destroy": (None, [ctypes.c_void_p]),
+    "cfg_partition_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_uint64,
+                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                             ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cfg_pack_records": (ctypes.c_int, [ctypes.c_char_p, U64P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int,
                                         ctypes.POINTER(Packed)]),
     "cfg_packed_free": (None, [ctypes.POINTER(Packed)]),
