@@ -85,6 +85,10 @@ SIGNATURES = {
     "cfg_partition_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_uint64,
                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
                                              ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "cfg_collate_lmtigs": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                          ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_uint64),
+                                          ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
+    "cfg_free": (None, [ctypes.c_void_p]),
     "cfg_pack_records": (ctypes.c_int, [ctypes.c_char_p, U64P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int,
                                         ctypes.POINTER(Packed)]),
     "cfg_packed_free": (None, [ctypes.POINTER(Packed)]),
@@ -246,6 +250,35 @@ class Compactor:
         d = RecordDump()
         _check(self.lib, self.ctx, self.lib.cfg_dump_records(self.ctx, ctypes.byref(d)), "cfg_dump_records")
         return [(d.records[i].pos, d.records[i].len, d.records[i].flags, d.records[i].g) for i in range(d.n)]
+
+
+def collate(k, lmtig_array, n, text_ptr):
+    """cfg_collate_lmtigs over raw buffers -> (FASTA bytes, n_unitigs, n_cycles)."""
+    lib = load()
+    out = ctypes.c_void_p()
+    nb, nu, nc = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+    rc = lib.cfg_collate_lmtigs(k, lmtig_array, n, text_ptr, ctypes.byref(out), ctypes.byref(nb), ctypes.byref(nu),
+                                ctypes.byref(nc))
+    _check(lib, None, rc, "cfg_collate_lmtigs")
+    data = ctypes.string_at(out, nb.value) if nb.value else b""
+    lib.cfg_free(out)
+    return data, nu.value, nc.value
+
+
+def collate_lmtig_records(k, lms):
+    """cfg_collate_lmtigs over LmtigRec objects (labels as str)."""
+    arr = (Lmtig * max(1, len(lms)))()
+    text = bytearray()
+    for i, m in enumerate(lms):
+        arr[i].u[0], arr[i].u[1] = m.u
+        arr[i].v[0], arr[i].v[1] = m.v
+        arr[i].label_off = len(text)
+        arr[i].label_len = len(m.label)
+        arr[i].g = m.g
+        arr[i].flags = m.flags
+        text += m.label.encode()
+    buf = ctypes.create_string_buffer(bytes(text) + b"\0")
+    return collate(k, arr, len(lms), buf)
 
 
 def kmer_label(key, k):

@@ -155,6 +155,19 @@ int cfg_dump_records(cfg_ctx* ctx, cfg_record_dump* out);
  * including the host-side planning between phases. */
 int cfg_last_timings(cfg_ctx* ctx, float out_ms[4]);
 
+/* Joins lm-tigs into global maximal unitigs: the discontinuity-graph phases of
+ * dBG_Contractor::construct (contract, expand, collate; src/dBG_Contractor.cpp:73-101,
+ * src/Discontinuity_Graph_Contractor.cpp, src/Contracted_Graph_Expander.cpp,
+ * src/Unitig_Collator.cpp).  Takes the lm-tigs and label text of cfg_fetch
+ * (or any set in that layout) and returns FASTA text ">0\nSEQ\n", each unitig
+ * in the reference's canonical orientation (cycles rotated to their smallest
+ * k-mer over both strands).  Together with the trivial unitigs of cfg_fetch this
+ * is the reference's <output>.fa content.  *out is malloc'd; free it with cfg_free.
+ * Runs on the host. */
+int cfg_collate_lmtigs(uint32_t k, const cfg_lmtig* lmtigs, uint64_t n_lmtigs, const char* label_text,
+                       char** out, uint64_t* out_bytes, uint64_t* n_unitigs, uint64_t* n_cycles);
+void cfg_free(void* p);
+
 /* Profiling aid: SM clock cycles of the last run's subgraph kernels, summed over
  * CTAs, per phase: [0] table build, [1] side terminations, [2] path walks,
  * [3] cycle walks, [4] state dump and counters. */

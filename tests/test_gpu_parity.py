@@ -115,3 +115,26 @@ def test_small_table_retry():
     g = synth.random_seq(rng, 60_000)
     counts = compare([g], 31, 20, 1, 64, load_pct=10)
     assert counts.n_retries > 0
+
+
+@pytest.mark.parametrize("k,l,c,seed", [(31, 20, 1, 31), (31, 20, 2, 32), (63, 20, 1, 33), (15, 7, 1, 34)])
+def test_final_unitigs_equal_global_oracle(k, l, c, seed):
+    """GPU lm-tigs stitched on the host plus GPU trivial unitigs == the global maximal unitigs."""
+    rng = np.random.default_rng(seed)
+    if c == 2:
+        g = synth.genome_with_repeats(rng, 30_000, n_copies=5, n_pal=3)
+        recs = synth.reads(rng, g, 3_000)
+    else:
+        recs = [synth.genome_with_repeats(rng, 40_000, n_copies=6, n_pal=4)] + \
+               [synth.adversarial(rng, 10_000, k) for _ in range(2)]
+        s = synth.random_seq(rng, 700)
+        recs.append(s + s[:k])   # a circular molecule
+    packed = cfgpu.PackedInput(recs, k)
+    with cfgpu.Compactor(k, l, c, 16384, table_load_pct=30 if c == 2 else 0) as cx:
+        cx.submit(packed)
+        cx.run()
+        counts, fasta, lms = cx.fetch()
+    stitched, _, _ = cfgpu.collate_lmtig_records(k, lms)
+    got = orc.fasta_multiset(fasta) + orc.fasta_multiset(stitched)
+    want = orc.OracleRun(recs, k, l, c, 1).fasta_records()
+    assert got == want
