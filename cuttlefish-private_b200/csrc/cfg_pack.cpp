@@ -68,6 +68,13 @@ extern "C" int cfg_pack_records(const char* seq, const uint64_t* rec_off, uint64
     out->words = (uint64_t*)host_alloc(8 * (words + 1), pinned);
     out->frag_off = (uint64_t*)host_alloc(8 * (off.size() + 1), pinned);
     out->frag_len = (uint32_t*)host_alloc(4 * (len.size() + 1), pinned);
+    if (pinned && (!out->words || !out->frag_off || !out->frag_len)) {   // no page-locking here: plain memory
+        cfg_packed_free(out);
+        out->pinned = 0;
+        out->words = (uint64_t*)host_alloc(8 * (words + 1), 0);
+        out->frag_off = (uint64_t*)host_alloc(8 * (off.size() + 1), 0);
+        out->frag_len = (uint32_t*)host_alloc(4 * (len.size() + 1), 0);
+    }
     if (!out->words || !out->frag_off || !out->frag_len) { cfg_packed_free(out); return CFG_ERR_OOM; }
     std::memset(out->words, 0, 8 * (words + 1));
     uint64_t at = 0;

@@ -1,0 +1,246 @@
+// gpu_contractor.cpp -- input reading, the construct() phases and the CLI of the
+// B200 path: `cuttlefish build` with the reference's options (src/commands.cpp:30-198).
+#include "gpu_contractor.hpp"
+
+#include <zlib.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+
+namespace cuttlefish_b200 {
+
+namespace {
+
+double since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// One whole (possibly gzipped) file in memory.
+std::string slurp(const std::string& path) {
+    gzFile f = gzopen(path.c_str(), "rb");
+    if (!f) throw cfg_error("cannot open input " + path, CFG_ERR_BAD_INPUT);
+    gzbuffer(f, 1 << 20);
+    std::string out;
+    std::vector<char> buf(1 << 22);
+    for (;;) {
+        const int n = gzread(f, buf.data(), (unsigned)buf.size());
+        if (n < 0) { gzclose(f); throw cfg_error("cannot read input " + path, CFG_ERR_BAD_INPUT); }
+        if (n == 0) break;
+        out.append(buf.data(), (size_t)n);
+    }
+    gzclose(f);
+    return out;
+}
+
+// FASTA: a record's sequence is its lines joined (RabbitFX chunkListFormat,
+// include/RabbitFX/io/Formater.cpp:87-130); FASTQ: the second line of each record.
+void parse_into(const std::string& text, Records& r) {
+    size_t i = 0;
+    const size_t n = text.size();
+    while (i < n && (text[i] == '\n' || text[i] == '\r')) ++i;
+    if (i == n) return;
+    if (text[i] == '@') {
+        while (i < n) {
+            size_t e = text.find('\n', i);             // header
+            if (e == std::string::npos) break;
+            size_t s = e + 1, t = text.find('\n', s);   // sequence
+            if (t == std::string::npos) t = n;
+            r.seq.append(text, s, t - s);
+            r.off.push_back(r.seq.size());
+            size_t p = t + 1;                            // '+' line, then quality
+            for (int skip = 0; skip < 2 && p < n; ++skip) {
+                const size_t q = text.find('\n', p);
+                p = q == std::string::npos ? n : q + 1;
+            }
+            i = p;
+            while (i < n && (text[i] == '\n' || text[i] == '\r')) ++i;
+        }
+        return;
+    }
+    bool in_rec = false;
+    while (i < n) {
+        size_t e = text.find('\n', i);
+        if (e == std::string::npos) e = n;
+        if (text[i] == '>') {
+            if (in_rec) r.off.push_back(r.seq.size());
+            in_rec = true;
+        } else if (in_rec) {
+            r.seq.append(text, i, e - i);
+        }
+        i = e + 1;
+    }
+    if (in_rec) r.off.push_back(r.seq.size());
+}
+
+}  // namespace
+
+Records read_records(const std::vector<std::string>& paths) {
+    std::vector<std::pair<uint64_t, std::string>> by_size;
+    for (const auto& p : paths) {
+        std::error_code ec;
+        const auto sz = std::filesystem::file_size(p, ec);
+        if (ec) throw cfg_error("cannot open input " + p, CFG_ERR_BAD_INPUT);
+        by_size.emplace_back(sz, p);
+    }
+    std::stable_sort(by_size.begin(), by_size.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+    Records r;
+    for (const auto& e : by_size) parse_into(slurp(e.second), r);
+    return r;
+}
+
+uint64_t write_unitigs(const std::string& path, uint32_t k, const cfg_results& r) {
+    char* stitched = nullptr;
+    uint64_t bytes = 0, n_units = 0, n_cycles = 0;
+    const int rc = cfg_collate_lmtigs(k, r.lmtigs, r.counts.n_lmtig, r.lmtig_text, &stitched, &bytes, &n_units, &n_cycles);
+    if (rc != CFG_OK) throw cfg_error("cfg_collate_lmtigs failed", rc);
+    std::ofstream out(path, std::ios::binary);
+    if (!out) { cfg_free(stitched); throw cfg_error("cannot write " + path, CFG_ERR_BAD_INPUT); }
+    out.write(r.fasta, (std::streamsize)r.counts.fasta_bytes);
+    out.write(stitched, (std::streamsize)bytes);
+    cfg_free(stitched);
+    if (!out) throw cfg_error("error writing " + path, CFG_ERR_BAD_INPUT);
+    return r.counts.n_trivial + n_units;
+}
+
+void construct_gpu(const Build_Params& p) {
+    const auto t0 = std::chrono::steady_clock::now();
+    Records recs = read_records(p.seq_paths);
+    cfg_packed packed{};
+    int rc = cfg_pack_records(recs.seq.data(), recs.off.data(), recs.off.size() - 1, p.k, 1, &packed);
+    if (rc != CFG_OK) throw cfg_error("cfg_pack_records failed", rc);
+    std::cerr << "Read " << recs.off.size() - 1 << " records, " << packed.n_bases << " bases in fragments. Time taken: "
+              << since(t0) << " seconds.\n";
+    {
+        std::string().swap(recs.seq);
+    }
+    Subgraphs_Manager G(p.k, p.min_len, p.effective_cutoff(), p.device,
+                        p.table_load_pct ? p.table_load_pct : (p.is_read_graph ? 15u : 0u));
+    const auto t1 = std::chrono::steady_clock::now();
+    G.partition(packed);
+    G.finalize();
+    G.process();
+    float ms[4] = {0, 0, 0, 0};
+    cfg_last_timings(G.context(), ms);
+    std::cerr << "Sequence splitting into subgraphs completed. Time taken: " << (ms[0] + ms[1]) / 1e3 << " seconds.\n";
+    std::cerr << "Subgraphs construction and contraction completed. Time taken: " << ms[2] / 1e3 << " seconds.\n";
+    std::cerr << "Trivial maximal unitig count: " << G.trivial_mtig_count() << ".\n";
+    std::cerr << "Isolated cycle count: " << G.icc_count() << ".\n";
+    std::cerr << "lm-tig count: " << G.results().counts.n_lmtig << ".\n";
+    cfg_packed_free(&packed);
+    const auto t2 = std::chrono::steady_clock::now();
+    const uint64_t units = write_unitigs(p.output_file_path(), p.k, G.results());
+    std::cerr << "Collated " << units << " maximal unitigs into " << p.output_file_path() << ". Time taken: "
+              << since(t2) << " seconds.\n";
+    std::cerr << "Device phases and transfers: " << std::chrono::duration<double>(t2 - t1).count()
+              << " seconds; total: " << since(t0) << " seconds.\n";
+}
+
+}  // namespace cuttlefish_b200
+
+// ---------------------------------------------------------------------------
+// `cuttlefish build` (src/main.cpp:29-59, src/commands.cpp:30-198).
+namespace {
+
+using cuttlefish_b200::Build_Params;
+
+void usage() {
+    std::cout << "cuttlefish build: construct the compacted de Bruijn graph on a B200 GPU\n"
+                 "  -s, --seq FILE[,FILE..]   input files (FASTA / FASTQ, optionally gzipped)\n"
+                 "  -l, --list FILE           files listing inputs, one per line\n"
+                 "  -d, --dir DIR             directories of inputs\n"
+                 "  -k, --kmer-len K          k-mer length (odd, <= 63; default 27)\n"
+                 "  -c, --cutoff C            (k+1)-mer frequency cutoff (default: refs 1, reads 2)\n"
+                 "      --read | --ref        read or reference de Bruijn graph\n"
+                 "      --min-len L           minimizer length (default 20)\n"
+                 "  -o, --output PREFIX       output; unitigs go to PREFIX.fa\n"
+                 "  -w, --work-dir DIR        working directory (default .)\n"
+                 "  -t, --threads N           accepted (host parsing is single pass)\n"
+                 "      --gpu N               device ordinal (default 0)\n"
+                 "      --subgraph-count N, --vertex-part-count N, --lmtig-bucket-count N, --gmtig-bucket-count N,\n"
+                 "      -m, --max-memory GB, --unrestrict-memory, --idx   accepted and ignored, as in the reference\n";
+}
+
+std::vector<std::string> split_commas(const std::string& v) {
+    std::vector<std::string> out;
+    std::stringstream ss(v);
+    std::string item;
+    while (std::getline(ss, item, ',')) if (!item.empty()) out.push_back(item);
+    return out;
+}
+
+int cf_build(int argc, char** argv) {
+    Build_Params p;
+    bool read = false, ref = false;
+    std::vector<std::string> seqs, lists, dirs;
+    for (int i = 1; i < argc; ++i) {
+        const std::string a = argv[i];
+        auto val = [&](void) -> std::string {
+            if (i + 1 >= argc) throw std::runtime_error("missing value for " + a);
+            return argv[++i];
+        };
+        if (a == "-h" || a == "--help") { usage(); return 0; }
+        else if (a == "-s" || a == "--seq") for (auto& x : split_commas(val())) seqs.push_back(x);
+        else if (a == "-l" || a == "--list") for (auto& x : split_commas(val())) lists.push_back(x);
+        else if (a == "-d" || a == "--dir") for (auto& x : split_commas(val())) dirs.push_back(x);
+        else if (a == "-k" || a == "--kmer-len") p.k = (uint16_t)std::stoi(val());
+        else if (a == "-c" || a == "--cutoff") p.cutoff = (uint32_t)std::stoul(val());
+        else if (a == "--min-len") p.min_len = (uint16_t)std::stoi(val());
+        else if (a == "-o" || a == "--output") p.output_prefix = val();
+        else if (a == "-w" || a == "--work-dir") p.working_dir = val();
+        else if (a == "-t" || a == "--threads") p.thread_count = (uint16_t)std::stoi(val());
+        else if (a == "--gpu") p.device = std::stoi(val());
+        else if (a == "--table-load-pct") p.table_load_pct = (uint32_t)std::stoul(val());
+        else if (a == "--read") read = true;
+        else if (a == "--ref") ref = true;
+        else if (a == "--subgraph-count" || a == "--vertex-part-count" || a == "--lmtig-bucket-count" ||
+                 a == "--gmtig-bucket-count" || a == "-m" || a == "--max-memory") val();
+        else if (a == "--unrestrict-memory" || a == "--idx") {}
+        else if (a == "--color" || a == "--path-cover" || a == "-f" || a == "--format")
+            throw std::runtime_error(a + " is not supported by the GPU path");
+        else throw std::runtime_error("unknown option " + a);
+    }
+    for (const auto& l : lists) {
+        std::ifstream in(l);
+        if (!in) throw std::runtime_error("cannot open list " + l);
+        std::string line;
+        while (std::getline(in, line)) if (!line.empty()) seqs.push_back(line);
+    }
+    for (const auto& d : dirs)
+        for (const auto& e : std::filesystem::directory_iterator(d))
+            if (e.is_regular_file()) seqs.push_back(e.path().string());
+    // Build_Params::is_valid (src/Build_Params.cpp:97-218)
+    bool valid = true;
+    if (seqs.empty()) { std::cout << "No sequence input provided for compacted de Bruijn graph construction.\n"; valid = false; }
+    if ((p.k % 2) == 0 || p.k == 1 || p.k > 63) { std::cout << "The k-mer length (k) needs to be odd and within 63.\n"; valid = false; }
+    if (read && ref) { std::cout << "Both read and reference de Bruijn graph specified.\n"; valid = false; }
+    if (p.output_prefix.empty()) { std::cout << "An output path (-o) is required.\n"; valid = false; }
+    if (p.min_len == 0 || p.min_len > 32 || p.min_len + 1 > p.k) { std::cout << "The minimizer length must be within [1, min(k-1, 32)].\n"; valid = false; }
+    if (!valid) { std::cout << "Invalid input configuration. Aborting.\n"; return 1; }
+    p.is_read_graph = read;
+    p.is_ref_graph = !read;
+    if (p.is_ref_graph && p.effective_cutoff() != 1) std::cout << "WARNING: cutoff frequency specified not to be 1 on reference sequences.\n";
+    p.seq_paths = seqs;
+    cuttlefish_b200::construct_gpu(p);
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    if (argc < 2 || std::string(argv[1]) != "build") {
+        std::cout << "usage: cuttlefish build [options]   (cuttlefish build --help)\n";
+        return argc < 2 ? 1 : (std::string(argv[1]) == "-h" || std::string(argv[1]) == "--help" ? 0 : 1);
+    }
+    try {
+        return cf_build(argc - 1, argv + 1);
+    } catch (const std::exception& e) {
+        std::cerr << "Error: " << e.what() << "\n";
+        return 1;
+    }
+}

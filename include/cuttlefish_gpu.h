@@ -179,8 +179,9 @@ const char* cfg_last_error_string(cfg_ctx* ctx);
  * into fragments -- maximal runs of A/C/G/T (either case) holding at least k+1
  * bases, which is the fragment rule of Graph_Partitioner::process_chunk
  * (src/Graph_Partitioner.cpp:461-501) -- and packs them into the layout
- * cfg_submit_packed takes.  With `pinned` the buffers are page-locked (faster
- * copies to the device).  Free with cfg_packed_free. */
+ * cfg_submit_packed takes.  With `pinned` the buffers are page-locked when the
+ * driver allows it (faster copies to the device; cfg_packed.pinned tells), plain
+ * memory otherwise.  Free with cfg_packed_free. */
 typedef struct cfg_packed {
     uint64_t n_bases;
     uint64_t n_frags;
