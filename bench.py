@@ -43,8 +43,10 @@ WORKLOADS = {
 
 def synth():
     lib = ctypes.CDLL(SYNTH_LIB)
-    for n in ("cfs_ref5m_len", "cfs_reads30x_genome_len", "cfs_ref500m_len"):
+    for n in ("cfs_ref5m_len", "cfs_reads30x_genome_len", "cfs_ref500m_len", "cfs_genome_len"):
         getattr(lib, n).restype = ctypes.c_uint64
+    lib.cfs_genome_len.argtypes = [ctypes.c_uint32]
+    lib.cfs_genome.argtypes = [ctypes.c_uint32, ctypes.c_char_p]
     lib.cfs_reads.argtypes = [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_double,
                               ctypes.c_uint64, ctypes.c_char_p]
     return lib
@@ -73,6 +75,132 @@ def make_workload(name, n_reads=10_000_000):
         lib.cfs_ref500m(g, cuts)
         return g, cuts, 20
     raise ValueError(name)
+
+
+def make_genomes(n_genomes):
+    """The batched workload: genome i has log-uniform length in [0.5, 8] Mbp, GC in
+    [0.3, 0.7] and 1% of it as copies of 500-5000 bp at 1% divergence (seed 1000+i)."""
+    lib = synth()
+    out = []
+    for i in range(n_genomes):
+        n = lib.cfs_genome_len(i)
+        g = ctypes.create_string_buffer(n)
+        lib.cfs_genome(i, g)
+        out.append((g, (ctypes.c_uint64 * 2)(0, n), 1))
+    return out
+
+
+def bench_batch(args, pg, local, world, peak, with_cpu):
+    """Batched form vs one plain launch per genome, on the same GPU and genomes.
+
+    One step = all genomes.  Plain: cfg_run per genome, input resident (device
+    time of each run summed) and end to end (submit from pinned memory + run +
+    fetch of every output).  Batched: one graph launch for all genomes (device
+    time), and end to end (submit + run + cfg_batch_job for every genome)."""
+    import cfgpu
+    k, l, cutoff = 31, 20, 1
+    t0 = time.perf_counter()
+    genomes = make_genomes(args.batch_genomes)
+    gen_s = time.perf_counter() - t0
+    packed = [cfgpu.PackedInput(None, k, pinned=True, data_offsets=g) for g in genomes]
+    bases = sum(p.n_bases for p in packed)
+    steps, warm = args.batch_steps, max(3, args.warmup)
+
+    b = cfgpu.Batch(k, l, cutoff, 16384, device=local if world > 1 else 0)
+    b.submit(packed)
+    tuning = b.tune()
+    for _ in range(warm):
+        b.run()
+    barrier(pg)
+    dev_ms = []
+    for _ in range(steps):
+        b.run()
+        dev_ms.append(b.info().device_ms)
+    info = b.info()
+    # plain launches on the same resident inputs
+    cx = cfgpu.Compactor(k, l, cutoff, 16384, device=local if world > 1 else 0)
+    dev_inputs = [b.device_input(j) for j in range(len(packed))]
+    plain_ms = []
+    plain_launches = 0
+    for it in range(1 + steps):
+        tot = 0.0
+        for d in dev_inputs:
+            cx.submit_device(*d)
+            cx.run()
+            tot += cx.timings()[3]
+            if it == 1:
+                plain_launches += cx.counts().n_launches
+        if it > 0:
+            plain_ms.append(tot)
+    barrier(pg)
+    # end to end, host buffers
+    def batch_e2e():
+        b.submit(packed)
+        b.run()
+        d2h = 0
+        for j in range(len(packed)):
+            r = b.job_raw(j)
+            d2h += r.counts.fasta_bytes + r.counts.lmtig_bytes + 48 * r.counts.n_lmtig
+        return d2h
+
+    def plain_e2e():
+        d2h = 0
+        for p in packed:
+            cx.submit(p)
+            cx.run()
+            r = cx.fetch_raw()
+            d2h += r.counts.fasta_bytes + r.counts.lmtig_bytes + 48 * r.counts.n_lmtig
+        return d2h
+
+    batch_e2e()
+    plain_e2e()
+    barrier(pg)
+    be, pe = [], []
+    for _ in range(steps):
+        t = time.perf_counter(); d2h = batch_e2e(); be.append(time.perf_counter() - t)
+        t = time.perf_counter(); plain_e2e(); pe.append(time.perf_counter() - t)
+    barrier(pg)
+    b_dev = allreduce_max(pg, local, sum(dev_ms))
+    p_dev = allreduce_max(pg, local, sum(plain_ms))
+    b_e2e = allreduce_max(pg, local, sum(be))
+    p_e2e = allreduce_max(pg, local, sum(pe))
+    cpu = None
+    if with_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import orc
+        threads = os.cpu_count() or 1
+        n_s, at, dt = 0, 0, 0.0
+        while n_s < len(genomes) and dt < 8.0:
+            g, o, n = genomes[n_s]
+            dt += orc.timed_run(g.raw, o, n, k, l, cutoff, 16384, threads)
+            at += o[1]
+            n_s += 1
+        cpu = {"value": at / dt, "unit": "bases/s", "cores": threads, "kind": "port",
+               "sample": f"first {n_s} genomes ({at} bases), each its own job", "seconds": round(dt, 2)}
+    out = {
+        "workload": f"batch{len(packed)}",
+        "description": f"{len(packed)} genomes, log-uniform 0.5-8 Mbp, GC 0.3-0.7, 1% repeats at 1%; k=31, cutoff 1, "
+                       "each genome its own job with its own outputs",
+        "n_genomes": len(packed), "bases": bases,
+        "batched": {"value": world * bases * steps / (b_dev / 1e3), "unit": "bases/s", "ms_per_step": b_dev / steps,
+                    "e2e": {"value": world * bases * steps / b_e2e, "ms_per_step": 1e3 * b_e2e / steps,
+                            "h2d_bytes_per_step": bases // 4, "d2h_bytes_per_step": d2h},
+                    "graph_launches_per_step": 1, "gpu_launches_per_step": int(info.kernels_per_run),
+                    "jobs_redone_alone": int(info.n_redone),
+                    "tuning": {"local_div": tuning.local_div, "cluster_threads": tuning.cluster_threads,
+                               "table_load_pct": tuning.table_load_pct, "tuned_ms": tuning.ms}},
+        "plain": {"value": world * bases * steps / (p_dev / 1e3), "unit": "bases/s", "ms_per_step": p_dev / steps,
+                  "e2e": {"value": world * bases * steps / p_e2e, "ms_per_step": 1e3 * p_e2e / steps},
+                  "gpu_launches_per_step": plain_launches},
+        "speedup_device": p_dev / b_dev, "speedup_e2e": p_e2e / b_e2e,
+        "generation_s": round(gen_s, 1),
+        "cpu_baseline": cpu,
+    }
+    cx.close()
+    b.close()
+    for p in packed:
+        p.close()
+    return out
 
 
 class ClockSampler:
@@ -204,6 +332,8 @@ def main():
     ap.add_argument("--cpu-sample-bases", type=int, default=60_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--table-load-pct", type=int, default=0, help="override the workload's table sizing factor")
+    ap.add_argument("--batch-genomes", type=int, default=1000, help="genomes of the batched comparison (0: skip it)")
+    ap.add_argument("--batch-steps", type=int, default=2)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -276,6 +406,7 @@ def main():
             launches += cx.counts().n_launches
     barrier(pg)
     counts = cx.counts()
+    phase_cycles = cx.phase_cycles()
     total_ms = sum(run_ms)
     total_ms_max = allreduce_max(pg, local, total_ms)
     e2e_s_max = allreduce_max(pg, local, sum(e2e_times))
@@ -306,6 +437,13 @@ def main():
         threads = os.cpu_count() or 1
         v, dt, label = cpu_reference(args, name, data, offs, n_rec, threads)
         cpu = {"value": v, "unit": "bases/s", "cores": threads, "kind": "port", "sample": label, "seconds": round(dt, 2)}
+    cx.close()
+    packed.close()
+    del data
+
+    batched = None
+    if args.batch_genomes > 0:
+        batched = bench_batch(args, pg, local, world, peak, rank == 0 and not args.no_cpu_baseline)
 
     if rank == 0:
         line = {
@@ -325,14 +463,13 @@ def main():
             "phases_ms": {"partition": statistics.mean(part_ms), "scatter": statistics.mean(scat_ms),
                           "subgraphs": statistics.mean(sub_ms), "run": statistics.mean(run_ms)},
             "counts": {n: getattr(counts, n) for n, _ in cfgpu.Counts._fields_},
-            "subgraph_phase_cycles": dict(zip(["build", "terminations", "paths", "cycles", "tail"], cx.phase_cycles())),
+            "subgraph_phase_cycles": dict(zip(["build", "terminations", "paths", "cycles", "tail"], phase_cycles)),
             "distinct_kmers_per_s": None,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "batched_vs_plain": batched,
         }
         print(json.dumps(line))
-    cx.close()
-    packed.close()
     if pg is not None:
         pg.destroy_process_group()
 

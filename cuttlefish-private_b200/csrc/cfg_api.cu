@@ -2,6 +2,7 @@
 // the launch sequence partition -> bucket scatter -> subgraph construct+walk.
 #include "cuttlefish_gpu.h"
 #include "cfg_device.cuh"
+#include "cfg_host.h"
 #include "cfg_internal.h"
 
 #include <algorithm>
@@ -21,37 +22,6 @@ uint64_t wy_seed0() {
 }
 
 }  // namespace
-
-struct DevBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-    bool ensure(size_t need) {
-        if (need <= bytes) return true;
-        if (p) cudaFree(p);
-        p = nullptr; bytes = 0;
-        size_t want = need + need / 4 + 4096;
-        if (cudaMalloc(&p, want) != cudaSuccess) { cudaGetLastError(); return false; }
-        bytes = want;
-        return true;
-    }
-    void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
-    template <typename T> T* as() const { return (T*)p; }
-};
-
-struct HostBuf {   // page-locked host memory for device->host result copies
-    void* p = nullptr;
-    size_t bytes = 0;
-    bool ensure(size_t need) {
-        if (need <= bytes) return true;
-        if (p) cudaFreeHost(p);
-        p = nullptr; bytes = 0;
-        const size_t want = need + need / 4 + 4096;
-        if (cudaMallocHost(&p, want) != cudaSuccess) { cudaGetLastError(); return false; }
-        bytes = want;
-        return true;
-    }
-    void release() { if (p) cudaFreeHost(p); p = nullptr; bytes = 0; }
-};
 
 struct cfg_ctx {
     int device = 0;
@@ -207,7 +177,7 @@ int launch_plan(cfg_ctx* c, const std::vector<Launch>& plan, uint64_t arena_slot
         a.packed = c->d_packed; a.recs = c->recs.as<uint64_t>(); a.bucket_off = c->bucket_off.as<uint32_t>();
         a.list = d_list; a.n_list = (uint32_t)L.list.size();
         a.tab_off = d_off; a.tab_cap = d_cap; a.smem_cap = L.per; a.arena = c->arena.as<unsigned char>();
-        a.k = c->p.k; a.fth = c->p.cutoff; a.load_limit_pct = 90;
+        a.k = c->p.k; a.fth = c->p.cutoff; a.load_limit_pct = 90; a.record_clocks = 1;
         a.fasta = c->fasta.as<char>(); a.fasta_cap = c->fasta_cap;
         a.lm_text = c->lm_text.as<char>(); a.lm_text_cap = c->lm_text_cap;
         a.lm = c->lm.as<LmtigOut>(); a.lm_cap = c->lm_cap;

@@ -1,0 +1,692 @@
+// cfg_batch.cu -- many independent jobs (genomes, read sets) compacted in one launch.
+//
+// The plain driver (cfg_api.cu) plans each job on the host between its phases:
+// it reads the subgraph histogram back, groups subgraphs by table shape and
+// launches one kernel per shape.  For small jobs those synchronisations and the
+// launch tails cost more than the work.  Here the whole pipeline of a batch is
+// planned on the device and recorded once as a CUDA graph:
+//
+//   partition (every job's fragments; job j's subgraph g is bucket j*G + g)
+//   -> multi-block scan of the J*G buckets -> scatter
+//   -> classify every bucket into a table class by its instance count
+//      (one CTA with 64..4096 slots, a cluster of 2..8 CTAs, or a global-memory
+//      table carved from an arena with a device-side bump allocator)
+//   -> give every job output regions sized from its record and instance counts
+//   -> one persistent launch per class, striding through that class's list.
+//
+// Replaying the graph costs one launch.  Each job's outputs land in its own
+// regions, in the layout of a plain run of that job alone: the same FASTA text,
+// lm-tigs and counters (as multisets; emission order is unspecified in both).
+// A job whose outputs or tables do not fit the preallocated arenas, or whose
+// table overflowed its class, is redone on its own through the plain driver.
+#include "cuttlefish_gpu.h"
+#include "cfg_device.cuh"
+#include "cfg_host.h"
+#include "cfg_internal.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace cfg;
+
+namespace {
+
+constexpr uint32_t NCLS = 16;   // LOCAL classes (<= 7), 7 cluster sizes, 1 global
+
+struct BatchWords {   // device-side scalars of one run, cleared by one memset
+    uint32_t count[NCLS], off[NCLS], fill[NCLS];
+    unsigned long long arena_cur, fasta_cur, lm_text_cur, lm_cur;
+    unsigned long long rec_cursor;
+    uint32_t err, pad;
+};
+
+struct ClassCfg {
+    uint32_t load;        // table_load_pct
+    uint32_t nl;          // LOCAL classes: class c < nl holds tables of 64 << c slots
+    uint32_t per_cl;      // slots per CTA of a cluster
+    uint32_t g_shift;     // log2 of subgraphs per job
+    uint32_t n_buckets;
+    uint64_t arena_slots;
+};
+
+__host__ __device__ inline uint64_t want_slots(uint32_t inst, uint32_t load) {
+    const uint64_t w = ((uint64_t)inst * load * 2 + 99) / 100;
+    return w < 64 ? 64 : w;
+}
+__host__ __device__ inline uint32_t ceil_pow2(uint64_t v) {   // v >= 2
+    uint32_t p = 64;
+    while (p < v) p <<= 1;
+    return p;
+}
+__host__ __device__ inline uint32_t class_of(uint32_t inst, const ClassCfg& c, uint64_t& want) {
+    want = want_slots(inst, c.load);
+    const uint64_t per_max = 64ull << (c.nl - 1);
+    if (want <= per_max) {
+        const uint32_t per = ceil_pow2(want);
+        uint32_t lg = 0;
+        while ((64u << lg) < per) ++lg;
+        return lg;
+    }
+    if (want <= (uint64_t)c.per_cl * 8) return c.nl + (uint32_t)((want + c.per_cl - 1) / c.per_cl) - 2;
+    return c.nl + 7;
+}
+
+// pass 0 counts buckets per class; pass 1 writes each bucket into its class's list
+// (and, for global tables, carves its table out of the arena).
+__global__ void __launch_bounds__(256) k_classify(const uint32_t* __restrict__ inst, ClassCfg cc, BatchWords* bw,
+                                                  uint32_t* list, uint64_t* tab_off, uint32_t* tab_cap, JobOut* jobs,
+                                                  int pass) {
+    __shared__ uint32_t cnt[NCLS], base[NCLS];
+    if (bw->err & DERR_REC_OVERFLOW) return;   // the run is redone with a larger record buffer
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t b0 = blockIdx.x * blockDim.x; b0 < cc.n_buckets; b0 += stride) {
+        if (threadIdx.x < NCLS) cnt[threadIdx.x] = 0;
+        __syncthreads();
+        const uint32_t b = b0 + threadIdx.x;
+        uint32_t c = NCLS, local = 0;
+        uint64_t want = 0;
+        if (b < cc.n_buckets) {
+            const uint32_t n = inst[b];
+            if (n) { c = class_of(n, cc, want); local = atomicAdd(&cnt[c], 1u); }
+        }
+        __syncthreads();
+        if (threadIdx.x < NCLS && cnt[threadIdx.x])
+            base[threadIdx.x] = atomicAdd(pass == 0 ? &bw->count[threadIdx.x] : &bw->fill[threadIdx.x], cnt[threadIdx.x]);
+        __syncthreads();
+        if (pass == 1 && c < NCLS) {
+            const uint32_t at = bw->off[c] + base[c] + local;
+            list[at] = b;
+            if (c == cc.nl + 7) {
+                const uint32_t cap = ceil_pow2(want);
+                const unsigned long long o = atomicAdd(&bw->arena_cur, (unsigned long long)cap);
+                if (o + cap <= cc.arena_slots) { tab_off[at] = o; tab_cap[at] = cap; }
+                else { tab_off[at] = 0; tab_cap[at] = 0; atomicOr(&jobs[b >> cc.g_shift].err, DERR_NO_ROOM); }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_class_offsets(BatchWords* bw) {
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (uint32_t c = 0; c < NCLS; ++c) { bw->off[c] = run; run += bw->count[c]; }
+    }
+}
+
+struct ArenaCaps { uint64_t fasta, lm_text, lm; uint32_t k, fasta_full; };
+
+// One CTA per job: its record and instance totals, and its output regions.
+__global__ void __launch_bounds__(256) k_job_regions(const uint32_t* __restrict__ bucket_off, const uint32_t* __restrict__ inst,
+                                                     const uint64_t* __restrict__ job_nbases, uint32_t g_shift,
+                                                     JobOut* jobs, BatchWords* bw, ArenaCaps caps) {
+    __shared__ unsigned long long part[8];
+    const uint32_t j = blockIdx.x, G = 1u << g_shift, b0 = j << g_shift;
+    unsigned long long s = 0;
+    for (uint32_t i = threadIdx.x; i < G; i += blockDim.x) s += inst[b0 + i];
+    for (int d = 16; d; d >>= 1) s += __shfl_down_sync(0xffffffffu, s, d);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    unsigned long long I = 0;
+    for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) I += part[w];
+    JobOut& J = jobs[j];
+    const uint64_t R = bucket_off[b0 + G] - bucket_off[b0];
+    const uint64_t N = job_nbases[j];
+    J.records = R; J.instances = I;
+    // trivial unitigs are rare when the job has many subgraphs, and make up all of
+    // its output when it has few
+    const uint64_t fc = (caps.fasta_full ? N + 8 * R : N / 8) + 4096;
+    const uint64_t tc = N / 2 + R * (caps.k + 2) + 4096, lc = R + 64;
+    const unsigned long long fo = atomicAdd(&bw->fasta_cur, (unsigned long long)fc);
+    const unsigned long long to = atomicAdd(&bw->lm_text_cur, (unsigned long long)tc);
+    const unsigned long long lo = atomicAdd(&bw->lm_cur, (unsigned long long)lc);
+    if (fo + fc <= caps.fasta && to + tc <= caps.lm_text && lo + lc <= caps.lm) {
+        J.fasta_off = fo; J.fasta_cap = fc; J.lm_text_off = to; J.lm_text_cap = tc; J.lm_off = lo; J.lm_cap = lc;
+    } else {
+        J.fasta_off = J.lm_text_off = J.lm_off = 0; J.fasta_cap = J.lm_text_cap = J.lm_cap = 0;
+        J.err |= DERR_NO_ROOM;
+    }
+}
+
+uint64_t wy_seed0() {
+    const __uint128_t r = (__uint128_t)WY_S0 * WY_S1;
+    return (uint64_t)r ^ (uint64_t)(r >> 64);
+}
+
+struct Shape { uint32_t cls, cluster, threads, per, grid; };
+
+}  // namespace
+
+struct cfg_batch {
+    int device = 0;
+    cfg_params p{};
+    uint32_t G = 16384, g_shift = 14;
+    int words = 1;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[2] = {};
+    std::string err;
+    cfg_batch_tuning tune{4, 512, 100, 0, 0.f};
+
+    // input: job j's bases start at word word_off[j] of the packed stream
+    DevBuf packed, frag_off, frag_off_rel, frag_len, frag_gbase, job_pos, job_nbases;
+    uint64_t n_bases = 0, n_frags = 0;
+    uint32_t n_jobs = 0;
+    std::vector<uint64_t> word_off, job_frag, nb;   // per job (+1 for job_frag)
+    bool have_input = false;
+
+    // pipeline
+    DevBuf flat, hist, bw, bucket_off, inst, fill, partials, recs, list, tab_off, tab_cap, arena, jobs,
+        fasta, lm_text, lm, retry, counters;
+    uint64_t rec_cap = 0, arena_slots = 0, fasta_cap = 0, lm_text_cap = 0, lm_cap = 0;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<Shape> shapes;
+    uint64_t launches_per_run = 0;
+
+    // results
+    std::vector<JobOut> h_jobs;
+    std::vector<uint8_t> redo;          // job redone through the plain driver
+    bool have_run = false;
+    float ms = 0, redo_ms = 0;
+    cfg_ctx* plain = nullptr;           // for jobs redone alone
+    // host views of redone jobs' results (copied out of the plain context)
+    std::vector<std::string> r_fasta, r_text;
+    std::vector<std::vector<cfg_lmtig>> r_lm;
+    std::vector<cfg_counts> r_counts;
+    HostBuf h_fasta, h_text, h_lm;      // one job's results (cfg_batch_job)
+};
+
+namespace {
+
+int bfail(cfg_batch* b, int code, const std::string& msg) {
+    if (b) b->err = msg;
+    return code;
+}
+
+#define BCK(call)                                                                        \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) return bfail(b, CFG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+void drop_graph(cfg_batch* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+}
+
+ClassCfg class_cfg(const cfg_batch* b) {
+    ClassCfg c{};
+    c.load = b->tune.table_load_pct ? b->tune.table_load_pct : 100;
+    const uint32_t per_max = subgraph_max_per_cta(b->words);
+    c.nl = 0;
+    while ((64u << c.nl) <= per_max) ++c.nl;
+    c.per_cl = subgraph_cluster_per_cta(b->words);
+    c.g_shift = b->g_shift;
+    c.n_buckets = b->n_jobs << b->g_shift;
+    c.arena_slots = b->arena_slots;
+    return c;
+}
+
+// Launch shapes of the classes, with persistent grids sized by occupancy.
+int plan_shapes(cfg_batch* b) {
+    b->shapes.clear();
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+    const ClassCfg cc = class_cfg(b);
+    for (uint32_t c = 0; c < cc.nl; ++c) {
+        const uint32_t per = 64u << c;
+        uint32_t t = per / std::max<uint32_t>(1, b->tune.local_div);
+        t = std::min<uint32_t>(512, std::max<uint32_t>(64, t));
+        t = (t + 31) / 32 * 32;
+        const int occ = subgraph_occupancy(b->words, 1, t, per);
+        if (occ <= 0) return bfail(b, CFG_ERR_CUDA, "no resident CTA for a table class");
+        b->shapes.push_back(Shape{c, 1, t, per, (uint32_t)(occ * sms)});
+    }
+    for (uint32_t cl = 2; cl <= 8; ++cl) {
+        const uint32_t t = b->tune.cluster_threads ? b->tune.cluster_threads : 512;
+        const int occ = subgraph_occupancy(b->words, cl, t, cc.per_cl);
+        if (occ <= 0) return bfail(b, CFG_ERR_CUDA, "no resident cluster for a table class");
+        b->shapes.push_back(Shape{cc.nl + cl - 2, cl, t, cc.per_cl, (uint32_t)occ * cl});
+    }
+    b->shapes.push_back(Shape{cc.nl + 7, 0, 512, 0, (uint32_t)(2 * sms)});
+    return CFG_OK;
+}
+
+// Buffers for the submitted batch (all sized before capture; a graph holds their addresses).
+int ensure_buffers(cfg_batch* b) {
+    const uint64_t NB = (uint64_t)b->n_jobs << b->g_shift;
+    const uint32_t w = b->p.k - b->p.l;
+    const uint64_t N = b->n_bases;
+    // weak super k-mers: about 2/(w+1) per base on random sequence
+    const uint64_t r_est = N * 2 / (w + 1) + 1024 * (uint64_t)b->n_jobs;
+    if (b->rec_cap < r_est + r_est / 2 + 65536) b->rec_cap = r_est + r_est / 2 + 65536;
+    b->arena_slots = std::max<uint64_t>(1u << 20, N / 64);
+    const bool fasta_full = b->G < 1024;
+    uint64_t act_bases = 0;
+    for (uint64_t x : b->nb) act_bases += x;
+    const uint64_t r_out = act_bases * 2 / (w + 1) * 23 / 20 + 1024 * (uint64_t)b->n_jobs;
+    b->fasta_cap = (fasta_full ? act_bases + 8 * r_out : act_bases / 8) + 4096ull * b->n_jobs + (1u << 20);
+    b->lm_text_cap = act_bases / 2 + r_out * (b->p.k + 2) + 4096ull * b->n_jobs;
+    b->lm_cap = r_out + 64ull * b->n_jobs;
+    const uint32_t np = (uint32_t)((NB + 8191) / 8192);
+    if (!b->flat.ensure(8 * b->rec_cap, false) || !b->recs.ensure(8 * b->rec_cap, false) || !b->hist.ensure(8 * NB) ||
+        !b->bw.ensure(sizeof(BatchWords)) || !b->bucket_off.ensure(4 * (NB + 1)) || !b->inst.ensure(4 * NB) ||
+        !b->fill.ensure(4 * NB) || !b->partials.ensure(4ull * np + 4) || !b->list.ensure(4 * NB) ||
+        !b->tab_off.ensure(8 * NB) || !b->tab_cap.ensure(4 * NB) ||
+        !b->arena.ensure(b->arena_slots * slot_bytes(b->words)) || !b->jobs.ensure(sizeof(JobOut) * b->n_jobs) ||
+        !b->fasta.ensure(b->fasta_cap, false) || !b->lm_text.ensure(b->lm_text_cap, false) ||
+        !b->lm.ensure(sizeof(LmtigOut) * b->lm_cap, false) ||
+        !b->retry.ensure(4 * NB) || !b->counters.ensure(sizeof(Counters)))
+        return bfail(b, CFG_ERR_OOM, "batch buffers");
+    return CFG_OK;
+}
+
+// The device work of one run, in stream order (captured into the graph).
+int enqueue(cfg_batch* b) {
+    cudaStream_t s = b->stream;
+    const uint64_t NB = (uint64_t)b->n_jobs << b->g_shift;
+    BatchWords* bw = b->bw.as<BatchWords>();
+    BCK(cudaMemsetAsync(b->hist.p, 0, 8 * NB, s));
+    BCK(cudaMemsetAsync(b->bw.p, 0, sizeof(BatchWords), s));
+    BCK(cudaMemsetAsync(b->jobs.p, 0, sizeof(JobOut) * b->n_jobs, s));
+    BCK(cudaMemsetAsync(b->counters.p, 0, sizeof(Counters), s));
+    uint64_t launches = 0;
+
+    PartitionArgs pa{};
+    pa.packed = b->packed.as<uint64_t>(); pa.frag_off = b->frag_off.as<uint64_t>(); pa.frag_len = b->frag_len.as<uint32_t>();
+    pa.n_frags = b->n_frags; pa.n_bases = b->n_bases;
+    pa.k = b->p.k; pa.l = b->p.l; pa.w = b->p.k - b->p.l;
+    pa.gmask = b->G - 1; pa.seed0 = wy_seed0(); pa.seg = 2048;
+    pa.recs = b->flat.as<uint64_t>(); pa.rec_cap = b->rec_cap;
+    pa.rec_cursor = &bw->rec_cursor; pa.hist = b->hist.as<unsigned long long>(); pa.err = &bw->err;
+    pa.frag_gbase = b->frag_gbase.as<uint32_t>();
+    if (b->n_bases) { launch_partition(pa, s); ++launches; }
+    BCK(cudaGetLastError());
+
+    launch_bucket_scan_large(b->hist.as<unsigned long long>(), (uint32_t)NB, b->bucket_off.as<uint32_t>(),
+                             b->inst.as<uint32_t>(), b->fill.as<uint32_t>(), b->partials.as<uint32_t>(), s);
+    launches += 3;
+    BCK(cudaGetLastError());
+
+    // the record count is on the device: scatter with a grid that covers the buffer's capacity
+    ScatterArgs sa{};
+    sa.flat = b->flat.as<uint64_t>(); sa.n = b->rec_cap;
+    sa.bucket_off = b->bucket_off.as<uint32_t>(); sa.bucket_fill = b->fill.as<uint32_t>();
+    sa.recs = b->recs.as<uint64_t>();
+    sa.job_pos = b->job_pos.as<uint64_t>(); sa.n_jobs = b->n_jobs; sa.g_shift = b->g_shift;
+    // bound the scatter by the number of records the scan counted (bucket_off[NB])
+    sa.n_dev = b->bucket_off.as<uint32_t>() + NB;
+    launch_scatter(sa, s);
+    ++launches;
+    BCK(cudaGetLastError());
+
+    const ClassCfg cc = class_cfg(b);
+    const uint32_t cgrid = (uint32_t)std::min<uint64_t>((NB + 255) / 256, 148ull * 8);
+    k_classify<<<cgrid, 256, 0, s>>>(b->inst.as<uint32_t>(), cc, bw, b->list.as<uint32_t>(), b->tab_off.as<uint64_t>(),
+                                     b->tab_cap.as<uint32_t>(), b->jobs.as<JobOut>(), 0);
+    k_class_offsets<<<1, 32, 0, s>>>(bw);
+    k_classify<<<cgrid, 256, 0, s>>>(b->inst.as<uint32_t>(), cc, bw, b->list.as<uint32_t>(), b->tab_off.as<uint64_t>(),
+                                     b->tab_cap.as<uint32_t>(), b->jobs.as<JobOut>(), 1);
+    ArenaCaps caps{b->fasta_cap, b->lm_text_cap, b->lm_cap, b->p.k, b->G < 1024 ? 1u : 0u};
+    k_job_regions<<<b->n_jobs, 256, 0, s>>>(b->bucket_off.as<uint32_t>(), b->inst.as<uint32_t>(), b->job_nbases.as<uint64_t>(),
+                                            b->g_shift, b->jobs.as<JobOut>(), bw, caps);
+    launches += 4;
+    BCK(cudaGetLastError());
+
+    SubgraphArgs a{};
+    a.packed = b->packed.as<uint64_t>(); a.recs = b->recs.as<uint64_t>(); a.bucket_off = b->bucket_off.as<uint32_t>();
+    a.list = b->list.as<uint32_t>(); a.tab_off = b->tab_off.as<uint64_t>(); a.tab_cap = b->tab_cap.as<uint32_t>();
+    a.arena = b->arena.as<unsigned char>();
+    a.k = b->p.k; a.fth = b->p.cutoff; a.load_limit_pct = 90;
+    a.fasta = b->fasta.as<char>(); a.lm_text = b->lm_text.as<char>(); a.lm = b->lm.as<LmtigOut>();
+    a.retry = b->retry.as<uint32_t>(); a.cnt = b->counters.as<Counters>(); a.err = &bw->err;
+    a.jobs = b->jobs.as<JobOut>(); a.g_shift = b->g_shift; a.record_clocks = 0;
+    for (const Shape& sh : b->shapes) {
+        a.list_base = &bw->off[sh.cls];
+        a.list_n = &bw->count[sh.cls];
+        BCK(launch_subgraphs_persistent(a, b->words, sh.cluster, sh.threads, sh.per, sh.grid, s));
+        ++launches;
+    }
+    b->launches_per_run = launches;
+    return CFG_OK;
+}
+
+int capture(cfg_batch* b) {
+    drop_graph(b);
+    int rc = plan_shapes(b);
+    if (rc) return rc;
+    cudaGraph_t g = nullptr;
+    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    rc = enqueue(b);
+    const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (rc) { if (g) cudaGraphDestroy(g); cudaGetLastError(); return rc; }
+    if (e != cudaSuccess) return bfail(b, CFG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    const cudaError_t ei = cudaGraphInstantiate(&b->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) { b->exec = nullptr; return bfail(b, CFG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei)); }
+    return CFG_OK;
+}
+
+// Jobs the batch could not finish alone run through the plain driver, from the
+// batch's device copy of their input.
+int redo_jobs(cfg_batch* b) {
+    b->r_fasta.assign(b->n_jobs, std::string());
+    b->r_text.assign(b->n_jobs, std::string());
+    b->r_lm.assign(b->n_jobs, std::vector<cfg_lmtig>());
+    b->r_counts.assign(b->n_jobs, cfg_counts{});
+    for (uint32_t j = 0; j < b->n_jobs; ++j) {
+        if (!b->redo[j]) continue;
+        if (!b->plain) {
+            cfg_params p = b->p;
+            p.flags = 0;
+            int rc = cfg_create(b->device, &p, &b->plain);
+            if (rc) return bfail(b, rc, "plain context for redone jobs");
+        }
+        const uint64_t f0 = b->job_frag[j], nf = b->job_frag[j + 1] - f0;
+        int rc = cfg_submit_packed_device(b->plain, b->packed.as<uint64_t>() + b->word_off[j], b->nb[j],
+                                          b->frag_off_rel.as<uint64_t>() + f0, b->frag_len.as<uint32_t>() + f0, nf);
+        if (!rc) rc = cfg_run(b->plain);
+        cfg_results r{};
+        if (!rc) rc = cfg_fetch(b->plain, &r);
+        if (rc) return bfail(b, rc, std::string("redone job: ") + cfg_last_error_string(b->plain));
+        b->r_fasta[j].assign(r.fasta, r.counts.fasta_bytes);
+        b->r_text[j].assign(r.lmtig_text, r.counts.lmtig_bytes);
+        b->r_lm[j].assign(r.lmtigs, r.lmtigs + r.counts.n_lmtig);
+        b->r_counts[j] = r.counts;
+    }
+    return CFG_OK;
+}
+
+int run_once(cfg_batch* b, bool& regrow) {
+    regrow = false;
+    if (!b->exec) { int rc = capture(b); if (rc) return rc; }
+    BCK(cudaEventRecord(b->ev[0], b->stream));
+    BCK(cudaGraphLaunch(b->exec, b->stream));
+    BCK(cudaEventRecord(b->ev[1], b->stream));
+    BatchWords w{};
+    Counters cnt{};
+    BCK(cudaMemcpyAsync(&w, b->bw.p, sizeof(w), cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaMemcpyAsync(&cnt, b->counters.p, sizeof(cnt), cudaMemcpyDeviceToHost, b->stream));
+    b->h_jobs.resize(b->n_jobs);
+    if (b->n_jobs) BCK(cudaMemcpyAsync(b->h_jobs.data(), b->jobs.p, sizeof(JobOut) * b->n_jobs, cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    cudaEventElapsedTime(&b->ms, b->ev[0], b->ev[1]);
+    if (w.err & DERR_MISSING_KEY) return bfail(b, CFG_ERR_WALK_LIMIT, "neighbour k-mer missing from its subgraph table");
+    if (w.err & DERR_WALK_LIMIT) return bfail(b, CFG_ERR_WALK_LIMIT, "unitig walk exceeded its step bound");
+    if (w.err & DERR_CAS_LIMIT) return bfail(b, CFG_ERR_WALK_LIMIT, "edge-count CAS loop exceeded its bound");
+    if ((w.err & DERR_REC_OVERFLOW) || w.rec_cursor > b->rec_cap) {
+        b->rec_cap = w.rec_cursor + w.rec_cursor / 8 + 65536;
+        regrow = true;
+        return CFG_OK;
+    }
+    b->redo.assign(b->n_jobs, 0);
+    for (uint32_t j = 0; j < b->n_jobs; ++j)
+        if (b->h_jobs[j].err) b->redo[j] = 1;
+    if (cnt.retry_count) {
+        std::vector<uint32_t> r(cnt.retry_count);
+        BCK(cudaMemcpyAsync(r.data(), b->retry.p, 4 * r.size(), cudaMemcpyDeviceToHost, b->stream));
+        BCK(cudaStreamSynchronize(b->stream));
+        for (uint32_t x : r) b->redo[x >> b->g_shift] = 1;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    int rc = redo_jobs(b);
+    b->redo_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cfg_batch_create(int device, const cfg_params* params, cfg_batch** out) {
+    if (!out) return CFG_ERR_BAD_INPUT;
+    *out = nullptr;
+    if (!params) return CFG_ERR_BAD_INPUT;
+    const cfg_params& p = *params;
+    if (p.k < 3 || p.k > 63 || (p.k % 2) == 0 || p.l < 1 || p.l > 32 || p.l > p.k - 1) return CFG_ERR_BAD_INPUT;
+    if (p.cutoff < 1 || p.cutoff > 15) return CFG_ERR_BAD_INPUT;
+    if (p.graph_count == 0 || p.graph_count > 65536 || (p.graph_count & (p.graph_count - 1))) return CFG_ERR_BAD_INPUT;
+    if (p.flags) return CFG_ERR_BAD_INPUT;   // no state or record dumps in batches
+    int n_dev = 0;
+    if (cudaGetDeviceCount(&n_dev) != cudaSuccess || device < 0 || device >= n_dev) { cudaGetLastError(); return CFG_ERR_CUDA; }
+    if (cudaSetDevice(device) != cudaSuccess) return CFG_ERR_CUDA;
+    cfg_batch* b = new (std::nothrow) cfg_batch();
+    if (!b) return CFG_ERR_OOM;
+    b->device = device; b->p = p; b->G = p.graph_count; b->words = p.k <= 31 ? 1 : 2;
+    b->g_shift = 0;
+    while ((1u << b->g_shift) < b->G) ++b->g_shift;
+    b->tune.table_load_pct = p.table_load_pct ? p.table_load_pct : 100;
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) { delete b; return CFG_ERR_CUDA; }
+    for (auto& e : b->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) { cfg_batch_destroy(b); return CFG_ERR_CUDA; }
+    *out = b;
+    return CFG_OK;
+}
+
+int cfg_batch_submit(cfg_batch* b, const cfg_packed* jobs, uint32_t n_jobs) {
+    if (!b || (n_jobs && !jobs)) return bfail(b, CFG_ERR_BAD_INPUT, "null input");
+    if (n_jobs == 0) return bfail(b, CFG_ERR_BAD_INPUT, "empty batch");
+    if (((uint64_t)n_jobs << b->g_shift) >= (1ull << 31)) return bfail(b, CFG_ERR_BAD_INPUT, "too many subgraphs in one batch");
+    BCK(cudaSetDevice(b->device));
+    // layout: each job starts on a word boundary of the packed stream
+    std::vector<uint64_t> word_off(n_jobs), job_frag(n_jobs + 1, 0), nb(n_jobs);
+    uint64_t words = 0, nf = 0;
+    for (uint32_t j = 0; j < n_jobs; ++j) {
+        const cfg_packed& J = jobs[j];
+        if ((J.n_bases && !J.words) || (J.n_frags && (!J.frag_off || !J.frag_len))) return bfail(b, CFG_ERR_BAD_INPUT, "null job input");
+        uint64_t at = 0;
+        for (uint64_t f = 0; f < J.n_frags; ++f) {
+            if (J.frag_off[f] != at || J.frag_len[f] < b->p.k + 1)
+                return bfail(b, CFG_ERR_BAD_INPUT, "job fragments must be back-to-back and hold at least k+1 bases");
+            at += J.frag_len[f];
+        }
+        if (at != J.n_bases) return bfail(b, CFG_ERR_BAD_INPUT, "job fragment lengths do not sum to its n_bases");
+        word_off[j] = words;
+        words += (J.n_bases + 31) / 32;
+        nf += J.n_frags;
+        job_frag[j + 1] = nf;
+        nb[j] = J.n_bases;
+    }
+    const uint64_t n_bases = words * 32;
+    if (n_bases >= (1ull << 32)) return bfail(b, CFG_ERR_BAD_INPUT, "a batch must hold fewer than 2^32 bases");
+    std::vector<uint64_t> fo(nf), fo_rel(nf), job_pos(n_jobs + 1);
+    std::vector<uint32_t> fl(nf), fg(nf);
+    for (uint32_t j = 0; j < n_jobs; ++j) {
+        job_pos[j] = word_off[j] * 32;
+        for (uint64_t f = 0; f < jobs[j].n_frags; ++f) {
+            const uint64_t i = job_frag[j] + f;
+            fo_rel[i] = jobs[j].frag_off[f];
+            fo[i] = job_pos[j] + jobs[j].frag_off[f];
+            fl[i] = jobs[j].frag_len[f];
+            fg[i] = j << b->g_shift;
+        }
+    }
+    job_pos[n_jobs] = n_bases;
+    const bool grow = words + 4 > b->packed.bytes / 8 || nf + 1 > b->frag_off.bytes / 8 || n_jobs + 1 > b->job_pos.bytes / 8;
+    if (!b->packed.ensure(8 * (words + 4)) || !b->frag_off.ensure(8 * (nf + 1)) || !b->frag_off_rel.ensure(8 * (nf + 1)) ||
+        !b->frag_len.ensure(4 * (nf + 1)) || !b->frag_gbase.ensure(4 * (nf + 1)) || !b->job_pos.ensure(8 * (n_jobs + 1)) ||
+        !b->job_nbases.ensure(8 * (n_jobs + 1)))
+        return bfail(b, CFG_ERR_OOM, "batch input buffers");
+    BCK(cudaMemsetAsync((uint64_t*)b->packed.p + words, 0, 32, b->stream));
+    for (uint32_t j = 0; j < n_jobs; ++j) {
+        const uint64_t w = (jobs[j].n_bases + 31) / 32;
+        if (w) BCK(cudaMemcpyAsync((uint64_t*)b->packed.p + word_off[j], jobs[j].words, 8 * w, cudaMemcpyHostToDevice, b->stream));
+    }
+    if (nf) {
+        BCK(cudaMemcpyAsync(b->frag_off.p, fo.data(), 8 * nf, cudaMemcpyHostToDevice, b->stream));
+        BCK(cudaMemcpyAsync(b->frag_off_rel.p, fo_rel.data(), 8 * nf, cudaMemcpyHostToDevice, b->stream));
+        BCK(cudaMemcpyAsync(b->frag_len.p, fl.data(), 4 * nf, cudaMemcpyHostToDevice, b->stream));
+        BCK(cudaMemcpyAsync(b->frag_gbase.p, fg.data(), 4 * nf, cudaMemcpyHostToDevice, b->stream));
+    }
+    BCK(cudaMemcpyAsync(b->job_pos.p, job_pos.data(), 8 * (n_jobs + 1), cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaMemcpyAsync(b->job_nbases.p, nb.data(), 8 * n_jobs, cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));   // the host vectors above go out of scope
+    // a graph stays valid while the batch's shape and every buffer address stay the same
+    const bool same = !grow && b->exec && b->n_bases == n_bases && b->n_frags == nf && b->n_jobs == n_jobs && b->nb == nb;
+    b->n_bases = n_bases; b->n_frags = nf; b->n_jobs = n_jobs;
+    b->word_off.swap(word_off); b->job_frag.swap(job_frag); b->nb.swap(nb);
+    b->have_input = true; b->have_run = false;
+    if (!same) {
+        drop_graph(b);
+        int rc = ensure_buffers(b);
+        if (rc) return rc;
+    }
+    return CFG_OK;
+}
+
+int cfg_batch_run(cfg_batch* b) {
+    if (!b) return CFG_ERR_BAD_INPUT;
+    if (!b->have_input) return bfail(b, CFG_ERR_STATE, "cfg_batch_run before cfg_batch_submit");
+    BCK(cudaSetDevice(b->device));
+    b->err.clear();
+    b->have_run = false;
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        bool regrow = false;
+        int rc = run_once(b, regrow);
+        if (rc) return rc;
+        if (!regrow) { b->have_run = true; return CFG_OK; }
+        drop_graph(b);
+        rc = ensure_buffers(b);
+        if (rc) return rc;
+    }
+    return bfail(b, CFG_ERR_OOM, "record buffer kept overflowing");
+}
+
+int cfg_batch_job(cfg_batch* b, uint32_t job, cfg_results* out) {
+    if (!b || !out) return CFG_ERR_BAD_INPUT;
+    if (!b->have_run) return bfail(b, CFG_ERR_STATE, "no completed batch run");
+    if (job >= b->n_jobs) return bfail(b, CFG_ERR_BAD_INPUT, "job index out of range");
+    if (b->redo[job]) {
+        out->counts = b->r_counts[job];
+        out->fasta = b->r_fasta[job].data();
+        out->lmtig_text = b->r_text[job].data();
+        out->lmtigs = b->r_lm[job].data();
+        return CFG_OK;
+    }
+    BCK(cudaSetDevice(b->device));
+    const JobOut& J = b->h_jobs[job];
+    cfg_counts& c = out->counts;
+    c = cfg_counts{};
+    c.n_bases = b->nb[job]; c.n_records = J.records; c.n_instances = J.instances;
+    c.n_vertices = J.vertices; c.n_isolated = J.isolated; c.n_phantom = J.phantom;
+    c.n_trivial = J.trivial; c.n_icc = J.icc; c.n_lmtig = J.lm_used;
+    c.fasta_bytes = J.fasta_used; c.lmtig_bytes = J.lm_text_used; c.n_retries = 0; c.n_launches = b->launches_per_run;
+    if (!b->h_fasta.ensure(c.fasta_bytes + 1) || !b->h_text.ensure(c.lmtig_bytes + 1) || !b->h_lm.ensure(sizeof(cfg_lmtig) * c.n_lmtig + 1))
+        return bfail(b, CFG_ERR_OOM, "pinned result buffers");
+    if (c.fasta_bytes) BCK(cudaMemcpyAsync(b->h_fasta.p, b->fasta.as<char>() + J.fasta_off, c.fasta_bytes, cudaMemcpyDeviceToHost, b->stream));
+    if (c.lmtig_bytes) BCK(cudaMemcpyAsync(b->h_text.p, b->lm_text.as<char>() + J.lm_text_off, c.lmtig_bytes, cudaMemcpyDeviceToHost, b->stream));
+    if (c.n_lmtig) BCK(cudaMemcpyAsync(b->h_lm.p, b->lm.as<LmtigOut>() + J.lm_off, sizeof(cfg_lmtig) * c.n_lmtig, cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    out->fasta = (const char*)b->h_fasta.p;
+    out->lmtig_text = (const char*)b->h_text.p;
+    out->lmtigs = (const cfg_lmtig*)b->h_lm.p;
+    return CFG_OK;
+}
+
+int cfg_batch_info(cfg_batch* b, cfg_batch_stats* out) {
+    if (!b || !out) return CFG_ERR_BAD_INPUT;
+    if (!b->have_run) return bfail(b, CFG_ERR_STATE, "no completed batch run");
+    cfg_batch_stats& s = *out;
+    s = cfg_batch_stats{};
+    s.n_jobs = b->n_jobs;
+    s.device_ms = b->ms;
+    s.redo_ms = b->redo_ms;
+    s.graph_launches = 1;
+    s.kernels_per_run = b->launches_per_run;
+    for (uint32_t j = 0; j < b->n_jobs; ++j) {
+        if (b->redo[j]) { ++s.n_redone; continue; }
+        const JobOut& J = b->h_jobs[j];
+        s.n_bases += b->nb[j]; s.n_records += J.records; s.n_vertices += J.vertices;
+        s.fasta_bytes += J.fasta_used; s.lmtig_bytes += J.lm_text_used; s.n_lmtig += J.lm_used;
+    }
+    for (uint32_t j = 0; j < b->n_jobs; ++j)
+        if (b->redo[j]) {
+            const cfg_counts& c = b->r_counts[j];
+            s.n_bases += c.n_bases; s.n_records += c.n_records; s.n_vertices += c.n_vertices;
+            s.fasta_bytes += c.fasta_bytes; s.lmtig_bytes += c.lmtig_bytes; s.n_lmtig += c.n_lmtig;
+        }
+    s.tuning = b->tune;
+    return CFG_OK;
+}
+
+int cfg_batch_job_device_input(cfg_batch* b, uint32_t job, const uint64_t** d_words, uint64_t* n_bases,
+                               const uint64_t** d_frag_off, const uint32_t** d_frag_len, uint64_t* n_frags) {
+    if (!b || !d_words || !n_bases || !d_frag_off || !d_frag_len || !n_frags) return CFG_ERR_BAD_INPUT;
+    if (!b->have_input || job >= b->n_jobs) return bfail(b, CFG_ERR_BAD_INPUT, "no such job");
+    const uint64_t f0 = b->job_frag[job];
+    *d_words = b->packed.as<uint64_t>() + b->word_off[job];
+    *n_bases = b->nb[job];
+    *d_frag_off = b->frag_off_rel.as<uint64_t>() + f0;
+    *d_frag_len = b->frag_len.as<uint32_t>() + f0;
+    *n_frags = b->job_frag[job + 1] - f0;
+    return CFG_OK;
+}
+
+int cfg_batch_set_tuning(cfg_batch* b, const cfg_batch_tuning* t) {
+    if (!b || !t) return CFG_ERR_BAD_INPUT;
+    if (t->local_div < 1 || t->local_div > 16 || (t->cluster_threads && (t->cluster_threads % 32 || t->cluster_threads > 512)) ||
+        t->table_load_pct > 100000)
+        return bfail(b, CFG_ERR_BAD_INPUT, "tuning out of range");
+    b->tune = *t;
+    if (!b->tune.table_load_pct) b->tune.table_load_pct = 100;
+    drop_graph(b);
+    return CFG_OK;
+}
+
+int cfg_batch_tune(cfg_batch* b, cfg_batch_tuning* out) {
+    if (!b) return CFG_ERR_BAD_INPUT;
+    if (!b->have_input) return bfail(b, CFG_ERR_STATE, "cfg_batch_tune before cfg_batch_submit");
+    const uint32_t base_load = b->tune.table_load_pct ? b->tune.table_load_pct : 100;
+    const uint32_t divs[] = {2, 4, 8};
+    const uint32_t loads[] = {base_load, base_load * 2};
+    const uint32_t cthreads[] = {256, 512};
+    cfg_batch_tuning best = b->tune;
+    best.ms = 1e30f;
+    for (uint32_t d : divs)
+        for (uint32_t ld : loads)
+            for (uint32_t ct : cthreads) {
+                cfg_batch_tuning t{d, ct, ld, 0, 0.f};
+                int rc = cfg_batch_set_tuning(b, &t);
+                if (rc) return rc;
+                // a redone job would time the plain driver, not this shape: skip such shapes
+                float m = 0;
+                bool ok = true;
+                for (int rep = 0; rep < 2 && ok; ++rep) {
+                    rc = cfg_batch_run(b);
+                    if (rc) return rc;
+                    for (uint32_t j = 0; j < b->n_jobs; ++j) if (b->redo[j]) ok = false;
+                    m = b->ms;   // the second run: the graph is built and warm
+                }
+                if (ok && m < best.ms) { best = t; best.ms = m; }
+            }
+    if (best.ms >= 1e30f) { best = cfg_batch_tuning{4, 512, base_load, 0, 0.f}; }
+    const float ms = best.ms;
+    int rc = cfg_batch_set_tuning(b, &best);
+    if (rc) return rc;
+    b->tune.ms = ms;
+    if (out) *out = b->tune;
+    return CFG_OK;
+}
+
+const char* cfg_batch_last_error_string(cfg_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+void cfg_batch_destroy(cfg_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    drop_graph(b);
+    DevBuf* bufs[] = {&b->packed, &b->frag_off, &b->frag_off_rel, &b->frag_len, &b->frag_gbase, &b->job_pos, &b->job_nbases,
+                      &b->flat, &b->hist, &b->bw, &b->bucket_off, &b->inst, &b->fill, &b->partials, &b->recs, &b->list,
+                      &b->tab_off, &b->tab_cap, &b->arena, &b->jobs, &b->fasta, &b->lm_text, &b->lm, &b->retry, &b->counters};
+    for (DevBuf* x : bufs) x->release();
+    b->h_fasta.release(); b->h_text.release(); b->h_lm.release();
+    if (b->plain) cfg_destroy(b->plain);
+    for (auto& e : b->ev) if (e) cudaEventDestroy(e);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+}  // extern "C"

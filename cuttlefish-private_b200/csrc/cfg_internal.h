@@ -27,6 +27,7 @@ enum : uint32_t {
     DERR_WALK_LIMIT = 8u,      // a walk exceeded its step bound (bug guard)
     DERR_CAS_LIMIT = 16u,      // a CAS retry loop exceeded its bound (bug guard)
     DERR_DUMP_OVERFLOW = 32u,  // state dump buffer too small (recoverable)
+    DERR_NO_ROOM = 64u,        // batch: a job's output regions or tables did not fit the arenas
 };
 
 struct PartitionArgs {
@@ -44,6 +45,7 @@ struct PartitionArgs {
     unsigned long long* rec_cursor;
     unsigned long long* hist;   // per subgraph: records (low 32) | instances (high 32)
     uint32_t* err;
+    const uint32_t* frag_gbase; // batch: first histogram entry of each fragment's job (nullptr: 0)
 };
 
 struct ScatterArgs {
@@ -52,6 +54,13 @@ struct ScatterArgs {
     const uint32_t* bucket_off;  // G + 1 offsets
     uint32_t* bucket_fill;       // G counters, zeroed
     uint64_t* recs;              // bucketed
+    // batch: job j owns stream bases [job_pos[j], job_pos[j+1]) and buckets
+    // [j << g_shift, (j+1) << g_shift); nullptr: one job
+    const uint64_t* job_pos;
+    uint32_t n_jobs, g_shift;
+    // batch: the record count is the device word *n_dev (n is the buffer's capacity; a
+    // count above it means the partition overflowed and nothing is scattered)
+    const uint32_t* n_dev;
 };
 
 struct LmtigOut {                // mirrors cfg_lmtig
@@ -67,6 +76,16 @@ struct StateOut {                // mirrors cfg_state
     uint32_t ef;
     uint16_t g;
     uint8_t status, pad;
+};
+
+// Output regions and counters of one job of a batch.  The six counters from
+// `vertices` on are laid out as the first six of Counters.
+struct JobOut {
+    unsigned long long fasta_off, fasta_cap, lm_text_off, lm_text_cap, lm_off, lm_cap;   // regions
+    unsigned long long fasta_used, lm_text_used, lm_used;                                // cursors
+    unsigned long long vertices, isolated, phantom, trivial, icc, lmtig;
+    unsigned long long records, instances;
+    uint32_t err, pad;   // DERR_OUT_OVERFLOW / DERR_NO_ROOM: redo this job alone
 };
 
 struct Counters {                // device-side counters of the subgraph phase
@@ -94,6 +113,14 @@ struct SubgraphArgs {
     uint32_t* retry;             // subgraphs whose table overflowed
     Counters* cnt;
     uint32_t* err;
+    // persistent launches: list, tab_off and tab_cap start at entry *list_base and hold
+    // *list_n entries (device words written by an earlier kernel); nullptr: 0 and n_list
+    const uint32_t* list_base;
+    const uint32_t* list_n;
+    // batch: bucket b belongs to job b >> g_shift and writes to jobs[b >> g_shift]; nullptr: one job
+    JobOut* jobs;
+    uint32_t g_shift;
+    uint32_t record_clocks;      // accumulate per-phase SM cycles into cnt->phase_cycles
 };
 
 // bytes per table slot: k-mer (8 per word) + state word (8) + meta (4) + work-list entry (4)
@@ -105,6 +132,16 @@ void launch_bucket_scan(const unsigned long long* hist, uint32_t G, uint32_t* bu
 void launch_scatter(const ScatterArgs& a, cudaStream_t s);
 // cluster == 0: tables in the global arena; 1: one CTA's shared memory; >1: a cluster's.
 cudaError_t launch_subgraphs(const SubgraphArgs& a, int words, uint32_t cluster, uint32_t threads, cudaStream_t s);
+// Persistent form: `grid` CTAs (a multiple of `cluster`) loop over the device-held list.
+cudaError_t launch_subgraphs_persistent(const SubgraphArgs& a, int words, uint32_t cluster, uint32_t threads,
+                                        uint32_t per, uint32_t grid, cudaStream_t s);
+// Resident CTAs per SM (cluster <= 1) or resident clusters per GPU (cluster > 1) of a
+// shared-table launch shape; also raises the kernel's dynamic shared-memory limit.
+int subgraph_occupancy(int words, uint32_t cluster, uint32_t threads, uint32_t per);
+// Multi-block exclusive scan of n >= 1 histogram entries (batch bucket counts):
+// bucket_off[0..n], inst[b], fill[b] = 0.  `partials` holds (n + 8191) / 8192 words.
+void launch_bucket_scan_large(const unsigned long long* hist, uint32_t n, uint32_t* bucket_off, uint32_t* inst,
+                              uint32_t* fill, uint32_t* partials, cudaStream_t s);
 uint32_t subgraph_max_per_cta(int words);      // one CTA owning a whole table
 uint32_t subgraph_cluster_per_cta(int words);  // each CTA of a cluster
 

@@ -28,8 +28,9 @@ __device__ __forceinline__ uint64_t lmer_at(const uint64_t* __restrict__ s, uint
 // Processes the (k-1)-mer positions [j0, j1) of one fragment: emits every weak
 // super k-mer whose run starts there.
 // mod_w[x] = x % w for x < 128 (w <= 62): the cap-cut test without a division.
+// hist: this fragment's job's histogram (the run's, or its job's slice of a batch's).
 __device__ void sweep_fragment(const PartitionArgs& a, uint64_t* ring, const uint8_t* mod_w, uint64_t F0, uint32_t FL,
-                               uint32_t j0, uint32_t j1) {
+                               uint32_t j0, uint32_t j1, unsigned long long* hist) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t k = a.k, l = a.l, w = a.w;
     const uint32_t M = FL - k + 2;                 // (k-1)-mers in the fragment
@@ -126,7 +127,7 @@ __device__ void sweep_fragment(const PartitionArgs& a, uint64_t* ring, const uin
             const uint64_t r = rec_pack((uint32_t)(F0 + c - lj), len, lj & cchg, is_chg ? 1u : 0u, cg);
             const unsigned long long idx = slot0 + __popc(emit & lanemask_lt());
             if (idx < a.rec_cap) a.recs[idx] = r; else atomicOr(a.err, DERR_REC_OVERFLOW);
-            atomicAdd(a.hist + cg, 1ull | ((unsigned long long)(len - k + 1) << 32));
+            atomicAdd(hist + cg, 1ull | ((unsigned long long)(len - k + 1) << 32));
         }
         // carries: last cut / run start of this chunk
         if (cut) {
@@ -143,7 +144,7 @@ __device__ void sweep_fragment(const PartitionArgs& a, uint64_t* ring, const uin
             const uint64_t r = rec_pack((uint32_t)(F0 + c - lj), len, lj & last_cut_chg, 0, last_cut_g);
             const unsigned long long idx = slot0 + __popc(emit);
             if (idx < a.rec_cap) a.recs[idx] = r; else atomicOr(a.err, DERR_REC_OVERFLOW);
-            atomicAdd(a.hist + last_cut_g, 1ull | ((unsigned long long)(len - k + 1) << 32));
+            atomicAdd(hist + last_cut_g, 1ull | ((unsigned long long)(len - k + 1) << 32));
         }
         if (stopping || fin) return;
     }
@@ -174,7 +175,7 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_partition(const Partit
             const uint32_t j0 = s0 > F0 ? (uint32_t)(s0 - F0) : 0;
             const uint64_t e = s1 - F0;
             const uint32_t j1 = e < M ? (uint32_t)e : M;
-            if (j0 < j1) sweep_fragment(a, ring, mod_w, F0, FL, j0, j1);
+            if (j0 < j1) sweep_fragment(a, ring, mod_w, F0, FL, j0, j1, a.hist + (a.frag_gbase ? a.frag_gbase[f] : 0u));
         }
     }
 }
@@ -206,10 +207,96 @@ __global__ void __launch_bounds__(1024) k_bucket_scan(const unsigned long long* 
     if (t == 1023) bucket_off[G] = part[1023];
 }
 
+// Multi-block scan for batches (millions of buckets): 8192 entries per block.
+constexpr uint32_t SCAN_PER_THREAD = 8, SCAN_BLOCK = 1024, SCAN_CHUNK = SCAN_PER_THREAD * SCAN_BLOCK;
+
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* warp_sums, uint32_t& total) {
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t x = v;
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= (uint32_t)d) x += y;
+    }
+    if (lane == 31) warp_sums[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t w = lane < (blockDim.x >> 5) ? warp_sums[lane] : 0;
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, d);
+            if (lane >= (uint32_t)d) w += y;
+        }
+        warp_sums[lane] = w;   // inclusive
+    }
+    __syncthreads();
+    total = warp_sums[(blockDim.x >> 5) - 1];
+    const uint32_t before = wid ? warp_sums[wid - 1] : 0;
+    __syncthreads();
+    return before + x - v;
+}
+
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_reduce(const unsigned long long* __restrict__ hist, uint32_t n,
+                                                            uint32_t* partials) {
+    __shared__ uint32_t ws[32];
+    const uint64_t b0 = (uint64_t)blockIdx.x * SCAN_CHUNK + (uint64_t)threadIdx.x * SCAN_PER_THREAD;
+    uint32_t sum = 0;
+    for (uint32_t i = 0; i < SCAN_PER_THREAD; ++i)
+        if (b0 + i < n) sum += (uint32_t)hist[b0 + i];
+    uint32_t total;
+    block_excl_scan(sum, ws, total);
+    if (threadIdx.x == 0) partials[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_partials(uint32_t* partials, uint32_t np) {
+    __shared__ uint32_t ws[32];
+    const uint32_t per = (np + SCAN_BLOCK - 1) / SCAN_BLOCK;
+    const uint32_t p0 = threadIdx.x * per;
+    uint32_t sum = 0;
+    for (uint32_t i = 0; i < per; ++i)
+        if (p0 + i < np) sum += partials[p0 + i];
+    uint32_t total;
+    uint32_t run = block_excl_scan(sum, ws, total);
+    for (uint32_t i = 0; i < per; ++i)
+        if (p0 + i < np) { const uint32_t v = partials[p0 + i]; partials[p0 + i] = run; run += v; }
+}
+
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_apply(const unsigned long long* __restrict__ hist, uint32_t n,
+                                                           const uint32_t* __restrict__ partials, uint32_t* bucket_off,
+                                                           uint32_t* inst, uint32_t* fill) {
+    __shared__ uint32_t ws[32];
+    const uint64_t b0 = (uint64_t)blockIdx.x * SCAN_CHUNK + (uint64_t)threadIdx.x * SCAN_PER_THREAD;
+    unsigned long long h[SCAN_PER_THREAD];
+    uint32_t sum = 0;
+    for (uint32_t i = 0; i < SCAN_PER_THREAD; ++i) {
+        h[i] = b0 + i < n ? hist[b0 + i] : 0ull;
+        sum += (uint32_t)h[i];
+    }
+    uint32_t total;
+    uint32_t run = partials[blockIdx.x] + block_excl_scan(sum, ws, total);
+    for (uint32_t i = 0; i < SCAN_PER_THREAD; ++i) {
+        if (b0 + i >= n) break;
+        bucket_off[b0 + i] = run;
+        inst[b0 + i] = (uint32_t)(h[i] >> 32);
+        fill[b0 + i] = 0;
+        run += (uint32_t)h[i];
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) bucket_off[n] = partials[blockIdx.x] + total;
+}
+
 __global__ void k_scatter(const ScatterArgs a) {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t n = a.n_dev ? *a.n_dev : a.n;
+    if (n > a.n) return;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t r = a.flat[i];
-        const uint32_t g = rec_g(r);
+        uint32_t g = rec_g(r);
+        if (a.job_pos) {   // the record's job: the last job starting at or before its first base
+            const uint64_t p = rec_pos(r);
+            uint32_t lo = 0, hi = a.n_jobs;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (a.job_pos[mid] <= p) lo = mid; else hi = mid;
+            }
+            g += lo << a.g_shift;
+        }
         const uint32_t slot = atomicAdd(a.bucket_fill + g, 1u);
         a.recs[a.bucket_off[g] + slot] = r;
     }
@@ -228,6 +315,14 @@ void launch_partition(const PartitionArgs& a, cudaStream_t s) {
 void launch_bucket_scan(const unsigned long long* hist, uint32_t G, uint32_t* bucket_off, uint32_t* inst,
                         uint32_t* fill, cudaStream_t s) {
     k_bucket_scan<<<1, 1024, 0, s>>>(hist, G, bucket_off, inst, fill);
+}
+
+void launch_bucket_scan_large(const unsigned long long* hist, uint32_t n, uint32_t* bucket_off, uint32_t* inst,
+                              uint32_t* fill, uint32_t* partials, cudaStream_t s) {
+    const uint32_t nb = (n + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    k_scan_reduce<<<nb, SCAN_BLOCK, 0, s>>>(hist, n, partials);
+    k_scan_partials<<<1, SCAN_BLOCK, 0, s>>>(partials, nb);
+    k_scan_apply<<<nb, SCAN_BLOCK, 0, s>>>(hist, n, partials, bucket_off, inst, fill);
 }
 
 void launch_scatter(const ScatterArgs& a, cudaStream_t s) {

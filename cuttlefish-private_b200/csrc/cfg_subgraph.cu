@@ -214,9 +214,35 @@ struct Tab {
     }
 };
 
+// Where one subgraph's outputs go: the run's arenas, or its job's regions in a batch.
+struct Sink {
+    char* fasta; unsigned long long fasta_cap; unsigned long long* fasta_cur;
+    char* lm_text; unsigned long long lm_text_cap; unsigned long long* lm_text_cur;
+    LmtigOut* lm; unsigned long long lm_cap; unsigned long long* lm_cur;
+    unsigned long long* cnt;   // vertices, isolated, phantom, trivial, icc, lmtig
+    uint32_t* oflow;           // DERR_OUT_OVERFLOW is raised here
+    uint32_t g;                // the subgraph's id within its job
+};
+
+__device__ __forceinline__ void sink_for(const SubgraphArgs& a, uint32_t b, Sink& o) {
+    if (a.jobs) {
+        JobOut& J = a.jobs[b >> a.g_shift];
+        o.fasta = a.fasta + J.fasta_off; o.fasta_cap = J.fasta_cap; o.fasta_cur = &J.fasta_used;
+        o.lm_text = a.lm_text + J.lm_text_off; o.lm_text_cap = J.lm_text_cap; o.lm_text_cur = &J.lm_text_used;
+        o.lm = a.lm + J.lm_off; o.lm_cap = J.lm_cap; o.lm_cur = &J.lm_used;
+        o.cnt = &J.vertices; o.oflow = &J.err; o.g = b & ((1u << a.g_shift) - 1);
+    } else {
+        o.fasta = a.fasta; o.fasta_cap = a.fasta_cap; o.fasta_cur = &a.cnt->fasta_bytes;
+        o.lm_text = a.lm_text; o.lm_text_cap = a.lm_text_cap; o.lm_text_cur = &a.cnt->lm_bytes;
+        o.lm = a.lm; o.lm_cap = a.lm_cap; o.lm_cur = &a.cnt->lm_count;
+        o.cnt = &a.cnt->vertices; o.oflow = a.err; o.g = b;
+    }
+}
+
 struct Block {   // per-CTA shared bookkeeping (in CLUSTER mode the flags of rank 0 are the cluster's)
     uint32_t inserted, overflow, wl_n, pad;
     unsigned long long vertices, isolated, phantom, trivial, icc, lmtig;
+    Sink sk;
 };
 
 __device__ __forceinline__ uint32_t lane_lt() { uint32_t m; asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m)); return m; }
@@ -293,11 +319,10 @@ __device__ __forceinline__ bool step(const Tab<W, MODE>& T, const KOps<W>& ops, 
     else return step_outline(T, ops, fth, v, side, s_in);
 }
 
-template <int W>
-__device__ __forceinline__ char* reserve_fasta(const SubgraphArgs& a, uint32_t L) {
-    const unsigned long long off = atomicAdd(&a.cnt->fasta_bytes, (unsigned long long)(L + 4));
-    if (off + L + 4 > a.fasta_cap) { atomicOr(a.err, DERR_OUT_OVERFLOW); return nullptr; }
-    char* p = a.fasta + off;
+__device__ __forceinline__ char* reserve_fasta(const Sink& sk, uint32_t L) {
+    const unsigned long long off = atomicAdd(sk.fasta_cur, (unsigned long long)(L + 4));
+    if (off + L + 4 > sk.fasta_cap) { atomicOr(sk.oflow, DERR_OUT_OVERFLOW); return nullptr; }
+    char* p = sk.fasta + off;
     p[0] = '>'; p[1] = '0'; p[2] = '\n'; p[3 + L] = '\n';
     return p + 3;
 }
@@ -324,7 +349,7 @@ __device__ void write_path(const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t f
 
 template <int W, int MODE>
 __device__ void emit_kmer_cycle(const SubgraphArgs& a, const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t s, Block& B) {
-    char* p = reserve_fasta<W>(a, ops.k);
+    char* p = reserve_fasta(B.sk, ops.k);
     if (p) { const Kmer<W> x = T.key(s); for (uint32_t i = 0; i < ops.k; ++i) p[i] = "ACGT"[ops.base(x, i)]; }
     atomicAdd(&B.trivial, 1ull); atomicAdd(&B.icc, 1ull);
 }
@@ -367,7 +392,7 @@ struct RecBases {
 };
 
 template <int W, int MODE>
-__device__ void emit_path(const SubgraphArgs& a, const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t g, const DV<W>& v0,
+__device__ void emit_path(const SubgraphArgs& a, const Tab<W, MODE>& T, const KOps<W>& ops, const DV<W>& v0,
                           int side0, uint32_t n, const DV<W>& vlast, EndInfo st, EndInfo en, bool seed_canon, Block& B) {
     const uint32_t k = ops.k, fth = a.fth;
     const uint32_t L = n + k - 1;
@@ -375,7 +400,7 @@ __device__ void emit_path(const SubgraphArgs& a, const Tab<W, MODE>& T, const KO
     if (!lm) {
         // trivial maximal unitig in canonical orientation (Maximal_Unitig_Scratch::finalize, :200-222)
         const bool rev = vlast.r < v0.d;   // rc(last k-mer) < first k-mer
-        char* p = reserve_fasta<W>(a, L);
+        char* p = reserve_fasta(B.sk, L);
         write_path(T, ops, fth, v0, side0, n, p, rev, true);
         atomicAdd(&B.trivial, 1ull);
         return;
@@ -385,12 +410,13 @@ __device__ void emit_path(const SubgraphArgs& a, const Tab<W, MODE>& T, const KO
     const EndInfo eu = rev ? en : st, ev = rev ? st : en;
     const bool u_first_canon = rev ? !en.canon : st.canon;     // label's first k-mer canonical?
     const bool v_last_canon = rev ? !st.canon : en.canon;      // label's last k-mer canonical?
-    const unsigned long long idx = atomicAdd(&a.cnt->lm_count, 1ull);
-    const unsigned long long off = atomicAdd(&a.cnt->lm_bytes, (unsigned long long)L);
+    const Sink& sk = B.sk;
+    const unsigned long long idx = atomicAdd(sk.lm_cur, 1ull);
+    const unsigned long long off = atomicAdd(sk.lm_text_cur, (unsigned long long)L);
     atomicAdd(&B.lmtig, 1ull);
-    const bool fits = idx < a.lm_cap && off + L <= a.lm_text_cap;
-    if (!fits) atomicOr(a.err, DERR_OUT_OVERFLOW);
-    write_path(T, ops, fth, v0, side0, n, fits ? a.lm_text + off : nullptr, rev, true);
+    const bool fits = idx < sk.lm_cap && off + L <= sk.lm_text_cap;
+    if (!fits) atomicOr(sk.oflow, DERR_OUT_OVERFLOW);
+    write_path(T, ops, fth, v0, side0, n, fits ? sk.lm_text + off : nullptr, rev, true);
     if (!fits) return;
     LmtigOut o;
     const Kmer<W> phi = phi_kmer(ops);
@@ -399,10 +425,10 @@ __device__ void emit_path(const SubgraphArgs& a, const Tab<W, MODE>& T, const KO
     put_key(o.v, v_exit ? T.key(ev.slot) : phi);
     const uint32_t s_u_back = u_exit ? (u_first_canon ? 1u : 0u) : 1u;
     const uint32_t s_v_back = v_exit ? (v_last_canon ? 0u : 1u) : 1u;
-    o.label_off = off; o.label_len = L; o.g = (uint16_t)g;
+    o.label_off = off; o.label_len = L; o.g = (uint16_t)sk.g;
     o.flags = (uint8_t)(s_u_back | (s_v_back << 1) | ((!u_exit) << 2) | ((!v_exit) << 3));
     o.pad = 0;
-    a.lm[idx] = o;
+    sk.lm[idx] = o;
 }
 
 // rank/nranks: this CTA's position in its cluster; per: slots owned by one CTA.
@@ -422,7 +448,10 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         lst[s] = 0xffffffff00000000ull;   // ef 0, first occurrence "none"
         lmeta[s] = 0;
     }
-    if (tid == 0) { B.inserted = 0; B.overflow = 0; B.wl_n = 0; B.vertices = B.isolated = B.phantom = B.trivial = B.icc = B.lmtig = 0; }
+    if (tid == 0) {
+        B.inserted = 0; B.overflow = 0; B.wl_n = 0; B.vertices = B.isolated = B.phantom = B.trivial = B.icc = B.lmtig = 0;
+        sink_for(a, g, B.sk);
+    }
     tsync<MODE>();
 
     // ---------------- build ----------------
@@ -541,7 +570,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
             else {
                 const DV<W> v = dv_at(T, ops, s, BACK);
                 const EndInfo st{s, term_of(meta, FRONT), true}, en{s, term_of(meta, BACK), true};
-                emit_path(a, T, ops, g, v, BACK, 1, v, st, en, true, B);
+                emit_path(a, T, ops, v, BACK, 1, v, st, en, true, B);
             }
             lmeta[ls] = lmeta[ls] | M_VISITED;
             continue;
@@ -595,7 +624,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
             uint32_t best = m_int; bool best_canon = m_int_canon;
             if (!fake0 && ins0 < best) { best = ins0; best_canon = side0 == BACK; }
             if (!fake1 && ins1 < best) { best = ins1; best_canon = e_side == BACK; }
-            emit_path(a, T, ops, g, vs, sd0, n2, ve, st, en, best_canon, B);
+            emit_path(a, T, ops, vs, sd0, n2, ve, st, en, best_canon, B);
         }
         if (fake0) T.or_meta(s, M_VISITED);
         if (fake1) T.or_meta(e, M_VISITED);
@@ -627,7 +656,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         if (!ok || !is_min) continue;
         // Character_Buffer::rotate_append_cycle (include/Character_Buffer.hpp:166-175): start at the
         // minimum vertex in its canonical orientation
-        char* p = reserve_fasta<W>(a, n + k - 1);
+        char* p = reserve_fasta(B.sk, n + k - 1);
         write_path(T, ops, fth, v0, BACK, n, p, false, true);
         atomicAdd(&B.trivial, 1ull); atomicAdd(&B.icc, 1ull);
     }
@@ -642,17 +671,18 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
             if (i >= a.dump_cap) { atomicOr(a.err, DERR_DUMP_OVERFLOW); continue; }
             StateOut o;
             put_key(o.key, T.key(s));
-            o.ef = st_ef(lst[ls]); o.g = (uint16_t)g; o.status = (uint8_t)(lmeta[ls] & 7); o.pad = 0;
+            o.ef = st_ef(lst[ls]); o.g = (uint16_t)B.sk.g; o.status = (uint8_t)(lmeta[ls] & 7); o.pad = 0;
             a.dump[i] = o;
         }
     }
     __syncthreads();
     if (tid == 0) {
         clk[5] = clock64();
-        for (int i = 0; i < 5; ++i) atomicAdd(&a.cnt->phase_cycles[i], (unsigned long long)(clk[i + 1] - clk[i]));
-        atomicAdd(&a.cnt->vertices, B.vertices); atomicAdd(&a.cnt->isolated, B.isolated);
-        atomicAdd(&a.cnt->phantom, B.phantom); atomicAdd(&a.cnt->trivial, B.trivial);
-        atomicAdd(&a.cnt->icc, B.icc); atomicAdd(&a.cnt->lmtig, B.lmtig);
+        if (a.record_clocks)
+            for (int i = 0; i < 5; ++i) atomicAdd(&a.cnt->phase_cycles[i], (unsigned long long)(clk[i + 1] - clk[i]));
+        const unsigned long long v[6] = {B.vertices, B.isolated, B.phantom, B.trivial, B.icc, B.lmtig};
+        for (int i = 0; i < 6; ++i)
+            if (v[i]) atomicAdd(B.sk.cnt + i, v[i]);
     }
     tsync<MODE>();   // no CTA leaves while another may still read its shared memory
 }
@@ -682,32 +712,52 @@ __global__ void __launch_bounds__(512) k_subgraph_shared(const SubgraphArgs a) {
     T.shift = 31 - __clz(per); T.pmask = per - 1;
     Block* Bc = &B;
     if constexpr (MODE == CLUSTER) Bc = cg::this_cluster().map_shared_rank(&B, 0);
-    const uint32_t i = blockIdx.x / nranks;
-    if (i < a.n_list) run_subgraph<W, MODE>(a, T, B, Bc, a.list[i], rank, nranks, per, lk, ls, lm, wl);
+    // one pass over the list (grid = list x cluster), or a persistent grid striding through it
+    const uint32_t* list = a.list + (a.list_base ? *a.list_base : 0u);
+    const uint32_t n = a.list_n ? *a.list_n : a.n_list;
+    for (uint32_t i = blockIdx.x / nranks; i < n; i += gridDim.x / nranks)
+        run_subgraph<W, MODE>(a, T, B, Bc, list[i], rank, nranks, per, lk, ls, lm, wl);
 }
 
 template <int W>
 __global__ void __launch_bounds__(512) k_subgraph_global(const SubgraphArgs a) {
     __shared__ Block B;
-    for (uint32_t i = blockIdx.x; i < a.n_list; i += gridDim.x) {
-        const uint32_t cap = a.tab_cap[i];
-        unsigned char* base = a.arena + a.tab_off[i] * (uint64_t)slot_bytes(W);
+    const uint32_t lb = a.list_base ? *a.list_base : 0u;
+    const uint32_t n = a.list_n ? *a.list_n : a.n_list;
+    for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const uint32_t cap = a.tab_cap[lb + i];
+        if (cap == 0) continue;   // no arena room: the job is redone on its own
+        unsigned char* base = a.arena + a.tab_off[lb + i] * (uint64_t)slot_bytes(W);
         Tab<W, GLOBAL> T;
         unsigned long long *lk, *ls; uint32_t *lm, *wl;
         carve<W>(base, cap, lk, ls, lm, wl);
         T.keys = (uint64_t)lk; T.st = (uint64_t)ls; T.meta = (uint64_t)lm;
         T.per = cap; T.nranks = 1; T.rank = 0; T.shift = 31; T.pmask = 0xffffffffu; T.err_flag = a.err;
-        run_subgraph<W, GLOBAL>(a, T, B, &B, a.list[i], 0, 1, cap, lk, ls, lm, wl);
+        run_subgraph<W, GLOBAL>(a, T, B, &B, a.list[lb + i], 0, 1, cap, lk, ls, lm, wl);
         __syncthreads();
     }
 }
 
+// The kernels' shared-memory limit is always raised to the largest table any launch
+// uses (it is process-wide state: lowering it would break launches recorded in graphs).
+template <int W> constexpr size_t max_table_bytes() { return (size_t)(W == 1 ? 4096 : 2048) * (W == 1 ? 24 : 32); }
 template <typename K>
-cudaError_t launch_shared(K kernel, const SubgraphArgs& a, uint32_t cluster, uint32_t threads, size_t bytes, cudaStream_t s) {
-    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e != cudaSuccess) return e;
+cudaError_t raise_smem_limit(K kernel, size_t bytes) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// grid 0: one pass (list x cluster CTAs), which first raises the kernel's shared-memory
+// limit; a persistent grid relies on subgraph_occupancy having raised it (no attribute
+// calls while a stream is being captured).
+template <typename K>
+cudaError_t launch_shared(K kernel, const SubgraphArgs& a, uint32_t cluster, uint32_t threads, size_t bytes, cudaStream_t s,
+                          uint32_t grid = 0, size_t limit = 0) {
+    if (!grid) {
+        cudaError_t e = raise_smem_limit(kernel, limit > bytes ? limit : bytes);
+        if (e != cudaSuccess) return e;
+    }
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(a.n_list * cluster);
+    cfg.gridDim = dim3(grid ? grid : a.n_list * cluster);
     cfg.blockDim = dim3(threads);
     cfg.dynamicSmemBytes = bytes;
     cfg.stream = s;
@@ -721,6 +771,31 @@ cudaError_t launch_shared(K kernel, const SubgraphArgs& a, uint32_t cluster, uin
 
 }  // namespace
 
+template <typename K>
+int occupancy_of(K kernel, uint32_t cluster, uint32_t threads, size_t bytes, size_t limit) {
+    if (raise_smem_limit(kernel, limit > bytes ? limit : bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    if (cluster <= 1) {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, (int)threads, bytes) != cudaSuccess) { cudaGetLastError(); return 0; }
+        return n;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cluster);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = bytes;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster; attr[0].val.clusterDim.y = 1; attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, kernel, &cfg) != cudaSuccess) { cudaGetLastError(); return 0; }
+    return n;
+}
+
 uint32_t subgraph_max_per_cta(int words) { return words == 1 ? 4096 : 2048; }
 uint32_t subgraph_cluster_per_cta(int words) { return words == 1 ? 4096 : 2048; }
 
@@ -733,10 +808,37 @@ cudaError_t launch_subgraphs(const SubgraphArgs& a, int words, uint32_t cluster,
     }
     const size_t bytes = (size_t)a.smem_cap * slot_bytes(words);
     if (cluster == 1)
-        return words == 1 ? launch_shared(k_subgraph_shared<1, LOCAL>, a, 1, threads, bytes, s)
-                          : launch_shared(k_subgraph_shared<2, LOCAL>, a, 1, threads, bytes, s);
-    return words == 1 ? launch_shared(k_subgraph_shared<1, CLUSTER>, a, cluster, threads, bytes, s)
-                      : launch_shared(k_subgraph_shared<2, CLUSTER>, a, cluster, threads, bytes, s);
+        return words == 1 ? launch_shared(k_subgraph_shared<1, LOCAL>, a, 1, threads, bytes, s, 0, max_table_bytes<1>())
+                          : launch_shared(k_subgraph_shared<2, LOCAL>, a, 1, threads, bytes, s, 0, max_table_bytes<2>());
+    return words == 1 ? launch_shared(k_subgraph_shared<1, CLUSTER>, a, cluster, threads, bytes, s, 0, max_table_bytes<1>())
+                      : launch_shared(k_subgraph_shared<2, CLUSTER>, a, cluster, threads, bytes, s, 0, max_table_bytes<2>());
+}
+
+int subgraph_occupancy(int words, uint32_t cluster, uint32_t threads, uint32_t per) {
+    const size_t bytes = (size_t)per * slot_bytes(words);
+    if (cluster <= 1)
+        return words == 1 ? occupancy_of(k_subgraph_shared<1, LOCAL>, 1, threads, bytes, max_table_bytes<1>())
+                          : occupancy_of(k_subgraph_shared<2, LOCAL>, 1, threads, bytes, max_table_bytes<2>());
+    return words == 1 ? occupancy_of(k_subgraph_shared<1, CLUSTER>, cluster, threads, bytes, max_table_bytes<1>())
+                      : occupancy_of(k_subgraph_shared<2, CLUSTER>, cluster, threads, bytes, max_table_bytes<2>());
+}
+
+cudaError_t launch_subgraphs_persistent(const SubgraphArgs& a, int words, uint32_t cluster, uint32_t threads,
+                                        uint32_t per, uint32_t grid, cudaStream_t s) {
+    if (grid == 0) return cudaSuccess;
+    if (cluster == 0) {
+        if (words == 1) k_subgraph_global<1><<<grid, threads, 0, s>>>(a);
+        else k_subgraph_global<2><<<grid, threads, 0, s>>>(a);
+        return cudaGetLastError();
+    }
+    SubgraphArgs b = a;
+    b.smem_cap = per;
+    const size_t bytes = (size_t)per * slot_bytes(words);
+    if (cluster == 1)
+        return words == 1 ? launch_shared(k_subgraph_shared<1, LOCAL>, b, 1, threads, bytes, s, grid)
+                          : launch_shared(k_subgraph_shared<2, LOCAL>, b, 1, threads, bytes, s, grid);
+    return words == 1 ? launch_shared(k_subgraph_shared<1, CLUSTER>, b, cluster, threads, bytes, s, grid)
+                      : launch_shared(k_subgraph_shared<2, CLUSTER>, b, cluster, threads, bytes, s, grid);
 }
 
 }  // namespace cfg

@@ -67,6 +67,18 @@ class Packed(ctypes.Structure):
                 ("frag_off", U64P), ("frag_len", U32P), ("pinned", ctypes.c_int)]
 
 
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("local_div", ctypes.c_uint32), ("cluster_threads", ctypes.c_uint32),
+                ("table_load_pct", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("ms", ctypes.c_float)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in (
+        "n_jobs", "n_redone", "n_bases", "n_records", "n_vertices", "n_lmtig", "fasta_bytes", "lmtig_bytes",
+        "kernels_per_run", "graph_launches")] + [("device_ms", ctypes.c_float), ("redo_ms", ctypes.c_float),
+                                                 ("tuning", BatchTuning)]
+
+
 # every exported entry point with its ctypes signature
 SIGNATURES = {
     "cfg_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(Params), ctypes.POINTER(ctypes.c_void_p)]),
@@ -92,6 +104,18 @@ SIGNATURES = {
     "cfg_pack_records": (ctypes.c_int, [ctypes.c_char_p, U64P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int,
                                         ctypes.POINTER(Packed)]),
     "cfg_packed_free": (None, [ctypes.POINTER(Packed)]),
+    "cfg_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(Params), ctypes.POINTER(ctypes.c_void_p)]),
+    "cfg_batch_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Packed), ctypes.c_uint32]),
+    "cfg_batch_run": (ctypes.c_int, [ctypes.c_void_p]),
+    "cfg_batch_job": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(Results)]),
+    "cfg_batch_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchStats)]),
+    "cfg_batch_job_device_input": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p),
+                                                  ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_void_p),
+                                                  ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_uint64)]),
+    "cfg_batch_tune": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchTuning)]),
+    "cfg_batch_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchTuning)]),
+    "cfg_batch_last_error_string": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "cfg_batch_destroy": (None, [ctypes.c_void_p]),
 }
 
 _lib = None
@@ -231,14 +255,7 @@ class Compactor:
     def fetch(self):
         r = Results()
         _check(self.lib, self.ctx, self.lib.cfg_fetch(self.ctx, ctypes.byref(r)), "cfg_fetch")
-        fasta = ctypes.string_at(r.fasta, r.counts.fasta_bytes) if r.counts.fasta_bytes else b""
-        text = ctypes.string_at(r.lmtig_text, r.counts.lmtig_bytes) if r.counts.lmtig_bytes else b""
-        lms = []
-        for i in range(r.counts.n_lmtig):
-            m = r.lmtigs[i]
-            lab = text[m.label_off:m.label_off + m.label_len].decode()
-            lms.append(LmtigRec((m.u[0], m.u[1]), (m.v[0], m.v[1]), lab, m.g, m.flags))
-        return r.counts, fasta, lms
+        return results_to_python(r)
 
     def states(self):
         d = StateDump()
@@ -250,6 +267,88 @@ class Compactor:
         d = RecordDump()
         _check(self.lib, self.ctx, self.lib.cfg_dump_records(self.ctx, ctypes.byref(d)), "cfg_dump_records")
         return [(d.records[i].pos, d.records[i].len, d.records[i].flags, d.records[i].g) for i in range(d.n)]
+
+
+def results_to_python(r: Results):
+    """(counts, FASTA bytes, [LmtigRec]) from a cfg_results view."""
+    fasta = ctypes.string_at(r.fasta, r.counts.fasta_bytes) if r.counts.fasta_bytes else b""
+    text = ctypes.string_at(r.lmtig_text, r.counts.lmtig_bytes) if r.counts.lmtig_bytes else b""
+    lms = []
+    for i in range(r.counts.n_lmtig):
+        m = r.lmtigs[i]
+        lab = text[m.label_off:m.label_off + m.label_len].decode()
+        lms.append(LmtigRec((m.u[0], m.u[1]), (m.v[0], m.v[1]), lab, m.g, m.flags))
+    return r.counts, fasta, lms
+
+
+class Batch:
+    """Batched form (cfg_batch): many jobs per device-planned, graph-captured run."""
+
+    def __init__(self, k: int, l: int = 20, cutoff: int = 1, graph_count: int = 16384, device: int = 0,
+                 table_load_pct: int = 0):
+        self.lib = load()
+        self.k = k
+        self.params = Params(k, l, cutoff, graph_count, 0, table_load_pct)
+        b = ctypes.c_void_p()
+        _check_b(self.lib, None, self.lib.cfg_batch_create(device, ctypes.byref(self.params), ctypes.byref(b)),
+                 "cfg_batch_create")
+        self.b = b
+        self.n_jobs = 0
+
+    def close(self):
+        if self.b:
+            self.lib.cfg_batch_destroy(self.b)
+            self.b = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def submit(self, jobs):
+        """jobs: list of PackedInput (one per genome / read set)."""
+        arr = (Packed * len(jobs))(*[j.p for j in jobs])
+        _check_b(self.lib, self.b, self.lib.cfg_batch_submit(self.b, arr, len(jobs)), "cfg_batch_submit")
+        self.n_jobs = len(jobs)
+
+    def run(self):
+        _check_b(self.lib, self.b, self.lib.cfg_batch_run(self.b), "cfg_batch_run")
+
+    def job_raw(self, j: int) -> Results:
+        r = Results()
+        _check_b(self.lib, self.b, self.lib.cfg_batch_job(self.b, j, ctypes.byref(r)), "cfg_batch_job")
+        return r
+
+    def job(self, j: int):
+        return results_to_python(self.job_raw(j))
+
+    def info(self) -> BatchStats:
+        s = BatchStats()
+        _check_b(self.lib, self.b, self.lib.cfg_batch_info(self.b, ctypes.byref(s)), "cfg_batch_info")
+        return s
+
+    def device_input(self, j: int):
+        w, n, fo, fl, nf = ctypes.c_void_p(), ctypes.c_uint64(), ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_uint64()
+        rc = self.lib.cfg_batch_job_device_input(self.b, j, ctypes.byref(w), ctypes.byref(n), ctypes.byref(fo),
+                                                 ctypes.byref(fl), ctypes.byref(nf))
+        _check_b(self.lib, self.b, rc, "cfg_batch_job_device_input")
+        return w.value, n.value, fo.value, fl.value, nf.value
+
+    def tune(self) -> BatchTuning:
+        t = BatchTuning()
+        _check_b(self.lib, self.b, self.lib.cfg_batch_tune(self.b, ctypes.byref(t)), "cfg_batch_tune")
+        return t
+
+    def set_tuning(self, local_div=4, cluster_threads=512, table_load_pct=100):
+        t = BatchTuning(local_div, cluster_threads, table_load_pct, 0, 0.0)
+        _check_b(self.lib, self.b, self.lib.cfg_batch_set_tuning(self.b, ctypes.byref(t)), "cfg_batch_set_tuning")
+
+
+def _check_b(lib, b, rc, what):
+    if rc != 0:
+        msg = lib.cfg_batch_last_error_string(b) if b else b""
+        raise CfgError(f"{what}: {ERRORS.get(rc, rc)} {msg.decode(errors='replace') if msg else ''}")
 
 
 def collate(k, lmtig_array, n, text_ptr):

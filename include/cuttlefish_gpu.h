@@ -196,6 +196,57 @@ void cfg_packed_free(cfg_packed* p);
 
 void cfg_destroy(cfg_ctx* ctx);
 
+/* ------------------------------------------------------------------------- */
+/* Batched form: many independent jobs (genomes, read sets) in one launch.
+ *
+ * cfg_batch_submit takes J jobs, each in the layout cfg_pack_records produces.
+ * cfg_batch_run partitions every job (job j's subgraph g is bucket j*G + g of
+ * one histogram), scatters, classifies every subgraph into a table shape, gives
+ * every job its output regions and runs one persistent kernel per table shape --
+ * all planned on the device and recorded once as a CUDA graph, which later runs
+ * of a batch of the same shape replay.  Each job's results (cfg_batch_job) are
+ * those of a plain run of that job alone: the same counts, trivial-unitig FASTA
+ * records and lm-tigs, as multisets.  Jobs that do not fit the preallocated
+ * arenas, or whose tables overflow, are redone alone through the plain driver.
+ * No state or record dumps (cfg_params.flags must be 0). */
+typedef struct cfg_batch cfg_batch;
+
+typedef struct cfg_batch_tuning {
+    uint32_t local_div;        /* one-CTA tables: threads = slots / local_div (64..512)   */
+    uint32_t cluster_threads;  /* threads per CTA of cluster tables (multiple of 32, <= 512) */
+    uint32_t table_load_pct;   /* as cfg_params.table_load_pct                            */
+    uint32_t reserved;
+    float    ms;               /* cfg_batch_tune: device time of the chosen shape          */
+} cfg_batch_tuning;
+
+typedef struct cfg_batch_stats {
+    uint64_t n_jobs, n_redone;
+    uint64_t n_bases, n_records, n_vertices, n_lmtig, fasta_bytes, lmtig_bytes;
+    uint64_t kernels_per_run, graph_launches;
+    float    device_ms;        /* the graph launch, CUDA events on the batch's stream */
+    float    redo_ms;          /* host wall time of jobs redone alone */
+    cfg_batch_tuning tuning;
+} cfg_batch_stats;
+
+int cfg_batch_create(int device, const cfg_params* params, cfg_batch** out);
+/* Copies J jobs to the device (each starts on a 32-base word boundary). */
+int cfg_batch_submit(cfg_batch* b, const cfg_packed* jobs, uint32_t n_jobs);
+int cfg_batch_run(cfg_batch* b);
+/* One job's results, copied to host memory owned by the batch; valid until the
+ * next cfg_batch_job / cfg_batch_run / cfg_batch_destroy. */
+int cfg_batch_job(cfg_batch* b, uint32_t job, cfg_results* out);
+int cfg_batch_info(cfg_batch* b, cfg_batch_stats* out);
+/* Device copy of one job's input in cfg_submit_packed_device's layout (for
+ * running that job through a plain context without another copy). */
+int cfg_batch_job_device_input(cfg_batch* b, uint32_t job, const uint64_t** d_words, uint64_t* n_bases,
+                               const uint64_t** d_frag_off, const uint32_t** d_frag_len, uint64_t* n_frags);
+/* Autotuner: times every candidate launch shape (threads per table class, table
+ * load factor) on the submitted batch and keeps the fastest. */
+int cfg_batch_tune(cfg_batch* b, cfg_batch_tuning* out);
+int cfg_batch_set_tuning(cfg_batch* b, const cfg_batch_tuning* t);
+const char* cfg_batch_last_error_string(cfg_batch* b);
+void cfg_batch_destroy(cfg_batch* b);
+
 /* No counterpart in the reference.  For callers that must not allocate memory:
  * code recording into a CUDA graph whose stream capture someone else owns,
  * plugins whose host framework owns every byte of device memory, real-time

@@ -70,3 +70,13 @@ def test_pack_matches_fragment_rule():
             at += len(f)
         assert p.n_bases == at
         p.close()
+
+
+def test_batch_create_rejects_bad_params():
+    lib = cfgpu.load()
+    b = ctypes.c_void_p()
+    for k, l, c, G, flags in ((30, 20, 1, 16384, 0), (31, 20, 1, 1000, 0), (31, 20, 0, 16384, 0),
+                              (31, 20, 1, 16384, cfgpu.CFG_FLAG_DUMP_STATES)):
+        p = cfgpu.Params(k, l, c, G, flags, 0)
+        assert lib.cfg_batch_create(0, ctypes.byref(p), ctypes.byref(b)) == 1
+    assert lib.cfg_batch_run(None) == 1
