@@ -221,7 +221,9 @@ int run_subgraphs(cfg_ctx* c, const std::vector<uint32_t>& inst_h) {
     for (uint32_t g = 0; g < G; ++g)
         if (inst_h[g]) want[g] = std::max<uint64_t>(64, ((uint64_t)inst_h[g] * load * 2 + 99) / 100);
     uint64_t fasta_need = c->n_bases + (c->n_records + 1024) * 8 + (1u << 20);
-    uint64_t lm_text_need = c->n_bases / 2 + (c->n_records + 1024) * (c->p.k + 2);
+    // lm-tig labels: at most every k-mer instance once plus k-1 bases per lm-tig, and the
+    // records' lengths sum to at most n_bases + k per record
+    uint64_t lm_text_need = c->n_bases + (c->n_records + 1024) * (c->p.k + 1);
     uint64_t lm_need = c->n_records + 1024;
     std::vector<uint32_t> todo;
     for (uint32_t g = 0; g < G; ++g) if (inst_h[g]) todo.push_back(g);

@@ -140,7 +140,10 @@ __global__ void __launch_bounds__(256) k_job_regions(const uint32_t* __restrict_
     // trivial unitigs are rare when the job has many subgraphs, and make up all of
     // its output when it has few
     const uint64_t fc = (caps.fasta_full ? N + 8 * R : N / 8) + 4096;
-    const uint64_t tc = N / 2 + R * (caps.k + 2) + 4096, lc = R + 64;
+    // lm-tig labels: the records' lengths sum to at most N + k R; every lm-tig adds k-1
+    // bases of overlap; lm-tigs number about one per record
+    const uint64_t lc = R + R / 16 + 64;
+    const uint64_t tc = N + R * (caps.k + 1) + (lc - R) * (caps.k - 1) + 4096;
     const unsigned long long fo = atomicAdd(&bw->fasta_cur, (unsigned long long)fc);
     const unsigned long long to = atomicAdd(&bw->lm_text_cur, (unsigned long long)tc);
     const unsigned long long lo = atomicAdd(&bw->lm_cur, (unsigned long long)lc);
@@ -150,6 +153,29 @@ __global__ void __launch_bounds__(256) k_job_regions(const uint32_t* __restrict_
         J.fasta_off = J.lm_text_off = J.lm_off = 0; J.fasta_cap = J.lm_text_cap = J.lm_cap = 0;
         J.err |= DERR_NO_ROOM;
     }
+}
+
+// One CTA per job: its subgraphs' counters summed into the job's.
+__global__ void __launch_bounds__(256) k_job_finalize(const uint32_t* __restrict__ bucket_cnt, uint32_t g_shift,
+                                                      JobOut* jobs) {
+    __shared__ unsigned long long part[8][5];
+    const uint32_t j = blockIdx.x, G = 1u << g_shift;
+    const uint64_t b0 = (uint64_t)j << g_shift;
+    unsigned long long v[5] = {0, 0, 0, 0, 0};
+    for (uint32_t i = threadIdx.x; i < G; i += blockDim.x)
+        for (int c = 0; c < 5; ++c) v[c] += bucket_cnt[5 * (b0 + i) + c];
+    for (int c = 0; c < 5; ++c) {
+        for (int d = 16; d; d >>= 1) v[c] += __shfl_down_sync(0xffffffffu, v[c], d);
+        if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5][c] = v[c];
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    unsigned long long t[5] = {0, 0, 0, 0, 0};
+    for (uint32_t w = 0; w < (blockDim.x >> 5); ++w)
+        for (int c = 0; c < 5; ++c) t[c] += part[w][c];
+    JobOut& J = jobs[j];
+    J.vertices = t[0]; J.isolated = t[1]; J.phantom = t[2]; J.trivial = t[3]; J.icc = t[4];
+    J.lmtig = J.lm_used;
 }
 
 uint64_t wy_seed0() {
@@ -180,7 +206,7 @@ struct cfg_batch {
 
     // pipeline
     DevBuf flat, hist, bw, bucket_off, inst, fill, partials, recs, list, tab_off, tab_cap, arena, jobs,
-        fasta, lm_text, lm, retry, counters;
+        fasta, lm_text, lm, retry, counters, bucket_cnt;
     uint64_t rec_cap = 0, arena_slots = 0, fasta_cap = 0, lm_text_cap = 0, lm_cap = 0;
     cudaGraphExec_t exec = nullptr;
     std::vector<Shape> shapes;
@@ -269,8 +295,9 @@ int ensure_buffers(cfg_batch* b) {
     for (uint64_t x : b->nb) act_bases += x;
     const uint64_t r_out = act_bases * 2 / (w + 1) * 23 / 20 + 1024 * (uint64_t)b->n_jobs;
     b->fasta_cap = (fasta_full ? act_bases + 8 * r_out : act_bases / 8) + 4096ull * b->n_jobs + (1u << 20);
-    b->lm_text_cap = act_bases / 2 + r_out * (b->p.k + 2) + 4096ull * b->n_jobs;
-    b->lm_cap = r_out + 64ull * b->n_jobs;
+    b->lm_cap = r_out + r_out / 16 + 64ull * b->n_jobs;
+    b->lm_text_cap = act_bases + r_out * (b->p.k + 1) + (r_out / 16 + 64ull * b->n_jobs) * (b->p.k - 1) +
+                     4096ull * b->n_jobs;
     const uint32_t np = (uint32_t)((NB + 8191) / 8192);
     if (!b->flat.ensure(8 * b->rec_cap, false) || !b->recs.ensure(8 * b->rec_cap, false) || !b->hist.ensure(8 * NB) ||
         !b->bw.ensure(sizeof(BatchWords)) || !b->bucket_off.ensure(4 * (NB + 1)) || !b->inst.ensure(4 * NB) ||
@@ -279,7 +306,7 @@ int ensure_buffers(cfg_batch* b) {
         !b->arena.ensure(b->arena_slots * slot_bytes(b->words)) || !b->jobs.ensure(sizeof(JobOut) * b->n_jobs) ||
         !b->fasta.ensure(b->fasta_cap, false) || !b->lm_text.ensure(b->lm_text_cap, false) ||
         !b->lm.ensure(sizeof(LmtigOut) * b->lm_cap, false) ||
-        !b->retry.ensure(4 * NB) || !b->counters.ensure(sizeof(Counters)))
+        !b->retry.ensure(4 * NB) || !b->counters.ensure(sizeof(Counters)) || !b->bucket_cnt.ensure(20 * NB))
         return bfail(b, CFG_ERR_OOM, "batch buffers");
     return CFG_OK;
 }
@@ -293,6 +320,7 @@ int enqueue(cfg_batch* b) {
     BCK(cudaMemsetAsync(b->bw.p, 0, sizeof(BatchWords), s));
     BCK(cudaMemsetAsync(b->jobs.p, 0, sizeof(JobOut) * b->n_jobs, s));
     BCK(cudaMemsetAsync(b->counters.p, 0, sizeof(Counters), s));
+    BCK(cudaMemsetAsync(b->bucket_cnt.p, 0, 20 * NB, s));
     uint64_t launches = 0;
 
     PartitionArgs pa{};
@@ -344,12 +372,16 @@ int enqueue(cfg_batch* b) {
     a.fasta = b->fasta.as<char>(); a.lm_text = b->lm_text.as<char>(); a.lm = b->lm.as<LmtigOut>();
     a.retry = b->retry.as<uint32_t>(); a.cnt = b->counters.as<Counters>(); a.err = &bw->err;
     a.jobs = b->jobs.as<JobOut>(); a.g_shift = b->g_shift; a.record_clocks = 0;
+    a.bucket_cnt = b->bucket_cnt.as<uint32_t>();
     for (const Shape& sh : b->shapes) {
         a.list_base = &bw->off[sh.cls];
         a.list_n = &bw->count[sh.cls];
         BCK(launch_subgraphs_persistent(a, b->words, sh.cluster, sh.threads, sh.per, sh.grid, s));
         ++launches;
     }
+    k_job_finalize<<<b->n_jobs, 256, 0, s>>>(b->bucket_cnt.as<uint32_t>(), b->g_shift, b->jobs.as<JobOut>());
+    ++launches;
+    BCK(cudaGetLastError());
     b->launches_per_run = launches;
     return CFG_OK;
 }
@@ -680,7 +712,8 @@ void cfg_batch_destroy(cfg_batch* b) {
     drop_graph(b);
     DevBuf* bufs[] = {&b->packed, &b->frag_off, &b->frag_off_rel, &b->frag_len, &b->frag_gbase, &b->job_pos, &b->job_nbases,
                       &b->flat, &b->hist, &b->bw, &b->bucket_off, &b->inst, &b->fill, &b->partials, &b->recs, &b->list,
-                      &b->tab_off, &b->tab_cap, &b->arena, &b->jobs, &b->fasta, &b->lm_text, &b->lm, &b->retry, &b->counters};
+                      &b->tab_off, &b->tab_cap, &b->arena, &b->jobs, &b->fasta, &b->lm_text, &b->lm, &b->retry, &b->counters,
+                      &b->bucket_cnt};
     for (DevBuf* x : bufs) x->release();
     b->h_fasta.release(); b->h_text.release(); b->h_lm.release();
     if (b->plain) cfg_destroy(b->plain);

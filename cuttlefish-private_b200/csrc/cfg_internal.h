@@ -121,6 +121,9 @@ struct SubgraphArgs {
     JobOut* jobs;
     uint32_t g_shift;
     uint32_t record_clocks;      // accumulate per-phase SM cycles into cnt->phase_cycles
+    // batch: per-subgraph vertices, isolated, phantom, trivial, icc (5 words each),
+    // summed per job after the run; nullptr: counters go to the sink
+    uint32_t* bucket_cnt;
 };
 
 // bytes per table slot: k-mer (8 per word) + state word (8) + meta (4) + work-list entry (4)

@@ -240,10 +240,76 @@ __device__ __forceinline__ void sink_for(const SubgraphArgs& a, uint32_t b, Sink
 }
 
 struct Block {   // per-CTA shared bookkeeping (in CLUSTER mode the flags of rank 0 are the cluster's)
-    uint32_t inserted, overflow, wl_n, pad;
+    uint32_t inserted, overflow, wl_n, scan_total;
     unsigned long long vertices, isolated, phantom, trivial, icc, lmtig;
     Sink sk;
+    uint32_t wsum[16];   // per-warp partial sums of a block scan (<= 512 threads)
 };
+
+constexpr uint32_t FULL = 0xffffffffu;
+
+// Exclusive scan of one value per thread over the CTA; B.scan_total gets the sum.
+// Every thread of the CTA must call it.
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, Block& B) {
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(FULL, x, d);
+        if (lane >= (uint32_t)d) x += y;
+    }
+    if (lane == 31) B.wsum[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t w = lane < nw ? B.wsum[lane] : 0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL, w, d);
+            if (lane >= (uint32_t)d) w += y;
+        }
+        if (lane < nw) B.wsum[lane] = w;
+        if (lane == nw - 1) B.scan_total = w;
+    }
+    __syncthreads();
+    const uint32_t before = wid ? B.wsum[wid - 1] : 0;
+    __syncthreads();
+    return before + x - v;
+}
+
+// Output space reserved for one lane: FASTA bytes, lm-tig records, lm-tig label bytes.
+struct Res { unsigned long long fa, lm_idx, lm_off; };
+
+// One atomic per warp and kind instead of one per unitig.  Every lane of the warp
+// must call it (the walk loops are uniform over the CTA for that reason).
+__device__ __forceinline__ Res reserve_warp(const Sink& sk, unsigned long long fa, uint32_t nlm, unsigned long long lmb) {
+    const uint32_t lane = threadIdx.x & 31;
+    unsigned long long a = fa, c = lmb;
+    uint32_t b = nlm;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const unsigned long long x = __shfl_up_sync(FULL, a, d), z = __shfl_up_sync(FULL, c, d);
+        const uint32_t y = __shfl_up_sync(FULL, b, d);
+        if (lane >= (uint32_t)d) { a += x; b += y; c += z; }
+    }
+    const unsigned long long ta = __shfl_sync(FULL, a, 31), tc = __shfl_sync(FULL, c, 31);
+    const uint32_t tb = __shfl_sync(FULL, b, 31);
+    unsigned long long ba = 0, bb = 0, bc = 0;
+    if (lane == 0) {
+        if (ta) ba = atomicAdd(sk.fasta_cur, ta);
+        if (tb) bb = atomicAdd(sk.lm_cur, (unsigned long long)tb);
+        if (tc) bc = atomicAdd(sk.lm_text_cur, tc);
+    }
+    ba = __shfl_sync(FULL, ba, 0); bb = __shfl_sync(FULL, bb, 0); bc = __shfl_sync(FULL, bc, 0);
+    return Res{ba + a - fa, bb + b - nlm, bc + c - lmb};
+}
+
+// The L bases of a reserved FASTA record ">0\n...\n" at offset o, or nullptr past the arena.
+__device__ __forceinline__ char* fasta_at(const Sink& sk, unsigned long long o, uint32_t L) {
+    if (o + L + 4 > sk.fasta_cap) { atomicOr(sk.oflow, DERR_OUT_OVERFLOW); return nullptr; }
+    char* p = sk.fasta + o;
+    p[0] = '>'; p[1] = '0'; p[2] = '\n'; p[3 + L] = '\n';
+    return p + 3;
+}
 
 __device__ __forceinline__ uint32_t lane_lt() { uint32_t m; asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m)); return m; }
 
@@ -319,13 +385,6 @@ __device__ __forceinline__ bool step(const Tab<W, MODE>& T, const KOps<W>& ops, 
     else return step_outline(T, ops, fth, v, side, s_in);
 }
 
-__device__ __forceinline__ char* reserve_fasta(const Sink& sk, uint32_t L) {
-    const unsigned long long off = atomicAdd(sk.fasta_cur, (unsigned long long)(L + 4));
-    if (off + L + 4 > sk.fasta_cap) { atomicOr(sk.oflow, DERR_OUT_OVERFLOW); return nullptr; }
-    char* p = sk.fasta + off;
-    p[0] = '>'; p[1] = '0'; p[2] = '\n'; p[3 + L] = '\n';
-    return p + 3;
-}
 
 // Writes the label of the path of n vertices that starts at v (in walk direction).
 template <int W, int MODE>
@@ -347,9 +406,10 @@ __device__ void write_path(const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t f
     }
 }
 
+// A one-k-mer cycle (a self-looped homopolymer seeded on its own) at reserved FASTA offset o.
 template <int W, int MODE>
-__device__ void emit_kmer_cycle(const SubgraphArgs& a, const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t s, Block& B) {
-    char* p = reserve_fasta(B.sk, ops.k);
+__device__ void write_kmer_cycle(const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t s, Block& B, unsigned long long o) {
+    char* p = fasta_at(B.sk, o, ops.k);
     if (p) { const Kmer<W> x = T.key(s); for (uint32_t i = 0; i < ops.k; ++i) p[i] = "ACGT"[ops.base(x, i)]; }
     atomicAdd(&B.trivial, 1ull); atomicAdd(&B.icc, 1ull);
 }
@@ -391,16 +451,20 @@ struct RecBases {
     }
 };
 
+// A path of n vertices from v0 (leaving through side0) to vlast, written into space
+// reserved by reserve_warp: a trivial maximal unitig at FASTA offset fo, or an lm-tig
+// (lm: one end exits the subgraph) as record idx with its label at offset off.
 template <int W, int MODE>
-__device__ void emit_path(const SubgraphArgs& a, const Tab<W, MODE>& T, const KOps<W>& ops, const DV<W>& v0,
-                          int side0, uint32_t n, const DV<W>& vlast, EndInfo st, EndInfo en, bool seed_canon, Block& B) {
+__device__ void write_emitted_path(const SubgraphArgs& a, const Tab<W, MODE>& T, const KOps<W>& ops, const DV<W>& v0,
+                                   int side0, uint32_t n, const DV<W>& vlast, EndInfo st, EndInfo en, bool seed_canon,
+                                   Block& B, bool lm, unsigned long long fo, unsigned long long idx,
+                                   unsigned long long off) {
     const uint32_t k = ops.k, fth = a.fth;
     const uint32_t L = n + k - 1;
-    const bool lm = st.term == T_EXIT || en.term == T_EXIT;
     if (!lm) {
         // trivial maximal unitig in canonical orientation (Maximal_Unitig_Scratch::finalize, :200-222)
         const bool rev = vlast.r < v0.d;   // rc(last k-mer) < first k-mer
-        char* p = reserve_fasta(B.sk, L);
+        char* p = fasta_at(B.sk, fo, L);
         write_path(T, ops, fth, v0, side0, n, p, rev, true);
         atomicAdd(&B.trivial, 1ull);
         return;
@@ -411,8 +475,6 @@ __device__ void emit_path(const SubgraphArgs& a, const Tab<W, MODE>& T, const KO
     const bool u_first_canon = rev ? !en.canon : st.canon;     // label's first k-mer canonical?
     const bool v_last_canon = rev ? !st.canon : en.canon;      // label's last k-mer canonical?
     const Sink& sk = B.sk;
-    const unsigned long long idx = atomicAdd(sk.lm_cur, 1ull);
-    const unsigned long long off = atomicAdd(sk.lm_text_cur, (unsigned long long)L);
     atomicAdd(&B.lmtig, 1ull);
     const bool fits = idx < sk.lm_cap && off + L <= sk.lm_text_cap;
     if (!fits) atomicOr(sk.oflow, DERR_OUT_OVERFLOW);
@@ -457,39 +519,88 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
     // ---------------- build ----------------
     const uint32_t limit = (uint32_t)(((uint64_t)per * a.load_limit_pct) / 100);
     const uint32_t r0 = a.bucket_off[g], r1 = a.bucket_off[g + 1];
-    for (uint32_t r = r0 + rank * nt + tid; r < r1; r += nranks * nt) {
-        if (*(volatile uint32_t*)&B.overflow) break;
-        const uint64_t rec = a.recs[r];
-        const uint32_t pos = rec_pos(rec), len = rec_len(rec), ld = rec_ld(rec), rd = rec_rd(rec);
-        const RecBases rb(a.packed, pos, len);   // the whole record in registers (<= 128 bases)
-        Kmer<W> fw = rb.first_kmer<W>(k);
-        Kmer<W> rc = ops.rc(fw);
-        Kmer<W> pred_can = fw;
-        for (uint32_t idx = 0;; ++idx) {
-            const bool canon = fw < rc;
-            const Kmer<W> can = canon ? fw : rc;
-            const uint32_t pred = idx == 0 ? BASE_E : rb.base(idx - 1);
-            const uint32_t succ = idx + k == len ? BASE_E : rb.base(idx + k);
-            uint32_t front = canon ? pred : compb(succ);
-            uint32_t back = canon ? succ : compb(pred);
-            if (idx > 0 && can == pred_can) { if (canon) front = BASE_E; else back = BASE_E; }
-            uint32_t owner, h;
-            T.place(can, owner, h);
-            bool fresh;
-            const uint32_t s = T.find_or_insert(can, owner, h, fresh);
-            if (s == NONE) { atomicOr(&B.overflow, 1u); break; }
-            // fresh vertices are counted per inserting CTA (records, hence inserts, are spread
-            // evenly, so one CTA's count stands for one sub-table's load)
-            if (fresh && atomicAdd(&B.inserted, 1u) + 1 > limit) { atomicOr(&B.overflow, 1u); break; }
-            T.update_state(s, front, back, pos + idx);
-            uint32_t disc = 0;
-            if (idx == 0 && ld) disc |= canon ? M_DISC_F : M_DISC_B;            // entrance side
-            if (idx + k == len && rd) disc |= canon ? M_DISC_B : M_DISC_F;      // exit side
-            if (disc) T.mark_disc(s, disc);
-            if (idx + k == len) break;
-            pred_can = can;
-            ops.push_back(fw, succ);
-            ops.push_front(rc, 3 - succ);
+    // HT_Router::update of one k-mer instance at stream position p (idx-th of its record):
+    // edges from its predecessor / successor bases, the self-loop rule against the
+    // previous k-mer's canonical form, and the record's entrance / exit marks.
+    auto insert = [&](const Kmer<W>& fw, const Kmer<W>& rc, const Kmer<W>& pred_can, uint32_t idx, uint32_t pred,
+                      uint32_t succ, uint32_t p, bool l_mark, bool r_mark) -> bool {
+        const bool canon = fw < rc;
+        const Kmer<W> can = canon ? fw : rc;
+        uint32_t front = canon ? pred : compb(succ);
+        uint32_t back = canon ? succ : compb(pred);
+        if (idx > 0 && can == pred_can) { if (canon) front = BASE_E; else back = BASE_E; }
+        uint32_t owner, h;
+        T.place(can, owner, h);
+        bool fresh;
+        const uint32_t s = T.find_or_insert(can, owner, h, fresh);
+        if (s == NONE) { atomicOr(&B.overflow, 1u); return false; }
+        // fresh vertices are counted per inserting CTA (records, hence inserts, are spread
+        // evenly, so one CTA's count stands for one sub-table's load)
+        if (fresh && atomicAdd(&B.inserted, 1u) + 1 > limit) { atomicOr(&B.overflow, 1u); return false; }
+        T.update_state(s, front, back, p);
+        uint32_t disc = 0;
+        if (l_mark) disc |= canon ? M_DISC_F : M_DISC_B;      // entrance side
+        if (r_mark) disc |= canon ? M_DISC_B : M_DISC_F;      // exit side
+        if (disc) T.mark_disc(s, disc);
+        return true;
+    };
+    bool by_instance = false;
+    if constexpr (MODE == LOCAL) by_instance = r1 - r0 <= per;
+    if (by_instance) {
+        // one thread per k-mer instance: the records' instance counts, prefix-summed into
+        // the (still unused) work list, map instances to records
+        const uint32_t nrec = r1 - r0;
+        const uint32_t chunk = (nrec + nt - 1) / nt;
+        const uint32_t c0 = min(nrec, tid * chunk), c1 = min(nrec, c0 + chunk);
+        uint32_t sum = 0;
+        for (uint32_t j = c0; j < c1; ++j) sum += rec_len(a.recs[r0 + j]) - k + 1;
+        uint32_t run = block_excl_scan(sum, B);
+        for (uint32_t j = c0; j < c1; ++j) { wl[j] = run; run += rec_len(a.recs[r0 + j]) - k + 1; }
+        __syncthreads();
+        const uint32_t total = B.scan_total;
+        for (uint32_t t = tid; t < total; t += nt) {
+            if (*(volatile uint32_t*)&B.overflow) break;
+            uint32_t lo = 0, hi = nrec;   // the record holding instance t: last j with wl[j] <= t
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (wl[mid] <= t) lo = mid; else hi = mid;
+            }
+            const uint64_t rec = a.recs[r0 + lo];
+            const uint32_t pos = rec_pos(rec), len = rec_len(rec);
+            const uint32_t idx = t - wl[lo];
+            const uint64_t p = (uint64_t)pos + idx;
+            const Kmer<W> fw = ops.load(a.packed, p);
+            const Kmer<W> rc = ops.rc(fw);
+            const uint32_t pred = idx == 0 ? BASE_E : base_at(a.packed, p - 1);
+            const uint32_t succ = idx + k == len ? BASE_E : base_at(a.packed, p + k);
+            Kmer<W> pc = fw;
+            if (idx > 0) {
+                Kmer<W> pf = fw;
+                ops.push_front(pf, pred);
+                const Kmer<W> pr = ops.rc(pf);
+                pc = pf < pr ? pf : pr;
+            }
+            if (!insert(fw, rc, pc, idx, pred, succ, (uint32_t)p, idx == 0 && rec_ld(rec), idx + k == len && rec_rd(rec)))
+                break;
+        }
+    } else {
+        for (uint32_t r = r0 + rank * nt + tid; r < r1; r += nranks * nt) {
+            if (*(volatile uint32_t*)&B.overflow) break;
+            const uint64_t rec = a.recs[r];
+            const uint32_t pos = rec_pos(rec), len = rec_len(rec), ld = rec_ld(rec), rd = rec_rd(rec);
+            const RecBases rb(a.packed, pos, len);   // the whole record in registers (<= 128 bases)
+            Kmer<W> fw = rb.first_kmer<W>(k);
+            Kmer<W> rc = ops.rc(fw);
+            Kmer<W> pred_can = fw;
+            for (uint32_t idx = 0;; ++idx) {
+                const uint32_t pred = idx == 0 ? BASE_E : rb.base(idx - 1);
+                const uint32_t succ = idx + k == len ? BASE_E : rb.base(idx + k);
+                if (!insert(fw, rc, pred_can, idx, pred, succ, pos + idx, idx == 0 && ld, idx + k == len && rd)) break;
+                if (idx + k == len) break;
+                pred_can = fw < rc ? fw : rc;
+                ops.push_back(fw, succ);
+                ops.push_front(rc, 3 - succ);
+            }
         }
     }
     // one CTA's overflow is the whole cluster's
@@ -560,74 +671,91 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         return !(m & M_ISO) && (term_of(m, FRONT) != T_OK || term_of(m, BACK) != T_OK);
     });
     __syncthreads();
-    for (uint32_t i = tid, nw = B.wl_n; i < nw; i += nt) {
-        const uint32_t ls = wl[i];
-        const uint32_t s = base_slot + ls;
-        const uint32_t meta = lmeta[ls];
-        const bool okf = term_of(meta, FRONT) == T_OK, okb = term_of(meta, BACK) == T_OK;
-        if (!okf && !okb) {         // one-vertex path
-            if (meta & M_Q) emit_kmer_cycle(a, T, ops, s, B);
-            else {
-                const DV<W> v = dv_at(T, ops, s, BACK);
-                const EndInfo st{s, term_of(meta, FRONT), true}, en{s, term_of(meta, BACK), true};
-                emit_path(a, T, ops, v, BACK, 1, v, st, en, true, B);
+    const uint32_t nw2 = B.wl_n;
+    for (uint32_t base = 0; base < nw2; base += nt) {   // uniform over the CTA: warps reserve output together
+        const uint32_t i = base + tid;
+        // what this lane emits: one-k-mer cycles at s and/or e, and one path vs..ve
+        bool kc0 = false, kc1 = false, mark0 = false, mark1 = false, path = false, lm = false;
+        uint32_t s = 0, e = 0, n2 = 0;
+        DV<W> vs{}, ve{};
+        int sd0 = BACK;
+        EndInfo st{0, 0, true}, en{0, 0, true};
+        bool best_canon = true;
+        if (i < nw2) {
+            const uint32_t ls = wl[i];
+            s = base_slot + ls;
+            e = s;
+            const uint32_t meta = lmeta[ls];
+            const bool okf = term_of(meta, FRONT) == T_OK, okb = term_of(meta, BACK) == T_OK;
+            if (!okf && !okb) {         // one-vertex path
+                if (meta & M_Q) kc0 = true;
+                else {
+                    vs = dv_at(T, ops, s, BACK); ve = vs; sd0 = BACK; n2 = 1; path = true;
+                    st = EndInfo{s, term_of(meta, FRONT), true}; en = EndInfo{s, term_of(meta, BACK), true};
+                }
+                lmeta[ls] = lmeta[ls] | M_VISITED;
+            } else {
+                const int side0 = okf ? FRONT : BACK;   // walk through the linked side
+                const uint32_t ins0 = st_ins(lst[ls]);
+                const DV<W> v0 = dv_at(T, ops, s, side0);
+                // pass 1: the other end, first-occurrence minima
+                DV<W> v = v0; int side = side0;
+                uint32_t n = 1;
+                uint32_t v1_slot = s; int v1_side = side0;     // second vertex
+                uint32_t vp_slot = s; int vp_side = side0;     // vertex before the current one
+                uint32_t m_int = 0xffffffffu; bool m_int_canon = true;
+                uint32_t cur_meta = meta;
+                bool ok = true;
+                while (term_of(cur_meta, side) == T_OK) {
+                    if (n > 1) {   // v is interior
+                        const uint32_t ic = st_ins(T.ld_st(v.slot));
+                        if (ic < m_int) { m_int = ic; m_int_canon = side == BACK; }
+                    }
+                    vp_slot = v.slot; vp_side = side;
+                    int s_in;
+                    if (!step(T, ops, fth, v, side, s_in)) { atomicOr(a.err, DERR_MISSING_KEY); ok = false; break; }
+                    side = 1 - s_in;
+                    cur_meta = T.ld_meta(v.slot);
+                    if (n == 1) { v1_slot = v.slot; v1_side = side; }
+                    if (++n > T.per * T.nranks + 1) { atomicOr(a.err, DERR_WALK_LIMIT); ok = false; break; }
+                }
+                if (ok && v.slot >= s) {   // the end with the smaller slot emits
+                    e = v.slot;
+                    const int e_side = side;   // the walk stops at e's side e_side
+                    const uint32_t meta_e = cur_meta;
+                    const uint32_t ins1 = st_ins(T.ld_st(e));
+                    const bool q0 = meta & M_Q, q1 = meta_e & M_Q;
+                    uint32_t m = m_int;
+                    if (!q0 && ins0 < m) m = ins0;
+                    if (!q1 && ins1 < m) m = ins1;
+                    const bool fake0 = q0 && ins0 < m, fake1 = q1 && ins1 < m;
+                    kc0 = mark0 = fake0; kc1 = mark1 = fake1;
+                    n2 = n - fake0 - fake1;
+                    if (n2 > 0) {
+                        path = true;
+                        if (!fake0) { st = EndInfo{s, term_of(meta, 1 - side0), side0 == BACK}; vs = v0; sd0 = side0; }
+                        else { st = EndInfo{v1_slot, T_CROSSED, v1_side == BACK}; vs = dv_at(T, ops, v1_slot, v1_side); sd0 = v1_side; }
+                        if (!fake1) { en = EndInfo{e, term_of(meta_e, e_side), e_side == BACK}; ve = v; }
+                        else { en = EndInfo{vp_slot, T_CROSSED, vp_side == BACK}; ve = dv_at(T, ops, vp_slot, vp_side); }
+                        // first-inserted vertex of the emitted path and its orientation along the walk
+                        uint32_t best = m_int; best_canon = m_int_canon;
+                        if (!fake0 && ins0 < best) { best = ins0; best_canon = side0 == BACK; }
+                        if (!fake1 && ins1 < best) { best = ins1; best_canon = e_side == BACK; }
+                    }
+                }
             }
-            lmeta[ls] = lmeta[ls] | M_VISITED;
-            continue;
+            if (path) lm = st.term == T_EXIT || en.term == T_EXIT;
         }
-        const int side0 = okf ? FRONT : BACK;   // walk through the linked side
-        const uint32_t ins0 = st_ins(lst[ls]);
-        const DV<W> v0 = dv_at(T, ops, s, side0);
-        // pass 1: the other end, first-occurrence minima
-        DV<W> v = v0; int side = side0;
-        uint32_t n = 1;
-        uint32_t v1_slot = s; int v1_side = side0;     // second vertex
-        uint32_t vp_slot = s; int vp_side = side0;     // vertex before the current one
-        uint32_t m_int = 0xffffffffu; bool m_int_canon = true;
-        uint32_t cur_meta = meta;
-        bool ok = true;
-        while (term_of(cur_meta, side) == T_OK) {
-            if (n > 1) {   // v is interior
-                const uint32_t ic = st_ins(T.ld_st(v.slot));
-                if (ic < m_int) { m_int = ic; m_int_canon = side == BACK; }
-            }
-            vp_slot = v.slot; vp_side = side;
-            int s_in;
-            if (!step(T, ops, fth, v, side, s_in)) { atomicOr(a.err, DERR_MISSING_KEY); ok = false; break; }
-            side = 1 - s_in;
-            cur_meta = T.ld_meta(v.slot);
-            if (n == 1) { v1_slot = v.slot; v1_side = side; }
-            if (++n > T.per * T.nranks + 1) { atomicOr(a.err, DERR_WALK_LIMIT); ok = false; break; }
-        }
-        if (!ok) continue;
-        const uint32_t e = v.slot; const int e_side = side;   // other end; the walk stops at its side e_side
-        if (e < s) continue;                                   // the smaller end emits
-        const uint32_t meta_e = cur_meta;
-        const uint32_t ins1 = st_ins(T.ld_st(e));
-        const bool q0 = meta & M_Q, q1 = meta_e & M_Q;
-        uint32_t m = m_int;
-        if (!q0 && ins0 < m) m = ins0;
-        if (!q1 && ins1 < m) m = ins1;
-        const bool fake0 = q0 && ins0 < m, fake1 = q1 && ins1 < m;
-        if (fake0) emit_kmer_cycle(a, T, ops, s, B);
-        if (fake1) emit_kmer_cycle(a, T, ops, e, B);
-        const uint32_t n2 = n - fake0 - fake1;
-        if (n2 > 0) {
-            EndInfo st, en;
-            DV<W> vs; int sd0;
-            if (!fake0) { st = EndInfo{s, term_of(meta, 1 - side0), side0 == BACK}; vs = v0; sd0 = side0; }
-            else { st = EndInfo{v1_slot, T_CROSSED, v1_side == BACK}; vs = dv_at(T, ops, v1_slot, v1_side); sd0 = v1_side; }
-            DV<W> ve;
-            if (!fake1) { en = EndInfo{e, term_of(meta_e, e_side), e_side == BACK}; ve = v; }
-            else { en = EndInfo{vp_slot, T_CROSSED, vp_side == BACK}; ve = dv_at(T, ops, vp_slot, vp_side); }
-            // first-inserted vertex of the emitted path and its orientation along the walk
-            uint32_t best = m_int; bool best_canon = m_int_canon;
-            if (!fake0 && ins0 < best) { best = ins0; best_canon = side0 == BACK; }
-            if (!fake1 && ins1 < best) { best = ins1; best_canon = e_side == BACK; }
-            emit_path(a, T, ops, vs, sd0, n2, ve, st, en, best_canon, B);
-        }
-        if (fake0) T.or_meta(s, M_VISITED);
-        if (fake1) T.or_meta(e, M_VISITED);
+        const uint32_t L = path ? n2 + k - 1 : 0;
+        __syncwarp();
+        const Res r = reserve_warp(B.sk, (kc0 ? k + 4 : 0) + (kc1 ? k + 4 : 0) + (path && !lm ? L + 4 : 0),
+                                   path && lm ? 1u : 0u, path && lm ? L : 0u);
+        unsigned long long fo = r.fa;
+        if (kc0) { write_kmer_cycle(T, ops, s, B, fo); fo += k + 4; }
+        if (kc1) { write_kmer_cycle(T, ops, e, B, fo); fo += k + 4; }
+        if (path) write_emitted_path(a, T, ops, vs, sd0, n2, ve, st, en, best_canon, B, lm, fo, r.lm_idx, r.lm_off);
+        if (mark0) T.or_meta(s, M_VISITED);
+        if (mark1) T.or_meta(e, M_VISITED);
     }
     tsync<MODE>();
 
@@ -639,26 +767,38 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         return !local_empty<W>(lkeys, ls) && !(lmeta[ls] & (M_ISO | M_VISITED));
     });
     __syncthreads();
-    for (uint32_t i = tid, nw = B.wl_n; i < nw; i += nt) {
-        const uint32_t ls = wl[i];
-        const uint32_t s = base_slot + ls;
-        if (*(volatile uint32_t*)(lmeta + ls) & M_VISITED) continue;
-        // every vertex left has both sides linked: walk the cycle from s out of its back side
-        const DV<W> v0 = dv_at(T, ops, s, BACK);
-        DV<W> v = v0; int side = BACK; uint32_t n = 0;
-        bool is_min = true, ok = true;
-        do {
-            int s_in;
-            if (!step(T, ops, fth, v, side, s_in) || ++n > T.per * T.nranks) { atomicOr(a.err, DERR_WALK_LIMIT); ok = false; break; }
-            side = 1 - s_in;
-            if (v.slot != s && (v.d < v.r ? v.d : v.r) < v0.d) is_min = false;
-        } while (v.slot != s);
-        if (!ok || !is_min) continue;
-        // Character_Buffer::rotate_append_cycle (include/Character_Buffer.hpp:166-175): start at the
-        // minimum vertex in its canonical orientation
-        char* p = reserve_fasta(B.sk, n + k - 1);
-        write_path(T, ops, fth, v0, BACK, n, p, false, true);
-        atomicAdd(&B.trivial, 1ull); atomicAdd(&B.icc, 1ull);
+    const uint32_t nw3 = B.wl_n;
+    for (uint32_t base = 0; base < nw3; base += nt) {
+        const uint32_t i = base + tid;
+        bool emit = false;
+        uint32_t n = 0;
+        DV<W> v0{};
+        if (i < nw3) {
+            const uint32_t ls = wl[i];
+            const uint32_t s = base_slot + ls;
+            if (!(*(volatile uint32_t*)(lmeta + ls) & M_VISITED)) {
+                // every vertex left has both sides linked: walk the cycle from s out of its back side
+                v0 = dv_at(T, ops, s, BACK);
+                DV<W> v = v0; int side = BACK;
+                bool is_min = true, ok = true;
+                do {
+                    int s_in;
+                    if (!step(T, ops, fth, v, side, s_in) || ++n > T.per * T.nranks) { atomicOr(a.err, DERR_WALK_LIMIT); ok = false; break; }
+                    side = 1 - s_in;
+                    if (v.slot != s && (v.d < v.r ? v.d : v.r) < v0.d) is_min = false;
+                } while (v.slot != s);
+                emit = ok && is_min;
+            }
+        }
+        __syncwarp();
+        const Res r = reserve_warp(B.sk, emit ? n + k + 3 : 0, 0, 0);
+        if (emit) {
+            // Character_Buffer::rotate_append_cycle (include/Character_Buffer.hpp:166-175): start at the
+            // minimum vertex in its canonical orientation
+            char* p = fasta_at(B.sk, r.fa, n + k - 1);
+            write_path(T, ops, fth, v0, BACK, n, p, false, true);
+            atomicAdd(&B.trivial, 1ull); atomicAdd(&B.icc, 1ull);
+        }
     }
     tsync<MODE>();
     clk[4] = clock64();
@@ -681,8 +821,13 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         if (a.record_clocks)
             for (int i = 0; i < 5; ++i) atomicAdd(&a.cnt->phase_cycles[i], (unsigned long long)(clk[i + 1] - clk[i]));
         const unsigned long long v[6] = {B.vertices, B.isolated, B.phantom, B.trivial, B.icc, B.lmtig};
-        for (int i = 0; i < 6; ++i)
-            if (v[i]) atomicAdd(B.sk.cnt + i, v[i]);
+        if (a.bucket_cnt) {   // batch: per-subgraph counters, summed per job afterwards (no contended atomics)
+            for (int i = 0; i < 5; ++i)
+                if (v[i]) atomicAdd(a.bucket_cnt + 5ull * g + i, (uint32_t)v[i]);
+        } else {
+            for (int i = 0; i < 6; ++i)
+                if (v[i]) atomicAdd(B.sk.cnt + i, v[i]);
+        }
     }
     tsync<MODE>();   // no CTA leaves while another may still read its shared memory
 }

@@ -13,6 +13,8 @@
 //             divergence, split into 20 records                        (seed 3)
 //   genome_i  one of 1000 genomes: log-uniform 0.5-8 Mbp, GC in [0.3, 0.7],
 //             1% as copies of 500-5000 bp at 1%                        (seed 1000+i)
+//   genome_n  a genome of a given length and seed: i.i.d. ACGT, 1% as copies of
+//             500-5000 bp at 1% (the serving mix's reference jobs and read sources)
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -204,6 +206,12 @@ void cfs_genome(uint32_t i, char* out) {
     const double gc = 0.3 + 0.4 * r.uni();
     iid(out, n, 1000003ull + i, gc);
     copies(r, out, n, n / 100, true, 500, 5000, 0.01);
+}
+
+void cfs_genome_n(uint64_t n, uint64_t seed, char* out) {
+    Rng r(seed);
+    iid(out, n, 7000003ull + seed, 0.5);
+    copies(r, out, n, n / 100, true, 500, std::min<uint64_t>(5000, n / 2), 0.01);
 }
 
 }  // extern "C"

@@ -72,6 +72,22 @@ class BatchTuning(ctypes.Structure):
                 ("table_load_pct", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("ms", ctypes.c_float)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("slots", ctypes.c_uint32), ("batch_max_jobs", ctypes.c_uint32), ("hbm_budget", ctypes.c_uint64),
+                ("batch_max_bases", ctypes.c_uint64), ("small_job_bases", ctypes.c_uint64)]
+
+
+class JobTiming(ctypes.Structure):
+    _fields_ = [("queued_s", ctypes.c_double), ("run_s", ctypes.c_double), ("latency_s", ctypes.c_double),
+                ("device_ms", ctypes.c_float), ("group_jobs", ctypes.c_uint32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in (
+        "submitted", "completed", "failed", "batches", "batched_jobs", "max_running", "bases", "held_bytes",
+        "hbm_budget")]
+
+
 class BatchStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in (
         "n_jobs", "n_redone", "n_bases", "n_records", "n_vertices", "n_lmtig", "fasta_bytes", "lmtig_bytes",
@@ -116,6 +132,15 @@ SIGNATURES = {
     "cfg_batch_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchTuning)]),
     "cfg_batch_last_error_string": (ctypes.c_char_p, [ctypes.c_void_p]),
     "cfg_batch_destroy": (None, [ctypes.c_void_p]),
+    "cfg_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ServerConfig), ctypes.POINTER(ctypes.c_void_p)]),
+    "cfg_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Params), ctypes.POINTER(Packed),
+                                         ctypes.POINTER(ctypes.c_uint64)]),
+    "cfg_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Results),
+                                       ctypes.POINTER(JobTiming)]),
+    "cfg_server_release": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    "cfg_server_query": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerStats)]),
+    "cfg_server_last_error_string": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "cfg_server_destroy": (None, [ctypes.c_void_p]),
 }
 
 _lib = None
@@ -343,6 +368,70 @@ class Batch:
     def set_tuning(self, local_div=4, cluster_threads=512, table_load_pct=100):
         t = BatchTuning(local_div, cluster_threads, table_load_pct, 0, 0.0)
         _check_b(self.lib, self.b, self.lib.cfg_batch_set_tuning(self.b, ctypes.byref(t)), "cfg_batch_set_tuning")
+
+
+class Server:
+    """Serving loop (cfg_server): submit jobs of mixed size and parameters, wait for each.
+
+    The packed input of a job must stay alive until its wait returns."""
+
+    def __init__(self, device: int = 0, slots: int = 4, hbm_budget: int = 0, batch_max_bases: int = 0,
+                 small_job_bases: int = 0, batch_max_jobs: int = 0):
+        self.lib = load()
+        cfg = ServerConfig(slots, batch_max_jobs, hbm_budget, batch_max_bases, small_job_bases)
+        s = ctypes.c_void_p()
+        rc = self.lib.cfg_server_create(device, ctypes.byref(cfg), ctypes.byref(s))
+        if rc:
+            raise CfgError(f"cfg_server_create: {ERRORS.get(rc, rc)}")
+        self.s = s
+        self._keep = {}
+
+    def _check(self, rc, what):
+        if rc:
+            msg = self.lib.cfg_server_last_error_string(self.s)
+            raise CfgError(f"{what}: {ERRORS.get(rc, rc)} {msg.decode(errors='replace') if msg else ''}")
+
+    def submit(self, packed: PackedInput, k: int, l: int = 20, cutoff: int = 1, graph_count: int = 16384,
+               table_load_pct: int = 0) -> int:
+        p = Params(k, l, cutoff, graph_count, 0, table_load_pct)
+        t = ctypes.c_uint64()
+        self._check(self.lib.cfg_server_submit(self.s, ctypes.byref(p), ctypes.byref(packed.p), ctypes.byref(t)),
+                    "cfg_server_submit")
+        self._keep[t.value] = packed
+        return t.value
+
+    def wait_raw(self, ticket: int):
+        r, tm = Results(), JobTiming()
+        self._check(self.lib.cfg_server_wait(self.s, ticket, ctypes.byref(r), ctypes.byref(tm)), "cfg_server_wait")
+        return r, tm
+
+    def wait(self, ticket: int):
+        """-> ((counts, FASTA bytes, [LmtigRec]), JobTiming); releases the ticket."""
+        r, tm = self.wait_raw(ticket)
+        out = results_to_python(r)
+        self.release(ticket)
+        return out, tm
+
+    def release(self, ticket: int):
+        self._check(self.lib.cfg_server_release(self.s, ticket), "cfg_server_release")
+        self._keep.pop(ticket, None)
+
+    def stats(self) -> ServerStats:
+        st = ServerStats()
+        self._check(self.lib.cfg_server_query(self.s, ctypes.byref(st)), "cfg_server_query")
+        return st
+
+    def close(self):
+        if self.s:
+            self.lib.cfg_server_destroy(self.s)
+            self.s = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def _check_b(lib, b, rc, what):

@@ -247,6 +247,51 @@ int cfg_batch_set_tuning(cfg_batch* b, const cfg_batch_tuning* t);
 const char* cfg_batch_last_error_string(cfg_batch* b);
 void cfg_batch_destroy(cfg_batch* b);
 
+/* ------------------------------------------------------------------------- */
+/* Serving loop: continuous admission of jobs of mixed size and parameters.
+ *
+ * cfg_server_submit queues one job (a genome or read set in cfg_pack_records'
+ * layout, with its own k / cutoff / table sizing; the input must stay valid
+ * until cfg_server_wait returns).  `slots` worker threads take queued work as
+ * soon as they are free and the device-memory budget allows: a large job runs
+ * alone on a plain context, small jobs waiting together with equal parameters run
+ * as one batch.  Jobs of different workers overlap on the device.  Contexts keep
+ * their device buffers between jobs.  Each job's results are exactly those of a
+ * plain run of it alone.  Results returned by cfg_server_wait stay valid until
+ * cfg_server_release, which every completed ticket needs (a plain context stays
+ * reserved for the ticket until then). */
+typedef struct cfg_server cfg_server;
+
+typedef struct cfg_server_config {
+    uint32_t slots;            /* worker threads / concurrent jobs (0: 4)                      */
+    uint32_t batch_max_jobs;   /* jobs per batch (0: 256)                                      */
+    uint64_t hbm_budget;       /* device bytes the server's contexts may hold (0: 70% of free) */
+    uint64_t batch_max_bases;  /* bases per batch (0: no batching)                             */
+    uint64_t small_job_bases;  /* jobs up to this size may be batched                          */
+} cfg_server_config;
+
+typedef struct cfg_job_timing {
+    double   queued_s;         /* submit -> start                 */
+    double   run_s;            /* start -> results on the host    */
+    double   latency_s;        /* submit -> results on the host   */
+    float    device_ms;        /* device time of the run that carried the job */
+    uint32_t group_jobs;       /* jobs in that run (1: plain)     */
+} cfg_job_timing;
+
+typedef struct cfg_server_stats {
+    uint64_t submitted, completed, failed, batches, batched_jobs, max_running, bases;
+    uint64_t held_bytes, hbm_budget;
+} cfg_server_stats;
+
+int cfg_server_create(int device, const cfg_server_config* config, cfg_server** out);
+int cfg_server_submit(cfg_server* s, const cfg_params* params, const cfg_packed* job, uint64_t* ticket);
+int cfg_server_wait(cfg_server* s, uint64_t ticket, cfg_results* out, cfg_job_timing* timing);
+int cfg_server_release(cfg_server* s, uint64_t ticket);
+int cfg_server_query(cfg_server* s, cfg_server_stats* out);
+const char* cfg_server_last_error_string(cfg_server* s);
+/* Finishes queued work, then frees every context. */
+void cfg_server_destroy(cfg_server* s);
+
 /* No counterpart in the reference.  For callers that must not allocate memory:
  * code recording into a CUDA graph whose stream capture someone else owns,
  * plugins whose host framework owns every byte of device memory, real-time

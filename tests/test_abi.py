@@ -80,3 +80,11 @@ def test_batch_create_rejects_bad_params():
         p = cfgpu.Params(k, l, c, G, flags, 0)
         assert lib.cfg_batch_create(0, ctypes.byref(p), ctypes.byref(b)) == 1
     assert lib.cfg_batch_run(None) == 1
+
+
+def test_server_rejects_bad_config():
+    lib = cfgpu.load()
+    s = ctypes.c_void_p()
+    cfg = cfgpu.ServerConfig(65, 0, 0, 0, 0)
+    assert lib.cfg_server_create(0, ctypes.byref(cfg), ctypes.byref(s)) == 1
+    assert lib.cfg_server_submit(None, None, None, None) == 1
