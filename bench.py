@@ -110,7 +110,7 @@ def bench_batch(args, pg, local, world, peak, with_cpu):
 
     b = cfgpu.Batch(k, l, cutoff, 16384, device=local if world > 1 else 0)
     b.submit(packed)
-    tuning = b.tune()
+    tuning = b.tune() if not args.no_tune else cfgpu.BatchTuning(4, 512, 100, 0, 0.0)
     for _ in range(warm):
         b.run()
     barrier(pg)
@@ -322,19 +322,27 @@ def bench_serve(args, local, world):
 
         th = threading.Thread(target=submitter)
         th.start()
-        lat, groups = [], []
-        for j in range(len(arr)):
-            while tickets[j] is None:
-                time.sleep(0.0005)
-            _, tm = srv.wait_raw(tickets[j])
-            srv.release(tickets[j])
+        lat, groups, done = [], [], []
+        for _ in range(len(arr)):          # completion order: results are released as soon as read
+            t, _, tm = srv.wait_any_raw()
+            srv.release(t)
             lat.append(tm.latency_s)
             groups.append(tm.group_jobs)
+            done.append(time.perf_counter() - start)
         th.join()
-        makespan = max(arr[j] + lat[j] for j in range(len(arr)))
-        return lat, makespan, groups
+        return lat, max(done), groups
 
-    run_server(arrivals(mu * 4, 99))     # warm the server's contexts
+    # warm every worker's contexts on the largest job of each kind (all workers take one at once)
+    for kind in ("ref", "read"):
+        big = max((j for j in range(len(jobs)) if jobs[j][0] == kind), key=lambda j: jobs[j][1].n_bases, default=None)
+        if big is None:
+            continue
+        _, p, c, load = jobs[big]
+        ts = [srv.submit(p, k, 20, c, table_load_pct=load) for _ in range(4)]
+        for _ in ts:
+            t, _, _ = srv.wait_any_raw()
+            srv.release(t)
+    run_server(arrivals(mu * 4, 99))
     rates = []
     for f in args.serve_load:
         arr = arrivals(mu * f, 1000 + int(100 * f))
@@ -492,7 +500,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="reads30x", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="reads30x", choices=sorted(WORKLOADS) + ["batch", "serve"],
+                    help="batch / serve: only the batched-vs-plain or the serving comparison")
+    ap.add_argument("--no-tune", action="store_true", help="batched form: the default launch shapes")
     ap.add_argument("--reads", type=int, default=10_000_000)
     ap.add_argument("--cpu-sample-reads", type=int, default=1_000_000)
     ap.add_argument("--cpu-sample-bases", type=int, default=60_000_000)
@@ -508,6 +518,17 @@ def main():
         args.warmup = 3
 
     rank, world, local, pg = dist_setup(args.gpus)
+    if args.workload in ("batch", "serve"):
+        peak, _ = measured_hbm_peak()
+        if args.workload == "batch":
+            out = bench_batch(args, pg, local, world, peak, rank == 0 and not args.no_cpu_baseline)
+        else:
+            out = bench_serve(args, local, world)
+        if rank == 0:
+            print(json.dumps(out))
+        if pg is not None:
+            pg.destroy_process_group()
+        return
     name = args.workload
     k, l, cutoff, load_pct, desc = WORKLOADS[name]
     if args.table_load_pct:

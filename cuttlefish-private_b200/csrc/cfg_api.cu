@@ -36,7 +36,8 @@ struct cfg_ctx {
     std::string err;
 
     // input
-    DevBuf packed, frag_off, frag_len;
+    DevBuf packed, frag_off, frag_len, text;
+    ParseBuffers parse;
     const uint64_t* d_packed = nullptr; const uint64_t* d_frag_off = nullptr; const uint32_t* d_frag_len = nullptr;
     uint64_t n_bases = 0, n_frags = 0;
     bool have_input = false, have_run = false;
@@ -373,6 +374,44 @@ int cfg_submit_packed(cfg_ctx* c, const uint64_t* packed, uint64_t n_bases, cons
     return CFG_OK;
 }
 
+int cfg_submit_text(cfg_ctx* c, const char* text, uint64_t bytes) {
+    if (!c || (bytes && !text)) return fail(c, CFG_ERR_BAD_INPUT, "null input");
+    CK(cudaSetDevice(c->device));
+    // FASTQ when the first byte after leading blank lines is '@', else FASTA
+    uint64_t i = 0;
+    while (i < bytes && (text[i] == '\n' || text[i] == '\r')) ++i;
+    const int fastq = i < bytes && text[i] == '@';
+    if (!c->text.ensure(bytes + 16)) return fail(c, CFG_ERR_OOM, "text buffer");
+    if (bytes) CK(cudaMemcpyAsync(c->text.p, text, bytes, cudaMemcpyHostToDevice, c->stream));
+    const int rc = parse_text_device(c->text.as<uint8_t>(), bytes, fastq, c->p.k, c->parse, c->stream);
+    if (rc == CFG_ERR_OOM) return fail(c, rc, "parse buffers");
+    if (rc == CFG_ERR_BAD_INPUT) return fail(c, rc, "a job must hold fewer than 2^32 bases");
+    if (rc) return fail(c, rc, std::string("text parse: ") + cudaGetErrorString(cudaGetLastError()));
+    c->d_packed = c->parse.packed; c->d_frag_off = c->parse.frag_off; c->d_frag_len = c->parse.frag_len;
+    c->n_bases = c->parse.n_bases; c->n_frags = c->parse.n_frags;
+    c->have_input = true; c->have_run = false;
+    return CFG_OK;
+}
+
+int cfg_input_counts(cfg_ctx* c, uint64_t* n_bases, uint64_t* n_frags) {
+    if (!c || !n_bases || !n_frags) return CFG_ERR_BAD_INPUT;
+    if (!c->have_input) return fail(c, CFG_ERR_STATE, "no input submitted");
+    *n_bases = c->n_bases; *n_frags = c->n_frags;
+    return CFG_OK;
+}
+
+int cfg_copy_input(cfg_ctx* c, uint64_t* words, uint64_t* frag_off, uint32_t* frag_len) {
+    if (!c) return CFG_ERR_BAD_INPUT;
+    if (!c->have_input) return fail(c, CFG_ERR_STATE, "no input submitted");
+    CK(cudaSetDevice(c->device));
+    const uint64_t w = (c->n_bases + 31) / 32;
+    if (words && w) CK(cudaMemcpyAsync(words, c->d_packed, 8 * w, cudaMemcpyDeviceToHost, c->stream));
+    if (frag_off && c->n_frags) CK(cudaMemcpyAsync(frag_off, c->d_frag_off, 8 * c->n_frags, cudaMemcpyDeviceToHost, c->stream));
+    if (frag_len && c->n_frags) CK(cudaMemcpyAsync(frag_len, c->d_frag_len, 4 * c->n_frags, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return CFG_OK;
+}
+
 int cfg_submit_packed_device(cfg_ctx* c, const uint64_t* d_packed, uint64_t n_bases, const uint64_t* d_frag_off,
                              const uint32_t* d_frag_len, uint64_t n_frags) {
     if (!c || (n_bases && !d_packed) || (n_frags && (!d_frag_off || !d_frag_len))) return fail(c, CFG_ERR_BAD_INPUT, "null input");
@@ -490,7 +529,8 @@ void cfg_destroy(cfg_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    DevBuf* bufs[] = {&c->packed, &c->frag_off, &c->frag_len, &c->flat, &c->hist, &c->misc, &c->bucket_off, &c->inst,
+    c->parse.release();
+    DevBuf* bufs[] = {&c->packed, &c->frag_off, &c->frag_len, &c->text, &c->flat, &c->hist, &c->misc, &c->bucket_off, &c->inst,
                       &c->fill, &c->recs, &c->list, &c->tab_off, &c->tab_cap, &c->arena, &c->fasta, &c->lm_text,
                       &c->lm, &c->dump, &c->retry, &c->counters};
     for (DevBuf* b : bufs) b->release();

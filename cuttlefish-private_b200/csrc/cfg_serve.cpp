@@ -78,6 +78,7 @@ struct Ticket {
     std::vector<cfg_lmtig> own_lm;
     uint32_t group = 1;      // jobs in the run that carried this one
     float device_ms = 0;
+    bool collected = false;  // returned by cfg_server_wait_any
 };
 
 struct Worker {
@@ -329,6 +330,28 @@ int cfg_server_wait(cfg_server* s, uint64_t ticket, cfg_results* out, cfg_job_ti
     if (t->rc) { s->err = t->err; return t->rc; }
     if (out) *out = t->res;
     return CFG_OK;
+}
+
+int cfg_server_wait_any(cfg_server* s, uint64_t* ticket, cfg_results* out, cfg_job_timing* timing) {
+    if (!s || !ticket) return CFG_ERR_BAD_INPUT;
+    uint64_t id = 0;
+    {
+        std::unique_lock<std::mutex> lock(s->mu);
+        for (;;) {
+            bool pending = false;
+            uint64_t best = 0;
+            for (auto& kv : s->tickets) {
+                Ticket* t = kv.second.get();
+                if (t->state == 2 && !t->collected && (best == 0 || t->id < best)) best = t->id;
+                if (!t->collected) pending = true;
+            }
+            if (best) { s->tickets[best]->collected = true; id = best; break; }
+            if (!pending) return CFG_ERR_STATE;   // nothing submitted and not yet collected
+            s->cv_done.wait(lock);
+        }
+    }
+    *ticket = id;
+    return cfg_server_wait(s, id, out, timing);
 }
 
 int cfg_server_release(cfg_server* s, uint64_t ticket) {

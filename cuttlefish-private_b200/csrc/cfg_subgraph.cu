@@ -544,18 +544,20 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         if (disc) T.mark_disc(s, disc);
         return true;
     };
-    bool by_instance = false;
-    if constexpr (MODE == LOCAL) by_instance = r1 - r0 <= per;
-    if (by_instance) {
-        // one thread per k-mer instance: the records' instance counts, prefix-summed into
-        // the (still unused) work list, map instances to records
-        const uint32_t nrec = r1 - r0;
+    // this CTA's share of the subgraph's records (all of them for one-CTA tables)
+    const uint32_t q0 = r0 + (uint32_t)((uint64_t)(r1 - r0) * rank / nranks);
+    const uint32_t q1 = r0 + (uint32_t)((uint64_t)(r1 - r0) * (rank + 1) / nranks);
+    if (q1 - q0 <= per) {
+        // one thread per k-mer instance (balanced whatever the record lengths): the records'
+        // instance counts, prefix-summed into the (still unused) work list, map
+        // instances to records
+        const uint32_t nrec = q1 - q0;
         const uint32_t chunk = (nrec + nt - 1) / nt;
         const uint32_t c0 = min(nrec, tid * chunk), c1 = min(nrec, c0 + chunk);
         uint32_t sum = 0;
-        for (uint32_t j = c0; j < c1; ++j) sum += rec_len(a.recs[r0 + j]) - k + 1;
+        for (uint32_t j = c0; j < c1; ++j) sum += rec_len(a.recs[q0 + j]) - k + 1;
         uint32_t run = block_excl_scan(sum, B);
-        for (uint32_t j = c0; j < c1; ++j) { wl[j] = run; run += rec_len(a.recs[r0 + j]) - k + 1; }
+        for (uint32_t j = c0; j < c1; ++j) { wl[j] = run; run += rec_len(a.recs[q0 + j]) - k + 1; }
         __syncthreads();
         const uint32_t total = B.scan_total;
         for (uint32_t t = tid; t < total; t += nt) {
@@ -565,7 +567,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
                 const uint32_t mid = (lo + hi) >> 1;
                 if (wl[mid] <= t) lo = mid; else hi = mid;
             }
-            const uint64_t rec = a.recs[r0 + lo];
+            const uint64_t rec = a.recs[q0 + lo];
             const uint32_t pos = rec_pos(rec), len = rec_len(rec);
             const uint32_t idx = t - wl[lo];
             const uint64_t p = (uint64_t)pos + idx;
@@ -584,7 +586,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
                 break;
         }
     } else {
-        for (uint32_t r = r0 + rank * nt + tid; r < r1; r += nranks * nt) {
+        for (uint32_t r = q0 + tid; r < q1; r += nt) {
             if (*(volatile uint32_t*)&B.overflow) break;
             const uint64_t rec = a.recs[r];
             const uint32_t pos = rec_pos(rec), len = rec_len(rec), ld = rec_ld(rec), rd = rec_rd(rec);

@@ -117,6 +117,9 @@ SIGNATURES = {
                                           ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_uint64),
                                           ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     "cfg_free": (None, [ctypes.c_void_p]),
+    "cfg_submit_text": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64]),
+    "cfg_input_counts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
+    "cfg_copy_input": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cfg_pack_records": (ctypes.c_int, [ctypes.c_char_p, U64P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int,
                                         ctypes.POINTER(Packed)]),
     "cfg_packed_free": (None, [ctypes.POINTER(Packed)]),
@@ -137,6 +140,8 @@ SIGNATURES = {
                                          ctypes.POINTER(ctypes.c_uint64)]),
     "cfg_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Results),
                                        ctypes.POINTER(JobTiming)]),
+    "cfg_server_wait_any": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(Results),
+                                           ctypes.POINTER(JobTiming)]),
     "cfg_server_release": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "cfg_server_query": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerStats)]),
     "cfg_server_last_error_string": (ctypes.c_char_p, [ctypes.c_void_p]),
@@ -248,6 +253,21 @@ class Compactor:
         p = packed.p
         rc = self.lib.cfg_submit_packed(self.ctx, p.words, p.n_bases, p.frag_off, p.frag_len, p.n_frags)
         _check(self.lib, self.ctx, rc, "cfg_submit_packed")
+
+    def submit_text(self, text: bytes):
+        """FASTA / FASTQ text, parsed on the device (cfg_submit_text)."""
+        rc = self.lib.cfg_submit_text(self.ctx, text, len(text))
+        _check(self.lib, self.ctx, rc, "cfg_submit_text")
+
+    def input_copy(self):
+        """-> (words list, frag_off list, frag_len list) of the submitted input."""
+        nb, nf = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(self.lib, self.ctx, self.lib.cfg_input_counts(self.ctx, ctypes.byref(nb), ctypes.byref(nf)), "cfg_input_counts")
+        w = (ctypes.c_uint64 * max(1, (nb.value + 31) // 32))()
+        fo = (ctypes.c_uint64 * max(1, nf.value))()
+        fl = (ctypes.c_uint32 * max(1, nf.value))()
+        _check(self.lib, self.ctx, self.lib.cfg_copy_input(self.ctx, w, fo, fl), "cfg_copy_input")
+        return nb.value, list(w)[: (nb.value + 31) // 32], list(fo)[: nf.value], list(fl)[: nf.value]
 
     def submit_device(self, d_words: int, n_bases: int, d_frag_off: int, d_frag_len: int, n_frags: int):
         rc = self.lib.cfg_submit_packed_device(self.ctx, d_words, n_bases, d_frag_off, d_frag_len, n_frags)
@@ -404,6 +424,13 @@ class Server:
         r, tm = Results(), JobTiming()
         self._check(self.lib.cfg_server_wait(self.s, ticket, ctypes.byref(r), ctypes.byref(tm)), "cfg_server_wait")
         return r, tm
+
+    def wait_any_raw(self):
+        """-> (ticket, Results, JobTiming) of the next completed job (completion order)."""
+        t, r, tm = ctypes.c_uint64(), Results(), JobTiming()
+        self._check(self.lib.cfg_server_wait_any(self.s, ctypes.byref(t), ctypes.byref(r), ctypes.byref(tm)),
+                    "cfg_server_wait_any")
+        return t.value, r, tm
 
     def wait(self, ticket: int):
         """-> ((counts, FASTA bytes, [LmtigRec]), JobTiming); releases the ticket."""

@@ -130,6 +130,20 @@ int cfg_submit_packed(cfg_ctx* ctx, const uint64_t* packed, uint64_t n_bases,
 int cfg_submit_packed_device(cfg_ctx* ctx, const uint64_t* d_packed, uint64_t n_bases,
                              const uint64_t* d_frag_off, const uint32_t* d_frag_len, uint64_t n_frags);
 
+/* Supplies one job as FASTA or FASTQ text (a whole file's content, plain; the format
+ * is FASTQ when the first byte after blank lines is '@').  The text is copied to the
+ * device and parsed there: a FASTA record's sequence is its lines joined, a FASTQ
+ * record's its second line; fragments are the maximal runs of ACGT (either case) of
+ * at least k+1 bases -- the input that cfg_pack_records + cfg_submit_packed give for
+ * the same records.  Replaces RabbitFX parsing (include/RabbitFX/io/Formater.cpp:87-130,
+ * 265-297) and the fragment scan (src/Graph_Partitioner.cpp:461-501). */
+int cfg_submit_text(cfg_ctx* ctx, const char* text, uint64_t bytes);
+
+/* The submitted input's size, and a copy of it in cfg_submit_packed's layout
+ * (words: (n_bases+31)/32 entries; any pointer may be NULL). */
+int cfg_input_counts(cfg_ctx* ctx, uint64_t* n_bases, uint64_t* n_frags);
+int cfg_copy_input(cfg_ctx* ctx, uint64_t* words, uint64_t* frag_off, uint32_t* frag_len);
+
 /* Partition -> subgraph construct -> local walk, all on the device.  Replaces
  * Graph_Partitioner::process_chunk (src/Graph_Partitioner.cpp:424-614),
  * Subgraphs_Manager::finalize/process (src/Subgraphs_Manager.cpp:84-255),
@@ -286,6 +300,9 @@ typedef struct cfg_server_stats {
 int cfg_server_create(int device, const cfg_server_config* config, cfg_server** out);
 int cfg_server_submit(cfg_server* s, const cfg_params* params, const cfg_packed* job, uint64_t* ticket);
 int cfg_server_wait(cfg_server* s, uint64_t ticket, cfg_results* out, cfg_job_timing* timing);
+/* Waits for the next completed ticket not yet returned by this call (completion
+ * order), so results can be released as soon as they are consumed. */
+int cfg_server_wait_any(cfg_server* s, uint64_t* ticket, cfg_results* out, cfg_job_timing* timing);
 int cfg_server_release(cfg_server* s, uint64_t ticket);
 int cfg_server_query(cfg_server* s, cfg_server_stats* out);
 const char* cfg_server_last_error_string(cfg_server* s);
