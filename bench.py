@@ -312,6 +312,8 @@ def bench_serve(args, local, world):
         start = time.perf_counter()
         tickets = [None] * len(arr)
 
+        submitted = threading.Semaphore(0)
+
         def submitter():
             for j, a in enumerate(arr):
                 now = time.perf_counter() - start
@@ -319,11 +321,13 @@ def bench_serve(args, local, world):
                     time.sleep(a - now)
                 _, p, c, load = jobs[j]
                 tickets[j] = srv.submit(p, k, 20, c, table_load_pct=load)
+                submitted.release()
 
         th = threading.Thread(target=submitter)
         th.start()
         lat, groups, done = [], [], []
         for _ in range(len(arr)):          # completion order: results are released as soon as read
+            submitted.acquire()            # one more job is in the server
             t, _, tm = srv.wait_any_raw()
             srv.release(t)
             lat.append(tm.latency_s)

@@ -47,8 +47,11 @@ struct cfg_ctx {
     // plan
     DevBuf list, tab_off, tab_cap, arena;
     // outputs
-    DevBuf fasta, lm_text, lm, dump, retry, counters;
-    uint64_t fasta_cap = 0, lm_text_cap = 0, lm_cap = 0, dump_cap = 0;
+    DevBuf fasta, lm_text, lm, dump, retry, counters, stripe_cur, stripe_base;
+    uint64_t fasta_cap = 0, lm_text_cap = 0, lm_cap = 0, dump_cap = 0;   // per output stripe
+    // per stripe, after a run: used FASTA bytes, label bytes, lm-tig records
+    uint64_t s_fasta[OUT_STRIPES] = {}, s_text[OUT_STRIPES] = {}, s_lm[OUT_STRIPES] = {};
+    uint32_t stripes = OUT_STRIPES;   // min(OUT_STRIPES, graph_count): every stripe gets subgraphs
 
     // host results
     HostBuf h_fasta, h_lm_text, h_lm;
@@ -182,6 +185,7 @@ int launch_plan(cfg_ctx* c, const std::vector<Launch>& plan, uint64_t arena_slot
         a.fasta = c->fasta.as<char>(); a.fasta_cap = c->fasta_cap;
         a.lm_text = c->lm_text.as<char>(); a.lm_text_cap = c->lm_text_cap;
         a.lm = c->lm.as<LmtigOut>(); a.lm_cap = c->lm_cap;
+        a.stripe_cur = c->stripe_cur.as<unsigned long long>(); a.stripes = c->stripes;
         a.dump = (c->p.flags & CFG_FLAG_DUMP_STATES) ? c->dump.as<StateOut>() : nullptr; a.dump_cap = c->dump_cap;
         a.retry = c->retry.as<uint32_t>(); a.cnt = c->counters.as<Counters>();
         a.err = &c->misc.as<MiscWords>()->err;
@@ -193,13 +197,19 @@ int launch_plan(cfg_ctx* c, const std::vector<Launch>& plan, uint64_t arena_slot
     return CFG_OK;
 }
 
+// Output arenas cut into OUT_STRIPES equal slices, each with room for its share of the
+// estimate plus an eighth (subgraphs fall into stripes by their index).
 int ensure_outputs(cfg_ctx* c, uint64_t fasta_need, uint64_t lm_text_need, uint64_t lm_need) {
-    if (!c->fasta.ensure(fasta_need)) return fail(c, CFG_ERR_OOM, "fasta arena");
-    c->fasta_cap = c->fasta.bytes;
-    if (!c->lm_text.ensure(lm_text_need)) return fail(c, CFG_ERR_OOM, "lm-tig arena");
-    c->lm_text_cap = c->lm_text.bytes;
-    if (!c->lm.ensure(lm_need * sizeof(LmtigOut))) return fail(c, CFG_ERR_OOM, "lm-tig records");
-    c->lm_cap = c->lm.bytes / sizeof(LmtigOut);
+    const uint32_t S = c->stripes;
+    auto slice = [S](uint64_t need) { const uint64_t s = need / S; return s + s / 8 + 4096; };
+    if (!c->fasta.ensure(S * slice(fasta_need))) return fail(c, CFG_ERR_OOM, "fasta arena");
+    c->fasta_cap = c->fasta.bytes / S;
+    if (!c->lm_text.ensure(S * slice(lm_text_need))) return fail(c, CFG_ERR_OOM, "lm-tig arena");
+    c->lm_text_cap = c->lm_text.bytes / S;
+    if (!c->lm.ensure(S * slice(lm_need) * sizeof(LmtigOut))) return fail(c, CFG_ERR_OOM, "lm-tig records");
+    c->lm_cap = c->lm.bytes / sizeof(LmtigOut) / S;
+    if (!c->stripe_cur.ensure(8ull * JOB_CUR_STRIDE * OUT_STRIPES) || !c->stripe_base.ensure(8ull * OUT_STRIPES))
+        return fail(c, CFG_ERR_OOM, "stripe cursors");
     if (!c->retry.ensure(4ull * c->G)) return fail(c, CFG_ERR_OOM, "retry list");
     if (!c->counters.ensure(sizeof(Counters))) return fail(c, CFG_ERR_OOM, "counters");
     if (c->p.flags & CFG_FLAG_DUMP_STATES) {
@@ -235,6 +245,7 @@ int run_subgraphs(cfg_ctx* c, const std::vector<uint32_t>& inst_h) {
         int rc = ensure_outputs(c, fasta_need, lm_text_need, lm_need);
         if (rc) return rc;
         CK(cudaMemsetAsync(c->counters.p, 0, sizeof(Counters), c->stream));
+        CK(cudaMemsetAsync(c->stripe_cur.p, 0, 8ull * JOB_CUR_STRIDE * OUT_STRIPES, c->stream));
         std::vector<uint32_t> work = todo;
         std::vector<uint64_t> cur_want = want;
         uint64_t retries = 0;
@@ -267,9 +278,18 @@ int run_subgraphs(cfg_ctx* c, const std::vector<uint32_t>& inst_h) {
             CK(cudaEventRecord(c->ev[6], c->stream));
             Counters h{};
             MiscWords m{};
+            unsigned long long cur[JOB_CUR_STRIDE * OUT_STRIPES];
             CK(cudaMemcpyAsync(&h, c->counters.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
             CK(cudaMemcpyAsync(&m, c->misc.p, sizeof(m), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaMemcpyAsync(cur, c->stripe_cur.p, sizeof(cur), cudaMemcpyDeviceToHost, c->stream));
             CK(cudaStreamSynchronize(c->stream));
+            uint64_t max_f = 0, max_t = 0, max_l = 0;
+            for (uint32_t st = 0; st < OUT_STRIPES; ++st) {
+                c->s_fasta[st] = cur[st * JOB_CUR_STRIDE]; c->s_text[st] = cur[st * JOB_CUR_STRIDE + 1];
+                c->s_lm[st] = cur[st * JOB_CUR_STRIDE + 2];
+                max_f = std::max<uint64_t>(max_f, c->s_fasta[st]); max_t = std::max<uint64_t>(max_t, c->s_text[st]);
+                max_l = std::max<uint64_t>(max_l, c->s_lm[st]);
+            }
             {
                 float ms = 0;
                 cudaEventElapsedTime(&ms, c->ev[5], c->ev[6]);
@@ -278,9 +298,9 @@ int run_subgraphs(cfg_ctx* c, const std::vector<uint32_t>& inst_h) {
             rc = check_err_word(c, m.err);
             if (rc) return rc;
             if (m.err & (DERR_OUT_OVERFLOW | DERR_DUMP_OVERFLOW)) {
-                fasta_need = std::max<uint64_t>(fasta_need, h.fasta_bytes) * 2;
-                lm_text_need = std::max<uint64_t>(lm_text_need, h.lm_bytes) * 2;
-                lm_need = std::max<uint64_t>(lm_need, h.lm_count) * 2;
+                fasta_need = std::max<uint64_t>(fasta_need, max_f * c->stripes) * 2;
+                lm_text_need = std::max<uint64_t>(lm_text_need, max_t * c->stripes) * 2;
+                lm_need = std::max<uint64_t>(lm_need, max_l * c->stripes) * 2;
                 CK(cudaMemsetAsync(&c->misc.as<MiscWords>()->err, 0, sizeof(uint32_t), c->stream));
                 overflow = true;
                 break;
@@ -302,11 +322,25 @@ int run_subgraphs(cfg_ctx* c, const std::vector<uint32_t>& inst_h) {
         Counters h{};
         CK(cudaMemcpyAsync(&h, c->counters.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
+        // label offsets of each stripe's lm-tigs become offsets into the joined label text
+        uint64_t fb = 0, tb = 0, nl = 0;
+        unsigned long long base[OUT_STRIPES];
+        for (uint32_t st = 0; st < OUT_STRIPES; ++st) {
+            base[st] = tb;
+            fb += c->s_fasta[st]; tb += c->s_text[st]; nl += c->s_lm[st];
+        }
+        if (nl) {
+            CK(cudaMemcpyAsync(c->stripe_base.p, base, sizeof(base), cudaMemcpyHostToDevice, c->stream));
+            launch_stripe_fixup(c->lm.as<LmtigOut>(), c->lm_cap, c->stripe_cur.as<unsigned long long>(),
+                                c->stripe_base.as<unsigned long long>(), OUT_STRIPES, c->stream);
+            CK(cudaGetLastError());
+            c->launches += 1;
+        }
         cfg_counts& o = c->counts;
         o.n_bases = c->n_bases; o.n_records = c->n_records; o.n_instances = c->n_instances;
         o.n_vertices = h.vertices; o.n_isolated = h.isolated; o.n_phantom = h.phantom;
-        o.n_trivial = h.trivial; o.n_icc = h.icc; o.n_lmtig = h.lm_count;
-        o.fasta_bytes = h.fasta_bytes; o.lmtig_bytes = h.lm_bytes; o.n_retries = retries;
+        o.n_trivial = h.trivial; o.n_icc = h.icc; o.n_lmtig = nl;
+        o.fasta_bytes = fb; o.lmtig_bytes = tb; o.n_retries = retries;
         o.n_launches = c->launches;
         c->dump_n = h.dump_count;
         for (int i = 0; i < 5; ++i) c->phase_cycles[i] = h.phase_cycles[i];
@@ -334,6 +368,7 @@ int cfg_create(int device, const cfg_params* params, cfg_ctx** out) {
     cfg_ctx* c = new (std::nothrow) cfg_ctx();
     if (!c) return CFG_ERR_OOM;
     c->device = device; c->p = p; c->G = p.graph_count; c->words = p.k <= 31 ? 1 : 2;
+    c->stripes = std::min<uint32_t>(OUT_STRIPES, p.graph_count);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return CFG_ERR_CUDA; }
     for (auto& e : c->ev)
         if (cudaEventCreate(&e) != cudaSuccess) { cfg_destroy(c); return CFG_ERR_CUDA; }
@@ -464,9 +499,20 @@ int cfg_fetch(cfg_ctx* c, cfg_results* out) {
     if (!c->h_fasta.ensure(n.fasta_bytes + 1) || !c->h_lm_text.ensure(n.lmtig_bytes + 1) ||
         !c->h_lm.ensure(n.n_lmtig * sizeof(cfg_lmtig) + 1))
         return fail(c, CFG_ERR_OOM, "pinned result buffers");
-    if (n.fasta_bytes) CK(cudaMemcpyAsync(c->h_fasta.p, c->fasta.p, n.fasta_bytes, cudaMemcpyDeviceToHost, c->stream));
-    if (n.lmtig_bytes) CK(cudaMemcpyAsync(c->h_lm_text.p, c->lm_text.p, n.lmtig_bytes, cudaMemcpyDeviceToHost, c->stream));
-    if (n.n_lmtig) CK(cudaMemcpyAsync(c->h_lm.p, c->lm.p, n.n_lmtig * sizeof(cfg_lmtig), cudaMemcpyDeviceToHost, c->stream));
+    // each output stripe's used part, joined in stripe order
+    uint64_t fo = 0, to = 0, lo = 0;
+    for (uint32_t st = 0; st < OUT_STRIPES; ++st) {
+        if (c->s_fasta[st])
+            CK(cudaMemcpyAsync((char*)c->h_fasta.p + fo, c->fasta.as<char>() + st * c->fasta_cap, c->s_fasta[st],
+                               cudaMemcpyDeviceToHost, c->stream));
+        if (c->s_text[st])
+            CK(cudaMemcpyAsync((char*)c->h_lm_text.p + to, c->lm_text.as<char>() + st * c->lm_text_cap, c->s_text[st],
+                               cudaMemcpyDeviceToHost, c->stream));
+        if (c->s_lm[st])
+            CK(cudaMemcpyAsync((cfg_lmtig*)c->h_lm.p + lo, c->lm.as<LmtigOut>() + st * c->lm_cap,
+                               c->s_lm[st] * sizeof(cfg_lmtig), cudaMemcpyDeviceToHost, c->stream));
+        fo += c->s_fasta[st]; to += c->s_text[st]; lo += c->s_lm[st];
+    }
     CK(cudaStreamSynchronize(c->stream));
     out->counts = n;
     out->fasta = (const char*)c->h_fasta.p;
@@ -532,7 +578,7 @@ void cfg_destroy(cfg_ctx* c) {
     c->parse.release();
     DevBuf* bufs[] = {&c->packed, &c->frag_off, &c->frag_len, &c->text, &c->flat, &c->hist, &c->misc, &c->bucket_off, &c->inst,
                       &c->fill, &c->recs, &c->list, &c->tab_off, &c->tab_cap, &c->arena, &c->fasta, &c->lm_text,
-                      &c->lm, &c->dump, &c->retry, &c->counters};
+                      &c->lm, &c->dump, &c->retry, &c->counters, &c->stripe_cur, &c->stripe_base};
     for (DevBuf* b : bufs) b->release();
     c->h_fasta.release(); c->h_lm_text.release(); c->h_lm.release();
     for (auto& e : c->ev) if (e) cudaEventDestroy(e);

@@ -82,13 +82,17 @@ __global__ void __launch_bounds__(256) k_classify(const uint32_t* __restrict__ i
     __shared__ uint32_t cnt[NCLS], base[NCLS];
     if (bw->err & DERR_REC_OVERFLOW) return;   // the run is redone with a larger record buffer
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t b0 = blockIdx.x * blockDim.x; b0 < cc.n_buckets; b0 += stride) {
+    const uint32_t n_jobs = cc.n_buckets >> cc.g_shift;
+    for (uint32_t t0 = blockIdx.x * blockDim.x; t0 < cc.n_buckets; t0 += stride) {
         if (threadIdx.x < NCLS) cnt[threadIdx.x] = 0;
         __syncthreads();
-        const uint32_t b = b0 + threadIdx.x;
+        // job-interleaved order: neighbouring list entries (run at the same time) belong
+        // to different jobs, so their output cursors are not contended
+        const uint32_t t = t0 + threadIdx.x;
+        const uint32_t b = t < cc.n_buckets ? ((t % n_jobs) << cc.g_shift) | (t / n_jobs) : 0;
         uint32_t c = NCLS, local = 0;
         uint64_t want = 0;
-        if (b < cc.n_buckets) {
+        if (t < cc.n_buckets) {
             const uint32_t n = inst[b];
             if (n) { c = class_of(n, cc, want); local = atomicAdd(&cnt[c], 1u); }
         }
@@ -157,7 +161,7 @@ __global__ void __launch_bounds__(256) k_job_regions(const uint32_t* __restrict_
 
 // One CTA per job: its subgraphs' counters summed into the job's.
 __global__ void __launch_bounds__(256) k_job_finalize(const uint32_t* __restrict__ bucket_cnt, uint32_t g_shift,
-                                                      JobOut* jobs) {
+                                                      JobOut* jobs, const unsigned long long* __restrict__ job_cur) {
     __shared__ unsigned long long part[8][5];
     const uint32_t j = blockIdx.x, G = 1u << g_shift;
     const uint64_t b0 = (uint64_t)j << g_shift;
@@ -174,7 +178,9 @@ __global__ void __launch_bounds__(256) k_job_finalize(const uint32_t* __restrict
     for (uint32_t w = 0; w < (blockDim.x >> 5); ++w)
         for (int c = 0; c < 5; ++c) t[c] += part[w][c];
     JobOut& J = jobs[j];
+    const unsigned long long* cur = job_cur + (size_t)j * JOB_CUR_STRIDE;
     J.vertices = t[0]; J.isolated = t[1]; J.phantom = t[2]; J.trivial = t[3]; J.icc = t[4];
+    J.fasta_used = cur[0]; J.lm_text_used = cur[1]; J.lm_used = cur[2];
     J.lmtig = J.lm_used;
 }
 
@@ -206,7 +212,7 @@ struct cfg_batch {
 
     // pipeline
     DevBuf flat, hist, bw, bucket_off, inst, fill, partials, recs, list, tab_off, tab_cap, arena, jobs,
-        fasta, lm_text, lm, retry, counters, bucket_cnt;
+        fasta, lm_text, lm, retry, counters, bucket_cnt, job_cur;
     uint64_t rec_cap = 0, arena_slots = 0, fasta_cap = 0, lm_text_cap = 0, lm_cap = 0;
     cudaGraphExec_t exec = nullptr;
     std::vector<Shape> shapes;
@@ -306,7 +312,8 @@ int ensure_buffers(cfg_batch* b) {
         !b->arena.ensure(b->arena_slots * slot_bytes(b->words)) || !b->jobs.ensure(sizeof(JobOut) * b->n_jobs) ||
         !b->fasta.ensure(b->fasta_cap, false) || !b->lm_text.ensure(b->lm_text_cap, false) ||
         !b->lm.ensure(sizeof(LmtigOut) * b->lm_cap, false) ||
-        !b->retry.ensure(4 * NB) || !b->counters.ensure(sizeof(Counters)) || !b->bucket_cnt.ensure(20 * NB))
+        !b->retry.ensure(4 * NB) || !b->counters.ensure(sizeof(Counters)) || !b->bucket_cnt.ensure(20 * NB) ||
+        !b->job_cur.ensure(8ull * JOB_CUR_STRIDE * b->n_jobs))
         return bfail(b, CFG_ERR_OOM, "batch buffers");
     return CFG_OK;
 }
@@ -321,6 +328,7 @@ int enqueue(cfg_batch* b) {
     BCK(cudaMemsetAsync(b->jobs.p, 0, sizeof(JobOut) * b->n_jobs, s));
     BCK(cudaMemsetAsync(b->counters.p, 0, sizeof(Counters), s));
     BCK(cudaMemsetAsync(b->bucket_cnt.p, 0, 20 * NB, s));
+    BCK(cudaMemsetAsync(b->job_cur.p, 0, 8ull * JOB_CUR_STRIDE * b->n_jobs, s));
     uint64_t launches = 0;
 
     PartitionArgs pa{};
@@ -373,13 +381,15 @@ int enqueue(cfg_batch* b) {
     a.retry = b->retry.as<uint32_t>(); a.cnt = b->counters.as<Counters>(); a.err = &bw->err;
     a.jobs = b->jobs.as<JobOut>(); a.g_shift = b->g_shift; a.record_clocks = 0;
     a.bucket_cnt = b->bucket_cnt.as<uint32_t>();
+    a.job_cur = b->job_cur.as<unsigned long long>();
     for (const Shape& sh : b->shapes) {
         a.list_base = &bw->off[sh.cls];
         a.list_n = &bw->count[sh.cls];
         BCK(launch_subgraphs_persistent(a, b->words, sh.cluster, sh.threads, sh.per, sh.grid, s));
         ++launches;
     }
-    k_job_finalize<<<b->n_jobs, 256, 0, s>>>(b->bucket_cnt.as<uint32_t>(), b->g_shift, b->jobs.as<JobOut>());
+    k_job_finalize<<<b->n_jobs, 256, 0, s>>>(b->bucket_cnt.as<uint32_t>(), b->g_shift, b->jobs.as<JobOut>(),
+                                             b->job_cur.as<unsigned long long>());
     ++launches;
     BCK(cudaGetLastError());
     b->launches_per_run = launches;
@@ -713,7 +723,7 @@ void cfg_batch_destroy(cfg_batch* b) {
     DevBuf* bufs[] = {&b->packed, &b->frag_off, &b->frag_off_rel, &b->frag_len, &b->frag_gbase, &b->job_pos, &b->job_nbases,
                       &b->flat, &b->hist, &b->bw, &b->bucket_off, &b->inst, &b->fill, &b->partials, &b->recs, &b->list,
                       &b->tab_off, &b->tab_cap, &b->arena, &b->jobs, &b->fasta, &b->lm_text, &b->lm, &b->retry, &b->counters,
-                      &b->bucket_cnt};
+                      &b->bucket_cnt, &b->job_cur};
     for (DevBuf* x : bufs) x->release();
     b->h_fasta.release(); b->h_text.release(); b->h_lm.release();
     if (b->plain) cfg_destroy(b->plain);

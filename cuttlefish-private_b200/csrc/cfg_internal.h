@@ -79,14 +79,18 @@ struct StateOut {                // mirrors cfg_state
 };
 
 // Output regions and counters of one job of a batch.  The six counters from
-// `vertices` on are laid out as the first six of Counters.
+// `vertices` on are laid out as the first six of Counters.  The cursors the
+// subgraph kernels advance live apart, one 128-byte line per job (JOB_CUR_STRIDE
+// words: fasta, lm-tig text, lm-tig records), so the region fields every task
+// reads are not on lines under atomic traffic.
 struct JobOut {
     unsigned long long fasta_off, fasta_cap, lm_text_off, lm_text_cap, lm_off, lm_cap;   // regions
-    unsigned long long fasta_used, lm_text_used, lm_used;                                // cursors
+    unsigned long long fasta_used, lm_text_used, lm_used;                                // final cursors
     unsigned long long vertices, isolated, phantom, trivial, icc, lmtig;
     unsigned long long records, instances;
     uint32_t err, pad;   // DERR_OUT_OVERFLOW / DERR_NO_ROOM: redo this job alone
 };
+constexpr uint32_t JOB_CUR_STRIDE = 16;
 
 struct Counters {                // device-side counters of the subgraph phase
     unsigned long long vertices, isolated, phantom, trivial, icc, lmtig;
@@ -119,12 +123,24 @@ struct SubgraphArgs {
     const uint32_t* list_n;
     // batch: bucket b belongs to job b >> g_shift and writes to jobs[b >> g_shift]; nullptr: one job
     JobOut* jobs;
+    unsigned long long* job_cur;  // batch: JOB_CUR_STRIDE words per job
+    // one job: the output arenas are cut into `stripes` (a power of two) slices of
+    // fasta_cap / lm_text_cap / lm_cap each; subgraph g writes to slice g % stripes and
+    // advances that slice's cursors (JOB_CUR_STRIDE words each) -- no contended cursor
+    unsigned long long* stripe_cur;
+    uint32_t stripes;
     uint32_t g_shift;
     uint32_t record_clocks;      // accumulate per-phase SM cycles into cnt->phase_cycles
     // batch: per-subgraph vertices, isolated, phantom, trivial, icc (5 words each),
     // summed per job after the run; nullptr: counters go to the sink
     uint32_t* bucket_cnt;
 };
+
+constexpr uint32_t OUT_STRIPES = 32;
+
+// Adds each stripe's label-text base to its lm-tigs' label offsets (one job's run).
+void launch_stripe_fixup(LmtigOut* lm, uint64_t lm_slice, const unsigned long long* lm_used,
+                         const unsigned long long* text_base, uint32_t stripes, cudaStream_t s);
 
 // bytes per table slot: k-mer (8 per word) + state word (8) + meta (4) + work-list entry (4)
 __host__ __device__ inline uint32_t slot_bytes(int words) { return words == 1 ? 24u : 32u; }

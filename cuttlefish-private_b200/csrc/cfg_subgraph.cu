@@ -226,15 +226,19 @@ struct Sink {
 
 __device__ __forceinline__ void sink_for(const SubgraphArgs& a, uint32_t b, Sink& o) {
     if (a.jobs) {
-        JobOut& J = a.jobs[b >> a.g_shift];
-        o.fasta = a.fasta + J.fasta_off; o.fasta_cap = J.fasta_cap; o.fasta_cur = &J.fasta_used;
-        o.lm_text = a.lm_text + J.lm_text_off; o.lm_text_cap = J.lm_text_cap; o.lm_text_cur = &J.lm_text_used;
-        o.lm = a.lm + J.lm_off; o.lm_cap = J.lm_cap; o.lm_cur = &J.lm_used;
+        const uint32_t j = b >> a.g_shift;
+        JobOut& J = a.jobs[j];
+        unsigned long long* cur = a.job_cur + (size_t)j * JOB_CUR_STRIDE;
+        o.fasta = a.fasta + J.fasta_off; o.fasta_cap = J.fasta_cap; o.fasta_cur = cur;
+        o.lm_text = a.lm_text + J.lm_text_off; o.lm_text_cap = J.lm_text_cap; o.lm_text_cur = cur + 1;
+        o.lm = a.lm + J.lm_off; o.lm_cap = J.lm_cap; o.lm_cur = cur + 2;
         o.cnt = &J.vertices; o.oflow = &J.err; o.g = b & ((1u << a.g_shift) - 1);
     } else {
-        o.fasta = a.fasta; o.fasta_cap = a.fasta_cap; o.fasta_cur = &a.cnt->fasta_bytes;
-        o.lm_text = a.lm_text; o.lm_text_cap = a.lm_text_cap; o.lm_text_cur = &a.cnt->lm_bytes;
-        o.lm = a.lm; o.lm_cap = a.lm_cap; o.lm_cur = &a.cnt->lm_count;
+        const uint32_t st = b & (a.stripes - 1);
+        unsigned long long* cur = a.stripe_cur + (size_t)st * JOB_CUR_STRIDE;
+        o.fasta = a.fasta + st * a.fasta_cap; o.fasta_cap = a.fasta_cap; o.fasta_cur = cur;
+        o.lm_text = a.lm_text + st * a.lm_text_cap; o.lm_text_cap = a.lm_text_cap; o.lm_text_cur = cur + 1;
+        o.lm = a.lm + st * a.lm_cap; o.lm_cap = a.lm_cap; o.lm_cur = cur + 2;
         o.cnt = &a.cnt->vertices; o.oflow = a.err; o.g = b;
     }
 }
@@ -943,6 +947,16 @@ int occupancy_of(K kernel, uint32_t cluster, uint32_t threads, size_t bytes, siz
     return n;
 }
 
+__global__ void k_stripe_fixup(LmtigOut* lm, uint64_t lm_slice, const unsigned long long* __restrict__ lm_used,
+                               const unsigned long long* __restrict__ text_base, uint32_t stripes) {
+    for (uint32_t st = blockIdx.y; st < stripes; st += gridDim.y) {
+        const unsigned long long n = lm_used[st * JOB_CUR_STRIDE + 2];
+        const unsigned long long base = text_base[st];
+        for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n && i < lm_slice; i += (uint64_t)gridDim.x * blockDim.x)
+            lm[st * lm_slice + i].label_off += base;
+    }
+}
+
 uint32_t subgraph_max_per_cta(int words) { return words == 1 ? 4096 : 2048; }
 uint32_t subgraph_cluster_per_cta(int words) { return words == 1 ? 4096 : 2048; }
 
@@ -959,6 +973,11 @@ cudaError_t launch_subgraphs(const SubgraphArgs& a, int words, uint32_t cluster,
                           : launch_shared(k_subgraph_shared<2, LOCAL>, a, 1, threads, bytes, s, 0, max_table_bytes<2>());
     return words == 1 ? launch_shared(k_subgraph_shared<1, CLUSTER>, a, cluster, threads, bytes, s, 0, max_table_bytes<1>())
                       : launch_shared(k_subgraph_shared<2, CLUSTER>, a, cluster, threads, bytes, s, 0, max_table_bytes<2>());
+}
+
+void launch_stripe_fixup(LmtigOut* lm, uint64_t lm_slice, const unsigned long long* lm_used,
+                         const unsigned long long* text_base, uint32_t stripes, cudaStream_t s) {
+    k_stripe_fixup<<<dim3(64, stripes), 256, 0, s>>>(lm, lm_slice, lm_used, text_base, stripes);
 }
 
 int subgraph_occupancy(int words, uint32_t cluster, uint32_t threads, uint32_t per) {

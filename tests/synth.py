@@ -42,7 +42,8 @@ def adversarial(rng, n, k):
         s[b:b + int(rng.integers(1, 4))] = bytes(rng.choice([b"N", b"n", b"-", b"R", b"Y"]))
     for _ in range(max(1, n // 1000)):                     # lowercase
         b = int(rng.integers(0, n))
-        s[b] = ord(chr(s[b]).lower()) if chr(s[b]) in "ACGT" else s[b]
+        if b < len(s):
+            s[b] = ord(chr(s[b]).lower()) if chr(s[b]) in "ACGT" else s[b]
     return bytes(s[:n]).decode()
 
 
