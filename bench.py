@@ -1,19 +1,20 @@
 #!/usr/bin/env python3
-"""Throughput of the B200 compaction hot path (partition -> subgraph build -> local walk).
+"""Throughput of the B200 compaction path (partition -> subgraph build -> local walk -> collation).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
-One JSON line on rank 0.  The metric is input bases per second to the
-per-subgraph unitig outputs (trivial maximal unitigs as FASTA, lm-tigs with
-their discontinuity edges), bit-identical to the CPU restatement of the
-reference.  Default workload "reads30x": 10M x 150 bp reads at 0.5% error from
-both strands of a 50 Mbp genome with 2% repeats, k=31, cutoff 2 (seeded
-synthetic data of that shape).
+One JSON line on rank 0.  The metric is input bases per second to the final
+maximal unitigs (the FASTA content `cuttlefish build` writes), bit-identical to
+the CPU restatement of the reference.  Default workload "reads30x": 10M x 150 bp
+reads at 0.5% error from both strands of a 50 Mbp genome with 2% repeats, k=31,
+cutoff 2 (seeded synthetic data of that shape).
 
-  value : device time of cfg_run with the packed input resident in HBM
-          (CUDA events on the library's stream, whole run incl. host planning).
+  value : device time of cfg_run + cfg_unitigs' collation with the packed input
+          resident in HBM (CUDA events on the library's stream, host planning included).
   e2e   : the same work through the C ABI from pinned host buffers:
-          cfg_submit_packed (H2D) + cfg_run + cfg_fetch (D2H of every output).
+          cfg_submit_packed (H2D) + cfg_run + cfg_unitigs (collation + D2H of the unitigs).
+The line also carries the batched-vs-plain comparison (1000 genomes) and the
+serving comparison (Poisson arrivals, p50/p99 latency); see --workload batch|serve.
 Each GPU runs its own replica of the job (the path has no cross-GPU exchange
 step on one node): value = all ranks' bases / max over ranks of the time.
 """
@@ -537,7 +538,7 @@ def main():
     k, l, cutoff, load_pct, desc = WORKLOADS[name]
     if args.table_load_pct:
         load_pct = args.table_load_pct
-    metric = "input bases/s to bit-exact unitigs (per-subgraph maximal unitigs + lm-tigs), 1 B200"
+    metric = "input bases/s to bit-exact maximal unitigs (the <o>.fa content), 1 B200"
     config = {"workload": name, "description": desc, "k": k, "l": l, "cutoff": cutoff, "graph_count": 16384,
               "table_load_pct": load_pct,
               "l2_flush": "inputs larger than L2 (packed input and tables exceed 126 MB)"}
@@ -566,11 +567,12 @@ def main():
     packed = cfgpu.PackedInput(None, k, pinned=True, data_offsets=(data, offs, n_rec))
     cx = cfgpu.Compactor(k, l, cutoff, 16384, device=local if world > 1 else 0, table_load_pct=load_pct)
 
-    # e2e: H2D + run + D2H through the C ABI, host buffers pinned
+    # e2e: H2D + run + device collation + D2H of the final unitigs, through the C ABI,
+    # host buffers pinned
     def e2e_step():
         cx.submit(packed)
         cx.run()
-        return cx.fetch_raw()
+        return cx.unitigs_raw()
 
     for _ in range(args.warmup):
         e2e_step()
@@ -578,25 +580,27 @@ def main():
     e2e_times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        res = e2e_step()
+        _, fin_bytes, n_units, _ = e2e_step()
         e2e_times.append(time.perf_counter() - t0)
-    counts = res.counts
+    counts = cx.counts()
     barrier(pg)
     h2d = packed.p.n_bases // 4 + 12 * packed.p.n_frags
-    d2h = counts.fasta_bytes + counts.lmtig_bytes + 48 * counts.n_lmtig + 96
+    d2h = fin_bytes + 96
 
     # value: input resident in HBM, device-timed
     cx.submit(packed)
     for _ in range(args.warmup):
         cx.run()
     barrier(pg)
-    run_ms, sub_ms, part_ms, scat_ms = [], [], [], []
+    run_ms, sub_ms, part_ms, scat_ms, col_ms = [], [], [], [], []
     launches = 0
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             cx.run()
             t = cx.timings()
-            part_ms.append(t[0]); scat_ms.append(t[1]); sub_ms.append(t[2]); run_ms.append(t[3])
+            _, _, _, ums = cx.unitigs_raw()
+            part_ms.append(t[0]); scat_ms.append(t[1]); sub_ms.append(t[2]); run_ms.append(t[3] + ums)
+            col_ms.append(ums)
             launches += cx.counts().n_launches
     barrier(pg)
     counts = cx.counts()
@@ -664,10 +668,13 @@ def main():
             "job_roofline": {"algorithmic_bytes": job_bytes, "achieved_gbs": job_bytes / (total_ms / args.steps / 1e3) / 1e9,
                              "frac": job_bytes / (total_ms / args.steps / 1e3) / 1e9 / peak},
             "phases_ms": {"partition": statistics.mean(part_ms), "scatter": statistics.mean(scat_ms),
-                          "subgraphs": statistics.mean(sub_ms), "run": statistics.mean(run_ms)},
+                          "subgraphs": statistics.mean(sub_ms), "collate": statistics.mean(col_ms),
+                          "run": statistics.mean(run_ms)},
+            "unitigs": {"n": n_units, "fasta_bytes": fin_bytes,
+                        "distinct_kmers": (fin_bytes - 4 * n_units) - n_units * (k - 1)},
             "counts": {n: getattr(counts, n) for n, _ in cfgpu.Counts._fields_},
             "subgraph_phase_cycles": dict(zip(["build", "terminations", "paths", "cycles", "tail"], phase_cycles)),
-            "distinct_kmers_per_s": None,
+            "distinct_kmers_per_s": ((fin_bytes - 4 * n_units) - n_units * (k - 1)) / (total_ms_max / args.steps / 1e3),
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
             "batched_vs_plain": batched,

@@ -47,7 +47,9 @@ struct cfg_ctx {
     // plan
     DevBuf list, tab_off, tab_cap, arena;
     // outputs
-    DevBuf fasta, lm_text, lm, dump, retry, counters, stripe_cur, stripe_base;
+    DevBuf fasta, lm_text, lm, dump, retry, counters, stripe_cur, stripe_base, ut_lmbase, cyc_lm, cyc_text, cyc_cnt;
+    UnitigBuffers ub;
+    HostBuf h_unitigs;
     uint64_t fasta_cap = 0, lm_text_cap = 0, lm_cap = 0, dump_cap = 0;   // per output stripe
     // per stripe, after a run: used FASTA bytes, label bytes, lm-tig records
     uint64_t s_fasta[OUT_STRIPES] = {}, s_text[OUT_STRIPES] = {}, s_lm[OUT_STRIPES] = {};
@@ -555,6 +557,84 @@ int cfg_dump_records(cfg_ctx* c, cfg_record_dump* out) {
     return CFG_OK;
 }
 
+int cfg_unitigs(cfg_ctx* c, const char** fasta, uint64_t* bytes, uint64_t* n_unitigs, float* device_ms) {
+    if (!c || !fasta || !bytes) return CFG_ERR_BAD_INPUT;
+    if (!c->have_run) return fail(c, CFG_ERR_STATE, "no completed run");
+    CK(cudaSetDevice(c->device));
+    const cfg_counts& n = c->counts;
+    unsigned long long lb[OUT_STRIPES], acc = 0;
+    for (uint32_t st = 0; st < OUT_STRIPES; ++st) { lb[st] = acc; acc += c->s_lm[st]; }
+    if (!c->ut_lmbase.ensure(sizeof(lb)) || !c->cyc_cnt.ensure(16)) return fail(c, CFG_ERR_OOM, "collation buffers");
+    CK(cudaMemcpyAsync(c->ut_lmbase.p, lb, sizeof(lb), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(&c->misc.as<MiscWords>()->err, 0, sizeof(uint32_t), c->stream));
+    CK(cudaEventRecord(c->ev[0], c->stream));
+    UnitigInput in{};
+    in.lm = c->lm.as<LmtigOut>(); in.lm_slice = c->lm_cap;
+    in.text = c->lm_text.as<char>(); in.text_slice = c->lm_text_cap;
+    in.stripe_cur = c->stripe_cur.as<unsigned long long>();
+    in.lm_base = c->ut_lmbase.as<unsigned long long>(); in.text_base = c->stripe_base.as<unsigned long long>();
+    in.stripes = c->stripes; in.k = c->p.k; in.n = n.n_lmtig; in.err = &c->misc.as<MiscWords>()->err;
+    UnitigResult res{};
+    int rc = collate_device(in, c->ub, c->stream, res);
+    if (rc == CFG_ERR_OOM) return fail(c, rc, "collation buffers");
+    if (rc) return fail(c, rc, std::string("collation: ") + cudaGetErrorString(cudaGetLastError()));
+    MiscWords m{};
+    CK(cudaMemcpyAsync(&m, c->misc.p, sizeof(m), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (m.err & DERR_BAD_GRAPH) return fail(c, CFG_ERR_STATE, "lm-tig ends do not form a valid discontinuity graph");
+    if (m.err & DERR_CAS_LIMIT) return fail(c, CFG_ERR_WALK_LIMIT, "vertex-table wait exceeded its bound");
+    // lm-tigs on closed chains: joined on the host (they need the rotation rule)
+    std::string cyc_fa;
+    uint64_t cyc_units = 0;
+    if (res.n_cycle_lmtigs) {
+        unsigned long long cnt[2] = {0, 0};
+        CK(cudaMemsetAsync(c->cyc_cnt.p, 0, 16, c->stream));
+        rc = collate_cycles_device(c->ub, n.n_lmtig, nullptr, nullptr, c->cyc_cnt.as<unsigned long long>(), c->stream);
+        if (rc) return fail(c, rc, "cycle sizing");
+        CK(cudaMemcpyAsync(cnt, c->cyc_cnt.p, 16, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (!c->cyc_lm.ensure(sizeof(LmtigOut) * (cnt[0] + 1)) || !c->cyc_text.ensure(cnt[1] + 1))
+            return fail(c, CFG_ERR_OOM, "cycle buffers");
+        CK(cudaMemsetAsync(c->cyc_cnt.p, 0, 16, c->stream));
+        rc = collate_cycles_device(c->ub, n.n_lmtig, c->cyc_lm.as<LmtigOut>(), c->cyc_text.as<char>(),
+                                   c->cyc_cnt.as<unsigned long long>(), c->stream);
+        if (rc) return fail(c, rc, "cycle gather");
+        std::vector<cfg_lmtig> hl(cnt[0]);
+        std::string ht(cnt[1], '\0');
+        if (cnt[0]) CK(cudaMemcpyAsync(hl.data(), c->cyc_lm.p, sizeof(cfg_lmtig) * cnt[0], cudaMemcpyDeviceToHost, c->stream));
+        if (cnt[1]) CK(cudaMemcpyAsync(&ht[0], c->cyc_text.p, cnt[1], cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        char* out = nullptr;
+        uint64_t ob = 0, nu = 0, nc = 0;
+        rc = cfg_collate_lmtigs(c->p.k, hl.data(), cnt[0], ht.data(), &out, &ob, &nu, &nc);
+        if (rc) return fail(c, rc, "cycle collation");
+        cyc_fa.assign(out, ob);
+        cfg_free(out);
+        cyc_units = nu;
+    }
+    CK(cudaEventRecord(c->ev[2], c->stream));   // device collation done
+    // trivial unitigs (per stripe) + collated unitigs + cycles, to host memory
+    const uint64_t total = n.fasta_bytes + res.bytes + cyc_fa.size();
+    if (!c->h_unitigs.ensure(total + 1)) return fail(c, CFG_ERR_OOM, "pinned unitig buffer");
+    char* h = (char*)c->h_unitigs.p;
+    uint64_t at = 0;
+    for (uint32_t st = 0; st < OUT_STRIPES; ++st) {
+        if (c->s_fasta[st])
+            CK(cudaMemcpyAsync(h + at, c->fasta.as<char>() + st * c->fasta_cap, c->s_fasta[st], cudaMemcpyDeviceToHost, c->stream));
+        at += c->s_fasta[st];
+    }
+    if (res.bytes) CK(cudaMemcpyAsync(h + at, c->ub.out, res.bytes, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    at += res.bytes;
+    if (!cyc_fa.empty()) std::memcpy(h + at, cyc_fa.data(), cyc_fa.size());
+    if (device_ms) { float ms = 0; cudaEventElapsedTime(&ms, c->ev[0], c->ev[2]); *device_ms = ms; }
+    *fasta = h;
+    *bytes = total;
+    if (n_unitigs) *n_unitigs = n.n_trivial + res.n_units + cyc_units;
+    return CFG_OK;
+}
+
 int cfg_last_timings(cfg_ctx* c, float out_ms[4]) {
     if (!c || !out_ms) return CFG_ERR_BAD_INPUT;
     if (!c->have_run) return fail(c, CFG_ERR_STATE, "no completed run");
@@ -576,9 +656,12 @@ void cfg_destroy(cfg_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->parse.release();
+    c->ub.release();
+    c->h_unitigs.release();
     DevBuf* bufs[] = {&c->packed, &c->frag_off, &c->frag_len, &c->text, &c->flat, &c->hist, &c->misc, &c->bucket_off, &c->inst,
                       &c->fill, &c->recs, &c->list, &c->tab_off, &c->tab_cap, &c->arena, &c->fasta, &c->lm_text,
-                      &c->lm, &c->dump, &c->retry, &c->counters, &c->stripe_cur, &c->stripe_base};
+                      &c->lm, &c->dump, &c->retry, &c->counters, &c->stripe_cur, &c->stripe_base,
+                      &c->ut_lmbase, &c->cyc_lm, &c->cyc_text, &c->cyc_cnt};
     for (DevBuf* b : bufs) b->release();
     c->h_fasta.release(); c->h_lm_text.release(); c->h_lm.release();
     for (auto& e : c->ev) if (e) cudaEventDestroy(e);

@@ -80,6 +80,53 @@ struct ParseBuffers {
     }
 };
 
+struct LmtigOut;
+
+// Device collation (cfg_unitig.cu): the run's striped lm-tigs ...
+struct UnitigInput {
+    const LmtigOut* lm; uint64_t lm_slice;        // stripe st's records at lm + st * lm_slice
+    const char* text; uint64_t text_slice;        // and their labels at text + st * text_slice
+    const unsigned long long* stripe_cur;         // per stripe: [2] records (JOB_CUR_STRIDE words each)
+    const unsigned long long* lm_base;            // per stripe: records before it (device)
+    const unsigned long long* text_base;          // per stripe: label bytes before it (device)
+    uint32_t stripes, k;
+    uint64_t n;                                   // records over all stripes
+    uint32_t* err;
+};
+// ... the buffers it works in ...
+struct UnitigBuffers {
+    DevBuf b_lm, b_label, b_tab, b_partner, b_P0, b_P1, b_R0, b_R1, b_A0, b_A1, b_fin, b_off, b_words, b_out;
+    LmtigOut* lm = nullptr;
+    const char** label = nullptr;
+    void* tab = nullptr;
+    uint64_t tab_n = 0;
+    uint32_t* partner = nullptr;
+    uint32_t* P[2] = {nullptr, nullptr};
+    uint32_t* R[2] = {nullptr, nullptr};
+    unsigned long long* A[2] = {nullptr, nullptr};
+    uint32_t* fin = nullptr;
+    unsigned long long* out_off = nullptr;
+    unsigned long long* words = nullptr;
+    char* out = nullptr;
+    bool ensure(uint64_t n);
+    bool ensure_out(uint64_t bytes) {
+        if (!b_out.ensure(bytes)) return false;
+        out = b_out.as<char>();
+        return true;
+    }
+    void release() {
+        DevBuf* all[] = {&b_lm, &b_label, &b_tab, &b_partner, &b_P0, &b_P1, &b_R0, &b_R1, &b_A0, &b_A1, &b_fin, &b_off,
+                         &b_words, &b_out};
+        for (DevBuf* b : all) b->release();
+    }
+};
+// ... and what it produced: `bytes` of FASTA records at out, the unitigs among them,
+// and the lm-tigs left on closed chains (for the host).
+struct UnitigResult { uint64_t bytes, n_units, n_cycle_lmtigs; uint32_t rounds; };
+int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, UnitigResult& res);
+int collate_cycles_device(const UnitigBuffers& ub, uint64_t n, LmtigOut* out, char* text, unsigned long long* cnt,
+                          cudaStream_t s);
+
 // FASTA (fastq = 0) or FASTQ text in device memory -> the packed stream and fragment
 // table in `pb` (cfg_parse.cu).  Synchronises the stream twice (two counts).
 int parse_text_device(const uint8_t* d_text, uint64_t bytes, int fastq, uint32_t k, ParseBuffers& pb, cudaStream_t s);

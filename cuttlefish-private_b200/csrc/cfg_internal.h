@@ -28,6 +28,7 @@ enum : uint32_t {
     DERR_CAS_LIMIT = 16u,      // a CAS retry loop exceeded its bound (bug guard)
     DERR_DUMP_OVERFLOW = 32u,  // state dump buffer too small (recoverable)
     DERR_NO_ROOM = 64u,        // batch: a job's output regions or tables did not fit the arenas
+    DERR_BAD_GRAPH = 128u,     // lm-tig ends that cannot meet (three at a vertex, or two on one side)
 };
 
 struct PartitionArgs {

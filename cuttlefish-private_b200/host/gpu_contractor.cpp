@@ -94,6 +94,32 @@ Records read_records(const std::vector<std::string>& paths) {
     return r;
 }
 
+std::string read_text(const std::vector<std::string>& paths, bool& mixed) {
+    std::vector<std::pair<uint64_t, std::string>> by_size;
+    for (const auto& p : paths) {
+        std::error_code ec;
+        const auto sz = std::filesystem::file_size(p, ec);
+        if (ec) throw cfg_error("cannot open input " + p, CFG_ERR_BAD_INPUT);
+        by_size.emplace_back(sz, p);
+    }
+    std::stable_sort(by_size.begin(), by_size.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+    std::string all;
+    int fmt = -1;   // 1 FASTQ, 0 FASTA
+    mixed = false;
+    for (const auto& e : by_size) {
+        std::string t = slurp(e.second);
+        size_t i = 0;
+        while (i < t.size() && (t[i] == '\n' || t[i] == '\r')) ++i;
+        if (i == t.size()) continue;
+        const int f = t[i] == '@';
+        if (fmt >= 0 && f != fmt) { mixed = true; return std::string(); }
+        fmt = f;
+        all += t;
+        if (all.back() != '\n') all += '\n';
+    }
+    return all;
+}
+
 uint64_t write_unitigs(const std::string& path, uint32_t k, const cfg_results& r) {
     char* stitched = nullptr;
     uint64_t bytes = 0, n_units = 0, n_cycles = 0;
@@ -110,19 +136,26 @@ uint64_t write_unitigs(const std::string& path, uint32_t k, const cfg_results& r
 
 void construct_gpu(const Build_Params& p) {
     const auto t0 = std::chrono::steady_clock::now();
-    Records recs = read_records(p.seq_paths);
-    cfg_packed packed{};
-    int rc = cfg_pack_records(recs.seq.data(), recs.off.data(), recs.off.size() - 1, p.k, 1, &packed);
-    if (rc != CFG_OK) throw cfg_error("cfg_pack_records failed", rc);
-    std::cerr << "Read " << recs.off.size() - 1 << " records, " << packed.n_bases << " bases in fragments. Time taken: "
-              << since(t0) << " seconds.\n";
-    {
-        std::string().swap(recs.seq);
-    }
+    bool mixed = false;
+    std::string text = read_text(p.seq_paths, mixed);
     Subgraphs_Manager G(p.k, p.min_len, p.effective_cutoff(), p.device,
                         p.table_load_pct ? p.table_load_pct : (p.is_read_graph ? 15u : 0u));
+    cfg_packed packed{};
+    if (!mixed) {
+        // parsed on the device (records, line joins, fragments)
+        G.partition_text(text.data(), text.size());
+        std::cerr << "Read " << text.size() << " bytes of " << p.seq_paths.size()
+                  << " input file(s); parsed on the device. Time taken: " << since(t0) << " seconds.\n";
+    } else {
+        Records recs = read_records(p.seq_paths);
+        int rc = cfg_pack_records(recs.seq.data(), recs.off.data(), recs.off.size() - 1, p.k, 1, &packed);
+        if (rc != CFG_OK) throw cfg_error("cfg_pack_records failed", rc);
+        std::cerr << "Read " << recs.off.size() - 1 << " records, " << packed.n_bases << " bases in fragments. Time taken: "
+                  << since(t0) << " seconds.\n";
+        G.partition(packed);
+    }
+    std::string().swap(text);
     const auto t1 = std::chrono::steady_clock::now();
-    G.partition(packed);
     G.finalize();
     G.process();
     float ms[4] = {0, 0, 0, 0};
@@ -132,11 +165,20 @@ void construct_gpu(const Build_Params& p) {
     std::cerr << "Trivial maximal unitig count: " << G.trivial_mtig_count() << ".\n";
     std::cerr << "Isolated cycle count: " << G.icc_count() << ".\n";
     std::cerr << "lm-tig count: " << G.results().counts.n_lmtig << ".\n";
-    cfg_packed_free(&packed);
+    if (packed.words) cfg_packed_free(&packed);
     const auto t2 = std::chrono::steady_clock::now();
-    const uint64_t units = write_unitigs(p.output_file_path(), p.k, G.results());
+    // the discontinuity-graph phases, on the device
+    const char* fa = nullptr;
+    uint64_t bytes = 0, units = 0;
+    float ums = 0;
+    const int rc = cfg_unitigs(G.context(), &fa, &bytes, &units, &ums);
+    if (rc != CFG_OK) throw cfg_error(std::string("cfg_unitigs: ") + cfg_last_error_string(G.context()), rc);
+    std::ofstream out(p.output_file_path(), std::ios::binary);
+    if (!out) throw cfg_error("cannot write " + p.output_file_path(), CFG_ERR_BAD_INPUT);
+    out.write(fa, (std::streamsize)bytes);
+    if (!out) throw cfg_error("error writing " + p.output_file_path(), CFG_ERR_BAD_INPUT);
     std::cerr << "Collated " << units << " maximal unitigs into " << p.output_file_path() << ". Time taken: "
-              << since(t2) << " seconds.\n";
+              << since(t2) << " seconds (device " << ums / 1e3 << ").\n";
     std::cerr << "Device phases and transfers: " << std::chrono::duration<double>(t2 - t1).count()
               << " seconds; total: " << since(t0) << " seconds.\n";
 }

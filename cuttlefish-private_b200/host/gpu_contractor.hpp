@@ -63,11 +63,18 @@ public:
     void partition(const cfg_packed& in) {
         check(cfg_submit_packed(ctx_, in.words, in.n_bases, in.frag_off, in.frag_len, in.n_frags), "cfg_submit_packed");
     }
+    // The same from FASTA / FASTQ text, parsed on the device.
+    void partition_text(const char* text, uint64_t bytes) { check(cfg_submit_text(ctx_, text, bytes), "cfg_submit_text"); }
     void finalize() {}   // the device buckets need no flush
     // Subgraphs_Manager::process: build and contract every subgraph.
     void process() {
         check(cfg_run(ctx_), "cfg_run");
+        check(cfg_fetch_counts(ctx_, &res_.counts), "cfg_fetch_counts");
+    }
+    // The outputs of process() in host memory (trivial unitigs, lm-tigs).
+    const cfg_results& fetch() {
         check(cfg_fetch(ctx_, &res_), "cfg_fetch");
+        return res_;
     }
     uint64_t trivial_mtig_count() const { return res_.counts.n_trivial; }
     uint64_t icc_count() const { return res_.counts.n_icc; }
@@ -95,6 +102,10 @@ Records read_records(const std::vector<std::string>& paths);
 
 // Joins lm-tigs into maximal unitigs and writes <prefix>.fa; returns unitig count.
 uint64_t write_unitigs(const std::string& path, uint32_t k, const cfg_results& r);
+
+// The inputs' text joined into one FASTA or one FASTQ text (files largest first,
+// each ending in a newline); empty when the files mix the two formats.
+std::string read_text(const std::vector<std::string>& paths, bool& mixed);
 
 // T_App<k>: drop-in for dBG_Contractor<k> in Application<MAX_K, T_App>.
 template <uint16_t k>

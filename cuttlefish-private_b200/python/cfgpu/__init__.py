@@ -118,6 +118,8 @@ SIGNATURES = {
                                           ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     "cfg_free": (None, [ctypes.c_void_p]),
     "cfg_submit_text": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64]),
+    "cfg_unitigs": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_uint64),
+                                   ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_float)]),
     "cfg_input_counts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     "cfg_copy_input": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cfg_pack_records": (ctypes.c_int, [ctypes.c_char_p, U64P, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int,
@@ -301,6 +303,18 @@ class Compactor:
         r = Results()
         _check(self.lib, self.ctx, self.lib.cfg_fetch(self.ctx, ctypes.byref(r)), "cfg_fetch")
         return results_to_python(r)
+
+    def unitigs_raw(self):
+        """cfg_unitigs: -> (pointer, bytes, n_unitigs, device ms); the text stays in the context."""
+        p, nb, nu, ms = ctypes.c_void_p(), ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_float()
+        _check(self.lib, self.ctx, self.lib.cfg_unitigs(self.ctx, ctypes.byref(p), ctypes.byref(nb), ctypes.byref(nu),
+                                                        ctypes.byref(ms)), "cfg_unitigs")
+        return p.value, nb.value, nu.value, ms.value
+
+    def unitigs(self):
+        """Final maximal unitigs joined on the device: (FASTA bytes, n_unitigs)."""
+        p, nb, nu, _ = self.unitigs_raw()
+        return (ctypes.string_at(p, nb) if nb else b""), nu
 
     def states(self):
         d = StateDump()

@@ -182,6 +182,15 @@ int cfg_collate_lmtigs(uint32_t k, const cfg_lmtig* lmtigs, uint64_t n_lmtigs, c
                        char** out, uint64_t* out_bytes, uint64_t* n_unitigs, uint64_t* n_cycles);
 void cfg_free(void* p);
 
+/* The last run's final maximal unitigs, joined on the device: trivial unitigs and
+ * the lm-tigs collated (the discontinuity-graph phases of dBG_Contractor::construct,
+ * src/dBG_Contractor.cpp:73-101, as cfg_collate_lmtigs does on the host; lm-tigs that
+ * close into cycles are joined on the host).  FASTA text ">0\nSEQ\n", each unitig in
+ * the reference's canonical orientation: the <output>.fa content.  The text is in
+ * host memory owned by the context, valid until the next run; device_ms (optional)
+ * is the device time of the collation (the copy to the host excluded). */
+int cfg_unitigs(cfg_ctx* ctx, const char** fasta, uint64_t* bytes, uint64_t* n_unitigs, float* device_ms);
+
 /* Profiling aid: SM clock cycles of the last run's subgraph kernels, summed over
  * CTAs, per phase: [0] table build, [1] side terminations, [2] path walks,
  * [3] cycle walks, [4] state dump and counters. */

@@ -138,3 +138,31 @@ def test_final_unitigs_equal_global_oracle(k, l, c, seed):
     got = orc.fasta_multiset(fasta) + orc.fasta_multiset(stitched)
     want = orc.OracleRun(recs, k, l, c, 1).fasta_records()
     assert got == want
+
+
+@pytest.mark.parametrize("k,l,c,G,seed", [(31, 20, 1, 16384, 41), (31, 20, 2, 16384, 42), (63, 20, 1, 16384, 43),
+                                          (15, 7, 1, 64, 44), (31, 20, 1, 4, 45), (9, 4, 1, 16, 46)])
+def test_device_unitigs(k, l, c, G, seed):
+    """cfg_unitigs (lm-tigs joined on the device) == host collation == the global maximal unitigs."""
+    rng = np.random.default_rng(seed)
+    if c == 2:
+        g = synth.genome_with_repeats(rng, 30_000, n_copies=5, n_pal=3)
+        recs = synth.reads(rng, g, 3_000)
+    else:
+        recs = [synth.genome_with_repeats(rng, 40_000, n_copies=6, n_pal=4)] + \
+               [synth.adversarial(rng, 10_000, k) for _ in range(2)]
+        for L in (700, 3 * k, 5000):         # circular molecules: lm-tigs closing into cycles
+            s = synth.random_seq(rng, L)
+            recs.append(s + s[:k])
+        recs += ["ACGT" * 40, "AACAC" * 30, "A" * 100]
+    packed = cfgpu.PackedInput(recs, k)
+    with cfgpu.Compactor(k, l, c, G, table_load_pct=30 if c == 2 else 0) as cx:
+        cx.submit(packed)
+        cx.run()
+        counts, fasta, lms = cx.fetch()
+        dev, n_units = cx.unitigs()
+    stitched, n_st, _ = cfgpu.collate_lmtig_records(k, lms)
+    host = orc.fasta_multiset(fasta) + orc.fasta_multiset(stitched)
+    assert orc.fasta_multiset(dev) == host
+    assert n_units == counts.n_trivial + n_st
+    assert host == orc.OracleRun(recs, k, l, c, 1).fasta_records()
