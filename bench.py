@@ -96,10 +96,12 @@ def make_genomes(n_genomes):
 def bench_batch(args, pg, local, world, peak, with_cpu):
     """Batched form vs one plain launch per genome, on the same GPU and genomes.
 
-    One step = all genomes.  Plain: cfg_run per genome, input resident (device
-    time of each run summed) and end to end (submit from pinned memory + run +
-    fetch of every output).  Batched: one graph launch for all genomes (device
-    time), and end to end (submit + run + cfg_batch_job for every genome)."""
+    One step = all genomes, ending at every genome's final maximal unitigs.  Plain:
+    per genome cfg_run + cfg_unitigs, input resident (device time of each summed) and
+    end to end (submit from pinned memory + run + collation + copy of the unitigs).
+    Batched: one graph launch for all genomes + one collation of all their lm-tigs
+    (device time), and end to end (submit + run + collation + cfg_batch_job_unitigs
+    for every genome)."""
     import cfgpu
     k, l, cutoff = 31, 20, 1
     t0 = time.perf_counter()
@@ -111,14 +113,17 @@ def bench_batch(args, pg, local, world, peak, with_cpu):
 
     b = cfgpu.Batch(k, l, cutoff, 16384, device=local if world > 1 else 0)
     b.submit(packed)
-    tuning = b.tune() if not args.no_tune else cfgpu.BatchTuning(4, 512, 100, 0, 0.0)
+    tuning = b.tune_unitigs() if not args.no_tune else cfgpu.BatchTuning(4, 512, 100, 0, 0.0)
     for _ in range(warm):
         b.run()
+        b.unitigs()
     barrier(pg)
-    dev_ms = []
+    dev_ms, run_ms, col_ms = [], [], []
     for _ in range(steps):
         b.run()
-        dev_ms.append(b.info().device_ms)
+        r = b.info().device_ms
+        c = b.unitigs()
+        run_ms.append(r); col_ms.append(c); dev_ms.append(r + c)
     info = b.info()
     # plain launches on the same resident inputs
     cx = cfgpu.Compactor(k, l, cutoff, 16384, device=local if world > 1 else 0)
@@ -130,38 +135,41 @@ def bench_batch(args, pg, local, world, peak, with_cpu):
         for d in dev_inputs:
             cx.submit_device(*d)
             cx.run()
-            tot += cx.timings()[3]
+            _, _, _, ums = cx.unitigs_raw()
+            tot += cx.timings()[3] + ums
             if it == 1:
                 plain_launches += cx.counts().n_launches
         if it > 0:
             plain_ms.append(tot)
     barrier(pg)
+
     # end to end, host buffers
     def batch_e2e():
         b.submit(packed)
         b.run()
-        d2h = 0
+        b.unitigs()
+        d2h = units = 0
         for j in range(len(packed)):
-            r = b.job_raw(j)
-            d2h += r.counts.fasta_bytes + r.counts.lmtig_bytes + 48 * r.counts.n_lmtig
-        return d2h
+            _, nb, nu = b.job_unitigs_raw(j)
+            d2h += nb; units += nu
+        return d2h, units
 
     def plain_e2e():
-        d2h = 0
+        d2h = units = 0
         for p in packed:
             cx.submit(p)
             cx.run()
-            r = cx.fetch_raw()
-            d2h += r.counts.fasta_bytes + r.counts.lmtig_bytes + 48 * r.counts.n_lmtig
-        return d2h
+            _, nb, nu, _ = cx.unitigs_raw()
+            d2h += nb; units += nu
+        return d2h, units
 
     batch_e2e()
     plain_e2e()
     barrier(pg)
     be, pe = [], []
     for _ in range(steps):
-        t = time.perf_counter(); d2h = batch_e2e(); be.append(time.perf_counter() - t)
-        t = time.perf_counter(); plain_e2e(); pe.append(time.perf_counter() - t)
+        t = time.perf_counter(); d2h, units = batch_e2e(); be.append(time.perf_counter() - t)
+        t = time.perf_counter(); d2h_p, units_p = plain_e2e(); pe.append(time.perf_counter() - t)
     barrier(pg)
     b_dev = allreduce_max(pg, local, sum(dev_ms))
     p_dev = allreduce_max(pg, local, sum(plain_ms))
@@ -179,21 +187,26 @@ def bench_batch(args, pg, local, world, peak, with_cpu):
             at += o[1]
             n_s += 1
         cpu = {"value": at / dt, "unit": "bases/s", "cores": threads, "kind": "port",
-               "sample": f"first {n_s} genomes ({at} bases), each its own job", "seconds": round(dt, 2)}
+               "sample": f"first {n_s} genomes ({at} bases), each its own job, to lm-tigs (host collation not timed)",
+               "seconds": round(dt, 2)}
     out = {
         "workload": f"batch{len(packed)}",
         "description": f"{len(packed)} genomes, log-uniform 0.5-8 Mbp, GC 0.3-0.7, 1% repeats at 1%; k=31, cutoff 1, "
-                       "each genome its own job with its own outputs",
-        "n_genomes": len(packed), "bases": bases,
+                       "each genome its own job ending at its own final maximal unitigs",
+        "n_genomes": len(packed), "bases": bases, "unitigs": units,
+        "outputs_equal": units == units_p and d2h == d2h_p,
         "batched": {"value": world * bases * steps / (b_dev / 1e3), "unit": "bases/s", "ms_per_step": b_dev / steps,
+                    "graph_ms": statistics.mean(run_ms), "collate_ms": statistics.mean(col_ms),
                     "e2e": {"value": world * bases * steps / b_e2e, "ms_per_step": 1e3 * b_e2e / steps,
                             "h2d_bytes_per_step": bases // 4, "d2h_bytes_per_step": d2h},
                     "graph_launches_per_step": 1, "gpu_launches_per_step": int(info.kernels_per_run),
                     "jobs_redone_alone": int(info.n_redone),
                     "tuning": {"local_div": tuning.local_div, "cluster_threads": tuning.cluster_threads,
-                               "table_load_pct": tuning.table_load_pct, "tuned_ms": tuning.ms}},
+                               "table_load_pct": tuning.table_load_pct,
+                               "graph_count": tuning.graph_count or 16384, "tuned_ms": tuning.ms}},
         "plain": {"value": world * bases * steps / (p_dev / 1e3), "unit": "bases/s", "ms_per_step": p_dev / steps,
-                  "e2e": {"value": world * bases * steps / p_e2e, "ms_per_step": 1e3 * p_e2e / steps},
+                  "e2e": {"value": world * bases * steps / p_e2e, "ms_per_step": 1e3 * p_e2e / steps,
+                          "d2h_bytes_per_step": d2h_p},
                   "gpu_launches_per_step": plain_launches},
         "speedup_device": p_dev / b_dev, "speedup_e2e": p_e2e / b_e2e,
         "generation_s": round(gen_s, 1),
@@ -204,182 +217,6 @@ def bench_batch(args, pg, local, world, peak, with_cpu):
     for p in packed:
         p.close()
     return out
-
-
-def make_serving_mix(n_jobs, k, seed=5):
-    """The serving mix: half reference jobs (one record, log-uniform 0.5-50 Mbp), half
-    read jobs (1-5 M reads of 150 bp, 0.5% errors, both strands, coverage 20-40x of a
-    genome of reads*150/coverage bases).  Returns [(kind, PackedInput, cutoff, load)]."""
-    import random
-
-    import numpy as np
-
-    import cfgpu
-    lib = synth()
-    rnd = random.Random(seed)
-    jobs = []
-    for i in range(n_jobs):
-        if i % 2 == 0:
-            n = int(math.exp(rnd.uniform(math.log(0.5e6), math.log(50e6))))
-            g = ctypes.create_string_buffer(n)
-            lib.cfs_genome_n(n, 50000 + i, g)
-            p = cfgpu.PackedInput(None, k, pinned=True, data_offsets=(g, (ctypes.c_uint64 * 2)(0, n), 1))
-            jobs.append(("ref", p, 1, 100))
-        else:
-            n_reads = rnd.randint(1_000_000, 5_000_000)
-            cov = rnd.uniform(20, 40)
-            gl = int(n_reads * 150 / cov)
-            g = ctypes.create_string_buffer(gl)
-            lib.cfs_genome_n(gl, 60000 + i, g)
-            out = ctypes.create_string_buffer(n_reads * 150)
-            lib.cfs_reads(g, gl, n_reads, 150, 0.005, 70000 + i, out)
-            del g
-            offs = np.arange(0, (n_reads + 1) * 150, 150, dtype=np.uint64)
-            p = cfgpu.PackedInput(None, k, pinned=True,
-                                  data_offsets=(out, offs.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), n_reads))
-            del out, offs
-            jobs.append(("read", p, 2, 15))
-    return jobs
-
-
-def percentile(xs, q):
-    ys = sorted(xs)
-    if not ys:
-        return None
-    i = min(len(ys) - 1, max(0, int(math.ceil(q / 100 * len(ys))) - 1))
-    return ys[i]
-
-
-def bench_serve(args, local, world):
-    """Serving loop vs the plain path on the same GPU, same jobs, same Poisson arrivals.
-
-    The plain path serves FIFO, one job at a time (submit + run + fetch per job).  The
-    server (4 slots, small jobs batched) admits jobs as they arrive.  Latency = arrival
-    -> results on the host.  Rates are multiples of the plain path's service rate."""
-    import random
-
-    import cfgpu
-    k = 31
-    t0 = time.perf_counter()
-    jobs = make_serving_mix(args.serve_jobs, k)
-    gen_s = time.perf_counter() - t0
-    total_bases = sum(p.n_bases for _, p, _, _ in jobs)
-    ctxs = {}
-
-    def plain_ctx(c, load):
-        if (c, load) not in ctxs:
-            ctxs[(c, load)] = cfgpu.Compactor(k, 20, c, 16384, device=local if world > 1 else 0, table_load_pct=load)
-        return ctxs[(c, load)]
-
-    def plain_one(j):
-        _, p, c, load = jobs[j]
-        cx = plain_ctx(c, load)
-        cx.submit(p)
-        cx.run()
-        cx.fetch_raw()
-
-    for j in range(len(jobs)):           # warm: every context grown to its largest job
-        plain_one(j)
-    t = time.perf_counter()
-    for j in range(len(jobs)):
-        plain_one(j)
-    seq_s = time.perf_counter() - t
-    mu = len(jobs) / seq_s               # plain service rate, jobs/s
-
-    def arrivals(lam, seed):
-        r = random.Random(seed)
-        at, out = 0.0, []
-        for _ in jobs:
-            out.append(at)
-            at += r.expovariate(lam)
-        return out
-
-    def run_plain(arr):
-        start = time.perf_counter()
-        lat, done = [], 0.0
-        for j, a in enumerate(arr):
-            now = time.perf_counter() - start
-            if now < a:
-                time.sleep(a - now)
-            plain_one(j)
-            done = time.perf_counter() - start
-            lat.append(done - a)
-        return lat, done
-
-    srv = cfgpu.Server(device=local if world > 1 else 0, slots=4, batch_max_bases=64_000_000,
-                       small_job_bases=4_000_000)
-
-    def run_server(arr):
-        start = time.perf_counter()
-        tickets = [None] * len(arr)
-
-        submitted = threading.Semaphore(0)
-
-        def submitter():
-            for j, a in enumerate(arr):
-                now = time.perf_counter() - start
-                if now < a:
-                    time.sleep(a - now)
-                _, p, c, load = jobs[j]
-                tickets[j] = srv.submit(p, k, 20, c, table_load_pct=load)
-                submitted.release()
-
-        th = threading.Thread(target=submitter)
-        th.start()
-        lat, groups, done = [], [], []
-        for _ in range(len(arr)):          # completion order: results are released as soon as read
-            submitted.acquire()            # one more job is in the server
-            t, _, tm = srv.wait_any_raw()
-            srv.release(t)
-            lat.append(tm.latency_s)
-            groups.append(tm.group_jobs)
-            done.append(time.perf_counter() - start)
-        th.join()
-        return lat, max(done), groups
-
-    # warm every worker's contexts on the largest job of each kind (all workers take one at once)
-    for kind in ("ref", "read"):
-        big = max((j for j in range(len(jobs)) if jobs[j][0] == kind), key=lambda j: jobs[j][1].n_bases, default=None)
-        if big is None:
-            continue
-        _, p, c, load = jobs[big]
-        ts = [srv.submit(p, k, 20, c, table_load_pct=load) for _ in range(4)]
-        for _ in ts:
-            t, _, _ = srv.wait_any_raw()
-            srv.release(t)
-    run_server(arrivals(mu * 4, 99))
-    rates = []
-    for f in args.serve_load:
-        arr = arrivals(mu * f, 1000 + int(100 * f))
-        sl, smk, groups = run_server(arr)
-        pl, pmk = run_plain(arr)
-        rates.append({
-            "load_vs_plain_capacity": f, "lambda_jobs_per_s": mu * f,
-            "server": {"p50_ms": 1e3 * percentile(sl, 50), "p99_ms": 1e3 * percentile(sl, 99),
-                       "mean_ms": 1e3 * statistics.mean(sl), "throughput_bases_per_s": total_bases / smk,
-                       "jobs_per_s": len(arr) / smk, "max_group": max(groups)},
-            "plain": {"p50_ms": 1e3 * percentile(pl, 50), "p99_ms": 1e3 * percentile(pl, 99),
-                      "mean_ms": 1e3 * statistics.mean(pl), "throughput_bases_per_s": total_bases / pmk,
-                      "jobs_per_s": len(arr) / pmk},
-        })
-    st = srv.stats()
-    srv.close()
-    for cx in ctxs.values():
-        cx.close()
-    for _, p, _, _ in jobs:
-        p.close()
-    return {
-        "workload": f"serve{len(jobs)}",
-        "description": "Poisson arrivals; half --ref jobs (0.5-50 Mbp log-uniform, cutoff 1), half --read jobs "
-                       "(1-5 M x 150 bp reads, 0.5% errors, 20-40x, cutoff 2); k=31; latency = arrival -> all "
-                       "outputs on the host",
-        "jobs": len(jobs), "bases": total_bases, "plain_service_jobs_per_s": mu,
-        "plain_sequential_bases_per_s": total_bases / seq_s,
-        "server": {"slots": 4, "batch_max_bases": 64_000_000, "small_job_bases": 4_000_000,
-                   "batches": int(st.batches), "batched_jobs": int(st.batched_jobs),
-                   "max_running": int(st.max_running)},
-        "rates": rates, "generation_s": round(gen_s, 1),
-    }
 
 
 class ClockSampler:

@@ -202,12 +202,14 @@ struct cfg_batch {
     cudaEvent_t ev[2] = {};
     std::string err;
     cfg_batch_tuning tune{4, 512, 100, 0, 0.f};
+    uint32_t G_params = 16384;
 
     // input: job j's bases start at word word_off[j] of the packed stream
     DevBuf packed, frag_off, frag_off_rel, frag_len, frag_gbase, job_pos, job_nbases;
     uint64_t n_bases = 0, n_frags = 0;
     uint32_t n_jobs = 0;
     std::vector<uint64_t> word_off, job_frag, nb;   // per job (+1 for job_frag)
+    std::vector<uint32_t> frag_job;                 // per fragment
     bool have_input = false;
 
     // pipeline
@@ -229,6 +231,16 @@ struct cfg_batch {
     std::vector<std::vector<cfg_lmtig>> r_lm;
     std::vector<cfg_counts> r_counts;
     HostBuf h_fasta, h_text, h_lm;      // one job's results (cfg_batch_job)
+
+    // device collation of all jobs' lm-tigs (cfg_batch_unitigs)
+    UnitigBuffers ub;
+    DevBuf u_n, u_base, u_out, u_cur, u_err, u_cyc_lm, u_cyc_text, u_cyc_job, u_cyc_cnt;
+    std::vector<unsigned long long> h_out_base, h_ucur;
+    std::vector<std::string> u_host;    // per job: unitigs joined on the host (cycles; redone jobs)
+    std::vector<uint64_t> u_host_n;
+    bool have_unitigs = false;
+    float unitig_ms = 0;
+    HostBuf h_unitigs;
 };
 
 namespace {
@@ -497,7 +509,7 @@ int cfg_batch_create(int device, const cfg_params* params, cfg_batch** out) {
     if (cudaSetDevice(device) != cudaSuccess) return CFG_ERR_CUDA;
     cfg_batch* b = new (std::nothrow) cfg_batch();
     if (!b) return CFG_ERR_OOM;
-    b->device = device; b->p = p; b->G = p.graph_count; b->words = p.k <= 31 ? 1 : 2;
+    b->device = device; b->p = p; b->G = p.graph_count; b->G_params = p.graph_count; b->words = p.k <= 31 ? 1 : 2;
     b->g_shift = 0;
     while ((1u << b->g_shift) < b->G) ++b->g_shift;
     b->tune.table_load_pct = p.table_load_pct ? p.table_load_pct : 100;
@@ -570,6 +582,9 @@ int cfg_batch_submit(cfg_batch* b, const cfg_packed* jobs, uint32_t n_jobs) {
     const bool same = !grow && b->exec && b->n_bases == n_bases && b->n_frags == nf && b->n_jobs == n_jobs && b->nb == nb;
     b->n_bases = n_bases; b->n_frags = nf; b->n_jobs = n_jobs;
     b->word_off.swap(word_off); b->job_frag.swap(job_frag); b->nb.swap(nb);
+    b->frag_job.resize(nf);
+    for (uint32_t j = 0; j < n_jobs; ++j)
+        for (uint64_t f = b->job_frag[j]; f < b->job_frag[j + 1]; ++f) b->frag_job[f] = j;
     b->have_input = true; b->have_run = false;
     if (!same) {
         drop_graph(b);
@@ -585,6 +600,7 @@ int cfg_batch_run(cfg_batch* b) {
     BCK(cudaSetDevice(b->device));
     b->err.clear();
     b->have_run = false;
+    b->have_unitigs = false;
     for (int attempt = 0; attempt < 3; ++attempt) {
         bool regrow = false;
         int rc = run_once(b, regrow);
@@ -670,11 +686,73 @@ int cfg_batch_job_device_input(cfg_batch* b, uint32_t job, const uint64_t** d_wo
 int cfg_batch_set_tuning(cfg_batch* b, const cfg_batch_tuning* t) {
     if (!b || !t) return CFG_ERR_BAD_INPUT;
     if (t->local_div < 1 || t->local_div > 16 || (t->cluster_threads && (t->cluster_threads % 32 || t->cluster_threads > 512)) ||
-        t->table_load_pct > 100000)
+        t->table_load_pct > 100000 || t->graph_count > 65536 || (t->graph_count & (t->graph_count - 1)))
         return bfail(b, CFG_ERR_BAD_INPUT, "tuning out of range");
     b->tune = *t;
     if (!b->tune.table_load_pct) b->tune.table_load_pct = 100;
     drop_graph(b);
+    const uint32_t G = t->graph_count ? t->graph_count : b->G_params;
+    if (G != b->G) {   // a new subgraph space: bucket bases per fragment, buffers
+        if (b->have_input && (((uint64_t)b->n_jobs * G) >= (1ull << 31))) return bfail(b, CFG_ERR_BAD_INPUT, "too many subgraphs");
+        b->G = G;
+        b->g_shift = 0;
+        while ((1u << b->g_shift) < b->G) ++b->g_shift;
+        b->have_run = false; b->have_unitigs = false;
+        if (b->have_input) {
+            BCK(cudaSetDevice(b->device));
+            std::vector<uint32_t> fg(b->n_frags);
+            for (uint64_t f = 0; f < b->n_frags; ++f) fg[f] = b->frag_job[f] << b->g_shift;
+            if (b->n_frags) BCK(cudaMemcpyAsync(b->frag_gbase.p, fg.data(), 4 * b->n_frags, cudaMemcpyHostToDevice, b->stream));
+            BCK(cudaStreamSynchronize(b->stream));
+            int rc = ensure_buffers(b);
+            if (rc) return rc;
+        }
+    }
+    return CFG_OK;
+}
+
+int cfg_batch_tune_unitigs(cfg_batch* b, cfg_batch_tuning* out) {
+    if (!b) return CFG_ERR_BAD_INPUT;
+    if (!b->have_input) return bfail(b, CFG_ERR_STATE, "cfg_batch_tune_unitigs before cfg_batch_submit");
+    const uint32_t base_load = b->tune.table_load_pct ? b->tune.table_load_pct : 100;
+    auto time_of = [&](const cfg_batch_tuning& t, float& ms) -> int {
+        int rc = cfg_batch_set_tuning(b, &t);
+        if (rc) return rc;
+        ms = 1e30f;
+        for (int rep = 0; rep < 2; ++rep) {
+            float u = 0;
+            rc = cfg_batch_run(b);
+            if (!rc) rc = cfg_batch_unitigs(b, &u);
+            if (rc) return rc;
+            ms = b->ms + u;   // the second run: the graph is built and warm
+        }
+        return CFG_OK;
+    };
+    // subgraph count first (default shapes), then the launch shapes at that count
+    cfg_batch_tuning best{4, 512, base_load, 0, 1e30f};
+    for (uint32_t G = b->G_params; G >= 1 && G + 1 > b->G_params / 64; G /= 4) {
+        cfg_batch_tuning t{4, 512, base_load, G == b->G_params ? 0u : G, 0.f};
+        float ms = 0;
+        int rc = time_of(t, ms);
+        if (rc) return rc;
+        if (ms < best.ms) { best = t; best.ms = ms; }
+        if (G < 4) break;
+    }
+    const uint32_t Gbest = best.graph_count;
+    for (uint32_t d : {2u, 4u, 8u})
+        for (uint32_t ct : {256u, 512u})
+            for (uint32_t ld : {base_load, base_load * 2}) {
+                cfg_batch_tuning t{d, ct, ld, Gbest, 0.f};
+                float ms = 0;
+                int rc = time_of(t, ms);
+                if (rc) return rc;
+                if (ms < best.ms) { best = t; best.ms = ms; }
+            }
+    const float ms = best.ms;
+    int rc = cfg_batch_set_tuning(b, &best);
+    if (rc) return rc;
+    b->tune.ms = ms;
+    if (out) *out = b->tune;
     return CFG_OK;
 }
 
@@ -690,7 +768,7 @@ int cfg_batch_tune(cfg_batch* b, cfg_batch_tuning* out) {
     for (uint32_t d : divs)
         for (uint32_t ld : loads)
             for (uint32_t ct : cthreads) {
-                cfg_batch_tuning t{d, ct, ld, 0, 0.f};
+                cfg_batch_tuning t{d, ct, ld, 0, 0.f};   // subgraph count: the params'
                 int rc = cfg_batch_set_tuning(b, &t);
                 if (rc) return rc;
                 // a redone job would time the plain driver, not this shape: skip such shapes
@@ -713,6 +791,129 @@ int cfg_batch_tune(cfg_batch* b, cfg_batch_tuning* out) {
     return CFG_OK;
 }
 
+int cfg_batch_unitigs(cfg_batch* b, float* device_ms) {
+    if (!b) return CFG_ERR_BAD_INPUT;
+    if (!b->have_run) return bfail(b, CFG_ERR_STATE, "no completed batch run");
+    BCK(cudaSetDevice(b->device));
+    const uint32_t J = b->n_jobs;
+    std::vector<unsigned long long> jn(J), jb(J), ob(J);
+    unsigned long long n = 0, out = 0;
+    for (uint32_t j = 0; j < J; ++j) {
+        const JobOut& x = b->h_jobs[j];
+        jn[j] = b->redo[j] ? 0 : x.lm_used;
+        jb[j] = n; n += jn[j];
+        ob[j] = out; out += b->redo[j] ? 0 : x.lm_text_used + 4 * x.lm_used + 16;
+    }
+    if (!b->u_n.ensure(8ull * J) || !b->u_base.ensure(8ull * J) || !b->u_out.ensure(8ull * J) ||
+        !b->u_cur.ensure(8ull * JOB_CUR_STRIDE * J) || !b->u_err.ensure(16) || !b->ub.ensure(n) || !b->ub.ensure_out(out + 16))
+        return bfail(b, CFG_ERR_OOM, "collation buffers");
+    BCK(cudaMemcpyAsync(b->u_n.p, jn.data(), 8ull * J, cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaMemcpyAsync(b->u_base.p, jb.data(), 8ull * J, cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaMemcpyAsync(b->u_out.p, ob.data(), 8ull * J, cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaMemsetAsync(b->u_cur.p, 0, 8ull * JOB_CUR_STRIDE * J, b->stream));
+    BCK(cudaMemsetAsync(b->u_err.p, 0, 16, b->stream));
+    BCK(cudaEventRecord(b->ev[0], b->stream));
+    UnitigInput in{};
+    in.k = b->p.k; in.n = n; in.err = b->u_err.as<uint32_t>();
+    in.jobs = b->jobs.as<JobOut>(); in.n_jobs = J;
+    in.job_n = b->u_n.as<unsigned long long>(); in.job_lm_base = b->u_base.as<unsigned long long>();
+    in.job_out_base = b->u_out.as<unsigned long long>(); in.job_cur = b->u_cur.as<unsigned long long>();
+    in.job_lm = b->lm.as<LmtigOut>(); in.job_text = b->lm_text.as<char>();
+    UnitigResult res{};
+    int rc = collate_device(in, b->ub, b->stream, res);
+    if (rc) return bfail(b, rc, "batch collation");
+    BCK(cudaEventRecord(b->ev[1], b->stream));
+    uint32_t err = 0;
+    b->h_ucur.resize((size_t)JOB_CUR_STRIDE * J);
+    BCK(cudaMemcpyAsync(&err, b->u_err.p, 4, cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaMemcpyAsync(b->h_ucur.data(), b->u_cur.p, 8ull * JOB_CUR_STRIDE * J, cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    if (err & DERR_BAD_GRAPH) return bfail(b, CFG_ERR_STATE, "lm-tig ends do not form a valid discontinuity graph");
+    if (err & DERR_CAS_LIMIT) return bfail(b, CFG_ERR_WALK_LIMIT, "vertex-table wait exceeded its bound");
+    cudaEventElapsedTime(&b->unitig_ms, b->ev[0], b->ev[1]);
+    b->h_out_base.swap(ob);
+    b->u_host.assign(J, std::string());
+    b->u_host_n.assign(J, 0);
+    // lm-tigs on closed chains: joined on the host, per job
+    if (res.n_cycle_lmtigs) {
+        if (!b->u_cyc_cnt.ensure(16)) return bfail(b, CFG_ERR_OOM, "cycle buffers");
+        unsigned long long cnt[2] = {0, 0};
+        BCK(cudaMemsetAsync(b->u_cyc_cnt.p, 0, 16, b->stream));
+        rc = collate_cycles_device(b->ub, n, nullptr, nullptr, b->u_cyc_cnt.as<unsigned long long>(), b->stream);
+        if (rc) return bfail(b, rc, "cycle sizing");
+        BCK(cudaMemcpyAsync(cnt, b->u_cyc_cnt.p, 16, cudaMemcpyDeviceToHost, b->stream));
+        BCK(cudaStreamSynchronize(b->stream));
+        if (!b->u_cyc_lm.ensure(sizeof(LmtigOut) * (cnt[0] + 1)) || !b->u_cyc_text.ensure(cnt[1] + 1) ||
+            !b->u_cyc_job.ensure(4 * (cnt[0] + 1)))
+            return bfail(b, CFG_ERR_OOM, "cycle buffers");
+        BCK(cudaMemsetAsync(b->u_cyc_cnt.p, 0, 16, b->stream));
+        rc = collate_cycles_device(b->ub, n, b->u_cyc_lm.as<LmtigOut>(), b->u_cyc_text.as<char>(),
+                                   b->u_cyc_cnt.as<unsigned long long>(), b->stream, b->u_cyc_job.as<uint32_t>());
+        if (rc) return bfail(b, rc, "cycle gather");
+        std::vector<cfg_lmtig> hl(cnt[0]);
+        std::vector<uint32_t> hj(cnt[0]);
+        std::string ht(cnt[1], '\0');
+        if (cnt[0]) {
+            BCK(cudaMemcpyAsync(hl.data(), b->u_cyc_lm.p, sizeof(cfg_lmtig) * cnt[0], cudaMemcpyDeviceToHost, b->stream));
+            BCK(cudaMemcpyAsync(hj.data(), b->u_cyc_job.p, 4 * cnt[0], cudaMemcpyDeviceToHost, b->stream));
+        }
+        if (cnt[1]) BCK(cudaMemcpyAsync(&ht[0], b->u_cyc_text.p, cnt[1], cudaMemcpyDeviceToHost, b->stream));
+        BCK(cudaStreamSynchronize(b->stream));
+        std::vector<std::vector<cfg_lmtig>> per(J);
+        for (uint64_t i = 0; i < cnt[0]; ++i) per[hj[i]].push_back(hl[i]);
+        for (uint32_t j = 0; j < J; ++j) {
+            if (per[j].empty()) continue;
+            char* o = nullptr;
+            uint64_t ob2 = 0, nu = 0, nc = 0;
+            rc = cfg_collate_lmtigs(b->p.k, per[j].data(), per[j].size(), ht.data(), &o, &ob2, &nu, &nc);
+            if (rc) return bfail(b, rc, "cycle collation");
+            b->u_host[j].assign(o, ob2);
+            cfg_free(o);
+            b->u_host_n[j] = nu;
+        }
+    }
+    // jobs redone alone: their lm-tigs are on the host already
+    for (uint32_t j = 0; j < J; ++j) {
+        if (!b->redo[j]) continue;
+        char* o = nullptr;
+        uint64_t ob2 = 0, nu = 0, nc = 0;
+        rc = cfg_collate_lmtigs(b->p.k, b->r_lm[j].data(), b->r_lm[j].size(), b->r_text[j].data(), &o, &ob2, &nu, &nc);
+        if (rc) return bfail(b, rc, "redone job collation");
+        b->u_host[j] = b->r_fasta[j] + std::string(o, ob2);
+        cfg_free(o);
+        b->u_host_n[j] = b->r_counts[j].n_trivial + nu;
+    }
+    b->have_unitigs = true;
+    if (device_ms) *device_ms = b->unitig_ms;
+    return CFG_OK;
+}
+
+int cfg_batch_job_unitigs(cfg_batch* b, uint32_t job, const char** fasta, uint64_t* bytes, uint64_t* n_unitigs) {
+    if (!b || !fasta || !bytes) return CFG_ERR_BAD_INPUT;
+    if (!b->have_unitigs) return bfail(b, CFG_ERR_STATE, "cfg_batch_unitigs has not run");
+    if (job >= b->n_jobs) return bfail(b, CFG_ERR_BAD_INPUT, "job index out of range");
+    BCK(cudaSetDevice(b->device));
+    if (b->redo[job]) {
+        *fasta = b->u_host[job].data();
+        *bytes = b->u_host[job].size();
+        if (n_unitigs) *n_unitigs = b->u_host_n[job];
+        return CFG_OK;
+    }
+    const JobOut& J = b->h_jobs[job];
+    const unsigned long long cb = b->h_ucur[(size_t)job * JOB_CUR_STRIDE], cu = b->h_ucur[(size_t)job * JOB_CUR_STRIDE + 1];
+    const uint64_t total = J.fasta_used + cb + b->u_host[job].size();
+    if (!b->h_unitigs.ensure(total + 1)) return bfail(b, CFG_ERR_OOM, "pinned unitig buffer");
+    char* h = (char*)b->h_unitigs.p;
+    if (J.fasta_used) BCK(cudaMemcpyAsync(h, b->fasta.as<char>() + J.fasta_off, J.fasta_used, cudaMemcpyDeviceToHost, b->stream));
+    if (cb) BCK(cudaMemcpyAsync(h + J.fasta_used, b->ub.out + b->h_out_base[job], cb, cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    if (!b->u_host[job].empty()) std::memcpy(h + J.fasta_used + cb, b->u_host[job].data(), b->u_host[job].size());
+    *fasta = h;
+    *bytes = total;
+    if (n_unitigs) *n_unitigs = J.trivial + cu + b->u_host_n[job];
+    return CFG_OK;
+}
+
 const char* cfg_batch_last_error_string(cfg_batch* b) { return b ? b->err.c_str() : "null batch"; }
 
 void cfg_batch_destroy(cfg_batch* b) {
@@ -725,7 +926,11 @@ void cfg_batch_destroy(cfg_batch* b) {
                       &b->tab_off, &b->tab_cap, &b->arena, &b->jobs, &b->fasta, &b->lm_text, &b->lm, &b->retry, &b->counters,
                       &b->bucket_cnt, &b->job_cur};
     for (DevBuf* x : bufs) x->release();
-    b->h_fasta.release(); b->h_text.release(); b->h_lm.release();
+    b->h_fasta.release(); b->h_text.release(); b->h_lm.release(); b->h_unitigs.release();
+    b->ub.release();
+    DevBuf* ubufs[] = {&b->u_n, &b->u_base, &b->u_out, &b->u_cur, &b->u_err, &b->u_cyc_lm, &b->u_cyc_text, &b->u_cyc_job,
+                       &b->u_cyc_cnt};
+    for (DevBuf* x : ubufs) x->release();
     if (b->plain) cfg_destroy(b->plain);
     for (auto& e : b->ev) if (e) cudaEventDestroy(e);
     if (b->stream) cudaStreamDestroy(b->stream);

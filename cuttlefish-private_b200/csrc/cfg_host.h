@@ -81,6 +81,7 @@ struct ParseBuffers {
 };
 
 struct LmtigOut;
+struct JobOut;
 
 // Device collation (cfg_unitig.cu): the run's striped lm-tigs ...
 struct UnitigInput {
@@ -90,13 +91,24 @@ struct UnitigInput {
     const unsigned long long* lm_base;            // per stripe: records before it (device)
     const unsigned long long* text_base;          // per stripe: label bytes before it (device)
     uint32_t stripes, k;
-    uint64_t n;                                   // records over all stripes
+    uint64_t n;                                   // records over all stripes (or jobs)
     uint32_t* err;
+    // batch: lm-tigs come from the jobs' regions instead of stripes; job j contributes
+    // job_n[j] records (0 for a job redone alone) placed at job_lm_base[j], and its
+    // unitigs go to [job_out_base[j], ...) with a cursor in job_cur (JOB_CUR_STRIDE words:
+    // [0] bytes, [1] unitigs).  Ends of different jobs never meet.
+    const struct JobOut* jobs;
+    uint32_t n_jobs;
+    const unsigned long long *job_n, *job_lm_base, *job_out_base;
+    unsigned long long* job_cur;
+    const LmtigOut* job_lm;                       // the batch's lm-tig arena
+    const char* job_text;                         // and label arena
 };
 // ... the buffers it works in ...
 struct UnitigBuffers {
-    DevBuf b_lm, b_label, b_tab, b_partner, b_P0, b_P1, b_R0, b_R1, b_A0, b_A1, b_fin, b_off, b_words, b_out;
+    DevBuf b_lm, b_label, b_tab, b_partner, b_P0, b_P1, b_R0, b_R1, b_A0, b_A1, b_fin, b_off, b_words, b_out, b_job;
     LmtigOut* lm = nullptr;
+    uint32_t* job = nullptr;   // batch: each gathered lm-tig's job
     const char** label = nullptr;
     void* tab = nullptr;
     uint64_t tab_n = 0;
@@ -116,7 +128,7 @@ struct UnitigBuffers {
     }
     void release() {
         DevBuf* all[] = {&b_lm, &b_label, &b_tab, &b_partner, &b_P0, &b_P1, &b_R0, &b_R1, &b_A0, &b_A1, &b_fin, &b_off,
-                         &b_words, &b_out};
+                         &b_words, &b_out, &b_job};
         for (DevBuf* b : all) b->release();
     }
 };
@@ -125,7 +137,7 @@ struct UnitigBuffers {
 struct UnitigResult { uint64_t bytes, n_units, n_cycle_lmtigs; uint32_t rounds; };
 int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, UnitigResult& res);
 int collate_cycles_device(const UnitigBuffers& ub, uint64_t n, LmtigOut* out, char* text, unsigned long long* cnt,
-                          cudaStream_t s);
+                          cudaStream_t s, uint32_t* out_job = nullptr);
 
 // FASTA (fastq = 0) or FASTQ text in device memory -> the packed stream and fragment
 // table in `pb` (cfg_parse.cu).  Synchronises the stream twice (two counts).

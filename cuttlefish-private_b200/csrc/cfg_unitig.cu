@@ -23,6 +23,8 @@
 #include "cfg_host.h"
 #include "cfg_internal.h"
 
+#include <algorithm>
+
 namespace cfg {
 
 namespace {
@@ -67,19 +69,39 @@ __global__ void k_ut_gather(const LmtigOut* lm, uint64_t lm_slice, const char* t
     }
 }
 
+// 0 (batch): gather every job's lm-tigs from its regions; the job rides along.
+__global__ void k_ut_gather_jobs(const LmtigOut* lm, const char* text, const JobOut* __restrict__ jobs, uint32_t n_jobs,
+                                 const unsigned long long* __restrict__ job_n, const unsigned long long* __restrict__ job_lm_base,
+                                 LmtigOut* out, const char** label, uint32_t* out_job) {
+    for (uint32_t j = blockIdx.y; j < n_jobs; j += gridDim.y) {
+        const unsigned long long n = job_n[j];
+        const JobOut& J = jobs[j];
+        for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+            const LmtigOut m = lm[J.lm_off + i];
+            const uint64_t g = job_lm_base[j] + i;
+            out[g] = m;
+            label[g] = text + J.lm_text_off + m.label_off;
+            out_job[g] = j;
+        }
+    }
+}
+
 // 1: every non-phi end into the vertex table; the second end at a vertex pairs.
-__global__ void k_ut_insert(const LmtigOut* __restrict__ lm, uint64_t n, EndSlot* tab, uint64_t mask, uint32_t* err) {
+// In a batch the vertex is (job, k-mer).
+__global__ void k_ut_insert(const LmtigOut* __restrict__ lm, const uint32_t* __restrict__ job, uint64_t n, EndSlot* tab,
+                            uint64_t mask, uint32_t* err) {
     for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < 2 * n; e += (uint64_t)gridDim.x * blockDim.x) {
         const LmtigOut& m = lm[e >> 1];
         const uint32_t end = (uint32_t)(e & 1);
         if (is_phi(m, end)) continue;
         const unsigned long long k0 = end ? m.v[0] : m.u[0], k1 = end ? m.v[1] : m.u[1];
-        uint64_t p = mix64(k0 ^ mix64(k1 + 0x9E3779B97F4A7C15ull)) & mask;
+        const uint32_t jb = job ? job[e >> 1] : 0u;
+        uint64_t p = mix64(k0 ^ mix64(k1 + 0x9E3779B97F4A7C15ull) ^ mix64(jb + 0x632BE59BD9B4E019ull)) & mask;
         for (uint64_t probe = 0; probe <= mask; ++probe, p = (p + 1) & mask) {
             EndSlot& s = tab[p];
             const uint32_t old = atomicCAS(&s.e0, NONE, (uint32_t)e);
             if (old == NONE) {
-                s.k0 = k0; s.k1 = k1;
+                s.k0 = k0; s.k1 = k1; s.pad = jb;
                 __threadfence();
                 atomicExch(&s.ready, 1u);
                 break;
@@ -89,7 +111,8 @@ __global__ void k_ut_insert(const LmtigOut* __restrict__ lm, uint64_t n, EndSlot
                 if (++spin > (1u << 22)) { atomicOr(err, DERR_CAS_LIMIT); return; }
             }
             __threadfence();
-            if (*(volatile unsigned long long*)&s.k0 == k0 && *(volatile unsigned long long*)&s.k1 == k1) {
+            if (*(volatile unsigned long long*)&s.k0 == k0 && *(volatile unsigned long long*)&s.k1 == k1 &&
+                *(volatile uint32_t*)&s.pad == jb) {
                 if (atomicCAS(&s.e1, NONE, (uint32_t)e) != NONE) atomicOr(err, DERR_BAD_GRAPH);   // a third end
                 break;
             }
@@ -149,7 +172,8 @@ __global__ void k_ut_choose(const LmtigOut* __restrict__ lm, const char* const* 
                             const uint32_t* __restrict__ partner, const uint32_t* __restrict__ P,
                             const uint32_t* __restrict__ R, const unsigned long long* __restrict__ A, uint32_t k,
                             uint32_t* fin, unsigned long long* out_off, unsigned long long* cursor, unsigned long long* n_units,
-                            unsigned long long* n_cyc) {
+                            unsigned long long* n_cyc, const uint32_t* __restrict__ job,
+                            const unsigned long long* __restrict__ job_out_base, unsigned long long* job_cur) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
@@ -187,19 +211,40 @@ __global__ void k_ut_choose(const LmtigOut* __restrict__ lm, const char* const* 
                 }
             }
         }
-        // warp-aggregated reservation of the unitigs' records
-        unsigned long long want = tail ? L + 4 : 0, x = want;
-        for (int d = 1; d < 32; d <<= 1) {
-            const unsigned long long y = __shfl_up_sync(0xffffffffu, x, d);
-            if (lane >= (uint32_t)d) x += y;
-        }
-        const unsigned long long tot = __shfl_sync(0xffffffffu, x, 31);
-        unsigned long long b0 = 0;
-        if (lane == 0 && tot) b0 = atomicAdd(cursor, tot);
-        b0 = __shfl_sync(0xffffffffu, b0, 0);
-        if (tail) {
-            out_off[head] = b0 + x - want;
-            atomicAdd(n_units, 1ull);
+        const unsigned long long want = tail ? L + 4 : 0;
+        if (!job) {   // warp-aggregated reservation of the unitigs' records
+            unsigned long long x = want;
+            for (int d = 1; d < 32; d <<= 1) {
+                const unsigned long long y = __shfl_up_sync(0xffffffffu, x, d);
+                if (lane >= (uint32_t)d) x += y;
+            }
+            const unsigned long long tot = __shfl_sync(0xffffffffu, x, 31);
+            unsigned long long b0 = 0;
+            if (lane == 0 && tot) b0 = atomicAdd(cursor, tot);
+            b0 = __shfl_sync(0xffffffffu, b0, 0);
+            if (tail) {
+                out_off[head] = b0 + x - want;
+                atomicAdd(n_units, 1ull);
+            }
+        } else {      // per job: lanes of one job reserve together from its cursor
+            const uint32_t jb = tail ? job[i] : NONE;
+            unsigned long long pre = 0, tot = 0, cnt = 0;
+            uint32_t leader = 32;
+            for (uint32_t l = 0; l < 32; ++l) {
+                const unsigned long long v = __shfl_sync(0xffffffffu, want, l);
+                const uint32_t jl = __shfl_sync(0xffffffffu, jb, l);
+                if (jl == jb) { tot += v; ++cnt; if (l < lane) pre += v; if (leader == 32) leader = l; }
+            }
+            unsigned long long b0 = 0;
+            if (tail && leader == lane) {
+                b0 = atomicAdd(job_cur + (size_t)jb * JOB_CUR_STRIDE, tot);
+                atomicAdd(job_cur + (size_t)jb * JOB_CUR_STRIDE + 1, cnt);
+            }
+            b0 = __shfl_sync(0xffffffffu, b0, leader & 31);
+            if (tail) {
+                out_off[head] = job_out_base[jb] + b0 + pre;
+                atomicAdd(n_units, 1ull);
+            }
         }
     }
 }
@@ -229,7 +274,8 @@ __global__ void k_ut_write(const LmtigOut* __restrict__ lm, const char* const* _
 
 // Lm-tigs on closed chains, with their labels, into small arrays for the host collator.
 __global__ void k_ut_cycles(const LmtigOut* __restrict__ lm, const char* const* __restrict__ label, uint64_t n,
-                            const uint32_t* __restrict__ fin, LmtigOut* out, char* text, unsigned long long* cnt) {
+                            const uint32_t* __restrict__ fin, LmtigOut* out, char* text, unsigned long long* cnt,
+                            const uint32_t* __restrict__ job, uint32_t* out_job) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         if (fin[i] != NONE) continue;
         LmtigOut m = lm[i];
@@ -239,6 +285,7 @@ __global__ void k_ut_cycles(const LmtigOut* __restrict__ lm, const char* const* 
         for (uint32_t j = 0; j < m.label_len; ++j) text[off + j] = label[i][j];
         m.label_off = off;
         out[slot] = m;
+        if (out_job) out_job[slot] = job ? job[i] : 0u;
     }
 }
 
@@ -251,8 +298,9 @@ bool UnitigBuffers::ensure(uint64_t n) {
     if (!b_lm.ensure(sizeof(LmtigOut) * (n + 1)) || !b_label.ensure(8 * (n + 1)) || !b_tab.ensure(sizeof(EndSlot) * t) ||
         !b_partner.ensure(4 * n2) || !b_P0.ensure(4 * n2) || !b_P1.ensure(4 * n2) || !b_R0.ensure(4 * n2) ||
         !b_R1.ensure(4 * n2) || !b_A0.ensure(8 * n2) || !b_A1.ensure(8 * n2) || !b_fin.ensure(4 * (n + 1)) ||
-        !b_off.ensure(8 * n2) || !b_words.ensure(64))
+        !b_off.ensure(8 * n2) || !b_words.ensure(64) || !b_job.ensure(4 * (n + 1)))
         return false;
+    job = b_job.as<uint32_t>();
     lm = b_lm.as<LmtigOut>(); label = (const char**)b_label.p; tab = b_tab.p; tab_n = t;
     partner = b_partner.as<uint32_t>(); P[0] = b_P0.as<uint32_t>(); P[1] = b_P1.as<uint32_t>();
     R[0] = b_R0.as<uint32_t>(); R[1] = b_R1.as<uint32_t>(); A[0] = b_A0.as<unsigned long long>();
@@ -262,8 +310,8 @@ bool UnitigBuffers::ensure(uint64_t n) {
 }
 
 int collate_cycles_device(const UnitigBuffers& ub, uint64_t n, LmtigOut* out, char* text, unsigned long long* cnt,
-                          cudaStream_t s) {
-    k_ut_cycles<<<148 * 4, 256, 0, s>>>(ub.lm, ub.label, n, ub.fin, out, text, cnt);
+                          cudaStream_t s, uint32_t* out_job) {
+    k_ut_cycles<<<148 * 4, 256, 0, s>>>(ub.lm, ub.label, n, ub.fin, out, text, cnt, ub.job, out_job);
     return cudaGetLastError() == cudaSuccess ? CFG_OK : CFG_ERR_CUDA;
 }
 
@@ -276,11 +324,16 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
     if (n == 0) return CFG_OK;
     const unsigned grid = 148 * 8;
     EndSlot* tab = (EndSlot*)ub.tab;
-    k_ut_gather<<<dim3(64, in.stripes), 256, 0, s>>>(in.lm, in.lm_slice, in.text, in.text_slice, in.lm_base, in.text_base,
-                                                     in.stripe_cur, in.stripes, ub.lm, ub.label);
+    const uint32_t* job = in.jobs ? ub.job : nullptr;
+    if (in.jobs)
+        k_ut_gather_jobs<<<dim3(16, std::min<uint32_t>(in.n_jobs, 65535)), 256, 0, s>>>(
+            in.job_lm, in.job_text, in.jobs, in.n_jobs, in.job_n, in.job_lm_base, ub.lm, ub.label, ub.job);
+    else
+        k_ut_gather<<<dim3(64, in.stripes), 256, 0, s>>>(in.lm, in.lm_slice, in.text, in.text_slice, in.lm_base, in.text_base,
+                                                         in.stripe_cur, in.stripes, ub.lm, ub.label);
     k_ut_tab_init<<<grid, 256, 0, s>>>(tab, ub.tab_n);
     if (cudaMemsetAsync(ub.partner, 0xff, 4 * 2 * n, s) != cudaSuccess) return CFG_ERR_CUDA;
-    k_ut_insert<<<grid, 256, 0, s>>>(ub.lm, n, tab, ub.tab_n - 1, in.err);
+    k_ut_insert<<<grid, 256, 0, s>>>(ub.lm, job, n, tab, ub.tab_n - 1, in.err);
     k_ut_pair<<<grid, 256, 0, s>>>(ub.lm, tab, ub.tab_n, ub.partner, in.err);
     k_ut_rank_init<<<grid, 256, 0, s>>>(ub.lm, n, ub.partner, in.k, ub.P[0], ub.R[0], ub.A[0]);
     int cur = 0;
@@ -299,11 +352,12 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
         last = active;
     }
     k_ut_choose<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, ub.partner, ub.P[cur], ub.R[cur], ub.A[cur], in.k, ub.fin,
-                                     ub.out_off, cursor, cursor + 1, cursor + 2);
+                                     ub.out_off, cursor, cursor + 1, cursor + 2, job, in.job_out_base, in.job_cur);
     unsigned long long w[3] = {0, 0, 0};
     if (cudaMemcpyAsync(w, cursor, 24, cudaMemcpyDeviceToHost, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
         return CFG_ERR_CUDA;
-    if (!ub.ensure_out(w[0] + 16)) return CFG_ERR_OOM;
+    // a batch's output regions are sized by the caller before the call
+    if (!in.jobs && !ub.ensure_out(w[0] + 16)) return CFG_ERR_OOM;
     k_ut_write<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, ub.fin, ub.partner, ub.R[cur], ub.A[cur], ub.out_off, ub.out);
     if (cudaGetLastError() != cudaSuccess) return CFG_ERR_CUDA;
     res.bytes = w[0]; res.n_units = w[1]; res.n_cycle_lmtigs = w[2];

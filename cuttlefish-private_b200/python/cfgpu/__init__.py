@@ -69,7 +69,7 @@ class Packed(ctypes.Structure):
 
 class BatchTuning(ctypes.Structure):
     _fields_ = [("local_div", ctypes.c_uint32), ("cluster_threads", ctypes.c_uint32),
-                ("table_load_pct", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("ms", ctypes.c_float)]
+                ("table_load_pct", ctypes.c_uint32), ("graph_count", ctypes.c_uint32), ("ms", ctypes.c_float)]
 
 
 class ServerConfig(ctypes.Structure):
@@ -134,7 +134,11 @@ SIGNATURES = {
                                                   ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_void_p),
                                                   ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_uint64)]),
     "cfg_batch_tune": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchTuning)]),
+    "cfg_batch_unitigs": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
+    "cfg_batch_job_unitigs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p),
+                                             ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     "cfg_batch_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchTuning)]),
+    "cfg_batch_tune_unitigs": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchTuning)]),
     "cfg_batch_last_error_string": (ctypes.c_char_p, [ctypes.c_void_p]),
     "cfg_batch_destroy": (None, [ctypes.c_void_p]),
     "cfg_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ServerConfig), ctypes.POINTER(ctypes.c_void_p)]),
@@ -394,13 +398,36 @@ class Batch:
         _check_b(self.lib, self.b, rc, "cfg_batch_job_device_input")
         return w.value, n.value, fo.value, fl.value, nf.value
 
+    def unitigs(self) -> float:
+        """cfg_batch_unitigs: every job's lm-tigs joined on the device; -> device ms."""
+        ms = ctypes.c_float()
+        _check_b(self.lib, self.b, self.lib.cfg_batch_unitigs(self.b, ctypes.byref(ms)), "cfg_batch_unitigs")
+        return ms.value
+
+    def job_unitigs_raw(self, j: int):
+        p, nb, nu = ctypes.c_void_p(), ctypes.c_uint64(), ctypes.c_uint64()
+        _check_b(self.lib, self.b, self.lib.cfg_batch_job_unitigs(self.b, j, ctypes.byref(p), ctypes.byref(nb),
+                                                                  ctypes.byref(nu)), "cfg_batch_job_unitigs")
+        return p.value, nb.value, nu.value
+
+    def job_unitigs(self, j: int):
+        """-> (FASTA bytes of job j's final unitigs, n_unitigs)."""
+        p, nb, nu = self.job_unitigs_raw(j)
+        return (ctypes.string_at(p, nb) if nb else b""), nu
+
     def tune(self) -> BatchTuning:
         t = BatchTuning()
         _check_b(self.lib, self.b, self.lib.cfg_batch_tune(self.b, ctypes.byref(t)), "cfg_batch_tune")
         return t
 
-    def set_tuning(self, local_div=4, cluster_threads=512, table_load_pct=100):
-        t = BatchTuning(local_div, cluster_threads, table_load_pct, 0, 0.0)
+    def tune_unitigs(self) -> BatchTuning:
+        """cfg_batch_tune_unitigs: launch shapes and the subgraph count, for final unitigs."""
+        t = BatchTuning()
+        _check_b(self.lib, self.b, self.lib.cfg_batch_tune_unitigs(self.b, ctypes.byref(t)), "cfg_batch_tune_unitigs")
+        return t
+
+    def set_tuning(self, local_div=4, cluster_threads=512, table_load_pct=100, graph_count=0):
+        t = BatchTuning(local_div, cluster_threads, table_load_pct, graph_count, 0.0)
         _check_b(self.lib, self.b, self.lib.cfg_batch_set_tuning(self.b, ctypes.byref(t)), "cfg_batch_set_tuning")
 
 

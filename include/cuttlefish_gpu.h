@@ -238,7 +238,8 @@ typedef struct cfg_batch_tuning {
     uint32_t local_div;        /* one-CTA tables: threads = slots / local_div (64..512)   */
     uint32_t cluster_threads;  /* threads per CTA of cluster tables (multiple of 32, <= 512) */
     uint32_t table_load_pct;   /* as cfg_params.table_load_pct                            */
-    uint32_t reserved;
+    uint32_t graph_count;      /* subgraphs per job (0: cfg_params.graph_count).  The
+                                  lm-tigs depend on it; the final unitigs do not.          */
     float    ms;               /* cfg_batch_tune: device time of the chosen shape          */
 } cfg_batch_tuning;
 
@@ -259,6 +260,14 @@ int cfg_batch_run(cfg_batch* b);
  * next cfg_batch_job / cfg_batch_run / cfg_batch_destroy. */
 int cfg_batch_job(cfg_batch* b, uint32_t job, cfg_results* out);
 int cfg_batch_info(cfg_batch* b, cfg_batch_stats* out);
+/* Joins every job's lm-tigs into its maximal unitigs on the device, after
+ * cfg_batch_run (as cfg_unitigs does for one job; jobs never join each other).
+ * device_ms (optional): the collation's device time. */
+int cfg_batch_unitigs(cfg_batch* b, float* device_ms);
+/* One job's final unitigs (trivial + joined) as FASTA text in host memory owned by
+ * the batch, valid until the next call; the content cfg_unitigs gives for that job
+ * run alone. */
+int cfg_batch_job_unitigs(cfg_batch* b, uint32_t job, const char** fasta, uint64_t* bytes, uint64_t* n_unitigs);
 /* Device copy of one job's input in cfg_submit_packed_device's layout (for
  * running that job through a plain context without another copy). */
 int cfg_batch_job_device_input(cfg_batch* b, uint32_t job, const uint64_t** d_words, uint64_t* n_bases,
@@ -266,6 +275,11 @@ int cfg_batch_job_device_input(cfg_batch* b, uint32_t job, const uint64_t** d_wo
 /* Autotuner: times every candidate launch shape (threads per table class, table
  * load factor) on the submitted batch and keeps the fastest. */
 int cfg_batch_tune(cfg_batch* b, cfg_batch_tuning* out);
+/* The same for batches whose product is final unitigs (cfg_batch_unitigs): also
+ * tunes the subgraph count per job, timing the run and the collation together.
+ * Afterwards cfg_batch_job_unitigs still gives each job's unitigs exactly; the
+ * lm-tigs of cfg_batch_job follow the chosen subgraph count. */
+int cfg_batch_tune_unitigs(cfg_batch* b, cfg_batch_tuning* out);
 int cfg_batch_set_tuning(cfg_batch* b, const cfg_batch_tuning* t);
 const char* cfg_batch_last_error_string(cfg_batch* b);
 void cfg_batch_destroy(cfg_batch* b);

@@ -149,3 +149,63 @@ def test_batch_device_input_runs_plain():
             assert summary(31, *cx.fetch()) == plain(31, 20, 1, 16384, jobs[j])
     for p in packed:
         p.close()
+
+
+@pytest.mark.parametrize("k,c,G,load", [(31, 1, 16384, 0), (31, 2, 16384, 0), (63, 1, 64, 0), (31, 1, 64, 10)])
+def test_batch_unitigs_equal_plain(k, c, G, load):
+    """cfg_batch_unitigs: every job's final unitigs (joined on the device, cycles and
+    redone jobs on the host) are those cfg_unitigs gives for the job run alone."""
+    rng = np.random.default_rng(108 + k + c + G)
+    jobs = make_jobs(rng, k, 7)
+    s = synth.random_seq(rng, 900)
+    jobs.append([s + s[:k], "ACGT" * 40])        # circular molecule + tandem repeat: cycles
+    jobs.append(["NNNN"])                         # empty job
+    packed = [cfgpu.PackedInput(r, k) for r in jobs]
+    expect = []
+    for p in packed:
+        with cfgpu.Compactor(k, 20, c, G, table_load_pct=load) as cx:
+            cx.submit(p)
+            cx.run()
+            fa, nu = cx.unitigs()
+            expect.append((orc.fasta_multiset(fa), nu))
+    with cfgpu.Batch(k, 20, c, G, table_load_pct=load) as b:
+        b.submit(packed)
+        b.run()
+        b.unitigs()
+        for j in range(len(jobs)):
+            fa, nu = b.job_unitigs(j)
+            assert (orc.fasta_multiset(fa), nu) == expect[j], f"job {j}"
+    for p in packed:
+        p.close()
+
+
+def test_batch_tuned_graph_count_keeps_unitigs():
+    """The subgraph count the unitig tuner may change leaves every job's unitigs as they are alone."""
+    rng = np.random.default_rng(109)
+    jobs = make_jobs(rng, 31, 6)
+    packed = [cfgpu.PackedInput(r, 31) for r in jobs]
+    expect = []
+    for p in packed:
+        with cfgpu.Compactor(31, 20, 1, 16384) as cx:
+            cx.submit(p)
+            cx.run()
+            fa, nu = cx.unitigs()
+            expect.append((orc.fasta_multiset(fa), nu))
+    with cfgpu.Batch(31, 20, 1, 16384) as b:
+        b.submit(packed)
+        for G in (256, 1024, 16384):
+            b.set_tuning(graph_count=G)
+            b.run()
+            b.unitigs()
+            for j in range(len(jobs)):
+                fa, nu = b.job_unitigs(j)
+                assert (orc.fasta_multiset(fa), nu) == expect[j], (G, j)
+        t = b.tune_unitigs()
+        assert t.graph_count in (0, 256, 1024, 4096)
+        b.run()
+        b.unitigs()
+        for j in range(len(jobs)):
+            fa, nu = b.job_unitigs(j)
+            assert (orc.fasta_multiset(fa), nu) == expect[j]
+    for p in packed:
+        p.close()
