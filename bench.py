@@ -219,6 +219,182 @@ def bench_batch(args, pg, local, world, peak, with_cpu):
     return out
 
 
+def make_serving_mix(n_jobs, k, seed=5):
+    """The serving mix: half reference jobs (one record, log-uniform 0.5-50 Mbp), half
+    read jobs (1-5 M reads of 150 bp, 0.5% errors, both strands, coverage 20-40x of a
+    genome of reads*150/coverage bases).  Returns [(kind, PackedInput, cutoff, load)]."""
+    import random
+
+    import numpy as np
+
+    import cfgpu
+    lib = synth()
+    rnd = random.Random(seed)
+    jobs = []
+    for i in range(n_jobs):
+        if i % 2 == 0:
+            n = int(math.exp(rnd.uniform(math.log(0.5e6), math.log(50e6))))
+            g = ctypes.create_string_buffer(n)
+            lib.cfs_genome_n(n, 50000 + i, g)
+            p = cfgpu.PackedInput(None, k, pinned=True, data_offsets=(g, (ctypes.c_uint64 * 2)(0, n), 1))
+            jobs.append(("ref", p, 1, 100))
+        else:
+            n_reads = rnd.randint(1_000_000, 5_000_000)
+            cov = rnd.uniform(20, 40)
+            gl = int(n_reads * 150 / cov)
+            g = ctypes.create_string_buffer(gl)
+            lib.cfs_genome_n(gl, 60000 + i, g)
+            out = ctypes.create_string_buffer(n_reads * 150)
+            lib.cfs_reads(g, gl, n_reads, 150, 0.005, 70000 + i, out)
+            del g
+            offs = np.arange(0, (n_reads + 1) * 150, 150, dtype=np.uint64)
+            p = cfgpu.PackedInput(None, k, pinned=True,
+                                  data_offsets=(out, offs.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), n_reads))
+            del out, offs
+            jobs.append(("read", p, 2, 15))
+    return jobs
+
+
+def percentile(xs, q):
+    ys = sorted(xs)
+    if not ys:
+        return None
+    i = min(len(ys) - 1, max(0, int(math.ceil(q / 100 * len(ys))) - 1))
+    return ys[i]
+
+
+def bench_serve(args, local, world):
+    """Serving loop vs the plain path on the same GPU, same jobs, same Poisson arrivals.
+
+    The plain path serves FIFO, one job at a time (submit + run + fetch per job).  The
+    server (4 slots, small jobs batched) admits jobs as they arrive.  Latency = arrival
+    -> results on the host.  Rates are multiples of the plain path's service rate."""
+    import random
+
+    import cfgpu
+    k = 31
+    t0 = time.perf_counter()
+    jobs = make_serving_mix(args.serve_jobs, k)
+    gen_s = time.perf_counter() - t0
+    total_bases = sum(p.n_bases for _, p, _, _ in jobs)
+    ctxs = {}
+
+    def plain_ctx(c, load):
+        if (c, load) not in ctxs:
+            ctxs[(c, load)] = cfgpu.Compactor(k, 20, c, 16384, device=local if world > 1 else 0, table_load_pct=load)
+        return ctxs[(c, load)]
+
+    def plain_one(j):
+        _, p, c, load = jobs[j]
+        cx = plain_ctx(c, load)
+        cx.submit(p)
+        cx.run()
+        cx.fetch_raw()
+
+    for j in range(len(jobs)):           # warm: every context grown to its largest job
+        plain_one(j)
+    t = time.perf_counter()
+    for j in range(len(jobs)):
+        plain_one(j)
+    seq_s = time.perf_counter() - t
+    mu = len(jobs) / seq_s               # plain service rate, jobs/s
+
+    def arrivals(lam, seed):
+        r = random.Random(seed)
+        at, out = 0.0, []
+        for _ in jobs:
+            out.append(at)
+            at += r.expovariate(lam)
+        return out
+
+    def run_plain(arr):
+        start = time.perf_counter()
+        lat, done = [], 0.0
+        for j, a in enumerate(arr):
+            now = time.perf_counter() - start
+            if now < a:
+                time.sleep(a - now)
+            plain_one(j)
+            done = time.perf_counter() - start
+            lat.append(done - a)
+        return lat, done
+
+    srv = cfgpu.Server(device=local if world > 1 else 0, slots=4, batch_max_bases=64_000_000,
+                       small_job_bases=4_000_000)
+
+    def run_server(arr):
+        start = time.perf_counter()
+        tickets = [None] * len(arr)
+
+        submitted = threading.Semaphore(0)
+
+        def submitter():
+            for j, a in enumerate(arr):
+                now = time.perf_counter() - start
+                if now < a:
+                    time.sleep(a - now)
+                _, p, c, load = jobs[j]
+                tickets[j] = srv.submit(p, k, 20, c, table_load_pct=load)
+                submitted.release()
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        lat, groups, done = [], [], []
+        for _ in range(len(arr)):          # completion order: results are released as soon as read
+            submitted.acquire()            # one more job is in the server
+            t, _, tm = srv.wait_any_raw()
+            srv.release(t)
+            lat.append(tm.latency_s)
+            groups.append(tm.group_jobs)
+            done.append(time.perf_counter() - start)
+        th.join()
+        return lat, max(done), groups
+
+    # warm every worker's contexts on the largest job of each kind (all workers take one at once)
+    for kind in ("ref", "read"):
+        big = max((j for j in range(len(jobs)) if jobs[j][0] == kind), key=lambda j: jobs[j][1].n_bases, default=None)
+        if big is None:
+            continue
+        _, p, c, load = jobs[big]
+        ts = [srv.submit(p, k, 20, c, table_load_pct=load) for _ in range(4)]
+        for _ in ts:
+            t, _, _ = srv.wait_any_raw()
+            srv.release(t)
+    run_server(arrivals(mu * 4, 99))
+    rates = []
+    for f in args.serve_load:
+        arr = arrivals(mu * f, 1000 + int(100 * f))
+        sl, smk, groups = run_server(arr)
+        pl, pmk = run_plain(arr)
+        rates.append({
+            "load_vs_plain_capacity": f, "lambda_jobs_per_s": mu * f,
+            "server": {"p50_ms": 1e3 * percentile(sl, 50), "p99_ms": 1e3 * percentile(sl, 99),
+                       "mean_ms": 1e3 * statistics.mean(sl), "throughput_bases_per_s": total_bases / smk,
+                       "jobs_per_s": len(arr) / smk, "max_group": max(groups)},
+            "plain": {"p50_ms": 1e3 * percentile(pl, 50), "p99_ms": 1e3 * percentile(pl, 99),
+                      "mean_ms": 1e3 * statistics.mean(pl), "throughput_bases_per_s": total_bases / pmk,
+                      "jobs_per_s": len(arr) / pmk},
+        })
+    st = srv.stats()
+    srv.close()
+    for cx in ctxs.values():
+        cx.close()
+    for _, p, _, _ in jobs:
+        p.close()
+    return {
+        "workload": f"serve{len(jobs)}",
+        "description": "Poisson arrivals; half --ref jobs (0.5-50 Mbp log-uniform, cutoff 1), half --read jobs "
+                       "(1-5 M x 150 bp reads, 0.5% errors, 20-40x, cutoff 2); k=31; latency = arrival -> all "
+                       "outputs on the host",
+        "jobs": len(jobs), "bases": total_bases, "plain_service_jobs_per_s": mu,
+        "plain_sequential_bases_per_s": total_bases / seq_s,
+        "server": {"slots": 4, "batch_max_bases": 64_000_000, "small_job_bases": 4_000_000,
+                   "batches": int(st.batches), "batched_jobs": int(st.batched_jobs),
+                   "max_running": int(st.max_running)},
+        "rates": rates, "generation_s": round(gen_s, 1),
+    }
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"

@@ -796,88 +796,109 @@ int cfg_batch_unitigs(cfg_batch* b, float* device_ms) {
     if (!b->have_run) return bfail(b, CFG_ERR_STATE, "no completed batch run");
     BCK(cudaSetDevice(b->device));
     const uint32_t J = b->n_jobs;
-    std::vector<unsigned long long> jn(J), jb(J), ob(J);
-    unsigned long long n = 0, out = 0;
+    std::vector<unsigned long long> jn(J), ob(J);
+    unsigned long long n_all = 0, out = 0;
     for (uint32_t j = 0; j < J; ++j) {
         const JobOut& x = b->h_jobs[j];
         jn[j] = b->redo[j] ? 0 : x.lm_used;
-        jb[j] = n; n += jn[j];
+        n_all += jn[j];
         ob[j] = out; out += b->redo[j] ? 0 : x.lm_text_used + 4 * x.lm_used + 16;
     }
     if (!b->u_n.ensure(8ull * J) || !b->u_base.ensure(8ull * J) || !b->u_out.ensure(8ull * J) ||
-        !b->u_cur.ensure(8ull * JOB_CUR_STRIDE * J) || !b->u_err.ensure(16) || !b->ub.ensure(n) || !b->ub.ensure_out(out + 16))
+        !b->u_cur.ensure(8ull * JOB_CUR_STRIDE * J) || !b->u_err.ensure(16) || !b->ub.ensure_out(out + 16))
         return bfail(b, CFG_ERR_OOM, "collation buffers");
+    // jobs are joined in chunks that fit the free device memory (jobs never join each other)
+    size_t fr = 0, tot = 0;
+    BCK(cudaMemGetInfo(&fr, &tot));
+    const unsigned long long per_lmtig = 300;   // bytes of collation buffers per lm-tig
+    const unsigned long long cap = std::max<unsigned long long>(1ull << 20, (unsigned long long)(fr / 10 * 6) / per_lmtig);
     BCK(cudaMemcpyAsync(b->u_n.p, jn.data(), 8ull * J, cudaMemcpyHostToDevice, b->stream));
-    BCK(cudaMemcpyAsync(b->u_base.p, jb.data(), 8ull * J, cudaMemcpyHostToDevice, b->stream));
     BCK(cudaMemcpyAsync(b->u_out.p, ob.data(), 8ull * J, cudaMemcpyHostToDevice, b->stream));
     BCK(cudaMemsetAsync(b->u_cur.p, 0, 8ull * JOB_CUR_STRIDE * J, b->stream));
     BCK(cudaMemsetAsync(b->u_err.p, 0, 16, b->stream));
-    BCK(cudaEventRecord(b->ev[0], b->stream));
-    UnitigInput in{};
-    in.k = b->p.k; in.n = n; in.err = b->u_err.as<uint32_t>();
-    in.jobs = b->jobs.as<JobOut>(); in.n_jobs = J;
-    in.job_n = b->u_n.as<unsigned long long>(); in.job_lm_base = b->u_base.as<unsigned long long>();
-    in.job_out_base = b->u_out.as<unsigned long long>(); in.job_cur = b->u_cur.as<unsigned long long>();
-    in.job_lm = b->lm.as<LmtigOut>(); in.job_text = b->lm_text.as<char>();
-    UnitigResult res{};
-    int rc = collate_device(in, b->ub, b->stream, res);
-    if (rc) return bfail(b, rc, "batch collation");
-    BCK(cudaEventRecord(b->ev[1], b->stream));
-    uint32_t err = 0;
-    b->h_ucur.resize((size_t)JOB_CUR_STRIDE * J);
-    BCK(cudaMemcpyAsync(&err, b->u_err.p, 4, cudaMemcpyDeviceToHost, b->stream));
-    BCK(cudaMemcpyAsync(b->h_ucur.data(), b->u_cur.p, 8ull * JOB_CUR_STRIDE * J, cudaMemcpyDeviceToHost, b->stream));
-    BCK(cudaStreamSynchronize(b->stream));
-    if (err & DERR_BAD_GRAPH) return bfail(b, CFG_ERR_STATE, "lm-tig ends do not form a valid discontinuity graph");
-    if (err & DERR_CAS_LIMIT) return bfail(b, CFG_ERR_WALK_LIMIT, "vertex-table wait exceeded its bound");
-    cudaEventElapsedTime(&b->unitig_ms, b->ev[0], b->ev[1]);
-    b->h_out_base.swap(ob);
     b->u_host.assign(J, std::string());
     b->u_host_n.assign(J, 0);
-    // lm-tigs on closed chains: joined on the host, per job
-    if (res.n_cycle_lmtigs) {
-        if (!b->u_cyc_cnt.ensure(16)) return bfail(b, CFG_ERR_OOM, "cycle buffers");
-        unsigned long long cnt[2] = {0, 0};
-        BCK(cudaMemsetAsync(b->u_cyc_cnt.p, 0, 16, b->stream));
-        rc = collate_cycles_device(b->ub, n, nullptr, nullptr, b->u_cyc_cnt.as<unsigned long long>(), b->stream);
-        if (rc) return bfail(b, rc, "cycle sizing");
-        BCK(cudaMemcpyAsync(cnt, b->u_cyc_cnt.p, 16, cudaMemcpyDeviceToHost, b->stream));
+    std::vector<unsigned long long> jb(J, 0);
+    float total_ms = 0;
+    for (uint32_t j0 = 0; j0 < J;) {
+        uint32_t j1 = j0;
+        unsigned long long n = 0;
+        while (j1 < J && (j1 == j0 || n + jn[j1] <= cap)) { jb[j1] = n; n += jn[j1]; ++j1; }
+        if (!b->ub.ensure(n)) return bfail(b, CFG_ERR_OOM, "collation buffers");
+        BCK(cudaMemcpyAsync(b->u_base.as<unsigned long long>() + j0, jb.data() + j0, 8ull * (j1 - j0), cudaMemcpyHostToDevice,
+                            b->stream));
+        BCK(cudaEventRecord(b->ev[0], b->stream));
+        UnitigInput in{};
+        in.k = b->p.k; in.n = n; in.err = b->u_err.as<uint32_t>();
+        in.jobs = b->jobs.as<JobOut>() + j0; in.n_jobs = j1 - j0;
+        in.job_n = b->u_n.as<unsigned long long>() + j0; in.job_lm_base = b->u_base.as<unsigned long long>() + j0;
+        in.job_out_base = b->u_out.as<unsigned long long>() + j0;
+        in.job_cur = b->u_cur.as<unsigned long long>() + (size_t)j0 * JOB_CUR_STRIDE;
+        in.job_lm = b->lm.as<LmtigOut>(); in.job_text = b->lm_text.as<char>();
+        UnitigResult res{};
+        int rc = collate_device(in, b->ub, b->stream, res);
+        if (rc) return bfail(b, rc, "batch collation");
+        BCK(cudaEventRecord(b->ev[1], b->stream));
+        uint32_t err = 0;
+        BCK(cudaMemcpyAsync(&err, b->u_err.p, 4, cudaMemcpyDeviceToHost, b->stream));
         BCK(cudaStreamSynchronize(b->stream));
-        if (!b->u_cyc_lm.ensure(sizeof(LmtigOut) * (cnt[0] + 1)) || !b->u_cyc_text.ensure(cnt[1] + 1) ||
-            !b->u_cyc_job.ensure(4 * (cnt[0] + 1)))
-            return bfail(b, CFG_ERR_OOM, "cycle buffers");
-        BCK(cudaMemsetAsync(b->u_cyc_cnt.p, 0, 16, b->stream));
-        rc = collate_cycles_device(b->ub, n, b->u_cyc_lm.as<LmtigOut>(), b->u_cyc_text.as<char>(),
-                                   b->u_cyc_cnt.as<unsigned long long>(), b->stream, b->u_cyc_job.as<uint32_t>());
-        if (rc) return bfail(b, rc, "cycle gather");
-        std::vector<cfg_lmtig> hl(cnt[0]);
-        std::vector<uint32_t> hj(cnt[0]);
-        std::string ht(cnt[1], '\0');
-        if (cnt[0]) {
-            BCK(cudaMemcpyAsync(hl.data(), b->u_cyc_lm.p, sizeof(cfg_lmtig) * cnt[0], cudaMemcpyDeviceToHost, b->stream));
-            BCK(cudaMemcpyAsync(hj.data(), b->u_cyc_job.p, 4 * cnt[0], cudaMemcpyDeviceToHost, b->stream));
+        if (err & DERR_BAD_GRAPH) return bfail(b, CFG_ERR_STATE, "lm-tig ends do not form a valid discontinuity graph");
+        if (err & DERR_CAS_LIMIT) return bfail(b, CFG_ERR_WALK_LIMIT, "vertex-table wait exceeded its bound");
+        float ms = 0;
+        cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]);
+        total_ms += ms;
+        // lm-tigs on closed chains: joined on the host, per job
+        if (res.n_cycle_lmtigs) {
+            if (!b->u_cyc_cnt.ensure(16)) return bfail(b, CFG_ERR_OOM, "cycle buffers");
+            unsigned long long cnt[2] = {0, 0};
+            BCK(cudaMemsetAsync(b->u_cyc_cnt.p, 0, 16, b->stream));
+            rc = collate_cycles_device(b->ub, n, nullptr, nullptr, b->u_cyc_cnt.as<unsigned long long>(), b->stream);
+            if (rc) return bfail(b, rc, "cycle sizing");
+            BCK(cudaMemcpyAsync(cnt, b->u_cyc_cnt.p, 16, cudaMemcpyDeviceToHost, b->stream));
+            BCK(cudaStreamSynchronize(b->stream));
+            if (!b->u_cyc_lm.ensure(sizeof(LmtigOut) * (cnt[0] + 1)) || !b->u_cyc_text.ensure(cnt[1] + 1) ||
+                !b->u_cyc_job.ensure(4 * (cnt[0] + 1)))
+                return bfail(b, CFG_ERR_OOM, "cycle buffers");
+            BCK(cudaMemsetAsync(b->u_cyc_cnt.p, 0, 16, b->stream));
+            rc = collate_cycles_device(b->ub, n, b->u_cyc_lm.as<LmtigOut>(), b->u_cyc_text.as<char>(),
+                                       b->u_cyc_cnt.as<unsigned long long>(), b->stream, b->u_cyc_job.as<uint32_t>());
+            if (rc) return bfail(b, rc, "cycle gather");
+            std::vector<cfg_lmtig> hl(cnt[0]);
+            std::vector<uint32_t> hj(cnt[0]);
+            std::string ht(cnt[1], '\0');
+            if (cnt[0]) {
+                BCK(cudaMemcpyAsync(hl.data(), b->u_cyc_lm.p, sizeof(cfg_lmtig) * cnt[0], cudaMemcpyDeviceToHost, b->stream));
+                BCK(cudaMemcpyAsync(hj.data(), b->u_cyc_job.p, 4 * cnt[0], cudaMemcpyDeviceToHost, b->stream));
+            }
+            if (cnt[1]) BCK(cudaMemcpyAsync(&ht[0], b->u_cyc_text.p, cnt[1], cudaMemcpyDeviceToHost, b->stream));
+            BCK(cudaStreamSynchronize(b->stream));
+            std::vector<std::vector<cfg_lmtig>> per(j1 - j0);
+            for (uint64_t i = 0; i < cnt[0]; ++i) per[hj[i]].push_back(hl[i]);
+            for (uint32_t j = j0; j < j1; ++j) {
+                if (per[j - j0].empty()) continue;
+                char* o = nullptr;
+                uint64_t ob2 = 0, nu = 0, nc = 0;
+                rc = cfg_collate_lmtigs(b->p.k, per[j - j0].data(), per[j - j0].size(), ht.data(), &o, &ob2, &nu, &nc);
+                if (rc) return bfail(b, rc, "cycle collation");
+                b->u_host[j].assign(o, ob2);
+                cfg_free(o);
+                b->u_host_n[j] = nu;
+            }
         }
-        if (cnt[1]) BCK(cudaMemcpyAsync(&ht[0], b->u_cyc_text.p, cnt[1], cudaMemcpyDeviceToHost, b->stream));
-        BCK(cudaStreamSynchronize(b->stream));
-        std::vector<std::vector<cfg_lmtig>> per(J);
-        for (uint64_t i = 0; i < cnt[0]; ++i) per[hj[i]].push_back(hl[i]);
-        for (uint32_t j = 0; j < J; ++j) {
-            if (per[j].empty()) continue;
-            char* o = nullptr;
-            uint64_t ob2 = 0, nu = 0, nc = 0;
-            rc = cfg_collate_lmtigs(b->p.k, per[j].data(), per[j].size(), ht.data(), &o, &ob2, &nu, &nc);
-            if (rc) return bfail(b, rc, "cycle collation");
-            b->u_host[j].assign(o, ob2);
-            cfg_free(o);
-            b->u_host_n[j] = nu;
-        }
+        j0 = j1;
     }
+    b->h_ucur.resize((size_t)JOB_CUR_STRIDE * J);
+    BCK(cudaMemcpyAsync(b->h_ucur.data(), b->u_cur.p, 8ull * JOB_CUR_STRIDE * J, cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    b->unitig_ms = total_ms;
+    b->h_out_base.swap(ob);
+    (void)n_all;
     // jobs redone alone: their lm-tigs are on the host already
     for (uint32_t j = 0; j < J; ++j) {
         if (!b->redo[j]) continue;
         char* o = nullptr;
         uint64_t ob2 = 0, nu = 0, nc = 0;
-        rc = cfg_collate_lmtigs(b->p.k, b->r_lm[j].data(), b->r_lm[j].size(), b->r_text[j].data(), &o, &ob2, &nu, &nc);
+        const int rc = cfg_collate_lmtigs(b->p.k, b->r_lm[j].data(), b->r_lm[j].size(), b->r_text[j].data(), &o, &ob2, &nu, &nc);
         if (rc) return bfail(b, rc, "redone job collation");
         b->u_host[j] = b->r_fasta[j] + std::string(o, ob2);
         cfg_free(o);

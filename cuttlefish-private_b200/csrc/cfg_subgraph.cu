@@ -133,9 +133,18 @@ struct Tab {
     }
     // owner rank and home index inside the owner's sub-table
     __device__ __forceinline__ void place(const Kmer<W>& x, uint32_t& r, uint32_t& h) const {
-        const uint64_t z = key_hash(x);
-        r = (uint32_t)(((uint64_t)(uint32_t)z * nranks) >> 32);
-        h = (uint32_t)(((z >> 32) * per) >> 32);
+        if constexpr (MODE == LOCAL) {
+            // one table: a multiplicative hash's top bits pick the home slot
+            uint64_t z;
+            if constexpr (W == 1) z = x.lo * 0x9E3779B97F4A7C15ull;
+            else z = (x.lo ^ (x.hi * 0xC2B2AE3D27D4EB4Full)) * 0x9E3779B97F4A7C15ull;
+            r = 0;
+            h = (uint32_t)(((z >> 32) * per) >> 32);
+        } else {
+            const uint64_t z = key_hash(x);
+            r = (uint32_t)(((uint64_t)(uint32_t)z * nranks) >> 32);
+            h = (uint32_t)(((z >> 32) * per) >> 32);
+        }
     }
     __device__ uint32_t find(const Kmer<W>& x) const {   // read-only phase, any CTA
         uint32_t r, h;
@@ -251,6 +260,7 @@ struct Block {   // per-CTA shared bookkeeping (in CLUSTER mode the flags of ran
 };
 
 constexpr uint32_t FULL = 0xffffffffu;
+constexpr uint32_t STEP_BUF = 64;   // bases a path walk keeps for its label (2 bits each)
 
 // Exclusive scan of one value per thread over the CTA; B.scan_total gets the sum.
 // Every thread of the CTA must call it.
@@ -390,24 +400,50 @@ __device__ __forceinline__ bool step(const Tab<W, MODE>& T, const KOps<W>& ops, 
 }
 
 
+// Bytes written one at a time in address order (rising or falling), gathered into
+// whole 8-byte words: one store per aligned word the run covers, byte stores only
+// at its two ragged ends.
+struct WordWriter {
+    unsigned long long base = ~0ull;   // address of the aligned word being gathered
+    unsigned long long w = 0;
+    uint32_t mask = 0;                 // bytes of that word gathered so far
+    __device__ __forceinline__ void flush() {
+        if (!mask) return;
+        if (mask == 0xFFu) *(unsigned long long*)base = w;
+        else
+            for (uint32_t b = 0; b < 8; ++b)
+                if ((mask >> b) & 1) ((char*)base)[b] = (char)(w >> (8 * b));
+        mask = 0; w = 0;
+    }
+    __device__ __forceinline__ void put(char* a, char c) {
+        const unsigned long long ad = (unsigned long long)a, wb = ad & ~7ull;
+        if (wb != base) { flush(); base = wb; }
+        const uint32_t o = (uint32_t)(ad & 7);
+        w |= (unsigned long long)(uint8_t)c << (8 * o);
+        mask |= 1u << o;
+    }
+};
+
 // Writes the label of the path of n vertices that starts at v (in walk direction).
 template <int W, int MODE>
 __device__ void write_path(const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t fth, DV<W> v, int side, uint32_t n,
                            char* dst, bool rev, bool mark) {
     const uint32_t k = ops.k, L = n + k - 1;
+    WordWriter ww;
     auto put = [&](uint32_t i, uint32_t b) {
-        if (!rev) dst[i] = "ACGT"[b];
-        else dst[L - 1 - i] = "ACGT"[3 - b];
+        if (!rev) ww.put(dst + i, "ACGT"[b]);
+        else ww.put(dst + (L - 1 - i), "ACGT"[3 - b]);
     };
     if (dst) for (uint32_t i = 0; i < k; ++i) put(i, ops.base(v.d, i));
     if (mark) T.or_meta(v.slot, M_VISITED);
     for (uint32_t t = 1; t < n; ++t) {
         int s_in;
-        if (!step(T, ops, fth, v, side, s_in)) return;
+        if (!step(T, ops, fth, v, side, s_in)) break;
         if (dst) put(k - 1 + t, ops.last_base(v.d));
         if (mark) T.or_meta(v.slot, M_VISITED);
         side = 1 - s_in;
     }
+    if (dst) ww.flush();
 }
 
 // A one-k-mer cycle (a self-looped homopolymer seeded on its own) at reserved FASTA offset o.
@@ -458,18 +494,38 @@ struct RecBases {
 // A path of n vertices from v0 (leaving through side0) to vlast, written into space
 // reserved by reserve_warp: a trivial maximal unitig at FASTA offset fo, or an lm-tig
 // (lm: one end exits the subgraph) as record idx with its label at offset off.
+// The label of a path whose bases the walk kept: the walk's first k-mer, then one base
+// per step; `skip` leading bases are not part of the path (a one-k-mer cycle at its start).
+template <int W>
+__device__ void write_buffered(const KOps<W>& ops, const Kmer<W>& first, unsigned long long steps0,
+                               unsigned long long steps1, uint32_t skip, uint32_t L, char* dst, bool rev) {
+    if (!dst) return;
+    const uint32_t k = ops.k;
+    WordWriter ww;
+    for (uint32_t i = 0; i < L; ++i) {
+        const uint32_t j = i + skip;   // index in the walk's base sequence
+        const uint32_t q = j - k;      // step index (j >= k)
+        const uint32_t b = j < k ? ops.base(first, j) : (uint32_t)((q < 32 ? steps0 : steps1) >> (2 * (q & 31))) & 3u;
+        if (!rev) ww.put(dst + i, "ACGT"[b]);
+        else ww.put(dst + (L - 1 - i), "ACGT"[3 - b]);
+    }
+    ww.flush();
+}
+
 template <int W, int MODE>
 __device__ void write_emitted_path(const SubgraphArgs& a, const Tab<W, MODE>& T, const KOps<W>& ops, const DV<W>& v0,
                                    int side0, uint32_t n, const DV<W>& vlast, EndInfo st, EndInfo en, bool seed_canon,
                                    Block& B, bool lm, unsigned long long fo, unsigned long long idx,
-                                   unsigned long long off) {
+                                   unsigned long long off, bool buffered, unsigned long long steps0,
+                                   unsigned long long steps1, const Kmer<W>& first, uint32_t skip) {
     const uint32_t k = ops.k, fth = a.fth;
     const uint32_t L = n + k - 1;
     if (!lm) {
         // trivial maximal unitig in canonical orientation (Maximal_Unitig_Scratch::finalize, :200-222)
         const bool rev = vlast.r < v0.d;   // rc(last k-mer) < first k-mer
         char* p = fasta_at(B.sk, fo, L);
-        write_path(T, ops, fth, v0, side0, n, p, rev, true);
+        if (buffered) write_buffered(ops, first, steps0, steps1, skip, L, p, rev);
+        else write_path(T, ops, fth, v0, side0, n, p, rev, true);
         atomicAdd(&B.trivial, 1ull);
         return;
     }
@@ -482,7 +538,8 @@ __device__ void write_emitted_path(const SubgraphArgs& a, const Tab<W, MODE>& T,
     atomicAdd(&B.lmtig, 1ull);
     const bool fits = idx < sk.lm_cap && off + L <= sk.lm_text_cap;
     if (!fits) atomicOr(sk.oflow, DERR_OUT_OVERFLOW);
-    write_path(T, ops, fth, v0, side0, n, fits ? sk.lm_text + off : nullptr, rev, true);
+    if (buffered) write_buffered(ops, first, steps0, steps1, skip, L, fits ? sk.lm_text + off : nullptr, rev);
+    else write_path(T, ops, fth, v0, side0, n, fits ? sk.lm_text + off : nullptr, rev, true);
     if (!fits) return;
     LmtigOut o;
     const Kmer<W> phi = phi_kmer(ops);
@@ -682,7 +739,9 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         const uint32_t i = base + tid;
         // what this lane emits: one-k-mer cycles at s and/or e, and one path vs..ve
         bool kc0 = false, kc1 = false, mark0 = false, mark1 = false, path = false, lm = false;
-        uint32_t s = 0, e = 0, n2 = 0;
+        uint32_t s = 0, e = 0, n2 = 0, walked = 0;   // walked: vertices of the two-end walk (0: one vertex)
+        unsigned long long steps0 = 0, steps1 = 0;   // bases of walk steps 1..32, 33..64
+        Kmer<W> first{};
         DV<W> vs{}, ve{};
         int sd0 = BACK;
         EndInfo st{0, 0, true}, en{0, 0, true};
@@ -704,7 +763,9 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
                 const int side0 = okf ? FRONT : BACK;   // walk through the linked side
                 const uint32_t ins0 = st_ins(lst[ls]);
                 const DV<W> v0 = dv_at(T, ops, s, side0);
-                // pass 1: the other end, first-occurrence minima
+                // pass 1: the other end, first-occurrence minima; the walk marks its vertices
+                // and keeps the bases it steps through (2 bits each, up to STEP_BUF of them),
+                // so the emitting end writes its label without walking again
                 DV<W> v = v0; int side = side0;
                 uint32_t n = 1;
                 uint32_t v1_slot = s; int v1_side = side0;     // second vertex
@@ -712,6 +773,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
                 uint32_t m_int = 0xffffffffu; bool m_int_canon = true;
                 uint32_t cur_meta = meta;
                 bool ok = true;
+                T.or_meta(s, M_VISITED);
                 while (term_of(cur_meta, side) == T_OK) {
                     if (n > 1) {   // v is interior
                         const uint32_t ic = st_ins(T.ld_st(v.slot));
@@ -722,6 +784,11 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
                     if (!step(T, ops, fth, v, side, s_in)) { atomicOr(a.err, DERR_MISSING_KEY); ok = false; break; }
                     side = 1 - s_in;
                     cur_meta = T.ld_meta(v.slot);
+                    T.or_meta(v.slot, M_VISITED);
+                    if (n <= STEP_BUF) {
+                        const unsigned long long bb = (unsigned long long)ops.last_base(v.d) << (2 * ((n - 1) & 31));
+                        if (n <= 32) steps0 |= bb; else steps1 |= bb;
+                    }
                     if (n == 1) { v1_slot = v.slot; v1_side = side; }
                     if (++n > T.per * T.nranks + 1) { atomicOr(a.err, DERR_WALK_LIMIT); ok = false; break; }
                 }
@@ -737,6 +804,8 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
                     const bool fake0 = q0 && ins0 < m, fake1 = q1 && ins1 < m;
                     kc0 = mark0 = fake0; kc1 = mark1 = fake1;
                     n2 = n - fake0 - fake1;
+                    walked = n;
+                    first = v0.d;
                     if (n2 > 0) {
                         path = true;
                         if (!fake0) { st = EndInfo{s, term_of(meta, 1 - side0), side0 == BACK}; vs = v0; sd0 = side0; }
@@ -759,7 +828,11 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         unsigned long long fo = r.fa;
         if (kc0) { write_kmer_cycle(T, ops, s, B, fo); fo += k + 4; }
         if (kc1) { write_kmer_cycle(T, ops, e, B, fo); fo += k + 4; }
-        if (path) write_emitted_path(a, T, ops, vs, sd0, n2, ve, st, en, best_canon, B, lm, fo, r.lm_idx, r.lm_off);
+        if (path) {
+            const bool buffered = walked > 0 && walked - 1 <= STEP_BUF;
+            write_emitted_path(a, T, ops, vs, sd0, n2, ve, st, en, best_canon, B, lm, fo, r.lm_idx, r.lm_off,
+                               buffered, steps0, steps1, first, kc0 ? 1u : 0u);
+        }
         if (mark0) T.or_meta(s, M_VISITED);
         if (mark1) T.or_meta(e, M_VISITED);
     }
