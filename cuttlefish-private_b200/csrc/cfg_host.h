@@ -106,7 +106,8 @@ struct UnitigInput {
 };
 // ... the buffers it works in ...
 struct UnitigBuffers {
-    DevBuf b_lm, b_label, b_tab, b_partner, b_P0, b_P1, b_R0, b_R1, b_A0, b_A1, b_fin, b_off, b_words, b_out, b_job;
+    DevBuf b_lm, b_label, b_tab, b_partner, b_P0, b_P1, b_R0, b_R1, b_A0, b_A1, b_fin, b_off, b_words, b_out, b_job, b_flip;
+    uint8_t* flipb = nullptr;  // per lm-tig heading its chain's walked list: flip it
     LmtigOut* lm = nullptr;
     uint32_t* job = nullptr;   // batch: each gathered lm-tig's job
     const char** label = nullptr;
@@ -128,7 +129,7 @@ struct UnitigBuffers {
     }
     void release() {
         DevBuf* all[] = {&b_lm, &b_label, &b_tab, &b_partner, &b_P0, &b_P1, &b_R0, &b_R1, &b_A0, &b_A1, &b_fin, &b_off,
-                         &b_words, &b_out, &b_job};
+                         &b_words, &b_out, &b_job, &b_flip};
         for (DevBuf* b : all) b->release();
     }
 };

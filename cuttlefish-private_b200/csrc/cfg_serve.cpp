@@ -10,12 +10,13 @@
 // Several workers run at once, so jobs overlap on the device (their kernels share
 // the SMs; their copies overlap other jobs' kernels).  Contexts keep their device
 // buffers between jobs (tables, record and output arenas stay allocated), so a
-// warm server allocates nothing per request.  Memory admission: every context
-// holds an estimate of its device footprint; a job starts only when the
-// footprints of all contexts, with the one it runs on grown to the job's
-// estimate, fit the budget (idle contexts are dropped first when they do not).
-// The job at the head of the queue always goes first, and runs alone when
-// nothing else is running, so nothing starves.
+// warm server allocates nothing per request.  Memory admission: every job (or
+// group) has a device-footprint estimate; it starts only when the footprints of the
+// groups already running plus its own fit the budget, decided under the queue lock
+// so two workers cannot both see room for one.  Idle contexts are dropped (oldest
+// first) when the contexts' footprints outgrow the budget.  The job at the head of
+// the queue always goes first, and runs alone when nothing else is running, so
+// nothing starves.
 //
 // A plain job's results stay in its context's page-locked buffers (no copy) until
 // the ticket is released; a batched job's results are copied out of the batch.
@@ -98,6 +99,7 @@ struct cfg_server {
     std::unordered_map<uint64_t, std::unique_ptr<Ticket>> tickets;
     uint64_t next_id = 1;
     uint64_t held_bytes = 0;      // footprints of every live context
+    uint64_t inflight = 0;        // footprints of the groups running now (admission)
     uint32_t running = 0;         // groups in flight
     bool stop = false;
     std::vector<std::unique_ptr<Worker>> workers;
@@ -129,15 +131,9 @@ std::vector<Ticket*> take_group(cfg_server* s, Worker& w, uint64_t& need, bool& 
     }
     batched = g.size() > 1;
     need = footprint(head->p, bases);
-    // device memory: this worker's matching context grows to `need`; others stay
-    uint64_t mine = 0;
-    if (batched) {
-        for (auto& b : w.batches) if (same_params(b->p, head->p)) mine = std::max(mine, b->bytes);
-    } else {
-        for (auto& c : w.ctxs) if (!c->busy && same_params(c->p, head->p)) mine = std::max(mine, c->bytes);
-    }
-    const uint64_t after = s->held_bytes - mine + std::max(mine, need);
-    if (after > s->cfg.hbm_budget && s->running > 0) { g.clear(); return g; }
+    // admitted when the running groups' footprints and this one fit the budget; the
+    // head runs alone when nothing else runs, so nothing starves
+    if (s->inflight + need > s->cfg.hbm_budget && s->running > 0) { g.clear(); return g; }
     for (Ticket* t : g) s->queue.erase(std::find(s->queue.begin(), s->queue.end(), t));
     return g;
 }
@@ -237,6 +233,7 @@ void worker_loop(cfg_server* s, Worker* w) {
             const auto now = Clock::now();
             for (Ticket* t : g) { t->state = 1; t->t_start = now; }
             ++s->running;
+            s->inflight += need;
             s->st.max_running = std::max<uint64_t>(s->st.max_running, s->running);
             if (batched) { ++s->st.batches; s->st.batched_jobs += g.size(); }
         }
@@ -253,6 +250,7 @@ void worker_loop(cfg_server* s, Worker* w) {
                 s->st.bases += t->in.n_bases;
             }
             --s->running;
+            s->inflight -= need;
         }
         s->cv_done.notify_all();
         s->cv_work.notify_all();

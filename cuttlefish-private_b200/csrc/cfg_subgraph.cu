@@ -42,6 +42,7 @@ namespace {
 constexpr uint32_t NONE = 0xffffffffu;
 constexpr uint64_t EMPTY = ~0ull;
 constexpr uint64_t BUSY = ~1ull;   // a two-word key's high word while its low word is written
+constexpr uint64_t ST_INIT = 0xffffffff00000000ull;   // a new slot's state: no edges, first occurrence "none"
 // walk termination kinds (Walk_Termination, include/Subgraph.hpp:362-369)
 constexpr uint32_t T_OK = 0, T_BRANCHED = 1, T_CROSSED = 2, T_DEAD = 3, T_EXIT = 4;
 // meta layout: bits 0-2 visited / disc front / disc back; 3 Q (self-looped homopolymer);
@@ -69,6 +70,7 @@ template <> struct Mem<LOCAL> {
     static __device__ __forceinline__ uint64_t exch64(A a, uint64_t v) { uint64_t o; asm volatile("atom.shared.exch.b64 %0, [%1], %2;" : "=l"(o) : "r"(a), "l"(v) : "memory"); return o; }
     static __device__ __forceinline__ void or32(A a, uint32_t v) { asm volatile("red.shared.or.b32 [%0], %1;" :: "r"(a), "r"(v) : "memory"); }
     static __device__ __forceinline__ void fence() { __threadfence_block(); }
+    static __device__ __forceinline__ void ld2(A a, uint64_t& x, uint64_t& y) { asm volatile("ld.volatile.shared.v2.u64 {%0, %1}, [%2];" : "=l"(x), "=l"(y) : "r"(a) : "memory"); }
 };
 template <> struct Mem<CLUSTER> {
     typedef uint32_t A;
@@ -80,6 +82,7 @@ template <> struct Mem<CLUSTER> {
     static __device__ __forceinline__ uint64_t exch64(A a, uint64_t v) { uint64_t o; asm volatile("atom.relaxed.cluster.shared::cluster.exch.b64 %0, [%1], %2;" : "=l"(o) : "r"(a), "l"(v) : "memory"); return o; }
     static __device__ __forceinline__ void or32(A a, uint32_t v) { asm volatile("red.relaxed.cluster.shared::cluster.or.b32 [%0], %1;" :: "r"(a), "r"(v) : "memory"); }
     static __device__ __forceinline__ void fence() { asm volatile("fence.acq_rel.cluster;" ::: "memory"); }
+    static __device__ __forceinline__ void ld2(A a, uint64_t& x, uint64_t& y) { asm volatile("ld.relaxed.cluster.shared::cluster.v2.u64 {%0, %1}, [%2];" : "=l"(x), "=l"(y) : "r"(a) : "memory"); }
 };
 template <> struct Mem<GLOBAL> {
     typedef uint64_t A;   // generic address of global memory
@@ -91,6 +94,9 @@ template <> struct Mem<GLOBAL> {
     static __device__ __forceinline__ uint64_t exch64(A a, uint64_t v) { return atomicExch((unsigned long long*)a, (unsigned long long)v); }
     static __device__ __forceinline__ void or32(A a, uint32_t v) { atomicOr((unsigned int*)a, v); }
     static __device__ __forceinline__ void fence() { __threadfence(); }
+    static __device__ __forceinline__ void ld2(A a, uint64_t& x, uint64_t& y) {
+        asm volatile("ld.volatile.v2.u64 {%0, %1}, [%2];" : "=l"(x), "=l"(y) : "l"(a) : "memory");
+    }
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -109,7 +115,9 @@ template <int W, int MODE>
 struct Tab {
     typedef Mem<MODE> M;
     typedef typename M::A A;
-    A keys, st, meta;           // this CTA's base addresses (W key words per slot, ef | ins << 32, meta)
+    // this CTA's base addresses: keys, states (ef | ins << 32), meta.  For k <= 31 a slot's
+    // key and state are one 16-byte pair (keys + 16 s, st = keys + 8), read by one load.
+    A keys, st, meta;
     uint32_t per, shift, pmask; // slots per sub-table; slot s lives in rank s >> shift at index s & pmask
     uint32_t nranks, rank;
     uint32_t* err_flag;         // set when a wait on a key being written exceeds its bound
@@ -118,8 +126,8 @@ struct Tab {
         if constexpr (MODE == CLUSTER) return mapa_cluster(base + (s & pmask) * bytes, s >> shift);
         else return base + (A)s * bytes;
     }
-    __device__ __forceinline__ A ka(uint32_t s) const { return addr(keys, s, 8 * W); }
-    __device__ __forceinline__ A sa(uint32_t s) const { return addr(st, s, 8); }
+    __device__ __forceinline__ A ka(uint32_t s) const { return addr(keys, s, 16); }
+    __device__ __forceinline__ A sa(uint32_t s) const { return addr(st, s, W == 1 ? 16 : 8); }
     __device__ __forceinline__ A ma(uint32_t s) const { return addr(meta, s, 4); }
 
     __device__ __forceinline__ uint64_t ld_st(uint32_t s) const { return M::ld64(sa(s)); }
@@ -146,34 +154,44 @@ struct Tab {
             h = (uint32_t)(((z >> 32) * per) >> 32);
         }
     }
-    __device__ uint32_t find(const Kmer<W>& x) const {   // read-only phase, any CTA
+    // read-only phases, any CTA: the slot of x (NONE if absent) and its state word
+    __device__ uint32_t find(const Kmer<W>& x, uint64_t& stv) const {
         uint32_t r, h;
         place(x, r, h);
         const uint32_t b = r * per;
         for (uint32_t p = 0; p < per; ++p) {
             const A a = ka(b + h);
-            const uint64_t top = M::ld64(a + 8 * (W - 1));
-            if (top == EMPTY) return NONE;
-            if constexpr (W == 1) { if (top == x.lo) return b + h; }
-            else { if (top == x.hi && M::ld64(a) == x.lo) return b + h; }
+            if constexpr (W == 1) {
+                uint64_t top;
+                M::ld2(a, top, stv);   // key and state together
+                if (top == EMPTY) return NONE;
+                if (top == x.lo) return b + h;
+            } else {
+                const uint64_t top = M::ld64(a + 8);
+                if (top == EMPTY) return NONE;
+                if (top == x.hi && M::ld64(a) == x.lo) { stv = ld_st(b + h); return b + h; }
+            }
             if (++h == per) h = 0;
         }
         return NONE;
     }
+    __device__ __forceinline__ uint32_t find(const Kmer<W>& x) const { uint64_t t; return find(x, t); }
     // build phase: find or insert x in sub-table `owner` starting at its home index h;
     // returns the global slot or NONE.  Other ranks' sub-tables are reached through DSMEM.
-    __device__ uint32_t find_or_insert(const Kmer<W>& x, uint32_t owner, uint32_t h, bool& fresh) const {
+    // `seen`: a recent value of the slot's state word, the first expected value of its CAS
+    __device__ uint32_t find_or_insert(const Kmer<W>& x, uint32_t owner, uint32_t h, bool& fresh, uint64_t& seen) const {
         fresh = false;
         const uint32_t b = owner * per;
         for (uint32_t p = 0; p < per; ++p) {
             const A a = ka(b + h);
             if constexpr (W == 1) {
-                const uint64_t cur = M::ld64(a);
-                if (cur == x.lo) return b + h;
+                uint64_t cur, stv;
+                M::ld2(a, cur, stv);   // key and state together
+                if (cur == x.lo) { seen = stv; return b + h; }
                 if (cur == EMPTY) {
                     const uint64_t old = M::cas64(a, EMPTY, x.lo);
-                    if (old == EMPTY) { fresh = true; return b + h; }
-                    if (old == x.lo) return b + h;
+                    if (old == EMPTY) { fresh = true; seen = ST_INIT; return b + h; }
+                    if (old == x.lo) { seen = stv; return b + h; }
                 }
             } else {
                 // two-word key: claim the high word with a 64-bit CAS (EMPTY -> BUSY), write
@@ -186,6 +204,7 @@ struct Tab {
                         M::fence();
                         M::exch64(a + 8, x.hi);
                         fresh = true;
+                        seen = ST_INIT;
                         return b + h;
                     }
                 }
@@ -195,7 +214,7 @@ struct Tab {
                 }
                 if (hi == x.hi) {
                     M::fence();
-                    if (M::ld64(a) == x.lo) return b + h;
+                    if (M::ld64(a) == x.lo) { seen = M::ld64(sa(b + h)); return b + h; }
                 }
             }
             if (++h == per) h = 0;
@@ -203,9 +222,8 @@ struct Tab {
         return NONE;
     }
     // state word update: ef gets the edges, ins the earliest position (one CAS unless unchanged)
-    __device__ __forceinline__ void update_state(uint32_t s, uint32_t front, uint32_t back, uint32_t pos) const {
+    __device__ __forceinline__ void update_state(uint32_t s, uint32_t front, uint32_t back, uint32_t pos, uint64_t cur) const {
         const A a = sa(s);
-        uint64_t cur = M::ld64(a);
         for (uint32_t it = 0;; ++it) {
             const uint32_t ef = ef_add((uint32_t)cur, front, back);
             const uint32_t in = min((uint32_t)(cur >> 32), pos);
@@ -360,28 +378,31 @@ template <int W>
 __device__ __forceinline__ void put_key(uint64_t out[2], const Kmer<W>& x) { out[0] = x.lo; out[1] = x.hi_word(); }
 
 // A vertex in walk direction: its directed k-mer, the reverse complement, and its slot.
-template <int W> struct DV { Kmer<W> d, r; uint32_t slot; };
+template <int W> struct DV { Kmer<W> d, r; uint32_t slot; uint64_t st; };   // st: the slot's state word
 
 // Oriented vertex leaving slot s through `side`: the directed form is the canonical
 // k-mer when leaving through the back side (Directed_Vertex exit_side, :295-299).
 template <int W, int MODE>
 __device__ __forceinline__ DV<W> dv_at(const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t s, int side) {
     const Kmer<W> x = T.key(s), xr = ops.rc(x);
-    return side == BACK ? DV<W>{x, xr, s} : DV<W>{xr, x, s};
+    const uint64_t st = T.ld_st(s);
+    return side == BACK ? DV<W>{x, xr, s, st} : DV<W>{xr, x, s, st};
 }
 
 // One walk step out of v through `side` (which must hold a single passing edge):
-// the next vertex and the side it is entered by.
+// the next vertex (with its state word) and the side it is entered by.
 template <int W, int MODE>
 __device__ __forceinline__ bool step_inline(const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t fth, DV<W>& v, int side, int& s_in) {
-    const uint32_t e = ef_edge_at(st_ef(T.ld_st(v.slot)), side, fth);
+    const uint32_t e = ef_edge_at(st_ef(v.st), side, fth);
     const uint32_t b = side == BACK ? e : 3 - e;
     ops.push_back(v.d, b);
     ops.push_front(v.r, 3 - b);
     const bool c = v.d < v.r;
-    const uint32_t u = T.find(c ? v.d : v.r);
+    uint64_t stv = 0;
+    const uint32_t u = T.find(c ? v.d : v.r, stv);
     if (u == NONE) return false;
     v.slot = u;
+    v.st = stv;
     s_in = c ? FRONT : BACK;
     return true;
 }
@@ -456,8 +477,10 @@ __device__ void write_kmer_cycle(const Tab<W, MODE>& T, const KOps<W>& ops, uint
 
 template <int W>
 __device__ __forceinline__ bool local_empty(const unsigned long long* lkeys, uint32_t ls) {
-    return lkeys[(size_t)ls * W + (W - 1)] == EMPTY;
+    return lkeys[(size_t)ls * 2 + (W - 1)] == EMPTY;   // the key's high word (16 bytes per slot's key part)
 }
+// index of local slot ls's state word in the state array (interleaved with the keys for k <= 31)
+template <int W> __device__ __forceinline__ uint32_t sti(uint32_t ls) { return W == 1 ? 2 * ls : ls; }
 
 struct EndInfo { uint32_t slot; uint32_t term; bool canon; };   // a path end in walk direction
 
@@ -567,8 +590,8 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
     const uint32_t base_slot = rank * per;
 
     for (uint32_t s = tid; s < per; s += nt) {
-        if constexpr (W == 1) lkeys[s] = EMPTY; else { lkeys[2 * s] = EMPTY; lkeys[2 * s + 1] = EMPTY; }
-        lst[s] = 0xffffffff00000000ull;   // ef 0, first occurrence "none"
+        if constexpr (W == 1) lkeys[2 * s] = EMPTY; else { lkeys[2 * s] = EMPTY; lkeys[2 * s + 1] = EMPTY; }
+        lst[sti<W>(s)] = ST_INIT;
         lmeta[s] = 0;
     }
     if (tid == 0) {
@@ -593,12 +616,13 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         uint32_t owner, h;
         T.place(can, owner, h);
         bool fresh;
-        const uint32_t s = T.find_or_insert(can, owner, h, fresh);
+        uint64_t seen = ST_INIT;
+        const uint32_t s = T.find_or_insert(can, owner, h, fresh, seen);
         if (s == NONE) { atomicOr(&B.overflow, 1u); return false; }
         // fresh vertices are counted per inserting CTA (records, hence inserts, are spread
         // evenly, so one CTA's count stands for one sub-table's load)
         if (fresh && atomicAdd(&B.inserted, 1u) + 1 > limit) { atomicOr(&B.overflow, 1u); return false; }
-        T.update_state(s, front, back, p);
+        T.update_state(s, front, back, p, seen);
         uint32_t disc = 0;
         if (l_mark) disc |= canon ? M_DISC_F : M_DISC_B;      // entrance side
         if (r_mark) disc |= canon ? M_DISC_B : M_DISC_F;      // exit side
@@ -687,7 +711,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
     for (uint32_t i = tid, nw = B.wl_n; i < nw; i += nt) {
         const uint32_t ls = wl[i];
         const uint32_t s = base_slot + ls;
-        const uint32_t ef = st_ef(lst[ls]);
+        const uint32_t ef = st_ef(lst[sti<W>(ls)]);
         uint32_t meta = lmeta[ls];
         const uint32_t cf = ef_count(ef, FRONT, fth), cb = ef_count(ef, BACK, fth);
         atomicAdd(&B.vertices, 1ull);
@@ -709,11 +733,12 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
                 if (side == BACK) { y = x; ops.push_back(y, e); yr = xr; ops.push_front(yr, 3 - e); }
                 else { y = xr; ops.push_back(y, 3 - e); yr = x; ops.push_front(yr, e); }
                 const bool yc = y < yr;
-                const uint32_t u = T.find(yc ? y : yr);
+                uint64_t ust = 0;
+                const uint32_t u = T.find(yc ? y : yr, ust);
                 const int s_in = yc ? FRONT : BACK;
                 if (u == NONE) { atomicOr(a.err, DERR_MISSING_KEY); term = T_CROSSED; }
                 else if (u == s) term = T_CROSSED;                                        // self-loop
-                else if (ef_count(st_ef(T.ld_st(u)), s_in, fth) > 1) term = T_CROSSED;    // branching entrance
+                else if (ef_count(st_ef(ust), s_in, fth) > 1) term = T_CROSSED;    // branching entrance
             }
             meta |= term << (side == FRONT ? 8 : 11);
         }
@@ -761,7 +786,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
                 lmeta[ls] = lmeta[ls] | M_VISITED;
             } else {
                 const int side0 = okf ? FRONT : BACK;   // walk through the linked side
-                const uint32_t ins0 = st_ins(lst[ls]);
+                const uint32_t ins0 = st_ins(lst[sti<W>(ls)]);
                 const DV<W> v0 = dv_at(T, ops, s, side0);
                 // pass 1: the other end, first-occurrence minima; the walk marks its vertices
                 // and keeps the bases it steps through (2 bits each, up to STEP_BUF of them),
@@ -776,7 +801,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
                 T.or_meta(s, M_VISITED);
                 while (term_of(cur_meta, side) == T_OK) {
                     if (n > 1) {   // v is interior
-                        const uint32_t ic = st_ins(T.ld_st(v.slot));
+                        const uint32_t ic = st_ins(v.st);
                         if (ic < m_int) { m_int = ic; m_int_canon = side == BACK; }
                     }
                     vp_slot = v.slot; vp_side = side;
@@ -796,7 +821,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
                     e = v.slot;
                     const int e_side = side;   // the walk stops at e's side e_side
                     const uint32_t meta_e = cur_meta;
-                    const uint32_t ins1 = st_ins(T.ld_st(e));
+                    const uint32_t ins1 = st_ins(v.st);
                     const bool q0 = meta & M_Q, q1 = meta_e & M_Q;
                     uint32_t m = m_int;
                     if (!q0 && ins0 < m) m = ins0;
@@ -890,7 +915,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
             if (i >= a.dump_cap) { atomicOr(a.err, DERR_DUMP_OVERFLOW); continue; }
             StateOut o;
             put_key(o.key, T.key(s));
-            o.ef = st_ef(lst[ls]); o.g = (uint16_t)B.sk.g; o.status = (uint8_t)(lmeta[ls] & 7); o.pad = 0;
+            o.ef = st_ef(lst[sti<W>(ls)]); o.g = (uint16_t)B.sk.g; o.status = (uint8_t)(lmeta[ls] & 7); o.pad = 0;
             a.dump[i] = o;
         }
     }
@@ -915,8 +940,8 @@ template <int W>
 __device__ __forceinline__ void carve(unsigned char* base, uint32_t per, unsigned long long*& keys, unsigned long long*& st,
                                       uint32_t*& meta, uint32_t*& wl) {
     keys = (unsigned long long*)base;
-    st = (unsigned long long*)(base + (size_t)per * 8 * W);
-    meta = (uint32_t*)(base + (size_t)per * (8 * W + 8));
+    st = W == 1 ? keys + 1 : (unsigned long long*)(base + (size_t)per * 16);   // k <= 31: interleaved with the keys
+    meta = (uint32_t*)(base + (size_t)per * (W == 1 ? 16 : 24));
     wl = meta + per;
 }
 

@@ -156,6 +156,7 @@ __global__ void k_ut_rank_round(uint64_t n2, const uint32_t* __restrict__ P, con
         P2[x] = pp; R2[x] = R[p]; A2[x] = A[x] + A[p];
         act += pp != NONE;
     }
+    if (!active) return;
     for (int d = 16; d; d >>= 1) act += __shfl_down_sync(0xffffffffu, act, d);
     if ((threadIdx.x & 31) == 0 && act) atomicAdd(active, (unsigned long long)act);
 }
@@ -166,14 +167,40 @@ __device__ __forceinline__ char oriented(const char* lab, uint32_t len, uint32_t
     return (x & 1) ? comp_char(lab[len - 1 - i]) : lab[i];
 }
 
-// 3+4a: per lm-tig, the final entry; per final tail, the unitig's FASTA record.
+// 3: per chain, once (by the lm-tig heading the list the host collator walks): flip the
+// list when its reverse complement starts with a smaller k-mer (ties keep the walk).
+__global__ void k_ut_flip(const LmtigOut* __restrict__ lm, const char* const* __restrict__ label, uint64_t n,
+                          const uint32_t* __restrict__ P, const uint32_t* __restrict__ R, uint32_t k, uint8_t* flipb) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t e0 = (uint32_t)(2 * i), e1 = e0 + 1;
+        if (P[e0] != NONE || P[e1] != NONE) continue;   // on a closed chain
+        const uint32_t h0 = R[e0], h1 = R[e1];
+        const uint32_t e = h0 < h1 ? e0 : e1;
+        const uint32_t h = R[e];
+        if (h != e) continue;                           // not the head of its list
+        const uint32_t t = R[e ^ 1] ^ 1u;               // the entry of the list's tail
+        const char* lh = label[h >> 1];
+        const char* lt = label[t >> 1];
+        const uint32_t nh = lm[h >> 1].label_len, nt = lm[t >> 1].label_len;
+        bool flip = false;
+        for (uint32_t j = 0; j < k; ++j) {
+            const char a = oriented(lh, nh, h, j);
+            const char b = comp_char(oriented(lt, nt, t, nt - 1 - j));
+            if (a != b) { flip = b < a; break; }
+        }
+        flipb[i] = flip;
+    }
+}
+
+// 4a: per lm-tig, the final entry; per final tail, the unitig's FASTA record.
 // final[i] = chosen entry of lm-tig i, or NONE when i lies on a cycle.
 __global__ void k_ut_choose(const LmtigOut* __restrict__ lm, const char* const* __restrict__ label, uint64_t n,
                             const uint32_t* __restrict__ partner, const uint32_t* __restrict__ P,
                             const uint32_t* __restrict__ R, const unsigned long long* __restrict__ A, uint32_t k,
                             uint32_t* fin, unsigned long long* out_off, unsigned long long* cursor, unsigned long long* n_units,
                             unsigned long long* n_cyc, const uint32_t* __restrict__ job,
-                            const unsigned long long* __restrict__ job_out_base, unsigned long long* job_cur) {
+                            const unsigned long long* __restrict__ job_out_base, unsigned long long* job_cur,
+                            const uint8_t* __restrict__ flipb) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
@@ -188,19 +215,8 @@ __global__ void k_ut_choose(const LmtigOut* __restrict__ lm, const char* const* 
                 atomicAdd(n_cyc, 1ull);
             } else {
                 const uint32_t h0 = R[e0], h1 = R[e1];
-                uint32_t e = h0 < h1 ? e0 : e1;           // the list the host collator walks
-                const uint32_t h = R[e], hm = R[e ^ 1];   // its head; the mirror list's head
-                const uint32_t t = hm ^ 1u;               // the entry of this list's tail
-                // flip when the reverse complement starts with a smaller k-mer (ties keep the walk)
-                const char* lh = label[h >> 1];
-                const char* lt = label[t >> 1];
-                const uint32_t nh = lm[h >> 1].label_len, nt = lm[t >> 1].label_len;
-                bool flip = false;
-                for (uint32_t j = 0; j < k; ++j) {
-                    const char a = oriented(lh, nh, h, j);
-                    const char b = comp_char(oriented(lt, nt, t, nt - 1 - j));
-                    if (a != b) { flip = b < a; break; }
-                }
+                const uint32_t e = h0 < h1 ? e0 : e1;     // the list the host collator walks
+                const bool flip = flipb[R[e] >> 1];       // decided by that list's head
                 f = flip ? (e ^ 1u) : e;
                 fin[i] = f;
                 // the final list's tail: its exit end has no partner (or is phi)
@@ -298,9 +314,10 @@ bool UnitigBuffers::ensure(uint64_t n) {
     if (!b_lm.ensure(sizeof(LmtigOut) * (n + 1)) || !b_label.ensure(8 * (n + 1)) || !b_tab.ensure(sizeof(EndSlot) * t) ||
         !b_partner.ensure(4 * n2) || !b_P0.ensure(4 * n2) || !b_P1.ensure(4 * n2) || !b_R0.ensure(4 * n2) ||
         !b_R1.ensure(4 * n2) || !b_A0.ensure(8 * n2) || !b_A1.ensure(8 * n2) || !b_fin.ensure(4 * (n + 1)) ||
-        !b_off.ensure(8 * n2) || !b_words.ensure(64) || !b_job.ensure(4 * (n + 1)))
+        !b_off.ensure(8 * n2) || !b_words.ensure(64) || !b_job.ensure(4 * (n + 1)) || !b_flip.ensure(n + 1))
         return false;
     job = b_job.as<uint32_t>();
+    flipb = b_flip.as<uint8_t>();
     lm = b_lm.as<LmtigOut>(); label = (const char**)b_label.p; tab = b_tab.p; tab_n = t;
     partner = b_partner.as<uint32_t>(); P[0] = b_P0.as<uint32_t>(); P[1] = b_P1.as<uint32_t>();
     R[0] = b_R0.as<uint32_t>(); R[1] = b_R1.as<uint32_t>(); A[0] = b_A0.as<unsigned long long>();
@@ -338,12 +355,15 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
     k_ut_rank_init<<<grid, 256, 0, s>>>(ub.lm, n, ub.partner, in.k, ub.P[0], ub.R[0], ub.A[0]);
     int cur = 0;
     unsigned long long last = ~0ull;
-    for (int round = 0; round < 64; ++round) {
+    for (int round = 0; round < 64; round += 2) {   // two rounds per look at the active count
+        k_ut_rank_round<<<grid, 256, 0, s>>>(2 * n, ub.P[cur], ub.R[cur], ub.A[cur], ub.P[cur ^ 1], ub.R[cur ^ 1],
+                                             ub.A[cur ^ 1], nullptr);
+        cur ^= 1;
         if (cudaMemsetAsync(cursor + 3, 0, 8, s) != cudaSuccess) return CFG_ERR_CUDA;
         k_ut_rank_round<<<grid, 256, 0, s>>>(2 * n, ub.P[cur], ub.R[cur], ub.A[cur], ub.P[cur ^ 1], ub.R[cur ^ 1],
                                              ub.A[cur ^ 1], cursor + 3);
         cur ^= 1;
-        ++res.rounds;
+        res.rounds += 2;
         unsigned long long active = 0;
         if (cudaMemcpyAsync(&active, cursor + 3, 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess)
@@ -351,8 +371,10 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
         if (active == 0 || active == last) break;   // resolved, or only closed chains left
         last = active;
     }
+    k_ut_flip<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, ub.P[cur], ub.R[cur], in.k, ub.flipb);
     k_ut_choose<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, ub.partner, ub.P[cur], ub.R[cur], ub.A[cur], in.k, ub.fin,
-                                     ub.out_off, cursor, cursor + 1, cursor + 2, job, in.job_out_base, in.job_cur);
+                                     ub.out_off, cursor, cursor + 1, cursor + 2, job, in.job_out_base, in.job_cur,
+                                     ub.flipb);
     unsigned long long w[3] = {0, 0, 0};
     if (cudaMemcpyAsync(w, cursor, 24, cudaMemcpyDeviceToHost, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
         return CFG_ERR_CUDA;
