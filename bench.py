@@ -80,6 +80,14 @@ def make_workload(name, n_reads=10_000_000):
     raise ValueError(name)
 
 
+T_START = time.perf_counter()
+
+
+def progress(msg):
+    """One timestamped line on stderr (the JSON line stays alone on stdout)."""
+    print(f"[bench {time.perf_counter() - T_START:8.1f}s] {msg}", file=sys.stderr, flush=True)
+
+
 def make_genomes(n_genomes):
     """The batched workload: genome i has log-uniform length in [0.5, 8] Mbp, GC in
     [0.3, 0.7] and 1% of it as copies of 500-5000 bp at 1% divergence (seed 1000+i)."""
@@ -112,12 +120,24 @@ def bench_batch(args, pg, local, world, peak, with_cpu):
     steps, warm = args.batch_steps, max(3, args.warmup)
 
     b = cfgpu.Batch(k, l, cutoff, 16384, device=local if world > 1 else 0)
+    # the autotuner times its candidate shapes on a sample (every tenth genome), and the
+    # whole batch runs with the shape it keeps
+    if not args.no_tune:
+        sample = packed[::10] if len(packed) >= 50 else packed
+        b.submit(sample)
+        progress(f"batch: tuning on {len(sample)} genomes")
+        tuning = b.tune_unitigs()
+        b.set_tuning(tuning.local_div, tuning.cluster_threads, tuning.table_load_pct, tuning.graph_count)
+    else:
+        tuning = cfgpu.BatchTuning(4, 512, 100, 0, 0.0)
+    progress(f"batch: tuned local_div={tuning.local_div} cluster_threads={tuning.cluster_threads} "
+             f"load={tuning.table_load_pct} graph_count={tuning.graph_count}; submitting {len(packed)} genomes")
     b.submit(packed)
-    tuning = b.tune_unitigs() if not args.no_tune else cfgpu.BatchTuning(4, 512, 100, 0, 0.0)
     for _ in range(warm):
         b.run()
         b.unitigs()
     barrier(pg)
+    progress("batch: warm runs done")
     dev_ms, run_ms, col_ms = [], [], []
     for _ in range(steps):
         b.run()
@@ -125,6 +145,7 @@ def bench_batch(args, pg, local, world, peak, with_cpu):
         c = b.unitigs()
         run_ms.append(r); col_ms.append(c); dev_ms.append(r + c)
     info = b.info()
+    progress(f"batch: timed runs {[round(x) for x in dev_ms]} ms; plain launches next")
     # plain launches on the same resident inputs
     cx = cfgpu.Compactor(k, l, cutoff, 16384, device=local if world > 1 else 0)
     dev_inputs = [b.device_input(j) for j in range(len(packed))]
@@ -163,6 +184,7 @@ def bench_batch(args, pg, local, world, peak, with_cpu):
             d2h += nb; units += nu
         return d2h, units
 
+    progress(f"batch: plain runs {[round(x) for x in plain_ms]} ms; end to end next")
     batch_e2e()
     plain_e2e()
     barrier(pg)
@@ -351,6 +373,7 @@ def bench_serve(args, local, world):
         return lat, max(done), groups
 
     # warm every worker's contexts on the largest job of each kind (all workers take one at once)
+    progress(f"serve: {len(jobs)} jobs generated, plain service {mu:.1f} jobs/s; warming the server")
     for kind in ("ref", "read"):
         big = max((j for j in range(len(jobs)) if jobs[j][0] == kind), key=lambda j: jobs[j][1].n_bases, default=None)
         if big is None:
@@ -363,6 +386,7 @@ def bench_serve(args, local, world):
     run_server(arrivals(mu * 4, 99))
     rates = []
     for f in args.serve_load:
+        progress(f"serve: load {f}")
         arr = arrivals(mu * f, 1000 + int(100 * f))
         sl, smk, groups = run_server(arr)
         pl, pmk = run_plain(arr)
@@ -587,6 +611,7 @@ def main():
         cx.run()
         return cx.unitigs_raw()
 
+    progress(f"{name}: input ready ({packed.p.n_bases} bases); end-to-end steps")
     for _ in range(args.warmup):
         e2e_step()
     barrier(pg)
@@ -643,6 +668,7 @@ def main():
         except ValueError:
             traffic = None
 
+    progress(f"{name}: device steps {[round(x, 1) for x in run_ms]} ms; CPU baseline next")
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
