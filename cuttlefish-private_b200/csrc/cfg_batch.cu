@@ -715,6 +715,8 @@ int cfg_batch_tune_unitigs(cfg_batch* b, cfg_batch_tuning* out) {
     if (!b) return CFG_ERR_BAD_INPUT;
     if (!b->have_input) return bfail(b, CFG_ERR_STATE, "cfg_batch_tune_unitigs before cfg_batch_submit");
     const uint32_t base_load = b->tune.table_load_pct ? b->tune.table_load_pct : 100;
+    // a shape that sends any job back to the plain driver is not a candidate: its device
+    // time would not include that job
     auto time_of = [&](const cfg_batch_tuning& t, float& ms) -> int {
         int rc = cfg_batch_set_tuning(b, &t);
         if (rc) return rc;
@@ -722,15 +724,20 @@ int cfg_batch_tune_unitigs(cfg_batch* b, cfg_batch_tuning* out) {
         for (int rep = 0; rep < 2; ++rep) {
             float u = 0;
             rc = cfg_batch_run(b);
-            if (!rc) rc = cfg_batch_unitigs(b, &u);
+            if (rc) return rc;
+            for (uint32_t j = 0; j < b->n_jobs; ++j)
+                if (b->redo[j]) { ms = 1e30f; return CFG_OK; }
+            rc = cfg_batch_unitigs(b, &u);
             if (rc) return rc;
             ms = b->ms + u;   // the second run: the graph is built and warm
         }
         return CFG_OK;
     };
-    // subgraph count first (default shapes), then the launch shapes at that count
+    // subgraph count first (default shapes), then the launch shapes at that count; the
+    // counts stop at a sixteenth of the params', where subgraphs of the largest jobs
+    // still fit cluster tables
     cfg_batch_tuning best{4, 512, base_load, 0, 1e30f};
-    for (uint32_t G = b->G_params; G >= 1 && G + 1 > b->G_params / 64; G /= 4) {
+    for (uint32_t G = b->G_params; G >= 1 && G + 1 > b->G_params / 16; G /= 4) {
         cfg_batch_tuning t{4, 512, base_load, G == b->G_params ? 0u : G, 0.f};
         float ms = 0;
         int rc = time_of(t, ms);
@@ -748,6 +755,7 @@ int cfg_batch_tune_unitigs(cfg_batch* b, cfg_batch_tuning* out) {
                 if (rc) return rc;
                 if (ms < best.ms) { best = t; best.ms = ms; }
             }
+    if (best.ms >= 1e30f) best = cfg_batch_tuning{4, 512, base_load, 0, 0.f};
     const float ms = best.ms;
     int rc = cfg_batch_set_tuning(b, &best);
     if (rc) return rc;

@@ -276,7 +276,9 @@ int cfg_batch_job_device_input(cfg_batch* b, uint32_t job, const uint64_t** d_wo
  * load factor) on the submitted batch and keeps the fastest. */
 int cfg_batch_tune(cfg_batch* b, cfg_batch_tuning* out);
 /* The same for batches whose product is final unitigs (cfg_batch_unitigs): also
- * tunes the subgraph count per job, timing the run and the collation together.
+ * tunes the subgraph count per job (down to a sixteenth of cfg_params.graph_count),
+ * timing the run and the collation together; shapes that send a job back to the
+ * plain driver are skipped.
  * Afterwards cfg_batch_job_unitigs still gives each job's unitigs exactly; the
  * lm-tigs of cfg_batch_job follow the chosen subgraph count. */
 int cfg_batch_tune_unitigs(cfg_batch* b, cfg_batch_tuning* out);
