@@ -106,7 +106,7 @@ struct UnitigInput {
 };
 // ... the buffers it works in ...
 struct UnitigBuffers {
-    DevBuf b_lm, b_label, b_tab, b_partner, b_P0, b_P1, b_R0, b_R1, b_A0, b_A1, b_fin, b_off, b_words, b_out, b_job, b_flip;
+    DevBuf b_lm, b_label, b_tab, b_partner, b_X0, b_X1, b_fin, b_off, b_words, b_out, b_job, b_flip;
     uint8_t* flipb = nullptr;  // per lm-tig heading its chain's walked list: flip it
     LmtigOut* lm = nullptr;
     uint32_t* job = nullptr;   // batch: each gathered lm-tig's job
@@ -114,9 +114,7 @@ struct UnitigBuffers {
     void* tab = nullptr;
     uint64_t tab_n = 0;
     uint32_t* partner = nullptr;
-    uint32_t* P[2] = {nullptr, nullptr};
-    uint32_t* R[2] = {nullptr, nullptr};
-    unsigned long long* A[2] = {nullptr, nullptr};
+    void* X[2] = {nullptr, nullptr};   // ranking records, double-buffered
     uint32_t* fin = nullptr;
     unsigned long long* out_off = nullptr;
     unsigned long long* words = nullptr;
@@ -128,8 +126,8 @@ struct UnitigBuffers {
         return true;
     }
     void release() {
-        DevBuf* all[] = {&b_lm, &b_label, &b_tab, &b_partner, &b_P0, &b_P1, &b_R0, &b_R1, &b_A0, &b_A1, &b_fin, &b_off,
-                         &b_words, &b_out, &b_job, &b_flip};
+        DevBuf* all[] = {&b_lm, &b_label, &b_tab, &b_partner, &b_X0, &b_X1, &b_fin, &b_off, &b_words, &b_out, &b_job,
+                         &b_flip};
         for (DevBuf* b : all) b->release();
     }
 };

@@ -2,8 +2,9 @@
 // jobs of mixed size and parameters onto one GPU.
 //
 // Requests (one genome or read set each, with its own k / cutoff / table sizing)
-// enter a FIFO queue.  `slots` worker threads, each with its own CUDA streams,
-// take work as soon as they are free and the device-memory budget allows:
+// enter a FIFO queue.  `slots` worker threads take work as soon as they are free
+// and the device-memory budget allows (contexts, each with its own CUDA stream, are
+// pooled and shared by the workers):
 //   - a large job runs alone through a plain context (cfg_ctx);
 //   - small jobs waiting together with equal parameters are taken as one group and
 //     run as one batch (cfg_batch), however many arrived since the last group.
@@ -84,7 +85,6 @@ struct Ticket {
 
 struct Worker {
     std::thread th;
-    std::vector<std::unique_ptr<Ctx>> ctxs;
     std::vector<std::unique_ptr<BatchCtx>> batches;
 };
 
@@ -103,6 +103,9 @@ struct cfg_server {
     uint32_t running = 0;         // groups in flight
     bool stop = false;
     std::vector<std::unique_ptr<Worker>> workers;
+    // plain contexts shared by all workers: a job takes any idle one with its parameters,
+    // so their number follows the jobs in flight, not workers x parameter sets
+    std::vector<std::unique_ptr<Ctx>> ctxs;
     cfg_server_stats st{};
     std::string err;
 };
@@ -138,29 +141,34 @@ std::vector<Ticket*> take_group(cfg_server* s, Worker& w, uint64_t& need, bool& 
     return g;
 }
 
-// Drops this worker's idle contexts (oldest first) until `need` more bytes fit.
-void make_room(cfg_server* s, Worker& w, uint64_t need) {
+// Drops idle plain contexts (oldest first) until `need` more bytes fit.
+void make_room(cfg_server* s, uint64_t need) {
     while (s->held_bytes + need > s->cfg.hbm_budget) {
         Ctx* victim = nullptr;
-        for (auto& c : w.ctxs)
+        for (auto& c : s->ctxs)
             if (!c->busy && (!victim || c->last < victim->last)) victim = c.get();
         if (!victim) return;
         s->held_bytes -= victim->bytes;
         cfg_destroy(victim->c);
-        w.ctxs.erase(std::find_if(w.ctxs.begin(), w.ctxs.end(), [&](auto& x) { return x.get() == victim; }));
+        s->ctxs.erase(std::find_if(s->ctxs.begin(), s->ctxs.end(), [&](auto& x) { return x.get() == victim; }));
     }
 }
 
-void run_plain(cfg_server* s, Worker& w, Ticket* t, uint64_t need) {
+void run_plain(cfg_server* s, Ticket* t, uint64_t need) {
     Ctx* ctx = nullptr;
     {
         std::lock_guard<std::mutex> lock(s->mu);
-        for (auto& c : w.ctxs) if (!c->busy && same_params(c->p, t->p)) { ctx = c.get(); break; }
-        if (!ctx) make_room(s, w, need);
-        if (ctx) { s->held_bytes += need > ctx->bytes ? need - ctx->bytes : 0; ctx->bytes = std::max(ctx->bytes, need); }
-        else {
-            w.ctxs.emplace_back(new Ctx());
-            ctx = w.ctxs.back().get();
+        // an idle context with these parameters, preferring one already grown to the job
+        for (auto& c : s->ctxs) {
+            if (c->busy || !same_params(c->p, t->p)) continue;
+            if (!ctx || (ctx->bytes < need && c->bytes > ctx->bytes) || (c->bytes >= need && c->bytes < ctx->bytes)) ctx = c.get();
+        }
+        if (ctx) {
+            if (need > ctx->bytes) { make_room(s, need - ctx->bytes); s->held_bytes += need - ctx->bytes; ctx->bytes = need; }
+        } else {
+            make_room(s, need);
+            s->ctxs.emplace_back(new Ctx());
+            ctx = s->ctxs.back().get();
             ctx->p = t->p; ctx->bytes = need;
             s->held_bytes += need;
         }
@@ -187,7 +195,7 @@ void run_batch(cfg_server* s, Worker& w, std::vector<Ticket*>& g, uint64_t need)
         std::lock_guard<std::mutex> lock(s->mu);
         for (auto& b : w.batches) if (same_params(b->p, p)) bc = b.get();
         if (!bc) { w.batches.emplace_back(new BatchCtx()); bc = w.batches.back().get(); bc->p = p; }
-        if (need > bc->bytes) { make_room(s, w, need - bc->bytes); s->held_bytes += need - bc->bytes; bc->bytes = need; }
+        if (need > bc->bytes) { make_room(s, need - bc->bytes); s->held_bytes += need - bc->bytes; bc->bytes = need; }
     }
     int rc = CFG_OK;
     if (!bc->b) rc = cfg_batch_create(s->device, &p, &bc->b);
@@ -238,7 +246,7 @@ void worker_loop(cfg_server* s, Worker* w) {
             if (batched) { ++s->st.batches; s->st.batched_jobs += g.size(); }
         }
         if (batched) run_batch(s, *w, g, need);
-        else run_plain(s, *w, g[0], need);
+        else run_plain(s, g[0], need);
         {
             std::lock_guard<std::mutex> lock(s->mu);
             const auto now = Clock::now();
@@ -387,8 +395,9 @@ void cfg_server_destroy(cfg_server* s) {
     s->cv_work.notify_all();
     for (auto& w : s->workers) if (w->th.joinable()) w->th.join();
     cudaSetDevice(s->device);
+    for (auto& c : s->ctxs) if (c->c) cfg_destroy(c->c);
     for (auto& w : s->workers) {
-        for (auto& c : w->ctxs) if (c->c) cfg_destroy(c->c);
+
         for (auto& b : w->batches) if (b->b) cfg_batch_destroy(b->b);
     }
     delete s;

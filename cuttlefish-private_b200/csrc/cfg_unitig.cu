@@ -37,6 +37,11 @@ struct EndSlot {   // hash slot of one vertex: its k-mer and the (at most two) l
     uint32_t ready, pad;
 };
 
+// One (lm-tig, direction) entry of the ranking: predecessor still to jump over (NONE
+// once resolved), the farthest known ancestor (the head once resolved), and the label
+// bases of the entries between them.
+struct RankRec { uint32_t P, R; unsigned long long A; };
+
 __device__ __forceinline__ uint64_t mix64(uint64_t z) {
     z ^= z >> 33; z *= 0xFF51AFD7ED558CCDull;
     z ^= z >> 33; z *= 0xC4CEB9FE1A85EC53ull;
@@ -133,28 +138,30 @@ __global__ void k_ut_pair(const LmtigOut* __restrict__ lm, const EndSlot* __rest
 }
 
 __global__ void k_ut_rank_init(const LmtigOut* __restrict__ lm, uint64_t n, const uint32_t* __restrict__ partner, uint32_t k,
-                               uint32_t* P, uint32_t* R, unsigned long long* A) {
+                               RankRec* X) {
     for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < 2 * n; x += (uint64_t)gridDim.x * blockDim.x) {
         // the predecessor left its lm-tig through the end paired with x's entry end
         const uint32_t q = partner[x];
         const uint32_t pred = q == NONE ? NONE : (q ^ 1u);
-        P[x] = pred;
-        R[x] = pred == NONE ? (uint32_t)x : pred;
-        A[x] = pred == NONE ? 0ull : (unsigned long long)(lm[pred >> 1].label_len - k);
+        RankRec r;
+        r.P = pred;
+        r.R = pred == NONE ? (uint32_t)x : pred;
+        r.A = pred == NONE ? 0ull : (unsigned long long)(lm[pred >> 1].label_len - k);
+        X[x] = r;
     }
 }
 
 // One pointer-jumping round (double-buffered); counts the entries still unresolved.
-__global__ void k_ut_rank_round(uint64_t n2, const uint32_t* __restrict__ P, const uint32_t* __restrict__ R,
-                                const unsigned long long* __restrict__ A, uint32_t* P2, uint32_t* R2, unsigned long long* A2,
-                                unsigned long long* active) {
+__global__ void k_ut_rank_round(uint64_t n2, const RankRec* __restrict__ X, RankRec* X2, unsigned long long* active) {
     uint32_t act = 0;
     for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n2; x += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t p = P[x];
-        if (p == NONE) { P2[x] = NONE; R2[x] = R[x]; A2[x] = A[x]; continue; }
-        const uint32_t pp = P[p];
-        P2[x] = pp; R2[x] = R[p]; A2[x] = A[x] + A[p];
-        act += pp != NONE;
+        RankRec r = X[x];
+        if (r.P != NONE) {   // one 16-byte gather of the predecessor's record
+            const RankRec q = X[r.P];
+            r.P = q.P; r.R = q.R; r.A += q.A;
+            act += q.P != NONE;
+        }
+        X2[x] = r;
     }
     if (!active) return;
     for (int d = 16; d; d >>= 1) act += __shfl_down_sync(0xffffffffu, act, d);
@@ -170,15 +177,15 @@ __device__ __forceinline__ char oriented(const char* lab, uint32_t len, uint32_t
 // 3: per chain, once (by the lm-tig heading the list the host collator walks): flip the
 // list when its reverse complement starts with a smaller k-mer (ties keep the walk).
 __global__ void k_ut_flip(const LmtigOut* __restrict__ lm, const char* const* __restrict__ label, uint64_t n,
-                          const uint32_t* __restrict__ P, const uint32_t* __restrict__ R, uint32_t k, uint8_t* flipb) {
+                          const RankRec* __restrict__ X, uint32_t k, uint8_t* flipb) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t e0 = (uint32_t)(2 * i), e1 = e0 + 1;
-        if (P[e0] != NONE || P[e1] != NONE) continue;   // on a closed chain
-        const uint32_t h0 = R[e0], h1 = R[e1];
-        const uint32_t e = h0 < h1 ? e0 : e1;
-        const uint32_t h = R[e];
+        const RankRec x0 = X[e0], x1 = X[e1];
+        if (x0.P != NONE || x1.P != NONE) continue;     // on a closed chain
+        const uint32_t e = x0.R < x1.R ? e0 : e1;
+        const uint32_t h = e == e0 ? x0.R : x1.R;
         if (h != e) continue;                           // not the head of its list
-        const uint32_t t = R[e ^ 1] ^ 1u;               // the entry of the list's tail
+        const uint32_t t = (e == e0 ? x1.R : x0.R) ^ 1u;   // the entry of the list's tail
         const char* lh = label[h >> 1];
         const char* lt = label[t >> 1];
         const uint32_t nh = lm[h >> 1].label_len, nt = lm[t >> 1].label_len;
@@ -195,8 +202,7 @@ __global__ void k_ut_flip(const LmtigOut* __restrict__ lm, const char* const* __
 // 4a: per lm-tig, the final entry; per final tail, the unitig's FASTA record.
 // final[i] = chosen entry of lm-tig i, or NONE when i lies on a cycle.
 __global__ void k_ut_choose(const LmtigOut* __restrict__ lm, const char* const* __restrict__ label, uint64_t n,
-                            const uint32_t* __restrict__ partner, const uint32_t* __restrict__ P,
-                            const uint32_t* __restrict__ R, const unsigned long long* __restrict__ A, uint32_t k,
+                            const uint32_t* __restrict__ partner, const RankRec* __restrict__ X, uint32_t k,
                             uint32_t* fin, unsigned long long* out_off, unsigned long long* cursor, unsigned long long* n_units,
                             unsigned long long* n_cyc, const uint32_t* __restrict__ job,
                             const unsigned long long* __restrict__ job_out_base, unsigned long long* job_cur,
@@ -210,20 +216,21 @@ __global__ void k_ut_choose(const LmtigOut* __restrict__ lm, const char* const* 
         uint32_t head = NONE, f = NONE;
         if (i < n) {
             const uint32_t e0 = (uint32_t)(2 * i), e1 = e0 + 1;
-            if (P[e0] != NONE || P[e1] != NONE) {   // on a closed chain
+            const RankRec x0 = X[e0], x1 = X[e1];
+            if (x0.P != NONE || x1.P != NONE) {   // on a closed chain
                 fin[i] = NONE;
                 atomicAdd(n_cyc, 1ull);
             } else {
-                const uint32_t h0 = R[e0], h1 = R[e1];
-                const uint32_t e = h0 < h1 ? e0 : e1;     // the list the host collator walks
-                const bool flip = flipb[R[e] >> 1];       // decided by that list's head
+                const uint32_t e = x0.R < x1.R ? e0 : e1;   // the list the host collator walks
+                const bool flip = flipb[(e == e0 ? x0.R : x1.R) >> 1];   // decided by that list's head
                 f = flip ? (e ^ 1u) : e;
                 fin[i] = f;
                 // the final list's tail: its exit end has no partner (or is phi)
                 if (partner[f ^ 1u] == NONE) {
                     tail = true;
-                    head = R[f];
-                    L = A[f] + lm[f >> 1].label_len;   // bases before the tail + its whole label
+                    const RankRec xf = f == e0 ? x0 : x1;
+                    head = xf.R;
+                    L = xf.A + lm[f >> 1].label_len;   // bases before the tail + its whole label
                 }
             }
         }
@@ -268,8 +275,7 @@ __global__ void k_ut_choose(const LmtigOut* __restrict__ lm, const char* const* 
 // 4b: every lm-tig's label at its place; heads write the header, tails the newline.
 __global__ void k_ut_write(const LmtigOut* __restrict__ lm, const char* const* __restrict__ label, uint64_t n,
                            const uint32_t* __restrict__ fin, const uint32_t* __restrict__ partner,
-                           const uint32_t* __restrict__ R, const unsigned long long* __restrict__ A,
-                           const unsigned long long* __restrict__ out_off, char* out) {
+                           const RankRec* __restrict__ X, const unsigned long long* __restrict__ out_off, char* out) {
     // one warp per lm-tig: lanes copy the label's bytes
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -278,11 +284,12 @@ __global__ void k_ut_write(const LmtigOut* __restrict__ lm, const char* const* _
         if (f == NONE) continue;
         const uint32_t len = lm[i].label_len;
         const char* lab = label[i];
-        char* rec = out + out_off[R[f]];
-        char* dst = rec + 3 + A[f];
+        const RankRec xf = X[f];
+        char* rec = out + out_off[xf.R];
+        char* dst = rec + 3 + xf.A;
         for (uint32_t j = lane; j < len; j += 32) dst[j] = oriented(lab, len, f, j);
         if (lane == 0) {
-            if (R[f] == f) { rec[0] = '>'; rec[1] = '0'; rec[2] = '\n'; }
+            if (xf.R == f) { rec[0] = '>'; rec[1] = '0'; rec[2] = '\n'; }
             if (partner[f ^ 1u] == NONE) dst[len] = '\n';
         }
     }
@@ -312,16 +319,15 @@ bool UnitigBuffers::ensure(uint64_t n) {
     while (t < 4 * n) t <<= 1;   // vertex table at most half full (2n ends)
     const uint64_t n2 = 2 * n + 2;
     if (!b_lm.ensure(sizeof(LmtigOut) * (n + 1)) || !b_label.ensure(8 * (n + 1)) || !b_tab.ensure(sizeof(EndSlot) * t) ||
-        !b_partner.ensure(4 * n2) || !b_P0.ensure(4 * n2) || !b_P1.ensure(4 * n2) || !b_R0.ensure(4 * n2) ||
-        !b_R1.ensure(4 * n2) || !b_A0.ensure(8 * n2) || !b_A1.ensure(8 * n2) || !b_fin.ensure(4 * (n + 1)) ||
+        !b_partner.ensure(4 * n2) || !b_X0.ensure(sizeof(RankRec) * n2) || !b_X1.ensure(sizeof(RankRec) * n2) ||
+        !b_fin.ensure(4 * (n + 1)) ||
         !b_off.ensure(8 * n2) || !b_words.ensure(64) || !b_job.ensure(4 * (n + 1)) || !b_flip.ensure(n + 1))
         return false;
     job = b_job.as<uint32_t>();
     flipb = b_flip.as<uint8_t>();
     lm = b_lm.as<LmtigOut>(); label = (const char**)b_label.p; tab = b_tab.p; tab_n = t;
-    partner = b_partner.as<uint32_t>(); P[0] = b_P0.as<uint32_t>(); P[1] = b_P1.as<uint32_t>();
-    R[0] = b_R0.as<uint32_t>(); R[1] = b_R1.as<uint32_t>(); A[0] = b_A0.as<unsigned long long>();
-    A[1] = b_A1.as<unsigned long long>(); fin = b_fin.as<uint32_t>(); out_off = b_off.as<unsigned long long>();
+    partner = b_partner.as<uint32_t>(); X[0] = b_X0.p; X[1] = b_X1.p;
+    fin = b_fin.as<uint32_t>(); out_off = b_off.as<unsigned long long>();
     words = b_words.as<unsigned long long>();
     return true;
 }
@@ -352,16 +358,15 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
     if (cudaMemsetAsync(ub.partner, 0xff, 4 * 2 * n, s) != cudaSuccess) return CFG_ERR_CUDA;
     k_ut_insert<<<grid, 256, 0, s>>>(ub.lm, job, n, tab, ub.tab_n - 1, in.err);
     k_ut_pair<<<grid, 256, 0, s>>>(ub.lm, tab, ub.tab_n, ub.partner, in.err);
-    k_ut_rank_init<<<grid, 256, 0, s>>>(ub.lm, n, ub.partner, in.k, ub.P[0], ub.R[0], ub.A[0]);
+    RankRec* Xb[2] = {(RankRec*)ub.X[0], (RankRec*)ub.X[1]};
+    k_ut_rank_init<<<grid, 256, 0, s>>>(ub.lm, n, ub.partner, in.k, Xb[0]);
     int cur = 0;
     unsigned long long last = ~0ull;
     for (int round = 0; round < 64; round += 2) {   // two rounds per look at the active count
-        k_ut_rank_round<<<grid, 256, 0, s>>>(2 * n, ub.P[cur], ub.R[cur], ub.A[cur], ub.P[cur ^ 1], ub.R[cur ^ 1],
-                                             ub.A[cur ^ 1], nullptr);
+        k_ut_rank_round<<<grid, 256, 0, s>>>(2 * n, Xb[cur], Xb[cur ^ 1], nullptr);
         cur ^= 1;
         if (cudaMemsetAsync(cursor + 3, 0, 8, s) != cudaSuccess) return CFG_ERR_CUDA;
-        k_ut_rank_round<<<grid, 256, 0, s>>>(2 * n, ub.P[cur], ub.R[cur], ub.A[cur], ub.P[cur ^ 1], ub.R[cur ^ 1],
-                                             ub.A[cur ^ 1], cursor + 3);
+        k_ut_rank_round<<<grid, 256, 0, s>>>(2 * n, Xb[cur], Xb[cur ^ 1], cursor + 3);
         cur ^= 1;
         res.rounds += 2;
         unsigned long long active = 0;
@@ -371,8 +376,8 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
         if (active == 0 || active == last) break;   // resolved, or only closed chains left
         last = active;
     }
-    k_ut_flip<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, ub.P[cur], ub.R[cur], in.k, ub.flipb);
-    k_ut_choose<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, ub.partner, ub.P[cur], ub.R[cur], ub.A[cur], in.k, ub.fin,
+    k_ut_flip<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, Xb[cur], in.k, ub.flipb);
+    k_ut_choose<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, ub.partner, Xb[cur], in.k, ub.fin,
                                      ub.out_off, cursor, cursor + 1, cursor + 2, job, in.job_out_base, in.job_cur,
                                      ub.flipb);
     unsigned long long w[3] = {0, 0, 0};
@@ -380,7 +385,7 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
         return CFG_ERR_CUDA;
     // a batch's output regions are sized by the caller before the call
     if (!in.jobs && !ub.ensure_out(w[0] + 16)) return CFG_ERR_OOM;
-    k_ut_write<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, ub.fin, ub.partner, ub.R[cur], ub.A[cur], ub.out_off, ub.out);
+    k_ut_write<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, ub.fin, ub.partner, Xb[cur], ub.out_off, ub.out);
     if (cudaGetLastError() != cudaSuccess) return CFG_ERR_CUDA;
     res.bytes = w[0]; res.n_units = w[1]; res.n_cycle_lmtigs = w[2];
     return CFG_OK;
