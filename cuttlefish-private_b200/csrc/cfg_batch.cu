@@ -818,7 +818,7 @@ int cfg_batch_unitigs(cfg_batch* b, float* device_ms) {
     // jobs are joined in chunks that fit the free device memory (jobs never join each other)
     size_t fr = 0, tot = 0;
     BCK(cudaMemGetInfo(&fr, &tot));
-    const unsigned long long per_lmtig = 300;   // bytes of collation buffers per lm-tig
+    const unsigned long long per_lmtig = 240;   // bytes of collation buffers per lm-tig
     const unsigned long long cap = std::max<unsigned long long>(1ull << 20, (unsigned long long)(fr / 10 * 6) / per_lmtig);
     BCK(cudaMemcpyAsync(b->u_n.p, jn.data(), 8ull * J, cudaMemcpyHostToDevice, b->stream));
     BCK(cudaMemcpyAsync(b->u_out.p, ob.data(), 8ull * J, cudaMemcpyHostToDevice, b->stream));
@@ -843,6 +843,7 @@ int cfg_batch_unitigs(cfg_batch* b, float* device_ms) {
         in.job_out_base = b->u_out.as<unsigned long long>() + j0;
         in.job_cur = b->u_cur.as<unsigned long long>() + (size_t)j0 * JOB_CUR_STRIDE;
         in.job_lm = b->lm.as<LmtigOut>(); in.job_text = b->lm_text.as<char>();
+        in.max_job_n = *std::max_element(jn.begin() + j0, jn.begin() + j1);
         UnitigResult res{};
         int rc = collate_device(in, b->ub, b->stream, res);
         if (rc) return bfail(b, rc, "batch collation");

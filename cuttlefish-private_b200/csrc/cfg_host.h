@@ -103,10 +103,11 @@ struct UnitigInput {
     unsigned long long* job_cur;
     const LmtigOut* job_lm;                       // the batch's lm-tig arena
     const char* job_text;                         // and label arena
+    uint64_t max_job_n;                           // the most records of one job
 };
 // ... the buffers it works in ...
 struct UnitigBuffers {
-    DevBuf b_lm, b_label, b_tab, b_partner, b_X0, b_X1, b_fin, b_off, b_words, b_out, b_job, b_flip;
+    DevBuf b_lm, b_label, b_tab, b_partner, b_X0, b_X1, b_fin, b_off, b_words, b_out, b_job, b_flip, b_sx;
     uint8_t* flipb = nullptr;  // per lm-tig heading its chain's walked list: flip it
     LmtigOut* lm = nullptr;
     uint32_t* job = nullptr;   // batch: each gathered lm-tig's job
@@ -116,6 +117,7 @@ struct UnitigBuffers {
     uint32_t* partner = nullptr;
     void* X[2] = {nullptr, nullptr};   // ranking records, double-buffered
     uint32_t* fin = nullptr;
+    uint32_t* sx = nullptr;    // ranking: entry of each splitter
     unsigned long long* out_off = nullptr;
     unsigned long long* words = nullptr;
     char* out = nullptr;
@@ -127,7 +129,7 @@ struct UnitigBuffers {
     }
     void release() {
         DevBuf* all[] = {&b_lm, &b_label, &b_tab, &b_partner, &b_X0, &b_X1, &b_fin, &b_off, &b_words, &b_out, &b_job,
-                         &b_flip};
+                         &b_flip, &b_sx};
         for (DevBuf* b : all) b->release();
     }
 };

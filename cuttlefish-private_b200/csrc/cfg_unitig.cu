@@ -6,10 +6,15 @@
 // set, as data-parallel steps over the lm-tigs of one run:
 //   1. pair the lm-tig ends that meet at a discontinuity vertex (a hash table on the
 //      vertex k-mer; a vertex carries at most one lm-tig on each side);
-//   2. list ranking by pointer jumping over the 2n (lm-tig, direction) entries: each
-//      entry's predecessor is the entry that leaves through its partner end; after
-//      ~log2(chain length) rounds every entry knows its chain's head and the label
-//      bases before it (each lm-tig adds its length minus the k-base overlap);
+//   2. list ranking over the 2n (lm-tig, direction) entries: each entry's predecessor
+//      is the entry that leaves through its partner end, and every entry needs its
+//      list's head and the label bases before it (each lm-tig adds its length minus
+//      the k-base overlap).  Sparse ruling set (Reid-Miller's list ranking; the GPU
+//      form of Rehman, Kothapalli & Narayanan, ICS 2009): heads, tails and a hashed
+//      1/16 sample of the entries are splitters; from every splitter one thread walks
+//      back to the previous splitter, labelling the entries it passes with their
+//      distance to it; pointer jumping then ranks the splitters alone, and one pass
+//      gives every entry its rank from its splitter's;
 //   3. of the two mirror lists of a chain, take the one whose head end has the
 //      smaller id (the host collator's walk), then flip it if its reverse complement
 //      starts with a smaller k-mer (Maximal_Unitig::canonicalize,
@@ -31,28 +36,24 @@ namespace {
 
 constexpr uint32_t NONE = 0xffffffffu;
 
-struct EndSlot {   // hash slot of one vertex: its k-mer and the (at most two) lm-tig ends there
-    unsigned long long k0, k1;
-    uint32_t e0, e1;
-    uint32_t ready, pad;
-};
+// Vertex table slot: the first and the second lm-tig end seen at a vertex (NONE when
+// free).  The vertex k-mer is not stored: it is read from the first end's lm-tig.
+using EndSlot = uint2;
 
 // One (lm-tig, direction) entry of the ranking: predecessor still to jump over (NONE
 // once resolved), the farthest known ancestor (the head once resolved), and the label
 // bases of the entries between them.
 struct RankRec { uint32_t P, R; unsigned long long A; };
 
+// Ranking marks: an entry that no splitter's walk passed lies on a closed chain.
+constexpr uint32_t UNOWNED = 0xfffffffeu;
+constexpr uint32_t SPLIT = 0x80000000u;    // in NodeRec.w: the entry is a splitter
+
 __device__ __forceinline__ uint64_t mix64(uint64_t z) {
     z ^= z >> 33; z *= 0xFF51AFD7ED558CCDull;
     z ^= z >> 33; z *= 0xC4CEB9FE1A85EC53ull;
     z ^= z >> 33;
     return z;
-}
-
-__global__ void k_ut_tab_init(EndSlot* tab, uint64_t n) {
-    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x) {
-        tab[p].e0 = NONE; tab[p].e1 = NONE; tab[p].ready = 0;
-    }
 }
 
 __device__ __forceinline__ bool is_phi(const LmtigOut& m, uint32_t end) { return (m.flags >> (end ? 3 : 2)) & 1; }
@@ -91,68 +92,137 @@ __global__ void k_ut_gather_jobs(const LmtigOut* lm, const char* text, const Job
     }
 }
 
-// 1: every non-phi end into the vertex table; the second end at a vertex pairs.
-// In a batch the vertex is (job, k-mer).
-__global__ void k_ut_insert(const LmtigOut* __restrict__ lm, const uint32_t* __restrict__ job, uint64_t n, EndSlot* tab,
-                            uint64_t mask, uint32_t* err) {
+// 1: every non-phi end into the vertex table; the second end at a vertex pairs with
+// the first (a third end, or two ends on one side of the vertex, is an invalid graph).
+// In a batch the vertex is (job, k-mer), and job j's ends have their own region of the
+// table, [4 base_j, 4 (base_j + n_j)) -- its lm-tigs are [base_j, base_j + n_j) -- so
+// while the grid sweeps the ends in job order the slots it touches stay in L2; a table
+// region larger than L2 is filled in `n_pass` passes over the ends, pass p inserting
+// the ends whose home slot lies in the p-th slice of their region.  The slot's first
+// end is claimed by CAS and its k-mer read from the (immutable) lm-tig, so no thread
+// waits on another.
+__global__ void k_ut_insert(const LmtigOut* __restrict__ lm, const uint32_t* __restrict__ job, uint64_t n,
+                            uint32_t* tab, const unsigned long long* __restrict__ job_lm_base,
+                            const unsigned long long* __restrict__ job_n, uint32_t pass, uint32_t n_pass,
+                            uint32_t* partner, uint32_t* err) {
     for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < 2 * n; e += (uint64_t)gridDim.x * blockDim.x) {
         const LmtigOut& m = lm[e >> 1];
         const uint32_t end = (uint32_t)(e & 1);
         if (is_phi(m, end)) continue;
         const unsigned long long k0 = end ? m.v[0] : m.u[0], k1 = end ? m.v[1] : m.u[1];
         const uint32_t jb = job ? job[e >> 1] : 0u;
-        uint64_t p = mix64(k0 ^ mix64(k1 + 0x9E3779B97F4A7C15ull) ^ mix64(jb + 0x632BE59BD9B4E019ull)) & mask;
-        for (uint64_t probe = 0; probe <= mask; ++probe, p = (p + 1) & mask) {
-            EndSlot& s = tab[p];
-            const uint32_t old = atomicCAS(&s.e0, NONE, (uint32_t)e);
-            if (old == NONE) {
-                s.k0 = k0; s.k1 = k1; s.pad = jb;
-                __threadfence();
-                atomicExch(&s.ready, 1u);
+        const uint64_t h = mix64(k0 ^ mix64(k1 + 0x9E3779B97F4A7C15ull) ^ mix64(jb + 0x632BE59BD9B4E019ull));
+        if (n_pass > 1 && __umul64hi(h, n_pass) != pass) continue;
+        const uint64_t base = job ? 4 * job_lm_base[jb] : 0, t = job ? 4 * job_n[jb] : 4 * n;
+        uint64_t p = base + __umul64hi(h, t);
+        for (uint64_t probe = 0; probe < t; ++probe) {
+            const uint32_t old = atomicCAS(tab + 2 * p, NONE, (uint32_t)e);
+            if (old == NONE) break;
+            const LmtigOut& o = lm[old >> 1];
+            const uint32_t oe = old & 1;
+            if ((oe ? o.v[0] : o.u[0]) == k0 && (oe ? o.v[1] : o.u[1]) == k1 && (!job || job[old >> 1] == jb)) {
+                if (atomicCAS(tab + 2 * p + 1, NONE, (uint32_t)e) != NONE || side_of(m, end) == side_of(o, oe)) {
+                    atomicOr(err, DERR_BAD_GRAPH);
+                } else {
+                    partner[e] = old;
+                    partner[old] = (uint32_t)e;
+                }
                 break;
             }
-            uint32_t spin = 0;
-            while (atomicAdd(&s.ready, 0u) == 0) {
-                if (++spin > (1u << 22)) { atomicOr(err, DERR_CAS_LIMIT); return; }
-            }
-            __threadfence();
-            if (*(volatile unsigned long long*)&s.k0 == k0 && *(volatile unsigned long long*)&s.k1 == k1 &&
-                *(volatile uint32_t*)&s.pad == jb) {
-                if (atomicCAS(&s.e1, NONE, (uint32_t)e) != NONE) atomicOr(err, DERR_BAD_GRAPH);   // a third end
-                break;
-            }
+            if (++p == base + t) p = base;
         }
     }
 }
 
-// 2: partners, and the first round of the ranking: each entry's predecessor entry.
-// Entry x = lm-tig x/2 entered through end x&1 (0: u, read forward; 1: v, reverse).
-__global__ void k_ut_pair(const LmtigOut* __restrict__ lm, const EndSlot* __restrict__ tab, uint64_t tab_n,
-                          uint32_t* partner, uint32_t* err) {
-    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < tab_n; p += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t a = tab[p].e0, b = tab[p].e1;
-        if (a == NONE || b == NONE) continue;
-        if (side_of(lm[a >> 1], a & 1) == side_of(lm[b >> 1], b & 1)) { atomicOr(err, DERR_BAD_GRAPH); continue; }
-        partner[a] = b; partner[b] = a;
+// 2a: per entry x: its predecessor, its own bases (label length - k) and whether it is
+// a splitter (a head, a tail, or sampled); splitters get dense ids.
+// Entry x = lm-tig x/2 entered through end x&1 (0: u, read forward; 1: v, reverse); its
+// predecessor left its lm-tig through the end paired with x's entry end, and its
+// successor entered through the end paired with x's exit end.
+__global__ void __launch_bounds__(256) k_rs_init(const LmtigOut* __restrict__ lm, uint64_t n,
+                                                  const uint32_t* __restrict__ partner, uint32_t k, uint32_t sample_mask,
+                                                  uint2* node, RankRec* X, uint32_t* sx, unsigned long long* n_split) {
+    __shared__ uint32_t wsum[8];
+    __shared__ unsigned long long bbase;
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint64_t n2 = 2 * n, stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n2; base += stride) {   // block-uniform trips
+        const uint64_t x = base + threadIdx.x;
+        bool split = false;
+        if (x < n2) {
+            const uint32_t q = partner[x];
+            const uint32_t pred = q == NONE ? NONE : (q ^ 1u);
+            const bool tail = partner[x ^ 1] == NONE;
+            split = pred == NONE || tail || (mix64(x + 0x2545F4914F6CDD1Dull) & sample_mask) == 0;
+            node[x] = make_uint2(pred, (lm[x >> 1].label_len - k) | (split ? SPLIT : 0u));
+        }
+        // one atomic per block for the splitters' ids
+        const uint32_t bal = __ballot_sync(0xffffffffu, split);
+        if (lane == 0) wsum[wid] = __popc(bal);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t tot = 0;
+            for (uint32_t w = 0; w < 8; ++w) { const uint32_t c = wsum[w]; wsum[w] = tot; tot += c; }
+            bbase = tot ? atomicAdd(n_split, (unsigned long long)tot) : 0ull;
+        }
+        __syncthreads();
+        if (x < n2) {
+            RankRec r{UNOWNED, 0u, 0ull};
+            if (split) {
+                const uint32_t sid = (uint32_t)(bbase + wsum[wid] + __popc(bal & ((1u << lane) - 1)));
+                sx[sid] = (uint32_t)x;
+                r.R = sid;
+            }
+            X[x] = r;
+        }
+        __syncthreads();
     }
 }
 
-__global__ void k_ut_rank_init(const LmtigOut* __restrict__ lm, uint64_t n, const uint32_t* __restrict__ partner, uint32_t k,
-                               RankRec* X) {
-    for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < 2 * n; x += (uint64_t)gridDim.x * blockDim.x) {
-        // the predecessor left its lm-tig through the end paired with x's entry end
-        const uint32_t q = partner[x];
-        const uint32_t pred = q == NONE ? NONE : (q ^ 1u);
-        RankRec r;
-        r.P = pred;
-        r.R = pred == NONE ? (uint32_t)x : pred;
-        r.A = pred == NONE ? 0ull : (unsigned long long)(lm[pred >> 1].label_len - k);
-        X[x] = r;
+// 2b: from every splitter, walk back through the entries before it to the previous
+// splitter: each entry passed records the splitter and the bases from its own start
+// to the splitter's; the splitter links to the previous one (or is a head).  Each lane
+// takes its next splitter as soon as its walk ends, so the warp keeps all lanes busy.
+__global__ void k_rs_walk(const uint32_t* __restrict__ sx, const unsigned long long* __restrict__ n_split,
+                          const uint2* __restrict__ node, RankRec* X, RankRec* S, uint64_t limit, uint32_t* err) {
+    const uint64_t ns = *n_split, stride = (uint64_t)gridDim.x * blockDim.x;
+    uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t cur = NONE, y = NONE;
+    unsigned long long B = 0;
+    for (uint64_t it = 0; it < limit; ++it) {
+        if (cur == NONE) {   // the next splitter
+            if (s >= ns) return;
+            cur = (uint32_t)s;
+            s += stride;
+            const uint32_t x = sx[cur];
+            y = node[x].x;
+            B = 0;
+            if (y == NONE) { S[cur] = RankRec{NONE, x, 0ull}; cur = NONE; }
+            continue;
+        }
+        const uint2 ny = node[y];
+        if (ny.y & SPLIT) {
+            S[cur] = RankRec{X[y].R, 0u, B + (ny.y & ~SPLIT)};
+            cur = NONE;
+            continue;
+        }
+        B += ny.y;
+        X[y] = RankRec{cur, 0u, B};
+        y = ny.x;
+        if (y == NONE) {   // heads are splitters: unreachable on a valid graph
+            atomicOr(err, DERR_BAD_GRAPH);
+            S[cur] = RankRec{NONE, sx[cur], 0ull};
+            cur = NONE;
+        }
     }
+    atomicOr(err, DERR_BAD_GRAPH);   // walk bound exceeded
 }
 
-// One pointer-jumping round (double-buffered); counts the entries still unresolved.
-__global__ void k_ut_rank_round(uint64_t n2, const RankRec* __restrict__ X, RankRec* X2, unsigned long long* active) {
+// One pointer-jumping round over the splitters (double-buffered); counts the entries
+// still unresolved.
+__global__ void k_ut_rank_round(const unsigned long long* __restrict__ n_split, const RankRec* __restrict__ X,
+                                RankRec* X2, unsigned long long* active) {
+    const uint64_t n2 = *n_split;
     uint32_t act = 0;
     for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n2; x += (uint64_t)gridDim.x * blockDim.x) {
         RankRec r = X[x];
@@ -166,6 +236,20 @@ __global__ void k_ut_rank_round(uint64_t n2, const RankRec* __restrict__ X, Rank
     if (!active) return;
     for (int d = 16; d; d >>= 1) act += __shfl_down_sync(0xffffffffu, act, d);
     if ((threadIdx.x & 31) == 0 && act) atomicAdd(active, (unsigned long long)act);
+}
+
+// 2c: every entry's rank from its splitter's: head entry and bases before it.  Entries
+// on closed chains keep a predecessor (P != NONE).
+__global__ void k_rs_final(uint64_t n2, const uint2* __restrict__ node, RankRec* X, const RankRec* __restrict__ S) {
+    for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n2; x += (uint64_t)gridDim.x * blockDim.x) {
+        const RankRec r = X[x];
+        if (node[x].y & SPLIT) {
+            X[x] = S[r.R];
+        } else if (r.P != UNOWNED) {
+            const RankRec q = S[r.P];
+            X[x] = RankRec{q.P, q.R, q.A - r.A};
+        }
+    }
 }
 
 __device__ __forceinline__ char comp_char(char c) { return c == 'A' ? 'T' : c == 'C' ? 'G' : c == 'G' ? 'C' : 'A'; }
@@ -273,24 +357,65 @@ __global__ void k_ut_choose(const LmtigOut* __restrict__ lm, const char* const* 
 }
 
 // 4b: every lm-tig's label at its place; heads write the header, tails the newline.
+// Each thread resolves one lm-tig's source and destination (a chain of dependent loads,
+// so 32 of them overlap per warp), then the warp copies the warp's labels one by one.
 __global__ void k_ut_write(const LmtigOut* __restrict__ lm, const char* const* __restrict__ label, uint64_t n,
                            const uint32_t* __restrict__ fin, const uint32_t* __restrict__ partner,
                            const RankRec* __restrict__ X, const unsigned long long* __restrict__ out_off, char* out) {
-    // one warp per lm-tig: lanes copy the label's bytes
     const uint32_t lane = threadIdx.x & 31;
-    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
-        const uint32_t f = fin[i];
-        if (f == NONE) continue;
-        const uint32_t len = lm[i].label_len;
-        const char* lab = label[i];
-        const RankRec xf = X[f];
-        char* rec = out + out_off[xf.R];
-        char* dst = rec + 3 + xf.A;
-        for (uint32_t j = lane; j < len; j += 32) dst[j] = oriented(lab, len, f, j);
-        if (lane == 0) {
-            if (xf.R == f) { rec[0] = '>'; rec[1] = '0'; rec[2] = '\n'; }
-            if (partner[f ^ 1u] == NONE) dst[len] = '\n';
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {   // warp-uniform trips
+        const uint64_t i = base + threadIdx.x;
+        uint32_t f = NONE, len = 0;
+        const char* lab = nullptr;
+        char* dst = nullptr;
+        if (i < n) {
+            f = fin[i];
+            if (f != NONE) {
+                len = lm[i].label_len;
+                lab = label[i];
+                const RankRec xf = X[f];
+                char* rec = out + out_off[xf.R];
+                dst = rec + 3 + xf.A;
+                if (xf.R == f) { rec[0] = '>'; rec[1] = '0'; rec[2] = '\n'; }
+                if (partner[f ^ 1u] == NONE) dst[len] = '\n';
+            }
+        }
+        // eight labels at a time: every lane loads its bytes of all eight before storing
+        // any, so their load latencies overlap (labels longer than 64 bases finish after)
+        uint32_t todo = __ballot_sync(0xffffffffu, f != NONE);
+        while (todo) {
+            const char* sl[8];
+            char* dl[8];
+            uint32_t ll[8], fl[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int l = todo ? __ffs(todo) - 1 : 0;
+                const bool has = todo != 0;
+                todo &= todo - 1;
+                sl[u] = (const char*)__shfl_sync(0xffffffffu, (unsigned long long)lab, l);
+                dl[u] = (char*)__shfl_sync(0xffffffffu, (unsigned long long)dst, l);
+                ll[u] = has ? __shfl_sync(0xffffffffu, len, l) : 0u;
+                fl[u] = __shfl_sync(0xffffffffu, f, l);
+            }
+            char c[8][2];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+#pragma unroll
+                for (int hf = 0; hf < 2; ++hf) {
+                    const uint32_t j = lane + 32 * hf;
+                    c[u][hf] = j < ll[u] ? oriented(sl[u], ll[u], fl[u], j) : 0;
+                }
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+#pragma unroll
+                for (int hf = 0; hf < 2; ++hf) {
+                    const uint32_t j = lane + 32 * hf;
+                    if (j < ll[u]) dl[u][j] = c[u][hf];
+                }
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                for (uint32_t j = 64 + lane; j < ll[u]; j += 32) dl[u][j] = oriented(sl[u], ll[u], fl[u], j);
         }
     }
 }
@@ -315,12 +440,13 @@ __global__ void k_ut_cycles(const LmtigOut* __restrict__ lm, const char* const* 
 }  // namespace
 
 bool UnitigBuffers::ensure(uint64_t n) {
-    uint64_t t = 64;
-    while (t < 4 * n) t <<= 1;   // vertex table at most half full (2n ends)
+    // vertex table: 4 slots per lm-tig (at most half full: 2 ends per lm-tig); after
+    // pairing it holds the splitters' second ranking buffer (up to 2n records)
+    const uint64_t t = 4 * n + 64;
     const uint64_t n2 = 2 * n + 2;
     if (!b_lm.ensure(sizeof(LmtigOut) * (n + 1)) || !b_label.ensure(8 * (n + 1)) || !b_tab.ensure(sizeof(EndSlot) * t) ||
         !b_partner.ensure(4 * n2) || !b_X0.ensure(sizeof(RankRec) * n2) || !b_X1.ensure(sizeof(RankRec) * n2) ||
-        !b_fin.ensure(4 * (n + 1)) ||
+        !b_fin.ensure(4 * (n + 1)) || !b_sx.ensure(4 * n2) ||
         !b_off.ensure(8 * n2) || !b_words.ensure(64) || !b_job.ensure(4 * (n + 1)) || !b_flip.ensure(n + 1))
         return false;
     job = b_job.as<uint32_t>();
@@ -328,6 +454,7 @@ bool UnitigBuffers::ensure(uint64_t n) {
     lm = b_lm.as<LmtigOut>(); label = (const char**)b_label.p; tab = b_tab.p; tab_n = t;
     partner = b_partner.as<uint32_t>(); X[0] = b_X0.p; X[1] = b_X1.p;
     fin = b_fin.as<uint32_t>(); out_off = b_off.as<unsigned long long>();
+    sx = b_sx.as<uint32_t>();
     words = b_words.as<unsigned long long>();
     return true;
 }
@@ -342,11 +469,12 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
     res = UnitigResult{};
     const uint64_t n = in.n;
     if (!ub.ensure(n)) return CFG_ERR_OOM;
-    if (cudaMemsetAsync(ub.words, 0, sizeof(unsigned long long) * 4, s) != cudaSuccess) return CFG_ERR_CUDA;
-    unsigned long long* cursor = ub.words;      // [0] output bytes, [1] unitigs, [2] cycle lm-tigs, [3] active
+    if (cudaMemsetAsync(ub.words, 0, sizeof(unsigned long long) * 8, s) != cudaSuccess) return CFG_ERR_CUDA;
+    // [0] output bytes, [1] unitigs, [2] cycle lm-tigs, [3] active entries, [4] splitters
+    unsigned long long* cursor = ub.words;
     if (n == 0) return CFG_OK;
+    if (2 * n >= SPLIT) return CFG_ERR_BAD_INPUT;   // entry ids are 31-bit
     const unsigned grid = 148 * 8;
-    EndSlot* tab = (EndSlot*)ub.tab;
     const uint32_t* job = in.jobs ? ub.job : nullptr;
     if (in.jobs)
         k_ut_gather_jobs<<<dim3(16, std::min<uint32_t>(in.n_jobs, 65535)), 256, 0, s>>>(
@@ -354,19 +482,28 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
     else
         k_ut_gather<<<dim3(64, in.stripes), 256, 0, s>>>(in.lm, in.lm_slice, in.text, in.text_slice, in.lm_base, in.text_base,
                                                          in.stripe_cur, in.stripes, ub.lm, ub.label);
-    k_ut_tab_init<<<grid, 256, 0, s>>>(tab, ub.tab_n);
-    if (cudaMemsetAsync(ub.partner, 0xff, 4 * 2 * n, s) != cudaSuccess) return CFG_ERR_CUDA;
-    k_ut_insert<<<grid, 256, 0, s>>>(ub.lm, job, n, tab, ub.tab_n - 1, in.err);
-    k_ut_pair<<<grid, 256, 0, s>>>(ub.lm, tab, ub.tab_n, ub.partner, in.err);
-    RankRec* Xb[2] = {(RankRec*)ub.X[0], (RankRec*)ub.X[1]};
-    k_ut_rank_init<<<grid, 256, 0, s>>>(ub.lm, n, ub.partner, in.k, Xb[0]);
+    if (cudaMemsetAsync(ub.tab, 0xff, sizeof(EndSlot) * ub.tab_n, s) != cudaSuccess ||
+        cudaMemsetAsync(ub.partner, 0xff, 4 * 2 * n, s) != cudaSuccess)
+        return CFG_ERR_CUDA;
+    // table regions over 64 MB are filled in slices that fit L2
+    const uint64_t big = in.jobs && in.max_job_n ? in.max_job_n : n;
+    const uint32_t n_pass = (uint32_t)std::max<uint64_t>(1, (4 * big * sizeof(EndSlot) + (64ull << 20) - 1) >> 26);
+    for (uint32_t pass = 0; pass < n_pass; ++pass)
+        k_ut_insert<<<grid, 256, 0, s>>>(ub.lm, job, n, (uint32_t*)ub.tab, in.job_lm_base, in.job_n, pass, n_pass,
+                                         ub.partner, in.err);
+    // ranking: splitters, their walks, pointer jumping over the splitters, every entry
+    RankRec* X = (RankRec*)ub.X[0];
+    uint2* node = (uint2*)ub.out_off;                          // free until the records are reserved
+    RankRec* Sb[2] = {(RankRec*)ub.X[1], (RankRec*)ub.tab};   // the vertex table is done with
+    k_rs_init<<<grid, 256, 0, s>>>(ub.lm, n, ub.partner, in.k, 15u, node, X, ub.sx, cursor + 4);
+    k_rs_walk<<<grid, 256, 0, s>>>(ub.sx, cursor + 4, node, X, Sb[0], 4 * n + 64, in.err);
     int cur = 0;
     unsigned long long last = ~0ull;
     for (int round = 0; round < 64; round += 2) {   // two rounds per look at the active count
-        k_ut_rank_round<<<grid, 256, 0, s>>>(2 * n, Xb[cur], Xb[cur ^ 1], nullptr);
+        k_ut_rank_round<<<grid, 256, 0, s>>>(cursor + 4, Sb[cur], Sb[cur ^ 1], nullptr);
         cur ^= 1;
         if (cudaMemsetAsync(cursor + 3, 0, 8, s) != cudaSuccess) return CFG_ERR_CUDA;
-        k_ut_rank_round<<<grid, 256, 0, s>>>(2 * n, Xb[cur], Xb[cur ^ 1], cursor + 3);
+        k_ut_rank_round<<<grid, 256, 0, s>>>(cursor + 4, Sb[cur], Sb[cur ^ 1], cursor + 3);
         cur ^= 1;
         res.rounds += 2;
         unsigned long long active = 0;
@@ -376,8 +513,9 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
         if (active == 0 || active == last) break;   // resolved, or only closed chains left
         last = active;
     }
-    k_ut_flip<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, Xb[cur], in.k, ub.flipb);
-    k_ut_choose<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, ub.partner, Xb[cur], in.k, ub.fin,
+    k_rs_final<<<grid, 256, 0, s>>>(2 * n, node, X, Sb[cur]);
+    k_ut_flip<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, X, in.k, ub.flipb);
+    k_ut_choose<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, ub.partner, X, in.k, ub.fin,
                                      ub.out_off, cursor, cursor + 1, cursor + 2, job, in.job_out_base, in.job_cur,
                                      ub.flipb);
     unsigned long long w[3] = {0, 0, 0};
@@ -385,7 +523,7 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
         return CFG_ERR_CUDA;
     // a batch's output regions are sized by the caller before the call
     if (!in.jobs && !ub.ensure_out(w[0] + 16)) return CFG_ERR_OOM;
-    k_ut_write<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, ub.fin, ub.partner, Xb[cur], ub.out_off, ub.out);
+    k_ut_write<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, ub.fin, ub.partner, X, ub.out_off, ub.out);
     if (cudaGetLastError() != cudaSuccess) return CFG_ERR_CUDA;
     res.bytes = w[0]; res.n_units = w[1]; res.n_cycle_lmtigs = w[2];
     return CFG_OK;
