@@ -150,19 +150,21 @@ def bench_batch(args, pg, local, world, peak, with_cpu):
     # plain launches on the same resident inputs
     cx = cfgpu.Compactor(k, l, cutoff, 16384, device=local if world > 1 else 0)
     dev_inputs = [b.device_input(j) for j in range(len(packed))]
-    plain_ms = []
+    plain_ms, plain_col = [], []
     plain_launches = 0
     for it in range(1 + steps):
-        tot = 0.0
+        tot = col = 0.0
         for d in dev_inputs:
             cx.submit_device(*d)
             cx.run()
             _, _, _, ums = cx.unitigs_raw()
             tot += cx.timings()[3] + ums
+            col += ums
             if it == 1:
                 plain_launches += cx.counts().n_launches
         if it > 0:
             plain_ms.append(tot)
+            plain_col.append(col)
     barrier(pg)
 
     # end to end, host buffers
@@ -228,6 +230,7 @@ def bench_batch(args, pg, local, world, peak, with_cpu):
                                "table_load_pct": tuning.table_load_pct,
                                "graph_count": tuning.graph_count or 16384, "tuned_ms": tuning.ms}},
         "plain": {"value": world * bases * steps / (p_dev / 1e3), "unit": "bases/s", "ms_per_step": p_dev / steps,
+                  "collate_ms": sum(plain_col) / steps,
                   "e2e": {"value": world * bases * steps / p_e2e, "ms_per_step": 1e3 * p_e2e / steps,
                           "d2h_bytes_per_step": d2h_p},
                   "gpu_launches_per_step": plain_launches},

@@ -577,12 +577,14 @@ int cfg_unitigs(cfg_ctx* c, const char** fasta, uint64_t* bytes, uint64_t* n_uni
     UnitigResult res{};
     int rc = collate_device(in, c->ub, c->stream, res);
     if (rc == CFG_ERR_OOM) return fail(c, rc, "collation buffers");
+    if (rc == CFG_ERR_STATE) return fail(c, rc, "lm-tig ends do not form a valid discontinuity graph");
+    if (rc == CFG_ERR_WALK_LIMIT) return fail(c, rc, "lm-tig ranking exceeded its bound");
     if (rc) return fail(c, rc, std::string("collation: ") + cudaGetErrorString(cudaGetLastError()));
     MiscWords m{};
     CK(cudaMemcpyAsync(&m, c->misc.p, sizeof(m), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     if (m.err & DERR_BAD_GRAPH) return fail(c, CFG_ERR_STATE, "lm-tig ends do not form a valid discontinuity graph");
-    if (m.err & DERR_CAS_LIMIT) return fail(c, CFG_ERR_WALK_LIMIT, "vertex-table wait exceeded its bound");
+    if (m.err & DERR_WALK_LIMIT) return fail(c, CFG_ERR_WALK_LIMIT, "lm-tig ranking exceeded its bound");
     // lm-tigs on closed chains: joined on the host (they need the rotation rule)
     std::string cyc_fa;
     uint64_t cyc_units = 0;

@@ -846,13 +846,15 @@ int cfg_batch_unitigs(cfg_batch* b, float* device_ms) {
         in.max_job_n = *std::max_element(jn.begin() + j0, jn.begin() + j1);
         UnitigResult res{};
         int rc = collate_device(in, b->ub, b->stream, res);
+        if (rc == CFG_ERR_STATE) return bfail(b, rc, "lm-tig ends do not form a valid discontinuity graph");
+        if (rc == CFG_ERR_WALK_LIMIT) return bfail(b, rc, "lm-tig ranking exceeded its bound");
         if (rc) return bfail(b, rc, "batch collation");
         BCK(cudaEventRecord(b->ev[1], b->stream));
         uint32_t err = 0;
         BCK(cudaMemcpyAsync(&err, b->u_err.p, 4, cudaMemcpyDeviceToHost, b->stream));
         BCK(cudaStreamSynchronize(b->stream));
         if (err & DERR_BAD_GRAPH) return bfail(b, CFG_ERR_STATE, "lm-tig ends do not form a valid discontinuity graph");
-        if (err & DERR_CAS_LIMIT) return bfail(b, CFG_ERR_WALK_LIMIT, "vertex-table wait exceeded its bound");
+        if (err & DERR_WALK_LIMIT) return bfail(b, CFG_ERR_WALK_LIMIT, "lm-tig ranking exceeded its bound");
         float ms = 0;
         cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]);
         total_ms += ms;

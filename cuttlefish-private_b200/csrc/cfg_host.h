@@ -107,7 +107,7 @@ struct UnitigInput {
 };
 // ... the buffers it works in ...
 struct UnitigBuffers {
-    DevBuf b_lm, b_label, b_tab, b_partner, b_X0, b_X1, b_fin, b_off, b_words, b_out, b_job, b_flip, b_sx;
+    DevBuf b_lm, b_label, b_tab, b_partner, b_X0, b_X1, b_fin, b_off, b_words, b_out, b_job, b_flip, b_sx, b_sw;
     uint8_t* flipb = nullptr;  // per lm-tig heading its chain's walked list: flip it
     LmtigOut* lm = nullptr;
     uint32_t* job = nullptr;   // batch: each gathered lm-tig's job
@@ -118,6 +118,7 @@ struct UnitigBuffers {
     void* X[2] = {nullptr, nullptr};   // ranking records, double-buffered
     uint32_t* fin = nullptr;
     uint32_t* sx = nullptr;    // ranking: entry of each splitter
+    uint32_t* sw = nullptr;    // and its bases (label length - k)
     unsigned long long* out_off = nullptr;
     unsigned long long* words = nullptr;
     char* out = nullptr;
@@ -129,7 +130,7 @@ struct UnitigBuffers {
     }
     void release() {
         DevBuf* all[] = {&b_lm, &b_label, &b_tab, &b_partner, &b_X0, &b_X1, &b_fin, &b_off, &b_words, &b_out, &b_job,
-                         &b_flip, &b_sx};
+                         &b_flip, &b_sx, &b_sw};
         for (DevBuf* b : all) b->release();
     }
 };

@@ -47,7 +47,8 @@ struct RankRec { uint32_t P, R; unsigned long long A; };
 
 // Ranking marks: an entry that no splitter's walk passed lies on a closed chain.
 constexpr uint32_t UNOWNED = 0xfffffffeu;
-constexpr uint32_t SPLIT = 0x80000000u;    // in NodeRec.w: the entry is a splitter
+constexpr uint32_t SPLIT = 0x80000000u;    // node[x].y: x is a splitter (low bits: its id)
+constexpr uint32_t OWNED = 0x80000000u;    // node[x].x: a walk passed x (low bits: its splitter)
 
 __device__ __forceinline__ uint64_t mix64(uint64_t z) {
     z ^= z >> 33; z *= 0xFF51AFD7ED558CCDull;
@@ -94,54 +95,71 @@ __global__ void k_ut_gather_jobs(const LmtigOut* lm, const char* text, const Job
 
 // 1: every non-phi end into the vertex table; the second end at a vertex pairs with
 // the first (a third end, or two ends on one side of the vertex, is an invalid graph).
-// In a batch the vertex is (job, k-mer), and job j's ends have their own region of the
-// table, [4 base_j, 4 (base_j + n_j)) -- its lm-tigs are [base_j, base_j + n_j) -- so
-// while the grid sweeps the ends in job order the slots it touches stay in L2; a table
-// region larger than L2 is filled in `n_pass` passes over the ends, pass p inserting
-// the ends whose home slot lies in the p-th slice of their region.  The slot's first
-// end is claimed by CAS and its k-mer read from the (immutable) lm-tig, so no thread
-// waits on another.
-__global__ void k_ut_insert(const LmtigOut* __restrict__ lm, const uint32_t* __restrict__ job, uint64_t n,
-                            uint32_t* tab, const unsigned long long* __restrict__ job_lm_base,
-                            const unsigned long long* __restrict__ job_n, uint32_t pass, uint32_t n_pass,
-                            uint32_t* partner, uint32_t* err) {
-    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < 2 * n; e += (uint64_t)gridDim.x * blockDim.x) {
-        const LmtigOut& m = lm[e >> 1];
-        const uint32_t end = (uint32_t)(e & 1);
-        if (is_phi(m, end)) continue;
-        const unsigned long long k0 = end ? m.v[0] : m.u[0], k1 = end ? m.v[1] : m.u[1];
-        const uint32_t jb = job ? job[e >> 1] : 0u;
-        const uint64_t h = mix64(k0 ^ mix64(k1 + 0x9E3779B97F4A7C15ull) ^ mix64(jb + 0x632BE59BD9B4E019ull));
-        if (n_pass > 1 && __umul64hi(h, n_pass) != pass) continue;
-        const uint64_t base = job ? 4 * job_lm_base[jb] : 0, t = job ? 4 * job_n[jb] : 4 * n;
-        uint64_t p = base + __umul64hi(h, t);
-        for (uint64_t probe = 0; probe < t; ++probe) {
-            const uint32_t old = atomicCAS(tab + 2 * p, NONE, (uint32_t)e);
-            if (old == NONE) break;
-            const LmtigOut& o = lm[old >> 1];
-            const uint32_t oe = old & 1;
-            if ((oe ? o.v[0] : o.u[0]) == k0 && (oe ? o.v[1] : o.u[1]) == k1 && (!job || job[old >> 1] == jb)) {
-                if (atomicCAS(tab + 2 * p + 1, NONE, (uint32_t)e) != NONE || side_of(m, end) == side_of(o, oe)) {
-                    atomicOr(err, DERR_BAD_GRAPH);
-                } else {
-                    partner[e] = old;
-                    partner[old] = (uint32_t)e;
+// In a batch job j's ends have their own region of the table, [4 base_j, 4 (base_j +
+// n_j)) -- its lm-tigs are [base_j, base_j + n_j) -- so a vertex is (job, k-mer) by
+// construction.  Blocks take tiles of ends from a counter, in order, so the ends in
+// flight span a window of about one job and the table slots, lm-tigs and partners
+// they touch stay in L2; a table region larger than L2 is filled in `n_pass` passes,
+// pass p inserting the ends whose home slot lies in the p-th slice of their region.
+// The slot's first end is claimed by CAS and its k-mer read from the (immutable)
+// lm-tig, so no thread waits on another.
+constexpr uint32_t INSERT_TILE = 1024;
+__global__ void __launch_bounds__(256, 6) k_ut_insert(const LmtigOut* __restrict__ lm, const uint32_t* __restrict__ job,
+                                                    uint64_t n, uint32_t* tab,
+                                                    const unsigned long long* __restrict__ job_lm_base,
+                                                    const unsigned long long* __restrict__ job_n, uint32_t pass,
+                                                    uint32_t n_pass, unsigned long long* tiles, uint32_t* partner,
+                                                    uint32_t* err) {
+    __shared__ unsigned long long tile;
+    const uint64_t n2 = 2 * n;
+    for (;;) {
+        if (threadIdx.x == 0) tile = atomicAdd(tiles, 1ull);
+        __syncthreads();
+        const uint64_t t0 = tile * INSERT_TILE;
+        __syncthreads();
+        if (t0 >= n2) return;
+        for (uint32_t u = threadIdx.x; u < INSERT_TILE; u += blockDim.x) {
+            const uint64_t e = t0 + u;
+            if (e >= n2) break;
+            const LmtigOut& m = lm[e >> 1];
+            const uint32_t end = (uint32_t)(e & 1);
+            if (is_phi(m, end)) continue;
+            const unsigned long long k0 = end ? m.v[0] : m.u[0], k1 = end ? m.v[1] : m.u[1];
+            const uint64_t h = mix64(k0 ^ mix64(k1 + 0x9E3779B97F4A7C15ull));
+            if (n_pass > 1 && __umul64hi(h, n_pass) != pass) continue;
+            const uint32_t jb = job ? job[e >> 1] : 0u;
+            const uint64_t base = job ? 4 * job_lm_base[jb] : 0, t = job ? 4 * job_n[jb] : 4 * n;
+            uint64_t p = base + __umul64hi(h, t);
+            for (uint64_t probe = 0; probe < t; ++probe) {
+                const uint32_t old = atomicCAS(tab + 2 * p, NONE, (uint32_t)e);
+                if (old == NONE) break;
+                const LmtigOut& o = lm[old >> 1];
+                const uint32_t oe = old & 1;
+                if ((oe ? o.v[0] : o.u[0]) == k0 && (oe ? o.v[1] : o.u[1]) == k1) {
+                    if (atomicCAS(tab + 2 * p + 1, NONE, (uint32_t)e) != NONE || side_of(m, end) == side_of(o, oe)) {
+                        atomicOr(err, DERR_BAD_GRAPH);
+                    } else {
+                        partner[e] = old;
+                        partner[old] = (uint32_t)e;
+                    }
+                    break;
                 }
-                break;
+                if (++p == base + t) p = base;
             }
-            if (++p == base + t) p = base;
         }
     }
 }
 
-// 2a: per entry x: its predecessor, its own bases (label length - k) and whether it is
-// a splitter (a head, a tail, or sampled); splitters get dense ids.
+// 2a: per entry x: its predecessor, its own bases w (label length - k) and whether it
+// is a splitter (a head, a tail, or sampled); splitters get dense ids.  node[x] holds
+// {pred, w} for an entry and {pred, sid | SPLIT} for a splitter (whose w goes to sw).
 // Entry x = lm-tig x/2 entered through end x&1 (0: u, read forward; 1: v, reverse); its
 // predecessor left its lm-tig through the end paired with x's entry end, and its
 // successor entered through the end paired with x's exit end.
 __global__ void __launch_bounds__(256) k_rs_init(const LmtigOut* __restrict__ lm, uint64_t n,
                                                   const uint32_t* __restrict__ partner, uint32_t k, uint32_t sample_mask,
-                                                  uint2* node, RankRec* X, uint32_t* sx, unsigned long long* n_split) {
+                                                  uint2* node, uint32_t* sx, uint32_t* sw, unsigned long long* n_split,
+                                                  uint32_t* err) {
     __shared__ uint32_t wsum[8];
     __shared__ unsigned long long bbase;
     const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -149,12 +167,14 @@ __global__ void __launch_bounds__(256) k_rs_init(const LmtigOut* __restrict__ lm
     for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n2; base += stride) {   // block-uniform trips
         const uint64_t x = base + threadIdx.x;
         bool split = false;
+        uint32_t pred = NONE, w = 0;
         if (x < n2) {
             const uint32_t q = partner[x];
-            const uint32_t pred = q == NONE ? NONE : (q ^ 1u);
+            pred = q == NONE ? NONE : (q ^ 1u);
             const bool tail = partner[x ^ 1] == NONE;
             split = pred == NONE || tail || (mix64(x + 0x2545F4914F6CDD1Dull) & sample_mask) == 0;
-            node[x] = make_uint2(pred, (lm[x >> 1].label_len - k) | (split ? SPLIT : 0u));
+            w = lm[x >> 1].label_len - k;
+            if (w & SPLIT) atomicOr(err, DERR_WALK_LIMIT);   // an lm-tig of 2^31 bases
         }
         // one atomic per block for the splitters' ids
         const uint32_t bal = __ballot_sync(0xffffffffu, split);
@@ -162,52 +182,76 @@ __global__ void __launch_bounds__(256) k_rs_init(const LmtigOut* __restrict__ lm
         __syncthreads();
         if (threadIdx.x == 0) {
             uint32_t tot = 0;
-            for (uint32_t w = 0; w < 8; ++w) { const uint32_t c = wsum[w]; wsum[w] = tot; tot += c; }
+            for (uint32_t v = 0; v < 8; ++v) { const uint32_t c = wsum[v]; wsum[v] = tot; tot += c; }
             bbase = tot ? atomicAdd(n_split, (unsigned long long)tot) : 0ull;
         }
         __syncthreads();
         if (x < n2) {
-            RankRec r{UNOWNED, 0u, 0ull};
             if (split) {
                 const uint32_t sid = (uint32_t)(bbase + wsum[wid] + __popc(bal & ((1u << lane) - 1)));
                 sx[sid] = (uint32_t)x;
-                r.R = sid;
+                sw[sid] = w;
+                node[x] = make_uint2(pred, sid | SPLIT);
+            } else {
+                node[x] = make_uint2(pred, w);
             }
-            X[x] = r;
         }
         __syncthreads();
     }
 }
 
 // 2b: from every splitter, walk back through the entries before it to the previous
-// splitter: each entry passed records the splitter and the bases from its own start
-// to the splitter's; the splitter links to the previous one (or is a head).  Each lane
-// takes its next splitter as soon as its walk ends, so the warp keeps all lanes busy.
-__global__ void k_rs_walk(const uint32_t* __restrict__ sx, const unsigned long long* __restrict__ n_split,
-                          const uint2* __restrict__ node, RankRec* X, RankRec* S, uint64_t limit, uint32_t* err) {
-    const uint64_t ns = *n_split, stride = (uint64_t)gridDim.x * blockDim.x;
-    uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+// splitter: each entry passed gets {splitter | OWNED, bases from its own start to the
+// splitter's} in place of its node word (read just before, so the write hits L2), and
+// the splitter links to the previous one (or is a head).  Warps take splitters from a
+// counter, 32 at a time and in order, so the walks in flight stay near each other in
+// memory; a lane takes the warp's next splitter as soon as its walk ends.
+__global__ void __launch_bounds__(256) k_rs_walk(const uint32_t* __restrict__ sx, const uint32_t* __restrict__ sw,
+                                                  const unsigned long long* __restrict__ n_split, uint2* node, RankRec* S,
+                                                  unsigned long long* pool_ctr, uint64_t limit, uint32_t* err) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t lt = (1u << lane) - 1;
+    const uint64_t ns = *n_split;
+    unsigned long long pool_next = 0, pool_end = 0;   // warp-uniform: splitters not yet taken
+    bool exhausted = false;
     uint32_t cur = NONE, y = NONE;
     unsigned long long B = 0;
     for (uint64_t it = 0; it < limit; ++it) {
-        if (cur == NONE) {   // the next splitter
-            if (s >= ns) return;
-            cur = (uint32_t)s;
-            s += stride;
-            const uint32_t x = sx[cur];
-            y = node[x].x;
-            B = 0;
-            if (y == NONE) { S[cur] = RankRec{NONE, x, 0ull}; cur = NONE; }
-            continue;
+        uint32_t need = __ballot_sync(0xffffffffu, cur == NONE);
+        while (need && !exhausted) {
+            if (pool_next == pool_end) {
+                unsigned long long b0 = 0;
+                if (lane == 0) b0 = atomicAdd(pool_ctr, 32ull);
+                b0 = __shfl_sync(0xffffffffu, b0, 0);
+                if (b0 >= ns) { exhausted = true; break; }
+                pool_next = b0;
+                pool_end = b0 + 32 < ns ? b0 + 32 : ns;
+            }
+            const uint32_t avail = (uint32_t)(pool_end - pool_next);
+            const uint32_t rank = __popc(need & lt);
+            if (((need >> lane) & 1) && rank < avail) {
+                cur = (uint32_t)(pool_next + rank);
+                const uint32_t x = sx[cur];
+                y = node[x].x;
+                B = 0;
+                if (y == NONE) { S[cur] = RankRec{NONE, x, 0ull}; cur = NONE; }   // a head
+            }
+            const uint32_t took = __popc(need) < avail ? __popc(need) : avail;
+            pool_next += took;
+            need = __ballot_sync(0xffffffffu, cur == NONE);
         }
+        if (__all_sync(0xffffffffu, cur == NONE)) return;   // only when the counter is spent
+        if (cur == NONE) continue;
         const uint2 ny = node[y];
         if (ny.y & SPLIT) {
-            S[cur] = RankRec{X[y].R, 0u, B + (ny.y & ~SPLIT)};
+            const uint32_t sid = ny.y & ~SPLIT;
+            S[cur] = RankRec{sid, 0u, B + sw[sid]};
             cur = NONE;
             continue;
         }
         B += ny.y;
-        X[y] = RankRec{cur, 0u, B};
+        if (B & SPLIT) { atomicOr(err, DERR_WALK_LIMIT); B = 0; }   // 2^31 bases between two splitters
+        node[y] = make_uint2(cur | OWNED, (uint32_t)B);
         y = ny.x;
         if (y == NONE) {   // heads are splitters: unreachable on a valid graph
             atomicOr(err, DERR_BAD_GRAPH);
@@ -215,7 +259,7 @@ __global__ void k_rs_walk(const uint32_t* __restrict__ sx, const unsigned long l
             cur = NONE;
         }
     }
-    atomicOr(err, DERR_BAD_GRAPH);   // walk bound exceeded
+    atomicOr(err, DERR_WALK_LIMIT);   // step bound exceeded
 }
 
 // One pointer-jumping round over the splitters (double-buffered); counts the entries
@@ -239,15 +283,18 @@ __global__ void k_ut_rank_round(const unsigned long long* __restrict__ n_split, 
 }
 
 // 2c: every entry's rank from its splitter's: head entry and bases before it.  Entries
-// on closed chains keep a predecessor (P != NONE).
+// on closed chains keep a predecessor (P != NONE); entries no walk passed are on closed
+// chains without a splitter.
 __global__ void k_rs_final(uint64_t n2, const uint2* __restrict__ node, RankRec* X, const RankRec* __restrict__ S) {
     for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < n2; x += (uint64_t)gridDim.x * blockDim.x) {
-        const RankRec r = X[x];
-        if (node[x].y & SPLIT) {
-            X[x] = S[r.R];
-        } else if (r.P != UNOWNED) {
-            const RankRec q = S[r.P];
-            X[x] = RankRec{q.P, q.R, q.A - r.A};
+        const uint2 nd = node[x];
+        if (nd.y & SPLIT) {
+            X[x] = S[nd.y & ~SPLIT];
+        } else if (nd.x != NONE && (nd.x & OWNED)) {
+            const RankRec q = S[nd.x & ~OWNED];
+            X[x] = RankRec{q.P, q.R, q.A - nd.y};
+        } else {
+            X[x] = RankRec{UNOWNED, 0u, 0ull};
         }
     }
 }
@@ -357,16 +404,19 @@ __global__ void k_ut_choose(const LmtigOut* __restrict__ lm, const char* const* 
 }
 
 // 4b: every lm-tig's label at its place; heads write the header, tails the newline.
-// Each thread resolves one lm-tig's source and destination (a chain of dependent loads,
-// so 32 of them overlap per warp), then the warp copies the warp's labels one by one.
+// An lm-tig writes only the bases its successor does not: all but its last k (the
+// vertex they share, which the successor writes), or all of them at the tail.  Each
+// thread resolves one lm-tig's source and destination and copies short pieces itself
+// (eight loads in flight before the stores); the warp copies long ones together.
 __global__ void k_ut_write(const LmtigOut* __restrict__ lm, const char* const* __restrict__ label, uint64_t n,
                            const uint32_t* __restrict__ fin, const uint32_t* __restrict__ partner,
-                           const RankRec* __restrict__ X, const unsigned long long* __restrict__ out_off, char* out) {
+                           const RankRec* __restrict__ X, const unsigned long long* __restrict__ out_off, uint32_t k,
+                           char* out) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {   // warp-uniform trips
         const uint64_t i = base + threadIdx.x;
-        uint32_t f = NONE, len = 0;
+        uint32_t f = NONE, len = 0, nc = 0;
         const char* lab = nullptr;
         char* dst = nullptr;
         if (i < n) {
@@ -378,44 +428,41 @@ __global__ void k_ut_write(const LmtigOut* __restrict__ lm, const char* const* _
                 char* rec = out + out_off[xf.R];
                 dst = rec + 3 + xf.A;
                 if (xf.R == f) { rec[0] = '>'; rec[1] = '0'; rec[2] = '\n'; }
-                if (partner[f ^ 1u] == NONE) dst[len] = '\n';
+                const bool tail = partner[f ^ 1u] == NONE;
+                nc = tail ? len : len - k;
+                if (tail) dst[len] = '\n';
             }
         }
-        // eight labels at a time: every lane loads its bytes of all eight before storing
-        // any, so their load latencies overlap (labels longer than 64 bases finish after)
-        uint32_t todo = __ballot_sync(0xffffffffu, f != NONE);
-        while (todo) {
-            const char* sl[8];
-            char* dl[8];
-            uint32_t ll[8], fl[8];
+        const bool longer = nc > 64;
+        if (!longer) {
+            for (uint32_t j0 = 0; j0 < nc; j0 += 8) {
+                char c[8];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int l = todo ? __ffs(todo) - 1 : 0;
-                const bool has = todo != 0;
-                todo &= todo - 1;
-                sl[u] = (const char*)__shfl_sync(0xffffffffu, (unsigned long long)lab, l);
-                dl[u] = (char*)__shfl_sync(0xffffffffu, (unsigned long long)dst, l);
-                ll[u] = has ? __shfl_sync(0xffffffffu, len, l) : 0u;
-                fl[u] = __shfl_sync(0xffffffffu, f, l);
+                for (int u = 0; u < 8; ++u) c[u] = j0 + u < nc ? oriented(lab, len, f, j0 + u) : 0;
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (j0 + u < nc) dst[j0 + u] = c[u];
             }
-            char c[8][2];
+        }
+        for (uint32_t todo = __ballot_sync(0xffffffffu, longer); todo; todo &= todo - 1) {
+            const int l = __ffs(todo) - 1;
+            const char* sl = (const char*)__shfl_sync(0xffffffffu, (unsigned long long)lab, l);
+            char* dl = (char*)__shfl_sync(0xffffffffu, (unsigned long long)dst, l);
+            const uint32_t ll = __shfl_sync(0xffffffffu, len, l), cl = __shfl_sync(0xffffffffu, nc, l);
+            const uint32_t fl = __shfl_sync(0xffffffffu, f, l);
+            for (uint32_t j0 = 0; j0 < cl; j0 += 128) {
+                char c[4];
 #pragma unroll
-            for (int u = 0; u < 8; ++u)
-#pragma unroll
-                for (int hf = 0; hf < 2; ++hf) {
-                    const uint32_t j = lane + 32 * hf;
-                    c[u][hf] = j < ll[u] ? oriented(sl[u], ll[u], fl[u], j) : 0;
+                for (int u = 0; u < 4; ++u) {
+                    const uint32_t j = j0 + 32 * u + lane;
+                    c[u] = j < cl ? oriented(sl, ll, fl, j) : 0;
                 }
 #pragma unroll
-            for (int u = 0; u < 8; ++u)
-#pragma unroll
-                for (int hf = 0; hf < 2; ++hf) {
-                    const uint32_t j = lane + 32 * hf;
-                    if (j < ll[u]) dl[u][j] = c[u][hf];
+                for (int u = 0; u < 4; ++u) {
+                    const uint32_t j = j0 + 32 * u + lane;
+                    if (j < cl) dl[j] = c[u];
                 }
-#pragma unroll
-            for (int u = 0; u < 8; ++u)
-                for (uint32_t j = 64 + lane; j < ll[u]; j += 32) dl[u][j] = oriented(sl[u], ll[u], fl[u], j);
+            }
         }
     }
 }
@@ -446,7 +493,7 @@ bool UnitigBuffers::ensure(uint64_t n) {
     const uint64_t n2 = 2 * n + 2;
     if (!b_lm.ensure(sizeof(LmtigOut) * (n + 1)) || !b_label.ensure(8 * (n + 1)) || !b_tab.ensure(sizeof(EndSlot) * t) ||
         !b_partner.ensure(4 * n2) || !b_X0.ensure(sizeof(RankRec) * n2) || !b_X1.ensure(sizeof(RankRec) * n2) ||
-        !b_fin.ensure(4 * (n + 1)) || !b_sx.ensure(4 * n2) ||
+        !b_fin.ensure(4 * (n + 1)) || !b_sx.ensure(4 * n2) || !b_sw.ensure(4 * n2) ||
         !b_off.ensure(8 * n2) || !b_words.ensure(64) || !b_job.ensure(4 * (n + 1)) || !b_flip.ensure(n + 1))
         return false;
     job = b_job.as<uint32_t>();
@@ -455,6 +502,7 @@ bool UnitigBuffers::ensure(uint64_t n) {
     partner = b_partner.as<uint32_t>(); X[0] = b_X0.p; X[1] = b_X1.p;
     fin = b_fin.as<uint32_t>(); out_off = b_off.as<unsigned long long>();
     sx = b_sx.as<uint32_t>();
+    sw = b_sw.as<uint32_t>();
     words = b_words.as<unsigned long long>();
     return true;
 }
@@ -470,7 +518,8 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
     const uint64_t n = in.n;
     if (!ub.ensure(n)) return CFG_ERR_OOM;
     if (cudaMemsetAsync(ub.words, 0, sizeof(unsigned long long) * 8, s) != cudaSuccess) return CFG_ERR_CUDA;
-    // [0] output bytes, [1] unitigs, [2] cycle lm-tigs, [3] active entries, [4] splitters
+    // [0] output bytes, [1] unitigs, [2] cycle lm-tigs, [3] active entries, [4] splitters,
+    // [5] insert tiles taken, [6] splitters taken by walks
     unsigned long long* cursor = ub.words;
     if (n == 0) return CFG_OK;
     if (2 * n >= SPLIT) return CFG_ERR_BAD_INPUT;   // entry ids are 31-bit
@@ -488,15 +537,17 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
     // table regions over 64 MB are filled in slices that fit L2
     const uint64_t big = in.jobs && in.max_job_n ? in.max_job_n : n;
     const uint32_t n_pass = (uint32_t)std::max<uint64_t>(1, (4 * big * sizeof(EndSlot) + (64ull << 20) - 1) >> 26);
-    for (uint32_t pass = 0; pass < n_pass; ++pass)
+    for (uint32_t pass = 0; pass < n_pass; ++pass) {
+        if (cudaMemsetAsync(cursor + 5, 0, 8, s) != cudaSuccess) return CFG_ERR_CUDA;
         k_ut_insert<<<grid, 256, 0, s>>>(ub.lm, job, n, (uint32_t*)ub.tab, in.job_lm_base, in.job_n, pass, n_pass,
-                                         ub.partner, in.err);
+                                         cursor + 5, ub.partner, in.err);
+    }
     // ranking: splitters, their walks, pointer jumping over the splitters, every entry
     RankRec* X = (RankRec*)ub.X[0];
     uint2* node = (uint2*)ub.out_off;                          // free until the records are reserved
     RankRec* Sb[2] = {(RankRec*)ub.X[1], (RankRec*)ub.tab};   // the vertex table is done with
-    k_rs_init<<<grid, 256, 0, s>>>(ub.lm, n, ub.partner, in.k, 15u, node, X, ub.sx, cursor + 4);
-    k_rs_walk<<<grid, 256, 0, s>>>(ub.sx, cursor + 4, node, X, Sb[0], 4 * n + 64, in.err);
+    k_rs_init<<<grid, 256, 0, s>>>(ub.lm, n, ub.partner, in.k, 15u, node, ub.sx, ub.sw, cursor + 4, in.err);
+    k_rs_walk<<<grid, 256, 0, s>>>(ub.sx, ub.sw, cursor + 4, node, Sb[0], cursor + 6, 4 * n + 64, in.err);
     int cur = 0;
     unsigned long long last = ~0ull;
     for (int round = 0; round < 64; round += 2) {   // two rounds per look at the active count
@@ -513,6 +564,12 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
         if (active == 0 || active == last) break;   // resolved, or only closed chains left
         last = active;
     }
+    // an invalid graph stops here, before any record is reserved or written
+    uint32_t e = 0;
+    if (cudaMemcpyAsync(&e, in.err, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
+        return CFG_ERR_CUDA;
+    if (e & DERR_BAD_GRAPH) return CFG_ERR_STATE;
+    if (e & DERR_WALK_LIMIT) return CFG_ERR_WALK_LIMIT;
     k_rs_final<<<grid, 256, 0, s>>>(2 * n, node, X, Sb[cur]);
     k_ut_flip<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, X, in.k, ub.flipb);
     k_ut_choose<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, ub.partner, X, in.k, ub.fin,
@@ -523,7 +580,7 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
         return CFG_ERR_CUDA;
     // a batch's output regions are sized by the caller before the call
     if (!in.jobs && !ub.ensure_out(w[0] + 16)) return CFG_ERR_OOM;
-    k_ut_write<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, ub.fin, ub.partner, X, ub.out_off, ub.out);
+    k_ut_write<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, ub.fin, ub.partner, X, ub.out_off, in.k, ub.out);
     if (cudaGetLastError() != cudaSuccess) return CFG_ERR_CUDA;
     res.bytes = w[0]; res.n_units = w[1]; res.n_cycle_lmtigs = w[2];
     return CFG_OK;
