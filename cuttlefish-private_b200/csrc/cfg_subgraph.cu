@@ -519,20 +519,72 @@ struct RecBases {
 // (lm: one end exits the subgraph) as record idx with its label at offset off.
 // The label of a path whose bases the walk kept: the walk's first k-mer, then one base
 // per step; `skip` leading bases are not part of the path (a one-k-mer cycle at its start).
+
+// The walk's bases as a little-endian 2-bit array over four words: base j at bits
+// 2 (j & 31) of word j >> 5 (first k-mer, then up to 64 steps: at most 127 bases).
+struct WalkSeq { uint64_t w0, w1, w2, w3; };
+__device__ __forceinline__ uint64_t rev_bases(uint64_t x) {   // reverses the order of 32 2-bit bases
+    const uint64_t r = __brevll(x);
+    return ((r >> 1) & 0x5555555555555555ull) | ((r & 0x5555555555555555ull) << 1);
+}
+template <int W>
+__device__ __forceinline__ WalkSeq walk_seq(uint32_t k, const Kmer<W>& first, uint64_t s0, uint64_t s1) {
+    WalkSeq q;
+    if constexpr (W == 1) {   // k <= 31
+        const uint32_t sh = 2 * k;
+        const uint64_t f = rev_bases(first.lo) >> (64 - sh);
+        q.w0 = f | (s0 << sh); q.w1 = (s0 >> (64 - sh)) | (s1 << sh); q.w2 = s1 >> (64 - sh); q.w3 = 0;
+    } else {                  // 33 <= k <= 63: hi holds the first k - 32 bases
+        const uint32_t sh = 2 * (k - 32);
+        const uint64_t h = rev_bases(first.hi) >> (64 - sh), lo = rev_bases(first.lo);
+        q.w0 = h | (lo << sh); q.w1 = (lo >> (64 - sh)) | (s0 << sh);
+        q.w2 = (s0 >> (64 - sh)) | (s1 << sh); q.w3 = s1 >> (64 - sh);
+    }
+    return q;
+}
+// bases j .. j+7 (j + 8 <= 128), base j in bits 1:0
+__device__ __forceinline__ uint32_t seq_get16(const WalkSeq& q, uint32_t j) {
+    const uint32_t w = j >> 5, o = 2 * (j & 31);
+    const uint64_t a = w == 0 ? q.w0 : w == 1 ? q.w1 : w == 2 ? q.w2 : q.w3;
+    const uint64_t b = w == 0 ? q.w1 : w == 1 ? q.w2 : w == 2 ? q.w3 : 0ull;
+    const uint64_t v = o ? ((a >> o) | (b << (64 - o))) : a;
+    return (uint32_t)v & 0xFFFFu;
+}
+// character tables for __byte_perm: byte b is the character of base b (or of its complement)
+constexpr uint32_t CH_FWD = 0x54474341u;   // A C G T
+constexpr uint32_t CH_CMP = 0x41434754u;   // T G C A
+__device__ __forceinline__ uint32_t sel4(uint32_t x) {   // four 2-bit bases -> one selector nibble each
+    return (x & 3u) | ((x & 0xCu) << 2) | ((x & 0x30u) << 4) | ((x & 0xC0u) << 6);
+}
+__device__ __forceinline__ uint64_t chars8(uint32_t x16, uint32_t table) {
+    return (uint64_t)__byte_perm(table, 0, sel4(x16 & 0xFFu)) | ((uint64_t)__byte_perm(table, 0, sel4(x16 >> 8)) << 32);
+}
+__device__ __forceinline__ uint32_t rev8bases(uint32_t x16) {   // reverses the order of 8 2-bit bases
+    const uint32_t r = __brev(x16) >> 16;
+    return ((r >> 1) & 0x5555u) | ((r & 0x5555u) << 1);
+}
+
+// Output byte i is base skip + i (forward), or the complement of base skip + L - 1 - i
+// (rev); written in address order, eight characters per aligned 8-byte store.
 template <int W>
 __device__ void write_buffered(const KOps<W>& ops, const Kmer<W>& first, unsigned long long steps0,
                                unsigned long long steps1, uint32_t skip, uint32_t L, char* dst, bool rev) {
     if (!dst) return;
-    const uint32_t k = ops.k;
-    WordWriter ww;
-    for (uint32_t i = 0; i < L; ++i) {
-        const uint32_t j = i + skip;   // index in the walk's base sequence
-        const uint32_t q = j - k;      // step index (j >= k)
-        const uint32_t b = j < k ? ops.base(first, j) : (uint32_t)((q < 32 ? steps0 : steps1) >> (2 * (q & 31))) & 3u;
-        if (!rev) ww.put(dst + i, "ACGT"[b]);
-        else ww.put(dst + (L - 1 - i), "ACGT"[3 - b]);
+    const WalkSeq q = walk_seq<W>(ops.k, first, steps0, steps1);
+    const uint32_t table = rev ? CH_CMP : CH_FWD;
+    auto one = [&](uint32_t i) {
+        const uint32_t b = seq_get16(q, rev ? skip + L - 1 - i : skip + i) & 3u;
+        dst[i] = (char)(table >> (8 * b));
+    };
+    const uint32_t off = (uint32_t)((unsigned long long)dst & 7);
+    const uint32_t head = off ? (L < 8 - off ? L : 8 - off) : 0;
+    uint32_t i = 0;
+    for (; i < head; ++i) one(i);
+    for (; i + 8 <= L; i += 8) {
+        const uint32_t x = rev ? rev8bases(seq_get16(q, skip + L - 8 - i)) : seq_get16(q, skip + i);
+        *(unsigned long long*)(dst + i) = chars8(x, table);
     }
-    ww.flush();
+    for (; i < L; ++i) one(i);
 }
 
 template <int W, int MODE>
@@ -661,10 +713,10 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
             const uint32_t pred = idx == 0 ? BASE_E : base_at(a.packed, p - 1);
             const uint32_t succ = idx + k == len ? BASE_E : base_at(a.packed, p + k);
             Kmer<W> pc = fw;
-            if (idx > 0) {
-                Kmer<W> pf = fw;
+            if (idx > 0) {   // the previous k-mer and its reverse complement, from fw and rc
+                Kmer<W> pf = fw, pr = rc;
                 ops.push_front(pf, pred);
-                const Kmer<W> pr = ops.rc(pf);
+                ops.push_back(pr, 3 - pred);
                 pc = pf < pr ? pf : pr;
             }
             if (!insert(fw, rc, pc, idx, pred, succ, (uint32_t)p, idx == 0 && rec_ld(rec), idx + k == len && rec_rd(rec)))
