@@ -554,6 +554,8 @@ def main():
     ap.add_argument("--cpu-sample-bases", type=int, default=60_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--table-load-pct", type=int, default=0, help="override the workload's table sizing factor")
+    ap.add_argument("--graph-count", type=int, default=0,
+                    help="subgraph count of the plain run (0: the fastest of 16384/32768/65536 to final unitigs)")
     ap.add_argument("--batch-genomes", type=int, default=1000, help="genomes of the batched comparison (0: skip it)")
     ap.add_argument("--batch-steps", type=int, default=2)
     ap.add_argument("--serve-jobs", type=int, default=16, help="jobs of the serving comparison (0: skip it)")
@@ -606,7 +608,21 @@ def main():
     import cfgpu
     data, offs, n_rec = make_workload(name, args.reads)
     packed = cfgpu.PackedInput(None, k, pinned=True, data_offsets=(data, offs, n_rec))
-    cx = cfgpu.Compactor(k, l, cutoff, 16384, device=local if world > 1 else 0, table_load_pct=load_pct)
+    # subgraph count: the fastest to final unitigs (they are the same for every count;
+    # the tuner checks that they are byte-identical across the candidates)
+    dev = local if world > 1 else 0
+    if args.graph_count:
+        gc, g_times, g_same = args.graph_count, None, None
+    else:
+        progress(f"{name}: tuning the subgraph count")
+        gc, g_times, g_same = cfgpu.tune_graph_count(packed, k, l, cutoff, load_pct, device=dev)
+        if not g_same:
+            raise RuntimeError("final unitigs differ between subgraph counts")
+    config["graph_count"] = gc
+    if g_times:
+        config["graph_count_tuning_ms"] = {str(g): round(t, 2) for g, t in g_times.items()}
+        config["unitigs_identical_across_graph_counts"] = g_same
+    cx = cfgpu.Compactor(k, l, cutoff, gc, device=dev, table_load_pct=load_pct)
 
     # e2e: H2D + run + device collation + D2H of the final unitigs, through the C ABI,
     # host buffers pinned

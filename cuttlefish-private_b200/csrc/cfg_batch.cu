@@ -283,7 +283,7 @@ int plan_shapes(cfg_batch* b) {
     for (uint32_t c = 0; c < cc.nl; ++c) {
         const uint32_t per = 64u << c;
         uint32_t t = per / std::max<uint32_t>(1, b->tune.local_div);
-        t = std::min<uint32_t>(512, std::max<uint32_t>(64, t));
+        t = std::min<uint32_t>(per > 4096 ? 1024 : 512, std::max<uint32_t>(64, t));
         t = (t + 31) / 32 * 32;
         const int occ = subgraph_occupancy(b->words, 1, t, per);
         if (occ <= 0) return bfail(b, CFG_ERR_CUDA, "no resident CTA for a table class");

@@ -274,7 +274,7 @@ struct Block {   // per-CTA shared bookkeeping (in CLUSTER mode the flags of ran
     uint32_t inserted, overflow, wl_n, scan_total;
     unsigned long long vertices, isolated, phantom, trivial, icc, lmtig;
     Sink sk;
-    uint32_t wsum[16];   // per-warp partial sums of a block scan (<= 512 threads)
+    uint32_t wsum[32];   // per-warp partial sums of a block scan (<= 1024 threads)
 };
 
 constexpr uint32_t FULL = 0xffffffffu;
@@ -999,7 +999,7 @@ __device__ __forceinline__ void carve(unsigned char* base, uint32_t per, unsigne
 
 // One subgraph per CTA (per = the table's whole capacity) or per cluster.
 template <int W, int MODE>
-__global__ void __launch_bounds__(512) k_subgraph_shared(const SubgraphArgs a) {
+__global__ void __launch_bounds__(W == 1 ? 1024 : 512) k_subgraph_shared(const SubgraphArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ Block B;
     uint32_t rank = 0, nranks = 1;
@@ -1041,7 +1041,7 @@ __global__ void __launch_bounds__(512) k_subgraph_global(const SubgraphArgs a) {
 
 // The kernels' shared-memory limit is always raised to the largest table any launch
 // uses (it is process-wide state: lowering it would break launches recorded in graphs).
-template <int W> constexpr size_t max_table_bytes() { return (size_t)(W == 1 ? 4096 : 2048) * (W == 1 ? 24 : 32); }
+template <int W> constexpr size_t max_table_bytes() { return (size_t)(W == 1 ? 8192 : 2048) * (W == 1 ? 24 : 32); }
 template <typename K>
 cudaError_t raise_smem_limit(K kernel, size_t bytes) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -1107,7 +1107,7 @@ __global__ void k_stripe_fixup(LmtigOut* lm, uint64_t lm_slice, const unsigned l
     }
 }
 
-uint32_t subgraph_max_per_cta(int words) { return words == 1 ? 4096 : 2048; }
+uint32_t subgraph_max_per_cta(int words) { return words == 1 ? 8192 : 2048; }
 uint32_t subgraph_cluster_per_cta(int words) { return words == 1 ? 4096 : 2048; }
 
 cudaError_t launch_subgraphs(const SubgraphArgs& a, int words, uint32_t cluster, uint32_t threads, cudaStream_t s) {

@@ -332,6 +332,39 @@ class Compactor:
         return [(d.records[i].pos, d.records[i].len, d.records[i].flags, d.records[i].g) for i in range(d.n)]
 
 
+def unitig_multiset(fasta: bytes):
+    """The sorted sequences of a unitig FASTA (record order and names carry no meaning)."""
+    return sorted(line for line in fasta.split(b"\n") if line and not line.startswith(b">"))
+
+
+def tune_graph_count(packed: PackedInput, k: int, l: int, cutoff: int, table_load_pct: int = 0, device: int = 0,
+                     candidates=(16384, 32768, 65536), runs: int = 2):
+    """Subgraph count for the fastest plain run to final unitigs.
+
+    The lm-tigs depend on the subgraph count, the final maximal unitigs do not: each
+    candidate is timed (device time of cfg_run + cfg_unitigs, the best of `runs` warm
+    runs) and its unitigs are compared with the first candidate's.
+    -> (best count, {count: ms}, unitigs identical for every candidate)."""
+    times, ref, same = {}, None, True
+    for g in candidates:
+        with Compactor(k, l, cutoff, g, device=device, table_load_pct=table_load_pct) as cx:
+            cx.submit(packed)
+            best = None
+            for _ in range(runs + 1):
+                cx.run()
+                _, _, _, ums = cx.unitigs_raw()
+                t = cx.timings()[3] + ums
+                best = t if best is None else min(best, t)
+            fa, nu = cx.unitigs()
+            ms = unitig_multiset(fa)
+            if ref is None:
+                ref = (ms, nu)
+            elif (ms, nu) != ref:
+                same = False
+            times[g] = best
+    return min(times, key=times.get), times, same
+
+
 def results_to_python(r: Results):
     """(counts, FASTA bytes, [LmtigRec]) from a cfg_results view."""
     fasta = ctypes.string_at(r.fasta, r.counts.fasta_bytes) if r.counts.fasta_bytes else b""

@@ -166,3 +166,24 @@ def test_device_unitigs(k, l, c, G, seed):
     assert orc.fasta_multiset(dev) == host
     assert n_units == counts.n_trivial + n_st
     assert host == orc.OracleRun(recs, k, l, c, 1).fasta_records()
+
+
+@pytest.mark.parametrize("k,c,seed", [(31, 2, 47), (31, 1, 48), (63, 1, 49)])
+def test_graph_count_tuner_keeps_unitigs(k, c, seed):
+    """tune_graph_count: the final unitigs of a plain run are the same at every subgraph
+    count it tries, and equal the global maximal unitigs."""
+    rng = np.random.default_rng(seed)
+    if c == 2:
+        g = synth.genome_with_repeats(rng, 40_000, n_copies=5, n_pal=3)
+        recs = synth.reads(rng, g, 4_000)
+    else:
+        recs = [synth.genome_with_repeats(rng, 60_000, n_copies=6, n_pal=4), synth.adversarial(rng, 8_000, k)]
+    packed = cfgpu.PackedInput(recs, k)
+    best, times, same = cfgpu.tune_graph_count(packed, k, 20, c, 30 if c == 2 else 0, candidates=(16, 1024, 16384, 65536))
+    assert same and best in times and len(times) == 4
+    with cfgpu.Compactor(k, 20, c, best, table_load_pct=30 if c == 2 else 0) as cx:
+        cx.submit(packed)
+        cx.run()
+        dev, _ = cx.unitigs()
+    assert orc.fasta_multiset(dev) == orc.OracleRun(recs, k, 20, c, 1).fasta_records()
+    packed.close()
