@@ -18,6 +18,7 @@ namespace {
 
 constexpr int RING = 128;             // per-warp ring of l-mer hashes (w <= 62)
 constexpr int WARPS_PER_BLOCK = 8;
+constexpr uint32_t STAGE = 256;       // records a warp gathers in shared memory per reservation
 
 __device__ __forceinline__ uint32_t lanemask_lt() { uint32_t m; asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m)); return m; }
 
@@ -25,12 +26,30 @@ __device__ __forceinline__ uint64_t lmer_at(const uint64_t* __restrict__ s, uint
     return window64(s, p) >> (64 - 2 * l);
 }
 
+// A warp's records wait in shared memory and are reserved in the flat array together:
+// one atomic on the run's record cursor per STAGE records instead of one per 32 positions.
+struct Stage { uint64_t* buf; uint32_t n; };
+__device__ __forceinline__ void stage_flush(const PartitionArgs& a, Stage& st) {
+    if (st.n == 0) return;
+    const uint32_t lane = threadIdx.x & 31;
+    unsigned long long b0 = 0;
+    if (lane == 0) b0 = atomicAdd(a.rec_cursor, (unsigned long long)st.n);
+    b0 = __shfl_sync(0xffffffffu, b0, 0);
+    __syncwarp();
+    for (uint32_t i = lane; i < st.n; i += 32) {
+        const unsigned long long idx = b0 + i;
+        if (idx < a.rec_cap) a.recs[idx] = st.buf[i]; else atomicOr(a.err, DERR_REC_OVERFLOW);
+    }
+    __syncwarp();
+    st.n = 0;
+}
+
 // Processes the (k-1)-mer positions [j0, j1) of one fragment: emits every weak
 // super k-mer whose run starts there.
 // mod_w[x] = x % w for x < 128 (w <= 62): the cap-cut test without a division.
 // hist: this fragment's job's histogram (the run's, or its job's slice of a batch's).
 __device__ void sweep_fragment(const PartitionArgs& a, uint64_t* ring, const uint8_t* mod_w, uint64_t F0, uint32_t FL,
-                               uint32_t j0, uint32_t j1, unsigned long long* hist) {
+                               uint32_t j0, uint32_t j1, unsigned long long* hist, Stage& st) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t k = a.k, l = a.l, w = a.w;
     const uint32_t M = FL - k + 2;                 // (k-1)-mers in the fragment
@@ -45,11 +64,21 @@ __device__ void sweep_fragment(const PartitionArgs& a, uint64_t* ring, const uin
     uint32_t r0 = 0, last_cut = 0, last_cut_g = 0, last_cut_chg = 0, carry_g = 0;
     uint32_t carry_rem = 0;   // (base - start of the run in progress) % w
 
+    // each chunk's new l-mer hash is computed one chunk ahead, so its loads and
+    // multiplies overlap the window minima of the chunk before (the ring holds both:
+    // 64 + w - 1 <= RING)
+    uint64_t h_next = 0;
+    {
+        const uint32_t q = start + w - 1 + lane;
+        if (q < n_lmers) h_next = lmer_hash(lmer_at(a.packed, F0 + q, l), l, a.seed0);
+    }
     for (uint32_t base = start;; base += 32) {
         __syncwarp();
         {
             const uint32_t q = base + w - 1 + lane;
-            if (q < n_lmers) ring[q & (RING - 1)] = lmer_hash(lmer_at(a.packed, F0 + q, l), l, a.seed0);
+            if (q < n_lmers) ring[q & (RING - 1)] = h_next;
+            const uint32_t q2 = q + 32;
+            h_next = q2 < n_lmers ? lmer_hash(lmer_at(a.packed, F0 + q2, l), l, a.seed0) : 0;
         }
         __syncwarp();
         const uint32_t j = base + lane;
@@ -113,11 +142,9 @@ __device__ void sweep_fragment(const PartitionArgs& a, uint64_t* ring, const uin
         const uint32_t pchg = __shfl_sync(0xffffffffu, (uint32_t)is_chg, pl);
         const bool fin = !stopping && (base + 32 >= M);      // the fragment's last (k-1)-mer is in this chunk
         const uint32_t n_emit = __popc(emit) + (fin ? 1 : 0);
-        unsigned long long slot0 = 0;
-        if (n_emit) {
-            if (lane == 0) slot0 = atomicAdd(a.rec_cursor, (unsigned long long)n_emit);
-            slot0 = __shfl_sync(0xffffffffu, slot0, 0);
-        }
+        if (st.n + n_emit > STAGE) stage_flush(a, st);
+        const uint32_t slot0 = st.n;
+        st.n += n_emit;
         if ((emit >> lane) & 1) {
             const uint32_t c = below ? base + pl : last_cut;
             const uint32_t cg = below ? pg : last_cut_g;
@@ -125,8 +152,7 @@ __device__ void sweep_fragment(const PartitionArgs& a, uint64_t* ring, const uin
             const uint32_t lj = c > 0;
             const uint32_t len = lj + (j - c + k - 2) + 1;
             const uint64_t r = rec_pack((uint32_t)(F0 + c - lj), len, lj & cchg, is_chg ? 1u : 0u, cg);
-            const unsigned long long idx = slot0 + __popc(emit & lanemask_lt());
-            if (idx < a.rec_cap) a.recs[idx] = r; else atomicOr(a.err, DERR_REC_OVERFLOW);
+            st.buf[slot0 + __popc(emit & lanemask_lt())] = r;
             atomicAdd(hist + cg, 1ull | ((unsigned long long)(len - k + 1) << 32));
         }
         // carries: last cut / run start of this chunk
@@ -142,8 +168,7 @@ __device__ void sweep_fragment(const PartitionArgs& a, uint64_t* ring, const uin
             const uint32_t c = last_cut, lj = c > 0;
             const uint32_t len = lj + (FL - c);
             const uint64_t r = rec_pack((uint32_t)(F0 + c - lj), len, lj & last_cut_chg, 0, last_cut_g);
-            const unsigned long long idx = slot0 + __popc(emit);
-            if (idx < a.rec_cap) a.recs[idx] = r; else atomicOr(a.err, DERR_REC_OVERFLOW);
+            st.buf[slot0 + __popc(emit)] = r;
             atomicAdd(hist + last_cut_g, 1ull | ((unsigned long long)(len - k + 1) << 32));
         }
         if (stopping || fin) return;
@@ -152,10 +177,12 @@ __device__ void sweep_fragment(const PartitionArgs& a, uint64_t* ring, const uin
 
 __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_partition(const PartitionArgs a) {
     __shared__ uint64_t rings[WARPS_PER_BLOCK][RING];
+    __shared__ uint64_t stages[WARPS_PER_BLOCK][STAGE];
     __shared__ uint8_t mod_w[128];
     if (threadIdx.x < 128) mod_w[threadIdx.x] = (uint8_t)(threadIdx.x % a.w);
     __syncthreads();
     uint64_t* ring = rings[threadIdx.x >> 5];
+    Stage st{stages[threadIdx.x >> 5], 0};
     const uint64_t n_seg = (a.n_bases + a.seg - 1) / a.seg;
     const uint64_t warp0 = (uint64_t)blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5);
     const uint64_t n_warps = (uint64_t)gridDim.x * WARPS_PER_BLOCK;
@@ -175,9 +202,10 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_partition(const Partit
             const uint32_t j0 = s0 > F0 ? (uint32_t)(s0 - F0) : 0;
             const uint64_t e = s1 - F0;
             const uint32_t j1 = e < M ? (uint32_t)e : M;
-            if (j0 < j1) sweep_fragment(a, ring, mod_w, F0, FL, j0, j1, a.hist + (a.frag_gbase ? a.frag_gbase[f] : 0u));
+            if (j0 < j1) sweep_fragment(a, ring, mod_w, F0, FL, j0, j1, a.hist + (a.frag_gbase ? a.frag_gbase[f] : 0u), st);
         }
     }
+    stage_flush(a, st);
 }
 
 // Exclusive scan of the per-subgraph record counts (one block).
