@@ -34,7 +34,7 @@ using namespace cfg;
 
 namespace {
 
-constexpr uint32_t NCLS = 16;   // LOCAL classes (<= 7), 7 cluster sizes, 1 global
+constexpr uint32_t NCLS = 16;   // LOCAL classes (64..8192 slots: <= 8), 7 cluster sizes, 1 global
 
 struct BatchWords {   // device-side scalars of one run, cleared by one memset
     uint32_t count[NCLS], off[NCLS], fill[NCLS];

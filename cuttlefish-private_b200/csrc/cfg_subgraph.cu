@@ -71,6 +71,12 @@ template <> struct Mem<LOCAL> {
     static __device__ __forceinline__ void or32(A a, uint32_t v) { asm volatile("red.shared.or.b32 [%0], %1;" :: "r"(a), "r"(v) : "memory"); }
     static __device__ __forceinline__ void fence() { __threadfence_block(); }
     static __device__ __forceinline__ void ld2(A a, uint64_t& x, uint64_t& y) { asm volatile("ld.volatile.shared.v2.u64 {%0, %1}, [%2];" : "=l"(x), "=l"(y) : "r"(a) : "memory"); }
+    // 16-byte compare-and-swap of {x, y} at a (16-byte aligned); returns the old pair in ox, oy
+    static __device__ __forceinline__ void cas128(A a, uint64_t cx, uint64_t cy, uint64_t nx, uint64_t ny, uint64_t& ox, uint64_t& oy) {
+        asm volatile("{\n\t.reg .b128 d, c, n;\n\tmov.b128 c, {%2, %3};\n\tmov.b128 n, {%4, %5};\n\t"
+                     "atom.shared.cas.b128 d, [%6], c, n;\n\tmov.b128 {%0, %1}, d;\n\t}"
+                     : "=l"(ox), "=l"(oy) : "l"(cx), "l"(cy), "l"(nx), "l"(ny), "r"(a) : "memory");
+    }
 };
 template <> struct Mem<CLUSTER> {
     typedef uint32_t A;
@@ -83,6 +89,11 @@ template <> struct Mem<CLUSTER> {
     static __device__ __forceinline__ void or32(A a, uint32_t v) { asm volatile("red.relaxed.cluster.shared::cluster.or.b32 [%0], %1;" :: "r"(a), "r"(v) : "memory"); }
     static __device__ __forceinline__ void fence() { asm volatile("fence.acq_rel.cluster;" ::: "memory"); }
     static __device__ __forceinline__ void ld2(A a, uint64_t& x, uint64_t& y) { asm volatile("ld.relaxed.cluster.shared::cluster.v2.u64 {%0, %1}, [%2];" : "=l"(x), "=l"(y) : "r"(a) : "memory"); }
+    static __device__ __forceinline__ void cas128(A a, uint64_t cx, uint64_t cy, uint64_t nx, uint64_t ny, uint64_t& ox, uint64_t& oy) {
+        asm volatile("{\n\t.reg .b128 d, c, n;\n\tmov.b128 c, {%2, %3};\n\tmov.b128 n, {%4, %5};\n\t"
+                     "atom.relaxed.cluster.shared::cluster.cas.b128 d, [%6], c, n;\n\tmov.b128 {%0, %1}, d;\n\t}"
+                     : "=l"(ox), "=l"(oy) : "l"(cx), "l"(cy), "l"(nx), "l"(ny), "r"(a) : "memory");
+    }
 };
 template <> struct Mem<GLOBAL> {
     typedef uint64_t A;   // generic address of global memory
@@ -96,6 +107,9 @@ template <> struct Mem<GLOBAL> {
     static __device__ __forceinline__ void fence() { __threadfence(); }
     static __device__ __forceinline__ void ld2(A a, uint64_t& x, uint64_t& y) {
         asm volatile("ld.volatile.v2.u64 {%0, %1}, [%2];" : "=l"(x), "=l"(y) : "l"(a) : "memory");
+    }
+    static __device__ __forceinline__ void cas128(A a, uint64_t cx, uint64_t cy, uint64_t nx, uint64_t ny, uint64_t& ox, uint64_t& oy) {
+        cfg::cas128((unsigned long long*)a, cx, cy, nx, ny, ox, oy);
     }
 };
 
@@ -217,6 +231,28 @@ struct Tab {
                     if (M::ld64(a) == x.lo) { seen = M::ld64(sa(b + h)); return b + h; }
                 }
             }
+            if (++h == per) h = 0;
+        }
+        return NONE;
+    }
+    // build phase, k <= 31: find or insert x together with its state update.  A free slot
+    // is claimed with x's first state by one 16-byte CAS (key and state are one pair; a
+    // free slot's state is ST_INIT); a slot holding x gets the state CAS of update_state.
+    __device__ uint32_t upsert(const Kmer<W>& x, uint32_t owner, uint32_t h, uint32_t front, uint32_t back, uint32_t pos,
+                               bool& fresh) const {
+        static_assert(W == 1, "one-word keys only");
+        fresh = false;
+        const uint32_t b = owner * per;
+        const uint64_t first = (uint64_t)ef_add(st_ef(ST_INIT), front, back) | ((uint64_t)min(st_ins(ST_INIT), pos) << 32);
+        for (uint32_t p = 0; p < per; ++p) {
+            const A a = ka(b + h);
+            uint64_t cur, stv;
+            M::ld2(a, cur, stv);
+            if (cur == EMPTY) {
+                M::cas128(a, EMPTY, ST_INIT, x.lo, first, cur, stv);
+                if (cur == EMPTY) { fresh = true; return b + h; }
+            }
+            if (cur == x.lo) { update_state(b + h, front, back, pos, stv); return b + h; }
             if (++h == per) h = 0;
         }
         return NONE;
@@ -654,6 +690,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
 
     // ---------------- build ----------------
     const uint32_t limit = (uint32_t)(((uint64_t)per * a.load_limit_pct) / 100);
+    uint32_t n_fresh = 0;   // vertices this thread inserted
     const uint32_t r0 = a.bucket_off[g], r1 = a.bucket_off[g + 1];
     // HT_Router::update of one k-mer instance at stream position p (idx-th of its record):
     // edges from its predecessor / successor bases, the self-loop rule against the
@@ -668,13 +705,16 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         uint32_t owner, h;
         T.place(can, owner, h);
         bool fresh;
-        uint64_t seen = ST_INIT;
-        const uint32_t s = T.find_or_insert(can, owner, h, fresh, seen);
+        uint32_t s;
+        if constexpr (W == 1) {
+            s = T.upsert(can, owner, h, front, back, p, fresh);
+        } else {
+            uint64_t seen = ST_INIT;
+            s = T.find_or_insert(can, owner, h, fresh, seen);
+            if (s != NONE) T.update_state(s, front, back, p, seen);
+        }
         if (s == NONE) { atomicOr(&B.overflow, 1u); return false; }
-        // fresh vertices are counted per inserting CTA (records, hence inserts, are spread
-        // evenly, so one CTA's count stands for one sub-table's load)
-        if (fresh && atomicAdd(&B.inserted, 1u) + 1 > limit) { atomicOr(&B.overflow, 1u); return false; }
-        T.update_state(s, front, back, p, seen);
+        n_fresh += fresh;
         uint32_t disc = 0;
         if (l_mark) disc |= canon ? M_DISC_F : M_DISC_B;      // entrance side
         if (r_mark) disc |= canon ? M_DISC_B : M_DISC_F;      // exit side
@@ -742,6 +782,13 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
             }
         }
     }
+    // fresh vertices are counted per inserting CTA (records, hence inserts, are spread
+    // evenly, so one CTA's count stands for one sub-table's load); a table over its load
+    // limit is retried larger
+    for (int d = 16; d; d >>= 1) n_fresh += __shfl_down_sync(0xffffffffu, n_fresh, d);
+    if ((tid & 31) == 0 && n_fresh) atomicAdd(&B.inserted, n_fresh);
+    __syncthreads();
+    if (tid == 0 && B.inserted > limit) B.overflow = 1;
     // one CTA's overflow is the whole cluster's
     __syncthreads();
     if (tid == 0 && B.overflow && Bc != &B) atomicOr(&Bc->overflow, 1u);
