@@ -244,7 +244,10 @@ struct Tab {
         fresh = false;
         const uint32_t b = owner * per;
         const uint64_t first = (uint64_t)ef_add(st_ef(ST_INIT), front, back) | ((uint64_t)min(st_ins(ST_INIT), pos) << 32);
-        for (uint32_t p = 0; p < per; ++p) {
+        // probe bound: a quarter of a large table (a run that long means the table is
+        // close to full: the insert fails and the subgraph is retried with a larger one)
+        const uint32_t bound = per > 256 ? per / 4 : per;
+        for (uint32_t p = 0; p < bound; ++p) {
             const A a = ka(b + h);
             uint64_t cur, stv;
             M::ld2(a, cur, stv);
@@ -783,8 +786,9 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         }
     }
     // fresh vertices are counted per inserting CTA (records, hence inserts, are spread
-    // evenly, so one CTA's count stands for one sub-table's load); a table over its load
-    // limit is retried larger
+    // evenly, so one CTA's count stands for one sub-table's load) and summed once: a table
+    // past its load limit is retried larger (one that fills up stops the build earlier,
+    // through an insert that exhausts its probe bound)
     for (int d = 16; d; d >>= 1) n_fresh += __shfl_down_sync(0xffffffffu, n_fresh, d);
     if ((tid & 31) == 0 && n_fresh) atomicAdd(&B.inserted, n_fresh);
     __syncthreads();
