@@ -242,10 +242,21 @@ int run_subgraphs(cfg_ctx* c, const std::vector<uint32_t>& inst_h) {
     // records' lengths sum to at most n_bases + k per record
     uint64_t lm_text_need = c->n_bases + (c->n_records + 1024) * (c->p.k + 1);
     uint64_t lm_need = c->n_records + 1024;
+    // larger subgraphs first (src/Subgraphs_Manager.cpp:222-231): a counting sort on a
+    // log-scale size key (eight steps per doubling), enough to start the big ones early
     std::vector<uint32_t> todo;
-    for (uint32_t g = 0; g < G; ++g) if (inst_h[g]) todo.push_back(g);
-    // larger subgraphs first (src/Subgraphs_Manager.cpp:222-231)
-    std::stable_sort(todo.begin(), todo.end(), [&](uint32_t a, uint32_t b) { return inst_h[a] > inst_h[b]; });
+    {
+        auto key = [](uint32_t n) -> uint32_t {   // 8 * log2(n), in [0, 255]
+            const uint32_t e = 31 - __builtin_clz(n);
+            const uint32_t frac = e >= 3 ? (n >> (e - 3)) & 7 : (n << (3 - e)) & 7;
+            return 8 * e + frac;
+        };
+        uint32_t cnt[257] = {0};
+        for (uint32_t g = 0; g < G; ++g) if (inst_h[g]) ++cnt[255 - key(inst_h[g]) + 1];
+        for (uint32_t b = 1; b < 257; ++b) cnt[b] += cnt[b - 1];
+        todo.resize(cnt[256]);
+        for (uint32_t g = 0; g < G; ++g) if (inst_h[g]) todo[cnt[255 - key(inst_h[g])]++] = g;
+    }
 
     for (int round = 0; round < 3; ++round) {   // output-arena overflow: regrow, rerun all
         int rc = ensure_outputs(c, fasta_need, lm_text_need, lm_need);
@@ -258,6 +269,8 @@ int run_subgraphs(cfg_ctx* c, const std::vector<uint32_t>& inst_h) {
         bool overflow = false;
         for (int pass = 0; pass < 12 && !work.empty(); ++pass) {
             std::vector<Launch> plan;
+            int shape_at[9 * 32];
+            std::fill(shape_at, shape_at + 9 * 32, -1);
             Launch glob; glob.cluster = 0;
             uint64_t arena_slots = 0;
             for (uint32_t g : work) {
@@ -271,10 +284,13 @@ int run_subgraphs(cfg_ctx* c, const std::vector<uint32_t>& inst_h) {
                     arena_slots += cap;
                     continue;
                 }
-                size_t i = 0;
-                while (i < plan.size() && !(plan[i].per == per && plan[i].cluster == cl)) ++i;
-                if (i == plan.size()) { plan.emplace_back(); plan.back().per = per; plan.back().cluster = cl; }
-                plan[i].list.push_back(g);
+                // launch of this shape: one per (cluster size, log2 slots)
+                const uint32_t sk = cl * 32 + (31 - __builtin_clz(per));
+                if (shape_at[sk] < 0) {
+                    shape_at[sk] = (int)plan.size();
+                    plan.emplace_back(); plan.back().per = per; plan.back().cluster = cl;
+                }
+                plan[shape_at[sk]].list.push_back(g);
             }
             plan.push_back(glob);
             CK(cudaMemsetAsync(&c->counters.as<Counters>()->retry_count, 0, sizeof(unsigned long long), c->stream));
