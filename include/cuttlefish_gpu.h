@@ -126,7 +126,9 @@ int cfg_create(int device, const cfg_params* params, cfg_ctx** out);
 int cfg_submit_packed(cfg_ctx* ctx, const uint64_t* packed, uint64_t n_bases,
                       const uint64_t* frag_off, const uint32_t* frag_len, uint64_t n_frags);
 
-/* Same, with the three arrays already in device memory (no copy). */
+/* Same, with the three arrays already in device memory (no copy).  d_packed must stay
+ * readable for 4 words past the word that holds the last base (the kernels read whole
+ * words around each record; cfg_pack_records and the batch's device copies have them). */
 int cfg_submit_packed_device(cfg_ctx* ctx, const uint64_t* d_packed, uint64_t n_bases,
                              const uint64_t* d_frag_off, const uint32_t* d_frag_len, uint64_t n_frags);
 
