@@ -233,7 +233,9 @@ int run_subgraphs(cfg_ctx* c, const std::vector<uint32_t>& inst_h) {
     const uint32_t load = c->p.table_load_pct ? c->p.table_load_pct : 100;
     const uint32_t per_max = subgraph_max_per_cta(W);   // one CTA's table
     const uint32_t per_cl = subgraph_cluster_per_cta(W);   // each CTA of a cluster
-    const uint32_t max_cluster = 8;
+    // k <= 31: clusters of up to 8 CTAs beat arena tables in HBM; k > 32 (24-byte key and
+    // state, 128-register kernels, one CTA per SM) the L2-resident arena tables win
+    const uint32_t max_cluster = W == 1 ? 8 : 1;
     std::vector<uint64_t> want(G, 0);                      // slots wanted per subgraph
     for (uint32_t g = 0; g < G; ++g)
         if (inst_h[g]) want[g] = std::max<uint64_t>(64, ((uint64_t)inst_h[g] * load * 2 + 99) / 100);

@@ -70,7 +70,8 @@ __host__ __device__ inline uint32_t class_of(uint32_t inst, const ClassCfg& c, u
         while ((64u << lg) < per) ++lg;
         return lg;
     }
-    if (want <= (uint64_t)c.per_cl * 8) return c.nl + (uint32_t)((want + c.per_cl - 1) / c.per_cl) - 2;
+    // clusters only for one-word keys (k > 32: arena tables in HBM are faster)
+    if (c.per_cl && want <= (uint64_t)c.per_cl * 8) return c.nl + (uint32_t)((want + c.per_cl - 1) / c.per_cl) - 2;
     return c.nl + 7;
 }
 
@@ -267,7 +268,7 @@ ClassCfg class_cfg(const cfg_batch* b) {
     const uint32_t per_max = subgraph_max_per_cta(b->words);
     c.nl = 0;
     while ((64u << c.nl) <= per_max) ++c.nl;
-    c.per_cl = subgraph_cluster_per_cta(b->words);
+    c.per_cl = b->words == 1 ? subgraph_cluster_per_cta(b->words) : 0;   // no cluster classes for k > 32
     c.g_shift = b->g_shift;
     c.n_buckets = b->n_jobs << b->g_shift;
     c.arena_slots = b->arena_slots;
@@ -289,7 +290,7 @@ int plan_shapes(cfg_batch* b) {
         if (occ <= 0) return bfail(b, CFG_ERR_CUDA, "no resident CTA for a table class");
         b->shapes.push_back(Shape{c, 1, t, per, (uint32_t)(occ * sms)});
     }
-    for (uint32_t cl = 2; cl <= 8; ++cl) {
+    for (uint32_t cl = 2; cc.per_cl && cl <= 8; ++cl) {   // cluster classes (k <= 31 only)
         const uint32_t t = b->tune.cluster_threads ? b->tune.cluster_threads : 512;
         const int occ = subgraph_occupancy(b->words, cl, t, cc.per_cl);
         if (occ <= 0) return bfail(b, CFG_ERR_CUDA, "no resident cluster for a table class");
