@@ -220,18 +220,18 @@ def bench_batch(args, pg, local, world, peak, with_cpu):
                        "each genome its own job ending at its own final maximal unitigs",
         "n_genomes": len(packed), "bases": bases, "unitigs": units,
         "outputs_equal": units == units_p and d2h == d2h_p,
-        "batched": {"value": world * bases * steps / (b_dev / 1e3), "unit": "bases/s", "ms_per_step": b_dev / steps,
+        "batched": {"value": job_rate(world, bases, steps, b_dev / 1e3), "unit": "bases/s", "ms_per_step": b_dev / steps,
                     "graph_ms": statistics.mean(run_ms), "collate_ms": statistics.mean(col_ms),
-                    "e2e": {"value": world * bases * steps / b_e2e, "ms_per_step": 1e3 * b_e2e / steps,
+                    "e2e": {"value": job_rate(world, bases, steps, b_e2e), "ms_per_step": 1e3 * b_e2e / steps,
                             "h2d_bytes_per_step": bases // 4, "d2h_bytes_per_step": d2h},
                     "graph_launches_per_step": 1, "gpu_launches_per_step": int(info.kernels_per_run),
                     "jobs_redone_alone": int(info.n_redone),
                     "tuning": {"local_div": tuning.local_div, "cluster_threads": tuning.cluster_threads,
                                "table_load_pct": tuning.table_load_pct,
                                "graph_count": tuning.graph_count or 16384, "tuned_ms": tuning.ms}},
-        "plain": {"value": world * bases * steps / (p_dev / 1e3), "unit": "bases/s", "ms_per_step": p_dev / steps,
+        "plain": {"value": job_rate(world, bases, steps, p_dev / 1e3), "unit": "bases/s", "ms_per_step": p_dev / steps,
                   "collate_ms": sum(plain_col) / steps,
-                  "e2e": {"value": world * bases * steps / p_e2e, "ms_per_step": 1e3 * p_e2e / steps,
+                  "e2e": {"value": job_rate(world, bases, steps, p_e2e), "ms_per_step": 1e3 * p_e2e / steps,
                           "d2h_bytes_per_step": d2h_p},
                   "gpu_launches_per_step": plain_launches},
         "speedup_device": p_dev / b_dev, "speedup_e2e": p_e2e / b_e2e,
@@ -479,6 +479,8 @@ def measured_hbm_peak():
 
 
 def dist_setup(n_gpus):
+    """One process per GPU under torchrun: (rank, world, local rank, process group or None).
+    The backend is NCCL; CFG_BENCH_BACKEND=gloo runs the same plumbing on CPU (tests)."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -488,17 +490,21 @@ def dist_setup(n_gpus):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        backend = os.environ.get("CFG_BENCH_BACKEND", "nccl")
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
         pg = dist
     return rank, world, local, pg
 
 
 def allreduce_max(pg, local, x):
+    """The maximum of x over all ranks (every rank's own time: the job's time is the slowest)."""
     if pg is None:
         return x
     import torch
-    t = torch.tensor([float(x)], device=f"cuda:{local}")
+    dev = f"cuda:{local}" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], device=dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
@@ -506,6 +512,12 @@ def allreduce_max(pg, local, x):
 def barrier(pg):
     if pg is not None:
         pg.barrier()
+
+
+def job_rate(world, units_per_rank, steps, seconds_max):
+    """Whole-job throughput of N replicas: every rank processes the same units each step,
+    timed as the slowest rank."""
+    return world * units_per_rank * steps / seconds_max
 
 
 def cpu_reference(args, name, data, offs, n_rec, threads):
@@ -667,8 +679,8 @@ def main():
     total_ms_max = allreduce_max(pg, local, total_ms)
     e2e_s_max = allreduce_max(pg, local, sum(e2e_times))
     bases = counts.n_bases
-    value = world * bases * args.steps / (total_ms_max / 1e3)
-    e2e_value = world * bases * args.steps / e2e_s_max
+    value = job_rate(world, bases, args.steps, total_ms_max / 1e3)
+    e2e_value = job_rate(world, bases, args.steps, e2e_s_max)
 
     # roofline of the dominant kernel (subgraph construct + walk): algorithmic bytes
     W = 1 if k <= 31 else 2
