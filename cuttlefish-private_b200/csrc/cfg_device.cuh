@@ -149,17 +149,21 @@ template <int W> __device__ __forceinline__ uint64_t key_hash(const Kmer<W>& x) 
 // ---------------------------------------------------------------------------
 // Per-vertex edge state, State_Config<false> (include/State_Config.hpp:24-268):
 // 4-bit saturating counts, front side in bits 0-15, back in 16-31, base b at 4b.
-__device__ __forceinline__ uint32_t ef_count(uint32_t ef, int side, uint32_t fth) {
-    const uint32_t h = ef >> (side == FRONT ? 0 : 16);
-    return (((h >> 0) & 15) >= fth) + (((h >> 4) & 15) >= fth) + (((h >> 8) & 15) >= fth) + (((h >> 12) & 15) >= fth);
+// The four 4-bit counts of one side spread to bytes; bit 7 of byte b is set iff count b
+// reaches the threshold fth (1..15): count + 128 - fth >= 128, no carry between bytes.
+__device__ __forceinline__ uint32_t ef_present(uint32_t ef, int side, uint32_t fth) {
+    const uint32_t h = (ef >> (side == FRONT ? 0 : 16)) & 0xFFFFu;
+    const uint32_t b = (h & 0xFu) | ((h & 0xF0u) << 4) | ((h & 0xF00u) << 8) | ((h & 0xF000u) << 12);
+    return (b + (0x80808080u - fth * 0x01010101u)) & 0x80808080u;
 }
+__device__ __forceinline__ uint32_t ef_count(uint32_t ef, int side, uint32_t fth) {
+    return __popc(ef_present(ef, side, fth));
+}
+// the side's single edge base, BASE_E without edges, BASE_N with several
 __device__ __forceinline__ uint32_t ef_edge_at(uint32_t ef, int side, uint32_t fth) {
-    const uint32_t h = ef >> (side == FRONT ? 0 : 16);
-    uint32_t c = 0, last = BASE_E;
-#pragma unroll
-    for (uint32_t b = 0; b < 4; ++b)
-        if (((h >> (4 * b)) & 15) >= fth) { ++c; last = b; }
-    return c == 0 ? BASE_E : (c == 1 ? last : BASE_N);
+    const uint32_t m = ef_present(ef, side, fth);
+    const uint32_t c = __popc(m);
+    return c == 0 ? BASE_E : (c == 1 ? (uint32_t)(__ffs(m) - 8) >> 3 : BASE_N);
 }
 // e_f after Vertex_Neighborhood::update_edges(front, back) (:255-268, :207-217).
 __device__ __forceinline__ uint32_t ef_add(uint32_t ef, uint32_t front, uint32_t back) {

@@ -811,16 +811,17 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
     // ---------------- W1: termination of every side ----------------
     compact(per, wl, &B.wl_n, [&](uint32_t ls) { return !local_empty<W>(lkeys, ls); });
     __syncthreads();
+    uint32_t n_vert = 0, n_iso = 0, n_phantom = 0;   // this thread's vertices (summed once per warp)
     for (uint32_t i = tid, nw = B.wl_n; i < nw; i += nt) {
         const uint32_t ls = wl[i];
         const uint32_t s = base_slot + ls;
         const uint32_t ef = st_ef(lst[sti<W>(ls)]);
         uint32_t meta = lmeta[ls];
         const uint32_t cf = ef_count(ef, FRONT, fth), cb = ef_count(ef, BACK, fth);
-        atomicAdd(&B.vertices, 1ull);
+        ++n_vert;
         if (cf == 0 && cb == 0) {
-            atomicAdd(&B.isolated, 1ull);
-            if (meta & (M_DISC_F | M_DISC_B)) atomicAdd(&B.phantom, 1ull);
+            ++n_iso;
+            if (meta & (M_DISC_F | M_DISC_B)) ++n_phantom;
             lmeta[ls] = meta | M_ISO;
             continue;
         }
@@ -849,6 +850,16 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         const uint32_t eb = ef_edge_at(ef, BACK, fth);
         if (eb < 2 && cf <= 1 && ops.is_homopolymer(x, eb)) meta |= M_Q;
         lmeta[ls] = meta;
+    }
+    for (int d = 16; d; d >>= 1) {
+        n_vert += __shfl_down_sync(0xffffffffu, n_vert, d);
+        n_iso += __shfl_down_sync(0xffffffffu, n_iso, d);
+        n_phantom += __shfl_down_sync(0xffffffffu, n_phantom, d);
+    }
+    if ((tid & 31) == 0) {
+        if (n_vert) atomicAdd(&B.vertices, (unsigned long long)n_vert);
+        if (n_iso) atomicAdd(&B.isolated, (unsigned long long)n_iso);
+        if (n_phantom) atomicAdd(&B.phantom, (unsigned long long)n_phantom);
     }
     tsync<MODE>();
 
