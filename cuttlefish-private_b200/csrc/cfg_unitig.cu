@@ -20,8 +20,9 @@
 //      starts with a smaller k-mer (Maximal_Unitig::canonicalize,
 //      include/Unitig_Collator.hpp:308-347);
 //   4. reserve each unitig's FASTA record, and let every lm-tig copy its label (read
-//      forward or reverse-complemented) to its offset -- neighbours write the shared
-//      k-mer twice, with the same bytes.
+//      forward or reverse-complemented) to its offset -- all of it at the unitig's
+//      tail, all but the last k bases elsewhere (its successor writes the k-mer they
+//      share).
 // Entries that never reach a head lie on closed chains (cycles); those lm-tigs are
 // handed back to the host collator, whose rotation rule they need (rare).
 #include "cuttlefish_gpu.h"
