@@ -844,7 +844,6 @@ int cfg_batch_unitigs(cfg_batch* b, float* device_ms) {
         in.job_out_base = b->u_out.as<unsigned long long>() + j0;
         in.job_cur = b->u_cur.as<unsigned long long>() + (size_t)j0 * JOB_CUR_STRIDE;
         in.job_lm = b->lm.as<LmtigOut>(); in.job_text = b->lm_text.as<char>();
-        in.max_job_n = *std::max_element(jn.begin() + j0, jn.begin() + j1);
         UnitigResult res{};
         int rc = collate_device(in, b->ub, b->stream, res);
         if (rc == CFG_ERR_STATE) return bfail(b, rc, "lm-tig ends do not form a valid discontinuity graph");

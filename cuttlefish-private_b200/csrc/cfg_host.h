@@ -103,7 +103,6 @@ struct UnitigInput {
     unsigned long long* job_cur;
     const LmtigOut* job_lm;                       // the batch's lm-tig arena
     const char* job_text;                         // and label arena
-    uint64_t max_job_n;                           // the most records of one job
 };
 // ... the buffers it works in ...
 struct UnitigBuffers {

@@ -100,16 +100,16 @@ __global__ void k_ut_gather_jobs(const LmtigOut* lm, const char* text, const Job
 // n_j)) -- its lm-tigs are [base_j, base_j + n_j) -- so a vertex is (job, k-mer) by
 // construction.  Blocks take tiles of ends from a counter, in order, so the ends in
 // flight span a window of about one job and the table slots, lm-tigs and partners
-// they touch stay in L2; a table region larger than L2 is filled in `n_pass` passes,
-// pass p inserting the ends whose home slot lies in the p-th slice of their region.
-// The slot's first end is claimed by CAS and its k-mer read from the (immutable)
-// lm-tig, so no thread waits on another.
+// they touch stay in L2 (one large job is inserted in one pass all the same: slicing
+// its region to fit L2 re-reads every end per slice and measured slower).  The slot's
+// first end is claimed by CAS and its k-mer read from the (immutable) lm-tig, so no
+// thread waits on another.
 constexpr uint32_t INSERT_TILE = 1024;
 __global__ void __launch_bounds__(256, 6) k_ut_insert(const LmtigOut* __restrict__ lm, const uint32_t* __restrict__ job,
                                                     uint64_t n, uint32_t* tab,
                                                     const unsigned long long* __restrict__ job_lm_base,
-                                                    const unsigned long long* __restrict__ job_n, uint32_t pass,
-                                                    uint32_t n_pass, unsigned long long* tiles, uint32_t* partner,
+                                                    const unsigned long long* __restrict__ job_n,
+                                                    unsigned long long* tiles, uint32_t* partner,
                                                     uint32_t* err) {
     __shared__ unsigned long long tile;
     const uint64_t n2 = 2 * n;
@@ -127,7 +127,6 @@ __global__ void __launch_bounds__(256, 6) k_ut_insert(const LmtigOut* __restrict
             if (is_phi(m, end)) continue;
             const unsigned long long k0 = end ? m.v[0] : m.u[0], k1 = end ? m.v[1] : m.u[1];
             const uint64_t h = mix64(k0 ^ mix64(k1 + 0x9E3779B97F4A7C15ull));
-            if (n_pass > 1 && __umul64hi(h, n_pass) != pass) continue;
             const uint32_t jb = job ? job[e >> 1] : 0u;
             const uint64_t base = job ? 4 * job_lm_base[jb] : 0, t = job ? 4 * job_n[jb] : 4 * n;
             uint64_t p = base + __umul64hi(h, t);
@@ -535,14 +534,8 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
     if (cudaMemsetAsync(ub.tab, 0xff, sizeof(EndSlot) * ub.tab_n, s) != cudaSuccess ||
         cudaMemsetAsync(ub.partner, 0xff, 4 * 2 * n, s) != cudaSuccess)
         return CFG_ERR_CUDA;
-    // table regions over 64 MB are filled in slices that fit L2
-    const uint64_t big = in.jobs && in.max_job_n ? in.max_job_n : n;
-    const uint32_t n_pass = (uint32_t)std::max<uint64_t>(1, (4 * big * sizeof(EndSlot) + (64ull << 20) - 1) >> 26);
-    for (uint32_t pass = 0; pass < n_pass; ++pass) {
-        if (cudaMemsetAsync(cursor + 5, 0, 8, s) != cudaSuccess) return CFG_ERR_CUDA;
-        k_ut_insert<<<grid, 256, 0, s>>>(ub.lm, job, n, (uint32_t*)ub.tab, in.job_lm_base, in.job_n, pass, n_pass,
-                                         cursor + 5, ub.partner, in.err);
-    }
+    k_ut_insert<<<grid, 256, 0, s>>>(ub.lm, job, n, (uint32_t*)ub.tab, in.job_lm_base, in.job_n, cursor + 5, ub.partner,
+                                     in.err);
     // ranking: splitters, their walks, pointer jumping over the splitters, every entry
     RankRec* X = (RankRec*)ub.X[0];
     uint2* node = (uint2*)ub.out_off;                          // free until the records are reserved
