@@ -103,7 +103,8 @@ def test_homopolymer_and_cycles():
 @pytest.mark.parametrize("k", [31, 63])
 @pytest.mark.parametrize("load_pct", [1500, 4500, 40000])
 def test_table_modes(k, load_pct):
-    """Oversized table requests route subgraphs to one-CTA, cluster (DSMEM) and global-arena tables."""
+    """Oversized table requests route subgraphs to one-CTA, cluster (DSMEM; k <= 31 only) and
+    global-arena tables."""
     rng = np.random.default_rng(24 + load_pct)
     recs = [synth.adversarial(rng, 20_000, k) for _ in range(2)]
     compare(recs, k, 20, 1, 64, load_pct=load_pct)
