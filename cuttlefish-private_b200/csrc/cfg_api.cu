@@ -420,6 +420,10 @@ int cfg_submit_packed(cfg_ctx* c, const uint64_t* packed, uint64_t n_bases, cons
                       const uint32_t* frag_len, uint64_t n_frags) {
     if (!c || (n_bases && !packed) || (n_frags && (!frag_off || !frag_len))) return fail(c, CFG_ERR_BAD_INPUT, "null input");
     if (n_bases >= (1ull << 32)) return fail(c, CFG_ERR_BAD_INPUT, "a job must hold fewer than 2^32 bases");
+    // the copy sizes must agree with the table before anything is read: the last fragment
+    // ends at n_bases (the full check below runs while the copies do)
+    if (n_frags ? frag_off[n_frags - 1] + frag_len[n_frags - 1] != n_bases : n_bases != 0)
+        return fail(c, CFG_ERR_BAD_INPUT, "fragment lengths do not sum to n_bases");
     CK(cudaSetDevice(c->device));
     c->have_input = false; c->have_run = false;
     const uint64_t words = (n_bases + 31) / 32;

@@ -12,6 +12,8 @@ from dataclasses import dataclass
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 LIB_PATH = os.path.join(PKG_DIR, "lib", "libcfgpu.so")
 
+# status codes of include/cuttlefish_gpu.h
+CFG_OK, CFG_ERR_BAD_INPUT, CFG_ERR_OOM, CFG_ERR_TABLE_FULL, CFG_ERR_WALK_LIMIT, CFG_ERR_CUDA, CFG_ERR_STATE = range(7)
 CFG_FLAG_DUMP_STATES = 0x1
 CFG_FLAG_DUMP_RECORDS = 0x2
 CFG_NOALLOC_MAX_BASES = 917472

@@ -188,3 +188,34 @@ def test_graph_count_tuner_keeps_unitigs(k, c, seed):
         dev, _ = cx.unitigs()
     assert orc.fasta_multiset(dev) == orc.OracleRun(recs, k, 20, c, 1).fasta_records()
     packed.close()
+
+
+def test_submit_rejects_bad_fragment_tables():
+    """cfg_submit_packed checks the fragment table while its copies run: a bad table is
+    refused (and leaves no input), and the next valid submission runs normally."""
+    import ctypes
+    rng = np.random.default_rng(50)
+    recs = [synth.random_seq(rng, 500), synth.random_seq(rng, 300)]
+    packed = cfgpu.PackedInput(recs, 31)
+    p = packed.p
+    lib = cfgpu.load()
+    off = [p.frag_off[i] for i in range(p.n_frags)]
+    ln = [p.frag_len[i] for i in range(p.n_frags)]
+    U64 = ctypes.c_uint64 * p.n_frags
+    U32 = ctypes.c_uint32 * p.n_frags
+    with cfgpu.Compactor(31, 20, 1, 16384) as cx:
+        bad_tables = [
+            (U64(*([off[0] + 1] + off[1:])), U32(*ln)),                 # not back to back
+            (U64(*off), U32(*([31] + ln[1:]))),                          # shorter than k + 1
+        ]
+        for fo, fl in bad_tables:
+            rc = lib.cfg_submit_packed(cx.ctx, p.words, p.n_bases, fo, fl, p.n_frags)
+            assert rc == cfgpu.CFG_ERR_BAD_INPUT
+            assert lib.cfg_run(cx.ctx) != 0          # nothing was left to run
+        rc = lib.cfg_submit_packed(cx.ctx, p.words, p.n_bases + 1, p.frag_off, p.frag_len, p.n_frags)
+        assert rc == cfgpu.CFG_ERR_BAD_INPUT         # lengths do not sum to n_bases
+        cx.submit(packed)
+        cx.run()
+        dev, _ = cx.unitigs()
+    assert orc.fasta_multiset(dev) == orc.OracleRun(recs, 31, 20, 1, 1).fasta_records()
+    packed.close()
