@@ -514,6 +514,13 @@ def barrier(pg):
         pg.barrier()
 
 
+def agree_graph_count(pg, local, times):
+    """Replicas run the same work: every rank takes each candidate's slowest time over the
+    ranks and picks the fastest of those, so all ranks choose the same subgraph count."""
+    agreed = {g: allreduce_max(pg, local, t) for g, t in sorted(times.items())}
+    return min(agreed, key=agreed.get), agreed
+
+
 def job_rate(world, units_per_rank, steps, seconds_max):
     """Whole-job throughput of N replicas: every rank processes the same units each step,
     timed as the slowest rank."""
@@ -630,6 +637,7 @@ def main():
         gc, g_times, g_same = cfgpu.tune_graph_count(packed, k, l, cutoff, load_pct, device=dev)
         if not g_same:
             raise RuntimeError("final unitigs differ between subgraph counts")
+        gc, g_times = agree_graph_count(pg, local, g_times)
     config["graph_count"] = gc
     if g_times:
         config["graph_count_tuning_ms"] = {str(g): round(t, 2) for g, t in g_times.items()}

@@ -28,7 +28,10 @@ def _rank(rank, world, port, out):
     assert (r, w, local) == (rank, world, rank) and pg is not None
     slowest = bench.allreduce_max(pg, local, 10.0 + 5.0 * rank)   # each rank's own seconds
     bench.barrier(pg)
-    out.put((rank, slowest, bench.job_rate(w, 1000, 3, slowest)))
+    # rank 0 alone would pick 16384, rank 1 alone 65536: both take the best worst case
+    times = {16384: 80.0 + 30.0 * rank, 32768: 95.0, 65536: 100.0 - 15.0 * rank}
+    g, agreed = bench.agree_graph_count(pg, local, times)
+    out.put((rank, slowest, bench.job_rate(w, 1000, 3, slowest), g))
     pg.destroy_process_group()
 
 
@@ -43,12 +46,14 @@ def test_two_gloo_ranks():
         p.join(120)
         assert p.exitcode == 0
     got = sorted(q.get(timeout=10) for _ in range(world))
-    # both ranks see the slowest rank's time and the same job rate: 2 replicas x 1000 units x 3 steps / 15 s
-    assert got == [(0, 15.0, 400.0), (1, 15.0, 400.0)]
+    # both ranks see the slowest rank's time and the same job rate (2 replicas x 1000 units x
+    # 3 steps / 15 s), and agree on the subgraph count with the best slowest time (32768: 95)
+    assert got == [(0, 15.0, 400.0, 32768), (1, 15.0, 400.0, 32768)]
 
 
 def test_single_process_needs_no_group():
     sys.path.insert(0, ROOT)
     import bench
     assert bench.allreduce_max(None, 0, 7.5) == 7.5
+    assert bench.agree_graph_count(None, 0, {16384: 90.0, 65536: 80.0})[0] == 65536
     assert bench.job_rate(1, 1500, 2, 3.0) == 1000.0
