@@ -116,7 +116,7 @@ double secs(Clock::time_point a, Clock::time_point b) { return std::chrono::dura
 
 // Picks the next group for a worker (called with the lock held); empty if nothing
 // may start now.
-std::vector<Ticket*> take_group(cfg_server* s, Worker& w, uint64_t& need, bool& batched) {
+std::vector<Ticket*> take_group(cfg_server* s, uint64_t& need, bool& batched) {
     std::vector<Ticket*> g;
     if (s->queue.empty()) return g;
     Ticket* head = s->queue.front();
@@ -234,7 +234,7 @@ void worker_loop(cfg_server* s, Worker* w) {
             std::unique_lock<std::mutex> lock(s->mu);
             for (;;) {
                 if (s->stop) return;
-                g = take_group(s, *w, need, batched);
+                g = take_group(s, need, batched);
                 if (!g.empty()) break;
                 s->cv_work.wait(lock);
             }
