@@ -13,16 +13,6 @@
 
 using namespace cfg;
 
-namespace {
-
-// seed ^= wymix(seed ^ s0, s1) for seed 0 (include/wyhash/wyhash.h:118), on the host.
-uint64_t wy_seed0() {
-    const __uint128_t r = (__uint128_t)WY_S0 * WY_S1;
-    return (uint64_t)r ^ (uint64_t)(r >> 64);
-}
-
-}  // namespace
-
 struct cfg_ctx {
     int device = 0;
     cfg_params p{};
@@ -116,7 +106,7 @@ int run_partition(cfg_ctx* c, std::vector<uint32_t>& inst_h, std::vector<uint32_
         a.packed = c->d_packed; a.frag_off = c->d_frag_off; a.frag_len = c->d_frag_len;
         a.n_frags = c->n_frags; a.n_bases = c->n_bases;
         a.k = c->p.k; a.l = c->p.l; a.w = c->p.k - c->p.l;
-        a.gmask = G - 1; a.seed0 = wy_seed0(); a.seg = 2048;
+        a.gmask = G - 1; a.seed0 = wy_seed0_host(); a.seg = 2048;
         a.recs = c->flat.as<uint64_t>(); a.rec_cap = cap;
         a.rec_cursor = &c->misc.as<MiscWords>()->rec_cursor;
         a.hist = c->hist.as<unsigned long long>();
@@ -129,6 +119,8 @@ int run_partition(cfg_ctx* c, std::vector<uint32_t>& inst_h, std::vector<uint32_
         MiscWords m{};
         CK(cudaMemcpyAsync(&m, c->misc.p, sizeof(m), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
+        if (m.err & DERR_BAD_FRAG)
+            return fail(c, CFG_ERR_BAD_INPUT, "a fragment runs past n_bases or holds fewer than k+1 bases");
         if (m.rec_cursor <= cap && !(m.err & DERR_REC_OVERFLOW)) { c->n_records = m.rec_cursor; break; }
         cap = m.rec_cursor + 1024;
         if (attempt == 2) return fail(c, CFG_ERR_OOM, "record buffer kept overflowing");

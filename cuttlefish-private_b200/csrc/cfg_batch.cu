@@ -185,11 +185,6 @@ __global__ void __launch_bounds__(256) k_job_finalize(const uint32_t* __restrict
     J.lmtig = J.lm_used;
 }
 
-uint64_t wy_seed0() {
-    const __uint128_t r = (__uint128_t)WY_S0 * WY_S1;
-    return (uint64_t)r ^ (uint64_t)(r >> 64);
-}
-
 struct Shape { uint32_t cls, cluster, threads, per, grid; };
 
 }  // namespace
@@ -348,7 +343,7 @@ int enqueue(cfg_batch* b) {
     pa.packed = b->packed.as<uint64_t>(); pa.frag_off = b->frag_off.as<uint64_t>(); pa.frag_len = b->frag_len.as<uint32_t>();
     pa.n_frags = b->n_frags; pa.n_bases = b->n_bases;
     pa.k = b->p.k; pa.l = b->p.l; pa.w = b->p.k - b->p.l;
-    pa.gmask = b->G - 1; pa.seed0 = wy_seed0(); pa.seg = 2048;
+    pa.gmask = b->G - 1; pa.seed0 = wy_seed0_host(); pa.seg = 2048;
     pa.recs = b->flat.as<uint64_t>(); pa.rec_cap = b->rec_cap;
     pa.rec_cursor = &bw->rec_cursor; pa.hist = b->hist.as<unsigned long long>(); pa.err = &bw->err;
     pa.frag_gbase = b->frag_gbase.as<uint32_t>();

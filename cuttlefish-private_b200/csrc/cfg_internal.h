@@ -4,6 +4,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "cfg_device.cuh"
+
 namespace cfg {
 
 // A weak super k-mer packed in 64 bits: start in the packed stream (bits 0-31),
@@ -29,7 +31,15 @@ enum : uint32_t {
     DERR_DUMP_OVERFLOW = 32u,  // state dump buffer too small (recoverable)
     DERR_NO_ROOM = 64u,        // batch: a job's output regions or tables did not fit the arenas
     DERR_BAD_GRAPH = 128u,     // lm-tig ends that cannot meet (three at a vertex, or two on one side)
+    DERR_BAD_FRAG = 256u,      // a device-resident fragment runs past n_bases or is shorter than k+1 (skipped)
 };
+
+// wyhash v4.2's seed after its first mix for seed 0: seed ^= wymix(seed ^ s0, s1)
+// (include/wyhash/wyhash.h:118), evaluated on the host.  Every partition launch uses it.
+inline uint64_t wy_seed0_host() {
+    const unsigned __int128 r = (unsigned __int128)WY_S0 * WY_S1;
+    return (uint64_t)r ^ (uint64_t)(r >> 64);
+}
 
 struct PartitionArgs {
     const uint64_t* packed;

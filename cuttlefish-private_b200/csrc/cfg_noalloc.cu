@@ -1,15 +1,15 @@
 // cfg_noalloc.cu -- partition + bucket scatter for callers that cannot allocate.
 //
-// Some callers may not call cudaMalloc at all: code recording into a CUDA graph
-// that someone else's stream capture owns, plugins whose host framework hands out
-// every byte of device memory from its own pool, or real-time services that
-// forbid allocation on their request path.  cfg_partition_noalloc serves them:
-// it partitions one small job's packed input into weak super k-mers bucketed by
-// subgraph, like the first two kernels of cfg_run, but keeps its scratch (record
-// cursor, per-subgraph histogram and fill counters, the unbucketed records) in a
-// file-scope device array instead of allocated buffers, and writes only to the
-// output buffers the caller passes in.  It allocates nothing, host or device, and
-// never synchronises.
+// Some callers may not call cudaMalloc at all: plugins whose host framework hands
+// out every byte of device memory from its own pool, and services that forbid
+// allocation on their request path (cudaMalloc and cudaFree may synchronise the
+// whole device, stalling every other stream's work).  cfg_partition_noalloc serves
+// them: it partitions one small job's packed input into weak super k-mers bucketed
+// by subgraph, like the first two kernels of cfg_run, but keeps its scratch
+// (record cursor, error word, per-subgraph histogram and fill counters, the
+// unbucketed records) in a file-scope device array instead of allocated buffers,
+// and writes only to the output buffers the caller passes in.  It allocates
+// nothing, host or device, and never synchronises.
 //
 // Limits and sharing:
 //   - the scratch array is NOALLOC_SCRATCH_BYTES (8 MiB); every GPU that loads the
@@ -21,8 +21,11 @@
 //     other's output.  Serialise them, e.g. on one stream.  Each call clears the
 //     parts that must start at zero itself.
 //   - the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress, once per device, with that device current); make
-//     that first call before any stream capture begins.
+//     (cudaGetSymbolAddress, once per device, with that device current).
+//   - a failure found on the device (a fragment past n_bases or shorter than k+1,
+//     more records than the caller's buffer holds) makes the scatter write
+//     CFG_NOALLOC_FAILED to *d_n_records and nothing else; the records and bucket
+//     offsets of that call are then not valid.
 #include "cuttlefish_gpu.h"
 #include "cfg_device.cuh"
 #include "cfg_internal.h"
@@ -53,14 +56,19 @@ struct NoallocMisc {
     uint32_t err;
 };
 
-// Bucketed placement of the flat records; the record count is read on the device.
+// Bucketed placement of the flat records; the record count and the partition's error
+// word are read on the device.  A failed partition, or more records than either the
+// scratch array or the caller's buffer (cap) holds, scatters nothing and reports
+// CFG_NOALLOC_FAILED as the record count.
 __global__ void k_noalloc_scatter(const uint32_t* __restrict__ bucket_off, cfg_record* __restrict__ out,
-                                  unsigned long long* __restrict__ n_out) {
+                                  uint64_t cap, unsigned long long* __restrict__ n_out) {
     const NoallocMisc* misc = (const NoallocMisc*)(g_noalloc_scratch + OFF_MISC);
     const uint64_t* flat = (const uint64_t*)(g_noalloc_scratch + OFF_RECS);
     uint32_t* fill = (uint32_t*)(g_noalloc_scratch + OFF_FILL);
     const uint64_t n = misc->rec_cursor;
-    if (blockIdx.x == 0 && threadIdx.x == 0) *n_out = n;
+    const bool failed = misc->err != 0 || n > NOALLOC_MAX_RECORDS || n > cap;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *n_out = failed ? (unsigned long long)CFG_NOALLOC_FAILED : n;
+    if (failed) return;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t r = flat[i];
         const uint32_t g = rec_g(r);
@@ -116,10 +124,7 @@ extern "C" int cfg_partition_noalloc(int device, const cfg_params* p, const uint
         a.n_frags = n_frags; a.n_bases = n_bases;
         a.k = p->k; a.l = p->l; a.w = p->k - p->l;
         a.gmask = p->graph_count - 1;
-        {
-            const __uint128_t r = (__uint128_t)WY_S0 * WY_S1;
-            a.seed0 = (uint64_t)r ^ (uint64_t)(r >> 64);
-        }
+        a.seed0 = wy_seed0_host();
         a.seg = 2048;
         a.recs = (uint64_t*)(s + OFF_RECS); a.rec_cap = NOALLOC_MAX_RECORDS;
         a.rec_cursor = &((NoallocMisc*)(s + OFF_MISC))->rec_cursor;
@@ -128,7 +133,7 @@ extern "C" int cfg_partition_noalloc(int device, const cfg_params* p, const uint
         if (n_bases) launch_partition(a, st);
         launch_bucket_scan((const unsigned long long*)(s + OFF_HIST), p->graph_count, d_bucket_off,
                            (uint32_t*)(s + OFF_INST), (uint32_t*)(s + OFF_FILL), st);
-        k_noalloc_scatter<<<148 * 4, 256, 0, st>>>(d_bucket_off, d_records, (unsigned long long*)d_n_records);
+        k_noalloc_scatter<<<148 * 4, 256, 0, st>>>(d_bucket_off, d_records, records_cap, (unsigned long long*)d_n_records);
         if (cudaGetLastError() != cudaSuccess) { rc = CFG_ERR_CUDA; break; }
     } while (0);
     if (prev != device) cudaSetDevice(prev);

@@ -198,6 +198,12 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_partition(const Partit
             const uint64_t F0 = a.frag_off[f];
             if (F0 >= s1) break;
             const uint32_t FL = a.frag_len[f];
+            // a device-resident fragment table is not checked on the host: a fragment past
+            // the input or too short for a (k+1)-mer is skipped and reported
+            if (FL < a.k + 1 || F0 + FL > a.n_bases) {
+                if ((threadIdx.x & 31) == 0) atomicOr(a.err, DERR_BAD_FRAG);
+                continue;
+            }
             const uint32_t M = FL - a.k + 2;
             const uint32_t j0 = s0 > F0 ? (uint32_t)(s0 - F0) : 0;
             const uint64_t e = s1 - F0;

@@ -337,22 +337,27 @@ const char* cfg_server_last_error_string(cfg_server* s);
 void cfg_server_destroy(cfg_server* s);
 
 /* No counterpart in the reference.  For callers that must not allocate memory:
- * code recording into a CUDA graph whose stream capture someone else owns,
- * plugins whose host framework owns every byte of device memory, real-time
- * services that forbid allocation while serving.  Partitions one small job
- * (at most CFG_NOALLOC_MAX_BASES bases, already in device memory with 4 words
- * of padding after the packed bases) into weak super k-mers bucketed by
+ * plugins whose host framework owns every byte of device memory, and services
+ * that forbid allocation on their request path (cudaMalloc and cudaFree may
+ * synchronise the whole device).  Partitions one small job (at most
+ * CFG_NOALLOC_MAX_BASES bases, already in device memory with 4 words of padding
+ * after the packed bases; its fragment table back to back, each fragment of at
+ * least k+1 bases, summing to n_bases) into weak super k-mers bucketed by
  * subgraph -- the records cfg_dump_records returns after cfg_run -- without any
  * allocation and without synchronising: the work is queued on `stream` (a
  * cudaStream_t, NULL for the default stream).  Outputs are caller-owned device
  * buffers: d_records (records_cap >= n_bases entries; the first *d_n_records
  * are written, grouped by subgraph, order inside a subgraph unspecified),
  * d_bucket_off (graph_count + 1 offsets) and d_n_records (one word).
+ * A failure found on the device (a fragment past n_bases or shorter than k+1)
+ * writes CFG_NOALLOC_FAILED to *d_n_records and no records; read it after the
+ * stream's work is done.
  * Scratch lives in one fixed 8 MiB device array that every GPU loading the
  * library keeps until exit; all calls share it, so calls whose work overlaps on
  * one GPU race -- serialise them.  The first call on a device looks the array
- * up (once per device); make it before any stream capture.  Larger inputs get
+ * up (once per device, with that device current).  Larger inputs get
  * CFG_ERR_BAD_INPUT. */
+#define CFG_NOALLOC_FAILED 0xFFFFFFFFFFFFFFFFull
 #define CFG_NOALLOC_MAX_BASES 917472u
 int cfg_partition_noalloc(int device, const cfg_params* params, const uint64_t* d_packed, uint64_t n_bases,
                           const uint64_t* d_frag_off, const uint32_t* d_frag_len, uint64_t n_frags,

@@ -4,7 +4,10 @@
 # Needs nothing beyond the reference tree: FIXED_K turns off the one boost macro
 # that include/globals.hpp would use (ref_shim/ holds an empty stand-in for that
 # include), and the vendored fmt is used header-only.
-REF      ?= /root/reference
+# REF: the reference tree, given on the command line (make -f ref.mk REF=<dir>)
+ifndef REF
+$(error REF=<reference tree> is required)
+endif
 CXX      ?= g++
 OUT      := _ref
 KS       := 3 5 7 9 15 23 31 63

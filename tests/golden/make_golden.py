@@ -60,7 +60,7 @@ def pipeline(records, k, l, c, G):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CF_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference"))
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={ref}"], check=True)
     rng = random.Random(2024)
 
