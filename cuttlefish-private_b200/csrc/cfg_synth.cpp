@@ -10,7 +10,8 @@
 //             divergence; 150 bp reads from both strands, 0.5% substitutions (seed 2)
 //   ref500m   500 Mbp, 10% tandem repeats (units 2-50 bp, segments 100-10000 bp),
 //             5% interspersed copies of 20 families (300-6000 bp) at 2-15%
-//             divergence, split into 20 records                        (seed 3)
+//             divergence, split into 20 records                        (seed 3);
+//             cfs_ref_repeats builds the same shape at any length and seed
 //   genome_i  one of 1000 genomes: log-uniform 0.5-8 Mbp, GC in [0.3, 0.7],
 //             1% as copies of 500-5000 bp at 1%                        (seed 1000+i)
 //   genome_n  a genome of a given length and seed: i.i.d. ACGT, 1% as copies of
@@ -151,11 +152,14 @@ void cfs_reads(const char* g, uint64_t n, uint64_t n_reads, uint32_t L, double e
 }
 
 uint64_t cfs_ref500m_len() { return 500000000; }
-// out: 500 Mbp; cuts: 21 record offsets (0 .. 500e6)
-void cfs_ref500m(char* out, uint64_t* cuts) {
-    const uint64_t n = 500000000;
-    iid(out, n, 3, 0.5);
-    Rng r(31);
+
+// The large-reference shape at any length n: i.i.d. ACGT (seed), 10% of n as
+// non-overlapping tandem repeats (segments 100-10000 bp of a 2-50 bp unit), 5% as
+// interspersed copies of 20 families (300-6000 bp) at 2-15% divergence, cut into
+// n_rec records at n_rec - 1 sorted uniform points.  cuts: n_rec + 1 offsets.
+void cfs_ref_repeats(uint64_t n, uint64_t seed, uint32_t n_rec, char* out, uint64_t* cuts) {
+    iid(out, n, seed, 0.5);
+    Rng r(10 * seed + 1);
     std::set<std::pair<uint64_t, uint64_t>> placed;   // non-overlapping tandem segments
     uint64_t total = 0;
     std::vector<char> unit;
@@ -186,13 +190,16 @@ void cfs_ref500m(char* out, uint64_t* cuts) {
         std::memcpy(out + b, buf.data(), buf.size());
         total += buf.size();
     }
-    std::vector<uint64_t> c(19);
+    std::vector<uint64_t> c(n_rec - 1);
     for (auto& x : c) x = r.range(1, n - 1);
     std::sort(c.begin(), c.end());
     cuts[0] = 0;
-    for (int i = 0; i < 19; ++i) cuts[i + 1] = c[i];
-    cuts[20] = n;
+    for (uint32_t i = 0; i + 1 < n_rec; ++i) cuts[i + 1] = c[i];
+    cuts[n_rec] = n;
 }
+
+// out: 500 Mbp; cuts: 21 record offsets (0 .. 500e6)
+void cfs_ref500m(char* out, uint64_t* cuts) { cfs_ref_repeats(500000000, 3, 20, out, cuts); }
 
 uint64_t cfs_genome_len(uint32_t i) {
     Rng r(1000 + i);

@@ -334,6 +334,53 @@ class Compactor:
         return [(d.records[i].pos, d.records[i].len, d.records[i].flags, d.records[i].g) for i in range(d.n)]
 
 
+STATE_DTYPE = [("lo", "<u8"), ("hi", "<u8"), ("ef", "<u4"), ("g", "<u2"), ("status", "u1"), ("pad", "u1")]
+RECORD_DTYPE = [("pos", "<u4"), ("len", "u1"), ("flags", "u1"), ("g", "<u2")]
+LMTIG_DTYPE = [("u_lo", "<u8"), ("u_hi", "<u8"), ("v_lo", "<u8"), ("v_hi", "<u8"), ("label_off", "<u8"),
+               ("label_len", "<u4"), ("g", "<u2"), ("flags", "u1"), ("pad", "u1")]
+
+
+def states_array(cx):
+    """cfg_dump_states as a numpy array (g, hi, lo, ef, status), sorted by (g, hi, lo)."""
+    import numpy as np
+    d = StateDump()
+    _check(cx.lib, cx.ctx, cx.lib.cfg_dump_states(cx.ctx, ctypes.byref(d)), "cfg_dump_states")
+    raw = np.frombuffer(ctypes.string_at(d.states, d.n * ctypes.sizeof(State)), dtype=STATE_DTYPE) if d.n else \
+        np.zeros(0, STATE_DTYPE)
+    out = np.zeros(d.n, dtype=[("g", "<u4"), ("hi", "<u8"), ("lo", "<u8"), ("ef", "<u4"), ("status", "u1")])
+    for f in ("g", "hi", "lo", "ef", "status"):
+        out[f] = raw[f]
+    return sort_rows(out, ["g", "hi", "lo"])
+
+
+def records_array(cx):
+    """cfg_dump_records as a numpy array (g, len, flags, src = stream position), sorted."""
+    import numpy as np
+    d = RecordDump()
+    _check(cx.lib, cx.ctx, cx.lib.cfg_dump_records(cx.ctx, ctypes.byref(d)), "cfg_dump_records")
+    raw = np.frombuffer(ctypes.string_at(d.records, d.n * ctypes.sizeof(Record)), dtype=RECORD_DTYPE) if d.n else \
+        np.zeros(0, RECORD_DTYPE)
+    out = np.zeros(d.n, dtype=[("g", "<u4"), ("len", "u1"), ("flags", "u1"), ("src", "<u8")])
+    out["g"], out["len"], out["flags"], out["src"] = raw["g"], raw["len"], raw["flags"], raw["pos"]
+    return sort_rows(out, ["g", "src", "len", "flags"])
+
+
+def lmtig_array(res: Results, hash_spans):
+    """The lm-tigs of a fetched run as comparison keys (g, u, v, flags, label hash), sorted;
+    hash_spans(text_address, offsets, lengths) hashes the labels."""
+    import numpy as np
+    n = res.counts.n_lmtig
+    key = [("g", "<u4"), ("u_hi", "<u8"), ("u_lo", "<u8"), ("v_hi", "<u8"), ("v_lo", "<u8"), ("flags", "u1"),
+           ("label", "<u8")]
+    out = np.zeros(n, dtype=key)
+    if n:
+        raw = np.frombuffer(ctypes.string_at(res.lmtigs, n * ctypes.sizeof(Lmtig)), dtype=LMTIG_DTYPE)
+        for f in ("g", "u_hi", "u_lo", "v_hi", "v_lo", "flags"):
+            out[f] = raw[f]
+        out["label"] = hash_spans(res.lmtig_text, raw["label_off"], raw["label_len"])
+    return sort_rows(out, [f for f, _ in key])
+
+
 def unitig_multiset(fasta: bytes):
     """The sorted sequences of a unitig FASTA (record order and names carry no meaning)."""
     return sorted(line for line in fasta.split(b"\n") if line and not line.startswith(b">"))
@@ -589,3 +636,10 @@ def unpack_bases(packed: PackedInput, start: int, n: int) -> str:
     for i in range(start, start + n):
         out.append("ACGT"[(w[i >> 5] >> (62 - 2 * (i & 31))) & 3])
     return "".join(out)
+
+def sort_rows(a, order):
+    """a sorted by the fields in `order` (first = most significant), via lexsort."""
+    import numpy as np
+    if len(a) == 0:
+        return a
+    return a[np.lexsort(tuple(a[f] for f in reversed(order)))]

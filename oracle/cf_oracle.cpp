@@ -624,4 +624,19 @@ void orc_state_update(uint32_t* ef, uint8_t* status, int front, int back, int s0
 
 int orc_edge_at(uint32_t ef, int side, uint32_t f_th) { return edge_at(ef, (Side)side, f_th); }
 
+/* Comparison helper for large parity cases (not part of the restated algorithm):
+ * a 64-bit hash of each text span [off[i], off[i] + len[i]), length included. */
+void orc_hash_spans(const char* text, const uint64_t* off, const uint64_t* len, uint64_t n, uint64_t* out) {
+    for (uint64_t i = 0; i < n; ++i) {
+        uint64_t h = 0x9E3779B97F4A7C15ull ^ (len[i] * 0xC2B2AE3D27D4EB4Full);
+        const unsigned char* p = (const unsigned char*)text + off[i];
+        for (uint64_t j = 0; j < len[i]; ++j) {
+            h = (h ^ p[j]) * 0x100000001B3ull;
+            h ^= h >> 29;
+        }
+        h ^= h >> 33; h *= 0xFF51AFD7ED558CCDull; h ^= h >> 33;
+        out[i] = h;
+    }
+}
+
 }  // extern "C"

@@ -93,6 +93,8 @@ int orc_record_labels(orc_ctx* c, char* out, uint64_t cap);
 void orc_destroy(orc_ctx* c);
 
 /* Primitive pins. */
+/* Large-case comparison helper: a 64-bit hash of each span [off[i], off[i] + len[i]) of text. */
+void orc_hash_spans(const char* text, const uint64_t* off, const uint64_t* len, uint64_t n, uint64_t* out);
 uint64_t orc_wyhash8(uint64_t x);                  /* wyhash v4.2 of 8 bytes, seed 0, the reference's salt */
 uint64_t orc_lmer_hash(uint64_t lmer, uint32_t l); /* min(hash(lmer), hash(rc(lmer))) */
 /* Minimizer hash of every (k-1)-mer of the ACGT string s[0..n); writes n-k+2 values. */

@@ -59,6 +59,7 @@ def load():
         lib.orc_km1_min_hashes.argtypes = [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, U64P]
         lib.orc_state_update.argtypes = [U32P, U8P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         lib.orc_edge_at.argtypes = [ctypes.c_uint32, ctypes.c_int, ctypes.c_uint32]
+        lib.orc_hash_spans.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
         _lib = lib
     return _lib
 
@@ -127,6 +128,91 @@ class OracleRun:
         return fasta_multiset(self.fasta)
 
 
+def hash_spans(text_ptr, off, length):
+    """64-bit hashes of the spans [off[i], off[i] + length[i]) of the text at text_ptr (an
+    address or bytes); a comparison key for multisets too large for Python collections."""
+    import numpy as np
+    off = np.ascontiguousarray(off, dtype=np.uint64)
+    length = np.ascontiguousarray(length, dtype=np.uint64)
+    out = np.empty(len(off), dtype=np.uint64)
+    keep = text_ptr
+    if isinstance(text_ptr, (bytes, bytearray)):
+        keep = ctypes.create_string_buffer(bytes(text_ptr), len(text_ptr) + 1)
+        text_ptr = ctypes.addressof(keep)
+    if len(off):
+        load().orc_hash_spans(text_ptr, off.ctypes.data, length.ctypes.data, len(off), out.ctypes.data)
+    del keep
+    return out
+
+
+def fasta_seq_hashes(fasta):
+    """Sorted hashes of the sequence lines of FASTA text (bytes) '>..\nSEQ\n...'."""
+    import numpy as np
+    t = np.frombuffer(fasta, dtype=np.uint8)
+    nl = np.flatnonzero(t == 10)
+    starts = np.concatenate(([0], nl[:-1] + 1))
+    seq = t[starts] != ord(">")
+    off, ln = starts[seq], (nl - starts)[seq]
+    return np.sort(hash_spans(fasta, off, ln))
+
+
+class OracleArrays:
+    """One oracle run with its outputs as numpy arrays (no per-item Python objects):
+    records (g, len, flags, src) sorted, states (g, hi, lo, ef, status) sorted,
+    trivial-unitig sequence hashes sorted, lm-tigs (g, u_hi, u_lo, v_hi, v_lo, flags,
+    label hash) sorted.  src is the record's start in the concatenated input text."""
+
+    def __init__(self, data, offsets, n_rec, k, l, cutoff, graph_count, threads=8):
+        import numpy as np
+        lib = load()
+        p = Params(k, l, cutoff, graph_count)
+        ctx = lib.orc_create(ctypes.byref(p))
+        if not ctx:
+            raise ValueError("invalid oracle parameters")
+        try:
+            assert lib.orc_run(ctx, data, offsets, n_rec, threads) == 0
+            r = Result()
+            lib.orc_get(ctx, ctypes.byref(r))
+            self.counts = {n: getattr(r, n) for n, _ in Result._fields_[:9]}
+            nr, nv, nl = r.n_records, r.n_vertices, r.n_lmtig
+
+            def arr(ptr, n, dt):
+                return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dt, copy=True) if n else np.zeros(0, dt)
+            rec = np.zeros(nr, dtype=[("g", "<u4"), ("len", "u1"), ("flags", "u1"), ("src", "<u8")])
+            rec["g"], rec["len"] = arr(r.rec_g, nr, np.uint32), arr(r.rec_len, nr, np.uint8)
+            rec["flags"], rec["src"] = arr(r.rec_flags, nr, np.uint8), arr(r.rec_src, nr, np.uint64)
+            self.records = sort_rows(rec, ["g", "src", "len", "flags"])
+            st = np.zeros(nv, dtype=[("g", "<u4"), ("hi", "<u8"), ("lo", "<u8"), ("ef", "<u4"), ("status", "u1")])
+            key = arr(r.vtx_key, 2 * nv, np.uint64)
+            st["g"], st["hi"], st["lo"] = arr(r.vtx_g, nv, np.uint32), key[0::2], key[1::2]
+            st["ef"], st["status"] = arr(r.vtx_ef, nv, np.uint32), arr(r.vtx_status, nv, np.uint8)
+            self.states = sort_rows(st, ["g", "hi", "lo"])
+            self.fasta = ctypes.string_at(r.fasta, r.fasta_bytes) if r.fasta_bytes else b""
+            self.trivial = fasta_seq_hashes(self.fasta)
+            lm = np.zeros(nl, dtype=LMTIG_KEY)
+            if nl:
+                off = arr(r.lm_off, nl + 1, np.uint64)
+                u, v = arr(r.lm_u, 2 * nl, np.uint64), arr(r.lm_v, 2 * nl, np.uint64)
+                lm["g"], lm["flags"] = arr(r.lm_g, nl, np.uint32), arr(r.lm_flags, nl, np.uint8)
+                lm["u_hi"], lm["u_lo"], lm["v_hi"], lm["v_lo"] = u[0::2], u[1::2], v[0::2], v[1::2]
+                lm["label"] = hash_spans(r.lm_text, off[:-1], np.diff(off))
+                self.lm_text = ctypes.string_at(r.lm_text, int(off[-1]))
+                self.lm_off = off
+            else:
+                self.lm_text, self.lm_off = b"", np.zeros(1, np.uint64)
+            self.lm_u, self.lm_v = (u, v) if nl else (np.zeros(0, np.uint64), np.zeros(0, np.uint64))
+            self.lm_flags = lm["flags"].copy()
+            self.lm_g = lm["g"].copy()
+            self.lmtigs = sort_rows(lm, list(lm.dtype.names))
+        finally:
+            lib.orc_destroy(ctx)
+
+
+# an lm-tig as a comparison key: subgraph, discontinuity vertices (k-mer words), flags, label hash
+LMTIG_KEY = [("g", "<u4"), ("u_hi", "<u8"), ("u_lo", "<u8"), ("v_hi", "<u8"), ("v_lo", "<u8"), ("flags", "u1"),
+             ("label", "<u8")]
+
+
 def timed_run(data, offsets, n_rec, k, l, cutoff, graph_count=16384, threads=1):
     """Runs the oracle once and returns its wall time in seconds (no Python-side conversion)."""
     import time
@@ -173,3 +259,10 @@ def state_update(ef, status, front, back, s0, s1):
 
 def edge_at(ef, side, fth):
     return load().orc_edge_at(ef, side, fth)
+
+def sort_rows(a, order):
+    """a sorted by the fields in `order` (first = most significant), via lexsort."""
+    import numpy as np
+    if len(a) == 0:
+        return a
+    return a[np.lexsort(tuple(a[f] for f in reversed(order)))]

@@ -1,0 +1,167 @@
+"""GPU parity on the reference's own fixtures and on the benchmark workloads' shapes.
+
+1. Every case of tests/golden/pipeline.json -- outputs of the reference's own classes
+   (oracle/ref_driver), including its data/ fixtures refs1.fa, refs2.fa, cycles.fa,
+   rob-palindrome.fa and reads.fq at k = 3 and 5 -- run through the CUDA path and
+   compared with the reference's outputs directly (records, vertex states, trivial
+   unitigs, lm-tigs).
+2. The benchmark configurations, bit-exact against the CPU oracle on the same seeded
+   input: config 1 in full (one 5 Mbp record with repeats and palindromes, k = 31,
+   16384 subgraphs); config 2 on its first million reads (k = 31, cutoff 2, 16384
+   subgraphs), whose final unitigs at 65536 subgraphs must equal the host collation of
+   the oracle's own lm-tigs; config 3's shape at 30 Mbp (k = 63, tandem units of 2-50 bp
+   and interspersed repeat families, 20 records).
+
+Large cases compare numpy arrays: records by (subgraph, stream position, length,
+flags), states by (subgraph, k-mer words, edge frequencies, status), unitig and
+lm-tig labels by 64-bit hashes of their text.  All inputs are pure ACGT, so a
+record's position in the packed stream equals its position in the input text.
+"""
+import collections
+import ctypes
+import json
+import os
+
+import numpy as np
+import pytest
+
+import cfgpu
+import orc
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SYNTH_LIB = os.path.join(os.path.dirname(HERE), "cuttlefish-private_b200", "lib", "libcfsynth.so")
+
+
+def synth():
+    lib = ctypes.CDLL(SYNTH_LIB)
+    for n in ("cfs_ref5m_len", "cfs_reads30x_genome_len"):
+        getattr(lib, n).restype = ctypes.c_uint64
+    lib.cfs_reads.argtypes = [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_double,
+                              ctypes.c_uint64, ctypes.c_char_p]
+    lib.cfs_ref_repeats.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_char_p,
+                                    ctypes.c_void_p]
+    return lib
+
+
+def config1():
+    lib = synth()
+    n = lib.cfs_ref5m_len()
+    g = ctypes.create_string_buffer(n)
+    lib.cfs_ref5m(g)
+    return g.raw[:n], (ctypes.c_uint64 * 2)(0, n), 1
+
+
+def config2_reads(n_reads):
+    """The first n_reads reads of the read-set workload (they do not depend on how many follow)."""
+    lib = synth()
+    n = lib.cfs_reads30x_genome_len()
+    g = ctypes.create_string_buffer(n)
+    lib.cfs_reads30x_genome(g)
+    out = ctypes.create_string_buffer(n_reads * 150)
+    lib.cfs_reads(g, n, n_reads, 150, 0.005, 2, out)
+    offs = (ctypes.c_uint64 * (n_reads + 1))(*range(0, (n_reads + 1) * 150, 150))
+    return out.raw[:n_reads * 150], offs, n_reads
+
+
+def config3_shape(n, seed, n_rec):
+    lib = synth()
+    g = ctypes.create_string_buffer(n)
+    cuts = (ctypes.c_uint64 * (n_rec + 1))()
+    lib.cfs_ref_repeats(n, seed, n_rec, g, cuts)
+    return g.raw[:n], cuts, n_rec
+
+
+def gpu_arrays(data_offsets, k, l, c, G, load_pct=0, flags=cfgpu.CFG_FLAG_DUMP_STATES | cfgpu.CFG_FLAG_DUMP_RECORDS):
+    packed = cfgpu.PackedInput(None, k, data_offsets=data_offsets)
+    assert packed.n_bases == len(data_offsets[0]), "pure ACGT input: every base is packed"
+    out = {}
+    with cfgpu.Compactor(k, l, c, G, flags=flags, table_load_pct=load_pct) as cx:
+        cx.submit(packed)
+        cx.run()
+        res = cx.fetch_raw()
+        out["counts"] = res.counts
+        if flags:
+            out["records"] = cfgpu.records_array(cx)
+            out["states"] = cfgpu.states_array(cx)
+            out["trivial"] = orc.fasta_seq_hashes(ctypes.string_at(res.fasta, res.counts.fasta_bytes))
+            out["lmtigs"] = cfgpu.lmtig_array(res, orc.hash_spans)
+        fa, n_units = cx.unitigs()
+        out["unitigs"] = orc.fasta_seq_hashes(fa)
+        out["n_units"] = n_units
+    packed.close()
+    return out
+
+
+def assert_equal_to_oracle(got, o):
+    n = got["counts"]
+    for name in ("n_records", "n_instances", "n_vertices", "n_isolated", "n_phantom", "n_trivial", "n_icc", "n_lmtig"):
+        assert getattr(n, name) == o.counts[name], name
+    assert np.array_equal(got["records"], o.records), "weak super k-mer records differ"
+    assert np.array_equal(got["states"], o.states), "vertex states differ"
+    assert np.array_equal(got["trivial"], o.trivial), "trivial maximal unitigs differ"
+    assert np.array_equal(got["lmtigs"], o.lmtigs), "lm-tigs differ"
+
+
+def oracle_final_unitigs(o, k):
+    """The oracle's trivial unitigs plus its lm-tigs joined by the host collator: the final
+    maximal unitigs, as sorted sequence hashes."""
+    nl = len(o.lm_g)
+    arr = np.zeros(max(nl, 1), dtype=cfgpu.LMTIG_DTYPE)
+    if nl:
+        arr["u_hi"][:nl], arr["u_lo"][:nl] = o.lm_u[0::2], o.lm_u[1::2]
+        arr["v_hi"][:nl], arr["v_lo"][:nl] = o.lm_v[0::2], o.lm_v[1::2]
+        arr["label_off"][:nl], arr["label_len"][:nl] = o.lm_off[:-1], np.diff(o.lm_off)
+        arr["g"][:nl], arr["flags"][:nl] = o.lm_g, o.lm_flags
+    text = ctypes.create_string_buffer(o.lm_text + b"\0")
+    joined, _, _ = cfgpu.collate(k, arr.ctypes.data, nl, text)
+    return np.sort(np.concatenate([orc.fasta_seq_hashes(o.fasta), orc.fasta_seq_hashes(joined)]))
+
+
+PIPELINE = json.load(open(os.path.join(HERE, "golden", "pipeline.json")))
+
+
+@pytest.mark.parametrize("case", PIPELINE, ids=lambda c: f"{c['name']}-k{c['k']}-G{c['graph_count']}")
+def test_reference_fixtures_on_gpu(case):
+    """The CUDA path against the reference's own classes on its data/ fixtures and seeded cases."""
+    from test_gpu_parity import gpu_run
+    k = case["k"]
+    counts, rec_ms, st, fa, lm = gpu_run(case["input"], k, case["l"], case["cutoff"], case["graph_count"])
+    assert rec_ms == collections.Counter((g, ln, fl, lab) for g, ln, fl, lab in case["records"])
+    assert st == {(g, lab): (ef, s) for g, lab, ef, s in case["states"]}
+    assert fa == orc.fasta_multiset(case["fasta"].encode())
+    assert lm == collections.Counter(tuple(x) for x in case["lmtigs"])
+
+
+def test_config1_ref5m_full():
+    """Config 1 in full: one 5 Mbp record, k = 31, cutoff 1, 16384 subgraphs."""
+    d = config1()
+    o = orc.OracleArrays(*d, 31, 20, 1, 16384)
+    got = gpu_arrays(d, 31, 20, 1, 16384, load_pct=100)
+    assert_equal_to_oracle(got, o)
+    assert np.array_equal(got["unitigs"], oracle_final_unitigs(o, 31))
+
+
+def test_config2_reads_1m():
+    """Config 2 on its first million reads: k = 31, cutoff 2, 16384 subgraphs, bit-exact;
+    final unitigs at 65536 subgraphs equal the collation of the oracle's lm-tigs."""
+    d = config2_reads(1_000_000)
+    o = orc.OracleArrays(*d, 31, 20, 2, 16384)
+    got = gpu_arrays(d, 31, 20, 2, 16384, load_pct=15)
+    assert_equal_to_oracle(got, o)
+    want = oracle_final_unitigs(o, 31)
+    assert np.array_equal(got["unitigs"], want)
+    at64k = gpu_arrays(d, 31, 20, 2, 65536, load_pct=15, flags=0)
+    assert np.array_equal(at64k["unitigs"], want)
+
+
+def test_config3_k63_30mbp():
+    """Config 3's shape at 30 Mbp: k = 63, 10 % tandem repeats of 2-50 bp units (the skew
+    case: long same-subgraph runs, arena and cluster tables), 5 % interspersed families,
+    20 records; 16384 subgraphs, bit-exact, and final unitigs."""
+    d = config3_shape(30_000_000, 3, 20)
+    o = orc.OracleArrays(*d, 63, 20, 1, 16384)
+    got = gpu_arrays(d, 63, 20, 1, 16384, load_pct=100)
+    assert_equal_to_oracle(got, o)
+    assert np.array_equal(got["unitigs"], oracle_final_unitigs(o, 63))
