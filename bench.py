@@ -478,6 +478,139 @@ def measured_hbm_peak():
         return 6650.0, "fallback"
 
 
+def bench_workload(args, name, pg, rank, local, world, with_cpu):
+    """One workload through the plain path, to its final maximal unitigs: the subgraph
+    count tuned (final unitigs are the same at every count, which the tuner checks),
+    `value` with the input resident in HBM (device time of cfg_run + cfg_unitigs), `e2e`
+    through the C ABI from pinned host buffers, the subgraph kernels' roofline and,
+    with_cpu, the CPU baseline on a bounded sample."""
+    import cfgpu
+    k, l, cutoff, load_pct, desc = WORKLOADS[name]
+    if args.table_load_pct:
+        load_pct = args.table_load_pct
+    metric = "input bases/s to bit-exact maximal unitigs (the <o>.fa content), 1 B200"
+    config = {"workload": name, "description": desc, "k": k, "l": l, "cutoff": cutoff, "graph_count": 16384,
+              "table_load_pct": load_pct,
+              "l2_flush": "inputs larger than L2 (packed input and tables exceed 126 MB)" if name != "ref5m" else
+              "input (1.25 MB packed) smaller than L2: launch- and latency-bound, no flush"}
+    data, offs, n_rec = make_workload(name, args.reads)
+    packed = cfgpu.PackedInput(None, k, pinned=True, data_offsets=(data, offs, n_rec))
+    # subgraph count: the fastest to final unitigs (they are the same for every count;
+    # the tuner checks that they are byte-identical across the candidates)
+    dev = local if world > 1 else 0
+    if args.graph_count:
+        gc, g_times, g_same = args.graph_count, None, None
+    else:
+        progress(f"{name}: tuning the subgraph count")
+        gc, g_times, g_same = cfgpu.tune_graph_count(packed, k, l, cutoff, load_pct, device=dev)
+        if not g_same:
+            raise RuntimeError("final unitigs differ between subgraph counts")
+        gc, g_times = agree_graph_count(pg, local, g_times)
+    config["graph_count"] = gc
+    if g_times:
+        config["graph_count_tuning_ms"] = {str(g): round(t, 2) for g, t in g_times.items()}
+        config["unitigs_identical_across_graph_counts"] = g_same
+    cx = cfgpu.Compactor(k, l, cutoff, gc, device=dev, table_load_pct=load_pct)
+
+    # e2e: H2D + run + device collation + D2H of the final unitigs, through the C ABI,
+    # host buffers pinned
+    def e2e_step():
+        cx.submit(packed)
+        cx.run()
+        return cx.unitigs_raw()
+
+    progress(f"{name}: input ready ({packed.p.n_bases} bases); end-to-end steps")
+    for _ in range(args.warmup):
+        e2e_step()
+    barrier(pg)
+    e2e_times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        _, fin_bytes, n_units, _ = e2e_step()
+        e2e_times.append(time.perf_counter() - t0)
+    counts = cx.counts()
+    barrier(pg)
+    h2d = packed.p.n_bases // 4 + 12 * packed.p.n_frags
+    d2h = fin_bytes + 96
+
+    # value: input resident in HBM, device-timed
+    cx.submit(packed)
+    for _ in range(args.warmup):
+        cx.run()
+    barrier(pg)
+    run_ms, sub_ms, part_ms, scat_ms, col_ms = [], [], [], [], []
+    launches = 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            cx.run()
+            t = cx.timings()
+            _, _, _, ums = cx.unitigs_raw()
+            part_ms.append(t[0]); scat_ms.append(t[1]); sub_ms.append(t[2]); run_ms.append(t[3] + ums)
+            col_ms.append(ums)
+            launches += cx.counts().n_launches
+    barrier(pg)
+    counts = cx.counts()
+    phase_cycles = cx.phase_cycles()
+    total_ms = sum(run_ms)
+    total_ms_max = allreduce_max(pg, local, total_ms)
+    e2e_s_max = allreduce_max(pg, local, sum(e2e_times))
+    bases = counts.n_bases
+    value = job_rate(world, bases, args.steps, total_ms_max / 1e3)
+    e2e_value = job_rate(world, bases, args.steps, e2e_s_max)
+
+    # roofline of the dominant kernel (subgraph construct + walk): algorithmic bytes
+    W = 1 if k <= 31 else 2
+    R = 4 + 8 * ((2 * (k - 1) - l + 2 + 31) // 32)        # reference record bytes
+    B_slot = 8 * ((k + 31) // 32) + 8
+    U_out = counts.fasta_bytes + counts.lmtig_bytes + 48 * counts.n_lmtig
+    sub_bytes = counts.n_records * R + 2 * counts.n_vertices * B_slot + U_out
+    sub_avg = statistics.mean(sub_ms) / 1e3
+    peak, peak_kind = measured_hbm_peak()
+    achieved = sub_bytes / sub_avg / 1e9
+    job_bytes = bases / 4 + 2 * counts.n_records * R + 2 * counts.n_vertices * B_slot + U_out
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", f"traffic_{name}.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get("subgraph_bytes_per_run")
+        except ValueError:
+            traffic = None
+
+    progress(f"{name}: device steps {[round(x, 1) for x in run_ms]} ms; CPU baseline next")
+    cpu = None
+    if with_cpu:
+        threads = os.cpu_count() or 1
+        v, dt, label = cpu_reference(args, name, data, offs, n_rec, threads)
+        cpu = {"value": v, "unit": "bases/s", "cores": threads, "kind": "port", "sample": label, "seconds": round(dt, 2)}
+    cx.close()
+    packed.close()
+    del data
+    return {
+        "metric": metric, "value": value, "unit": "bases/s", "ms_per_step": total_ms_max / args.steps,
+        "config": dict(config, parallelism=f"replicas{world}"),
+        "e2e": {"value": e2e_value, "unit": "bases/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": 1e3 * e2e_s_max / args.steps},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": "k_subgraph (construct + walk, all launches of a run)",
+                     "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "algorithmic_bytes": sub_bytes, "kernel_ms": sub_avg * 1e3},
+        "job_roofline": {"algorithmic_bytes": job_bytes, "achieved_gbs": job_bytes / (total_ms / args.steps / 1e3) / 1e9,
+                         "frac": job_bytes / (total_ms / args.steps / 1e3) / 1e9 / peak},
+        "phases_ms": {"partition": statistics.mean(part_ms), "scatter": statistics.mean(scat_ms),
+                      "subgraphs": statistics.mean(sub_ms), "collate": statistics.mean(col_ms),
+                      "run": statistics.mean(run_ms)},
+        "unitigs": {"n": n_units, "fasta_bytes": fin_bytes,
+                    "distinct_kmers": (fin_bytes - 4 * n_units) - n_units * (k - 1)},
+        "counts": {n: getattr(counts, n) for n, _ in cfgpu.Counts._fields_},
+        "subgraph_phase_cycles": dict(zip(["build", "terminations", "paths", "cycles", "tail"], phase_cycles)),
+        "distinct_kmers_per_s": ((fin_bytes - 4 * n_units) - n_units * (k - 1)) / (total_ms_max / args.steps / 1e3),
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+
+
+
 def dist_setup(n_gpus):
     """One process per GPU under torchrun: (rank, world, local rank, process group or None).
     The backend is NCCL; CFG_BENCH_BACKEND=gloo runs the same plumbing on CPU (tests)."""
@@ -574,7 +707,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--table-load-pct", type=int, default=0, help="override the workload's table sizing factor")
     ap.add_argument("--graph-count", type=int, default=0,
-                    help="subgraph count of the plain run (0: the fastest of 16384/32768/65536 to final unitigs)")
+                    help="subgraph count of the plain run (0: the fastest of 16384 ... 262144 to final unitigs)")
+    ap.add_argument("--extra-workloads", default="ref5m,ref500m",
+                    help="further plain-path workloads reported under \"workloads\" (comma list; empty: none)")
     ap.add_argument("--batch-genomes", type=int, default=1000, help="genomes of the batched comparison (0: skip it)")
     ap.add_argument("--batch-steps", type=int, default=2)
     ap.add_argument("--serve-jobs", type=int, default=16, help="jobs of the serving comparison (0: skip it)")
@@ -624,100 +759,15 @@ def main():
                           "e2e": {"value": v, "unit": "bases/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
 
-    import cfgpu
-    data, offs, n_rec = make_workload(name, args.reads)
-    packed = cfgpu.PackedInput(None, k, pinned=True, data_offsets=(data, offs, n_rec))
-    # subgraph count: the fastest to final unitigs (they are the same for every count;
-    # the tuner checks that they are byte-identical across the candidates)
-    dev = local if world > 1 else 0
-    if args.graph_count:
-        gc, g_times, g_same = args.graph_count, None, None
-    else:
-        progress(f"{name}: tuning the subgraph count")
-        gc, g_times, g_same = cfgpu.tune_graph_count(packed, k, l, cutoff, load_pct, device=dev)
-        if not g_same:
-            raise RuntimeError("final unitigs differ between subgraph counts")
-        gc, g_times = agree_graph_count(pg, local, g_times)
-    config["graph_count"] = gc
-    if g_times:
-        config["graph_count_tuning_ms"] = {str(g): round(t, 2) for g, t in g_times.items()}
-        config["unitigs_identical_across_graph_counts"] = g_same
-    cx = cfgpu.Compactor(k, l, cutoff, gc, device=dev, table_load_pct=load_pct)
-
-    # e2e: H2D + run + device collation + D2H of the final unitigs, through the C ABI,
-    # host buffers pinned
-    def e2e_step():
-        cx.submit(packed)
-        cx.run()
-        return cx.unitigs_raw()
-
-    progress(f"{name}: input ready ({packed.p.n_bases} bases); end-to-end steps")
-    for _ in range(args.warmup):
-        e2e_step()
-    barrier(pg)
-    e2e_times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        _, fin_bytes, n_units, _ = e2e_step()
-        e2e_times.append(time.perf_counter() - t0)
-    counts = cx.counts()
-    barrier(pg)
-    h2d = packed.p.n_bases // 4 + 12 * packed.p.n_frags
-    d2h = fin_bytes + 96
-
-    # value: input resident in HBM, device-timed
-    cx.submit(packed)
-    for _ in range(args.warmup):
-        cx.run()
-    barrier(pg)
-    run_ms, sub_ms, part_ms, scat_ms, col_ms = [], [], [], [], []
-    launches = 0
-    with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            cx.run()
-            t = cx.timings()
-            _, _, _, ums = cx.unitigs_raw()
-            part_ms.append(t[0]); scat_ms.append(t[1]); sub_ms.append(t[2]); run_ms.append(t[3] + ums)
-            col_ms.append(ums)
-            launches += cx.counts().n_launches
-    barrier(pg)
-    counts = cx.counts()
-    phase_cycles = cx.phase_cycles()
-    total_ms = sum(run_ms)
-    total_ms_max = allreduce_max(pg, local, total_ms)
-    e2e_s_max = allreduce_max(pg, local, sum(e2e_times))
-    bases = counts.n_bases
-    value = job_rate(world, bases, args.steps, total_ms_max / 1e3)
-    e2e_value = job_rate(world, bases, args.steps, e2e_s_max)
-
-    # roofline of the dominant kernel (subgraph construct + walk): algorithmic bytes
-    W = 1 if k <= 31 else 2
-    R = 4 + 8 * ((2 * (k - 1) - l + 2 + 31) // 32)        # reference record bytes
-    B_slot = 8 * ((k + 31) // 32) + 8
-    U_out = counts.fasta_bytes + counts.lmtig_bytes + 48 * counts.n_lmtig
-    sub_bytes = counts.n_records * R + 2 * counts.n_vertices * B_slot + U_out
-    sub_avg = statistics.mean(sub_ms) / 1e3
-    peak, peak_kind = measured_hbm_peak()
-    achieved = sub_bytes / sub_avg / 1e9
-    job_bytes = bases / 4 + 2 * counts.n_records * R + 2 * counts.n_vertices * B_slot + U_out
-    traffic = None
-    tf = os.path.join(ROOT, "profiles", f"traffic_{name}.json")
-    if os.path.exists(tf):
+    rec = bench_workload(args, name, pg, rank, local, world, rank == 0 and not args.no_cpu_baseline)
+    extra = {}
+    for other in [w for w in args.extra_workloads.split(",") if w and w != name]:
         try:
-            traffic = json.load(open(tf)).get("subgraph_bytes_per_run")
-        except ValueError:
-            traffic = None
+            extra[other] = bench_workload(args, other, pg, rank, local, world, rank == 0 and not args.no_cpu_baseline)
+        except Exception as ex:   # the headline line is still printed
+            extra[other] = {"error": f"{type(ex).__name__}: {ex}"}
 
-    progress(f"{name}: device steps {[round(x, 1) for x in run_ms]} ms; CPU baseline next")
-    cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        v, dt, label = cpu_reference(args, name, data, offs, n_rec, threads)
-        cpu = {"value": v, "unit": "bases/s", "cores": threads, "kind": "port", "sample": label, "seconds": round(dt, 2)}
-    cx.close()
-    packed.close()
-    del data
-
+    peak, _ = measured_hbm_peak()
     batched = None
     if args.batch_genomes > 0:
         try:
@@ -733,32 +783,14 @@ def main():
 
     if rank == 0:
         line = {
-            "metric": metric, "value": value, "unit": "bases/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
+            "metric": rec["metric"], "value": rec["value"], "unit": "bases/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": rec["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-            "config": dict(config, parallelism=f"replicas{world}"),
-            "e2e": {"value": e2e_value, "unit": "bases/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "ms_per_step": 1e3 * e2e_s_max / args.steps},
-            "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "kernel": "k_subgraph (construct + walk, all launches of a run)",
-                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "algorithmic_bytes": sub_bytes, "kernel_ms": sub_avg * 1e3},
-            "job_roofline": {"algorithmic_bytes": job_bytes, "achieved_gbs": job_bytes / (total_ms / args.steps / 1e3) / 1e9,
-                             "frac": job_bytes / (total_ms / args.steps / 1e3) / 1e9 / peak},
-            "phases_ms": {"partition": statistics.mean(part_ms), "scatter": statistics.mean(scat_ms),
-                          "subgraphs": statistics.mean(sub_ms), "collate": statistics.mean(col_ms),
-                          "run": statistics.mean(run_ms)},
-            "unitigs": {"n": n_units, "fasta_bytes": fin_bytes,
-                        "distinct_kmers": (fin_bytes - 4 * n_units) - n_units * (k - 1)},
-            "counts": {n: getattr(counts, n) for n, _ in cfgpu.Counts._fields_},
-            "subgraph_phase_cycles": dict(zip(["build", "terminations", "paths", "cycles", "tail"], phase_cycles)),
-            "distinct_kmers_per_s": ((fin_bytes - 4 * n_units) - n_units * (k - 1)) / (total_ms_max / args.steps / 1e3),
-            "clocks": clk.summary(),
-            "cpu_baseline": cpu,
-            "batched_vs_plain": batched,
-            "serving": serving,
         }
+        line.update({x: v for x, v in rec.items() if x not in ("metric", "value", "ms_per_step")})
+        line["batched_vs_plain"] = batched
+        line["serving"] = serving
+        line["workloads"] = extra
         print(json.dumps(line))
     if pg is not None:
         pg.destroy_process_group()

@@ -33,7 +33,7 @@ struct cfg_ctx {
     bool have_input = false, have_run = false;
 
     // partition
-    DevBuf flat, hist, misc, bucket_off, inst, fill, recs;
+    DevBuf flat, hist, misc, bucket_off, inst, fill, recs, scan_part;
     // plan
     DevBuf list, tab_off, tab_cap, arena;
     // outputs
@@ -129,8 +129,14 @@ int run_partition(cfg_ctx* c, std::vector<uint32_t>& inst_h, std::vector<uint32_
     if (!c->bucket_off.ensure(4ull * (G + 1)) || !c->inst.ensure(4ull * G) || !c->fill.ensure(4ull * G))
         return fail(c, CFG_ERR_OOM, "bucket arrays");
     if (!c->recs.ensure(8 * std::max<uint64_t>(c->n_records, 1))) return fail(c, CFG_ERR_OOM, "bucketed records");
-    launch_bucket_scan(c->hist.as<unsigned long long>(), G, c->bucket_off.as<uint32_t>(), c->inst.as<uint32_t>(),
-                       c->fill.as<uint32_t>(), c->stream);
+    if (G <= 65536) {
+        launch_bucket_scan(c->hist.as<unsigned long long>(), G, c->bucket_off.as<uint32_t>(), c->inst.as<uint32_t>(),
+                           c->fill.as<uint32_t>(), c->stream);
+    } else {   // multi-block scan of the larger histograms
+        if (!c->scan_part.ensure(4ull * (G / 8192 + 1))) return fail(c, CFG_ERR_OOM, "scan partials");
+        launch_bucket_scan_large(c->hist.as<unsigned long long>(), G, c->bucket_off.as<uint32_t>(), c->inst.as<uint32_t>(),
+                                 c->fill.as<uint32_t>(), c->scan_part.as<uint32_t>(), c->stream);
+    }
     ScatterArgs s{};
     s.flat = c->flat.as<uint64_t>(); s.n = c->n_records;
     s.bucket_off = c->bucket_off.as<uint32_t>(); s.bucket_fill = c->fill.as<uint32_t>();
@@ -377,7 +383,7 @@ int cfg_create(int device, const cfg_params* params, cfg_ctx** out) {
     if (p.k < 3 || p.k > 63 || (p.k % 2) == 0) return CFG_ERR_BAD_INPUT;
     if (p.l < 1 || p.l > 32 || p.l > p.k - 1) return CFG_ERR_BAD_INPUT;
     if (p.cutoff < 1 || p.cutoff > 15) return CFG_ERR_BAD_INPUT;
-    if (p.graph_count == 0 || p.graph_count > 65536 || (p.graph_count & (p.graph_count - 1))) return CFG_ERR_BAD_INPUT;
+    if (p.graph_count == 0 || p.graph_count > MAX_GRAPH_COUNT || (p.graph_count & (p.graph_count - 1))) return CFG_ERR_BAD_INPUT;
     int n_dev = 0;
     if (cudaGetDeviceCount(&n_dev) != cudaSuccess || device < 0 || device >= n_dev) { cudaGetLastError(); return CFG_ERR_CUDA; }
     if (cudaSetDevice(device) != cudaSuccess) return CFG_ERR_CUDA;
@@ -686,7 +692,7 @@ void cfg_destroy(cfg_ctx* c) {
     c->parse.release();
     c->ub.release();
     c->h_unitigs.release();
-    DevBuf* bufs[] = {&c->packed, &c->frag_off, &c->frag_len, &c->text, &c->flat, &c->hist, &c->misc, &c->bucket_off, &c->inst,
+    DevBuf* bufs[] = {&c->packed, &c->frag_off, &c->frag_len, &c->text, &c->flat, &c->hist, &c->misc, &c->bucket_off, &c->inst, &c->scan_part,
                       &c->fill, &c->recs, &c->list, &c->tab_off, &c->tab_cap, &c->arena, &c->fasta, &c->lm_text,
                       &c->lm, &c->dump, &c->retry, &c->counters, &c->stripe_cur, &c->stripe_base,
                       &c->ut_lmbase, &c->cyc_lm, &c->cyc_text, &c->cyc_cnt};

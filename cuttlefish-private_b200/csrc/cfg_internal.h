@@ -9,17 +9,19 @@
 namespace cfg {
 
 // A weak super k-mer packed in 64 bits: start in the packed stream (bits 0-31),
-// length in bases (32-39), l_disc (40), r_disc (41), subgraph (48-63).  It is the
-// reference's Super_Kmer_Attributes<false> (include/Super_Kmer_Attributes.hpp:25-61)
-// with the label replaced by its position in the resident 2-bit input.
+// length in bases (32-39), l_disc (40), r_disc (41), subgraph (42-63, up to 2^22).
+// It is the reference's Super_Kmer_Attributes<false>
+// (include/Super_Kmer_Attributes.hpp:25-61) with the label replaced by its position in
+// the resident 2-bit input.
+constexpr uint32_t MAX_GRAPH_COUNT = 1u << 20;   // subgraphs of one job (the reference: 16384)
 __host__ __device__ inline uint64_t rec_pack(uint32_t pos, uint32_t len, uint32_t ld, uint32_t rd, uint32_t g) {
-    return (uint64_t)pos | ((uint64_t)len << 32) | ((uint64_t)ld << 40) | ((uint64_t)rd << 41) | ((uint64_t)g << 48);
+    return (uint64_t)pos | ((uint64_t)len << 32) | ((uint64_t)ld << 40) | ((uint64_t)rd << 41) | ((uint64_t)g << 42);
 }
 __host__ __device__ inline uint32_t rec_pos(uint64_t r) { return (uint32_t)r; }
 __host__ __device__ inline uint32_t rec_len(uint64_t r) { return (uint32_t)(r >> 32) & 0xFF; }
 __host__ __device__ inline uint32_t rec_ld(uint64_t r) { return (uint32_t)(r >> 40) & 1; }
 __host__ __device__ inline uint32_t rec_rd(uint64_t r) { return (uint32_t)(r >> 41) & 1; }
-__host__ __device__ inline uint32_t rec_g(uint64_t r) { return (uint32_t)(r >> 48); }
+__host__ __device__ inline uint32_t rec_g(uint64_t r) { return (uint32_t)(r >> 42); }
 
 // Device error word bits.
 enum : uint32_t {

@@ -16,7 +16,6 @@ namespace cfg {
 
 namespace {
 
-constexpr int RING = 128;             // per-warp ring of l-mer hashes (w <= 62)
 constexpr int WARPS_PER_BLOCK = 8;
 constexpr uint32_t STAGE = 256;       // records a warp gathers in shared memory per reservation
 
@@ -44,54 +43,77 @@ __device__ __forceinline__ void stage_flush(const PartitionArgs& a, Stage& st) {
     st.n = 0;
 }
 
+// The value lane (lane - d) holds in this chunk, or for lanes < d the value lane
+// (lane - d + 32) held in the previous chunk (0 <= d <= 31): each source lane supplies
+// exactly one of the two, so one shuffle serves both.
+__device__ __forceinline__ uint64_t from_back(uint64_t cur, uint64_t prev, uint32_t d, uint32_t lane) {
+    return __shfl_sync(0xffffffffu, lane >= 32 - d ? prev : cur, (lane - d) & 31);
+}
+__device__ __forceinline__ uint64_t min64(uint64_t a, uint64_t b) { return a < b ? a : b; }
+
+constexpr int LEVELS = 6;   // sparse-table levels 2^0 .. 2^5 (w <= 62)
+
 // Processes the (k-1)-mer positions [j0, j1) of one fragment: emits every weak
 // super k-mer whose run starts there.
 // mod_w[x] = x % w for x < 128 (w <= 62): the cap-cut test without a division.
 // hist: this fragment's job's histogram (the run's, or its job's slice of a batch's).
-__device__ void sweep_fragment(const PartitionArgs& a, uint64_t* ring, const uint8_t* mod_w, uint64_t F0, uint32_t FL,
+//
+// Window minima with warp shuffles: in the chunk of (k-1)-mers base .. base+31, lane L
+// holds the newest l-mer hash, at q = base + w - 1 + L.  Level i of a sparse table holds
+// at position q - 2^i + 1 the minimum of the 2^i hashes starting there: the minimum of
+// the lane's own level i-1 value and that of the lane 2^(i-1) before it (for the first
+// lanes, from the previous chunk).  The window of (k-1)-mer j = q - w + 1 is then two
+// overlapping blocks of 2^e hashes, e = floor(log2 w): min(level_e[j], level_e[q-2^e+1]),
+// the second the lane's own value, the first that of the lane w - 2^e before it.
+// O(log w) work per position, no shared memory.
+__device__ void sweep_fragment(const PartitionArgs& a, const uint8_t* mod_w, uint64_t F0, uint32_t FL,
                                uint32_t j0, uint32_t j1, unsigned long long* hist, Stage& st) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t k = a.k, l = a.l, w = a.w;
     const uint32_t M = FL - k + 2;                 // (k-1)-mers in the fragment
     const uint32_t n_lmers = FL - l + 1;
     const uint32_t start = j0 == 0 ? 0 : j0 - 1;   // position j0-1 only primes the change test
-
-    // l-mers [start, start + w - 1) before the first chunk
-    for (uint32_t q = start + lane; q < start + w - 1; q += 32)
-        if (q < n_lmers) ring[q & (RING - 1)] = lmer_hash(lmer_at(a.packed, F0 + q, l), l, a.seed0);
+    const uint32_t e = 31 - __clz(w), dq = w - (1u << e);
+    // hash of l-mer q, or "none" (all ones, above every hash) outside the fragment
+    auto hash_at = [&](int64_t q) -> uint64_t {
+        return (q >= 0 && q < (int64_t)n_lmers) ? lmer_hash(lmer_at(a.packed, F0 + (uint64_t)q, l), l, a.seed0) : ~0ull;
+    };
+    uint64_t lv[LEVELS], pv[LEVELS];   // this chunk's / the previous chunk's level values
+#pragma unroll
+    for (int i = 0; i < LEVELS; ++i) pv[i] = ~0ull;
+    auto levels = [&](uint64_t h) -> uint64_t {   // adds this chunk's hashes; the window minimum
+        lv[0] = h;
+#pragma unroll
+        for (int i = 1; i < LEVELS; ++i)
+            lv[i] = (uint32_t)i <= e ? min64(lv[i - 1], from_back(lv[i - 1], pv[i - 1], 1u << (i - 1), lane)) : ~0ull;
+        uint64_t top = lv[0], ptop = pv[0];
+#pragma unroll
+        for (int i = 1; i < LEVELS; ++i)
+            if ((uint32_t)i == e) { top = lv[i]; ptop = pv[i]; }
+        const uint64_t m = min64(top, from_back(top, ptop, dq, lane));
+#pragma unroll
+        for (int i = 0; i < LEVELS; ++i) pv[i] = lv[i];
+        return m;
+    };
+    // prime the levels with the chunks before the first (their newest hashes reach back to
+    // l-mer `start`: one chunk for w <= 33, two up to w = 62)
+    if (w - 1 > 32) levels(hash_at((int64_t)start - 64 + w - 1 + lane));
+    levels(hash_at((int64_t)start - 32 + w - 1 + lane));
 
     bool active = false;
     uint32_t r0 = 0, last_cut = 0, last_cut_g = 0, last_cut_chg = 0, carry_g = 0;
     uint32_t carry_rem = 0;   // (base - start of the run in progress) % w
 
     // each chunk's new l-mer hash is computed one chunk ahead, so its loads and
-    // multiplies overlap the window minima of the chunk before (the ring holds both:
-    // 64 + w - 1 <= RING)
-    uint64_t h_next = 0;
-    {
-        const uint32_t q = start + w - 1 + lane;
-        if (q < n_lmers) h_next = lmer_hash(lmer_at(a.packed, F0 + q, l), l, a.seed0);
-    }
+    // multiplies overlap the window minima of the chunk before
+    uint64_t h_next = hash_at((int64_t)start + w - 1 + lane);
     for (uint32_t base = start;; base += 32) {
-        __syncwarp();
-        {
-            const uint32_t q = base + w - 1 + lane;
-            if (q < n_lmers) ring[q & (RING - 1)] = h_next;
-            const uint32_t q2 = q + 32;
-            h_next = q2 < n_lmers ? lmer_hash(lmer_at(a.packed, F0 + q2, l), l, a.seed0) : 0;
-        }
-        __syncwarp();
+        const uint64_t h = h_next;
+        h_next = hash_at((int64_t)base + 32 + w - 1 + lane);
+        const uint64_t m = levels(h);
         const uint32_t j = base + lane;
         const bool valid = j < M;
-        uint32_t g = 0;
-        if (valid) {
-            uint64_t m = ~0ull;
-            for (uint32_t t = 0; t < w; ++t) {
-                const uint64_t h = ring[(j + t) & (RING - 1)];
-                m = h < m ? h : m;
-            }
-            g = (uint32_t)m & a.gmask;
-        }
+        const uint32_t g = valid ? (uint32_t)m & a.gmask : 0u;
         uint32_t gprev = __shfl_up_sync(0xffffffffu, g, 1);
         if (lane == 0) gprev = carry_g;
         const bool is_chg = valid && j >= j0 && (j == 0 || gprev != g);
@@ -176,12 +198,10 @@ __device__ void sweep_fragment(const PartitionArgs& a, uint64_t* ring, const uin
 }
 
 __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_partition(const PartitionArgs a) {
-    __shared__ uint64_t rings[WARPS_PER_BLOCK][RING];
     __shared__ uint64_t stages[WARPS_PER_BLOCK][STAGE];
     __shared__ uint8_t mod_w[128];
     if (threadIdx.x < 128) mod_w[threadIdx.x] = (uint8_t)(threadIdx.x % a.w);
     __syncthreads();
-    uint64_t* ring = rings[threadIdx.x >> 5];
     Stage st{stages[threadIdx.x >> 5], 0};
     const uint64_t n_seg = (a.n_bases + a.seg - 1) / a.seg;
     const uint64_t warp0 = (uint64_t)blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5);
@@ -208,7 +228,7 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_partition(const Partit
             const uint32_t j0 = s0 > F0 ? (uint32_t)(s0 - F0) : 0;
             const uint64_t e = s1 - F0;
             const uint32_t j1 = e < M ? (uint32_t)e : M;
-            if (j0 < j1) sweep_fragment(a, ring, mod_w, F0, FL, j0, j1, a.hist + (a.frag_gbase ? a.frag_gbase[f] : 0u), st);
+            if (j0 < j1) sweep_fragment(a, mod_w, F0, FL, j0, j1, a.hist + (a.frag_gbase ? a.frag_gbase[f] : 0u), st);
         }
     }
     stage_flush(a, st);

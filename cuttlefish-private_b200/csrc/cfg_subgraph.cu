@@ -310,7 +310,7 @@ __device__ __forceinline__ void sink_for(const SubgraphArgs& a, uint32_t b, Sink
 }
 
 struct Block {   // per-CTA shared bookkeeping (in CLUSTER mode the flags of rank 0 are the cluster's)
-    uint32_t inserted, overflow, wl_n, scan_total;
+    uint32_t inserted, overflow, wl_n;
     unsigned long long vertices, isolated, phantom, trivial, icc, lmtig;
     Sink sk;
     uint32_t wsum[32];   // per-warp partial sums of a block scan (<= 1024 threads)
@@ -318,34 +318,6 @@ struct Block {   // per-CTA shared bookkeeping (in CLUSTER mode the flags of ran
 
 constexpr uint32_t FULL = 0xffffffffu;
 constexpr uint32_t STEP_BUF = 64;   // bases a path walk keeps for its label (2 bits each)
-
-// Exclusive scan of one value per thread over the CTA; B.scan_total gets the sum.
-// Every thread of the CTA must call it.
-__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, Block& B) {
-    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    uint32_t x = v;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const uint32_t y = __shfl_up_sync(FULL, x, d);
-        if (lane >= (uint32_t)d) x += y;
-    }
-    if (lane == 31) B.wsum[wid] = x;
-    __syncthreads();
-    if (wid == 0) {
-        uint32_t w = lane < nw ? B.wsum[lane] : 0;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t y = __shfl_up_sync(FULL, w, d);
-            if (lane >= (uint32_t)d) w += y;
-        }
-        if (lane < nw) B.wsum[lane] = w;
-        if (lane == nw - 1) B.scan_total = w;
-    }
-    __syncthreads();
-    const uint32_t before = wid ? B.wsum[wid - 1] : 0;
-    __syncthreads();
-    return before + x - v;
-}
 
 // Output space reserved for one lane: FASTA bytes, lm-tig records, lm-tig label bytes.
 struct Res { unsigned long long fa, lm_idx, lm_off; };
@@ -523,33 +495,57 @@ template <int W> __device__ __forceinline__ uint32_t sti(uint32_t ls) { return W
 
 struct EndInfo { uint32_t slot; uint32_t term; bool canon; };   // a path end in walk direction
 
-// The bases of one weak super k-mer (<= 128 of them), loaded once as four 64-bit
-// windows: the words are read up front, so the k-mer loop makes no memory access
-// for its predecessor/successor bases.  The packed stream carries 4 words of padding.
-struct RecBases {
-    uint64_t w0, w1, w2, w3;
-    __device__ __forceinline__ RecBases(const uint64_t* __restrict__ s, uint32_t pos, uint32_t len) {
+// The bases of one weak super k-mer, MSB-first from its first base (base 0 at bits
+// 63:62 of w[0]): 2 words for k <= 31 (a record holds at most 2(k-1)-l+2 <= 61
+// bases), 4 for k <= 63 (<= 125).  The packed stream carries 4 words of padding.
+template <int W>
+struct RecWords {
+    static constexpr int NW = W == 1 ? 2 : 4;
+    uint64_t w[NW];
+    __device__ __forceinline__ RecWords() {}
+    __device__ __forceinline__ RecWords(const uint64_t* __restrict__ s, uint32_t pos, bool has) {
         const uint64_t q = pos >> 5;
         const uint32_t sh = 2 * (pos & 31);
-        const uint64_t a0 = __ldg(s + q), a1 = __ldg(s + q + 1), a2 = len > 32 ? __ldg(s + q + 2) : 0;
-        const uint64_t a3 = len > 64 ? __ldg(s + q + 3) : 0, a4 = len > 96 ? __ldg(s + q + 4) : 0;
-        if (sh == 0) { w0 = a0; w1 = a1; w2 = a2; w3 = a3; }
-        else {
-            w0 = (a0 << sh) | (a1 >> (64 - sh)); w1 = (a1 << sh) | (a2 >> (64 - sh));
-            w2 = (a2 << sh) | (a3 >> (64 - sh)); w3 = (a3 << sh) | (a4 >> (64 - sh));
-        }
+        uint64_t a[NW + 1];
+#pragma unroll
+        for (int i = 0; i <= NW; ++i) a[i] = has ? __ldg(s + q + i) : 0ull;
+#pragma unroll
+        for (int i = 0; i < NW; ++i) w[i] = sh ? (a[i] << sh) | (a[i + 1] >> (64 - sh)) : a[i];
     }
-    __device__ __forceinline__ uint32_t base(uint32_t i) const {
-        const uint32_t j = i >> 5;
-        const uint64_t w = j == 0 ? w0 : j == 1 ? w1 : j == 2 ? w2 : w3;
-        return (uint32_t)(w >> (62 - 2 * (i & 31))) & 3;
+    // the words of the record held by lane j of the warp
+    __device__ __forceinline__ RecWords from_lane(uint32_t j) const {
+        RecWords r;
+#pragma unroll
+        for (int i = 0; i < NW; ++i) r.w[i] = __shfl_sync(0xffffffffu, w[i], j);
+        return r;
     }
-    template <int W> __device__ __forceinline__ Kmer<W> first_kmer(uint32_t k) const {
-        if constexpr (W == 1) return Kmer<1>{w0 >> (64 - 2 * k)};
-        else {
-            const uint32_t nh = k - 32;   // bases in the high word
-            return Kmer<2>{(w0 << (2 * nh)) | (w1 >> (64 - 2 * nh)), w0 >> (64 - 2 * nh)};
+    __device__ __forceinline__ uint64_t word(uint32_t i) const {   // word i, 0 past the end
+        uint64_t v = 0;
+#pragma unroll
+        for (int x = 0; x < NW; ++x) v = i == (uint32_t)x ? w[x] : v;
+        return v;
+    }
+    __device__ __forceinline__ uint64_t bases64(uint32_t i) const {   // bases i .. i+31, base i at 63:62
+        const uint32_t j = i >> 5, o = 2 * (i & 31);
+        const uint64_t a = word(j);
+        return o ? (a << o) | (word(j + 1) >> (64 - o)) : a;
+    }
+    __device__ __forceinline__ uint32_t base(uint32_t i) const { return (uint32_t)(word(i >> 5) >> (62 - 2 * (i & 31))) & 3; }
+    // the k-mer at offset idx of a record of len bases, its predecessor and successor base
+    // (BASE_E at the record's ends)
+    __device__ __forceinline__ void kmer_at(uint32_t k, uint32_t idx, uint32_t len, Kmer<W>& x, uint32_t& pred,
+                                            uint32_t& succ) const {
+        if constexpr (W == 1) {
+            const uint64_t win = bases64(idx);   // idx + k <= 61 < 64: the k-mer and its successor
+            x.lo = win >> (64 - 2 * k);
+            succ = idx + k == len ? BASE_E : (uint32_t)(win >> (62 - 2 * k)) & 3;
+        } else {
+            const uint32_t nh = k - 32;          // bases in the high word
+            x.hi = bases64(idx) >> (64 - 2 * nh);
+            x.lo = bases64(idx + nh);
+            succ = idx + k == len ? BASE_E : base(idx + k);
         }
+        pred = idx == 0 ? BASE_E : base(idx - 1);
     }
 };
 
@@ -727,61 +723,59 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
     // this CTA's share of the subgraph's records (all of them for one-CTA tables)
     const uint32_t q0 = r0 + (uint32_t)((uint64_t)(r1 - r0) * rank / nranks);
     const uint32_t q1 = r0 + (uint32_t)((uint64_t)(r1 - r0) * (rank + 1) / nranks);
-    if (q1 - q0 <= per) {
-        // one thread per k-mer instance (balanced whatever the record lengths): the records'
-        // instance counts, prefix-summed into the (still unused) work list, map
-        // instances to records
-        const uint32_t nrec = q1 - q0;
-        const uint32_t chunk = (nrec + nt - 1) / nt;
-        const uint32_t c0 = min(nrec, tid * chunk), c1 = min(nrec, c0 + chunk);
-        uint32_t sum = 0;
-        for (uint32_t j = c0; j < c1; ++j) sum += rec_len(a.recs[q0 + j]) - k + 1;
-        uint32_t run = block_excl_scan(sum, B);
-        for (uint32_t j = c0; j < c1; ++j) { wl[j] = run; run += rec_len(a.recs[q0 + j]) - k + 1; }
-        __syncthreads();
-        const uint32_t total = B.scan_total;
-        for (uint32_t t = tid; t < total; t += nt) {
-            if (*(volatile uint32_t*)&B.overflow) break;
-            uint32_t lo = 0, hi = nrec;   // the record holding instance t: last j with wl[j] <= t
-            while (hi - lo > 1) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (wl[mid] <= t) lo = mid; else hi = mid;
+    // Each warp takes 32 records at a time; lane i loads record i and its bases once (<= 2
+    // words for k <= 31, <= 4 for k <= 63).  The records' k-mer instances are then dealt
+    // out 32 per round, so every lane has work whatever the record lengths: the lane of
+    // instance t finds its record from the bit mask of the records starting in the round
+    // and takes that record's words from its owner lane by shuffles.
+    {
+        const uint32_t lane = tid & 31, nwarps = nt >> 5;
+        const uint32_t le_mask = lane_lt() | (1u << lane);
+        bool stop = false;
+        for (uint32_t rb = q0 + (tid >> 5) * 32; rb < q1 && !stop; rb += nwarps * 32) {
+            const uint32_t r = rb + lane;
+            const bool has = r < q1;
+            const uint64_t rec = has ? a.recs[r] : 0ull;
+            const uint32_t ninst = has ? rec_len(rec) - k + 1 : 0u;
+            uint32_t incl = ninst;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t y = __shfl_up_sync(FULL, incl, d);
+                if (lane >= (uint32_t)d) incl += y;
             }
-            const uint64_t rec = a.recs[q0 + lo];
-            const uint32_t pos = rec_pos(rec), len = rec_len(rec);
-            const uint32_t idx = t - wl[lo];
-            const uint64_t p = (uint64_t)pos + idx;
-            const Kmer<W> fw = ops.load(a.packed, p);
-            const Kmer<W> rc = ops.rc(fw);
-            const uint32_t pred = idx == 0 ? BASE_E : base_at(a.packed, p - 1);
-            const uint32_t succ = idx + k == len ? BASE_E : base_at(a.packed, p + k);
-            Kmer<W> pc = fw;
-            if (idx > 0) {   // the previous k-mer and its reverse complement, from fw and rc
-                Kmer<W> pf = fw, pr = rc;
-                ops.push_front(pf, pred);
-                ops.push_back(pr, 3 - pred);
-                pc = pf < pr ? pf : pr;
-            }
-            if (!insert(fw, rc, pc, idx, pred, succ, (uint32_t)p, idx == 0 && rec_ld(rec), idx + k == len && rec_rd(rec)))
-                break;
-        }
-    } else {
-        for (uint32_t r = q0 + tid; r < q1; r += nt) {
-            if (*(volatile uint32_t*)&B.overflow) break;
-            const uint64_t rec = a.recs[r];
-            const uint32_t pos = rec_pos(rec), len = rec_len(rec), ld = rec_ld(rec), rd = rec_rd(rec);
-            const RecBases rb(a.packed, pos, len);   // the whole record in registers (<= 128 bases)
-            Kmer<W> fw = rb.first_kmer<W>(k);
-            Kmer<W> rc = ops.rc(fw);
-            Kmer<W> pred_can = fw;
-            for (uint32_t idx = 0;; ++idx) {
-                const uint32_t pred = idx == 0 ? BASE_E : rb.base(idx - 1);
-                const uint32_t succ = idx + k == len ? BASE_E : rb.base(idx + k);
-                if (!insert(fw, rc, pred_can, idx, pred, succ, pos + idx, idx == 0 && ld, idx + k == len && rd)) break;
-                if (idx + k == len) break;
-                pred_can = fw < rc ? fw : rc;
-                ops.push_back(fw, succ);
-                ops.push_front(rc, 3 - succ);
+            const uint32_t P = incl - ninst;                      // first instance of record `lane`
+            const uint32_t total = __shfl_sync(FULL, incl, 31);
+            const RecWords<W> rw(a.packed, has ? rec_pos(rec) : 0u, has);
+            uint32_t started = 0;                                 // records started before the round
+            for (uint32_t t0 = 0; t0 < total; t0 += 32) {
+                const uint32_t bit = (has && P >= t0 && P < t0 + 32) ? 1u << (P - t0) : 0u;
+                const uint32_t smask = __reduce_or_sync(FULL, bit);
+                const uint32_t jj = started + __popc(smask & le_mask);
+                const uint32_t j = jj ? min(jj - 1, 31u) : 0u;   // the record of instance t0 + lane
+                started += __popc(smask);
+                const uint64_t rj = __shfl_sync(FULL, rec, j);
+                const uint32_t Pj = __shfl_sync(FULL, P, j);
+                const RecWords<W> xw = rw.from_lane(j);
+                const uint32_t t = t0 + lane;
+                bool ok = true;
+                if (t < total) {
+                    const uint32_t idx = t - Pj, len = rec_len(rj);
+                    Kmer<W> fw;
+                    uint32_t pred, succ;
+                    xw.kmer_at(k, idx, len, fw, pred, succ);
+                    const Kmer<W> rc = ops.rc(fw);
+                    Kmer<W> pc = fw;
+                    if (idx > 0) {   // the previous k-mer and its reverse complement, from fw and rc
+                        Kmer<W> pf = fw, pr = rc;
+                        ops.push_front(pf, pred);
+                        ops.push_back(pr, 3 - pred);
+                        pc = pf < pr ? pf : pr;
+                    }
+                    ok = insert(fw, rc, pc, idx, pred, succ, rec_pos(rj) + idx, idx == 0 && rec_ld(rj),
+                                idx + k == len && rec_rd(rj));
+                }
+                // a failed insert (table full) stops the build: warp-uniform, between rounds
+                if (__any_sync(FULL, !ok || *(volatile uint32_t*)&B.overflow)) { stop = true; break; }
             }
         }
     }

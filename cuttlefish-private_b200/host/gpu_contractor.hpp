@@ -85,7 +85,9 @@ public:
 
 private:
     void check(int rc, const char* what) {
-        if (rc != CFG_OK) throw cfg_error(std::string(what) + ": " + (ctx_ ? cfg_last_error_string(ctx_) : "error"), rc);
+        if (rc != CFG_OK)
+            throw cfg_error(std::string(what) + ": " + (ctx_ ? std::string(cfg_last_error_string(ctx_))
+                                                             : "error code " + std::to_string(rc)), rc);
     }
     cfg_ctx* ctx_ = nullptr;
     cfg_results res_{};

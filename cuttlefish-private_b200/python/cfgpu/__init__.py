@@ -387,7 +387,7 @@ def unitig_multiset(fasta: bytes):
 
 
 def tune_graph_count(packed: PackedInput, k: int, l: int, cutoff: int, table_load_pct: int = 0, device: int = 0,
-                     candidates=(16384, 32768, 65536), runs: int = 2):
+                     candidates=(16384, 32768, 65536, 131072, 262144), runs: int = 2):
     """Subgraph count for the fastest plain run to final unitigs.
 
     The lm-tigs depend on the subgraph count, the final maximal unitigs do not: each

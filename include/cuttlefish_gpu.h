@@ -48,7 +48,10 @@ typedef struct cfg_params {
     uint32_t k;            /* odd, 3..63                                       (Build_Params::k) */
     uint32_t l;            /* minimizer length, 1..min(k-1, 32)                 (--min-len)      */
     uint32_t cutoff;       /* edge-frequency threshold, 1..15                   (-c)             */
-    uint32_t graph_count;  /* power of two <= 65536; the reference uses 16384 (include/Atlas.hpp:33-35) */
+    uint32_t graph_count;  /* power of two <= 2^20; the reference uses 16384 (include/Atlas.hpp:33-35).
+                              lm-tigs depend on it, final unitigs do not.  The 16-bit subgraph
+                              fields of cfg_lmtig, cfg_state and cfg_record hold the subgraph id
+                              modulo 65536 when graph_count exceeds 65536. */
     uint32_t flags;        /* CFG_FLAG_* */
     uint32_t table_load_pct;  /* expected distinct vertices per k-mer instance, in percent, used to
                                  size subgraph tables (at about half load); 0 = default 100 (one
