@@ -1,6 +1,6 @@
 // Stand-in for a cereal header (serialization library, not in the reference tree) in
-// the drop-in test: the uncolored build path never (de)serialises, so archives are
-// declared with no-op operators.  Test infrastructure only.
+// the builds of the reference here: its build path never (de)serialises, so archives are
+// declared with no-op operators.  Test and baseline infrastructure only.
 #pragma once
 
 #include <istream>

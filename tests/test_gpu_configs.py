@@ -165,3 +165,72 @@ def test_config3_k63_30mbp():
     got = gpu_arrays(d, 63, 20, 1, 16384, load_pct=100)
     assert_equal_to_oracle(got, o)
     assert np.array_equal(got["unitigs"], oracle_final_unitigs(o, 63))
+
+
+def reference_build(k, data_offsets, tmp_path, read):
+    """<o>.fa of the reference's own `cuttlefish build` (oracle/ref_app.mk) on the records:
+    reads as FASTQ split over four files, references one FASTA file per record."""
+    import subprocess
+    exe = os.path.join(os.path.dirname(HERE), "oracle", "_ref", f"cuttlefish_ref_{k}")
+    if not os.path.exists(exe):
+        pytest.skip("reference build not compiled (oracle/ref_app.mk needs the reference tree)")
+    data, offs, n = data_offsets
+    files = []
+    if read:
+        per = (n + 3) // 4
+        for w in range(0, n, per):
+            p = tmp_path / f"in{len(files)}.fq"
+            with open(p, "wb") as f:
+                for i in range(w, min(n, w + per)):
+                    r = data[offs[i]:offs[i + 1]]
+                    f.write(b"@r%d\n%s\n+\n%s\n" % (i, r, b"I" * len(r)))
+            files.append(str(p))
+    else:
+        for i in range(n):
+            p = tmp_path / f"in{i}.fa"
+            r = data[offs[i]:offs[i + 1]]
+            with open(p, "wb") as f:
+                f.write(b">r%d\n" % i + b"\n".join(r[j:j + 80] for j in range(0, len(r), 80)) + b"\n")
+            files.append(str(p))
+    work = tmp_path / "work"
+    work.mkdir()
+    r = subprocess.run([exe, "read" if read else "ref", "0", str(work / "out"), str(work)] + files,
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    return (work / "out.fa").read_bytes()
+
+
+def canonical_hashes(fa):
+    """Sorted hashes of the unitig sequences in min(seq, rc(seq)) form."""
+    tr = bytes.maketrans(b"ACGT", b"TGCA")
+    seqs = [line for line in fa.split(b"\n") if line and not line.startswith(b">")]
+    canon = [min(s, s.translate(tr)[::-1]) for s in seqs]
+    blob = b"".join(canon)
+    off = np.cumsum([0] + [len(s) for s in canon])[:-1]
+    return np.sort(orc.hash_spans(blob, off, [len(s) for s in canon]))
+
+
+def gpu_unitig_fasta(data_offsets, k, l, c, G, load_pct):
+    packed = cfgpu.PackedInput(None, k, data_offsets=data_offsets)
+    with cfgpu.Compactor(k, l, c, G, table_load_pct=load_pct) as cx:
+        cx.submit(packed)
+        cx.run()
+        fa, _ = cx.unitigs()
+    packed.close()
+    return fa
+
+
+def test_reference_build_equals_gpu_config1(tmp_path):
+    """Config 1 in full: the reference's own build and the GPU (131072 subgraphs) write the
+    same maximal unitigs."""
+    d = config1()
+    want = canonical_hashes(reference_build(31, d, tmp_path, read=False))
+    assert np.array_equal(canonical_hashes(gpu_unitig_fasta(d, 31, 20, 1, 131072, 100)), want)
+
+
+def test_reference_build_equals_gpu_config2_sample(tmp_path):
+    """Config 2's first 200000 reads (cutoff 2): the reference's own build and the GPU
+    (131072 subgraphs) write the same maximal unitigs."""
+    d = config2_reads(200_000)
+    want = canonical_hashes(reference_build(31, d, tmp_path, read=True))
+    assert np.array_equal(canonical_hashes(gpu_unitig_fasta(d, 31, 20, 2, 131072, 15)), want)
