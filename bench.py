@@ -292,9 +292,12 @@ def percentile(xs, q):
 def bench_serve(args, local, world):
     """Serving loop vs the plain path on the same GPU, same jobs, same Poisson arrivals.
 
-    The plain path serves FIFO, one job at a time (submit + run + fetch per job).  The
-    server (4 slots, small jobs batched) admits jobs as they arrive.  Latency = arrival
-    -> results on the host.  Rates are multiples of the plain path's service rate."""
+    A pool of args.serve_jobs generated jobs; each rate's stream is args.serve_arrivals
+    arrivals, each a job drawn from the pool (seeded), so the tail percentiles rest on
+    hundreds of latencies.  The plain path serves FIFO, one job at a time (submit + run
+    + fetch per job).  The server (4 slots, jobs up to small_job_bases that wait together
+    batched) admits jobs as they arrive.  Latency = arrival -> results on the host.
+    Rates are multiples of the plain path's service rate."""
     import random
 
     import cfgpu
@@ -302,7 +305,6 @@ def bench_serve(args, local, world):
     t0 = time.perf_counter()
     jobs = make_serving_mix(args.serve_jobs, k)
     gen_s = time.perf_counter() - t0
-    total_bases = sum(p.n_bases for _, p, _, _ in jobs)
     ctxs = {}
 
     def plain_ctx(c, load):
@@ -316,6 +318,7 @@ def bench_serve(args, local, world):
         cx.submit(p)
         cx.run()
         cx.fetch_raw()
+        return cx.timings()[3]           # device ms of the run
 
     for j in range(len(jobs)):           # warm: every context grown to its largest job
         plain_one(j)
@@ -323,58 +326,60 @@ def bench_serve(args, local, world):
     for j in range(len(jobs)):
         plain_one(j)
     seq_s = time.perf_counter() - t
-    mu = len(jobs) / seq_s               # plain service rate, jobs/s
+    mu = len(jobs) / seq_s               # plain service rate of the pool, jobs/s
 
     def arrivals(lam, seed):
+        """(arrival time, pool job) pairs: exponential gaps at rate lam, jobs drawn uniformly."""
         r = random.Random(seed)
         at, out = 0.0, []
-        for _ in jobs:
-            out.append(at)
+        for _ in range(args.serve_arrivals):
+            out.append((at, r.randrange(len(jobs))))
             at += r.expovariate(lam)
         return out
 
     def run_plain(arr):
         start = time.perf_counter()
-        lat, done = [], 0.0
-        for j, a in enumerate(arr):
+        lat, dev, done = [], 0.0, 0.0
+        for a, j in arr:
             now = time.perf_counter() - start
             if now < a:
                 time.sleep(a - now)
-            plain_one(j)
+            dev += plain_one(j)
             done = time.perf_counter() - start
             lat.append(done - a)
-        return lat, done
+        return lat, done, dev / 1e3
 
     srv = cfgpu.Server(device=local if world > 1 else 0, slots=4, batch_max_bases=64_000_000,
                        small_job_bases=4_000_000)
 
     def run_server(arr):
         start = time.perf_counter()
-        tickets = [None] * len(arr)
-
         submitted = threading.Semaphore(0)
 
         def submitter():
-            for j, a in enumerate(arr):
+            for a, j in arr:
                 now = time.perf_counter() - start
                 if now < a:
                     time.sleep(a - now)
                 _, p, c, load = jobs[j]
-                tickets[j] = srv.submit(p, k, 20, c, table_load_pct=load)
+                srv.submit(p, k, 20, c, table_load_pct=load)
                 submitted.release()
 
+        st0 = srv.stats()
         th = threading.Thread(target=submitter)
         th.start()
-        lat, groups, done = [], [], []
+        lat, groups, done, dev = [], [], [], 0.0
         for _ in range(len(arr)):          # completion order: results are released as soon as read
             submitted.acquire()            # one more job is in the server
             t, _, tm = srv.wait_any_raw()
             srv.release(t)
             lat.append(tm.latency_s)
             groups.append(tm.group_jobs)
+            dev += tm.device_ms / max(1, tm.group_jobs)
             done.append(time.perf_counter() - start)
         th.join()
-        return lat, max(done), groups
+        st1 = srv.stats()
+        return lat, max(done), groups, dev / 1e3, st1.batches - st0.batches, st1.batched_jobs - st0.batched_jobs
 
     # warm every worker's contexts on the largest job of each kind (all workers take one at once)
     progress(f"serve: {len(jobs)} jobs generated, plain service {mu:.1f} jobs/s; warming the server")
@@ -387,21 +392,25 @@ def bench_serve(args, local, world):
         for _ in ts:
             t, _, _ = srv.wait_any_raw()
             srv.release(t)
-    run_server(arrivals(mu * 4, 99))
+    run_server(arrivals(mu * 4, 99)[:4 * len(jobs)])
     rates = []
     for f in args.serve_load:
         progress(f"serve: load {f}")
         arr = arrivals(mu * f, 1000 + int(100 * f))
-        sl, smk, groups = run_server(arr)
-        pl, pmk = run_plain(arr)
+        bases = sum(jobs[j][1].n_bases for _, j in arr)
+        small = sum(1 for _, j in arr if jobs[j][1].n_bases <= 4_000_000)
+        sl, smk, groups, sdev, nb, nbj = run_server(arr)
+        pl, pmk, pdev = run_plain(arr)
         rates.append({
-            "load_vs_plain_capacity": f, "lambda_jobs_per_s": mu * f,
+            "load_vs_plain_capacity": f, "lambda_jobs_per_s": mu * f, "arrivals": len(arr), "bases": bases,
+            "small_jobs": small,
             "server": {"p50_ms": 1e3 * percentile(sl, 50), "p99_ms": 1e3 * percentile(sl, 99),
-                       "mean_ms": 1e3 * statistics.mean(sl), "throughput_bases_per_s": total_bases / smk,
-                       "jobs_per_s": len(arr) / smk, "max_group": max(groups)},
+                       "mean_ms": 1e3 * statistics.mean(sl), "throughput_bases_per_s": bases / smk,
+                       "jobs_per_s": len(arr) / smk, "max_group": max(groups), "batches": nb, "batched_jobs": nbj,
+                       "device_time_over_makespan": sdev / smk},
             "plain": {"p50_ms": 1e3 * percentile(pl, 50), "p99_ms": 1e3 * percentile(pl, 99),
-                      "mean_ms": 1e3 * statistics.mean(pl), "throughput_bases_per_s": total_bases / pmk,
-                      "jobs_per_s": len(arr) / pmk},
+                      "mean_ms": 1e3 * statistics.mean(pl), "throughput_bases_per_s": bases / pmk,
+                      "jobs_per_s": len(arr) / pmk, "gpu_busy_fraction": pdev / pmk},
         })
     st = srv.stats()
     srv.close()
@@ -409,13 +418,14 @@ def bench_serve(args, local, world):
         cx.close()
     for _, p, _, _ in jobs:
         p.close()
+    pool_bases = sum(p.n_bases for _, p, _, _ in jobs)
     return {
-        "workload": f"serve{len(jobs)}",
-        "description": "Poisson arrivals; half --ref jobs (0.5-50 Mbp log-uniform, cutoff 1), half --read jobs "
-                       "(1-5 M x 150 bp reads, 0.5% errors, 20-40x, cutoff 2); k=31; latency = arrival -> all "
-                       "outputs on the host",
-        "jobs": len(jobs), "bases": total_bases, "plain_service_jobs_per_s": mu,
-        "plain_sequential_bases_per_s": total_bases / seq_s,
+        "workload": f"serve{len(jobs)}x{args.serve_arrivals}",
+        "description": "Poisson arrivals; a pool of jobs, half --ref (0.5-50 Mbp log-uniform, cutoff 1), half --read "
+                       "(1-5 M x 150 bp reads, 0.5% errors, 20-40x, cutoff 2); each arrival a pool job drawn "
+                       "uniformly; k=31; latency = arrival -> all outputs on the host",
+        "pool_jobs": len(jobs), "pool_bases": pool_bases, "arrivals_per_rate": args.serve_arrivals,
+        "plain_service_jobs_per_s": mu, "plain_sequential_bases_per_s": pool_bases / seq_s,
         "server": {"slots": 4, "batch_max_bases": 64_000_000, "small_job_bases": 4_000_000,
                    "batches": int(st.batches), "batched_jobs": int(st.batched_jobs),
                    "max_running": int(st.max_running)},
@@ -813,7 +823,8 @@ def main():
                     help="further plain-path workloads reported under \"workloads\" (comma list; empty: none)")
     ap.add_argument("--batch-genomes", type=int, default=1000, help="genomes of the batched comparison (0: skip it)")
     ap.add_argument("--batch-steps", type=int, default=2)
-    ap.add_argument("--serve-jobs", type=int, default=16, help="jobs of the serving comparison (0: skip it)")
+    ap.add_argument("--serve-jobs", type=int, default=16, help="generated jobs of the serving pool (0: skip serving)")
+    ap.add_argument("--serve-arrivals", type=int, default=240, help="arrivals per rate, each a job of the pool")
     ap.add_argument("--serve-load", type=float, nargs="+", default=[0.5, 1.0, 2.0],
                     help="arrival rates as multiples of the plain path's service rate")
     args = ap.parse_args()

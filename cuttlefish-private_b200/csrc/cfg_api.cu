@@ -182,6 +182,7 @@ int launch_plan(cfg_ctx* c, const std::vector<Launch>& plan, uint64_t arena_slot
         a.list = d_list; a.n_list = (uint32_t)L.list.size();
         a.tab_off = d_off; a.tab_cap = d_cap; a.smem_cap = L.per; a.arena = c->arena.as<unsigned char>();
         a.k = c->p.k; a.fth = c->p.cutoff; a.load_limit_pct = 90; a.record_clocks = 1;
+        a.dedup = record_dedup(c->p.k, c->p.l, c->p.cutoff, c->p.flags);
         a.fasta = c->fasta.as<char>(); a.fasta_cap = c->fasta_cap;
         a.lm_text = c->lm_text.as<char>(); a.lm_text_cap = c->lm_text_cap;
         a.lm = c->lm.as<LmtigOut>(); a.lm_cap = c->lm_cap;

@@ -385,6 +385,7 @@ int enqueue(cfg_batch* b) {
     a.list = b->list.as<uint32_t>(); a.tab_off = b->tab_off.as<uint64_t>(); a.tab_cap = b->tab_cap.as<uint32_t>();
     a.arena = b->arena.as<unsigned char>();
     a.k = b->p.k; a.fth = b->p.cutoff; a.load_limit_pct = 90;
+    a.dedup = record_dedup(b->p.k, b->p.l, b->p.cutoff, b->p.flags);
     a.fasta = b->fasta.as<char>(); a.lm_text = b->lm_text.as<char>(); a.lm = b->lm.as<LmtigOut>();
     a.retry = b->retry.as<uint32_t>(); a.cnt = b->counters.as<Counters>(); a.err = &bw->err;
     a.jobs = b->jobs.as<JobOut>(); a.g_shift = b->g_shift; a.record_clocks = 0;

@@ -172,6 +172,14 @@ __device__ __forceinline__ uint32_t ef_add(uint32_t ef, uint32_t front, uint32_t
     return ef;
 }
 
+// e_f after m instances of the edge pair (front, back): each count still saturates at 15
+// (m = 1 is ef_add).
+__device__ __forceinline__ uint32_t ef_add_m(uint32_t ef, uint32_t front, uint32_t back, uint32_t m) {
+    if (front < 4) { const uint32_t off = 4 * front, c = (ef >> off) & 15; ef += (min(c + m, 15u) - c) << off; }
+    if (back < 4)  { const uint32_t off = 16 + 4 * back, c = (ef >> off) & 15; ef += (min(c + m, 15u) - c) << off; }
+    return ef;
+}
+
 // meta bits
 constexpr uint32_t M_VISITED = 1u, M_DISC_F = 2u, M_DISC_B = 4u;
 

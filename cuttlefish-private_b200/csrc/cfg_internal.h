@@ -147,7 +147,18 @@ struct SubgraphArgs {
     // batch: per-subgraph vertices, isolated, phantom, trivial, icc (5 words each),
     // summed per job after the run; nullptr: counters go to the sink
     uint32_t* bucket_cnt;
+    // merge identical records of a subgraph before its vertex table is built (one-CTA
+    // tables, k <= 31): each distinct record applied once with its multiplicity
+    uint32_t dedup;
 };
+
+// Whether the subgraph kernels merge identical records for these parameters: read sets
+// (cutoff >= 2, where most records are copies of a genomic stretch) unless a flag says.
+// A merged record's key holds at most 60 bases: 2(k-1) - l + 2 <= 60.
+inline uint32_t record_dedup(uint32_t k, uint32_t l, uint32_t cutoff, uint32_t flags) {
+    if (k > 31 || 2 * (k - 1) + 2 > 60 + l || (flags & 0x8u)) return 0;   // CFG_FLAG_NO_RECORD_DEDUP
+    return (flags & 0x4u) || cutoff >= 2;     // CFG_FLAG_RECORD_DEDUP
+}
 
 constexpr uint32_t OUT_STRIPES = 32;
 

@@ -239,11 +239,11 @@ struct Tab {
     // is claimed with x's first state by one 16-byte CAS (key and state are one pair; a
     // free slot's state is ST_INIT); a slot holding x gets the state CAS of update_state.
     __device__ uint32_t upsert(const Kmer<W>& x, uint32_t owner, uint32_t h, uint32_t front, uint32_t back, uint32_t pos,
-                               bool& fresh) const {
+                               uint32_t m, bool& fresh) const {
         static_assert(W == 1, "one-word keys only");
         fresh = false;
         const uint32_t b = owner * per;
-        const uint64_t first = (uint64_t)ef_add(st_ef(ST_INIT), front, back) | ((uint64_t)min(st_ins(ST_INIT), pos) << 32);
+        const uint64_t first = (uint64_t)ef_add_m(st_ef(ST_INIT), front, back, m) | ((uint64_t)min(st_ins(ST_INIT), pos) << 32);
         // probe bound: a quarter of a large table (a run that long means the table is
         // close to full: the insert fails and the subgraph is retried with a larger one)
         const uint32_t bound = per > 256 ? per / 4 : per;
@@ -255,16 +255,18 @@ struct Tab {
                 M::cas128(a, EMPTY, ST_INIT, x.lo, first, cur, stv);
                 if (cur == EMPTY) { fresh = true; return b + h; }
             }
-            if (cur == x.lo) { update_state(b + h, front, back, pos, stv); return b + h; }
+            if (cur == x.lo) { update_state(b + h, front, back, pos, m, stv); return b + h; }
             if (++h == per) h = 0;
         }
         return NONE;
     }
-    // state word update: ef gets the edges, ins the earliest position (one CAS unless unchanged)
-    __device__ __forceinline__ void update_state(uint32_t s, uint32_t front, uint32_t back, uint32_t pos, uint64_t cur) const {
+    // state word update: ef gets m instances of the edges, ins the earliest position (one
+    // CAS unless unchanged)
+    __device__ __forceinline__ void update_state(uint32_t s, uint32_t front, uint32_t back, uint32_t pos, uint32_t m,
+                                                 uint64_t cur) const {
         const A a = sa(s);
         for (uint32_t it = 0;; ++it) {
-            const uint32_t ef = ef_add((uint32_t)cur, front, back);
+            const uint32_t ef = ef_add_m((uint32_t)cur, front, back, m);
             const uint32_t in = min((uint32_t)(cur >> 32), pos);
             const uint64_t nv = (uint64_t)ef | ((uint64_t)in << 32);
             if (nv == cur) return;
@@ -310,7 +312,7 @@ __device__ __forceinline__ void sink_for(const SubgraphArgs& a, uint32_t b, Sink
 }
 
 struct Block {   // per-CTA shared bookkeeping (in CLUSTER mode the flags of rank 0 are the cluster's)
-    uint32_t inserted, overflow, wl_n;
+    uint32_t inserted, overflow, wl_n, covered;   // covered: vertices of the paths and one-k-mer cycles emitted
     unsigned long long vertices, isolated, phantom, trivial, icc, lmtig;
     Sink sk;
     uint32_t wsum[32];   // per-warp partial sums of a block scan (<= 1024 threads)
@@ -356,10 +358,11 @@ __device__ __forceinline__ char* fasta_at(const Sink& sk, unsigned long long o, 
 
 __device__ __forceinline__ uint32_t lane_lt() { uint32_t m; asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m)); return m; }
 
-// Appends every local slot ls < per with pred(ls) to the shared work list wl (order
-// unspecified).  All threads of the CTA must call it; blockDim is a multiple of 32.
-template <typename Pred>
-__device__ __forceinline__ void compact(uint32_t per, uint32_t* wl, uint32_t* n, Pred pred) {
+// Appends val(ls) for every local slot ls < per with pred(ls) to the shared work list wl
+// (order unspecified; compact appends ls itself).  All threads of the CTA must call it;
+// blockDim is a multiple of 32.
+template <typename Pred, typename Val>
+__device__ __forceinline__ void compact_to(uint32_t per, uint32_t* wl, uint32_t* n, Pred pred, Val val) {
     const uint32_t nt = blockDim.x;
     for (uint32_t base = 0; base < per; base += nt) {
         const uint32_t ls = base + threadIdx.x;
@@ -368,8 +371,12 @@ __device__ __forceinline__ void compact(uint32_t per, uint32_t* wl, uint32_t* n,
         uint32_t at = 0;
         if ((threadIdx.x & 31) == 0 && m) at = atomicAdd(n, (uint32_t)__popc(m));
         at = __shfl_sync(0xffffffffu, at, 0);
-        if (p) wl[at + __popc(m & lane_lt())] = ls;
+        if (p) wl[at + __popc(m & lane_lt())] = val(ls);
     }
+}
+template <typename Pred>
+__device__ __forceinline__ void compact(uint32_t per, uint32_t* wl, uint32_t* n, Pred pred) {
+    compact_to(per, wl, n, pred, [](uint32_t ls) { return ls; });
 }
 
 template <int MODE> __device__ __forceinline__ void tsync() {
@@ -665,6 +672,63 @@ __device__ void write_emitted_path(const SubgraphArgs& a, const Tab<W, MODE>& T,
 }
 
 // rank/nranks: this CTA's position in its cluster; per: slots owned by one CTA.
+// Merges the identical records of [q0, q1) (one-CTA tables, k <= 31, records of at most
+// 60 bases).  A table of per / 2 entries of 32 bytes is laid over the still unused vertex
+// table (lkeys): key = the record's bases, MSB-first, in two words with its length and
+// discontinuity marks in the low byte of the second (all ones in both: empty -- a real
+// second word never ends in 0xFF, since lengths stay below 63); value = the smallest
+// (stream position << 32 | index from q0) of its copies and their count.  Every probe is
+// a 16-byte compare-and-swap, which returns the entry's whole key in one atomic step, so
+// no reader sees half a key.  On success wl holds one entry per distinct record -- the
+// index from q0 of its first copy in the stream | min(count, 15) << 20 -- and B.wl_n their
+// number; false (nothing merged) when the table filled up.  All threads of the CTA call it.
+__device__ bool dedup_records(const SubgraphArgs& a, Block& B, uint32_t q0, uint32_t q1, uint32_t per,
+                              unsigned long long* lkeys, uint32_t* wl) {
+    typedef Mem<LOCAL> M;
+    const uint32_t tid = threadIdx.x, nt = blockDim.x, D = per / 2;
+    for (uint32_t e = tid; e < D; e += nt) {
+        lkeys[4 * e] = EMPTY; lkeys[4 * e + 1] = EMPTY; lkeys[4 * e + 2] = ~0ull; lkeys[4 * e + 3] = 0;
+    }
+    if (tid == 0) { B.overflow = 0; B.wl_n = 0; }
+    __syncthreads();
+    const uint32_t base = smem_addr(lkeys);
+    const uint32_t bound = D > 256 ? D / 4 : D;
+    for (uint32_t r = q0 + tid; r < q1; r += nt) {
+        if (*(volatile uint32_t*)&B.overflow) break;
+        const uint64_t rec = a.recs[r];
+        const uint32_t len = rec_len(rec), pos = rec_pos(rec);
+        const RecWords<1> rw(a.packed, pos, true);
+        const uint64_t k0 = len >= 32 ? rw.w[0] : rw.w[0] & ~(~0ull >> (2 * len));
+        const uint64_t k1 = (len > 32 ? rw.w[1] & ~(~0ull >> (2 * (len - 32))) : 0ull) | (uint64_t)len |
+                            ((uint64_t)rec_ld(rec) << 6) | ((uint64_t)rec_rd(rec) << 7);
+        const uint64_t z = (k0 ^ (k1 * 0xC2B2AE3D27D4EB4Full)) * 0x9E3779B97F4A7C15ull;
+        uint32_t h = (uint32_t)(((z >> 32) * D) >> 32);
+        bool done = false;
+        for (uint32_t p = 0; p < bound; ++p) {
+            const uint32_t ea = base + h * 32;
+            uint64_t o0, o1;
+            M::cas128(ea, EMPTY, EMPTY, k0, k1, o0, o1);
+            if ((o0 == EMPTY && o1 == EMPTY) || (o0 == k0 && o1 == k1)) {
+                const uint64_t pi = ((uint64_t)pos << 32) | (r - q0);
+                asm volatile("red.shared.min.u64 [%0], %1;" :: "r"(ea + 16), "l"(pi) : "memory");
+                asm volatile("red.shared.add.u32 [%0], %1;" :: "r"(ea + 24), "r"(1u) : "memory");
+                done = true;
+                break;
+            }
+            if (++h == D) h = 0;
+        }
+        if (!done) { atomicOr(&B.overflow, 1u); break; }
+    }
+    __syncthreads();
+    if (*(volatile uint32_t*)&B.overflow) return false;
+    compact_to(D, wl, &B.wl_n, [&](uint32_t e) { return lkeys[4 * e + 1] != EMPTY; }, [&](uint32_t e) {
+        const uint32_t c = (uint32_t)lkeys[4 * e + 3];
+        return ((uint32_t)lkeys[4 * e + 2] & 0xFFFFFu) | ((c < 15u ? c : 15u) << 20);
+    });
+    __syncthreads();
+    return true;
+}
+
 template <int W, int MODE>
 __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block& B, Block* Bc,
                              uint32_t g, uint32_t rank, uint32_t nranks, uint32_t per,
@@ -675,6 +739,20 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
     const uint32_t k = a.k, fth = a.fth;
     const uint32_t tid = threadIdx.x, nt = blockDim.x;
     const uint32_t base_slot = rank * per;
+    const uint32_t r0 = a.bucket_off[g], r1 = a.bucket_off[g + 1];
+    // this CTA's share of the subgraph's records (all of them for one-CTA tables)
+    const uint32_t q0 = r0 + (uint32_t)((uint64_t)(r1 - r0) * rank / nranks);
+    const uint32_t q1 = r0 + (uint32_t)((uint64_t)(r1 - r0) * (rank + 1) / nranks);
+    // the build's items: the records [q0, q1), or the distinct ones in wl when merged
+    uint32_t n_items = q1 - q0;
+    bool from_list = false;
+    if constexpr (W == 1 && MODE == LOCAL) {
+        if (a.dedup && n_items >= 64 && n_items < (1u << 20) && dedup_records(a, B, q0, q1, per, lkeys, wl)) {
+            from_list = true;
+            n_items = B.wl_n;
+            __syncthreads();   // every thread has read the count before it is reset below
+        }
+    }
 
     for (uint32_t s = tid; s < per; s += nt) {
         if constexpr (W == 1) lkeys[2 * s] = EMPTY; else { lkeys[2 * s] = EMPTY; lkeys[2 * s + 1] = EMPTY; }
@@ -682,7 +760,8 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         lmeta[s] = 0;
     }
     if (tid == 0) {
-        B.inserted = 0; B.overflow = 0; B.wl_n = 0; B.vertices = B.isolated = B.phantom = B.trivial = B.icc = B.lmtig = 0;
+        B.inserted = 0; B.overflow = 0; B.wl_n = 0; B.covered = 0;
+        B.vertices = B.isolated = B.phantom = B.trivial = B.icc = B.lmtig = 0;
         sink_for(a, g, B.sk);
     }
     tsync<MODE>();
@@ -690,12 +769,11 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
     // ---------------- build ----------------
     const uint32_t limit = (uint32_t)(((uint64_t)per * a.load_limit_pct) / 100);
     uint32_t n_fresh = 0;   // vertices this thread inserted
-    const uint32_t r0 = a.bucket_off[g], r1 = a.bucket_off[g + 1];
     // HT_Router::update of one k-mer instance at stream position p (idx-th of its record):
     // edges from its predecessor / successor bases, the self-loop rule against the
     // previous k-mer's canonical form, and the record's entrance / exit marks.
     auto insert = [&](const Kmer<W>& fw, const Kmer<W>& rc, const Kmer<W>& pred_can, uint32_t idx, uint32_t pred,
-                      uint32_t succ, uint32_t p, bool l_mark, bool r_mark) -> bool {
+                      uint32_t succ, uint32_t p, bool l_mark, bool r_mark, uint32_t m) -> bool {
         const bool canon = fw < rc;
         const Kmer<W> can = canon ? fw : rc;
         uint32_t front = canon ? pred : compb(succ);
@@ -706,11 +784,11 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         bool fresh;
         uint32_t s;
         if constexpr (W == 1) {
-            s = T.upsert(can, owner, h, front, back, p, fresh);
+            s = T.upsert(can, owner, h, front, back, p, m, fresh);
         } else {
             uint64_t seen = ST_INIT;
             s = T.find_or_insert(can, owner, h, fresh, seen);
-            if (s != NONE) T.update_state(s, front, back, p, seen);
+            if (s != NONE) T.update_state(s, front, back, p, m, seen);
         }
         if (s == NONE) { atomicOr(&B.overflow, 1u); return false; }
         n_fresh += fresh;
@@ -720,22 +798,22 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         if (disc) T.mark_disc(s, disc);
         return true;
     };
-    // this CTA's share of the subgraph's records (all of them for one-CTA tables)
-    const uint32_t q0 = r0 + (uint32_t)((uint64_t)(r1 - r0) * rank / nranks);
-    const uint32_t q1 = r0 + (uint32_t)((uint64_t)(r1 - r0) * (rank + 1) / nranks);
-    // Each warp takes 32 records at a time; lane i loads record i and its bases once (<= 2
-    // words for k <= 31, <= 4 for k <= 63).  The records' k-mer instances are then dealt
-    // out 32 per round, so every lane has work whatever the record lengths: the lane of
-    // instance t finds its record from the bit mask of the records starting in the round
-    // and takes that record's words from its owner lane by shuffles.
+    // Each warp takes 32 items (records, or distinct records with their multiplicity) at
+    // a time; lane i loads item i's record and its bases once (<= 2 words for k <= 31, <= 4
+    // for k <= 63).  The records' k-mer instances are then dealt out 32 per round, so every
+    // lane has work whatever the record lengths: the lane of instance t finds its record
+    // from the bit mask of the records starting in the round and takes that record's words
+    // (and multiplicity) from its owner lane by shuffles.
     {
         const uint32_t lane = tid & 31, nwarps = nt >> 5;
         const uint32_t le_mask = lane_lt() | (1u << lane);
         bool stop = false;
-        for (uint32_t rb = q0 + (tid >> 5) * 32; rb < q1 && !stop; rb += nwarps * 32) {
-            const uint32_t r = rb + lane;
-            const bool has = r < q1;
-            const uint64_t rec = has ? a.recs[r] : 0ull;
+        for (uint32_t rb = (tid >> 5) * 32; rb < n_items && !stop; rb += nwarps * 32) {
+            const uint32_t i = rb + lane;
+            const bool has = i < n_items;
+            const uint32_t item = has && from_list ? wl[i] : i;
+            const uint64_t rec = has ? a.recs[q0 + (from_list ? item & 0xFFFFFu : item)] : 0ull;
+            const uint32_t mult = from_list ? item >> 20 : 1u;
             const uint32_t ninst = has ? rec_len(rec) - k + 1 : 0u;
             uint32_t incl = ninst;
 #pragma unroll
@@ -755,6 +833,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
                 started += __popc(smask);
                 const uint64_t rj = __shfl_sync(FULL, rec, j);
                 const uint32_t Pj = __shfl_sync(FULL, P, j);
+                const uint32_t mj = __shfl_sync(FULL, mult, j);
                 const RecWords<W> xw = rw.from_lane(j);
                 const uint32_t t = t0 + lane;
                 bool ok = true;
@@ -772,7 +851,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
                         pc = pf < pr ? pf : pr;
                     }
                     ok = insert(fw, rc, pc, idx, pred, succ, rec_pos(rj) + idx, idx == 0 && rec_ld(rj),
-                                idx + k == len && rec_rd(rj));
+                                idx + k == len && rec_rd(rj), mj);
                 }
                 // a failed insert (table full) stops the build: warp-uniform, between rounds
                 if (__any_sync(FULL, !ok || *(volatile uint32_t*)&B.overflow)) { stop = true; break; }
@@ -868,6 +947,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
     });
     __syncthreads();
     const uint32_t nw2 = B.wl_n;
+    uint32_t n_cov = 0;   // vertices of what this thread emitted
     for (uint32_t base = 0; base < nw2; base += nt) {   // uniform over the CTA: warps reserve output together
         const uint32_t i = base + tid;
         // what this lane emits: one-k-mer cycles at s and/or e, and one path vs..ve
@@ -968,48 +1048,56 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         }
         if (mark0) T.or_meta(s, M_VISITED);
         if (mark1) T.or_meta(e, M_VISITED);
+        n_cov += (kc0 ? 1u : 0u) + (kc1 ? 1u : 0u) + (path ? n2 : 0u);
     }
+    for (int d = 16; d; d >>= 1) n_cov += __shfl_down_sync(0xffffffffu, n_cov, d);
+    if ((tid & 31) == 0 && n_cov) atomicAdd(&B.covered, n_cov);
     tsync<MODE>();
 
     clk[3] = clock64();
     // ---------------- W3: isolated cycles ----------------
+    // Every path is emitted once, with its vertices counted: when they cover every vertex
+    // with an edge, no isolated cycle is left (one CTA's table; a cluster's paths span CTAs)
+    const bool no_cycles = MODE != CLUSTER && B.covered == B.vertices - B.isolated;
     if (tid == 0) B.wl_n = 0;
     __syncthreads();
-    compact(per, wl, &B.wl_n, [&](uint32_t ls) {
-        return !local_empty<W>(lkeys, ls) && !(lmeta[ls] & (M_ISO | M_VISITED));
-    });
-    __syncthreads();
-    const uint32_t nw3 = B.wl_n;
-    for (uint32_t base = 0; base < nw3; base += nt) {
-        const uint32_t i = base + tid;
-        bool emit = false;
-        uint32_t n = 0;
-        DV<W> v0{};
-        if (i < nw3) {
-            const uint32_t ls = wl[i];
-            const uint32_t s = base_slot + ls;
-            if (!(*(volatile uint32_t*)(lmeta + ls) & M_VISITED)) {
-                // every vertex left has both sides linked: walk the cycle from s out of its back side
-                v0 = dv_at(T, ops, s, BACK);
-                DV<W> v = v0; int side = BACK;
-                bool is_min = true, ok = true;
-                do {
-                    int s_in;
-                    if (!step(T, ops, fth, v, side, s_in) || ++n > T.per * T.nranks) { atomicOr(a.err, DERR_WALK_LIMIT); ok = false; break; }
-                    side = 1 - s_in;
-                    if (v.slot != s && (v.d < v.r ? v.d : v.r) < v0.d) is_min = false;
-                } while (v.slot != s);
-                emit = ok && is_min;
+    if (!no_cycles) {
+        compact(per, wl, &B.wl_n, [&](uint32_t ls) {
+            return !local_empty<W>(lkeys, ls) && !(lmeta[ls] & (M_ISO | M_VISITED));
+        });
+        __syncthreads();
+        const uint32_t nw3 = B.wl_n;
+        for (uint32_t base = 0; base < nw3; base += nt) {
+            const uint32_t i = base + tid;
+            bool emit = false;
+            uint32_t n = 0;
+            DV<W> v0{};
+            if (i < nw3) {
+                const uint32_t ls = wl[i];
+                const uint32_t s = base_slot + ls;
+                if (!(*(volatile uint32_t*)(lmeta + ls) & M_VISITED)) {
+                    // every vertex left has both sides linked: walk the cycle from s out of its back side
+                    v0 = dv_at(T, ops, s, BACK);
+                    DV<W> v = v0; int side = BACK;
+                    bool is_min = true, ok = true;
+                    do {
+                        int s_in;
+                        if (!step(T, ops, fth, v, side, s_in) || ++n > T.per * T.nranks) { atomicOr(a.err, DERR_WALK_LIMIT); ok = false; break; }
+                        side = 1 - s_in;
+                        if (v.slot != s && (v.d < v.r ? v.d : v.r) < v0.d) is_min = false;
+                    } while (v.slot != s);
+                    emit = ok && is_min;
+                }
             }
-        }
-        __syncwarp();
-        const Res r = reserve_warp(B.sk, emit ? n + k + 3 : 0, 0, 0);
-        if (emit) {
-            // Character_Buffer::rotate_append_cycle (include/Character_Buffer.hpp:166-175): start at the
-            // minimum vertex in its canonical orientation
-            char* p = fasta_at(B.sk, r.fa, n + k - 1);
-            write_path(T, ops, fth, v0, BACK, n, p, false, true);
-            atomicAdd(&B.trivial, 1ull); atomicAdd(&B.icc, 1ull);
+            __syncwarp();
+            const Res r = reserve_warp(B.sk, emit ? n + k + 3 : 0, 0, 0);
+            if (emit) {
+                // Character_Buffer::rotate_append_cycle (include/Character_Buffer.hpp:166-175): start at the
+                // minimum vertex in its canonical orientation
+                char* p = fasta_at(B.sk, r.fa, n + k - 1);
+                write_path(T, ops, fth, v0, BACK, n, p, false, true);
+                atomicAdd(&B.trivial, 1ull); atomicAdd(&B.icc, 1ull);
+            }
         }
     }
     tsync<MODE>();

@@ -16,6 +16,8 @@ LIB_PATH = os.path.join(PKG_DIR, "lib", "libcfgpu.so")
 CFG_OK, CFG_ERR_BAD_INPUT, CFG_ERR_OOM, CFG_ERR_TABLE_FULL, CFG_ERR_WALK_LIMIT, CFG_ERR_CUDA, CFG_ERR_STATE = range(7)
 CFG_FLAG_DUMP_STATES = 0x1
 CFG_FLAG_DUMP_RECORDS = 0x2
+CFG_FLAG_RECORD_DEDUP = 4
+CFG_FLAG_NO_RECORD_DEDUP = 8
 CFG_NOALLOC_MAX_BASES = 917472
 
 ERRORS = {0: "OK", 1: "BAD_INPUT", 2: "OOM", 3: "TABLE_FULL", 4: "WALK_LIMIT", 5: "CUDA", 6: "STATE"}

@@ -43,6 +43,12 @@ enum {
 /* cfg_params.flags */
 #define CFG_FLAG_DUMP_STATES   0x1u  /* keep every vertex state for cfg_dump_states */
 #define CFG_FLAG_DUMP_RECORDS  0x2u  /* keep the bucketed weak super k-mers for cfg_dump_records */
+/* Identical weak super k-mers of a subgraph (same bases, length and discontinuity
+ * marks: a read set's copies of one genomic stretch) are merged before the vertex
+ * table is built, each distinct one applied once with its multiplicity; the states and
+ * every output are the same either way.  Default: on for cutoff >= 2 (read sets). */
+#define CFG_FLAG_RECORD_DEDUP     0x4u  /* merge identical records whatever the cutoff */
+#define CFG_FLAG_NO_RECORD_DEDUP  0x8u  /* never merge them */
 
 typedef struct cfg_params {
     uint32_t k;            /* odd, 3..63                                       (Build_Params::k) */

@@ -17,9 +17,9 @@ import synth
 pytestmark = pytest.mark.gpu
 
 
-def gpu_run(records, k, l, c, G, load_pct=0):
+def gpu_run(records, k, l, c, G, load_pct=0, extra_flags=0):
     packed = cfgpu.PackedInput(records, k)
-    flags = cfgpu.CFG_FLAG_DUMP_STATES | cfgpu.CFG_FLAG_DUMP_RECORDS
+    flags = cfgpu.CFG_FLAG_DUMP_STATES | cfgpu.CFG_FLAG_DUMP_RECORDS | extra_flags
     with cfgpu.Compactor(k, l, c, G, flags=flags, table_load_pct=load_pct) as cx:
         cx.submit(packed)
         cx.run()
@@ -37,9 +37,9 @@ def gpu_run(records, k, l, c, G, load_pct=0):
     return counts, rec_ms, st, orc.fasta_multiset(fasta), lm
 
 
-def compare(records, k, l, c, G, load_pct=0):
+def compare(records, k, l, c, G, load_pct=0, extra_flags=0):
     o = orc.OracleRun(records, k, l, c, G)
-    counts, rec_ms, st, fa, lm = gpu_run(records, k, l, c, G, load_pct)
+    counts, rec_ms, st, fa, lm = gpu_run(records, k, l, c, G, load_pct, extra_flags)
     assert counts.n_records == o.counts["n_records"]
     assert counts.n_instances == o.counts["n_instances"]
     assert rec_ms == o.records, "weak super k-mer records differ"
@@ -219,3 +219,25 @@ def test_submit_rejects_bad_fragment_tables():
         dev, _ = cx.unitigs()
     assert orc.fasta_multiset(dev) == orc.OracleRun(recs, 31, 20, 1, 1).fasta_records()
     packed.close()
+
+
+@pytest.mark.parametrize("case", ["genome", "reads", "homopolymers", "reads_no_merge"])
+def test_record_merging(case):
+    """Identical weak super k-mers merged before the table build (CFG_FLAG_RECORD_DEDUP; the
+    default for cutoff >= 2) give the same states and outputs as building from every copy:
+    forced on for cutoff-1 inputs full of copies, forced off for a read set.  Subgraph
+    counts keep at least 64 records per subgraph, below which nothing is merged."""
+    rng = np.random.default_rng(60)
+    if case == "genome":
+        g = synth.genome_with_repeats(rng, 100_000, n_copies=40, n_pal=20)
+        compare([g, g[5000:60000], g[:30000]], 31, 20, 1, 64, extra_flags=cfgpu.CFG_FLAG_RECORD_DEDUP)
+    elif case == "reads":
+        g = synth.genome_with_repeats(rng, 20_000, n_copies=5, n_pal=3)
+        compare(synth.reads(rng, g, 6_000), 31, 20, 2, 256, load_pct=30)
+    elif case == "homopolymers":
+        recs = ["A" * 200] * 20 + ["ACGT" * 30] * 17 + ["AACAC" * 20] * 40 + [synth.random_seq(rng, 500)] * 30
+        for k, l in ((9, 4), (31, 20)):
+            compare(recs, k, l, 1, 16, extra_flags=cfgpu.CFG_FLAG_RECORD_DEDUP)
+    else:
+        g = synth.genome_with_repeats(rng, 20_000, n_copies=5, n_pal=3)
+        compare(synth.reads(rng, g, 6_000), 31, 20, 2, 256, load_pct=30, extra_flags=cfgpu.CFG_FLAG_NO_RECORD_DEDUP)
