@@ -17,6 +17,7 @@ struct cfg_ctx {
     int device = 0;
     cfg_params p{};
     uint32_t G = 16384;
+    uint32_t sms = 148;
     int words = 1;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[8] = {};
@@ -94,13 +95,17 @@ int check_err_word(cfg_ctx* c, uint32_t e) {
 // instance counts in `inst_h`.
 int run_partition(cfg_ctx* c, std::vector<uint32_t>& inst_h, std::vector<uint32_t>& off_h) {
     const uint32_t G = c->G;
-    if (!c->hist.ensure(sizeof(unsigned long long) * G)) return fail(c, CFG_ERR_OOM, "hist");
     if (!c->misc.ensure(sizeof(MiscWords))) return fail(c, CFG_ERR_OOM, "misc");
     uint64_t cap = std::max<uint64_t>(c->n_bases / 4 + 1024, 1u << 16);
     for (int attempt = 0; attempt < 3; ++attempt) {
-        if (!c->flat.ensure(cap * 8)) return fail(c, CFG_ERR_OOM, "flat records");
-        cap = c->flat.bytes / 8;
-        CK(cudaMemsetAsync(c->hist.p, 0, sizeof(unsigned long long) * G, c->stream));
+        {   // the partition's records and the bucket sort's: equal capacities, because the two
+            // buffers trade places after every sort (and neither may be reallocated after the
+            // partition has written into one)
+            const size_t want = (std::max<size_t>(cap * 8, std::max(c->flat.bytes, c->recs.bytes)) + (2u << 20) - 1) &
+                                ~(size_t)((2u << 20) - 1);
+            if (!c->flat.ensure_exact(want) || !c->recs.ensure_exact(want)) return fail(c, CFG_ERR_OOM, "record buffers");
+        }
+        cap = std::min(c->flat.bytes, c->recs.bytes) / 8;
         CK(cudaMemsetAsync(c->misc.p, 0, sizeof(MiscWords), c->stream));
         PartitionArgs a{};
         a.packed = c->d_packed; a.frag_off = c->d_frag_off; a.frag_len = c->d_frag_len;
@@ -109,7 +114,7 @@ int run_partition(cfg_ctx* c, std::vector<uint32_t>& inst_h, std::vector<uint32_
         a.gmask = G - 1; a.seed0 = wy_seed0_host(); a.seg = 2048;
         a.recs = c->flat.as<uint64_t>(); a.rec_cap = cap;
         a.rec_cursor = &c->misc.as<MiscWords>()->rec_cursor;
-        a.hist = c->hist.as<unsigned long long>();
+        a.hist = nullptr;   // the bucket sort counts records and instances per subgraph
         a.err = &c->misc.as<MiscWords>()->err;
         CK(cudaEventRecord(c->ev[1], c->stream));
         launch_partition(a, c->stream);
@@ -126,25 +131,16 @@ int run_partition(cfg_ctx* c, std::vector<uint32_t>& inst_h, std::vector<uint32_
         if (attempt == 2) return fail(c, CFG_ERR_OOM, "record buffer kept overflowing");
     }
     CK(cudaEventRecord(c->ev[3], c->stream));
-    if (!c->bucket_off.ensure(4ull * (G + 1)) || !c->inst.ensure(4ull * G) || !c->fill.ensure(4ull * G))
-        return fail(c, CFG_ERR_OOM, "bucket arrays");
-    if (!c->recs.ensure(8 * std::max<uint64_t>(c->n_records, 1))) return fail(c, CFG_ERR_OOM, "bucketed records");
-    if (G <= 65536) {
-        launch_bucket_scan(c->hist.as<unsigned long long>(), G, c->bucket_off.as<uint32_t>(), c->inst.as<uint32_t>(),
-                           c->fill.as<uint32_t>(), c->stream);
-    } else {   // multi-block scan of the larger histograms
-        if (!c->scan_part.ensure(4ull * (G / 8192 + 1))) return fail(c, CFG_ERR_OOM, "scan partials");
-        launch_bucket_scan_large(c->hist.as<unsigned long long>(), G, c->bucket_off.as<uint32_t>(), c->inst.as<uint32_t>(),
-                                 c->fill.as<uint32_t>(), c->scan_part.as<uint32_t>(), c->stream);
-    }
-    ScatterArgs s{};
-    s.flat = c->flat.as<uint64_t>(); s.n = c->n_records;
-    s.bucket_off = c->bucket_off.as<uint32_t>(); s.bucket_fill = c->fill.as<uint32_t>();
-    s.recs = c->recs.as<uint64_t>();
-    launch_scatter(s, c->stream);
-    CK(cudaGetLastError());
+    if (!c->bucket_off.ensure(4ull * (G + 1)) || !c->inst.ensure(4ull * G)) return fail(c, CFG_ERR_OOM, "bucket arrays");
+    // flat -> recs (by super-bucket) -> flat (by subgraph), then the two buffers trade
+    // places: c->recs holds the bucketed records, c->flat the next run's partition output
+    if (!c->scan_part.ensure(4ull * bucket_sort_scratch_words(G, c->sms))) return fail(c, CFG_ERR_OOM, "sort scratch");
+    CK(launch_bucket_sort(c->flat.as<uint64_t>(), c->n_records, G, c->p.k, c->sms, c->scan_part.as<uint32_t>(),
+                          c->recs.as<uint64_t>(), c->flat.as<uint64_t>(), c->bucket_off.as<uint32_t>(),
+                          c->inst.as<uint32_t>(), c->stream));
+    std::swap(c->flat, c->recs);
     CK(cudaEventRecord(c->ev[4], c->stream));
-    c->launches += 1 + (c->n_records ? 1 : 0);
+    c->launches += 5;
     inst_h.resize(G); off_h.resize(G + 1);
     CK(cudaMemcpyAsync(inst_h.data(), c->inst.p, 4ull * G, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpyAsync(off_h.data(), c->bucket_off.p, 4ull * (G + 1), cudaMemcpyDeviceToHost, c->stream));
@@ -391,6 +387,10 @@ int cfg_create(int device, const cfg_params* params, cfg_ctx** out) {
     cfg_ctx* c = new (std::nothrow) cfg_ctx();
     if (!c) return CFG_ERR_OOM;
     c->device = device; c->p = p; c->G = p.graph_count; c->words = p.k <= 31 ? 1 : 2;
+    {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0) c->sms = (uint32_t)sms;
+    }
     c->stripes = std::min<uint32_t>(OUT_STRIPES, p.graph_count);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return CFG_ERR_CUDA; }
     for (auto& e : c->ev)

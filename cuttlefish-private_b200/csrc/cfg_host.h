@@ -21,6 +21,15 @@ struct DevBuf {
         bytes = want;
         return true;
     }
+    // exactly `cap` bytes when it must grow (buffers that have to keep equal capacities)
+    bool ensure_exact(size_t cap) {
+        if (cap <= bytes) return true;
+        if (p) cudaFree(p);
+        p = nullptr; bytes = 0;
+        if (cudaMalloc(&p, cap) != cudaSuccess) { cudaGetLastError(); return false; }
+        bytes = cap;
+        return true;
+    }
     void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
     template <typename T> T* as() const { return (T*)p; }
 };

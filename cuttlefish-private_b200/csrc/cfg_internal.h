@@ -56,7 +56,7 @@ struct PartitionArgs {
     uint64_t* recs;             // flat records
     uint64_t rec_cap;
     unsigned long long* rec_cursor;
-    unsigned long long* hist;   // per subgraph: records (low 32) | instances (high 32)
+    unsigned long long* hist;   // per subgraph: records (low 32) | instances (high 32); nullptr: not counted
     uint32_t* err;
     const uint32_t* frag_gbase; // batch: first histogram entry of each fragment's job (nullptr: 0)
 };
@@ -173,6 +173,12 @@ void launch_partition(const PartitionArgs& a, cudaStream_t s);
 void launch_bucket_scan(const unsigned long long* hist, uint32_t G, uint32_t* bucket_off, uint32_t* inst,
                         uint32_t* fill, cudaStream_t s);
 void launch_scatter(const ScatterArgs& a, cudaStream_t s);
+// Bucket sort of n flat records by subgraph (cfg_bucket_sort.cu) without a global atomic
+// per record: flat -> tmp (by super-bucket) -> out (by subgraph); bucket_off[0..G] and
+// inst[0..G) come out of it.  scratch: bucket_sort_scratch_words(G, sms) words.
+uint64_t bucket_sort_scratch_words(uint32_t G, uint32_t sms);
+cudaError_t launch_bucket_sort(const uint64_t* flat, uint64_t n, uint32_t G, uint32_t k, uint32_t sms, uint32_t* scratch,
+                               uint64_t* tmp, uint64_t* out, uint32_t* bucket_off, uint32_t* inst, cudaStream_t s);
 // cluster == 0: tables in the global arena; 1: one CTA's shared memory; >1: a cluster's.
 cudaError_t launch_subgraphs(const SubgraphArgs& a, int words, uint32_t cluster, uint32_t threads, cudaStream_t s);
 // Persistent form: `grid` CTAs (a multiple of `cluster`) loop over the device-held list.

@@ -56,7 +56,8 @@ constexpr int LEVELS = 6;   // sparse-table levels 2^0 .. 2^5 (w <= 62)
 // Processes the (k-1)-mer positions [j0, j1) of one fragment: emits every weak
 // super k-mer whose run starts there.
 // mod_w[x] = x % w for x < 128 (w <= 62): the cap-cut test without a division.
-// hist: this fragment's job's histogram (the run's, or its job's slice of a batch's).
+// hist: this fragment's job's histogram (the run's, or its job's slice of a batch's);
+// nullptr when the bucket sort counts the records itself.
 //
 // Window minima with warp shuffles: in the chunk of (k-1)-mers base .. base+31, lane L
 // holds the newest l-mer hash, at q = base + w - 1 + L.  Level i of a sparse table holds
@@ -175,7 +176,7 @@ __device__ void sweep_fragment(const PartitionArgs& a, const uint8_t* mod_w, uin
             const uint32_t len = lj + (j - c + k - 2) + 1;
             const uint64_t r = rec_pack((uint32_t)(F0 + c - lj), len, lj & cchg, is_chg ? 1u : 0u, cg);
             st.buf[slot0 + __popc(emit & lanemask_lt())] = r;
-            atomicAdd(hist + cg, 1ull | ((unsigned long long)(len - k + 1) << 32));
+            if (hist) atomicAdd(hist + cg, 1ull | ((unsigned long long)(len - k + 1) << 32));
         }
         // carries: last cut / run start of this chunk
         if (cut) {
@@ -191,7 +192,7 @@ __device__ void sweep_fragment(const PartitionArgs& a, const uint8_t* mod_w, uin
             const uint32_t len = lj + (FL - c);
             const uint64_t r = rec_pack((uint32_t)(F0 + c - lj), len, lj & last_cut_chg, 0, last_cut_g);
             st.buf[slot0 + __popc(emit)] = r;
-            atomicAdd(hist + last_cut_g, 1ull | ((unsigned long long)(len - k + 1) << 32));
+            if (hist) atomicAdd(hist + last_cut_g, 1ull | ((unsigned long long)(len - k + 1) << 32));
         }
         if (stopping || fin) return;
     }
@@ -228,7 +229,8 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_partition(const Partit
             const uint32_t j0 = s0 > F0 ? (uint32_t)(s0 - F0) : 0;
             const uint64_t e = s1 - F0;
             const uint32_t j1 = e < M ? (uint32_t)e : M;
-            if (j0 < j1) sweep_fragment(a, mod_w, F0, FL, j0, j1, a.hist + (a.frag_gbase ? a.frag_gbase[f] : 0u), st);
+            if (j0 < j1) sweep_fragment(a, mod_w, F0, FL, j0, j1,
+                                          a.hist ? a.hist + (a.frag_gbase ? a.frag_gbase[f] : 0u) : nullptr, st);
         }
     }
     stage_flush(a, st);

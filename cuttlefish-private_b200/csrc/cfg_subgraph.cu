@@ -425,19 +425,10 @@ __device__ __forceinline__ bool step_inline(const Tab<W, MODE>& T, const KOps<W>
     return true;
 }
 
-// Two-word (k > 32) walks take the step out of line: inlined into the path walk at
-// ptxas -O2/-O3 they failed lookups that the same source finds at -O1 or out of line.
-template <int W, int MODE>
-__device__ __noinline__ bool step_outline(const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t fth, DV<W>& v, int side,
-                                          int& s_in) {
-    return step_inline(T, ops, fth, v, side, s_in);
-}
 template <int W, int MODE>
 __device__ __forceinline__ bool step(const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t fth, DV<W>& v, int side, int& s_in) {
-    if constexpr (W == 1) return step_inline(T, ops, fth, v, side, s_in);
-    else return step_outline(T, ops, fth, v, side, s_in);
+    return step_inline(T, ops, fth, v, side, s_in);
 }
-
 
 // Bytes written one at a time in address order (rising or falling), gathered into
 // whole 8-byte words: one store per aligned word the run covers, byte stores only
@@ -1185,7 +1176,7 @@ __global__ void __launch_bounds__(512) k_subgraph_global(const SubgraphArgs a) {
 
 // The kernels' shared-memory limit is always raised to the largest table any launch
 // uses (it is process-wide state: lowering it would break launches recorded in graphs).
-template <int W> constexpr size_t max_table_bytes() { return (size_t)(W == 1 ? 8192 : 2048) * (W == 1 ? 24 : 32); }
+template <int W> constexpr size_t max_table_bytes() { return (size_t)(W == 1 ? 8192 : 4096) * (W == 1 ? 24 : 32); }
 template <typename K>
 cudaError_t raise_smem_limit(K kernel, size_t bytes) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -1251,7 +1242,7 @@ __global__ void k_stripe_fixup(LmtigOut* lm, uint64_t lm_slice, const unsigned l
     }
 }
 
-uint32_t subgraph_max_per_cta(int words) { return words == 1 ? 8192 : 2048; }
+uint32_t subgraph_max_per_cta(int words) { return words == 1 ? 8192 : 4096; }
 uint32_t subgraph_cluster_per_cta(int words) { return words == 1 ? 4096 : 2048; }
 
 cudaError_t launch_subgraphs(const SubgraphArgs& a, int words, uint32_t cluster, uint32_t threads, cudaStream_t s) {
@@ -1265,8 +1256,8 @@ cudaError_t launch_subgraphs(const SubgraphArgs& a, int words, uint32_t cluster,
     if (cluster == 1)
         return words == 1 ? launch_shared(k_subgraph_shared<1, LOCAL>, a, 1, threads, bytes, s, 0, max_table_bytes<1>())
                           : launch_shared(k_subgraph_shared<2, LOCAL>, a, 1, threads, bytes, s, 0, max_table_bytes<2>());
-    return words == 1 ? launch_shared(k_subgraph_shared<1, CLUSTER>, a, cluster, threads, bytes, s, 0, max_table_bytes<1>())
-                      : launch_shared(k_subgraph_shared<2, CLUSTER>, a, cluster, threads, bytes, s, 0, max_table_bytes<2>());
+    if (words != 1) return cudaErrorInvalidValue;   // k > 32 tables are one CTA's or the arena's
+    return launch_shared(k_subgraph_shared<1, CLUSTER>, a, cluster, threads, bytes, s, 0, max_table_bytes<1>());
 }
 
 void launch_stripe_fixup(LmtigOut* lm, uint64_t lm_slice, const unsigned long long* lm_used,
@@ -1279,8 +1270,8 @@ int subgraph_occupancy(int words, uint32_t cluster, uint32_t threads, uint32_t p
     if (cluster <= 1)
         return words == 1 ? occupancy_of(k_subgraph_shared<1, LOCAL>, 1, threads, bytes, max_table_bytes<1>())
                           : occupancy_of(k_subgraph_shared<2, LOCAL>, 1, threads, bytes, max_table_bytes<2>());
-    return words == 1 ? occupancy_of(k_subgraph_shared<1, CLUSTER>, cluster, threads, bytes, max_table_bytes<1>())
-                      : occupancy_of(k_subgraph_shared<2, CLUSTER>, cluster, threads, bytes, max_table_bytes<2>());
+    if (words != 1) return 0;   // no cluster tables for k > 32
+    return occupancy_of(k_subgraph_shared<1, CLUSTER>, cluster, threads, bytes, max_table_bytes<1>());
 }
 
 cudaError_t launch_subgraphs_persistent(const SubgraphArgs& a, int words, uint32_t cluster, uint32_t threads,
@@ -1297,8 +1288,8 @@ cudaError_t launch_subgraphs_persistent(const SubgraphArgs& a, int words, uint32
     if (cluster == 1)
         return words == 1 ? launch_shared(k_subgraph_shared<1, LOCAL>, b, 1, threads, bytes, s, grid)
                           : launch_shared(k_subgraph_shared<2, LOCAL>, b, 1, threads, bytes, s, grid);
-    return words == 1 ? launch_shared(k_subgraph_shared<1, CLUSTER>, b, cluster, threads, bytes, s, grid)
-                      : launch_shared(k_subgraph_shared<2, CLUSTER>, b, cluster, threads, bytes, s, grid);
+    if (words != 1) return cudaErrorInvalidValue;   // no cluster tables for k > 32
+    return launch_shared(k_subgraph_shared<1, CLUSTER>, b, cluster, threads, bytes, s, grid);
 }
 
 }  // namespace cfg
