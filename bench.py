@@ -122,7 +122,11 @@ def bench_batch(args, pg, local, world, peak, with_cpu):
     b = cfgpu.Batch(k, l, cutoff, 16384, device=local if world > 1 else 0)
     # the autotuner times its candidate shapes on a sample (every tenth genome), and the
     # whole batch runs with the shape it keeps
-    if not args.no_tune:
+    if args.batch_tuning:
+        ld, ct, lp, gc = (int(x) for x in args.batch_tuning.split(","))
+        tuning = cfgpu.BatchTuning(ld, ct, lp, gc, 0.0)
+        b.set_tuning(ld, ct, lp, gc)
+    elif not args.no_tune:
         sample = packed[::10] if len(packed) >= 50 else packed
         b.submit(sample)
         progress(f"batch: tuning on {len(sample)} genomes")
@@ -350,7 +354,7 @@ def bench_serve(args, local, world):
         return lat, done, dev / 1e3
 
     srv = cfgpu.Server(device=local if world > 1 else 0, slots=4, batch_max_bases=64_000_000,
-                       small_job_bases=4_000_000)
+                       small_job_bases=4_000_000, large_job_bases=64 << 20, large_slots=2)
 
     def run_server(arr):
         start = time.perf_counter()
@@ -427,8 +431,9 @@ def bench_serve(args, local, world):
         "pool_jobs": len(jobs), "pool_bases": pool_bases, "arrivals_per_rate": args.serve_arrivals,
         "plain_service_jobs_per_s": mu, "plain_sequential_bases_per_s": pool_bases / seq_s,
         "server": {"slots": 4, "batch_max_bases": 64_000_000, "small_job_bases": 4_000_000,
+                   "large_job_bases": 64 << 20, "large_slots": 2,
                    "batches": int(st.batches), "batched_jobs": int(st.batched_jobs),
-                   "max_running": int(st.max_running)},
+                   "max_running": int(st.max_running), "max_running_large": int(st.max_running_large)},
         "rates": rates, "generation_s": round(gen_s, 1),
     }
 
@@ -812,6 +817,8 @@ def main():
     ap.add_argument("--workload", default="reads30x", choices=sorted(WORKLOADS) + ["batch", "serve"],
                     help="batch / serve: only the batched-vs-plain or the serving comparison")
     ap.add_argument("--no-tune", action="store_true", help="batched form: the default launch shapes")
+    ap.add_argument("--batch-tuning", default="",
+                    help="batched form: local_div,cluster_threads,table_load_pct,graph_count instead of tuning")
     ap.add_argument("--reads", type=int, default=10_000_000)
     ap.add_argument("--cpu-sample-reads", type=int, default=1_000_000)
     ap.add_argument("--cpu-sample-bases", type=int, default=60_000_000)

@@ -7,9 +7,13 @@
 // pooled and shared by the workers):
 //   - a large job runs alone through a plain context (cfg_ctx);
 //   - small jobs waiting together with equal parameters are taken as one group and
-//     run as one batch (cfg_batch), however many arrived since the last group.
+//     run as one batch (cfg_batch), however many arrived since the last group;
+//   - at most `large_slots` large jobs (above `large_job_bases`) run at once: a large
+//     job fills the GPU by itself, so more of them at once only stretch each one, and
+//     their latency is better served FIFO.  While the large slots are taken, smaller
+//     jobs behind a waiting large job start past it.
 // Several workers run at once, so jobs overlap on the device (their kernels share
-// the SMs; their copies overlap other jobs' kernels).  Contexts keep their device
+// the SMs; their copies and host-side planning overlap other jobs' kernels).  Contexts keep their device
 // buffers between jobs (tables, record and output arenas stay allocated), so a
 // warm server allocates nothing per request.  Memory admission: every job (or
 // group) has a device-footprint estimate; it starts only when the footprints of the
@@ -101,6 +105,7 @@ struct cfg_server {
     uint64_t held_bytes = 0;      // footprints of every live context
     uint64_t inflight = 0;        // footprints of the groups running now (admission)
     uint32_t running = 0;         // groups in flight
+    uint32_t running_large = 0;   // of which large jobs
     bool stop = false;
     std::vector<std::unique_ptr<Worker>> workers;
     // plain contexts shared by all workers: a job takes any idle one with its parameters,
@@ -114,17 +119,27 @@ namespace {
 
 double secs(Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double>(b - a).count(); }
 
+bool is_large(const cfg_server* s, const Ticket* t) { return t->in.n_bases > s->cfg.large_job_bases; }
+
 // Picks the next group for a worker (called with the lock held); empty if nothing
-// may start now.
-std::vector<Ticket*> take_group(cfg_server* s, uint64_t& need, bool& batched) {
+// may start now.  The group starts at the head of the queue, unless the head is a
+// large job and every large slot is taken: then at the first job behind it that is
+// not large (large jobs keep their FIFO order and take the next free large slot).
+std::vector<Ticket*> take_group(cfg_server* s, uint64_t& need, bool& batched, bool& large) {
     std::vector<Ticket*> g;
     if (s->queue.empty()) return g;
-    Ticket* head = s->queue.front();
+    size_t at = 0;
+    if (is_large(s, s->queue[0]) && s->running_large >= s->cfg.large_slots) {
+        while (at < s->queue.size() && is_large(s, s->queue[at])) ++at;
+        if (at == s->queue.size()) return g;
+    }
+    Ticket* head = s->queue[at];
+    large = is_large(s, head);
     const bool small = s->cfg.batch_max_bases && head->in.n_bases <= s->cfg.small_job_bases;
     uint64_t bases = head->in.n_bases;
     g.push_back(head);
     if (small) {
-        for (size_t i = 1; i < s->queue.size() && g.size() < s->cfg.batch_max_jobs; ++i) {
+        for (size_t i = at + 1; i < s->queue.size() && g.size() < s->cfg.batch_max_jobs; ++i) {
             Ticket* t = s->queue[i];
             if (!same_params(t->p, head->p) || t->in.n_bases > s->cfg.small_job_bases) continue;
             if (bases + t->in.n_bases > s->cfg.batch_max_bases) break;
@@ -229,20 +244,22 @@ void worker_loop(cfg_server* s, Worker* w) {
     for (;;) {
         std::vector<Ticket*> g;
         uint64_t need = 0;
-        bool batched = false;
+        bool batched = false, large = false;
         {
             std::unique_lock<std::mutex> lock(s->mu);
             for (;;) {
                 if (s->stop) return;
-                g = take_group(s, need, batched);
+                g = take_group(s, need, batched, large);
                 if (!g.empty()) break;
                 s->cv_work.wait(lock);
             }
             const auto now = Clock::now();
             for (Ticket* t : g) { t->state = 1; t->t_start = now; }
             ++s->running;
+            if (large) ++s->running_large;
             s->inflight += need;
             s->st.max_running = std::max<uint64_t>(s->st.max_running, s->running);
+            s->st.max_running_large = std::max<uint64_t>(s->st.max_running_large, s->running_large);
             if (batched) { ++s->st.batches; s->st.batched_jobs += g.size(); }
         }
         if (batched) run_batch(s, *w, g, need);
@@ -258,6 +275,7 @@ void worker_loop(cfg_server* s, Worker* w) {
                 s->st.bases += t->in.n_bases;
             }
             --s->running;
+            if (large) --s->running_large;
             s->inflight -= need;
         }
         s->cv_done.notify_all();
@@ -277,6 +295,9 @@ int cfg_server_create(int device, const cfg_server_config* config, cfg_server** 
     if (c.slots > 64) return CFG_ERR_BAD_INPUT;
     if (c.batch_max_jobs == 0) c.batch_max_jobs = 256;
     if (c.batch_max_jobs > 4096) return CFG_ERR_BAD_INPUT;
+    if (c.large_job_bases == 0) c.large_job_bases = 64ull << 20;
+    if (c.large_slots == 0) c.large_slots = 2;
+    if (c.large_slots > c.slots) c.large_slots = c.slots;
     int n_dev = 0;
     if (cudaGetDeviceCount(&n_dev) != cudaSuccess || device < 0 || device >= n_dev) { cudaGetLastError(); return CFG_ERR_CUDA; }
     if (cudaSetDevice(device) != cudaSuccess) return CFG_ERR_CUDA;

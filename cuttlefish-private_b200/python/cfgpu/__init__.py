@@ -78,7 +78,8 @@ class BatchTuning(ctypes.Structure):
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("slots", ctypes.c_uint32), ("batch_max_jobs", ctypes.c_uint32), ("hbm_budget", ctypes.c_uint64),
-                ("batch_max_bases", ctypes.c_uint64), ("small_job_bases", ctypes.c_uint64)]
+                ("batch_max_bases", ctypes.c_uint64), ("small_job_bases", ctypes.c_uint64),
+                ("large_job_bases", ctypes.c_uint64), ("large_slots", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 class JobTiming(ctypes.Structure):
@@ -89,7 +90,7 @@ class JobTiming(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in (
         "submitted", "completed", "failed", "batches", "batched_jobs", "max_running", "bases", "held_bytes",
-        "hbm_budget")]
+        "hbm_budget", "max_running_large")]
 
 
 class BatchStats(ctypes.Structure):
@@ -521,9 +522,10 @@ class Server:
     The packed input of a job must stay alive until its wait returns."""
 
     def __init__(self, device: int = 0, slots: int = 4, hbm_budget: int = 0, batch_max_bases: int = 0,
-                 small_job_bases: int = 0, batch_max_jobs: int = 0):
+                 small_job_bases: int = 0, batch_max_jobs: int = 0, large_job_bases: int = 0, large_slots: int = 0):
         self.lib = load()
-        cfg = ServerConfig(slots, batch_max_jobs, hbm_budget, batch_max_bases, small_job_bases)
+        cfg = ServerConfig(slots, batch_max_jobs, hbm_budget, batch_max_bases, small_job_bases, large_job_bases,
+                           large_slots, 0)
         s = ctypes.c_void_p()
         rc = self.lib.cfg_server_create(device, ctypes.byref(cfg), ctypes.byref(s))
         if rc:

@@ -318,6 +318,10 @@ typedef struct cfg_server_config {
     uint64_t hbm_budget;       /* device bytes the server's contexts may hold (0: 70% of free) */
     uint64_t batch_max_bases;  /* bases per batch (0: no batching)                             */
     uint64_t small_job_bases;  /* jobs up to this size may be batched                          */
+    uint64_t large_job_bases;  /* jobs above this size are large (0: 64 M bases)               */
+    uint32_t large_slots;      /* large jobs running at once (0: 2); the others wait in FIFO
+                                  order while smaller jobs behind them start                  */
+    uint32_t reserved;         /* 0                                                             */
 } cfg_server_config;
 
 typedef struct cfg_job_timing {
@@ -331,6 +335,7 @@ typedef struct cfg_job_timing {
 typedef struct cfg_server_stats {
     uint64_t submitted, completed, failed, batches, batched_jobs, max_running, bases;
     uint64_t held_bytes, hbm_budget;
+    uint64_t max_running_large;   /* most large jobs seen running at once */
 } cfg_server_stats;
 
 int cfg_server_create(int device, const cfg_server_config* config, cfg_server** out);

@@ -92,3 +92,24 @@ def test_serving_memory_budget_serialises():
         assert srv.stats().max_running == 1
     for p in packed:
         p.close()
+
+
+def test_serving_large_slots_limit():
+    """Jobs above large_job_bases run at most large_slots at a time (FIFO among
+    themselves) while smaller jobs start past a waiting large one; results as alone."""
+    rng = np.random.default_rng(203)
+    jobs = mixed_jobs(rng, 12)
+    packed = [cfgpu.PackedInput(r, k) for k, _, _, _, r in jobs]
+    expect = [alone(k, l, c, load, p) for (k, l, c, load, _), p in zip(jobs, packed)]
+    large = 60_000
+    assert sum(p.n_bases > large for p in packed) >= 3
+    with cfgpu.Server(slots=4, large_job_bases=large, large_slots=1) as srv:
+        ts = [srv.submit(p, k, l, c, table_load_pct=load) for (k, l, c, load, _), p in zip(jobs, packed)]
+        for i, t in enumerate(ts):
+            (counts, fasta, lms), _ = srv.wait(t)
+            assert summary(jobs[i][0], counts, fasta, lms) == expect[i]
+        st = srv.stats()
+        assert st.max_running_large == 1
+        assert st.max_running >= 2, "smaller jobs never ran beside a large one"
+    for p in packed:
+        p.close()
