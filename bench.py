@@ -55,6 +55,33 @@ def synth():
     return lib
 
 
+def input_text(name, data, offs, n_rec):
+    """The workload's records as the text of an input file, in pinned host memory (a torch
+    uint8 tensor): FASTQ for reads (header '@', quality all 'I'), FASTA otherwise (one
+    sequence line per record)."""
+    import numpy as np
+    import torch
+    o = np.ctypeslib.as_array(offs, shape=(n_rec + 1,)).astype(np.int64)
+    seq = np.frombuffer(data, dtype=np.uint8, count=int(o[-1]))
+    if name == "reads30x":
+        L = int(o[1] - o[0])
+        arr = np.empty((n_rec, 2 * L + 6), dtype=np.uint8)
+        arr[:, 0] = ord("@"); arr[:, 1] = ord("\n")
+        arr[:, 2:2 + L] = seq.reshape(n_rec, L)
+        arr[:, 2 + L] = ord("\n"); arr[:, 3 + L] = ord("+"); arr[:, 4 + L] = ord("\n")
+        arr[:, 5 + L:5 + 2 * L] = ord("I")
+        arr[:, 5 + 2 * L] = ord("\n")
+        flat = arr.reshape(-1)
+    else:
+        parts = []
+        for i in range(n_rec):
+            parts += [np.frombuffer(b">r\n", dtype=np.uint8), seq[o[i]:o[i + 1]], np.frombuffer(b"\n", dtype=np.uint8)]
+        flat = np.concatenate(parts)
+    pinned = torch.empty(flat.size, dtype=torch.uint8, pin_memory=True)
+    pinned.numpy()[:] = flat
+    return pinned
+
+
 def make_workload(name, n_reads=10_000_000):
     """-> (bytes of concatenated records, ctypes offsets, n_records)."""
     lib = synth()
@@ -120,14 +147,14 @@ def bench_batch(args, pg, local, world, peak, with_cpu):
     steps, warm = args.batch_steps, max(3, args.warmup)
 
     b = cfgpu.Batch(k, l, cutoff, 16384, device=local if world > 1 else 0)
-    # the autotuner times its candidate shapes on a sample (every tenth genome), and the
+    # the autotuner times its candidate shapes on a sample (every fifth genome), and the
     # whole batch runs with the shape it keeps
     if args.batch_tuning:
         ld, ct, lp, gc = (int(x) for x in args.batch_tuning.split(","))
         tuning = cfgpu.BatchTuning(ld, ct, lp, gc, 0.0)
         b.set_tuning(ld, ct, lp, gc)
     elif not args.no_tune:
-        sample = packed[::10] if len(packed) >= 50 else packed
+        sample = packed[::5] if len(packed) >= 50 else packed
         b.submit(sample)
         progress(f"batch: tuning on {len(sample)} genomes")
         tuning = b.tune_unitigs()
@@ -548,6 +575,28 @@ def bench_workload(args, name, pg, rank, local, world, with_cpu):
     h2d = packed.p.n_bases // 4 + 12 * packed.p.n_frags
     d2h = fin_bytes + 96
 
+    # e2e from the file's text: the same records as FASTQ (reads) or FASTA (references)
+    # in pinned memory, through cfg_submit_text (H2D of the text, parse and packing on the
+    # device) + run + collation + D2H of the unitigs
+    text = input_text(name, data, offs, n_rec)
+    text_bytes = text.numel()
+    for _ in range(1):
+        cx.submit_text_ptr(text.data_ptr(), text_bytes)
+        cx.run()
+        cx.unitigs_raw()
+    barrier(pg)
+    text_times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        cx.submit_text_ptr(text.data_ptr(), text_bytes)
+        cx.run()
+        _, tb, _, _ = cx.unitigs_raw()
+        text_times.append(time.perf_counter() - t0)
+        if tb != fin_bytes:
+            raise RuntimeError("unitigs from the text path differ in size from the packed path's")
+    del text
+    text_s_max = allreduce_max(pg, local, sum(text_times))
+
     # value: input resident in HBM, device-timed
     cx.submit(packed)
     for _ in range(args.warmup):
@@ -603,6 +652,11 @@ def bench_workload(args, name, pg, rank, local, world, with_cpu):
         "config": dict(config, parallelism=f"replicas{world}"),
         "e2e": {"value": e2e_value, "unit": "bases/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": 1e3 * e2e_s_max / args.steps},
+        "e2e_text": {"value": job_rate(world, bases, args.steps, text_s_max), "unit": "bases/s",
+                     "h2d_bytes_per_step": text_bytes, "d2h_bytes_per_step": d2h,
+                     "ms_per_step": 1e3 * text_s_max / args.steps,
+                     "input": "FASTQ text (@, sequence, +, quality lines)" if name == "reads30x" else
+                              "FASTA text (one line per record)"},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": "k_subgraph (construct + walk, all launches of a run)",
                      "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",

@@ -186,11 +186,13 @@ int launch_plan(cfg_ctx* c, const std::vector<Launch>& plan, uint64_t arena_slot
         a.dump = (c->p.flags & CFG_FLAG_DUMP_STATES) ? c->dump.as<StateOut>() : nullptr; a.dump_cap = c->dump_cap;
         a.retry = c->retry.as<uint32_t>(); a.cnt = c->counters.as<Counters>();
         a.err = &c->misc.as<MiscWords>()->err;
-        // a quarter of the slots, up to 512 threads (two such CTAs per SM); the largest
-        // one-CTA table (one per SM) gets 1024
-        const uint32_t threads = L.cluster == 0 ? 512
-                                 : L.cluster == 1 && L.per > 4096 ? 1024
-                                 : std::min<uint32_t>(512, std::max<uint32_t>(64, L.per / 4));
+        // a quarter of the slots, up to the table class's largest CTA (k <= 31: 512 threads,
+        // two CTAs per SM, and 1024 for the 8192-slot tables; k > 32: 256 up to 2048 slots,
+        // three CTAs per SM); arena tables: that largest CTA
+        const uint32_t tmax = subgraph_max_threads(W, L.cluster == 0 ? 0u : L.per);
+        const uint32_t threads = L.cluster == 0 ? tmax
+                                 : L.cluster == 1 && L.per > 4096 ? tmax
+                                 : std::min<uint32_t>(tmax, std::max<uint32_t>(64, L.per / 4));
         CK(launch_subgraphs(a, W, L.cluster, threads, c->stream));
         c->launches += 1;
         at += L.list.size();

@@ -279,7 +279,7 @@ int plan_shapes(cfg_batch* b) {
     for (uint32_t c = 0; c < cc.nl; ++c) {
         const uint32_t per = 64u << c;
         uint32_t t = per / std::max<uint32_t>(1, b->tune.local_div);
-        t = std::min<uint32_t>(per > 4096 ? 1024 : 512, std::max<uint32_t>(64, t));
+        t = std::min<uint32_t>(subgraph_max_threads(b->words, per), std::max<uint32_t>(64, t));
         t = (t + 31) / 32 * 32;
         const int occ = subgraph_occupancy(b->words, 1, t, per);
         if (occ <= 0) return bfail(b, CFG_ERR_CUDA, "no resident CTA for a table class");
@@ -291,7 +291,8 @@ int plan_shapes(cfg_batch* b) {
         if (occ <= 0) return bfail(b, CFG_ERR_CUDA, "no resident cluster for a table class");
         b->shapes.push_back(Shape{cc.nl + cl - 2, cl, t, cc.per_cl, (uint32_t)occ * cl});
     }
-    b->shapes.push_back(Shape{cc.nl + 7, 0, 512, 0, (uint32_t)(2 * sms)});
+    b->shapes.push_back(Shape{cc.nl + 7, 0, subgraph_max_threads(b->words, 0), 0,
+                              (uint32_t)((b->words == 1 ? 2 : 3) * sms)});
     return CFG_OK;
 }
 
@@ -731,10 +732,10 @@ int cfg_batch_tune_unitigs(cfg_batch* b, cfg_batch_tuning* out) {
         return CFG_OK;
     };
     // subgraph count first (default shapes), then the launch shapes at that count; the
-    // counts stop at a sixteenth of the params', where subgraphs of the largest jobs
-    // still fit cluster tables
+    // counts halve down to a sixteenth of the params', where subgraphs of the largest
+    // jobs still fit cluster tables
     cfg_batch_tuning best{4, 512, base_load, 0, 1e30f};
-    for (uint32_t G = b->G_params; G >= 1 && G + 1 > b->G_params / 16; G /= 4) {
+    for (uint32_t G = b->G_params; G >= 1 && G + 1 > b->G_params / 16; G /= 2) {
         cfg_batch_tuning t{4, 512, base_load, G == b->G_params ? 0u : G, 0.f};
         float ms = 0;
         int rc = time_of(t, ms);
@@ -742,10 +743,13 @@ int cfg_batch_tune_unitigs(cfg_batch* b, cfg_batch_tuning* out) {
         if (ms < best.ms) { best = t; best.ms = ms; }
         if (G < 4) break;
     }
+    // table sizing from three quarters of the expected load (smaller tables, more CTAs
+    // per SM; a table that overflows sends its job back to the plain driver, which
+    // disqualifies the shape) to twice it
     const uint32_t Gbest = best.graph_count;
-    for (uint32_t d : {2u, 4u, 8u})
+    for (uint32_t d : {2u, 4u, 8u, 16u})
         for (uint32_t ct : {256u, 512u})
-            for (uint32_t ld : {base_load, base_load * 2}) {
+            for (uint32_t ld : {base_load * 3 / 4, base_load, base_load * 2}) {
                 cfg_batch_tuning t{d, ct, ld, Gbest, 0.f};
                 float ms = 0;
                 int rc = time_of(t, ms);

@@ -192,6 +192,8 @@ int subgraph_occupancy(int words, uint32_t cluster, uint32_t threads, uint32_t p
 void launch_bucket_scan_large(const unsigned long long* hist, uint32_t n, uint32_t* bucket_off, uint32_t* inst,
                               uint32_t* fill, uint32_t* partials, cudaStream_t s);
 uint32_t subgraph_max_per_cta(int words);      // one CTA owning a whole table
+// Largest CTA of a launch of `per`-slot tables (per 0: arena tables).
+uint32_t subgraph_max_threads(int words, uint32_t per);
 uint32_t subgraph_cluster_per_cta(int words);  // each CTA of a cluster
 
 }  // namespace cfg

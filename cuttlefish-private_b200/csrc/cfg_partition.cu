@@ -51,7 +51,8 @@ __device__ __forceinline__ uint64_t from_back(uint64_t cur, uint64_t prev, uint3
 }
 __device__ __forceinline__ uint64_t min64(uint64_t a, uint64_t b) { return a < b ? a : b; }
 
-constexpr int LEVELS = 6;   // sparse-table levels 2^0 .. 2^5 (w <= 62)
+// The sparse table's depth E = floor(log2 w) is a template argument: levels 2^0 .. 2^E,
+// none more (w <= 62: E <= 5).
 
 // Processes the (k-1)-mer positions [j0, j1) of one fragment: emits every weak
 // super k-mer whose run starts there.
@@ -64,9 +65,10 @@ constexpr int LEVELS = 6;   // sparse-table levels 2^0 .. 2^5 (w <= 62)
 // at position q - 2^i + 1 the minimum of the 2^i hashes starting there: the minimum of
 // the lane's own level i-1 value and that of the lane 2^(i-1) before it (for the first
 // lanes, from the previous chunk).  The window of (k-1)-mer j = q - w + 1 is then two
-// overlapping blocks of 2^e hashes, e = floor(log2 w): min(level_e[j], level_e[q-2^e+1]),
-// the second the lane's own value, the first that of the lane w - 2^e before it.
+// overlapping blocks of 2^E hashes, E = floor(log2 w): min(level_E[j], level_E[q-2^E+1]),
+// the second the lane's own value, the first that of the lane w - 2^E before it.
 // O(log w) work per position, no shared memory.
+template <int E>
 __device__ void sweep_fragment(const PartitionArgs& a, const uint8_t* mod_w, uint64_t F0, uint32_t FL,
                                uint32_t j0, uint32_t j1, unsigned long long* hist, Stage& st) {
     const uint32_t lane = threadIdx.x & 31;
@@ -74,26 +76,21 @@ __device__ void sweep_fragment(const PartitionArgs& a, const uint8_t* mod_w, uin
     const uint32_t M = FL - k + 2;                 // (k-1)-mers in the fragment
     const uint32_t n_lmers = FL - l + 1;
     const uint32_t start = j0 == 0 ? 0 : j0 - 1;   // position j0-1 only primes the change test
-    const uint32_t e = 31 - __clz(w), dq = w - (1u << e);
+    const uint32_t dq = w - (1u << E);
     // hash of l-mer q, or "none" (all ones, above every hash) outside the fragment
     auto hash_at = [&](int64_t q) -> uint64_t {
         return (q >= 0 && q < (int64_t)n_lmers) ? lmer_hash(lmer_at(a.packed, F0 + (uint64_t)q, l), l, a.seed0) : ~0ull;
     };
-    uint64_t lv[LEVELS], pv[LEVELS];   // this chunk's / the previous chunk's level values
+    uint64_t lv[E + 1], pv[E + 1];   // this chunk's / the previous chunk's level values
 #pragma unroll
-    for (int i = 0; i < LEVELS; ++i) pv[i] = ~0ull;
+    for (int i = 0; i <= E; ++i) pv[i] = ~0ull;
     auto levels = [&](uint64_t h) -> uint64_t {   // adds this chunk's hashes; the window minimum
         lv[0] = h;
 #pragma unroll
-        for (int i = 1; i < LEVELS; ++i)
-            lv[i] = (uint32_t)i <= e ? min64(lv[i - 1], from_back(lv[i - 1], pv[i - 1], 1u << (i - 1), lane)) : ~0ull;
-        uint64_t top = lv[0], ptop = pv[0];
+        for (int i = 1; i <= E; ++i) lv[i] = min64(lv[i - 1], from_back(lv[i - 1], pv[i - 1], 1u << (i - 1), lane));
+        const uint64_t m = min64(lv[E], from_back(lv[E], pv[E], dq, lane));
 #pragma unroll
-        for (int i = 1; i < LEVELS; ++i)
-            if ((uint32_t)i == e) { top = lv[i]; ptop = pv[i]; }
-        const uint64_t m = min64(top, from_back(top, ptop, dq, lane));
-#pragma unroll
-        for (int i = 0; i < LEVELS; ++i) pv[i] = lv[i];
+        for (int i = 0; i <= E; ++i) pv[i] = lv[i];
         return m;
     };
     // prime the levels with the chunks before the first (their newest hashes reach back to
@@ -198,6 +195,7 @@ __device__ void sweep_fragment(const PartitionArgs& a, const uint8_t* mod_w, uin
     }
 }
 
+template <int E>
 __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_partition(const PartitionArgs a) {
     __shared__ uint64_t stages[WARPS_PER_BLOCK][STAGE];
     __shared__ uint8_t mod_w[128];
@@ -229,7 +227,7 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_partition(const Partit
             const uint32_t j0 = s0 > F0 ? (uint32_t)(s0 - F0) : 0;
             const uint64_t e = s1 - F0;
             const uint32_t j1 = e < M ? (uint32_t)e : M;
-            if (j0 < j1) sweep_fragment(a, mod_w, F0, FL, j0, j1,
+            if (j0 < j1) sweep_fragment<E>(a, mod_w, F0, FL, j0, j1,
                                           a.hist ? a.hist + (a.frag_gbase ? a.frag_gbase[f] : 0u) : nullptr, st);
         }
     }
@@ -365,7 +363,15 @@ void launch_partition(const PartitionArgs& a, cudaStream_t s) {
     uint64_t blocks = (n_seg + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
     if (blocks > (1u << 20)) blocks = 1u << 20;
     if (blocks == 0) return;
-    k_partition<<<(unsigned)blocks, WARPS_PER_BLOCK * 32, 0, s>>>(a);
+    const dim3 grid((unsigned)blocks), block(WARPS_PER_BLOCK * 32);
+    switch (31 - __builtin_clz(a.w)) {   // floor(log2 w), w = k - l in [1, 62]
+        case 0: k_partition<0><<<grid, block, 0, s>>>(a); break;
+        case 1: k_partition<1><<<grid, block, 0, s>>>(a); break;
+        case 2: k_partition<2><<<grid, block, 0, s>>>(a); break;
+        case 3: k_partition<3><<<grid, block, 0, s>>>(a); break;
+        case 4: k_partition<4><<<grid, block, 0, s>>>(a); break;
+        default: k_partition<5><<<grid, block, 0, s>>>(a); break;
+    }
 }
 
 void launch_bucket_scan(const unsigned long long* hist, uint32_t G, uint32_t* bucket_off, uint32_t* inst,

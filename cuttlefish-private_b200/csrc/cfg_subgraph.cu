@@ -45,12 +45,21 @@ constexpr uint64_t BUSY = ~1ull;   // a two-word key's high word while its low w
 constexpr uint64_t ST_INIT = 0xffffffff00000000ull;   // a new slot's state: no edges, first occurrence "none"
 // walk termination kinds (Walk_Termination, include/Subgraph.hpp:362-369)
 constexpr uint32_t T_OK = 0, T_BRANCHED = 1, T_CROSSED = 2, T_DEAD = 3, T_EXIT = 4;
-// meta layout: bits 0-2 visited / disc front / disc back; 3 Q (self-looped homopolymer);
-// 4 isolated; 8-10 front termination; 11-13 back termination
-constexpr uint32_t M_Q = 8u, M_ISO = 16u;
+// meta layout: bits 0-2 visited / disc front / disc back; 3 isolated; 4-17 the front side
+// and 18-31 the back side.  A side is 1 | u << 1 | s_in << 13 when its walk step leads to
+// slot u, entered by side s_in (one-CTA tables of at most LINK_SLOTS slots: the walks
+// follow these links instead of looking the neighbour up again), else its termination
+// kind << 1 (T_OK, 0, for an unlinked side that continues).
+constexpr uint32_t M_ISO = 8u;
+constexpr uint32_t LINK_SLOTS = 4096;
 enum { LOCAL = 0, CLUSTER = 1, GLOBAL = 2 };
 
-__device__ __forceinline__ uint32_t term_of(uint32_t meta, int side) { return (meta >> (side == FRONT ? 8 : 11)) & 7; }
+__device__ __forceinline__ uint32_t side_field(uint32_t meta, int side) { return (meta >> (side == FRONT ? 4 : 18)) & 0x3FFFu; }
+__device__ __forceinline__ uint32_t side_bits(uint32_t field, int side) { return field << (side == FRONT ? 4 : 18); }
+__device__ __forceinline__ uint32_t term_of(uint32_t meta, int side) {
+    const uint32_t f = side_field(meta, side);
+    return (f & 1) ? T_OK : f >> 1;
+}
 __device__ __forceinline__ uint32_t compb(uint32_t b) { return b < 4 ? 3 - b : b; }
 __device__ __forceinline__ uint32_t st_ef(uint64_t st) { return (uint32_t)st; }
 __device__ __forceinline__ uint32_t st_ins(uint64_t st) { return (uint32_t)(st >> 32); }
@@ -428,6 +437,15 @@ __device__ __forceinline__ bool step_inline(const Tab<W, MODE>& T, const KOps<W>
 template <int W, int MODE>
 __device__ __forceinline__ bool step(const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t fth, DV<W>& v, int side, int& s_in) {
     return step_inline(T, ops, fth, v, side, s_in);
+}
+
+// A homopolymer b^k (b in {A, C}; x canonical) whose back side holds only its self-loop
+// and whose front side holds at most one edge: seeded on its own, the reference's walk
+// records it as a one-vertex cycle.
+template <int W>
+__device__ __forceinline__ bool looped_homopolymer(const KOps<W>& ops, const Kmer<W>& x, uint32_t ef, uint32_t fth) {
+    const uint32_t eb = ef_edge_at(ef, BACK, fth);
+    return eb < 2 && ef_count(ef, FRONT, fth) <= 1 && ops.is_homopolymer(x, eb);
 }
 
 // Bytes written one at a time in address order (rising or falling), gathered into
@@ -875,6 +893,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
     // ---------------- W1: termination of every side ----------------
     compact(per, wl, &B.wl_n, [&](uint32_t ls) { return !local_empty<W>(lkeys, ls); });
     __syncthreads();
+    const bool links = MODE == LOCAL && per <= LINK_SLOTS;
     uint32_t n_vert = 0, n_iso = 0, n_phantom = 0;   // this thread's vertices (summed once per warp)
     for (uint32_t i = tid, nw = B.wl_n; i < nw; i += nt) {
         const uint32_t ls = wl[i];
@@ -893,7 +912,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         const Kmer<W> xr = ops.rc(x);
         for (int side = 0; side < 2; ++side) {
             const uint32_t e = ef_edge_at(ef, side, fth);
-            uint32_t term = T_OK;
+            uint32_t term = T_OK, link = 0;
             if (e == BASE_N) term = T_BRANCHED;
             else if (e == BASE_E) term = (meta & (side == FRONT ? M_DISC_F : M_DISC_B)) ? T_EXIT : T_DEAD;
             else {
@@ -907,12 +926,10 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
                 if (u == NONE) { atomicOr(a.err, DERR_MISSING_KEY); term = T_CROSSED; }
                 else if (u == s) term = T_CROSSED;                                        // self-loop
                 else if (ef_count(st_ef(ust), s_in, fth) > 1) term = T_CROSSED;    // branching entrance
+                else if (links) link = 1u | (u << 1) | ((uint32_t)s_in << 13);
             }
-            meta |= term << (side == FRONT ? 8 : 11);
+            meta |= side_bits(link ? link : term << 1, side);
         }
-        // homopolymer b^k (b in {A, C}) whose back side holds only its self-loop
-        const uint32_t eb = ef_edge_at(ef, BACK, fth);
-        if (eb < 2 && cf <= 1 && ops.is_homopolymer(x, eb)) meta |= M_Q;
         lmeta[ls] = meta;
     }
     for (int d = 16; d; d >>= 1) {
@@ -957,7 +974,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
             const uint32_t meta = lmeta[ls];
             const bool okf = term_of(meta, FRONT) == T_OK, okb = term_of(meta, BACK) == T_OK;
             if (!okf && !okb) {         // one-vertex path
-                if (meta & M_Q) kc0 = true;
+                if (looped_homopolymer(ops, T.key(s), st_ef(lst[sti<W>(ls)]), fth)) kc0 = true;
                 else {
                     vs = dv_at(T, ops, s, BACK); ve = vs; sd0 = BACK; n2 = 1; path = true;
                     st = EndInfo{s, term_of(meta, FRONT), true}; en = EndInfo{s, term_of(meta, BACK), true};
@@ -985,23 +1002,36 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
                     }
                     vp_slot = v.slot; vp_side = side;
                     int s_in;
-                    if (!step(T, ops, fth, v, side, s_in)) { atomicOr(a.err, DERR_MISSING_KEY); ok = false; break; }
+                    uint32_t b;   // the base the step appends in walk direction
+                    if (links) {  // the neighbour W1 found: no lookup; v.d / v.r are rebuilt at the end
+                        const uint32_t f = side_field(cur_meta, side);
+                        const uint32_t e = ef_edge_at(st_ef(v.st), side, fth);
+                        b = side == BACK ? e : 3 - e;
+                        v.slot = (f >> 1) & (LINK_SLOTS - 1);
+                        s_in = (int)(f >> 13);
+                        v.st = T.ld_st(v.slot);
+                    } else {
+                        if (!step(T, ops, fth, v, side, s_in)) { atomicOr(a.err, DERR_MISSING_KEY); ok = false; break; }
+                        b = ops.last_base(v.d);
+                    }
                     side = 1 - s_in;
                     cur_meta = T.ld_meta(v.slot);
                     T.or_meta(v.slot, M_VISITED);
                     if (n <= STEP_BUF) {
-                        const unsigned long long bb = (unsigned long long)ops.last_base(v.d) << (2 * ((n - 1) & 31));
+                        const unsigned long long bb = (unsigned long long)b << (2 * ((n - 1) & 31));
                         if (n <= 32) steps0 |= bb; else steps1 |= bb;
                     }
                     if (n == 1) { v1_slot = v.slot; v1_side = side; }
                     if (++n > T.per * T.nranks + 1) { atomicOr(a.err, DERR_WALK_LIMIT); ok = false; break; }
                 }
+                if (links && ok && n > 1) v = dv_at(T, ops, v.slot, side);   // the end, leaving by `side`
                 if (ok && v.slot >= s) {   // the end with the smaller slot emits
                     e = v.slot;
                     const int e_side = side;   // the walk stops at e's side e_side
                     const uint32_t meta_e = cur_meta;
                     const uint32_t ins1 = st_ins(v.st);
-                    const bool q0 = meta & M_Q, q1 = meta_e & M_Q;
+                    const bool q0 = looped_homopolymer(ops, side0 == BACK ? v0.d : v0.r, st_ef(v0.st), fth);
+                    const bool q1 = looped_homopolymer(ops, side == BACK ? v.d : v.r, st_ef(v.st), fth);
                     uint32_t m = m_int;
                     if (!q0 && ins0 < m) m = ins0;
                     if (!q1 && ins1 < m) m = ins1;
@@ -1132,9 +1162,12 @@ __device__ __forceinline__ void carve(unsigned char* base, uint32_t per, unsigne
     wl = meta + per;
 }
 
-// One subgraph per CTA (per = the table's whole capacity) or per cluster.
-template <int W, int MODE>
-__global__ void __launch_bounds__(W == 1 ? 1024 : 512) k_subgraph_shared(const SubgraphArgs a) {
+// One subgraph per CTA (per = the table's whole capacity) or per cluster.  LB: the
+// largest CTA.  k > 32 (104 registers at LB 512) has a second form for tables of up to
+// 2048 slots, LB 256 at three CTAs per SM (80 registers): a 512-thread CTA of the wide
+// form holds a whole SM's registers, so one subgraph's phase barriers idle the SM.
+template <int W, int MODE, int LB>
+__global__ void __launch_bounds__(LB, LB <= 256 ? 3 : 1) k_subgraph_shared(const SubgraphArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ Block B;
     uint32_t rank = 0, nranks = 1;
@@ -1155,8 +1188,12 @@ __global__ void __launch_bounds__(W == 1 ? 1024 : 512) k_subgraph_shared(const S
         run_subgraph<W, MODE>(a, T, B, Bc, list[i], rank, nranks, per, lk, ls, lm, wl);
 }
 
+// Tables in the arena: no shared memory to share, so k > 32 runs three 256-thread CTAs
+// per SM (80 registers) instead of one of 512.
+template <int W> struct GlobalBounds { static constexpr int threads = 512, min_blocks = 2; };   // 64 registers
+template <> struct GlobalBounds<2> { static constexpr int threads = 256, min_blocks = 3; };     // 80 registers
 template <int W>
-__global__ void __launch_bounds__(512) k_subgraph_global(const SubgraphArgs a) {
+__global__ void __launch_bounds__(GlobalBounds<W>::threads, GlobalBounds<W>::min_blocks) k_subgraph_global(const SubgraphArgs a) {
     __shared__ Block B;
     const uint32_t lb = a.list_base ? *a.list_base : 0u;
     const uint32_t n = a.list_n ? *a.list_n : a.n_list;
@@ -1243,21 +1280,30 @@ __global__ void k_stripe_fixup(LmtigOut* lm, uint64_t lm_slice, const unsigned l
 }
 
 uint32_t subgraph_max_per_cta(int words) { return words == 1 ? 8192 : 4096; }
+uint32_t subgraph_max_threads(int words, uint32_t per) {
+    if (per == 0) return words == 1 ? 512 : 256;          // arena tables
+    if (words == 1) return per > 4096 ? 1024 : 512;
+    return per > 2048 ? 512 : 256;
+}
 uint32_t subgraph_cluster_per_cta(int words) { return words == 1 ? 4096 : 2048; }
 
 cudaError_t launch_subgraphs(const SubgraphArgs& a, int words, uint32_t cluster, uint32_t threads, cudaStream_t s) {
     if (a.n_list == 0) return cudaSuccess;
     if (cluster == 0) {   // global-memory tables
+        if (threads > subgraph_max_threads(words, 0)) return cudaErrorInvalidValue;
         if (words == 1) k_subgraph_global<1><<<a.n_list, threads, 0, s>>>(a);
         else k_subgraph_global<2><<<a.n_list, threads, 0, s>>>(a);
         return cudaGetLastError();
     }
     const size_t bytes = (size_t)a.smem_cap * slot_bytes(words);
-    if (cluster == 1)
-        return words == 1 ? launch_shared(k_subgraph_shared<1, LOCAL>, a, 1, threads, bytes, s, 0, max_table_bytes<1>())
-                          : launch_shared(k_subgraph_shared<2, LOCAL>, a, 1, threads, bytes, s, 0, max_table_bytes<2>());
+    if (threads > subgraph_max_threads(words, a.smem_cap)) return cudaErrorInvalidValue;
+    if (cluster == 1) {
+        if (words == 1) return launch_shared(k_subgraph_shared<1, LOCAL, 1024>, a, 1, threads, bytes, s, 0, max_table_bytes<1>());
+        return threads <= 256 ? launch_shared(k_subgraph_shared<2, LOCAL, 256>, a, 1, threads, bytes, s, 0, max_table_bytes<2>())
+                              : launch_shared(k_subgraph_shared<2, LOCAL, 512>, a, 1, threads, bytes, s, 0, max_table_bytes<2>());
+    }
     if (words != 1) return cudaErrorInvalidValue;   // k > 32 tables are one CTA's or the arena's
-    return launch_shared(k_subgraph_shared<1, CLUSTER>, a, cluster, threads, bytes, s, 0, max_table_bytes<1>());
+    return launch_shared(k_subgraph_shared<1, CLUSTER, 1024>, a, cluster, threads, bytes, s, 0, max_table_bytes<1>());
 }
 
 void launch_stripe_fixup(LmtigOut* lm, uint64_t lm_slice, const unsigned long long* lm_used,
@@ -1267,17 +1313,21 @@ void launch_stripe_fixup(LmtigOut* lm, uint64_t lm_slice, const unsigned long lo
 
 int subgraph_occupancy(int words, uint32_t cluster, uint32_t threads, uint32_t per) {
     const size_t bytes = (size_t)per * slot_bytes(words);
-    if (cluster <= 1)
-        return words == 1 ? occupancy_of(k_subgraph_shared<1, LOCAL>, 1, threads, bytes, max_table_bytes<1>())
-                          : occupancy_of(k_subgraph_shared<2, LOCAL>, 1, threads, bytes, max_table_bytes<2>());
+    if (threads > subgraph_max_threads(words, per)) return 0;
+    if (cluster <= 1) {
+        if (words == 1) return occupancy_of(k_subgraph_shared<1, LOCAL, 1024>, 1, threads, bytes, max_table_bytes<1>());
+        return threads <= 256 ? occupancy_of(k_subgraph_shared<2, LOCAL, 256>, 1, threads, bytes, max_table_bytes<2>())
+                              : occupancy_of(k_subgraph_shared<2, LOCAL, 512>, 1, threads, bytes, max_table_bytes<2>());
+    }
     if (words != 1) return 0;   // no cluster tables for k > 32
-    return occupancy_of(k_subgraph_shared<1, CLUSTER>, cluster, threads, bytes, max_table_bytes<1>());
+    return occupancy_of(k_subgraph_shared<1, CLUSTER, 1024>, cluster, threads, bytes, max_table_bytes<1>());
 }
 
 cudaError_t launch_subgraphs_persistent(const SubgraphArgs& a, int words, uint32_t cluster, uint32_t threads,
                                         uint32_t per, uint32_t grid, cudaStream_t s) {
     if (grid == 0) return cudaSuccess;
     if (cluster == 0) {
+        if (threads > subgraph_max_threads(words, 0)) return cudaErrorInvalidValue;
         if (words == 1) k_subgraph_global<1><<<grid, threads, 0, s>>>(a);
         else k_subgraph_global<2><<<grid, threads, 0, s>>>(a);
         return cudaGetLastError();
@@ -1285,11 +1335,14 @@ cudaError_t launch_subgraphs_persistent(const SubgraphArgs& a, int words, uint32
     SubgraphArgs b = a;
     b.smem_cap = per;
     const size_t bytes = (size_t)per * slot_bytes(words);
-    if (cluster == 1)
-        return words == 1 ? launch_shared(k_subgraph_shared<1, LOCAL>, b, 1, threads, bytes, s, grid)
-                          : launch_shared(k_subgraph_shared<2, LOCAL>, b, 1, threads, bytes, s, grid);
+    if (threads > subgraph_max_threads(words, per)) return cudaErrorInvalidValue;
+    if (cluster == 1) {
+        if (words == 1) return launch_shared(k_subgraph_shared<1, LOCAL, 1024>, b, 1, threads, bytes, s, grid);
+        return threads <= 256 ? launch_shared(k_subgraph_shared<2, LOCAL, 256>, b, 1, threads, bytes, s, grid)
+                              : launch_shared(k_subgraph_shared<2, LOCAL, 512>, b, 1, threads, bytes, s, grid);
+    }
     if (words != 1) return cudaErrorInvalidValue;   // no cluster tables for k > 32
-    return launch_shared(k_subgraph_shared<1, CLUSTER>, b, cluster, threads, bytes, s, grid);
+    return launch_shared(k_subgraph_shared<1, CLUSTER, 1024>, b, cluster, threads, bytes, s, grid);
 }
 
 }  // namespace cfg

@@ -270,6 +270,11 @@ class Compactor:
         rc = self.lib.cfg_submit_text(self.ctx, text, len(text))
         _check(self.lib, self.ctx, rc, "cfg_submit_text")
 
+    def submit_text_ptr(self, ptr: int, n: int):
+        """cfg_submit_text on `n` bytes of text at host address `ptr` (e.g. pinned memory)."""
+        rc = self.lib.cfg_submit_text(self.ctx, ctypes.cast(ptr, ctypes.c_char_p), n)
+        _check(self.lib, self.ctx, rc, "cfg_submit_text")
+
     def input_copy(self):
         """-> (words list, frag_off list, frag_len list) of the submitted input."""
         nb, nf = ctypes.c_uint64(), ctypes.c_uint64()
@@ -390,13 +395,16 @@ def unitig_multiset(fasta: bytes):
 
 
 def tune_graph_count(packed: PackedInput, k: int, l: int, cutoff: int, table_load_pct: int = 0, device: int = 0,
-                     candidates=(16384, 32768, 65536, 131072, 262144), runs: int = 2):
+                     candidates=None, runs: int = 2):
     """Subgraph count for the fastest plain run to final unitigs.
 
     The lm-tigs depend on the subgraph count, the final maximal unitigs do not: each
     candidate is timed (device time of cfg_run + cfg_unitigs, the best of `runs` warm
-    runs) and its unitigs are compared with the first candidate's.
+    runs) and its unitigs are compared with the first candidate's.  Default candidates:
+    16384 .. 262144, and 524288 for k > 32 (whose one-CTA tables hold half the slots).
     -> (best count, {count: ms}, unitigs identical for every candidate)."""
+    if candidates is None:
+        candidates = (16384, 32768, 65536, 131072, 262144) + ((524288,) if k > 32 else ())
     times, ref, same = {}, None, True
     for g in candidates:
         with Compactor(k, l, cutoff, g, device=device, table_load_pct=table_load_pct) as cx:

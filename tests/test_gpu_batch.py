@@ -201,7 +201,7 @@ def test_batch_tuned_graph_count_keeps_unitigs():
                 fa, nu = b.job_unitigs(j)
                 assert (orc.fasta_multiset(fa), nu) == expect[j], (G, j)
         t = b.tune_unitigs()
-        assert t.graph_count in (0, 1024, 4096)
+        assert t.graph_count in (0, 1024, 2048, 4096, 8192)   # 16384 (the params' count) reads as 0
         b.run()
         b.unitigs()
         for j in range(len(jobs)):
