@@ -460,7 +460,9 @@ def bench_serve(args, local, world):
         "server": {"slots": 4, "batch_max_bases": 64_000_000, "small_job_bases": 4_000_000,
                    "large_job_bases": 64 << 20, "large_slots": 2,
                    "batches": int(st.batches), "batched_jobs": int(st.batched_jobs),
-                   "max_running": int(st.max_running), "max_running_large": int(st.max_running_large)},
+                   "max_running": int(st.max_running), "max_running_large": int(st.max_running_large),
+                   "hbm_budget": int(st.hbm_budget), "contexts_created": int(st.contexts_created),
+                   "contexts_dropped": int(st.contexts_dropped)},
         "rates": rates, "generation_s": round(gen_s, 1),
     }
 

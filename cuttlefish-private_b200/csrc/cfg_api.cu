@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 using namespace cfg;
@@ -28,6 +29,13 @@ struct cfg_ctx {
 
     // input
     DevBuf packed, frag_off, frag_len, text;
+    // cfg_submit_packed copies the input in pieces on its own stream; the partition of a
+    // piece waits only for that piece's copies (no pieces: the input is already resident)
+    static constexpr int MAX_PIECES = 8;
+    struct Piece { uint64_t f0, f1, b0, b1; };
+    std::vector<Piece> pieces;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t piece_ev[MAX_PIECES] = {}, idle_ev = nullptr;
     ParseBuffers parse;
     const uint64_t* d_packed = nullptr; const uint64_t* d_frag_off = nullptr; const uint32_t* d_frag_len = nullptr;
     uint64_t n_bases = 0, n_frags = 0;
@@ -117,10 +125,20 @@ int run_partition(cfg_ctx* c, std::vector<uint32_t>& inst_h, std::vector<uint32_
         a.hist = nullptr;   // the bucket sort counts records and instances per subgraph
         a.err = &c->misc.as<MiscWords>()->err;
         CK(cudaEventRecord(c->ev[1], c->stream));
-        launch_partition(a, c->stream);
+        if (c->pieces.empty()) {
+            launch_partition(a, c->stream);
+            c->launches += 1;
+        } else {   // each piece of the input as soon as its copies have landed
+            for (size_t i = 0; i < c->pieces.size(); ++i) {
+                const cfg_ctx::Piece& pc = c->pieces[i];
+                CK(cudaStreamWaitEvent(c->stream, c->piece_ev[i], 0));
+                a.base0 = pc.b0; a.base1 = pc.b1; a.frag_lo = pc.f0; a.frag_hi = pc.f1;
+                launch_partition(a, c->stream);
+                c->launches += 1;
+            }
+        }
         CK(cudaGetLastError());
         CK(cudaEventRecord(c->ev[2], c->stream));
-        c->launches += 1;
         MiscWords m{};
         CK(cudaMemcpyAsync(&m, c->misc.p, sizeof(m), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
@@ -395,25 +413,44 @@ int cfg_create(int device, const cfg_params* params, cfg_ctx** out) {
     }
     c->stripes = std::min<uint32_t>(OUT_STRIPES, p.graph_count);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return CFG_ERR_CUDA; }
+    if (cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess) { cfg_destroy(c); return CFG_ERR_CUDA; }
     for (auto& e : c->ev)
         if (cudaEventCreate(&e) != cudaSuccess) { cfg_destroy(c); return CFG_ERR_CUDA; }
+    for (auto& e : c->piece_ev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) { cfg_destroy(c); return CFG_ERR_CUDA; }
+    if (cudaEventCreateWithFlags(&c->idle_ev, cudaEventDisableTiming) != cudaSuccess) { cfg_destroy(c); return CFG_ERR_CUDA; }
     *out = c;
     return CFG_OK;
 }
 
 static int check_frags(cfg_ctx* c, uint64_t n_bases, const uint64_t* frag_off, const uint32_t* frag_len, uint64_t n_frags) {
     if (n_bases >= (1ull << 32)) return fail(c, CFG_ERR_BAD_INPUT, "a job must hold fewer than 2^32 bases");
-    // one branch-free pass (10 M fragments in a few ms): back to back, each >= k+1 bases
-    uint64_t at = 0, bad_off = 0, bad_len = 0;
+    // back to back from 0 to n_bases, each >= k+1 bases: branch-free passes over slices of
+    // the table on up to 8 threads (10 M fragments in about a millisecond), each slice
+    // checking that every fragment starts where the one before it ends
     const uint32_t min_len = c->p.k + 1;
-    for (uint64_t i = 0; i < n_frags; ++i) {
-        bad_off |= frag_off[i] ^ at;
-        bad_len |= frag_len[i] < min_len;
-        at += frag_len[i];
-    }
-    if (bad_off) return fail(c, CFG_ERR_BAD_INPUT, "fragments must be back-to-back in input order");
-    if (bad_len) return fail(c, CFG_ERR_BAD_INPUT, "fragments must hold at least k+1 bases");
-    if (at != n_bases) return fail(c, CFG_ERR_BAD_INPUT, "fragment lengths do not sum to n_bases");
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned T = n_frags < (1u << 18) ? 1u : std::min(8u, hw);
+    std::vector<uint64_t> bad_off(T, 0), bad_len(T, 0);
+    auto slice = [&](unsigned t) {
+        const uint64_t i0 = n_frags * t / T, i1 = n_frags * (t + 1) / T;
+        uint64_t bo = 0, bl = 0;
+        for (uint64_t i = i0; i < i1; ++i) {
+            bo |= frag_off[i] ^ (i ? frag_off[i - 1] + frag_len[i - 1] : 0ull);
+            bl |= frag_len[i] < min_len;
+        }
+        bad_off[t] = bo; bad_len[t] = bl;
+    };
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < T; ++t) th.emplace_back(slice, t);
+    slice(0);
+    for (auto& x : th) x.join();
+    uint64_t bo = 0, bl = 0;
+    for (unsigned t = 0; t < T; ++t) { bo |= bad_off[t]; bl |= bad_len[t]; }
+    if (bo) return fail(c, CFG_ERR_BAD_INPUT, "fragments must be back-to-back in input order");
+    if (bl) return fail(c, CFG_ERR_BAD_INPUT, "fragments must hold at least k+1 bases");
+    if (n_frags ? frag_off[n_frags - 1] + frag_len[n_frags - 1] != n_bases : n_bases != 0)
+        return fail(c, CFG_ERR_BAD_INPUT, "fragment lengths do not sum to n_bases");
     return CFG_OK;
 }
 
@@ -427,19 +464,42 @@ int cfg_submit_packed(cfg_ctx* c, const uint64_t* packed, uint64_t n_bases, cons
         return fail(c, CFG_ERR_BAD_INPUT, "fragment lengths do not sum to n_bases");
     CK(cudaSetDevice(c->device));
     c->have_input = false; c->have_run = false;
+    c->pieces.clear();
     const uint64_t words = (n_bases + 31) / 32;
     if (!c->packed.ensure(8 * (words + 4)) || !c->frag_off.ensure(8 * (n_frags + 1)) || !c->frag_len.ensure(4 * (n_frags + 1)))
         return fail(c, CFG_ERR_OOM, "input buffers");
-    // the copies start first (asynchronous from pinned memory), the fragment table is
-    // checked on the host while they run; an invalid table leaves no input behind
-    CK(cudaMemsetAsync(c->packed.as<uint64_t>() + words, 0, 8 * 4, c->stream));   // the 4 padding words
-    if (words) CK(cudaMemcpyAsync(c->packed.p, packed, 8 * words, cudaMemcpyHostToDevice, c->stream));
-    if (n_frags) {
-        CK(cudaMemcpyAsync(c->frag_off.p, frag_off, 8 * n_frags, cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(c->frag_len.p, frag_len, 4 * n_frags, cudaMemcpyHostToDevice, c->stream));
+    // The copies start first (asynchronous from pinned memory) on the copy stream, after
+    // everything queued on the context's stream (the last run still reads the buffers),
+    // in pieces cut at fragment boundaries: cfg_run partitions each piece as soon as it
+    // has landed, so the copy of the rest overlaps the partition.  The fragment table is
+    // checked on the host while they run; an invalid table leaves no input behind.
+    CK(cudaEventRecord(c->idle_ev, c->stream));
+    CK(cudaStreamWaitEvent(c->copy_stream, c->idle_ev, 0));
+    CK(cudaMemsetAsync(c->packed.as<uint64_t>() + words, 0, 8 * 4, c->copy_stream));   // the 4 padding words
+    const int n_pieces = (n_bases >= (64ull << 20) && n_frags >= (uint64_t)cfg_ctx::MAX_PIECES) ? cfg_ctx::MAX_PIECES : 1;
+    for (int i = 0; i < n_pieces && n_frags; ++i) {
+        const uint64_t f0 = c->pieces.empty() ? 0 : c->pieces.back().f1;
+        // the first fragment starting at or past this piece's share of the bases
+        const uint64_t f1 = i + 1 == n_pieces ? n_frags
+                          : (uint64_t)(std::lower_bound(frag_off + f0, frag_off + n_frags, n_bases * (i + 1) / n_pieces) - frag_off);
+        if (f1 <= f0) continue;
+        const uint64_t b0 = frag_off[f0], b1 = f1 < n_frags ? frag_off[f1] : n_bases;
+        // the words holding bases [b0, b1); a word shared with the next piece is copied by
+        // both (the same bytes), so a piece never waits for its neighbour
+        const uint64_t w0 = b0 >> 5, w1 = (b1 + 31) >> 5;
+        CK(cudaMemcpyAsync(c->packed.as<uint64_t>() + w0, packed + w0, 8 * (w1 - w0), cudaMemcpyHostToDevice, c->copy_stream));
+        CK(cudaMemcpyAsync(c->frag_off.as<uint64_t>() + f0, frag_off + f0, 8 * (f1 - f0), cudaMemcpyHostToDevice, c->copy_stream));
+        CK(cudaMemcpyAsync(c->frag_len.as<uint32_t>() + f0, frag_len + f0, 4 * (f1 - f0), cudaMemcpyHostToDevice, c->copy_stream));
+        CK(cudaEventRecord(c->piece_ev[c->pieces.size()], c->copy_stream));
+        c->pieces.push_back(cfg_ctx::Piece{f0, f1, b0, b1});
     }
+    if (!n_frags && words) CK(cudaMemcpyAsync(c->packed.p, packed, 8 * words, cudaMemcpyHostToDevice, c->copy_stream));
     const int rc = check_frags(c, n_bases, frag_off, frag_len, n_frags);
-    if (rc) { cudaStreamSynchronize(c->stream); return rc; }   // the caller may free its buffers at once
+    if (rc) { cudaStreamSynchronize(c->copy_stream); c->pieces.clear(); return rc; }   // the caller may free its buffers at once
+    if (c->pieces.empty()) {   // no fragment: the context's stream still orders after the copies
+        CK(cudaEventRecord(c->idle_ev, c->copy_stream));
+        CK(cudaStreamWaitEvent(c->stream, c->idle_ev, 0));
+    }
     c->d_packed = c->packed.as<uint64_t>(); c->d_frag_off = c->frag_off.as<uint64_t>(); c->d_frag_len = c->frag_len.as<uint32_t>();
     c->n_bases = n_bases; c->n_frags = n_frags;
     c->have_input = true;
@@ -455,6 +515,7 @@ int cfg_submit_text(cfg_ctx* c, const char* text, uint64_t bytes) {
     const int fastq = i < bytes && text[i] == '@';
     if (!c->text.ensure(bytes + 16)) return fail(c, CFG_ERR_OOM, "text buffer");
     if (bytes) CK(cudaMemcpyAsync(c->text.p, text, bytes, cudaMemcpyHostToDevice, c->stream));
+    c->pieces.clear();
     const int rc = parse_text_device(c->text.as<uint8_t>(), bytes, fastq, c->p.k, c->parse, c->stream);
     if (rc == CFG_ERR_OOM) return fail(c, rc, "parse buffers");
     if (rc == CFG_ERR_BAD_INPUT) return fail(c, rc, "a job must hold fewer than 2^32 bases");
@@ -476,6 +537,7 @@ int cfg_copy_input(cfg_ctx* c, uint64_t* words, uint64_t* frag_off, uint32_t* fr
     if (!c) return CFG_ERR_BAD_INPUT;
     if (!c->have_input) return fail(c, CFG_ERR_STATE, "no input submitted");
     CK(cudaSetDevice(c->device));
+    if (!c->pieces.empty()) CK(cudaStreamWaitEvent(c->stream, c->piece_ev[c->pieces.size() - 1], 0));   // every piece landed
     const uint64_t w = (c->n_bases + 31) / 32;
     if (words && w) CK(cudaMemcpyAsync(words, c->d_packed, 8 * w, cudaMemcpyDeviceToHost, c->stream));
     if (frag_off && c->n_frags) CK(cudaMemcpyAsync(frag_off, c->d_frag_off, 8 * c->n_frags, cudaMemcpyDeviceToHost, c->stream));
@@ -490,6 +552,7 @@ int cfg_submit_packed_device(cfg_ctx* c, const uint64_t* d_packed, uint64_t n_ba
     if (n_bases >= (1ull << 32)) return fail(c, CFG_ERR_BAD_INPUT, "a job must hold fewer than 2^32 bases");
     c->d_packed = d_packed; c->d_frag_off = d_frag_off; c->d_frag_len = d_frag_len;
     c->n_bases = n_bases; c->n_frags = n_frags;
+    c->pieces.clear();
     c->have_input = true; c->have_run = false;
     return CFG_OK;
 }
@@ -692,6 +755,7 @@ void cfg_destroy(cfg_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     c->parse.release();
     c->ub.release();
     c->h_unitigs.release();
@@ -702,6 +766,9 @@ void cfg_destroy(cfg_ctx* c) {
     for (DevBuf* b : bufs) b->release();
     c->h_fasta.release(); c->h_lm_text.release(); c->h_lm.release();
     for (auto& e : c->ev) if (e) cudaEventDestroy(e);
+    for (auto& e : c->piece_ev) if (e) cudaEventDestroy(e);
+    if (c->idle_ev) cudaEventDestroy(c->idle_ev);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }

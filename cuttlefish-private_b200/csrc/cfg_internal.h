@@ -59,6 +59,10 @@ struct PartitionArgs {
     unsigned long long* hist;   // per subgraph: records (low 32) | instances (high 32); nullptr: not counted
     uint32_t* err;
     const uint32_t* frag_gbase; // batch: first histogram entry of each fragment's job (nullptr: 0)
+    // this launch's share of the input: the stream bases [base0, base1) and the fragments
+    // [frag_lo, frag_hi) that tile them (base1 == 0: the whole input, every fragment).  A
+    // job whose input arrives in pieces partitions each piece as soon as it has landed.
+    uint64_t base0, base1, frag_lo, frag_hi;
 };
 
 struct ScatterArgs {

@@ -202,18 +202,22 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_partition(const Partit
     if (threadIdx.x < 128) mod_w[threadIdx.x] = (uint8_t)(threadIdx.x % a.w);
     __syncthreads();
     Stage st{stages[threadIdx.x >> 5], 0};
-    const uint64_t n_seg = (a.n_bases + a.seg - 1) / a.seg;
+    // this launch's bases and fragments (the fragment table is read only inside them:
+    // the entries of other pieces may not have landed yet)
+    const uint64_t b0 = a.base1 ? a.base0 : 0, b1 = a.base1 ? a.base1 : a.n_bases;
+    const uint64_t f_lo = a.base1 ? a.frag_lo : 0, f_hi = a.base1 ? a.frag_hi : a.n_frags;
+    const uint64_t n_seg = (b1 - b0 + a.seg - 1) / a.seg;
     const uint64_t warp0 = (uint64_t)blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5);
     const uint64_t n_warps = (uint64_t)gridDim.x * WARPS_PER_BLOCK;
     for (uint64_t sgi = warp0; sgi < n_seg; sgi += n_warps) {
-        const uint64_t s0 = sgi * a.seg, s1 = min(s0 + a.seg, a.n_bases);
+        const uint64_t s0 = b0 + sgi * a.seg, s1 = min(s0 + a.seg, b1);
         // last fragment starting at or before s0
-        uint64_t lo = 0, hi = a.n_frags;
+        uint64_t lo = f_lo, hi = f_hi;
         while (hi - lo > 1) {
             const uint64_t mid = (lo + hi) >> 1;
             if (a.frag_off[mid] <= s0) lo = mid; else hi = mid;
         }
-        for (uint64_t f = lo; f < a.n_frags; ++f) {
+        for (uint64_t f = lo; f < f_hi; ++f) {
             const uint64_t F0 = a.frag_off[f];
             if (F0 >= s1) break;
             const uint32_t FL = a.frag_len[f];
@@ -359,7 +363,7 @@ __global__ void k_scatter(const ScatterArgs a) {
 }  // namespace
 
 void launch_partition(const PartitionArgs& a, cudaStream_t s) {
-    const uint64_t n_seg = (a.n_bases + a.seg - 1) / a.seg;
+    const uint64_t n_seg = ((a.base1 ? a.base1 - a.base0 : a.n_bases) + a.seg - 1) / a.seg;
     uint64_t blocks = (n_seg + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
     if (blocks > (1u << 20)) blocks = 1u << 20;
     if (blocks == 0) return;

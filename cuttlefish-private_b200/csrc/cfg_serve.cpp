@@ -165,6 +165,7 @@ void make_room(cfg_server* s, uint64_t need) {
         if (!victim) return;
         s->held_bytes -= victim->bytes;
         cfg_destroy(victim->c);
+        ++s->st.contexts_dropped;
         s->ctxs.erase(std::find_if(s->ctxs.begin(), s->ctxs.end(), [&](auto& x) { return x.get() == victim; }));
     }
 }
@@ -179,10 +180,12 @@ void run_plain(cfg_server* s, Ticket* t, uint64_t need) {
             if (!ctx || (ctx->bytes < need && c->bytes > ctx->bytes) || (c->bytes >= need && c->bytes < ctx->bytes)) ctx = c.get();
         }
         if (ctx) {
+            ctx->busy = true;   // before make_room, which drops idle contexts: never this one
             if (need > ctx->bytes) { make_room(s, need - ctx->bytes); s->held_bytes += need - ctx->bytes; ctx->bytes = need; }
         } else {
             make_room(s, need);
             s->ctxs.emplace_back(new Ctx());
+            ++s->st.contexts_created;
             ctx = s->ctxs.back().get();
             ctx->p = t->p; ctx->bytes = need;
             s->held_bytes += need;

@@ -90,7 +90,7 @@ class JobTiming(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in (
         "submitted", "completed", "failed", "batches", "batched_jobs", "max_running", "bases", "held_bytes",
-        "hbm_budget", "max_running_large")]
+        "hbm_budget", "max_running_large", "contexts_created", "contexts_dropped")]
 
 
 class BatchStats(ctypes.Structure):

@@ -129,7 +129,11 @@ int cfg_create(int device, const cfg_params* params, cfg_ctx** out);
  * fragments: maximal ACGT runs of at least k+1 bases, frag_off[i] their first
  * base in the stream, frag_len[i] their length, in input order and
  * back-to-back (frag_off[i+1] == frag_off[i] + frag_len[i]).  The stream must
- * hold fewer than 2^32 bases.  Copies to the device on the context's stream.
+ * hold fewer than 2^32 bases.  Starts the copies to the device and returns once the
+ * fragment table is checked: the copies run on a copy stream of the context, in pieces
+ * cut at fragment boundaries, and cfg_run partitions each piece as soon as it has
+ * landed.  The three buffers must stay valid and unchanged until cfg_run returns
+ * (pinned memory lets the copies run asynchronously).
  * Replaces the input side of Graph_Partitioner::partition
  * (src/Graph_Partitioner.cpp:120-185,461-501). */
 int cfg_submit_packed(cfg_ctx* ctx, const uint64_t* packed, uint64_t n_bases,
@@ -336,6 +340,7 @@ typedef struct cfg_server_stats {
     uint64_t submitted, completed, failed, batches, batched_jobs, max_running, bases;
     uint64_t held_bytes, hbm_budget;
     uint64_t max_running_large;   /* most large jobs seen running at once */
+    uint64_t contexts_created, contexts_dropped;   /* plain contexts made, and freed to fit the budget */
 } cfg_server_stats;
 
 int cfg_server_create(int device, const cfg_server_config* config, cfg_server** out);
