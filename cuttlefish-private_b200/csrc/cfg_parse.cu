@@ -37,6 +37,35 @@ struct Fsm {
     uint32_t n, start;
 };
 
+// The tables of an FSM of at most 5 states packed into registers: entry (class c, state s)
+// at index i = 5 c + s, its next state in 3 bits (bits 3i.. of nx_lo for i < 21, of nx_hi
+// above) and its emission in 2 bits of em.  A lookup is a few shifts on values every
+// thread holds, where an indexed table (in the kernel's parameters or in memory) would
+// serialise the warp's lanes over their distinct (state, class) pairs.
+struct FsmBits {
+    unsigned long long nx_lo, nx_hi, em;
+    uint32_t n, start;
+};
+__device__ __forceinline__ uint32_t fsm_next(const FsmBits& f, uint32_t st, uint32_t cl) {
+    const uint32_t i = 5 * cl + st;
+    return i < 21 ? (uint32_t)(f.nx_lo >> (3 * i)) & 7u : (uint32_t)(f.nx_hi >> (3 * (i - 21))) & 7u;
+}
+__device__ __forceinline__ uint32_t fsm_emit(const FsmBits& f, uint32_t st, uint32_t cl) {
+    return (uint32_t)(f.em >> (2 * (5 * cl + st))) & 3u;
+}
+FsmBits pack_fsm(const Fsm& m) {
+    FsmBits b{};
+    b.n = m.n; b.start = m.start;
+    for (uint32_t c = 0; c < NCLASS; ++c)
+        for (uint32_t st = 0; st < m.n; ++st) {
+            const uint32_t i = 5 * c + st;
+            if (i < 21) b.nx_lo |= (unsigned long long)m.next[st][c] << (3 * i);
+            else b.nx_hi |= (unsigned long long)m.next[st][c] << (3 * (i - 21));
+            b.em |= (unsigned long long)m.emit[st][c] << (2 * i);
+        }
+    return b;
+}
+
 __device__ __forceinline__ uint32_t byte_class(uint32_t c) {
     if (c == '\n') return C_NL;
     if (c == '>') return C_GT;
@@ -65,7 +94,7 @@ __host__ __device__ __forceinline__ uint32_t identity(uint32_t n) {
 struct ParseArgs {
     const uint8_t* text;
     uint64_t bytes, n_chunks;
-    Fsm fsm;
+    FsmBits fsm;
     uint32_t* chunk_f;             // A: transfer function; B: start state
     unsigned long long* chunk_b;   // C: bases; D: bases before the chunk
     unsigned long long* chunk_k;   // C: breaks; D: breaks before the chunk
@@ -94,7 +123,7 @@ __device__ __forceinline__ uint32_t thread_transfer(const ParseArgs& a, const ui
         uint32_t st = s;
 #pragma unroll
         for (int i = 0; i < BPT; ++i)
-            if ((uint32_t)i < nb) st = a.fsm.next[st][byte_class(v[i])];
+            if ((uint32_t)i < nb) st = fsm_next(a.fsm, st, byte_class(v[i]));
         f |= st << (3 * s);
     }
     return f;
@@ -184,9 +213,9 @@ __device__ __forceinline__ void thread_counts(const ParseArgs& a, const ThreadPo
     for (int i = 0; i < BPT; ++i) {
         if ((uint32_t)i >= tp.nb) break;
         const uint32_t cl = byte_class(tp.v[i]);
-        const uint32_t e = a.fsm.emit[st][cl];
+        const uint32_t e = fsm_emit(a.fsm, st, cl);
         nb += e == E_BASE; nk += e == E_BREAK;
-        st = a.fsm.next[st][cl];
+        st = fsm_next(a.fsm, st, cl);
     }
 }
 
@@ -267,13 +296,14 @@ __global__ void __launch_bounds__(TPB) k_parse_breaks(ParseArgs a) {
         block_sum2(nb, nk, sh, eb, ek, tb, tk);
         unsigned long long r = a.chunk_b[c] + eb, kk = a.chunk_k[c] + ek;
         uint32_t st = tp.state;
+#pragma unroll
         for (int i = 0; i < BPT; ++i) {
             if ((uint32_t)i >= tp.nb) break;
             const uint32_t cl = byte_class(tp.v[i]);
-            const uint32_t e = a.fsm.emit[st][cl];
+            const uint32_t e = fsm_emit(a.fsm, st, cl);
             if (e == E_BASE) ++r;
             else if (e == E_BREAK) a.brk_rank[kk++] = r;
-            st = a.fsm.next[st][cl];
+            st = fsm_next(a.fsm, st, cl);
         }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) a.brk_rank[a.chunk_k[a.n_chunks]] = a.chunk_b[a.n_chunks];
@@ -394,10 +424,11 @@ __global__ void __launch_bounds__(TPB) k_parse_pack(ParseArgs a) {
         unsigned long long r = a.chunk_b[c] + eb, kk = a.chunk_k[c] + ek;
         uint32_t st = tp.state;
         uint64_t word = ~0ull, acc = 0;
+#pragma unroll
         for (int i = 0; i < BPT; ++i) {
             if ((uint32_t)i >= tp.nb) break;
             const uint32_t ch = tp.v[i], cl = byte_class(ch);
-            const uint32_t e = a.fsm.emit[st][cl];
+            const uint32_t e = fsm_emit(a.fsm, st, cl);
             if (e == E_BASE) {
                 const unsigned long long o = a.frag_out[kk];
                 if (o != ~0ull) {
@@ -413,7 +444,7 @@ __global__ void __launch_bounds__(TPB) k_parse_pack(ParseArgs a) {
             } else if (e == E_BREAK) {
                 ++kk;
             }
-            st = a.fsm.next[st][cl];
+            st = fsm_next(a.fsm, st, cl);
         }
         if (word != ~0ull) atomicOr((unsigned long long*)a.packed + word, (unsigned long long)acc);
     }
@@ -460,7 +491,7 @@ int parse_text_device(const uint8_t* d_text, uint64_t bytes, int fastq, uint32_t
     ParseArgs a{};
     a.text = d_text; a.bytes = bytes;
     a.n_chunks = (bytes + CHUNK - 1) / CHUNK;
-    a.fsm = fastq ? fastq_fsm() : fasta_fsm();
+    a.fsm = pack_fsm(fastq ? fastq_fsm() : fasta_fsm());
     const uint64_t nc = a.n_chunks;
     if (!pb.ensure_chunks(nc + 1)) return CFG_ERR_OOM;
     a.chunk_f = pb.chunk_f; a.chunk_b = pb.chunk_b; a.chunk_k = pb.chunk_k;
