@@ -125,7 +125,14 @@ int run_partition(cfg_ctx* c, std::vector<uint32_t>& inst_h, std::vector<uint32_
         a.hist = nullptr;   // the bucket sort counts records and instances per subgraph
         a.err = &c->misc.as<MiscWords>()->err;
         CK(cudaEventRecord(c->ev[1], c->stream));
-        if (c->pieces.empty()) {
+        // input still in flight: a launch per piece as it lands; all landed: one launch
+        bool landed = c->pieces.empty();
+        if (!landed) {
+            const cudaError_t q = cudaEventQuery(c->piece_ev[c->pieces.size() - 1]);
+            if (q != cudaSuccess && q != cudaErrorNotReady) return cuda_fail(c, q, "cudaEventQuery");
+            landed = q == cudaSuccess;
+        }
+        if (landed) {
             launch_partition(a, c->stream);
             c->launches += 1;
         } else {   // each piece of the input as soon as its copies have landed

@@ -12,7 +12,8 @@
 // a base, or a break (a non-ACGT character, a record boundary).  The state at
 // each 4 KiB chunk is found by composing the chunks' state-transfer functions
 // (a scan), so every chunk runs independently:
-//   A  transfer function of every chunk            B  scan: each chunk's start state
+//   A  transfer function of every chunk (and of every thread's bytes before it, kept
+//      for C, E and G)                              B  scan: each chunk's start state
 //   C  bases and breaks of every chunk             D  scan: each chunk's offsets
 //   E  the base rank of every break                F  fragments: lengths, keep, offsets
 //   G  bases written 2 bits each into the packed stream.
@@ -44,6 +45,11 @@ struct Fsm {
 // serialise the warp's lanes over their distinct (state, class) pairs.
 struct FsmBits {
     unsigned long long nx_lo, nx_hi, em;
+    // class c's whole next-state map as a transfer function (3 bits per state): bits 15c..
+    // of cf_lo for c < 4, cf_hi for c = 4; idem bit c: that map is idempotent (a run of
+    // class-c bytes acts as one)
+    unsigned long long cf_lo;
+    uint32_t cf_hi, idem;
     uint32_t n, start;
 };
 __device__ __forceinline__ uint32_t fsm_next(const FsmBits& f, uint32_t st, uint32_t cl) {
@@ -56,14 +62,24 @@ __device__ __forceinline__ uint32_t fsm_emit(const FsmBits& f, uint32_t st, uint
 FsmBits pack_fsm(const Fsm& m) {
     FsmBits b{};
     b.n = m.n; b.start = m.start;
-    for (uint32_t c = 0; c < NCLASS; ++c)
+    for (uint32_t c = 0; c < NCLASS; ++c) {
+        uint32_t F = 0;
+        bool idem = true;
         for (uint32_t st = 0; st < m.n; ++st) {
             const uint32_t i = 5 * c + st;
             if (i < 21) b.nx_lo |= (unsigned long long)m.next[st][c] << (3 * i);
             else b.nx_hi |= (unsigned long long)m.next[st][c] << (3 * (i - 21));
             b.em |= (unsigned long long)m.emit[st][c] << (2 * i);
+            F |= (uint32_t)m.next[st][c] << (3 * st);
+            idem = idem && m.next[m.next[st][c]][c] == m.next[st][c];
         }
+        if (c < 4) b.cf_lo |= (unsigned long long)F << (15 * c); else b.cf_hi = F;
+        if (idem) b.idem |= 1u << c;
+    }
     return b;
+}
+__device__ __forceinline__ uint32_t class_fn(const FsmBits& f, uint32_t cl) {
+    return cl < 4 ? (uint32_t)(f.cf_lo >> (15 * cl)) & 0x7FFFu : f.cf_hi;
 }
 
 __device__ __forceinline__ uint32_t byte_class(uint32_t c) {
@@ -96,6 +112,7 @@ struct ParseArgs {
     uint64_t bytes, n_chunks;
     FsmBits fsm;
     uint32_t* chunk_f;             // A: transfer function; B: start state
+    uint16_t* thread_f;            // A: per thread, the chunk's function before the thread's bytes
     unsigned long long* chunk_b;   // C: bases; D: bases before the chunk
     unsigned long long* chunk_k;   // C: breaks; D: breaks before the chunk
     unsigned long long* brk_rank;  // E: bases before break i (NB + 1 entries)
@@ -117,14 +134,16 @@ __device__ __forceinline__ void load_bytes(const ParseArgs& a, uint64_t chunk, u
     }
 }
 
+// The transfer function of a thread's bytes: the class maps composed in byte order, a run
+// of one idempotent class composed once (text is mostly runs of bases or quality letters).
 __device__ __forceinline__ uint32_t thread_transfer(const ParseArgs& a, const uint8_t (&v)[BPT], uint32_t nb) {
-    uint32_t f = 0;
-    for (uint32_t s = 0; s < a.fsm.n; ++s) {
-        uint32_t st = s;
+    uint32_t f = identity(a.fsm.n), prev = NCLASS;
 #pragma unroll
-        for (int i = 0; i < BPT; ++i)
-            if ((uint32_t)i < nb) st = fsm_next(a.fsm, st, byte_class(v[i]));
-        f |= st << (3 * s);
+    for (int i = 0; i < BPT; ++i) {
+        if ((uint32_t)i >= nb) break;
+        const uint32_t cl = byte_class(v[i]);
+        if (cl != prev || !((a.fsm.idem >> cl) & 1)) f = compose(f, class_fn(a.fsm, cl), a.fsm.n);
+        prev = cl;
     }
     return f;
 }
@@ -166,7 +185,8 @@ __global__ void __launch_bounds__(TPB) k_parse_transfer(ParseArgs a) {
         uint8_t v[BPT];
         load_bytes(a, c, v);
         const uint32_t f = thread_transfer(a, v, bytes_of_thread(a, c));
-        block_scan_f(f, a.fsm.n, sh);
+        const uint32_t ex = block_scan_f(f, a.fsm.n, sh);
+        a.thread_f[c * TPB + threadIdx.x] = (uint16_t)ex;
         if (threadIdx.x == 0) a.chunk_f[c] = sh[TPB / 32];
         __syncthreads();
     }
@@ -198,12 +218,10 @@ __global__ void __launch_bounds__(1024) k_parse_states(ParseArgs a) {
 // Each thread's start state and its class counts, from the chunk's start state.
 struct ThreadPos { uint32_t state; uint8_t v[BPT]; uint32_t nb; };
 
-__device__ __forceinline__ void thread_start(const ParseArgs& a, uint64_t c, ThreadPos& tp, uint32_t* sh) {
+__device__ __forceinline__ void thread_start(const ParseArgs& a, uint64_t c, ThreadPos& tp, uint32_t*) {
     load_bytes(a, c, tp.v);
     tp.nb = bytes_of_thread(a, c);
-    const uint32_t f = thread_transfer(a, tp.v, tp.nb);
-    const uint32_t ex = block_scan_f(f, a.fsm.n, sh);
-    tp.state = f_at(ex, a.chunk_f[c]);
+    tp.state = f_at(a.thread_f[c * TPB + threadIdx.x], a.chunk_f[c]);   // pass A's prefix from B's start state
 }
 
 __device__ __forceinline__ void thread_counts(const ParseArgs& a, const ThreadPos& tp, uint32_t& nb, uint32_t& nk) {
@@ -494,7 +512,7 @@ int parse_text_device(const uint8_t* d_text, uint64_t bytes, int fastq, uint32_t
     a.fsm = pack_fsm(fastq ? fastq_fsm() : fasta_fsm());
     const uint64_t nc = a.n_chunks;
     if (!pb.ensure_chunks(nc + 1)) return CFG_ERR_OOM;
-    a.chunk_f = pb.chunk_f; a.chunk_b = pb.chunk_b; a.chunk_k = pb.chunk_k;
+    a.chunk_f = pb.chunk_f; a.chunk_b = pb.chunk_b; a.chunk_k = pb.chunk_k; a.thread_f = pb.thread_f;
     const unsigned grid = (unsigned)std::min<uint64_t>(std::max<uint64_t>(nc, 1), 148ull * 16);
     if (nc) {
         k_parse_transfer<<<grid, TPB, 0, s>>>(a);

@@ -324,7 +324,7 @@ struct Block {   // per-CTA shared bookkeeping (in CLUSTER mode the flags of ran
     uint32_t inserted, overflow, wl_n, covered;   // covered: vertices of the paths and one-k-mer cycles emitted
     unsigned long long vertices, isolated, phantom, trivial, icc, lmtig;
     Sink sk;
-    uint32_t wsum[32];   // per-warp partial sums of a block scan (<= 1024 threads)
+    unsigned long long rs[3][32];   // reserve_block: per-warp totals (<= 1024 threads), then their offsets
 };
 
 constexpr uint32_t FULL = 0xffffffffu;
@@ -355,6 +355,34 @@ __device__ __forceinline__ Res reserve_warp(const Sink& sk, unsigned long long f
     }
     ba = __shfl_sync(FULL, ba, 0); bb = __shfl_sync(FULL, bb, 0); bc = __shfl_sync(FULL, bc, 0);
     return Res{ba + a - fa, bb + b - nlm, bc + c - lmb};
+}
+
+// The same for the whole CTA: one atomic per kind and CTA (the cursors are shared by
+// every subgraph of a job, or of an output stripe, that runs at the same time).  Every
+// thread of the CTA must call it.
+__device__ __forceinline__ Res reserve_block(const Sink& sk, Block& B, unsigned long long fa, uint32_t nlm,
+                                             unsigned long long lmb) {
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    unsigned long long a = fa, c = lmb, b = nlm;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const unsigned long long x = __shfl_up_sync(FULL, a, d), y = __shfl_up_sync(FULL, b, d), z = __shfl_up_sync(FULL, c, d);
+        if (lane >= (uint32_t)d) { a += x; b += y; c += z; }
+    }
+    if (lane == 31) { B.rs[0][wid] = a; B.rs[1][wid] = b; B.rs[2][wid] = c; }
+    __syncthreads();
+    if (threadIdx.x < 3) {   // thread q: kind q's warp totals into offsets, one atomic
+        unsigned long long* r = B.rs[threadIdx.x];
+        unsigned long long run = 0;
+        for (uint32_t w = 0; w < nw; ++w) { const unsigned long long t = r[w]; r[w] = run; run += t; }
+        unsigned long long* cur = threadIdx.x == 0 ? sk.fasta_cur : threadIdx.x == 1 ? sk.lm_cur : sk.lm_text_cur;
+        const unsigned long long base = run ? atomicAdd(cur, run) : 0ull;
+        for (uint32_t w = 0; w < nw; ++w) r[w] += base;
+    }
+    __syncthreads();
+    const Res out{B.rs[0][wid] + a - fa, B.rs[1][wid] + b - nlm, B.rs[2][wid] + c - lmb};
+    __syncthreads();   // the offsets are read before the next reservation overwrites them
+    return out;
 }
 
 // The L bases of a reserved FASTA record ">0\n...\n" at offset o, or nullptr past the arena.
@@ -1057,7 +1085,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         }
         const uint32_t L = path ? n2 + k - 1 : 0;
         __syncwarp();
-        const Res r = reserve_warp(B.sk, (kc0 ? k + 4 : 0) + (kc1 ? k + 4 : 0) + (path && !lm ? L + 4 : 0),
+        const Res r = reserve_block(B.sk, B, (kc0 ? k + 4 : 0) + (kc1 ? k + 4 : 0) + (path && !lm ? L + 4 : 0),
                                    path && lm ? 1u : 0u, path && lm ? L : 0u);
         unsigned long long fo = r.fa;
         if (kc0) { write_kmer_cycle(T, ops, s, B, fo); fo += k + 4; }
