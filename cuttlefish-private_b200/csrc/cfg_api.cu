@@ -300,7 +300,8 @@ int run_subgraphs(cfg_ctx* c, const std::vector<uint32_t>& inst_h) {
             for (uint32_t g : work) {
                 const uint64_t w = cur_want[g];
                 uint32_t cl, per;
-                if (w <= per_max) { cl = 1; per = next_pow2(w); }
+                uint32_t lc = 0;   // one-CTA table class
+                if (w <= per_max) { cl = 1; while (local_per(lc) < w) ++lc; per = local_per(lc); }
                 else if (w <= (uint64_t)per_cl * max_cluster) { cl = (uint32_t)((w + per_cl - 1) / per_cl); per = per_cl; }
                 else {
                     const uint32_t cap = next_pow2(w);
@@ -309,7 +310,7 @@ int run_subgraphs(cfg_ctx* c, const std::vector<uint32_t>& inst_h) {
                     continue;
                 }
                 // launch of this shape: one per (cluster size, log2 slots)
-                const uint32_t sk = cl * 32 + (31 - __builtin_clz(per));
+                const uint32_t sk = cl == 1 ? 32 + lc : cl * 32 + (31 - __builtin_clz(per));
                 if (shape_at[sk] < 0) {
                     shape_at[sk] = (int)plan.size();
                     plan.emplace_back(); plan.back().per = per; plan.back().cluster = cl;
