@@ -46,7 +46,7 @@ struct cfg_ctx {
     // plan
     DevBuf list, tab_off, tab_cap, arena;
     // outputs
-    DevBuf fasta, lm_text, lm, dump, retry, counters, stripe_cur, stripe_base, ut_lmbase, cyc_lm, cyc_text, cyc_cnt;
+    DevBuf fasta, lm_text, lm, dump, retry, counters, stripe_cur, stripe_base, ut_lmbase, cyc_work, cyc_scratch, cyc_out;
     UnitigBuffers ub;
     HostBuf h_unitigs;
     uint64_t fasta_cap = 0, lm_text_cap = 0, lm_cap = 0, dump_cap = 0;   // per output stripe
@@ -300,8 +300,7 @@ int run_subgraphs(cfg_ctx* c, const std::vector<uint32_t>& inst_h) {
             for (uint32_t g : work) {
                 const uint64_t w = cur_want[g];
                 uint32_t cl, per;
-                uint32_t lc = 0;   // one-CTA table class
-                if (w <= per_max) { cl = 1; while (local_per(lc) < w) ++lc; per = local_per(lc); }
+                if (w <= per_max) { cl = 1; per = next_pow2(w); }
                 else if (w <= (uint64_t)per_cl * max_cluster) { cl = (uint32_t)((w + per_cl - 1) / per_cl); per = per_cl; }
                 else {
                     const uint32_t cap = next_pow2(w);
@@ -310,7 +309,7 @@ int run_subgraphs(cfg_ctx* c, const std::vector<uint32_t>& inst_h) {
                     continue;
                 }
                 // launch of this shape: one per (cluster size, log2 slots)
-                const uint32_t sk = cl == 1 ? 32 + lc : cl * 32 + (31 - __builtin_clz(per));
+                const uint32_t sk = cl * 32 + (31 - __builtin_clz(per));
                 if (shape_at[sk] < 0) {
                     shape_at[sk] = (int)plan.size();
                     plan.emplace_back(); plan.back().per = per; plan.back().cluster = cl;
@@ -670,7 +669,7 @@ int cfg_unitigs(cfg_ctx* c, const char** fasta, uint64_t* bytes, uint64_t* n_uni
     const cfg_counts& n = c->counts;
     unsigned long long lb[OUT_STRIPES], acc = 0;
     for (uint32_t st = 0; st < OUT_STRIPES; ++st) { lb[st] = acc; acc += c->s_lm[st]; }
-    if (!c->ut_lmbase.ensure(sizeof(lb)) || !c->cyc_cnt.ensure(16)) return fail(c, CFG_ERR_OOM, "collation buffers");
+    if (!c->ut_lmbase.ensure(sizeof(lb)) || !c->cyc_out.ensure(16)) return fail(c, CFG_ERR_OOM, "collation buffers");
     CK(cudaMemcpyAsync(c->ut_lmbase.p, lb, sizeof(lb), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(&c->misc.as<MiscWords>()->err, 0, sizeof(uint32_t), c->stream));
     CK(cudaEventRecord(c->ev[0], c->stream));
@@ -691,38 +690,20 @@ int cfg_unitigs(cfg_ctx* c, const char** fasta, uint64_t* bytes, uint64_t* n_uni
     CK(cudaStreamSynchronize(c->stream));
     if (m.err & DERR_BAD_GRAPH) return fail(c, CFG_ERR_STATE, "lm-tig ends do not form a valid discontinuity graph");
     if (m.err & DERR_WALK_LIMIT) return fail(c, CFG_ERR_WALK_LIMIT, "lm-tig ranking exceeded its bound");
-    // lm-tigs on closed chains: joined on the host (they need the rotation rule)
-    std::string cyc_fa;
-    uint64_t cyc_units = 0;
+    // lm-tigs on closed chains: joined into cycles on the device, rotated to their canonical start
+    uint64_t cyc_bytes = 0, cyc_units = 0;
     if (res.n_cycle_lmtigs) {
-        unsigned long long cnt[2] = {0, 0};
-        CK(cudaMemsetAsync(c->cyc_cnt.p, 0, 16, c->stream));
-        rc = collate_cycles_device(c->ub, n.n_lmtig, nullptr, nullptr, c->cyc_cnt.as<unsigned long long>(), c->stream);
-        if (rc) return fail(c, rc, "cycle sizing");
-        CK(cudaMemcpyAsync(cnt, c->cyc_cnt.p, 16, cudaMemcpyDeviceToHost, c->stream));
+        rc = collate_cycles_on_device(c->ub, n.n_lmtig, res.n_cycle_lmtigs, c->p.k, &c->misc.as<MiscWords>()->err,
+                                      c->cyc_work, c->cyc_scratch, c->cyc_out, c->stream, cyc_bytes, cyc_units);
+        if (rc == CFG_ERR_OOM) return fail(c, rc, "cycle buffers");
+        if (rc) return fail(c, rc, std::string("cycle collation: ") + cudaGetErrorString(cudaGetLastError()));
+        CK(cudaMemcpyAsync(&m, c->misc.p, sizeof(m), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
-        if (!c->cyc_lm.ensure(sizeof(LmtigOut) * (cnt[0] + 1)) || !c->cyc_text.ensure(cnt[1] + 1))
-            return fail(c, CFG_ERR_OOM, "cycle buffers");
-        CK(cudaMemsetAsync(c->cyc_cnt.p, 0, 16, c->stream));
-        rc = collate_cycles_device(c->ub, n.n_lmtig, c->cyc_lm.as<LmtigOut>(), c->cyc_text.as<char>(),
-                                   c->cyc_cnt.as<unsigned long long>(), c->stream);
-        if (rc) return fail(c, rc, "cycle gather");
-        std::vector<cfg_lmtig> hl(cnt[0]);
-        std::string ht(cnt[1], '\0');
-        if (cnt[0]) CK(cudaMemcpyAsync(hl.data(), c->cyc_lm.p, sizeof(cfg_lmtig) * cnt[0], cudaMemcpyDeviceToHost, c->stream));
-        if (cnt[1]) CK(cudaMemcpyAsync(&ht[0], c->cyc_text.p, cnt[1], cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        char* out = nullptr;
-        uint64_t ob = 0, nu = 0, nc = 0;
-        rc = cfg_collate_lmtigs(c->p.k, hl.data(), cnt[0], ht.data(), &out, &ob, &nu, &nc);
-        if (rc) return fail(c, rc, "cycle collation");
-        cyc_fa.assign(out, ob);
-        cfg_free(out);
-        cyc_units = nu;
+        if (m.err & DERR_BAD_GRAPH) return fail(c, CFG_ERR_STATE, "lm-tig ends on a closed chain do not pair up");
     }
     CK(cudaEventRecord(c->ev[2], c->stream));   // device collation done
     // trivial unitigs (per stripe) + collated unitigs + cycles, to host memory
-    const uint64_t total = n.fasta_bytes + res.bytes + cyc_fa.size();
+    const uint64_t total = n.fasta_bytes + res.bytes + cyc_bytes;
     if (!c->h_unitigs.ensure(total + 1)) return fail(c, CFG_ERR_OOM, "pinned unitig buffer");
     char* h = (char*)c->h_unitigs.p;
     uint64_t at = 0;
@@ -732,10 +713,10 @@ int cfg_unitigs(cfg_ctx* c, const char** fasta, uint64_t* bytes, uint64_t* n_uni
         at += c->s_fasta[st];
     }
     if (res.bytes) CK(cudaMemcpyAsync(h + at, c->ub.out, res.bytes, cudaMemcpyDeviceToHost, c->stream));
+    at += res.bytes;
+    if (cyc_bytes) CK(cudaMemcpyAsync(h + at, c->cyc_out.p, cyc_bytes, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaEventRecord(c->ev[1], c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    at += res.bytes;
-    if (!cyc_fa.empty()) std::memcpy(h + at, cyc_fa.data(), cyc_fa.size());
     if (device_ms) { float ms = 0; cudaEventElapsedTime(&ms, c->ev[0], c->ev[2]); *device_ms = ms; }
     *fasta = h;
     *bytes = total;
@@ -770,7 +751,7 @@ void cfg_destroy(cfg_ctx* c) {
     DevBuf* bufs[] = {&c->packed, &c->frag_off, &c->frag_len, &c->text, &c->flat, &c->hist, &c->misc, &c->bucket_off, &c->inst, &c->scan_part,
                       &c->fill, &c->recs, &c->list, &c->tab_off, &c->tab_cap, &c->arena, &c->fasta, &c->lm_text,
                       &c->lm, &c->dump, &c->retry, &c->counters, &c->stripe_cur, &c->stripe_base,
-                      &c->ut_lmbase, &c->cyc_lm, &c->cyc_text, &c->cyc_cnt};
+                      &c->ut_lmbase, &c->cyc_work, &c->cyc_scratch, &c->cyc_out};
     for (DevBuf* b : bufs) b->release();
     c->h_fasta.release(); c->h_lm_text.release(); c->h_lm.release();
     for (auto& e : c->ev) if (e) cudaEventDestroy(e);

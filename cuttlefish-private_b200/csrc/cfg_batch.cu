@@ -34,7 +34,7 @@ using namespace cfg;
 
 namespace {
 
-constexpr uint32_t NCLS = 24;   // LOCAL classes (64, 96, 128, 192 .. 8192 slots: <= 15), 7 cluster sizes, 1 global
+constexpr uint32_t NCLS = 16;   // LOCAL classes (64..8192 slots: <= 8), 7 cluster sizes, 1 global
 
 struct BatchWords {   // device-side scalars of one run, cleared by one memset
     uint32_t count[NCLS], off[NCLS], fill[NCLS];
@@ -45,7 +45,7 @@ struct BatchWords {   // device-side scalars of one run, cleared by one memset
 
 struct ClassCfg {
     uint32_t load;        // table_load_pct
-    uint32_t nl;          // LOCAL classes: class c < nl holds tables of local_per(c) slots
+    uint32_t nl;          // LOCAL classes: class c < nl holds tables of 64 << c slots
     uint32_t per_cl;      // slots per CTA of a cluster
     uint32_t g_shift;     // log2 of subgraphs per job
     uint32_t n_buckets;
@@ -63,10 +63,12 @@ __host__ __device__ inline uint32_t ceil_pow2(uint64_t v) {   // v >= 2
 }
 __host__ __device__ inline uint32_t class_of(uint32_t inst, const ClassCfg& c, uint64_t& want) {
     want = want_slots(inst, c.load);
-    if (want <= local_per(c.nl - 1)) {
-        uint32_t cl = 0;
-        while (local_per(cl) < want) ++cl;
-        return cl;
+    const uint64_t per_max = 64ull << (c.nl - 1);
+    if (want <= per_max) {
+        const uint32_t per = ceil_pow2(want);
+        uint32_t lg = 0;
+        while ((64u << lg) < per) ++lg;
+        return lg;
     }
     // clusters only for one-word keys (k > 32: arena tables in HBM are faster)
     if (c.per_cl && want <= (uint64_t)c.per_cl * 8) return c.nl + (uint32_t)((want + c.per_cl - 1) / c.per_cl) - 2;
@@ -260,7 +262,7 @@ ClassCfg class_cfg(const cfg_batch* b) {
     c.load = b->tune.table_load_pct ? b->tune.table_load_pct : 100;
     const uint32_t per_max = subgraph_max_per_cta(b->words);
     c.nl = 0;
-    while (local_per(c.nl) <= per_max) ++c.nl;   // 15 classes up to 8192 slots, 13 up to 4096
+    while ((64u << c.nl) <= per_max) ++c.nl;
     c.per_cl = b->words == 1 ? subgraph_cluster_per_cta(b->words) : 0;   // no cluster classes for k > 32
     c.g_shift = b->g_shift;
     c.n_buckets = b->n_jobs << b->g_shift;
@@ -275,7 +277,7 @@ int plan_shapes(cfg_batch* b) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
     const ClassCfg cc = class_cfg(b);
     for (uint32_t c = 0; c < cc.nl; ++c) {
-        const uint32_t per = local_per(c);
+        const uint32_t per = 64u << c;
         uint32_t t = per / std::max<uint32_t>(1, b->tune.local_div);
         t = std::min<uint32_t>(subgraph_max_threads(b->words, per), std::max<uint32_t>(64, t));
         t = (t + 31) / 32 * 32;

@@ -196,11 +196,6 @@ int subgraph_occupancy(int words, uint32_t cluster, uint32_t threads, uint32_t p
 void launch_bucket_scan_large(const unsigned long long* hist, uint32_t n, uint32_t* bucket_off, uint32_t* inst,
                               uint32_t* fill, uint32_t* partials, cudaStream_t s);
 uint32_t subgraph_max_per_cta(int words);      // one CTA owning a whole table
-// One-CTA table sizes in steps of 1.5 and 4/3: class c holds 64, 96, 128, 192, 256, ...
-// slots.  The half steps keep a table within 1.5x of what its subgraph wants (powers of
-// two alone leave up to 2x), so a launch holds more CTAs per SM; a k-mer's home slot is a
-// multiply-shift of its hash by the table size, which needs no power of two.
-__host__ __device__ inline uint32_t local_per(uint32_t c) { return (c & 1 ? 96u : 64u) << (c >> 1); }
 // Largest CTA of a launch of `per`-slot tables (per 0: arena tables).
 uint32_t subgraph_max_threads(int words, uint32_t per);
 uint32_t subgraph_cluster_per_cta(int words);  // each CTA of a cluster

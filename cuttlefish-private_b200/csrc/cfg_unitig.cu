@@ -23,8 +23,9 @@
 //      forward or reverse-complemented) to its offset -- all of it at the unitig's
 //      tail, all but the last k bases elsewhere (its successor writes the k-mer they
 //      share).
-// Entries that never reach a head lie on closed chains (cycles); those lm-tigs are
-// handed back to the host collator, whose rotation rule they need (rare).
+// Entries that never reach a head lie on closed chains (cycles): a second set of passes
+// (collate_cycles_on_device, below) joins them and writes each cycle from its canonical
+// start; the batched form hands them to the host collator instead (they are rare).
 #include "cuttlefish_gpu.h"
 #include "cfg_host.h"
 #include "cfg_internal.h"
@@ -484,6 +485,200 @@ __global__ void k_ut_cycles(const LmtigOut* __restrict__ lm, const char* const* 
     }
 }
 
+// ---- closed chains (cycles), joined on the device ----
+// The lm-tigs left on closed chains (fin == NONE) are numbered 0..m-1; entry X = 2 c + d
+// of cycle lm-tig c is it entered by its end d (0: u, read forward).  X's successor
+// enters the lm-tig paired with X's exit end.  Every closed chain appears twice, once per
+// orientation; the one whose smallest original entry id is even is kept.  Pointer
+// jumping gives each kept entry its chain's head (that smallest entry) and its offset in
+// the chain's circular text C (T bases: every lm-tig adds its label minus the k bases it
+// shares with the next).  One CTA per chain then finds the smallest k-mer of C over both
+// strands and writes C rotated to start there, in that strand, k-1 bases longer than T
+// (canonicalize_cycle, include/Unitig_Collator.hpp:367-407): a chain's k-mers are all
+// distinct vertices, so the smallest is unique and the result does not depend on where the
+// walk started.
+constexpr uint32_t CYC = 0x80000000u;
+
+__global__ void k_cy_number(uint32_t* fin, uint64_t n, uint32_t* cyc_lm, unsigned long long* cnt) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (fin[i] != NONE) continue;
+        const uint32_t c = (uint32_t)atomicAdd(cnt, 1ull);
+        fin[i] = CYC | c;
+        cyc_lm[c] = (uint32_t)i;
+    }
+}
+
+struct CyArgs {
+    const LmtigOut* lm; const char* const* label; const uint32_t* partner; const uint32_t* fin;
+    const uint32_t* cyc_lm; uint64_t m2;    // entries: 2 x cycle lm-tigs
+    uint32_t k;
+    uint32_t *succ, *jmp0, *jmp1, *mn0, *mn1, *head;
+    unsigned long long *w, *acc0, *acc1, *pos;
+    uint32_t* err;
+};
+
+// successor, first jump, own original entry id, own bases
+__global__ void k_cy_init(CyArgs a) {
+    for (uint64_t X = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; X < a.m2; X += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t i = a.cyc_lm[X >> 1], d = (uint32_t)(X & 1);
+        const uint32_t y = a.partner[2 * i + (d ^ 1u)];          // the entry after i's exit end
+        uint32_t nx = (uint32_t)X;
+        if (y == NONE || !(a.fin[y >> 1] & CYC) || a.fin[y >> 1] == NONE) atomicOr(a.err, DERR_BAD_GRAPH);
+        else nx = 2 * (a.fin[y >> 1] & ~CYC) + (y & 1);
+        a.succ[X] = nx; a.jmp0[X] = nx;
+        a.mn0[X] = 2 * i + d;
+        const uint32_t len = a.lm[i].label_len;
+        a.w[X] = len >= a.k ? len - a.k : 0;
+    }
+}
+
+// one round of minimum propagation along the chain (double-buffered)
+__global__ void k_cy_min(uint64_t m2, const uint32_t* __restrict__ jmp, const uint32_t* __restrict__ mn, uint32_t* jmp2,
+                         uint32_t* mn2) {
+    for (uint64_t X = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; X < m2; X += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t j = jmp[X];
+        const uint32_t a = mn[X], b = mn[j];
+        mn2[X] = a < b ? a : b;
+        jmp2[X] = jmp[j];
+    }
+}
+
+// head of every kept entry (NONE for the mirror orientation); the suffix-sum start
+__global__ void k_cy_head(CyArgs a, const uint32_t* __restrict__ mn) {
+    for (uint64_t X = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; X < a.m2; X += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t e = mn[X];
+        uint32_t H = NONE;
+        if (!(e & 1)) H = 2 * (a.fin[e >> 1] & ~CYC) + (e & 1);
+        a.head[X] = H;
+        const bool is_h = H == (uint32_t)X;
+        a.jmp0[X] = is_h ? (uint32_t)X : a.succ[X];
+        a.acc0[X] = (H == NONE || is_h) ? 0ull : a.w[X];
+    }
+}
+
+// one round of suffix sums towards the head (the head is terminal: a self-loop of weight 0)
+__global__ void k_cy_sum(uint64_t m2, const uint32_t* __restrict__ head, const uint32_t* __restrict__ jmp,
+                         const unsigned long long* __restrict__ acc, uint32_t* jmp2, unsigned long long* acc2) {
+    for (uint64_t X = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; X < m2; X += (uint64_t)gridDim.x * blockDim.x) {
+        if (head[X] == NONE) continue;
+        const uint32_t j = jmp[X];
+        acc2[X] = acc[X] + acc[j];
+        jmp2[X] = jmp[j];
+    }
+}
+
+// every kept entry's offset in its chain's text; per head the chain's length T and its
+// space in the scratch text and in the output (">0\n" + T + k - 1 bases + "\n")
+__global__ void k_cy_place(CyArgs a, const unsigned long long* __restrict__ D, unsigned long long* T_of,
+                           unsigned long long* scr_off, unsigned long long* out_off, uint32_t* heads,
+                           unsigned long long* cur) {   // cur: [0] scratch bytes, [1] output bytes, [2] chains
+    for (uint64_t X = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; X < a.m2; X += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t H = a.head[X];
+        if (H == NONE) continue;
+        const unsigned long long T = a.w[H] + D[a.succ[H]];
+        a.pos[X] = X == H ? 0ull : T - D[X];
+        if (X == H) {
+            T_of[X] = T;
+            scr_off[X] = atomicAdd(cur, T);
+            out_off[X] = atomicAdd(cur + 1, T + a.k - 1 + 4);
+            heads[atomicAdd(cur + 2, 1ull)] = (uint32_t)X;
+        }
+    }
+}
+
+// every kept entry's label (in its orientation), all but its last k bases, into the text
+__global__ void k_cy_text(CyArgs a, const unsigned long long* __restrict__ scr_off, char* scr) {
+    for (uint64_t X = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; X < a.m2; X += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t H = a.head[X];
+        if (H == NONE) continue;
+        const uint32_t i = a.cyc_lm[X >> 1], len = a.lm[i].label_len;
+        const char* lab = a.label[i];
+        char* dst = scr + scr_off[H] + a.pos[X];
+        const uint64_t wx = a.w[X];
+        for (uint64_t t = 0; t < wx; ++t) dst[t] = oriented(lab, len, (uint32_t)(X & 1), (uint32_t)t);
+    }
+}
+
+__device__ __forceinline__ uint32_t code_of(char c) { return c == 'A' ? 0u : c == 'C' ? 1u : c == 'G' ? 2u : 3u; }
+// (hi, lo, index, strand) ordered lexicographically: the k-mer first (big-endian 2-bit,
+// so numeric order is character order), then where it was found
+struct CyKey { unsigned long long hi, lo; unsigned long long i; uint32_t s; };
+__device__ __forceinline__ bool cy_less(const CyKey& a, const CyKey& b) {
+    if (a.hi != b.hi) return a.hi < b.hi;
+    if (a.lo != b.lo) return a.lo < b.lo;
+    if (a.i != b.i) return a.i < b.i;
+    return a.s < b.s;
+}
+
+// one CTA per chain: the smallest k-mer over both strands, then the rotated record
+__global__ void __launch_bounds__(256) k_cy_rotate(const uint32_t* __restrict__ heads, const unsigned long long* __restrict__ n_heads,
+                                                   const unsigned long long* __restrict__ T_of,
+                                                   const unsigned long long* __restrict__ scr_off,
+                                                   const unsigned long long* __restrict__ out_off, const char* scr,
+                                                   uint32_t k, char* out) {
+    __shared__ CyKey red[8];
+    const uint64_t nh = *n_heads;
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint32_t kb = 2 * k;   // bits of a k-mer (k <= 63: at most 126)
+    for (uint64_t h = blockIdx.x; h < nh; h += gridDim.x) {
+        const uint32_t H = heads[h];
+        const unsigned long long T = T_of[H];
+        const char* C = scr + scr_off[H];
+        // positions [j0, j1) of this thread; the k-mer at j covers C[j .. j+k) circularly
+        const unsigned long long j0 = T * threadIdx.x / blockDim.x, j1 = T * (threadIdx.x + 1) / blockDim.x;
+        CyKey best{~0ull, ~0ull, ~0ull, 1u};
+        unsigned long long fh = 0, fl = 0, rh = 0, rl = 0;   // forward / reverse-complement k-mer
+        auto push = [&](uint32_t b) {   // appends base b to the forward k-mer, prepends comp(b) to the rc
+            fh = ((fh << 2) | (fl >> 62));
+            fl = (fl << 2) | b;
+            if (kb <= 64) { fl &= kb == 64 ? ~0ull : ((1ull << kb) - 1); fh = 0; }
+            else fh &= (1ull << (kb - 64)) - 1;
+            const uint32_t cb = 3u - b;
+            rl = (rl >> 2) | (rh << 62);
+            rh >>= 2;
+            if (kb <= 64) rl |= (unsigned long long)cb << (kb - 2);
+            else rh |= (unsigned long long)cb << (kb - 64 - 2);
+        };
+        if (j0 < j1) {
+            for (uint32_t t = 0; t + 1 < k; ++t) push(code_of(C[(j0 + t) % T]));
+            for (unsigned long long j = j0; j < j1; ++j) {
+                push(code_of(C[(j + k - 1) % T]));
+                const CyKey f{fh, fl, j, 0u}, r{rh, rl, T - 1 - j, 1u};
+                if (cy_less(f, best)) best = f;
+                if (cy_less(r, best)) best = r;
+            }
+        }
+        for (int d = 16; d; d >>= 1) {
+            CyKey o;
+            o.hi = __shfl_down_sync(0xffffffffu, best.hi, d); o.lo = __shfl_down_sync(0xffffffffu, best.lo, d);
+            o.i = __shfl_down_sync(0xffffffffu, best.i, d); o.s = __shfl_down_sync(0xffffffffu, best.s, d);
+            if (cy_less(o, best)) best = o;
+        }
+        if (lane == 0) red[wid] = best;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (uint32_t v = 1; v < blockDim.x / 32; ++v) if (cy_less(red[v], red[0])) red[0] = red[v];
+        }
+        __syncthreads();
+        const CyKey b = red[0];
+        char* o = out + out_off[H];
+        const unsigned long long L = T + k - 1;
+        if (threadIdx.x == 0) { o[0] = '>'; o[1] = '0'; o[2] = '\n'; o[3 + L] = '\n'; }
+        // strand 0: C from b.i; strand 1: the reverse complement read so that its base u is
+        // comp(C[(k - 2 - b.i - u) mod T])
+        for (unsigned long long u = threadIdx.x; u < L; u += blockDim.x) {
+            char c;
+            if (b.s == 0) c = C[(b.i + u) % T];
+            else {
+                const long long q = ((long long)k - 2 - (long long)b.i - (long long)u) % (long long)T;
+                c = comp_char(C[q < 0 ? q + (long long)T : q]);
+            }
+            o[3 + u] = c;
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 bool UnitigBuffers::ensure(uint64_t n) {
@@ -511,6 +706,63 @@ int collate_cycles_device(const UnitigBuffers& ub, uint64_t n, LmtigOut* out, ch
                           cudaStream_t s, uint32_t* out_job) {
     k_ut_cycles<<<148 * 4, 256, 0, s>>>(ub.lm, ub.label, n, ub.fin, out, text, cnt, ub.job, out_job);
     return cudaGetLastError() == cudaSuccess ? CFG_OK : CFG_ERR_CUDA;
+}
+
+int collate_cycles_on_device(UnitigBuffers& ub, uint64_t n, uint64_t m, uint32_t k, uint32_t* err, DevBuf& work,
+                             DevBuf& scratch, DevBuf& out, cudaStream_t s, uint64_t& out_bytes, uint64_t& n_cycles) {
+    out_bytes = 0; n_cycles = 0;
+    if (m == 0) return CFG_OK;
+    if (2 * m >= CYC) return CFG_ERR_BAD_INPUT;
+    const uint64_t m2 = 2 * m;
+    // per entry: succ, jmp0, jmp1, mn0, mn1, head (u32); w, acc0, acc1, pos, T, scratch and
+    // output offsets (u64); heads (u32); the cycle lm-tigs (u32, m); three counters
+    const size_t need = m2 * (7 * 4 + 7 * 8) + 4 * m + 512;   // + each array's 16-byte alignment
+    if (!work.ensure(need)) return CFG_ERR_OOM;
+    unsigned char* p = work.as<unsigned char>();
+    auto take = [&](size_t bytes) { unsigned char* q = p; p += (bytes + 15) & ~(size_t)15; return q; };
+    unsigned long long* cur = (unsigned long long*)take(32);
+    CyArgs a{};
+    a.lm = ub.lm; a.label = ub.label; a.partner = ub.partner; a.fin = ub.fin; a.m2 = m2; a.k = k; a.err = err;
+    a.w = (unsigned long long*)take(8 * m2); a.acc0 = (unsigned long long*)take(8 * m2);
+    a.acc1 = (unsigned long long*)take(8 * m2); a.pos = (unsigned long long*)take(8 * m2);
+    unsigned long long* T_of = (unsigned long long*)take(8 * m2);
+    unsigned long long* scr_off = (unsigned long long*)take(8 * m2);
+    unsigned long long* out_off = (unsigned long long*)take(8 * m2);
+    a.succ = (uint32_t*)take(4 * m2); a.jmp0 = (uint32_t*)take(4 * m2); a.jmp1 = (uint32_t*)take(4 * m2);
+    a.mn0 = (uint32_t*)take(4 * m2); a.mn1 = (uint32_t*)take(4 * m2); a.head = (uint32_t*)take(4 * m2);
+    uint32_t* heads = (uint32_t*)take(4 * m2);
+    uint32_t* cyc_lm = (uint32_t*)take(4 * m);
+    a.cyc_lm = cyc_lm;
+    if (cudaMemsetAsync(cur, 0, 32, s) != cudaSuccess) return CFG_ERR_CUDA;
+    const unsigned grid = (unsigned)std::min<uint64_t>(148ull * 8, (m2 + 255) / 256 + 1);
+    k_cy_number<<<148 * 4, 256, 0, s>>>(ub.fin, n, cyc_lm, cur + 3);   // cur: scratch, output, chains, lm-tigs
+    k_cy_init<<<grid, 256, 0, s>>>(a);
+    uint32_t rounds = 1;
+    while ((1ull << rounds) < m2) ++rounds;
+    ++rounds;
+    uint32_t *jA = a.jmp0, *jB = a.jmp1, *mA = a.mn0, *mB = a.mn1;
+    for (uint32_t r = 0; r < rounds; ++r) {
+        k_cy_min<<<grid, 256, 0, s>>>(m2, jA, mA, jB, mB);
+        std::swap(jA, jB); std::swap(mA, mB);
+    }
+    k_cy_head<<<grid, 256, 0, s>>>(a, mA);   // restarts jmp0 / acc0 for the sums
+    jA = a.jmp0; jB = a.jmp1;
+    unsigned long long *sA = a.acc0, *sB = a.acc1;
+    for (uint32_t r = 0; r < rounds; ++r) {
+        k_cy_sum<<<grid, 256, 0, s>>>(m2, a.head, jA, sA, jB, sB);
+        std::swap(jA, jB); std::swap(sA, sB);
+    }
+    k_cy_place<<<grid, 256, 0, s>>>(a, sA, T_of, scr_off, out_off, heads, cur);
+    unsigned long long h[3] = {0, 0, 0};
+    if (cudaMemcpyAsync(h, cur, 24, cudaMemcpyDeviceToHost, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
+        return CFG_ERR_CUDA;
+    if (!scratch.ensure(h[0] + 16) || !out.ensure(h[1] + 16)) return CFG_ERR_OOM;
+    k_cy_text<<<grid, 256, 0, s>>>(a, scr_off, scratch.as<char>());
+    k_cy_rotate<<<(unsigned)std::min<unsigned long long>(std::max<unsigned long long>(h[2], 1), 148ull * 8), 256, 0, s>>>(
+        heads, cur + 2, T_of, scr_off, out_off, scratch.as<char>(), k, out.as<char>());
+    if (cudaGetLastError() != cudaSuccess) return CFG_ERR_CUDA;
+    out_bytes = h[1]; n_cycles = h[2];
+    return CFG_OK;
 }
 
 int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, UnitigResult& res) {
