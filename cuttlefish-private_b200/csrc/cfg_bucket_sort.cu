@@ -146,28 +146,48 @@ __global__ void __launch_bounds__(SB_THREADS) k_sb_scan_apply(uint32_t* __restri
 
 // Pass 1b: slab s moved to its super-buckets, tile by tile through shared memory.
 // counts holds the exclusive prefix over (super-bucket, slab): slab s's base for h.
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
+                 "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// One CTA per SM walks its slab tile by tile with two tile buffers: the copy of tile t+1
+// into one (cp.async) is in flight while tile t is sorted in the other, which then holds
+// the sorted tile until it is written out.
 __global__ void __launch_bounds__(SB_THREADS) k_sb_move_hi(const uint64_t* __restrict__ flat, uint64_t n, uint32_t lbits,
                                                            uint32_t H, const uint32_t* __restrict__ counts,
                                                            uint64_t* __restrict__ tmp) {
     extern __shared__ __align__(16) unsigned char sm[];
-    uint64_t* stage = (uint64_t*)sm;                                  // SB_TILE records
-    uint32_t* run = (uint32_t*)(stage + SB_TILE);                     // H: next write position per super-bucket
+    uint64_t* const bufs = (uint64_t*)sm;                             // two tile buffers of SB_TILE records
+    uint32_t* run = (uint32_t*)(bufs + 2 * SB_TILE);                  // H: next write position per super-bucket
     uint32_t* tcnt = run + SB_MAX_BINS;                               // H: this tile's counts, then offsets
     uint32_t* ws = tcnt + SB_MAX_BINS;                                // scan scratch
     const uint32_t S = gridDim.x, s = blockIdx.x;
     for (uint32_t h = threadIdx.x; h < H; h += blockDim.x) run[h] = counts[(uint64_t)h * S + s];
-    const uint64_t e = slab_begin(n, s + 1, S);
+    const uint64_t b = slab_begin(n, s, S), e = slab_begin(n, s + 1, S);
     constexpr uint32_t PER = SB_TILE / SB_THREADS;
-    for (uint64_t t0 = slab_begin(n, s, S); t0 < e; t0 += SB_TILE) {
+    auto fetch = [&](uint64_t t0, uint64_t* dst) {   // tile at t0 into dst, asynchronously
+        const uint32_t tn = (uint32_t)(e - t0 < SB_TILE ? e - t0 : SB_TILE);
+        for (uint32_t i = threadIdx.x; i < tn; i += SB_THREADS) cp_async8(dst + i, flat + t0 + i);
+        cp_async_commit();
+    };
+    if (b < e) fetch(b, bufs);
+    uint32_t cur = 0;
+    for (uint64_t t0 = b; t0 < e; t0 += SB_TILE, cur ^= 1) {
         const uint32_t tn = (uint32_t)(e - t0 < SB_TILE ? e - t0 : SB_TILE);
         for (uint32_t h = threadIdx.x; h < H; h += blockDim.x) tcnt[h] = 0;
-        __syncthreads();
+        cp_async_wait_all();
+        __syncthreads();   // tile t has landed; the other buffer's sorted tile is written out
+        if (t0 + SB_TILE < e) fetch(t0 + SB_TILE, bufs + (cur ^ 1) * SB_TILE);
+        uint64_t* in = bufs + cur * SB_TILE;
         uint64_t r[PER];
         uint32_t rank[PER];
 #pragma unroll
         for (uint32_t j = 0; j < PER; ++j) {
             const uint32_t i = j * SB_THREADS + threadIdx.x;
-            r[j] = i < tn ? flat[t0 + i] : 0ull;
+            r[j] = i < tn ? in[i] : 0ull;
             rank[j] = i < tn ? atomicAdd(&tcnt[rec_g(r[j]) >> lbits], 1u) : 0u;
         }
         __syncthreads();
@@ -176,12 +196,12 @@ __global__ void __launch_bounds__(SB_THREADS) k_sb_move_hi(const uint64_t* __res
 #pragma unroll
         for (uint32_t j = 0; j < PER; ++j) {
             const uint32_t i = j * SB_THREADS + threadIdx.x;
-            if (i < tn) stage[tcnt[rec_g(r[j]) >> lbits] + rank[j]] = r[j];
+            if (i < tn) in[tcnt[rec_g(r[j]) >> lbits] + rank[j]] = r[j];   // the tile, sorted, in place
         }
         __syncthreads();
         // consecutive staged records of one super-bucket go to consecutive addresses
         for (uint32_t i = threadIdx.x; i < tn; i += blockDim.x) {
-            const uint64_t x = stage[i];
+            const uint64_t x = in[i];
             const uint32_t h = rec_g(x) >> lbits;
             tmp[run[h] + (i - tcnt[h])] = x;
         }
@@ -191,8 +211,9 @@ __global__ void __launch_bounds__(SB_THREADS) k_sb_move_hi(const uint64_t* __res
             const uint32_t nxt = h + 1 < H ? tcnt[h + 1] : tn;
             run[h] += nxt - tcnt[h];
         }
-        __syncthreads();
+        __syncthreads();   // tcnt is read above before the next tile clears it
     }
+    cp_async_wait_all();
 }
 
 // Pass 2: super-bucket h = [base_h, base_{h+1}) of tmp sorted by the low bits of g into
@@ -249,14 +270,14 @@ __global__ void __launch_bounds__(SB_THREADS) k_sb_move_lo(const uint64_t* __res
 
 uint64_t bucket_sort_scratch_words(uint32_t G, uint32_t sms) {
     const uint32_t gbits = 31 - __builtin_clz(G), hbits = gbits < 10 ? gbits : 10;
-    const uint64_t m = (uint64_t)(1u << hbits) * (2 * sms);
+    const uint64_t m = (uint64_t)(1u << hbits) * sms;
     return m + (m + SCAN_ITEMS - 1) / SCAN_ITEMS + 1;
 }
 
 cudaError_t launch_bucket_sort(const uint64_t* flat, uint64_t n, uint32_t G, uint32_t k, uint32_t sms, uint32_t* scratch,
                                uint64_t* tmp, uint64_t* out, uint32_t* bucket_off, uint32_t* inst, cudaStream_t s) {
     const uint32_t gbits = 31 - __builtin_clz(G), hbits = gbits < 10 ? gbits : 10, lbits = gbits - hbits;
-    const uint32_t H = 1u << hbits, S = 2 * sms;
+    const uint32_t H = 1u << hbits, S = sms;   // slabs: one CTA of k_sb_move_hi per SM
     const uint64_t m = (uint64_t)H * S;
     uint32_t* counts = scratch;
     uint32_t* sums = scratch + m;
@@ -264,7 +285,7 @@ cudaError_t launch_bucket_sort(const uint64_t* flat, uint64_t n, uint32_t G, uin
     k_sb_count<<<S, SB_THREADS, 0, s>>>(flat, n, lbits, H, counts);
     k_sb_scan_sums<<<nsums, SB_THREADS, 0, s>>>(counts, m, sums);
     k_sb_scan_apply<<<nsums, SB_THREADS, 0, s>>>(counts, m, sums, nsums);
-    const size_t smem = SB_TILE * 8 + 2 * SB_MAX_BINS * 4 + (SB_THREADS / 32 + 1) * 4;
+    const size_t smem = 2 * SB_TILE * 8 + 2 * SB_MAX_BINS * 4 + (SB_THREADS / 32 + 1) * 4;
     cudaError_t e = cudaFuncSetAttribute(k_sb_move_hi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k_sb_move_hi<<<S, SB_THREADS, smem, s>>>(flat, n, lbits, H, counts, tmp);
