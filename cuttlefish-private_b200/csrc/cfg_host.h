@@ -117,7 +117,9 @@ struct UnitigInput {
 };
 // ... the buffers it works in ...
 struct UnitigBuffers {
-    DevBuf b_lm, b_label, b_tab, b_partner, b_X0, b_X1, b_fin, b_off, b_words, b_out, b_job, b_flip, b_sx, b_sw;
+    DevBuf b_lm, b_label, b_tab, b_partner, b_X0, b_X1, b_fin, b_off, b_words, b_out, b_job, b_flip, b_sx, b_sw, b_len, b_ends;
+    ulonglong2* ends = nullptr;   // both ends of each gathered lm-tig, packed for the pairing pass
+    uint32_t* len = nullptr;   // each gathered lm-tig's label length (the kernels that need only it read 4 bytes, not 48)
     uint8_t* flipb = nullptr;  // per lm-tig heading its chain's walked list: flip it
     LmtigOut* lm = nullptr;
     uint32_t* job = nullptr;   // batch: each gathered lm-tig's job
@@ -140,7 +142,7 @@ struct UnitigBuffers {
     }
     void release() {
         DevBuf* all[] = {&b_lm, &b_label, &b_tab, &b_partner, &b_X0, &b_X1, &b_fin, &b_off, &b_words, &b_out, &b_job,
-                         &b_flip, &b_sx, &b_sw};
+                         &b_flip, &b_sx, &b_sw, &b_len, &b_ends};
         for (DevBuf* b : all) b->release();
     }
 };

@@ -59,20 +59,29 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
     return z;
 }
 
-__device__ __forceinline__ bool is_phi(const LmtigOut& m, uint32_t end) { return (m.flags >> (end ? 3 : 2)) & 1; }
-__device__ __forceinline__ uint32_t side_of(const LmtigOut& m, uint32_t end) { return (m.flags >> end) & 1; }
+
+// An lm-tig end as the pairing pass reads it: the vertex k-mer (low word, high word) with
+// the end's side in bit 62 and its phi flag in bit 63 of the high word (a k-mer of k <= 63
+// leaves both free).
+constexpr unsigned long long END_SIDE = 1ull << 62, END_PHI = 1ull << 63;
+__device__ __forceinline__ void put_ends(ulonglong2* ends, uint64_t g, const LmtigOut& m) {
+    ends[2 * g] = make_ulonglong2(m.u[0], m.u[1] | ((m.flags & 1ull) << 62) | ((m.flags >> 2 & 1ull) << 63));
+    ends[2 * g + 1] = make_ulonglong2(m.v[0], m.v[1] | ((m.flags >> 1 & 1ull) << 62) | ((m.flags >> 3 & 1ull) << 63));
+}
 
 // 0: gather the striped lm-tigs into one array with their label addresses.
 __global__ void k_ut_gather(const LmtigOut* lm, uint64_t lm_slice, const char* text, uint64_t text_slice,
                             const unsigned long long* __restrict__ lm_base, const unsigned long long* __restrict__ text_base,
                             const unsigned long long* __restrict__ stripe_cur, uint32_t stripes, LmtigOut* out,
-                            const char** label) {
+                            const char** label, uint32_t* lens, ulonglong2* ends) {
     for (uint32_t st = blockIdx.y; st < stripes; st += gridDim.y) {
         const unsigned long long n = stripe_cur[st * JOB_CUR_STRIDE + 2];
         for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
             const LmtigOut m = lm[st * lm_slice + i];
             const uint64_t g = lm_base[st] + i;
             out[g] = m;
+            lens[g] = m.label_len;
+            put_ends(ends, g, m);
             label[g] = text + st * text_slice + (m.label_off - text_base[st]);
         }
     }
@@ -81,7 +90,8 @@ __global__ void k_ut_gather(const LmtigOut* lm, uint64_t lm_slice, const char* t
 // 0 (batch): gather every job's lm-tigs from its regions; the job rides along.
 __global__ void k_ut_gather_jobs(const LmtigOut* lm, const char* text, const JobOut* __restrict__ jobs, uint32_t n_jobs,
                                  const unsigned long long* __restrict__ job_n, const unsigned long long* __restrict__ job_lm_base,
-                                 LmtigOut* out, const char** label, uint32_t* out_job) {
+                                 LmtigOut* out, const char** label, uint32_t* out_job, uint32_t* lens,
+                                 ulonglong2* ends) {
     for (uint32_t j = blockIdx.y; j < n_jobs; j += gridDim.y) {
         const unsigned long long n = job_n[j];
         const JobOut& J = jobs[j];
@@ -89,6 +99,8 @@ __global__ void k_ut_gather_jobs(const LmtigOut* lm, const char* text, const Job
             const LmtigOut m = lm[J.lm_off + i];
             const uint64_t g = job_lm_base[j] + i;
             out[g] = m;
+            lens[g] = m.label_len;
+            put_ends(ends, g, m);
             label[g] = text + J.lm_text_off + m.label_off;
             out_job[g] = j;
         }
@@ -106,7 +118,7 @@ __global__ void k_ut_gather_jobs(const LmtigOut* lm, const char* text, const Job
 // first end is claimed by CAS and its k-mer read from the (immutable) lm-tig, so no
 // thread waits on another.
 constexpr uint32_t INSERT_TILE = 1024;
-__global__ void __launch_bounds__(256, 6) k_ut_insert(const LmtigOut* __restrict__ lm, const uint32_t* __restrict__ job,
+__global__ void __launch_bounds__(256, 6) k_ut_insert(const ulonglong2* __restrict__ ends, const uint32_t* __restrict__ job,
                                                     uint64_t n, uint32_t* tab,
                                                     const unsigned long long* __restrict__ job_lm_base,
                                                     const unsigned long long* __restrict__ job_n,
@@ -123,10 +135,9 @@ __global__ void __launch_bounds__(256, 6) k_ut_insert(const LmtigOut* __restrict
         for (uint32_t u = threadIdx.x; u < INSERT_TILE; u += blockDim.x) {
             const uint64_t e = t0 + u;
             if (e >= n2) break;
-            const LmtigOut& m = lm[e >> 1];
-            const uint32_t end = (uint32_t)(e & 1);
-            if (is_phi(m, end)) continue;
-            const unsigned long long k0 = end ? m.v[0] : m.u[0], k1 = end ? m.v[1] : m.u[1];
+            const ulonglong2 me = ends[e];
+            if (me.y & END_PHI) continue;
+            const unsigned long long k0 = me.x, k1 = me.y & ~(END_SIDE | END_PHI);
             const uint64_t h = mix64(k0 ^ mix64(k1 + 0x9E3779B97F4A7C15ull));
             const uint32_t jb = job ? job[e >> 1] : 0u;
             const uint64_t base = job ? 4 * job_lm_base[jb] : 0, t = job ? 4 * job_n[jb] : 4 * n;
@@ -134,10 +145,9 @@ __global__ void __launch_bounds__(256, 6) k_ut_insert(const LmtigOut* __restrict
             for (uint64_t probe = 0; probe < t; ++probe) {
                 const uint32_t old = atomicCAS(tab + 2 * p, NONE, (uint32_t)e);
                 if (old == NONE) break;
-                const LmtigOut& o = lm[old >> 1];
-                const uint32_t oe = old & 1;
-                if ((oe ? o.v[0] : o.u[0]) == k0 && (oe ? o.v[1] : o.u[1]) == k1) {
-                    if (atomicCAS(tab + 2 * p + 1, NONE, (uint32_t)e) != NONE || side_of(m, end) == side_of(o, oe)) {
+                const ulonglong2 oe = ends[old];
+                if (oe.x == k0 && (oe.y & ~(END_SIDE | END_PHI)) == k1) {
+                    if (atomicCAS(tab + 2 * p + 1, NONE, (uint32_t)e) != NONE || ((me.y ^ oe.y) & END_SIDE) == 0) {
                         atomicOr(err, DERR_BAD_GRAPH);
                     } else {
                         partner[e] = old;
@@ -157,7 +167,7 @@ __global__ void __launch_bounds__(256, 6) k_ut_insert(const LmtigOut* __restrict
 // Entry x = lm-tig x/2 entered through end x&1 (0: u, read forward; 1: v, reverse); its
 // predecessor left its lm-tig through the end paired with x's entry end, and its
 // successor entered through the end paired with x's exit end.
-__global__ void __launch_bounds__(256) k_rs_init(const LmtigOut* __restrict__ lm, uint64_t n,
+__global__ void __launch_bounds__(256) k_rs_init(const uint32_t* __restrict__ lens, uint64_t n,
                                                   const uint32_t* __restrict__ partner, uint32_t k, uint32_t sample_mask,
                                                   uint2* node, uint32_t* sx, uint32_t* sw, unsigned long long* n_split,
                                                   uint32_t* err) {
@@ -174,7 +184,7 @@ __global__ void __launch_bounds__(256) k_rs_init(const LmtigOut* __restrict__ lm
             pred = q == NONE ? NONE : (q ^ 1u);
             const bool tail = partner[x ^ 1] == NONE;
             split = pred == NONE || tail || (mix64(x + 0x2545F4914F6CDD1Dull) & sample_mask) == 0;
-            w = lm[x >> 1].label_len - k;
+            w = lens[x >> 1] - k;
             if (w & SPLIT) atomicOr(err, DERR_WALK_LIMIT);   // an lm-tig of 2^31 bases
         }
         // one atomic per block for the splitters' ids
@@ -308,7 +318,7 @@ __device__ __forceinline__ char oriented(const char* lab, uint32_t len, uint32_t
 
 // 3: per chain, once (by the lm-tig heading the list the host collator walks): flip the
 // list when its reverse complement starts with a smaller k-mer (ties keep the walk).
-__global__ void k_ut_flip(const LmtigOut* __restrict__ lm, const char* const* __restrict__ label, uint64_t n,
+__global__ void k_ut_flip(const uint32_t* __restrict__ lens, const char* const* __restrict__ label, uint64_t n,
                           const RankRec* __restrict__ X, uint32_t k, uint8_t* flipb) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t e0 = (uint32_t)(2 * i), e1 = e0 + 1;
@@ -320,7 +330,7 @@ __global__ void k_ut_flip(const LmtigOut* __restrict__ lm, const char* const* __
         const uint32_t t = (e == e0 ? x1.R : x0.R) ^ 1u;   // the entry of the list's tail
         const char* lh = label[h >> 1];
         const char* lt = label[t >> 1];
-        const uint32_t nh = lm[h >> 1].label_len, nt = lm[t >> 1].label_len;
+        const uint32_t nh = lens[h >> 1], nt = lens[t >> 1];
         bool flip = false;
         for (uint32_t j = 0; j < k; ++j) {
             const char a = oriented(lh, nh, h, j);
@@ -333,7 +343,7 @@ __global__ void k_ut_flip(const LmtigOut* __restrict__ lm, const char* const* __
 
 // 4a: per lm-tig, the final entry; per final tail, the unitig's FASTA record.
 // final[i] = chosen entry of lm-tig i, or NONE when i lies on a cycle.
-__global__ void k_ut_choose(const LmtigOut* __restrict__ lm, const char* const* __restrict__ label, uint64_t n,
+__global__ void k_ut_choose(const uint32_t* __restrict__ lens, const char* const* __restrict__ label, uint64_t n,
                             const uint32_t* __restrict__ partner, const RankRec* __restrict__ X, uint32_t k,
                             uint32_t* fin, unsigned long long* out_off, unsigned long long* cursor, unsigned long long* n_units,
                             unsigned long long* n_cyc, const uint32_t* __restrict__ job,
@@ -362,7 +372,7 @@ __global__ void k_ut_choose(const LmtigOut* __restrict__ lm, const char* const* 
                     tail = true;
                     const RankRec xf = f == e0 ? x0 : x1;
                     head = xf.R;
-                    L = xf.A + lm[f >> 1].label_len;   // bases before the tail + its whole label
+                    L = xf.A + lens[f >> 1];   // bases before the tail + its whole label
                 }
             }
         }
@@ -409,7 +419,7 @@ __global__ void k_ut_choose(const LmtigOut* __restrict__ lm, const char* const* 
 // vertex they share, which the successor writes), or all of them at the tail.  Each
 // thread resolves one lm-tig's source and destination and copies short pieces itself
 // (eight loads in flight before the stores); the warp copies long ones together.
-__global__ void k_ut_write(const LmtigOut* __restrict__ lm, const char* const* __restrict__ label, uint64_t n,
+__global__ void k_ut_write(const uint32_t* __restrict__ lens, const char* const* __restrict__ label, uint64_t n,
                            const uint32_t* __restrict__ fin, const uint32_t* __restrict__ partner,
                            const RankRec* __restrict__ X, const unsigned long long* __restrict__ out_off, uint32_t k,
                            char* out) {
@@ -423,7 +433,7 @@ __global__ void k_ut_write(const LmtigOut* __restrict__ lm, const char* const* _
         if (i < n) {
             f = fin[i];
             if (f != NONE) {
-                len = lm[i].label_len;
+                len = lens[i];
                 lab = label[i];
                 const RankRec xf = X[f];
                 char* rec = out + out_off[xf.R];
@@ -689,8 +699,11 @@ bool UnitigBuffers::ensure(uint64_t n) {
     if (!b_lm.ensure(sizeof(LmtigOut) * (n + 1)) || !b_label.ensure(8 * (n + 1)) || !b_tab.ensure(sizeof(EndSlot) * t) ||
         !b_partner.ensure(4 * n2) || !b_X0.ensure(sizeof(RankRec) * n2) || !b_X1.ensure(sizeof(RankRec) * n2) ||
         !b_fin.ensure(4 * (n + 1)) || !b_sx.ensure(4 * n2) || !b_sw.ensure(4 * n2) ||
-        !b_off.ensure(8 * n2) || !b_words.ensure(64) || !b_job.ensure(4 * (n + 1)) || !b_flip.ensure(n + 1))
+        !b_off.ensure(8 * n2) || !b_words.ensure(64) || !b_job.ensure(4 * (n + 1)) || !b_flip.ensure(n + 1) ||
+        !b_len.ensure(4 * (n + 1)) || !b_ends.ensure(32 * (n + 1)))
         return false;
+    len = b_len.as<uint32_t>();
+    ends = b_ends.as<ulonglong2>();
     job = b_job.as<uint32_t>();
     flipb = b_flip.as<uint8_t>();
     lm = b_lm.as<LmtigOut>(); label = (const char**)b_label.p; tab = b_tab.p; tab_n = t;
@@ -779,20 +792,20 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
     const uint32_t* job = in.jobs ? ub.job : nullptr;
     if (in.jobs)
         k_ut_gather_jobs<<<dim3(16, std::min<uint32_t>(in.n_jobs, 65535)), 256, 0, s>>>(
-            in.job_lm, in.job_text, in.jobs, in.n_jobs, in.job_n, in.job_lm_base, ub.lm, ub.label, ub.job);
+            in.job_lm, in.job_text, in.jobs, in.n_jobs, in.job_n, in.job_lm_base, ub.lm, ub.label, ub.job, ub.len, ub.ends);
     else
         k_ut_gather<<<dim3(64, in.stripes), 256, 0, s>>>(in.lm, in.lm_slice, in.text, in.text_slice, in.lm_base, in.text_base,
-                                                         in.stripe_cur, in.stripes, ub.lm, ub.label);
+                                                         in.stripe_cur, in.stripes, ub.lm, ub.label, ub.len, ub.ends);
     if (cudaMemsetAsync(ub.tab, 0xff, sizeof(EndSlot) * ub.tab_n, s) != cudaSuccess ||
         cudaMemsetAsync(ub.partner, 0xff, 4 * 2 * n, s) != cudaSuccess)
         return CFG_ERR_CUDA;
-    k_ut_insert<<<grid, 256, 0, s>>>(ub.lm, job, n, (uint32_t*)ub.tab, in.job_lm_base, in.job_n, cursor + 5, ub.partner,
+    k_ut_insert<<<grid, 256, 0, s>>>(ub.ends, job, n, (uint32_t*)ub.tab, in.job_lm_base, in.job_n, cursor + 5, ub.partner,
                                      in.err);
     // ranking: splitters, their walks, pointer jumping over the splitters, every entry
     RankRec* X = (RankRec*)ub.X[0];
     uint2* node = (uint2*)ub.out_off;                          // free until the records are reserved
     RankRec* Sb[2] = {(RankRec*)ub.X[1], (RankRec*)ub.tab};   // the vertex table is done with
-    k_rs_init<<<grid, 256, 0, s>>>(ub.lm, n, ub.partner, in.k, 15u, node, ub.sx, ub.sw, cursor + 4, in.err);
+    k_rs_init<<<grid, 256, 0, s>>>(ub.len, n, ub.partner, in.k, 15u, node, ub.sx, ub.sw, cursor + 4, in.err);
     k_rs_walk<<<grid, 256, 0, s>>>(ub.sx, ub.sw, cursor + 4, node, Sb[0], cursor + 6, 4 * n + 64, in.err);
     int cur = 0;
     unsigned long long last = ~0ull;
@@ -817,8 +830,8 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
     if (e & DERR_BAD_GRAPH) return CFG_ERR_STATE;
     if (e & DERR_WALK_LIMIT) return CFG_ERR_WALK_LIMIT;
     k_rs_final<<<grid, 256, 0, s>>>(2 * n, node, X, Sb[cur]);
-    k_ut_flip<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, X, in.k, ub.flipb);
-    k_ut_choose<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, ub.partner, X, in.k, ub.fin,
+    k_ut_flip<<<grid, 256, 0, s>>>(ub.len, ub.label, n, X, in.k, ub.flipb);
+    k_ut_choose<<<grid, 256, 0, s>>>(ub.len, ub.label, n, ub.partner, X, in.k, ub.fin,
                                      ub.out_off, cursor, cursor + 1, cursor + 2, job, in.job_out_base, in.job_cur,
                                      ub.flipb);
     unsigned long long w[3] = {0, 0, 0};
@@ -826,7 +839,7 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
         return CFG_ERR_CUDA;
     // a batch's output regions are sized by the caller before the call
     if (!in.jobs && !ub.ensure_out(w[0] + 16)) return CFG_ERR_OOM;
-    k_ut_write<<<grid, 256, 0, s>>>(ub.lm, ub.label, n, ub.fin, ub.partner, X, ub.out_off, in.k, ub.out);
+    k_ut_write<<<grid, 256, 0, s>>>(ub.len, ub.label, n, ub.fin, ub.partner, X, ub.out_off, in.k, ub.out);
     if (cudaGetLastError() != cudaSuccess) return CFG_ERR_CUDA;
     res.bytes = w[0]; res.n_units = w[1]; res.n_cycle_lmtigs = w[2];
     return CFG_OK;
