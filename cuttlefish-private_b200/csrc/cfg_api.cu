@@ -42,7 +42,7 @@ struct cfg_ctx {
     bool have_input = false, have_run = false;
 
     // partition
-    DevBuf flat, hist, misc, bucket_off, inst, fill, recs, scan_part;
+    DevBuf flat, hist, misc, bucket_off, inst, fill, recs, scan_part, rcw;
     // plan
     DevBuf list, tab_off, tab_cap, arena;
     // outputs
@@ -124,6 +124,9 @@ int run_partition(cfg_ctx* c, std::vector<uint32_t>& inst_h, std::vector<uint32_
         a.rec_cursor = &c->misc.as<MiscWords>()->rec_cursor;
         a.hist = nullptr;   // the bucket sort counts records and instances per subgraph
         a.err = &c->misc.as<MiscWords>()->err;
+        const uint64_t n_words = (c->n_bases + 31) / 32;
+        if (!c->rcw.ensure(8 * (n_words + 4))) return fail(c, CFG_ERR_OOM, "reverse-complement words");
+        a.rcw = c->rcw.as<uint64_t>();
         CK(cudaEventRecord(c->ev[1], c->stream));
         // input still in flight: a launch per piece as it lands; all landed: one launch
         bool landed = c->pieces.empty();
@@ -133,15 +136,17 @@ int run_partition(cfg_ctx* c, std::vector<uint32_t>& inst_h, std::vector<uint32_
             landed = q == cudaSuccess;
         }
         if (landed) {
+            launch_rc_words(c->d_packed, 0, n_words, c->rcw.as<uint64_t>(), c->stream);
             launch_partition(a, c->stream);
-            c->launches += 1;
+            c->launches += 2;
         } else {   // each piece of the input as soon as its copies have landed
             for (size_t i = 0; i < c->pieces.size(); ++i) {
                 const cfg_ctx::Piece& pc = c->pieces[i];
                 CK(cudaStreamWaitEvent(c->stream, c->piece_ev[i], 0));
                 a.base0 = pc.b0; a.base1 = pc.b1; a.frag_lo = pc.f0; a.frag_hi = pc.f1;
+                launch_rc_words(c->d_packed, pc.b0 >> 5, (pc.b1 + 31) >> 5, c->rcw.as<uint64_t>(), c->stream);
                 launch_partition(a, c->stream);
-                c->launches += 1;
+                c->launches += 2;
             }
         }
         CK(cudaGetLastError());
@@ -748,7 +753,7 @@ void cfg_destroy(cfg_ctx* c) {
     c->parse.release();
     c->ub.release();
     c->h_unitigs.release();
-    DevBuf* bufs[] = {&c->packed, &c->frag_off, &c->frag_len, &c->text, &c->flat, &c->hist, &c->misc, &c->bucket_off, &c->inst, &c->scan_part,
+    DevBuf* bufs[] = {&c->packed, &c->frag_off, &c->frag_len, &c->text, &c->flat, &c->hist, &c->misc, &c->bucket_off, &c->inst, &c->scan_part, &c->rcw,
                       &c->fill, &c->recs, &c->list, &c->tab_off, &c->tab_cap, &c->arena, &c->fasta, &c->lm_text,
                       &c->lm, &c->dump, &c->retry, &c->counters, &c->stripe_cur, &c->stripe_base,
                       &c->ut_lmbase, &c->cyc_work, &c->cyc_scratch, &c->cyc_out};

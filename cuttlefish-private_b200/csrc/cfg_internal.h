@@ -63,7 +63,13 @@ struct PartitionArgs {
     // [frag_lo, frag_hi) that tile them (base1 == 0: the whole input, every fragment).  A
     // job whose input arrives in pieces partitions each piece as soon as it has landed.
     uint64_t base0, base1, frag_lo, frag_hi;
+    // every packed word reverse-complemented in place (its 32 bases reversed, each
+    // complemented), written by launch_rc_words for this launch's words; nullptr: each
+    // l-mer's reverse complement is computed from the l-mer itself
+    const uint64_t* rcw;
 };
+// rcw[w] for the packed words [w0, w1): the reverse complement of word w.
+void launch_rc_words(const uint64_t* packed, uint64_t w0, uint64_t w1, uint64_t* rcw, cudaStream_t s);
 
 struct ScatterArgs {
     const uint64_t* flat;

@@ -12,6 +12,8 @@
 #include "cfg_device.cuh"
 #include "cfg_internal.h"
 
+#include <algorithm>
+
 namespace cfg {
 
 namespace {
@@ -23,6 +25,31 @@ __device__ __forceinline__ uint32_t lanemask_lt() { uint32_t m; asm("mov.u32 %0,
 
 __device__ __forceinline__ uint64_t lmer_at(const uint64_t* __restrict__ s, uint64_t p, uint32_t l) {
     return window64(s, p) >> (64 - 2 * l);
+}
+
+// min(hash(l-mer at p), hash(its reverse complement)).  With the reverse-complemented
+// words at hand, the reverse complement is a second window: its first base is the
+// l-mer's last, e = p + l - 1, at index 31 - (e mod 32) of rcw[e / 32], and it continues
+// into rcw[e / 32 - 1] -- two loads and a funnel shift instead of a bit reversal per
+// l-mer (this kernel is bound by the integer ALU pipe, not by loads).
+__device__ __forceinline__ uint64_t lmer_hash_at(const PartitionArgs& a, uint64_t p, uint32_t l) {
+    const uint64_t fw = lmer_at(a.packed, p, l);
+    if (!a.rcw) return lmer_hash(fw, l, a.seed0);
+    const uint64_t e = p + l - 1, w2 = e >> 5;
+    const uint32_t j = 31 - (uint32_t)(e & 31);
+    const uint64_t hi = __ldg(a.rcw + w2);
+    const uint64_t win = j == 0 ? hi : (hi << (2 * j)) | (w2 ? __ldg(a.rcw + w2 - 1) >> (64 - 2 * j) : 0ull);
+    const uint64_t rc = win >> (64 - 2 * l);
+    const uint64_t x = wyhash8(fw, a.seed0), y = wyhash8(rc, a.seed0);
+    return x < y ? x : y;
+}
+
+__global__ void k_rc_words(const uint64_t* __restrict__ packed, uint64_t w0, uint64_t w1, uint64_t* rcw) {
+    for (uint64_t w = w0 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < w1; w += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t r = __brevll(packed[w]);                                             // bits reversed
+        r = ((r >> 1) & 0x5555555555555555ull) | ((r & 0x5555555555555555ull) << 1);  // each base's two bits restored
+        rcw[w] = ~r;                                                                  // complemented: b -> 3 - b
+    }
 }
 
 // A warp's records wait in shared memory and are reserved in the flat array together:
@@ -79,7 +106,7 @@ __device__ void sweep_fragment(const PartitionArgs& a, const uint8_t* mod_w, uin
     const uint32_t dq = w - (1u << E);
     // hash of l-mer q, or "none" (all ones, above every hash) outside the fragment
     auto hash_at = [&](int64_t q) -> uint64_t {
-        return (q >= 0 && q < (int64_t)n_lmers) ? lmer_hash(lmer_at(a.packed, F0 + (uint64_t)q, l), l, a.seed0) : ~0ull;
+        return (q >= 0 && q < (int64_t)n_lmers) ? lmer_hash_at(a, F0 + (uint64_t)q, l) : ~0ull;
     };
     uint64_t lv[E + 1], pv[E + 1];   // this chunk's / the previous chunk's level values
 #pragma unroll
@@ -376,6 +403,12 @@ void launch_partition(const PartitionArgs& a, cudaStream_t s) {
         case 4: k_partition<4><<<grid, block, 0, s>>>(a); break;
         default: k_partition<5><<<grid, block, 0, s>>>(a); break;
     }
+}
+
+void launch_rc_words(const uint64_t* packed, uint64_t w0, uint64_t w1, uint64_t* rcw, cudaStream_t s) {
+    if (w1 <= w0) return;
+    const uint64_t blocks = std::min<uint64_t>((w1 - w0 + 255) / 256, 148ull * 16);
+    k_rc_words<<<(unsigned)blocks, 256, 0, s>>>(packed, w0, w1, rcw);
 }
 
 void launch_bucket_scan(const unsigned long long* hist, uint32_t G, uint32_t* bucket_off, uint32_t* inst,
