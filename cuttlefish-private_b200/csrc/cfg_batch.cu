@@ -230,7 +230,7 @@ struct cfg_batch {
 
     // device collation of all jobs' lm-tigs (cfg_batch_unitigs)
     UnitigBuffers ub;
-    DevBuf u_n, u_base, u_out, u_cur, u_err, u_cyc_lm, u_cyc_text, u_cyc_job, u_cyc_cnt;
+    DevBuf u_n, u_base, u_out, u_cur, u_err, u_cyc_work, u_cyc_scratch, u_cyc_out;
     std::vector<unsigned long long> h_out_base, h_ucur;
     std::vector<std::string> u_host;    // per job: unitigs joined on the host (cycles; redone jobs)
     std::vector<uint64_t> u_host_n;
@@ -858,42 +858,23 @@ int cfg_batch_unitigs(cfg_batch* b, float* device_ms) {
         float ms = 0;
         cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]);
         total_ms += ms;
-        // lm-tigs on closed chains: joined on the host, per job
+        // lm-tigs on closed chains: joined into cycles on the device; each record goes to its job
         if (res.n_cycle_lmtigs) {
-            if (!b->u_cyc_cnt.ensure(16)) return bfail(b, CFG_ERR_OOM, "cycle buffers");
-            unsigned long long cnt[2] = {0, 0};
-            BCK(cudaMemsetAsync(b->u_cyc_cnt.p, 0, 16, b->stream));
-            rc = collate_cycles_device(b->ub, n, nullptr, nullptr, b->u_cyc_cnt.as<unsigned long long>(), b->stream);
-            if (rc) return bfail(b, rc, "cycle sizing");
-            BCK(cudaMemcpyAsync(cnt, b->u_cyc_cnt.p, 16, cudaMemcpyDeviceToHost, b->stream));
+            uint64_t cyc_bytes = 0, cyc_n = 0;
+            std::vector<CycleRecord> recs;
+            rc = collate_cycles_on_device(b->ub, n, res.n_cycle_lmtigs, b->p.k, b->u_err.as<uint32_t>(), b->u_cyc_work,
+                                          b->u_cyc_scratch, b->u_cyc_out, b->stream, cyc_bytes, cyc_n, b->ub.job, &recs);
+            if (rc == CFG_ERR_OOM) return bfail(b, rc, "cycle buffers");
+            if (rc) return bfail(b, rc, "cycle collation");
+            std::string all(cyc_bytes, '\0');
+            if (cyc_bytes) BCK(cudaMemcpyAsync(&all[0], b->u_cyc_out.p, cyc_bytes, cudaMemcpyDeviceToHost, b->stream));
+            BCK(cudaMemcpyAsync(&err, b->u_err.p, 4, cudaMemcpyDeviceToHost, b->stream));
             BCK(cudaStreamSynchronize(b->stream));
-            if (!b->u_cyc_lm.ensure(sizeof(LmtigOut) * (cnt[0] + 1)) || !b->u_cyc_text.ensure(cnt[1] + 1) ||
-                !b->u_cyc_job.ensure(4 * (cnt[0] + 1)))
-                return bfail(b, CFG_ERR_OOM, "cycle buffers");
-            BCK(cudaMemsetAsync(b->u_cyc_cnt.p, 0, 16, b->stream));
-            rc = collate_cycles_device(b->ub, n, b->u_cyc_lm.as<LmtigOut>(), b->u_cyc_text.as<char>(),
-                                       b->u_cyc_cnt.as<unsigned long long>(), b->stream, b->u_cyc_job.as<uint32_t>());
-            if (rc) return bfail(b, rc, "cycle gather");
-            std::vector<cfg_lmtig> hl(cnt[0]);
-            std::vector<uint32_t> hj(cnt[0]);
-            std::string ht(cnt[1], '\0');
-            if (cnt[0]) {
-                BCK(cudaMemcpyAsync(hl.data(), b->u_cyc_lm.p, sizeof(cfg_lmtig) * cnt[0], cudaMemcpyDeviceToHost, b->stream));
-                BCK(cudaMemcpyAsync(hj.data(), b->u_cyc_job.p, 4 * cnt[0], cudaMemcpyDeviceToHost, b->stream));
-            }
-            if (cnt[1]) BCK(cudaMemcpyAsync(&ht[0], b->u_cyc_text.p, cnt[1], cudaMemcpyDeviceToHost, b->stream));
-            BCK(cudaStreamSynchronize(b->stream));
-            std::vector<std::vector<cfg_lmtig>> per(j1 - j0);
-            for (uint64_t i = 0; i < cnt[0]; ++i) per[hj[i]].push_back(hl[i]);
-            for (uint32_t j = j0; j < j1; ++j) {
-                if (per[j - j0].empty()) continue;
-                char* o = nullptr;
-                uint64_t ob2 = 0, nu = 0, nc = 0;
-                rc = cfg_collate_lmtigs(b->p.k, per[j - j0].data(), per[j - j0].size(), ht.data(), &o, &ob2, &nu, &nc);
-                if (rc) return bfail(b, rc, "cycle collation");
-                b->u_host[j].assign(o, ob2);
-                cfg_free(o);
-                b->u_host_n[j] = nu;
+            if (err & DERR_BAD_GRAPH) return bfail(b, CFG_ERR_STATE, "lm-tig ends on a closed chain do not pair up");
+            for (const CycleRecord& r : recs) {
+                const uint32_t j = j0 + r.job;   // the gathered lm-tigs' jobs count from j0
+                b->u_host[j].append(all, r.off, r.bytes);
+                ++b->u_host_n[j];
             }
         }
         j0 = j1;
@@ -960,8 +941,8 @@ void cfg_batch_destroy(cfg_batch* b) {
     for (DevBuf* x : bufs) x->release();
     b->h_fasta.release(); b->h_text.release(); b->h_lm.release(); b->h_unitigs.release();
     b->ub.release();
-    DevBuf* ubufs[] = {&b->u_n, &b->u_base, &b->u_out, &b->u_cur, &b->u_err, &b->u_cyc_lm, &b->u_cyc_text, &b->u_cyc_job,
-                       &b->u_cyc_cnt};
+    DevBuf* ubufs[] = {&b->u_n, &b->u_base, &b->u_out, &b->u_cur, &b->u_err, &b->u_cyc_work, &b->u_cyc_scratch,
+                       &b->u_cyc_out};
     for (DevBuf* x : ubufs) x->release();
     if (b->plain) cfg_destroy(b->plain);
     for (auto& e : b->ev) if (e) cudaEventDestroy(e);

@@ -3,6 +3,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 namespace cfg {
@@ -147,16 +148,17 @@ struct UnitigBuffers {
     }
 };
 // ... and what it produced: `bytes` of FASTA records at out, the unitigs among them,
-// and the lm-tigs left on closed chains (for the host).
+// and how many lm-tigs are left on closed chains (collate_cycles_on_device joins them).
 struct UnitigResult { uint64_t bytes, n_units, n_cycle_lmtigs; uint32_t rounds; };
 int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, UnitigResult& res);
-int collate_cycles_device(const UnitigBuffers& ub, uint64_t n, LmtigOut* out, char* text, unsigned long long* cnt,
-                          cudaStream_t s, uint32_t* out_job = nullptr);
 // The m lm-tigs on closed chains (fin == NONE after collate_device) joined into cycles on
 // the device, each written rotated to its canonical start: out_bytes of FASTA records at
 // `out`, n_cycles of them.  `work`, `scratch` and `out` grow as needed.  Renumbers fin.
+// With `records`, also where each record lies in `out` and (a batch: `job` non-null) whose it is.
+struct CycleRecord { uint32_t job; unsigned long long off, bytes; };
 int collate_cycles_on_device(UnitigBuffers& ub, uint64_t n, uint64_t m, uint32_t k, uint32_t* err, DevBuf& work,
-                             DevBuf& scratch, DevBuf& out, cudaStream_t s, uint64_t& out_bytes, uint64_t& n_cycles);
+                             DevBuf& scratch, DevBuf& out, cudaStream_t s, uint64_t& out_bytes, uint64_t& n_cycles,
+                             const uint32_t* job = nullptr, std::vector<CycleRecord>* records = nullptr);
 
 // FASTA (fastq = 0) or FASTQ text in device memory -> the packed stream and fragment
 // table in `pb` (cfg_parse.cu).  Synchronises the stream twice (two counts).

@@ -478,23 +478,6 @@ __global__ void k_ut_write(const uint32_t* __restrict__ lens, const char* const*
     }
 }
 
-// Lm-tigs on closed chains, with their labels, into small arrays for the host collator.
-__global__ void k_ut_cycles(const LmtigOut* __restrict__ lm, const char* const* __restrict__ label, uint64_t n,
-                            const uint32_t* __restrict__ fin, LmtigOut* out, char* text, unsigned long long* cnt,
-                            const uint32_t* __restrict__ job, uint32_t* out_job) {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        if (fin[i] != NONE) continue;
-        LmtigOut m = lm[i];
-        const unsigned long long slot = atomicAdd(cnt, 1ull);
-        const unsigned long long off = atomicAdd(cnt + 1, (unsigned long long)m.label_len);
-        if (!text) continue;   // sizing pass
-        for (uint32_t j = 0; j < m.label_len; ++j) text[off + j] = label[i][j];
-        m.label_off = off;
-        out[slot] = m;
-        if (out_job) out_job[slot] = job ? job[i] : 0u;
-    }
-}
-
 // ---- closed chains (cycles), joined on the device ----
 // The lm-tigs left on closed chains (fin == NONE) are numbered 0..m-1; entry X = 2 c + d
 // of cycle lm-tig c is it entered by its end d (0: u, read forward).  X's successor
@@ -521,6 +504,8 @@ __global__ void k_cy_number(uint32_t* fin, uint64_t n, uint32_t* cyc_lm, unsigne
 struct CyArgs {
     const LmtigOut* lm; const char* const* label; const uint32_t* partner; const uint32_t* fin;
     const uint32_t* cyc_lm; uint64_t m2;    // entries: 2 x cycle lm-tigs
+    const uint32_t* job;                    // batch: each gathered lm-tig's job (nullptr: one job)
+    uint32_t* rec_job;                      // per cycle record (in head order): its job
     uint32_t k;
     uint32_t *succ, *jmp0, *jmp1, *mn0, *mn1, *head;
     unsigned long long *w, *acc0, *acc1, *pos;
@@ -591,7 +576,9 @@ __global__ void k_cy_place(CyArgs a, const unsigned long long* __restrict__ D, u
             T_of[X] = T;
             scr_off[X] = atomicAdd(cur, T);
             out_off[X] = atomicAdd(cur + 1, T + a.k - 1 + 4);
-            heads[atomicAdd(cur + 2, 1ull)] = (uint32_t)X;
+            const unsigned long long hi = atomicAdd(cur + 2, 1ull);
+            heads[hi] = (uint32_t)X;
+            a.rec_job[hi] = a.job ? a.job[a.cyc_lm[X >> 1]] : 0u;
         }
     }
 }
@@ -715,21 +702,17 @@ bool UnitigBuffers::ensure(uint64_t n) {
     return true;
 }
 
-int collate_cycles_device(const UnitigBuffers& ub, uint64_t n, LmtigOut* out, char* text, unsigned long long* cnt,
-                          cudaStream_t s, uint32_t* out_job) {
-    k_ut_cycles<<<148 * 4, 256, 0, s>>>(ub.lm, ub.label, n, ub.fin, out, text, cnt, ub.job, out_job);
-    return cudaGetLastError() == cudaSuccess ? CFG_OK : CFG_ERR_CUDA;
-}
-
 int collate_cycles_on_device(UnitigBuffers& ub, uint64_t n, uint64_t m, uint32_t k, uint32_t* err, DevBuf& work,
-                             DevBuf& scratch, DevBuf& out, cudaStream_t s, uint64_t& out_bytes, uint64_t& n_cycles) {
+                             DevBuf& scratch, DevBuf& out, cudaStream_t s, uint64_t& out_bytes, uint64_t& n_cycles,
+                             const uint32_t* job, std::vector<CycleRecord>* records) {
     out_bytes = 0; n_cycles = 0;
+    if (records) records->clear();
     if (m == 0) return CFG_OK;
     if (2 * m >= CYC) return CFG_ERR_BAD_INPUT;
     const uint64_t m2 = 2 * m;
     // per entry: succ, jmp0, jmp1, mn0, mn1, head (u32); w, acc0, acc1, pos, T, scratch and
     // output offsets (u64); heads (u32); the cycle lm-tigs (u32, m); three counters
-    const size_t need = m2 * (7 * 4 + 7 * 8) + 4 * m + 512;   // + each array's 16-byte alignment
+    const size_t need = m2 * (8 * 4 + 7 * 8) + 4 * m + 512;   // + each array's 16-byte alignment
     if (!work.ensure(need)) return CFG_ERR_OOM;
     unsigned char* p = work.as<unsigned char>();
     auto take = [&](size_t bytes) { unsigned char* q = p; p += (bytes + 15) & ~(size_t)15; return q; };
@@ -744,8 +727,9 @@ int collate_cycles_on_device(UnitigBuffers& ub, uint64_t n, uint64_t m, uint32_t
     a.succ = (uint32_t*)take(4 * m2); a.jmp0 = (uint32_t*)take(4 * m2); a.jmp1 = (uint32_t*)take(4 * m2);
     a.mn0 = (uint32_t*)take(4 * m2); a.mn1 = (uint32_t*)take(4 * m2); a.head = (uint32_t*)take(4 * m2);
     uint32_t* heads = (uint32_t*)take(4 * m2);
+    a.rec_job = (uint32_t*)take(4 * m2);
     uint32_t* cyc_lm = (uint32_t*)take(4 * m);
-    a.cyc_lm = cyc_lm;
+    a.cyc_lm = cyc_lm; a.job = job;
     if (cudaMemsetAsync(cur, 0, 32, s) != cudaSuccess) return CFG_ERR_CUDA;
     const unsigned grid = (unsigned)std::min<uint64_t>(148ull * 8, (m2 + 255) / 256 + 1);
     k_cy_number<<<148 * 4, 256, 0, s>>>(ub.fin, n, cyc_lm, cur + 3);   // cur: scratch, output, chains, lm-tigs
@@ -775,6 +759,19 @@ int collate_cycles_on_device(UnitigBuffers& ub, uint64_t n, uint64_t m, uint32_t
         heads, cur + 2, T_of, scr_off, out_off, scratch.as<char>(), k, out.as<char>());
     if (cudaGetLastError() != cudaSuccess) return CFG_ERR_CUDA;
     out_bytes = h[1]; n_cycles = h[2];
+    if (records && h[2]) {   // where each record went and whose it is (head order)
+        std::vector<uint32_t> hh(h[2]), hj(h[2]);
+        std::vector<unsigned long long> off(m2), T(m2);
+        if (cudaMemcpyAsync(hh.data(), heads, 4 * h[2], cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaMemcpyAsync(hj.data(), a.rec_job, 4 * h[2], cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaMemcpyAsync(off.data(), out_off, 8 * m2, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaMemcpyAsync(T.data(), T_of, 8 * m2, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            return CFG_ERR_CUDA;
+        records->resize(h[2]);
+        for (uint64_t i = 0; i < h[2]; ++i)
+            (*records)[i] = CycleRecord{hj[i], off[hh[i]], T[hh[i]] + k - 1 + 4};
+    }
     return CFG_OK;
 }
 
