@@ -220,9 +220,10 @@ int launch_plan(cfg_ctx* c, const std::vector<Launch>& plan, uint64_t arena_slot
         // two CTAs per SM, and 1024 for the 8192-slot tables; k > 32: 256 up to 2048 slots,
         // three CTAs per SM); arena tables: that largest CTA
         const uint32_t tmax = subgraph_max_threads(W, L.cluster == 0 ? 0u : L.per);
+        const uint32_t div = c->p.slots_per_thread ? c->p.slots_per_thread : 4;
         const uint32_t threads = L.cluster == 0 ? tmax
                                  : L.cluster == 1 && L.per > 4096 ? tmax
-                                 : std::min<uint32_t>(tmax, std::max<uint32_t>(64, L.per / 4));
+                                 : std::min<uint32_t>(tmax, (std::max<uint32_t>(64, L.per / div) + 31) / 32 * 32);
         CK(launch_subgraphs(a, W, L.cluster, threads, c->stream));
         c->launches += 1;
         at += L.list.size();
@@ -409,7 +410,7 @@ int cfg_create(int device, const cfg_params* params, cfg_ctx** out) {
     *out = nullptr;
     if (!params) return CFG_ERR_BAD_INPUT;
     const cfg_params& p = *params;
-    if (p.k < 3 || p.k > 63 || (p.k % 2) == 0) return CFG_ERR_BAD_INPUT;
+    if (p.k < 3 || p.k > MAX_K || (p.k % 2) == 0) return CFG_ERR_BAD_INPUT;
     if (p.l < 1 || p.l > 32 || p.l > p.k - 1) return CFG_ERR_BAD_INPUT;
     if (p.cutoff < 1 || p.cutoff > 15) return CFG_ERR_BAD_INPUT;
     if (p.graph_count == 0 || p.graph_count > MAX_GRAPH_COUNT || (p.graph_count & (p.graph_count - 1))) return CFG_ERR_BAD_INPUT;
@@ -418,7 +419,7 @@ int cfg_create(int device, const cfg_params* params, cfg_ctx** out) {
     if (cudaSetDevice(device) != cudaSuccess) return CFG_ERR_CUDA;
     cfg_ctx* c = new (std::nothrow) cfg_ctx();
     if (!c) return CFG_ERR_OOM;
-    c->device = device; c->p = p; c->G = p.graph_count; c->words = p.k <= 31 ? 1 : 2;
+    c->device = device; c->p = p; c->G = p.graph_count; c->words = key_words(p.k);
     {
         int sms = 0;
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0) c->sms = (uint32_t)sms;

@@ -292,7 +292,7 @@ int plan_shapes(cfg_batch* b) {
         b->shapes.push_back(Shape{cc.nl + cl - 2, cl, t, cc.per_cl, (uint32_t)occ * cl});
     }
     b->shapes.push_back(Shape{cc.nl + 7, 0, subgraph_max_threads(b->words, 0), 0,
-                              (uint32_t)((b->words == 1 ? 2 : 3) * sms)});
+                              (uint32_t)((b->words == 2 ? 3 : 2) * sms)});   // the arena kernels' CTAs per SM
     return CFG_OK;
 }
 
@@ -498,7 +498,7 @@ int cfg_batch_create(int device, const cfg_params* params, cfg_batch** out) {
     *out = nullptr;
     if (!params) return CFG_ERR_BAD_INPUT;
     const cfg_params& p = *params;
-    if (p.k < 3 || p.k > 63 || (p.k % 2) == 0 || p.l < 1 || p.l > 32 || p.l > p.k - 1) return CFG_ERR_BAD_INPUT;
+    if (p.k < 3 || p.k > MAX_K || (p.k % 2) == 0 || p.l < 1 || p.l > 32 || p.l > p.k - 1) return CFG_ERR_BAD_INPUT;
     if (p.cutoff < 1 || p.cutoff > 15) return CFG_ERR_BAD_INPUT;
     if (p.graph_count == 0 || p.graph_count > 65536 || (p.graph_count & (p.graph_count - 1))) return CFG_ERR_BAD_INPUT;
     if (p.flags) return CFG_ERR_BAD_INPUT;   // no state or record dumps in batches
@@ -507,7 +507,7 @@ int cfg_batch_create(int device, const cfg_params* params, cfg_batch** out) {
     if (cudaSetDevice(device) != cudaSuccess) return CFG_ERR_CUDA;
     cfg_batch* b = new (std::nothrow) cfg_batch();
     if (!b) return CFG_ERR_OOM;
-    b->device = device; b->p = p; b->G = p.graph_count; b->G_params = p.graph_count; b->words = p.k <= 31 ? 1 : 2;
+    b->device = device; b->p = p; b->G = p.graph_count; b->G_params = p.graph_count; b->words = key_words(p.k);
     b->g_shift = 0;
     while ((1u << b->g_shift) < b->G) ++b->g_shift;
     b->tune.table_load_pct = p.table_load_pct ? p.table_load_pct : 100;

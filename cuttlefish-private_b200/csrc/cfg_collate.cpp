@@ -23,15 +23,22 @@
 namespace {
 
 struct End {          // one non-phi end of an lm-tig
-    uint64_t hi, lo;  // canonical k-mer
+    uint64_t w[4];    // canonical k-mer, words as in cfg_lmtig::u
     uint32_t side;    // attachment side: 0 front, 1 back
     uint32_t id;      // lm-tig index << 1 | end (0 = u, 1 = v)
+    bool same_vertex(const End& o) const { return std::memcmp(w, o.w, sizeof w) == 0; }
     bool operator<(const End& o) const {
-        if (hi != o.hi) return hi < o.hi;
-        if (lo != o.lo) return lo < o.lo;
+        for (int j = 3; j >= 0; --j)
+            if (w[j] != o.w[j]) return w[j] < o.w[j];
         return side < o.side;
     }
 };
+End end_of(const uint64_t* key, uint32_t side, uint32_t id) {
+    End e;
+    std::memcpy(e.w, key, sizeof e.w);
+    e.side = side; e.id = id;
+    return e;
+}
 
 inline char comp(char c) { return c == 'A' ? 'T' : c == 'C' ? 'G' : c == 'G' ? 'C' : 'A'; }
 
@@ -80,20 +87,20 @@ void canonical_cycle(std::string& s, uint32_t k) {
 
 extern "C" int cfg_collate_lmtigs(uint32_t k, const cfg_lmtig* lm, uint64_t n_lm, const char* text,
                                   char** out, uint64_t* out_bytes, uint64_t* n_unitigs, uint64_t* n_cycles) {
-    if (!out || !out_bytes || (n_lm && (!lm || !text)) || k < 3 || k > 63 || n_lm >= (1ull << 31)) return CFG_ERR_BAD_INPUT;
+    if (!out || !out_bytes || (n_lm && (!lm || !text)) || k < 3 || k > 127 || n_lm >= (1ull << 31)) return CFG_ERR_BAD_INPUT;
     std::vector<End> ends;
     ends.reserve(2 * n_lm);
     for (uint64_t i = 0; i < n_lm; ++i) {
         const uint8_t f = lm[i].flags;
-        if (!(f & 4)) ends.push_back(End{lm[i].u[1], lm[i].u[0], (uint32_t)(f & 1), (uint32_t)(i << 1)});
-        if (!(f & 8)) ends.push_back(End{lm[i].v[1], lm[i].v[0], (uint32_t)((f >> 1) & 1), (uint32_t)((i << 1) | 1)});
+        if (!(f & 4)) ends.push_back(end_of(lm[i].u, (uint32_t)(f & 1), (uint32_t)(i << 1)));
+        if (!(f & 8)) ends.push_back(end_of(lm[i].v, (uint32_t)((f >> 1) & 1), (uint32_t)((i << 1) | 1)));
     }
     std::sort(ends.begin(), ends.end());
     // partner of each end: the other side of the same vertex
     std::vector<uint32_t> partner(2 * n_lm, 0xffffffffu);
     for (size_t a = 0; a < ends.size();) {
         size_t b = a;
-        while (b < ends.size() && ends[b].hi == ends[a].hi && ends[b].lo == ends[a].lo) ++b;
+        while (b < ends.size() && ends[b].same_vertex(ends[a])) ++b;
         if (b - a > 2 || (b - a == 2 && ends[a].side == ends[a + 1].side)) return CFG_ERR_STATE;   // not a valid graph
         if (b - a == 2) { partner[ends[a].id] = ends[a + 1].id; partner[ends[a + 1].id] = ends[a].id; }
         a = b;

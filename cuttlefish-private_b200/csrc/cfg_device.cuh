@@ -1,8 +1,8 @@
 // cfg_device.cuh -- device primitives of the compaction hot path (sm_100a).
 //
 // 2-bit bases A0 C1 G2 T3 (include/DNA.hpp:16-24); a k-mer is the big-endian
-// 2-bit number of its bases, split in a low word (last 32 bases) and a high
-// word (the first k-32 bases), which is Kmer<k>'s layout
+// 2-bit number of its bases in W = ceil(k/32) words, the lowest word holding the
+// last 32 bases and the highest the first k - 32(W-1), which is Kmer<k>'s layout
 // (include/Kmer.hpp:45-54) and its ordering (:509-521).
 #pragma once
 
@@ -66,19 +66,38 @@ __device__ __forceinline__ uint32_t base_at(const uint64_t* __restrict__ s, uint
 }
 
 // ---------------------------------------------------------------------------
-// k-mer words.  W = 1 (k <= 31) or 2 (33 <= k <= 63).
-template <int W> struct Kmer;
+// k-mer words.  W = 1 (k <= 31), 2 (33 <= k <= 63), 3 (65 <= k <= 95) or 4 (97 <= k <= 127).
+// word(i): word i from the lowest (the last 32 bases); i < W.
+template <int W> struct Kmer {   // W = 3, 4
+    uint64_t w[W];
+    __device__ __forceinline__ bool operator==(const Kmer& o) const {
+        bool e = true;
+#pragma unroll
+        for (int i = 0; i < W; ++i) e &= w[i] == o.w[i];
+        return e;
+    }
+    __device__ __forceinline__ bool operator<(const Kmer& o) const {   // words compared from the highest
+#pragma unroll
+        for (int i = W - 1; i > 0; --i)
+            if (w[i] != o.w[i]) return w[i] < o.w[i];
+        return w[0] < o.w[0];
+    }
+    __device__ __forceinline__ uint64_t hi_word() const { return w[W - 1]; }
+    __device__ __forceinline__ uint64_t word(int i) const { return w[i]; }
+};
 template <> struct Kmer<1> {
     uint64_t lo;
     __device__ __forceinline__ bool operator==(const Kmer& o) const { return lo == o.lo; }
     __device__ __forceinline__ bool operator<(const Kmer& o) const { return lo < o.lo; }
     __device__ __forceinline__ uint64_t hi_word() const { return 0; }
+    __device__ __forceinline__ uint64_t word(int) const { return lo; }
 };
 template <> struct Kmer<2> {
     uint64_t lo, hi;
     __device__ __forceinline__ bool operator==(const Kmer& o) const { return lo == o.lo && hi == o.hi; }
     __device__ __forceinline__ bool operator<(const Kmer& o) const { return hi != o.hi ? hi < o.hi : lo < o.lo; }
     __device__ __forceinline__ uint64_t hi_word() const { return hi; }
+    __device__ __forceinline__ uint64_t word(int i) const { return i ? hi : lo; }
 };
 
 template <int W> struct KOps;
@@ -137,9 +156,70 @@ template <> struct KOps<2> {
         return x.lo == rep && x.hi == (rep & mhi);
     }
 };
+// W = 3, 4: the highest word holds nh = k - 32(W-1) bases (1..31), every other word 32.
+template <int W> struct KOps {
+    uint32_t k, nh; uint64_t mhi;
+    __host__ __device__ KOps(uint32_t k_) : k(k_), nh(k_ - 32 * (W - 1)), mhi((1ull << (2 * (k_ - 32 * (W - 1)))) - 1) {}
+    __device__ __forceinline__ void push_back(Kmer<W>& x, uint32_t b) const {
+#pragma unroll
+        for (int i = W - 1; i > 0; --i) x.w[i] = (x.w[i] << 2) | (x.w[i - 1] >> 62);
+        x.w[W - 1] &= mhi;
+        x.w[0] = (x.w[0] << 2) | b;
+    }
+    __device__ __forceinline__ void push_front(Kmer<W>& x, uint32_t b) const {
+#pragma unroll
+        for (int i = 0; i < W - 1; ++i) x.w[i] = (x.w[i] >> 2) | (x.w[i + 1] << 62);
+        x.w[W - 1] = (x.w[W - 1] >> 2) | ((uint64_t)b << (2 * (nh - 1)));
+    }
+    // reverse complement: the words' own reverse complements in reverse order form that
+    // of the 32W-base number with 32 - nh leading A's; dropping its last 32 - nh bases
+    // (a right shift by 2(32 - nh) bits, 2..62) leaves the k-mer's
+    __device__ __forceinline__ Kmer<W> rc(const Kmer<W>& x) const {
+        uint64_t r[W];
+#pragma unroll
+        for (int j = 0; j < W; ++j) r[j] = rc_word(x.w[W - 1 - j], 32);
+        const uint32_t sh = 2 * (32 - nh);
+        Kmer<W> o;
+#pragma unroll
+        for (int j = 0; j < W - 1; ++j) o.w[j] = (r[j] >> sh) | (r[j + 1] << (64 - sh));
+        o.w[W - 1] = r[W - 1] >> sh;
+        return o;
+    }
+    __device__ __forceinline__ uint32_t first_base(const Kmer<W>& x) const { return (uint32_t)(x.w[W - 1] >> (2 * (nh - 1))) & 3; }
+    __device__ __forceinline__ uint32_t last_base(const Kmer<W>& x) const { return (uint32_t)x.w[0] & 3; }
+    __device__ __forceinline__ uint32_t base(const Kmer<W>& x, uint32_t i) const {
+        const uint32_t bp = 2 * (k - 1 - i), wi = bp >> 6;
+        uint64_t v = x.w[0];
+#pragma unroll
+        for (int j = 1; j < W; ++j) v = wi == (uint32_t)j ? x.w[j] : v;   // a select, not an indexed load
+        return (uint32_t)(v >> (bp & 63)) & 3;
+    }
+    __device__ __forceinline__ Kmer<W> load(const uint64_t* s, uint64_t p) const {
+        Kmer<W> r;
+        r.w[W - 1] = window64(s, p) >> (64 - 2 * nh);
+#pragma unroll
+        for (int j = W - 2; j >= 0; --j) r.w[j] = window64(s, p + nh + 32 * (W - 2 - j));
+        return r;
+    }
+    __device__ __forceinline__ bool is_homopolymer(const Kmer<W>& x, uint32_t b) const {
+        const uint64_t rep = 0x5555555555555555ull * b;
+        bool e = x.w[W - 1] == (rep & mhi);
+#pragma unroll
+        for (int j = 0; j < W - 1; ++j) e &= x.w[j] == rep;
+        return e;
+    }
+};
 
+// the k-mer's words folded into one (W >= 3); W <= 2 fold inline below
+template <int W> __device__ __forceinline__ uint64_t fold_words(const Kmer<W>& x) {
+    const uint64_t C[3] = {0xC2B2AE3D27D4EB4Full, 0x165667B19E3779F9ull, 0x27D4EB2F165667C5ull};
+    uint64_t t = x.word(0);
+#pragma unroll
+    for (int j = 1; j < W; ++j) t ^= x.word(j) * C[j - 1];
+    return t;
+}
 template <int W> __device__ __forceinline__ uint64_t key_hash(const Kmer<W>& x) {
-    uint64_t z = x.lo ^ (x.hi_word() * 0x9E3779B97F4A7C15ull);
+    uint64_t z = W <= 2 ? x.word(0) ^ (x.hi_word() * 0x9E3779B97F4A7C15ull) : fold_words(x) * 0x9E3779B97F4A7C15ull;
     z ^= z >> 33; z *= 0xFF51AFD7ED558CCDull;
     z ^= z >> 33; z *= 0xC4CEB9FE1A85EC53ull;
     z ^= z >> 33;

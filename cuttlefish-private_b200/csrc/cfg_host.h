@@ -120,6 +120,7 @@ struct UnitigInput {
 struct UnitigBuffers {
     DevBuf b_lm, b_label, b_tab, b_partner, b_X0, b_X1, b_fin, b_off, b_words, b_out, b_job, b_flip, b_sx, b_sw, b_len, b_ends;
     ulonglong2* ends = nullptr;   // both ends of each gathered lm-tig, packed for the pairing pass
+    uint32_t end_words = 2;       // 64-bit words per end there: 2 for k <= 63, 4 beyond (set from k)
     uint32_t* len = nullptr;   // each gathered lm-tig's label length (the kernels that need only it read 4 bytes, not 48)
     uint8_t* flipb = nullptr;  // per lm-tig heading its chain's walked list: flip it
     LmtigOut* lm = nullptr;

@@ -87,7 +87,7 @@ struct ScatterArgs {
 };
 
 struct LmtigOut {                // mirrors cfg_lmtig
-    uint64_t u[2], v[2];
+    uint64_t u[4], v[4];
     uint64_t label_off;
     uint32_t label_len;
     uint16_t g;
@@ -95,7 +95,7 @@ struct LmtigOut {                // mirrors cfg_lmtig
 };
 
 struct StateOut {                // mirrors cfg_state
-    uint64_t key[2];
+    uint64_t key[4];
     uint32_t ef;
     uint16_t g;
     uint8_t status, pad;
@@ -176,8 +176,14 @@ constexpr uint32_t OUT_STRIPES = 32;
 void launch_stripe_fixup(LmtigOut* lm, uint64_t lm_slice, const unsigned long long* lm_used,
                          const unsigned long long* text_base, uint32_t stripes, cudaStream_t s);
 
-// bytes per table slot: k-mer (8 per word) + state word (8) + meta (4) + work-list entry (4)
-__host__ __device__ inline uint32_t slot_bytes(int words) { return words == 1 ? 24u : 32u; }
+// Largest k: Kmer<k> of the reference built with INSTANCE_COUNT = 64 (include/globals.hpp:16-22,45).
+constexpr uint32_t MAX_K = 127;
+// 64-bit words of a k-mer: 1 for k <= 31, 2 up to 63, 3 up to 95, 4 up to 127.
+__host__ __device__ constexpr int key_words(uint32_t k) { return (int)((k + 31) / 32); }
+
+// bytes per table slot: k-mer (8 per word; 16 bytes for 2 words, 32 for 3 or 4) + state
+// word (8) + meta (4) + work-list entry (4)
+__host__ __device__ constexpr uint32_t slot_bytes(int words) { return words == 1 ? 24u : words == 2 ? 32u : 48u; }
 
 void launch_partition(const PartitionArgs& a, cudaStream_t s);
 void launch_bucket_scan(const unsigned long long* hist, uint32_t G, uint32_t* bucket_off, uint32_t* inst,

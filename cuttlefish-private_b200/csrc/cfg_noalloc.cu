@@ -103,7 +103,7 @@ extern "C" int cfg_partition_noalloc(int device, const cfg_params* p, const uint
                                      const uint64_t* d_frag_off, const uint32_t* d_frag_len, uint64_t n_frags,
                                      cfg_record* d_records, uint64_t records_cap, uint32_t* d_bucket_off,
                                      uint64_t* d_n_records, void* stream) {
-    if (!p || p->k < 3 || p->k > 63 || (p->k % 2) == 0 || p->l < 1 || p->l > 32 || p->l > p->k - 1) return CFG_ERR_BAD_INPUT;
+    if (!p || p->k < 3 || p->k > MAX_K || (p->k % 2) == 0 || p->l < 1 || p->l > 32 || p->l > p->k - 1) return CFG_ERR_BAD_INPUT;
     if (p->graph_count == 0 || p->graph_count > NOALLOC_MAX_GRAPHS || (p->graph_count & (p->graph_count - 1))) return CFG_ERR_BAD_INPUT;
     if (n_bases > NOALLOC_MAX_BASES) return CFG_ERR_BAD_INPUT;   // beyond the fixed scratch: refuse, never overflow
     if ((n_bases && !d_packed) || (n_frags && (!d_frag_off || !d_frag_len)) || !d_bucket_off || !d_n_records) return CFG_ERR_BAD_INPUT;

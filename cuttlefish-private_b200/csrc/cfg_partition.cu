@@ -20,6 +20,7 @@ namespace {
 
 constexpr int WARPS_PER_BLOCK = 8;
 constexpr uint32_t STAGE = 256;       // records a warp gathers in shared memory per reservation
+constexpr uint32_t MODW = 160;        // residues kept: the cut test indexes up to w - 1 + 32
 
 __device__ __forceinline__ uint32_t lanemask_lt() { uint32_t m; asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m)); return m; }
 
@@ -79,11 +80,11 @@ __device__ __forceinline__ uint64_t from_back(uint64_t cur, uint64_t prev, uint3
 __device__ __forceinline__ uint64_t min64(uint64_t a, uint64_t b) { return a < b ? a : b; }
 
 // The sparse table's depth E = floor(log2 w) is a template argument: levels 2^0 .. 2^E,
-// none more (w <= 62: E <= 5).
+// none more (w = k - l <= 126: E <= 6).
 
 // Processes the (k-1)-mer positions [j0, j1) of one fragment: emits every weak
 // super k-mer whose run starts there.
-// mod_w[x] = x % w for x < 128 (w <= 62): the cap-cut test without a division.
+// mod_w[x] = x % w for x < MODW (w <= 126): the cap-cut test without a division.
 // hist: this fragment's job's histogram (the run's, or its job's slice of a batch's);
 // nullptr when the bucket sort counts the records itself.
 //
@@ -94,7 +95,8 @@ __device__ __forceinline__ uint64_t min64(uint64_t a, uint64_t b) { return a < b
 // lanes, from the previous chunk).  The window of (k-1)-mer j = q - w + 1 is then two
 // overlapping blocks of 2^E hashes, E = floor(log2 w): min(level_E[j], level_E[q-2^E+1]),
 // the second the lane's own value, the first that of the lane w - 2^E before it.
-// O(log w) work per position, no shared memory.
+// O(log w) work per position, no shared memory.  For w >= 96 (E = 6, dq = w - 64 > 32)
+// the second block starts two chunks back: level E of the chunk before the previous is kept.
 template <int E>
 __device__ void sweep_fragment(const PartitionArgs& a, const uint8_t* mod_w, uint64_t F0, uint32_t FL,
                                uint32_t j0, uint32_t j1, unsigned long long* hist, Stage& st) {
@@ -109,21 +111,28 @@ __device__ void sweep_fragment(const PartitionArgs& a, const uint8_t* mod_w, uin
         return (q >= 0 && q < (int64_t)n_lmers) ? lmer_hash_at(a, F0 + (uint64_t)q, l) : ~0ull;
     };
     uint64_t lv[E + 1], pv[E + 1];   // this chunk's / the previous chunk's level values
+    uint64_t ppE = ~0ull;            // level E two chunks back (E = 6 only)
 #pragma unroll
     for (int i = 0; i <= E; ++i) pv[i] = ~0ull;
     auto levels = [&](uint64_t h) -> uint64_t {   // adds this chunk's hashes; the window minimum
         lv[0] = h;
 #pragma unroll
         for (int i = 1; i <= E; ++i) lv[i] = min64(lv[i - 1], from_back(lv[i - 1], pv[i - 1], 1u << (i - 1), lane));
-        const uint64_t m = min64(lv[E], from_back(lv[E], pv[E], dq, lane));
+        uint64_t m;
+        if constexpr (E >= 6) {   // dq <= 63: the block's start lies in one of the two chunks before
+            m = dq <= 32 ? min64(lv[E], from_back(lv[E], pv[E], dq, lane))
+                         : min64(lv[E], from_back(pv[E], ppE, dq - 32, lane));
+            ppE = pv[E];
+        } else {
+            m = min64(lv[E], from_back(lv[E], pv[E], dq, lane));
+        }
 #pragma unroll
         for (int i = 0; i <= E; ++i) pv[i] = lv[i];
         return m;
     };
-    // prime the levels with the chunks before the first (their newest hashes reach back to
-    // l-mer `start`: one chunk for w <= 33, two up to w = 62)
-    if (w - 1 > 32) levels(hash_at((int64_t)start - 64 + w - 1 + lane));
-    levels(hash_at((int64_t)start - 32 + w - 1 + lane));
+    // prime the levels with the chunks before the first: their hashes reach back to l-mer
+    // `start`, ceil((w - 1) / 32) chunks (at least one)
+    for (int c = (int)max(1u, (w - 1 + 31) / 32); c >= 1; --c) levels(hash_at((int64_t)start - 32 * c + w - 1 + lane));
 
     bool active = false;
     uint32_t r0 = 0, last_cut = 0, last_cut_g = 0, last_cut_chg = 0, carry_g = 0;
@@ -225,8 +234,8 @@ __device__ void sweep_fragment(const PartitionArgs& a, const uint8_t* mod_w, uin
 template <int E>
 __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) k_partition(const PartitionArgs a) {
     __shared__ uint64_t stages[WARPS_PER_BLOCK][STAGE];
-    __shared__ uint8_t mod_w[128];
-    if (threadIdx.x < 128) mod_w[threadIdx.x] = (uint8_t)(threadIdx.x % a.w);
+    __shared__ uint8_t mod_w[MODW];
+    if (threadIdx.x < MODW) mod_w[threadIdx.x] = (uint8_t)(threadIdx.x % a.w);
     __syncthreads();
     Stage st{stages[threadIdx.x >> 5], 0};
     // this launch's bases and fragments (the fragment table is read only inside them:
@@ -395,13 +404,14 @@ void launch_partition(const PartitionArgs& a, cudaStream_t s) {
     if (blocks > (1u << 20)) blocks = 1u << 20;
     if (blocks == 0) return;
     const dim3 grid((unsigned)blocks), block(WARPS_PER_BLOCK * 32);
-    switch (31 - __builtin_clz(a.w)) {   // floor(log2 w), w = k - l in [1, 62]
+    switch (31 - __builtin_clz(a.w)) {   // floor(log2 w), w = k - l in [1, 126]
         case 0: k_partition<0><<<grid, block, 0, s>>>(a); break;
         case 1: k_partition<1><<<grid, block, 0, s>>>(a); break;
         case 2: k_partition<2><<<grid, block, 0, s>>>(a); break;
         case 3: k_partition<3><<<grid, block, 0, s>>>(a); break;
         case 4: k_partition<4><<<grid, block, 0, s>>>(a); break;
-        default: k_partition<5><<<grid, block, 0, s>>>(a); break;
+        case 5: k_partition<5><<<grid, block, 0, s>>>(a); break;
+        default: k_partition<6><<<grid, block, 0, s>>>(a); break;
     }
 }
 

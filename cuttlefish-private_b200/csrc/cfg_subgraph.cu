@@ -149,7 +149,9 @@ struct Tab {
         if constexpr (MODE == CLUSTER) return mapa_cluster(base + (s & pmask) * bytes, s >> shift);
         else return base + (A)s * bytes;
     }
-    __device__ __forceinline__ A ka(uint32_t s) const { return addr(keys, s, 16); }
+    // a slot's key: 16 bytes for k <= 63 (for k <= 31 with the state word), 32 beyond
+    static constexpr uint32_t KB = W <= 2 ? 16 : 32;
+    __device__ __forceinline__ A ka(uint32_t s) const { return addr(keys, s, KB); }
     __device__ __forceinline__ A sa(uint32_t s) const { return addr(st, s, W == 1 ? 16 : 8); }
     __device__ __forceinline__ A ma(uint32_t s) const { return addr(meta, s, 4); }
 
@@ -160,7 +162,13 @@ struct Tab {
     __device__ __forceinline__ Kmer<W> key(uint32_t s) const {
         const A a = ka(s);
         if constexpr (W == 1) return Kmer<1>{M::ld64(a)};
-        else return Kmer<2>{M::ld64(a), M::ld64(a + 8)};
+        else if constexpr (W == 2) return Kmer<2>{M::ld64(a), M::ld64(a + 8)};
+        else {
+            Kmer<W> x;
+#pragma unroll
+            for (int j = 0; j < W; ++j) x.w[j] = M::ld64(a + 8 * j);
+            return x;
+        }
     }
     // owner rank and home index inside the owner's sub-table
     __device__ __forceinline__ void place(const Kmer<W>& x, uint32_t& r, uint32_t& h) const {
@@ -168,7 +176,8 @@ struct Tab {
             // one table: a multiplicative hash's top bits pick the home slot
             uint64_t z;
             if constexpr (W == 1) z = x.lo * 0x9E3779B97F4A7C15ull;
-            else z = (x.lo ^ (x.hi * 0xC2B2AE3D27D4EB4Full)) * 0x9E3779B97F4A7C15ull;
+            else if constexpr (W == 2) z = (x.lo ^ (x.hi * 0xC2B2AE3D27D4EB4Full)) * 0x9E3779B97F4A7C15ull;
+            else z = fold_words(x) * 0x9E3779B97F4A7C15ull;
             r = 0;
             h = (uint32_t)(((z >> 32) * per) >> 32);
         } else {
@@ -190,15 +199,22 @@ struct Tab {
                 if (top == EMPTY) return NONE;
                 if (top == x.lo) return b + h;
             } else {
-                const uint64_t top = M::ld64(a + 8);
+                const uint64_t top = M::ld64(a + 8 * (W - 1));
                 if (top == EMPTY) return NONE;
-                if (top == x.hi && M::ld64(a) == x.lo) { stv = ld_st(b + h); return b + h; }
+                if (top == x.hi_word() && low_words_match(a, x)) { stv = ld_st(b + h); return b + h; }
             }
             if (++h == per) h = 0;
         }
         return NONE;
     }
     __device__ __forceinline__ uint32_t find(const Kmer<W>& x) const { uint64_t t; return find(x, t); }
+    // words 0 .. W-2 of the key at a equal x's (W >= 2)
+    __device__ __forceinline__ bool low_words_match(A a, const Kmer<W>& x) const {
+        bool e = true;
+#pragma unroll
+        for (int j = 0; j < W - 1; ++j) e &= M::ld64(a + 8 * j) == x.word(j);
+        return e;
+    }
     // build phase: find or insert x in sub-table `owner` starting at its home index h;
     // returns the global slot or NONE.  Other ranks' sub-tables are reached through DSMEM.
     // `seen`: a recent value of the slot's state word, the first expected value of its CAS
@@ -217,15 +233,17 @@ struct Tab {
                     if (old == x.lo) { seen = stv; return b + h; }
                 }
             } else {
-                // two-word key: claim the high word with a 64-bit CAS (EMPTY -> BUSY), write
-                // the low word, then publish the high word; readers wait (bounded) on BUSY
-                uint64_t hi = M::ld64(a + 8);
+                // multi-word key: claim the highest word with a 64-bit CAS (EMPTY -> BUSY),
+                // write the others, then publish the highest; readers wait (bounded) on BUSY
+                const A at = a + 8 * (W - 1);
+                uint64_t hi = M::ld64(at);
                 if (hi == EMPTY) {
-                    hi = M::cas64(a + 8, EMPTY, BUSY);
+                    hi = M::cas64(at, EMPTY, BUSY);
                     if (hi == EMPTY) {
-                        M::st64(a, x.lo);
+#pragma unroll
+                        for (int j = 0; j < W - 1; ++j) M::st64(a + 8 * j, x.word(j));
                         M::fence();
-                        M::exch64(a + 8, x.hi);
+                        M::exch64(at, x.hi_word());
                         fresh = true;
                         seen = ST_INIT;
                         return b + h;
@@ -233,11 +251,11 @@ struct Tab {
                 }
                 for (uint32_t spin = 0; hi == BUSY; ++spin) {
                     if (spin > (1u << 24)) { atomicOr(err_flag, DERR_CAS_LIMIT); return NONE; }
-                    hi = M::ld64(a + 8);
+                    hi = M::ld64(at);
                 }
-                if (hi == x.hi) {
+                if (hi == x.hi_word()) {
                     M::fence();
-                    if (M::ld64(a) == x.lo) { seen = M::ld64(sa(b + h)); return b + h; }
+                    if (low_words_match(a, x)) { seen = M::ld64(sa(b + h)); return b + h; }
                 }
             }
             if (++h == per) h = 0;
@@ -425,12 +443,20 @@ template <int W>
 __device__ __forceinline__ Kmer<W> phi_kmer(const KOps<W>& ops) {   // all-T k-mer, include/Discontinuity_Graph.hpp:44-49
     Kmer<W> x;
     if constexpr (W == 1) x.lo = ops.mask;
-    else { x.lo = ~0ull; x.hi = ops.mhi; }
+    else if constexpr (W == 2) { x.lo = ~0ull; x.hi = ops.mhi; }
+    else {
+#pragma unroll
+        for (int j = 0; j < W - 1; ++j) x.w[j] = ~0ull;
+        x.w[W - 1] = ops.mhi;
+    }
     return x;
 }
 
 template <int W>
-__device__ __forceinline__ void put_key(uint64_t out[2], const Kmer<W>& x) { out[0] = x.lo; out[1] = x.hi_word(); }
+__device__ __forceinline__ void put_key(uint64_t out[4], const Kmer<W>& x) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) out[j] = j < W ? x.word(j < W ? j : 0) : 0ull;
+}
 
 // A vertex in walk direction: its directed k-mer, the reverse complement, and its slot.
 template <int W> struct DV { Kmer<W> d, r; uint32_t slot; uint64_t st; };   // st: the slot's state word
@@ -532,7 +558,8 @@ __device__ void write_kmer_cycle(const Tab<W, MODE>& T, const KOps<W>& ops, uint
 
 template <int W>
 __device__ __forceinline__ bool local_empty(const unsigned long long* lkeys, uint32_t ls) {
-    return lkeys[(size_t)ls * 2 + (W - 1)] == EMPTY;   // the key's high word (16 bytes per slot's key part)
+    // the key's highest word (16 bytes per slot's key part for k <= 63, 32 beyond)
+    return lkeys[(size_t)ls * (W <= 2 ? 2 : 4) + (W - 1)] == EMPTY;
 }
 // index of local slot ls's state word in the state array (interleaved with the keys for k <= 31)
 template <int W> __device__ __forceinline__ uint32_t sti(uint32_t ls) { return W == 1 ? 2 * ls : ls; }
@@ -541,18 +568,21 @@ struct EndInfo { uint32_t slot; uint32_t term; bool canon; };   // a path end in
 
 // The bases of one weak super k-mer, MSB-first from its first base (base 0 at bits
 // 63:62 of w[0]): 2 words for k <= 31 (a record holds at most 2(k-1)-l+2 <= 61
-// bases), 4 for k <= 63 (<= 125).  The packed stream carries 4 words of padding.
+// bases), 4 for k <= 63 (<= 125), 6 for k <= 95 (<= 189), 8 for k <= 127 (<= 253).
+// The packed stream carries 4 words of padding, which covers the unconditional loads
+// of k <= 63; wider records load only the words that hold their len bases.
 template <int W>
 struct RecWords {
-    static constexpr int NW = W == 1 ? 2 : 4;
+    static constexpr int NW = 2 * W;
     uint64_t w[NW];
     __device__ __forceinline__ RecWords() {}
-    __device__ __forceinline__ RecWords(const uint64_t* __restrict__ s, uint32_t pos, bool has) {
+    __device__ __forceinline__ RecWords(const uint64_t* __restrict__ s, uint32_t pos, bool has, uint32_t len = 0) {
         const uint64_t q = pos >> 5;
         const uint32_t sh = 2 * (pos & 31);
+        const uint32_t last = ((pos & 31) + (len ? len : 1) - 1) >> 5;   // the record's last word, from q
         uint64_t a[NW + 1];
 #pragma unroll
-        for (int i = 0; i <= NW; ++i) a[i] = has ? __ldg(s + q + i) : 0ull;
+        for (int i = 0; i <= NW; ++i) a[i] = has && (W <= 2 || (uint32_t)i <= last) ? __ldg(s + q + i) : 0ull;
 #pragma unroll
         for (int i = 0; i < NW; ++i) w[i] = sh ? (a[i] << sh) | (a[i + 1] >> (64 - sh)) : a[i];
     }
@@ -583,10 +613,16 @@ struct RecWords {
             const uint64_t win = bases64(idx);   // idx + k <= 61 < 64: the k-mer and its successor
             x.lo = win >> (64 - 2 * k);
             succ = idx + k == len ? BASE_E : (uint32_t)(win >> (62 - 2 * k)) & 3;
-        } else {
+        } else if constexpr (W == 2) {
             const uint32_t nh = k - 32;          // bases in the high word
             x.hi = bases64(idx) >> (64 - 2 * nh);
             x.lo = bases64(idx + nh);
+            succ = idx + k == len ? BASE_E : base(idx + k);
+        } else {
+            const uint32_t nh = k - 32 * (W - 1);   // bases in the highest word
+            x.w[W - 1] = bases64(idx) >> (64 - 2 * nh);
+#pragma unroll
+            for (int j = W - 2; j >= 0; --j) x.w[j] = bases64(idx + nh + 32 * (W - 2 - j));
             succ = idx + k == len ? BASE_E : base(idx + k);
         }
         pred = idx == 0 ? BASE_E : base(idx - 1);
@@ -613,11 +649,13 @@ __device__ __forceinline__ WalkSeq walk_seq(uint32_t k, const Kmer<W>& first, ui
         const uint32_t sh = 2 * k;
         const uint64_t f = rev_bases(first.lo) >> (64 - sh);
         q.w0 = f | (s0 << sh); q.w1 = (s0 >> (64 - sh)) | (s1 << sh); q.w2 = s1 >> (64 - sh); q.w3 = 0;
-    } else {                  // 33 <= k <= 63: hi holds the first k - 32 bases
+    } else if constexpr (W == 2) {   // 33 <= k <= 63: hi holds the first k - 32 bases
         const uint32_t sh = 2 * (k - 32);
         const uint64_t h = rev_bases(first.hi) >> (64 - sh), lo = rev_bases(first.lo);
         q.w0 = h | (lo << sh); q.w1 = (lo >> (64 - sh)) | (s0 << sh);
         q.w2 = (s0 >> (64 - sh)) | (s1 << sh); q.w3 = s1 >> (64 - sh);
+    } else {                  // k > 63 keeps no buffered labels (first k-mer + steps exceed 128 bases)
+        q.w0 = q.w1 = q.w2 = q.w3 = 0;
     }
     return q;
 }
@@ -648,7 +686,7 @@ __device__ __forceinline__ uint32_t rev8bases(uint32_t x16) {   // reverses the 
 template <int W>
 __device__ void write_buffered(const KOps<W>& ops, const Kmer<W>& first, unsigned long long steps0,
                                unsigned long long steps1, uint32_t skip, uint32_t L, char* dst, bool rev) {
-    if (!dst) return;
+    if (!dst || W > 2) return;
     const WalkSeq q = walk_seq<W>(ops.k, first, steps0, steps1);
     const uint32_t table = rev ? CH_CMP : CH_FWD;
     auto one = [&](uint32_t i) {
@@ -792,7 +830,9 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
     }
 
     for (uint32_t s = tid; s < per; s += nt) {
-        if constexpr (W == 1) lkeys[2 * s] = EMPTY; else { lkeys[2 * s] = EMPTY; lkeys[2 * s + 1] = EMPTY; }
+        if constexpr (W == 1) lkeys[2 * s] = EMPTY;
+        else if constexpr (W == 2) { lkeys[2 * s] = EMPTY; lkeys[2 * s + 1] = EMPTY; }
+        else { lkeys[4 * s] = EMPTY; lkeys[4 * s + 1] = EMPTY; lkeys[4 * s + 2] = EMPTY; lkeys[4 * s + 3] = EMPTY; }
         lst[sti<W>(s)] = ST_INIT;
         lmeta[s] = 0;
     }
@@ -860,7 +900,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
             }
             const uint32_t P = incl - ninst;                      // first instance of record `lane`
             const uint32_t total = __shfl_sync(FULL, incl, 31);
-            const RecWords<W> rw(a.packed, has ? rec_pos(rec) : 0u, has);
+            const RecWords<W> rw(a.packed, has ? rec_pos(rec) : 0u, has, has ? rec_len(rec) : 0u);
             uint32_t started = 0;                                 // records started before the round
             for (uint32_t t0 = 0; t0 < total; t0 += 32) {
                 const uint32_t bit = (has && P >= t0 && P < t0 + 32) ? 1u << (P - t0) : 0u;
@@ -1091,7 +1131,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         if (kc0) { write_kmer_cycle(T, ops, s, B, fo); fo += k + 4; }
         if (kc1) { write_kmer_cycle(T, ops, e, B, fo); fo += k + 4; }
         if (path) {
-            const bool buffered = walked > 0 && walked - 1 <= STEP_BUF;
+            const bool buffered = W <= 2 && walked > 0 && walked - 1 <= STEP_BUF;
             write_emitted_path(a, T, ops, vs, sd0, n2, ve, st, en, best_canon, B, lm, fo, r.lm_idx, r.lm_off,
                                buffered, steps0, steps1, first, kc0 ? 1u : 0u);
         }
@@ -1184,9 +1224,10 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
 template <int W>
 __device__ __forceinline__ void carve(unsigned char* base, uint32_t per, unsigned long long*& keys, unsigned long long*& st,
                                       uint32_t*& meta, uint32_t*& wl) {
+    constexpr size_t KB = W <= 2 ? 16 : 32;   // key bytes per slot
     keys = (unsigned long long*)base;
-    st = W == 1 ? keys + 1 : (unsigned long long*)(base + (size_t)per * 16);   // k <= 31: interleaved with the keys
-    meta = (uint32_t*)(base + (size_t)per * (W == 1 ? 16 : 24));
+    st = W == 1 ? keys + 1 : (unsigned long long*)(base + (size_t)per * KB);   // k <= 31: interleaved with the keys
+    meta = (uint32_t*)(base + (size_t)per * (W == 1 ? 16 : KB + 8));
     wl = meta + per;
 }
 
@@ -1194,8 +1235,10 @@ __device__ __forceinline__ void carve(unsigned char* base, uint32_t per, unsigne
 // largest CTA.  k > 32 (104 registers at LB 512) has a second form for tables of up to
 // 2048 slots, LB 256 at three CTAs per SM (80 registers): a 512-thread CTA of the wide
 // form holds a whole SM's registers, so one subgraph's phase barriers idle the SM.
+// k > 63 runs 256-thread CTAs, two per SM (128 registers).
+constexpr int shared_min_blocks(int W, int LB) { return W > 2 ? 2 : LB <= 256 ? 3 : 1; }
 template <int W, int MODE, int LB>
-__global__ void __launch_bounds__(LB, LB <= 256 ? 3 : 1) k_subgraph_shared(const SubgraphArgs a) {
+__global__ void __launch_bounds__(LB, shared_min_blocks(W, LB)) k_subgraph_shared(const SubgraphArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ Block B;
     uint32_t rank = 0, nranks = 1;
@@ -1220,6 +1263,8 @@ __global__ void __launch_bounds__(LB, LB <= 256 ? 3 : 1) k_subgraph_shared(const
 // per SM (80 registers) instead of one of 512.
 template <int W> struct GlobalBounds { static constexpr int threads = 512, min_blocks = 2; };   // 64 registers
 template <> struct GlobalBounds<2> { static constexpr int threads = 256, min_blocks = 3; };     // 80 registers
+template <> struct GlobalBounds<3> { static constexpr int threads = 256, min_blocks = 2; };     // 128 registers
+template <> struct GlobalBounds<4> { static constexpr int threads = 256, min_blocks = 2; };
 template <int W>
 __global__ void __launch_bounds__(GlobalBounds<W>::threads, GlobalBounds<W>::min_blocks) k_subgraph_global(const SubgraphArgs a) {
     __shared__ Block B;
@@ -1241,7 +1286,7 @@ __global__ void __launch_bounds__(GlobalBounds<W>::threads, GlobalBounds<W>::min
 
 // The kernels' shared-memory limit is always raised to the largest table any launch
 // uses (it is process-wide state: lowering it would break launches recorded in graphs).
-template <int W> constexpr size_t max_table_bytes() { return (size_t)(W == 1 ? 8192 : 4096) * (W == 1 ? 24 : 32); }
+template <int W> constexpr size_t max_table_bytes() { return (size_t)(W == 1 ? 8192 : W == 2 ? 4096 : 2048) * slot_bytes(W); }
 template <typename K>
 cudaError_t raise_smem_limit(K kernel, size_t bytes) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -1307,29 +1352,62 @@ __global__ void k_stripe_fixup(LmtigOut* lm, uint64_t lm_slice, const unsigned l
     }
 }
 
-uint32_t subgraph_max_per_cta(int words) { return words == 1 ? 8192 : 4096; }
+uint32_t subgraph_max_per_cta(int words) { return words == 1 ? 8192 : words == 2 ? 4096 : 2048; }
 uint32_t subgraph_max_threads(int words, uint32_t per) {
+    if (words > 2) return 256;                            // k > 63: one 256-thread form
     if (per == 0) return words == 1 ? 512 : 256;          // arena tables
     if (words == 1) return per > 4096 ? 1024 : 512;
     return per > 2048 ? 512 : 256;
 }
 uint32_t subgraph_cluster_per_cta(int words) { return words == 1 ? 4096 : 2048; }
 
+namespace {
+// the kernel of a one-CTA shared-memory table, by key words and CTA size
+template <int W> cudaError_t launch_local_w(const SubgraphArgs& a, uint32_t threads, size_t bytes, cudaStream_t s,
+                                            uint32_t grid, size_t limit) {
+    if constexpr (W == 1) return launch_shared(k_subgraph_shared<1, LOCAL, 1024>, a, 1, threads, bytes, s, grid, limit);
+    else if constexpr (W == 2)
+        return threads <= 256 ? launch_shared(k_subgraph_shared<2, LOCAL, 256>, a, 1, threads, bytes, s, grid, limit)
+                              : launch_shared(k_subgraph_shared<2, LOCAL, 512>, a, 1, threads, bytes, s, grid, limit);
+    else return launch_shared(k_subgraph_shared<W, LOCAL, 256>, a, 1, threads, bytes, s, grid, limit);
+}
+template <int W> int occupancy_local_w(uint32_t threads, size_t bytes) {
+    if constexpr (W == 1) return occupancy_of(k_subgraph_shared<1, LOCAL, 1024>, 1, threads, bytes, max_table_bytes<1>());
+    else if constexpr (W == 2)
+        return threads <= 256 ? occupancy_of(k_subgraph_shared<2, LOCAL, 256>, 1, threads, bytes, max_table_bytes<2>())
+                              : occupancy_of(k_subgraph_shared<2, LOCAL, 512>, 1, threads, bytes, max_table_bytes<2>());
+    else return occupancy_of(k_subgraph_shared<W, LOCAL, 256>, 1, threads, bytes, max_table_bytes<W>());
+}
+cudaError_t launch_local(const SubgraphArgs& a, int words, uint32_t threads, size_t bytes, cudaStream_t s, uint32_t grid) {
+    switch (words) {
+        case 1: return launch_local_w<1>(a, threads, bytes, s, grid, grid ? 0 : max_table_bytes<1>());
+        case 2: return launch_local_w<2>(a, threads, bytes, s, grid, grid ? 0 : max_table_bytes<2>());
+        case 3: return launch_local_w<3>(a, threads, bytes, s, grid, grid ? 0 : max_table_bytes<3>());
+        case 4: return launch_local_w<4>(a, threads, bytes, s, grid, grid ? 0 : max_table_bytes<4>());
+        default: return cudaErrorInvalidValue;
+    }
+}
+cudaError_t launch_global(const SubgraphArgs& a, int words, uint32_t threads, uint32_t grid, cudaStream_t s) {
+    switch (words) {
+        case 1: k_subgraph_global<1><<<grid, threads, 0, s>>>(a); break;
+        case 2: k_subgraph_global<2><<<grid, threads, 0, s>>>(a); break;
+        case 3: k_subgraph_global<3><<<grid, threads, 0, s>>>(a); break;
+        case 4: k_subgraph_global<4><<<grid, threads, 0, s>>>(a); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+}  // namespace
+
 cudaError_t launch_subgraphs(const SubgraphArgs& a, int words, uint32_t cluster, uint32_t threads, cudaStream_t s) {
     if (a.n_list == 0) return cudaSuccess;
     if (cluster == 0) {   // global-memory tables
         if (threads > subgraph_max_threads(words, 0)) return cudaErrorInvalidValue;
-        if (words == 1) k_subgraph_global<1><<<a.n_list, threads, 0, s>>>(a);
-        else k_subgraph_global<2><<<a.n_list, threads, 0, s>>>(a);
-        return cudaGetLastError();
+        return launch_global(a, words, threads, a.n_list, s);
     }
     const size_t bytes = (size_t)a.smem_cap * slot_bytes(words);
     if (threads > subgraph_max_threads(words, a.smem_cap)) return cudaErrorInvalidValue;
-    if (cluster == 1) {
-        if (words == 1) return launch_shared(k_subgraph_shared<1, LOCAL, 1024>, a, 1, threads, bytes, s, 0, max_table_bytes<1>());
-        return threads <= 256 ? launch_shared(k_subgraph_shared<2, LOCAL, 256>, a, 1, threads, bytes, s, 0, max_table_bytes<2>())
-                              : launch_shared(k_subgraph_shared<2, LOCAL, 512>, a, 1, threads, bytes, s, 0, max_table_bytes<2>());
-    }
+    if (cluster == 1) return launch_local(a, words, threads, bytes, s, 0);
     if (words != 1) return cudaErrorInvalidValue;   // k > 32 tables are one CTA's or the arena's
     return launch_shared(k_subgraph_shared<1, CLUSTER, 1024>, a, cluster, threads, bytes, s, 0, max_table_bytes<1>());
 }
@@ -1343,9 +1421,13 @@ int subgraph_occupancy(int words, uint32_t cluster, uint32_t threads, uint32_t p
     const size_t bytes = (size_t)per * slot_bytes(words);
     if (threads > subgraph_max_threads(words, per)) return 0;
     if (cluster <= 1) {
-        if (words == 1) return occupancy_of(k_subgraph_shared<1, LOCAL, 1024>, 1, threads, bytes, max_table_bytes<1>());
-        return threads <= 256 ? occupancy_of(k_subgraph_shared<2, LOCAL, 256>, 1, threads, bytes, max_table_bytes<2>())
-                              : occupancy_of(k_subgraph_shared<2, LOCAL, 512>, 1, threads, bytes, max_table_bytes<2>());
+        switch (words) {
+            case 1: return occupancy_local_w<1>(threads, bytes);
+            case 2: return occupancy_local_w<2>(threads, bytes);
+            case 3: return occupancy_local_w<3>(threads, bytes);
+            case 4: return occupancy_local_w<4>(threads, bytes);
+            default: return 0;
+        }
     }
     if (words != 1) return 0;   // no cluster tables for k > 32
     return occupancy_of(k_subgraph_shared<1, CLUSTER, 1024>, cluster, threads, bytes, max_table_bytes<1>());
@@ -1356,19 +1438,13 @@ cudaError_t launch_subgraphs_persistent(const SubgraphArgs& a, int words, uint32
     if (grid == 0) return cudaSuccess;
     if (cluster == 0) {
         if (threads > subgraph_max_threads(words, 0)) return cudaErrorInvalidValue;
-        if (words == 1) k_subgraph_global<1><<<grid, threads, 0, s>>>(a);
-        else k_subgraph_global<2><<<grid, threads, 0, s>>>(a);
-        return cudaGetLastError();
+        return launch_global(a, words, threads, grid, s);
     }
     SubgraphArgs b = a;
     b.smem_cap = per;
     const size_t bytes = (size_t)per * slot_bytes(words);
     if (threads > subgraph_max_threads(words, per)) return cudaErrorInvalidValue;
-    if (cluster == 1) {
-        if (words == 1) return launch_shared(k_subgraph_shared<1, LOCAL, 1024>, b, 1, threads, bytes, s, grid);
-        return threads <= 256 ? launch_shared(k_subgraph_shared<2, LOCAL, 256>, b, 1, threads, bytes, s, grid)
-                              : launch_shared(k_subgraph_shared<2, LOCAL, 512>, b, 1, threads, bytes, s, grid);
-    }
+    if (cluster == 1) return launch_local(b, words, threads, bytes, s, grid);
     if (words != 1) return cudaErrorInvalidValue;   // no cluster tables for k > 32
     return launch_shared(k_subgraph_shared<1, CLUSTER, 1024>, b, cluster, threads, bytes, s, grid);
 }

@@ -25,7 +25,7 @@
 //      share).
 // Entries that never reach a head lie on closed chains (cycles): a second set of passes
 // (collate_cycles_on_device, below) joins them and writes each cycle from its canonical
-// start; the batched form hands them to the host collator instead (they are rare).
+// start.
 #include "cuttlefish_gpu.h"
 #include "cfg_host.h"
 #include "cfg_internal.h"
@@ -60,20 +60,55 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
 }
 
 
-// An lm-tig end as the pairing pass reads it: the vertex k-mer (low word, high word) with
-// the end's side in bit 62 and its phi flag in bit 63 of the high word (a k-mer of k <= 63
-// leaves both free).
+// An lm-tig end as the pairing pass reads it: the vertex k-mer's words with the end's side
+// in bit 62 and its phi flag in bit 63 of the last word -- 16 bytes (words 0, 1) for
+// k <= 63, 32 bytes (words 0..3) for k <= 127; the highest word of a k-mer leaves both
+// bits free.  ew: 2 or 4 words per end.
 constexpr unsigned long long END_SIDE = 1ull << 62, END_PHI = 1ull << 63;
-__device__ __forceinline__ void put_ends(ulonglong2* ends, uint64_t g, const LmtigOut& m) {
-    ends[2 * g] = make_ulonglong2(m.u[0], m.u[1] | ((m.flags & 1ull) << 62) | ((m.flags >> 2 & 1ull) << 63));
-    ends[2 * g + 1] = make_ulonglong2(m.v[0], m.v[1] | ((m.flags >> 1 & 1ull) << 62) | ((m.flags >> 3 & 1ull) << 63));
+__device__ __forceinline__ void put_ends(ulonglong2* ends, uint64_t g, const LmtigOut& m, uint32_t ew) {
+    const unsigned long long fu = ((m.flags & 1ull) << 62) | ((m.flags >> 2 & 1ull) << 63);
+    const unsigned long long fv = ((m.flags >> 1 & 1ull) << 62) | ((m.flags >> 3 & 1ull) << 63);
+    if (ew == 2) {
+        ends[2 * g] = make_ulonglong2(m.u[0], m.u[1] | fu);
+        ends[2 * g + 1] = make_ulonglong2(m.v[0], m.v[1] | fv);
+    } else {
+        ends[4 * g] = make_ulonglong2(m.u[0], m.u[1]);
+        ends[4 * g + 1] = make_ulonglong2(m.u[2], m.u[3] | fu);
+        ends[4 * g + 2] = make_ulonglong2(m.v[0], m.v[1]);
+        ends[4 * g + 3] = make_ulonglong2(m.v[2], m.v[3] | fv);
+    }
 }
+// end e's k-mer words (flags cleared) and its flag word
+template <int EW> struct EndKey {
+    unsigned long long w[EW], flags;
+    __device__ __forceinline__ EndKey(const ulonglong2* __restrict__ ends, uint64_t e) {
+        if constexpr (EW == 2) {
+            const ulonglong2 a = ends[e];
+            w[0] = a.x; w[1] = a.y & ~(END_SIDE | END_PHI); flags = a.y;
+        } else {
+            const ulonglong2 a = ends[2 * e], b = ends[2 * e + 1];
+            w[0] = a.x; w[1] = a.y; w[2] = b.x; w[3] = b.y & ~(END_SIDE | END_PHI); flags = b.y;
+        }
+    }
+    __device__ __forceinline__ bool same(const EndKey& o) const {
+        bool e = true;
+#pragma unroll
+        for (int j = 0; j < EW; ++j) e &= w[j] == o.w[j];
+        return e;
+    }
+    __device__ __forceinline__ uint64_t hash() const {
+        uint64_t h = mix64(w[EW - 1] + 0x9E3779B97F4A7C15ull);
+#pragma unroll
+        for (int j = EW - 2; j >= 1; --j) h = mix64(w[j] ^ h);
+        return mix64(w[0] ^ h);
+    }
+};
 
 // 0: gather the striped lm-tigs into one array with their label addresses.
 __global__ void k_ut_gather(const LmtigOut* lm, uint64_t lm_slice, const char* text, uint64_t text_slice,
                             const unsigned long long* __restrict__ lm_base, const unsigned long long* __restrict__ text_base,
                             const unsigned long long* __restrict__ stripe_cur, uint32_t stripes, LmtigOut* out,
-                            const char** label, uint32_t* lens, ulonglong2* ends) {
+                            const char** label, uint32_t* lens, ulonglong2* ends, uint32_t ew) {
     for (uint32_t st = blockIdx.y; st < stripes; st += gridDim.y) {
         const unsigned long long n = stripe_cur[st * JOB_CUR_STRIDE + 2];
         for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -81,7 +116,7 @@ __global__ void k_ut_gather(const LmtigOut* lm, uint64_t lm_slice, const char* t
             const uint64_t g = lm_base[st] + i;
             out[g] = m;
             lens[g] = m.label_len;
-            put_ends(ends, g, m);
+            put_ends(ends, g, m, ew);
             label[g] = text + st * text_slice + (m.label_off - text_base[st]);
         }
     }
@@ -91,7 +126,7 @@ __global__ void k_ut_gather(const LmtigOut* lm, uint64_t lm_slice, const char* t
 __global__ void k_ut_gather_jobs(const LmtigOut* lm, const char* text, const JobOut* __restrict__ jobs, uint32_t n_jobs,
                                  const unsigned long long* __restrict__ job_n, const unsigned long long* __restrict__ job_lm_base,
                                  LmtigOut* out, const char** label, uint32_t* out_job, uint32_t* lens,
-                                 ulonglong2* ends) {
+                                 ulonglong2* ends, uint32_t ew) {
     for (uint32_t j = blockIdx.y; j < n_jobs; j += gridDim.y) {
         const unsigned long long n = job_n[j];
         const JobOut& J = jobs[j];
@@ -100,7 +135,7 @@ __global__ void k_ut_gather_jobs(const LmtigOut* lm, const char* text, const Job
             const uint64_t g = job_lm_base[j] + i;
             out[g] = m;
             lens[g] = m.label_len;
-            put_ends(ends, g, m);
+            put_ends(ends, g, m, ew);
             label[g] = text + J.lm_text_off + m.label_off;
             out_job[g] = j;
         }
@@ -118,6 +153,7 @@ __global__ void k_ut_gather_jobs(const LmtigOut* lm, const char* text, const Job
 // first end is claimed by CAS and its k-mer read from the (immutable) lm-tig, so no
 // thread waits on another.
 constexpr uint32_t INSERT_TILE = 1024;
+template <int EW>
 __global__ void __launch_bounds__(256, 6) k_ut_insert(const ulonglong2* __restrict__ ends, const uint32_t* __restrict__ job,
                                                     uint64_t n, uint32_t* tab,
                                                     const unsigned long long* __restrict__ job_lm_base,
@@ -135,19 +171,18 @@ __global__ void __launch_bounds__(256, 6) k_ut_insert(const ulonglong2* __restri
         for (uint32_t u = threadIdx.x; u < INSERT_TILE; u += blockDim.x) {
             const uint64_t e = t0 + u;
             if (e >= n2) break;
-            const ulonglong2 me = ends[e];
-            if (me.y & END_PHI) continue;
-            const unsigned long long k0 = me.x, k1 = me.y & ~(END_SIDE | END_PHI);
-            const uint64_t h = mix64(k0 ^ mix64(k1 + 0x9E3779B97F4A7C15ull));
+            const EndKey<EW> me(ends, e);
+            if (me.flags & END_PHI) continue;
+            const uint64_t h = me.hash();
             const uint32_t jb = job ? job[e >> 1] : 0u;
             const uint64_t base = job ? 4 * job_lm_base[jb] : 0, t = job ? 4 * job_n[jb] : 4 * n;
             uint64_t p = base + __umul64hi(h, t);
             for (uint64_t probe = 0; probe < t; ++probe) {
                 const uint32_t old = atomicCAS(tab + 2 * p, NONE, (uint32_t)e);
                 if (old == NONE) break;
-                const ulonglong2 oe = ends[old];
-                if (oe.x == k0 && (oe.y & ~(END_SIDE | END_PHI)) == k1) {
-                    if (atomicCAS(tab + 2 * p + 1, NONE, (uint32_t)e) != NONE || ((me.y ^ oe.y) & END_SIDE) == 0) {
+                const EndKey<EW> oe(ends, old);
+                if (oe.same(me)) {
+                    if (atomicCAS(tab + 2 * p + 1, NONE, (uint32_t)e) != NONE || ((me.flags ^ oe.flags) & END_SIDE) == 0) {
                         atomicOr(err, DERR_BAD_GRAPH);
                     } else {
                         partner[e] = old;
@@ -597,12 +632,14 @@ __global__ void k_cy_text(CyArgs a, const unsigned long long* __restrict__ scr_o
 }
 
 __device__ __forceinline__ uint32_t code_of(char c) { return c == 'A' ? 0u : c == 'C' ? 1u : c == 'G' ? 2u : 3u; }
-// (hi, lo, index, strand) ordered lexicographically: the k-mer first (big-endian 2-bit,
-// so numeric order is character order), then where it was found
-struct CyKey { unsigned long long hi, lo; unsigned long long i; uint32_t s; };
+// (k-mer words from the highest, index, strand) ordered lexicographically: the k-mer
+// first (big-endian 2-bit, so numeric order is character order), then where it was found.
+// Four words hold any k <= 127.
+struct CyKey { unsigned long long w[4]; unsigned long long i; uint32_t s; };
 __device__ __forceinline__ bool cy_less(const CyKey& a, const CyKey& b) {
-    if (a.hi != b.hi) return a.hi < b.hi;
-    if (a.lo != b.lo) return a.lo < b.lo;
+#pragma unroll
+    for (int j = 3; j >= 0; --j)
+        if (a.w[j] != b.w[j]) return a.w[j] < b.w[j];
     if (a.i != b.i) return a.i < b.i;
     return a.s < b.s;
 }
@@ -616,38 +653,46 @@ __global__ void __launch_bounds__(256) k_cy_rotate(const uint32_t* __restrict__ 
     __shared__ CyKey red[8];
     const uint64_t nh = *n_heads;
     const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const uint32_t kb = 2 * k;   // bits of a k-mer (k <= 63: at most 126)
+    const uint32_t kb = 2 * k;   // bits of a k-mer (k <= 127: at most 254)
+    unsigned long long mask[4];   // the bits of each word a k-mer uses
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int left = (int)kb - 64 * j;
+        mask[j] = left >= 64 ? ~0ull : left <= 0 ? 0ull : ((1ull << left) - 1);
+    }
+    const uint32_t top = (kb - 2) >> 6, top_sh = (kb - 2) & 63;   // where the rc's first base goes
     for (uint64_t h = blockIdx.x; h < nh; h += gridDim.x) {
         const uint32_t H = heads[h];
         const unsigned long long T = T_of[H];
         const char* C = scr + scr_off[H];
         // positions [j0, j1) of this thread; the k-mer at j covers C[j .. j+k) circularly
         const unsigned long long j0 = T * threadIdx.x / blockDim.x, j1 = T * (threadIdx.x + 1) / blockDim.x;
-        CyKey best{~0ull, ~0ull, ~0ull, 1u};
-        unsigned long long fh = 0, fl = 0, rh = 0, rl = 0;   // forward / reverse-complement k-mer
+        CyKey best{{~0ull, ~0ull, ~0ull, ~0ull}, ~0ull, 1u};
+        unsigned long long f[4] = {0, 0, 0, 0}, r[4] = {0, 0, 0, 0};   // forward / reverse-complement k-mer
         auto push = [&](uint32_t b) {   // appends base b to the forward k-mer, prepends comp(b) to the rc
-            fh = ((fh << 2) | (fl >> 62));
-            fl = (fl << 2) | b;
-            if (kb <= 64) { fl &= kb == 64 ? ~0ull : ((1ull << kb) - 1); fh = 0; }
-            else fh &= (1ull << (kb - 64)) - 1;
-            const uint32_t cb = 3u - b;
-            rl = (rl >> 2) | (rh << 62);
-            rh >>= 2;
-            if (kb <= 64) rl |= (unsigned long long)cb << (kb - 2);
-            else rh |= (unsigned long long)cb << (kb - 64 - 2);
+#pragma unroll
+            for (int j = 3; j > 0; --j) f[j] = ((f[j] << 2) | (f[j - 1] >> 62)) & mask[j];
+            f[0] = ((f[0] << 2) | b) & mask[0];
+            const unsigned long long cb = 3u - b;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) r[j] = (r[j] >> 2) | (r[j + 1] << 62);
+            r[3] >>= 2;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) r[j] |= top == (uint32_t)j ? cb << top_sh : 0ull;
         };
         if (j0 < j1) {
             for (uint32_t t = 0; t + 1 < k; ++t) push(code_of(C[(j0 + t) % T]));
             for (unsigned long long j = j0; j < j1; ++j) {
                 push(code_of(C[(j + k - 1) % T]));
-                const CyKey f{fh, fl, j, 0u}, r{rh, rl, T - 1 - j, 1u};
-                if (cy_less(f, best)) best = f;
-                if (cy_less(r, best)) best = r;
+                const CyKey fk{{f[0], f[1], f[2], f[3]}, j, 0u}, rk{{r[0], r[1], r[2], r[3]}, T - 1 - j, 1u};
+                if (cy_less(fk, best)) best = fk;
+                if (cy_less(rk, best)) best = rk;
             }
         }
         for (int d = 16; d; d >>= 1) {
             CyKey o;
-            o.hi = __shfl_down_sync(0xffffffffu, best.hi, d); o.lo = __shfl_down_sync(0xffffffffu, best.lo, d);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) o.w[j] = __shfl_down_sync(0xffffffffu, best.w[j], d);
             o.i = __shfl_down_sync(0xffffffffu, best.i, d); o.s = __shfl_down_sync(0xffffffffu, best.s, d);
             if (cy_less(o, best)) best = o;
         }
@@ -687,7 +732,7 @@ bool UnitigBuffers::ensure(uint64_t n) {
         !b_partner.ensure(4 * n2) || !b_X0.ensure(sizeof(RankRec) * n2) || !b_X1.ensure(sizeof(RankRec) * n2) ||
         !b_fin.ensure(4 * (n + 1)) || !b_sx.ensure(4 * n2) || !b_sw.ensure(4 * n2) ||
         !b_off.ensure(8 * n2) || !b_words.ensure(64) || !b_job.ensure(4 * (n + 1)) || !b_flip.ensure(n + 1) ||
-        !b_len.ensure(4 * (n + 1)) || !b_ends.ensure(32 * (n + 1)))
+        !b_len.ensure(4 * (n + 1)) || !b_ends.ensure(16ull * end_words * (n + 1)))
         return false;
     len = b_len.as<uint32_t>();
     ends = b_ends.as<ulonglong2>();
@@ -778,6 +823,7 @@ int collate_cycles_on_device(UnitigBuffers& ub, uint64_t n, uint64_t m, uint32_t
 int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, UnitigResult& res) {
     res = UnitigResult{};
     const uint64_t n = in.n;
+    ub.end_words = in.k > 63 ? 4 : 2;
     if (!ub.ensure(n)) return CFG_ERR_OOM;
     if (cudaMemsetAsync(ub.words, 0, sizeof(unsigned long long) * 8, s) != cudaSuccess) return CFG_ERR_CUDA;
     // [0] output bytes, [1] unitigs, [2] cycle lm-tigs, [3] active entries, [4] splitters,
@@ -789,15 +835,19 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
     const uint32_t* job = in.jobs ? ub.job : nullptr;
     if (in.jobs)
         k_ut_gather_jobs<<<dim3(16, std::min<uint32_t>(in.n_jobs, 65535)), 256, 0, s>>>(
-            in.job_lm, in.job_text, in.jobs, in.n_jobs, in.job_n, in.job_lm_base, ub.lm, ub.label, ub.job, ub.len, ub.ends);
+            in.job_lm, in.job_text, in.jobs, in.n_jobs, in.job_n, in.job_lm_base, ub.lm, ub.label, ub.job, ub.len, ub.ends, ub.end_words);
     else
         k_ut_gather<<<dim3(64, in.stripes), 256, 0, s>>>(in.lm, in.lm_slice, in.text, in.text_slice, in.lm_base, in.text_base,
-                                                         in.stripe_cur, in.stripes, ub.lm, ub.label, ub.len, ub.ends);
+                                                         in.stripe_cur, in.stripes, ub.lm, ub.label, ub.len, ub.ends, ub.end_words);
     if (cudaMemsetAsync(ub.tab, 0xff, sizeof(EndSlot) * ub.tab_n, s) != cudaSuccess ||
         cudaMemsetAsync(ub.partner, 0xff, 4 * 2 * n, s) != cudaSuccess)
         return CFG_ERR_CUDA;
-    k_ut_insert<<<grid, 256, 0, s>>>(ub.ends, job, n, (uint32_t*)ub.tab, in.job_lm_base, in.job_n, cursor + 5, ub.partner,
-                                     in.err);
+    if (ub.end_words == 2)
+        k_ut_insert<2><<<grid, 256, 0, s>>>(ub.ends, job, n, (uint32_t*)ub.tab, in.job_lm_base, in.job_n, cursor + 5,
+                                            ub.partner, in.err);
+    else
+        k_ut_insert<4><<<grid, 256, 0, s>>>(ub.ends, job, n, (uint32_t*)ub.tab, in.job_lm_base, in.job_n, cursor + 5,
+                                            ub.partner, in.err);
     // ranking: splitters, their walks, pointer jumping over the splitters, every entry
     RankRec* X = (RankRec*)ub.X[0];
     uint2* node = (uint2*)ub.out_off;                          // free until the records are reserved

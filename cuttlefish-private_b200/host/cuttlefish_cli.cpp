@@ -17,7 +17,7 @@ void usage() {
                  "  -s, --seq FILE[,FILE..]   input files (FASTA / FASTQ, optionally gzipped)\n"
                  "  -l, --list FILE           files listing inputs, one per line\n"
                  "  -d, --dir DIR             directories of inputs\n"
-                 "  -k, --kmer-len K          k-mer length (odd, <= 63; default 27)\n"
+                 "  -k, --kmer-len K          k-mer length (odd, <= 127; default 27)\n"
                  "  -c, --cutoff C            (k+1)-mer frequency cutoff (default: refs 1, reads 2)\n"
                  "      --read | --ref        read or reference de Bruijn graph\n"
                  "      --min-len L           minimizer length (default 20)\n"
@@ -80,7 +80,7 @@ int cf_build(int argc, char** argv) {
     // Build_Params::is_valid (src/Build_Params.cpp:97-218)
     bool valid = true;
     if (seqs.empty()) { std::cout << "No sequence input provided for compacted de Bruijn graph construction.\n"; valid = false; }
-    if ((p.k % 2) == 0 || p.k == 1 || p.k > 63) { std::cout << "The k-mer length (k) needs to be odd and within 63.\n"; valid = false; }
+    if ((p.k % 2) == 0 || p.k == 1 || p.k > 127) { std::cout << "The k-mer length (k) needs to be odd and within 127.\n"; valid = false; }
     if (read && ref) { std::cout << "Both read and reference de Bruijn graph specified.\n"; valid = false; }
     if (p.output_prefix.empty()) { std::cout << "An output path (-o) is required.\n"; valid = false; }
     if (p.min_len == 0 || p.min_len > 32 || p.min_len + 1 > p.k) { std::cout << "The minimizer length must be within [1, min(k-1, 32)].\n"; valid = false; }

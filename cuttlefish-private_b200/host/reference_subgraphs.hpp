@@ -77,13 +77,12 @@ public:
     }
 
 private:
-    // Kmer<k> of a cfg_lmtig k-mer: (low word, high word), the first base most significant.
-    static Kmer<k> kmer_of(const uint64_t w[2]) {
+    // Kmer<k> of a cfg_lmtig k-mer: words from the lowest, the first base most significant.
+    static Kmer<k> kmer_of(const uint64_t w[4]) {
         char s[k + 1];
         for (uint32_t i = 0; i < k; ++i) {
             const uint32_t bp = 2 * (k - 1 - i);
-            const uint64_t b = bp >= 64 ? (w[1] >> (bp - 64)) & 3 : (w[0] >> bp) & 3;
-            s[i] = "ACGT"[b];
+            s[i] = "ACGT"[(w[bp >> 6] >> (bp & 63)) & 3];
         }
         s[k] = '\0';
         return Kmer<k>(s);

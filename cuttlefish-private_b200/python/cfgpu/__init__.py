@@ -29,7 +29,7 @@ U32P = ctypes.POINTER(ctypes.c_uint32)
 class Params(ctypes.Structure):
     _fields_ = [("k", ctypes.c_uint32), ("l", ctypes.c_uint32), ("cutoff", ctypes.c_uint32),
                 ("graph_count", ctypes.c_uint32), ("flags", ctypes.c_uint32),
-                ("table_load_pct", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 2)]
+                ("table_load_pct", ctypes.c_uint32), ("slots_per_thread", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 class Counts(ctypes.Structure):
@@ -39,7 +39,7 @@ class Counts(ctypes.Structure):
 
 
 class Lmtig(ctypes.Structure):
-    _fields_ = [("u", ctypes.c_uint64 * 2), ("v", ctypes.c_uint64 * 2), ("label_off", ctypes.c_uint64),
+    _fields_ = [("u", ctypes.c_uint64 * 4), ("v", ctypes.c_uint64 * 4), ("label_off", ctypes.c_uint64),
                 ("label_len", ctypes.c_uint32), ("g", ctypes.c_uint16), ("flags", ctypes.c_uint8),
                 ("pad", ctypes.c_uint8)]
 
@@ -50,7 +50,7 @@ class Results(ctypes.Structure):
 
 
 class State(ctypes.Structure):
-    _fields_ = [("key", ctypes.c_uint64 * 2), ("ef", ctypes.c_uint32), ("g", ctypes.c_uint16),
+    _fields_ = [("key", ctypes.c_uint64 * 4), ("ef", ctypes.c_uint32), ("g", ctypes.c_uint16),
                 ("status", ctypes.c_uint8), ("pad", ctypes.c_uint8)]
 
 
@@ -240,10 +240,10 @@ class Compactor:
     """One GPU context (cfg_ctx): submit -> run -> fetch."""
 
     def __init__(self, k: int, l: int = 20, cutoff: int = 1, graph_count: int = 16384, device: int = 0,
-                 flags: int = 0, table_load_pct: int = 0):
+                 flags: int = 0, table_load_pct: int = 0, slots_per_thread: int = 0):
         self.lib = load()
         self.k = k
-        self.params = Params(k, l, cutoff, graph_count, flags, table_load_pct)
+        self.params = Params(k, l, cutoff, graph_count, flags, table_load_pct, slots_per_thread)
         ctx = ctypes.c_void_p()
         rc = self.lib.cfg_create(device, ctypes.byref(self.params), ctypes.byref(ctx))
         _check(self.lib, None, rc, "cfg_create")
@@ -333,8 +333,7 @@ class Compactor:
     def states(self):
         d = StateDump()
         _check(self.lib, self.ctx, self.lib.cfg_dump_states(self.ctx, ctypes.byref(d)), "cfg_dump_states")
-        return [(d.states[i].g, (d.states[i].key[0], d.states[i].key[1]), d.states[i].ef, d.states[i].status)
-                for i in range(d.n)]
+        return [(d.states[i].g, tuple(d.states[i].key), d.states[i].ef, d.states[i].status) for i in range(d.n)]
 
     def records(self):
         d = RecordDump()
@@ -342,23 +341,39 @@ class Compactor:
         return [(d.records[i].pos, d.records[i].len, d.records[i].flags, d.records[i].g) for i in range(d.n)]
 
 
-STATE_DTYPE = [("lo", "<u8"), ("hi", "<u8"), ("ef", "<u4"), ("g", "<u2"), ("status", "u1"), ("pad", "u1")]
+# k-mer words: lo = word 0 (the last 32 bases), hi = word 1, k2 / k3 = words 2, 3 (k > 63)
+def view_array(ptr, n, item, dtype):
+    """n items of `item` bytes at ptr (a ctypes pointer or address) as a numpy copy with
+    dtype; sizes past 2 GB too (ctypes.string_at takes an int)."""
+    import numpy as np
+    if not n:
+        return np.zeros(0, dtype)
+    addr = ptr if isinstance(ptr, int) else ctypes.cast(ptr, ctypes.c_void_p).value
+    return np.frombuffer((ctypes.c_char * (n * item)).from_address(addr), dtype=dtype).copy()
+
+
+STATE_DTYPE = [("lo", "<u8"), ("hi", "<u8"), ("k2", "<u8"), ("k3", "<u8"), ("ef", "<u4"), ("g", "<u2"), ("status", "u1"),
+               ("pad", "u1")]
 RECORD_DTYPE = [("pos", "<u4"), ("len", "u1"), ("flags", "u1"), ("g", "<u2")]
-LMTIG_DTYPE = [("u_lo", "<u8"), ("u_hi", "<u8"), ("v_lo", "<u8"), ("v_hi", "<u8"), ("label_off", "<u8"),
-               ("label_len", "<u4"), ("g", "<u2"), ("flags", "u1"), ("pad", "u1")]
+LMTIG_DTYPE = [("u_lo", "<u8"), ("u_hi", "<u8"), ("u_2", "<u8"), ("u_3", "<u8"), ("v_lo", "<u8"), ("v_hi", "<u8"),
+               ("v_2", "<u8"), ("v_3", "<u8"), ("label_off", "<u8"), ("label_len", "<u4"), ("g", "<u2"), ("flags", "u1"),
+               ("pad", "u1")]
+# comparison keys (the oracle builds the same): vertex k-mer words from the highest
+STATE_KEY = [("g", "<u4"), ("k3", "<u8"), ("k2", "<u8"), ("hi", "<u8"), ("lo", "<u8"), ("ef", "<u4"), ("status", "u1")]
+LMTIG_KEY = [("g", "<u4"), ("u_3", "<u8"), ("u_2", "<u8"), ("u_hi", "<u8"), ("u_lo", "<u8"), ("v_3", "<u8"), ("v_2", "<u8"),
+             ("v_hi", "<u8"), ("v_lo", "<u8"), ("flags", "u1"), ("label", "<u8")]
 
 
 def states_array(cx):
-    """cfg_dump_states as a numpy array (g, hi, lo, ef, status), sorted by (g, hi, lo)."""
+    """cfg_dump_states as a numpy array (g, k3, k2, hi, lo, ef, status), sorted by (g, k3, k2, hi, lo)."""
     import numpy as np
     d = StateDump()
     _check(cx.lib, cx.ctx, cx.lib.cfg_dump_states(cx.ctx, ctypes.byref(d)), "cfg_dump_states")
-    raw = np.frombuffer(ctypes.string_at(d.states, d.n * ctypes.sizeof(State)), dtype=STATE_DTYPE) if d.n else \
-        np.zeros(0, STATE_DTYPE)
-    out = np.zeros(d.n, dtype=[("g", "<u4"), ("hi", "<u8"), ("lo", "<u8"), ("ef", "<u4"), ("status", "u1")])
-    for f in ("g", "hi", "lo", "ef", "status"):
+    raw = view_array(d.states, d.n, ctypes.sizeof(State), STATE_DTYPE)
+    out = np.zeros(d.n, dtype=STATE_KEY)
+    for f, _ in STATE_KEY:
         out[f] = raw[f]
-    return sort_rows(out, ["g", "hi", "lo"])
+    return sort_rows(out, ["g", "k3", "k2", "hi", "lo"])
 
 
 def records_array(cx):
@@ -366,8 +381,7 @@ def records_array(cx):
     import numpy as np
     d = RecordDump()
     _check(cx.lib, cx.ctx, cx.lib.cfg_dump_records(cx.ctx, ctypes.byref(d)), "cfg_dump_records")
-    raw = np.frombuffer(ctypes.string_at(d.records, d.n * ctypes.sizeof(Record)), dtype=RECORD_DTYPE) if d.n else \
-        np.zeros(0, RECORD_DTYPE)
+    raw = view_array(d.records, d.n, ctypes.sizeof(Record), RECORD_DTYPE)
     out = np.zeros(d.n, dtype=[("g", "<u4"), ("len", "u1"), ("flags", "u1"), ("src", "<u8")])
     out["g"], out["len"], out["flags"], out["src"] = raw["g"], raw["len"], raw["flags"], raw["pos"]
     return sort_rows(out, ["g", "src", "len", "flags"])
@@ -378,15 +392,13 @@ def lmtig_array(res: Results, hash_spans):
     hash_spans(text_address, offsets, lengths) hashes the labels."""
     import numpy as np
     n = res.counts.n_lmtig
-    key = [("g", "<u4"), ("u_hi", "<u8"), ("u_lo", "<u8"), ("v_hi", "<u8"), ("v_lo", "<u8"), ("flags", "u1"),
-           ("label", "<u8")]
-    out = np.zeros(n, dtype=key)
+    out = np.zeros(n, dtype=LMTIG_KEY)
     if n:
-        raw = np.frombuffer(ctypes.string_at(res.lmtigs, n * ctypes.sizeof(Lmtig)), dtype=LMTIG_DTYPE)
-        for f in ("g", "u_hi", "u_lo", "v_hi", "v_lo", "flags"):
+        raw = view_array(res.lmtigs, n, ctypes.sizeof(Lmtig), LMTIG_DTYPE)
+        for f, _ in LMTIG_KEY[:-1]:
             out[f] = raw[f]
         out["label"] = hash_spans(res.lmtig_text, raw["label_off"], raw["label_len"])
-    return sort_rows(out, [f for f, _ in key])
+    return sort_rows(out, [f for f, _ in LMTIG_KEY])
 
 
 def unitig_multiset(fasta: bytes):
@@ -433,7 +445,7 @@ def results_to_python(r: Results):
     for i in range(r.counts.n_lmtig):
         m = r.lmtigs[i]
         lab = text[m.label_off:m.label_off + m.label_len].decode()
-        lms.append(LmtigRec((m.u[0], m.u[1]), (m.v[0], m.v[1]), lab, m.g, m.flags))
+        lms.append(LmtigRec(tuple(m.u), tuple(m.v), lab, m.g, m.flags))
     return r.counts, fasta, lms
 
 
@@ -620,8 +632,10 @@ def collate_lmtig_records(k, lms):
     arr = (Lmtig * max(1, len(lms)))()
     text = bytearray()
     for i, m in enumerate(lms):
-        arr[i].u[0], arr[i].u[1] = m.u
-        arr[i].v[0], arr[i].v[1] = m.v
+        for j, x in enumerate(m.u):
+            arr[i].u[j] = x
+        for j, x in enumerate(m.v):
+            arr[i].v[j] = x
         arr[i].label_off = len(text)
         arr[i].label_len = len(m.label)
         arr[i].g = m.g
@@ -632,13 +646,11 @@ def collate_lmtig_records(k, lms):
 
 
 def kmer_label(key, k):
-    """(low, high) words of a k-mer -> ACGT string."""
-    lo, hi = key
+    """The words of a k-mer, from the lowest (the last 32 bases) -> ACGT string."""
     out = []
     for i in range(k):
         bp = 2 * (k - 1 - i)
-        b = (hi >> (bp - 64)) & 3 if bp >= 64 else (lo >> bp) & 3
-        out.append("ACGT"[b])
+        out.append("ACGT"[(key[bp >> 6] >> (bp & 63)) & 3])
     return "".join(out)
 
 

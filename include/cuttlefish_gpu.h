@@ -51,7 +51,9 @@ enum {
 #define CFG_FLAG_NO_RECORD_DEDUP  0x8u  /* never merge them */
 
 typedef struct cfg_params {
-    uint32_t k;            /* odd, 3..63                                       (Build_Params::k) */
+    uint32_t k;            /* odd, 3..127 (the reference's k <= MAX_K = 2 INSTANCE_COUNT - 1,
+                              include/globals.hpp:16-22,45: 63 by default, 127 at INSTANCE_COUNT 64)
+                                                                                (Build_Params::k) */
     uint32_t l;            /* minimizer length, 1..min(k-1, 32)                 (--min-len)      */
     uint32_t cutoff;       /* edge-frequency threshold, 1..15                   (-c)             */
     uint32_t graph_count;  /* power of two <= 2^20; the reference uses 16384 (include/Atlas.hpp:33-35).
@@ -63,7 +65,11 @@ typedef struct cfg_params {
                                  size subgraph tables (at about half load); 0 = default 100 (one
                                  genome); deep read sets need ~20.  A wrong guess costs only a
                                  rebuild of the tables that overflow. */
-    uint32_t reserved[2];
+    uint32_t slots_per_thread; /* one-CTA subgraph tables run slots / slots_per_thread threads (rounded
+                                  up to whole warps, at least 64, at most the kernel form's largest
+                                  CTA); 0 = default 4.  8 runs 256-thread CTAs on 2048-slot tables,
+                                  four per SM.  Speed only: results never depend on it. */
+    uint32_t reserved;
 } cfg_params;
 
 typedef struct cfg_ctx cfg_ctx;
@@ -87,8 +93,9 @@ typedef struct cfg_counts {
 
 /* One discontinuity edge with its lm-tig (Discontinuity_Graph::add_edge arguments). */
 typedef struct cfg_lmtig {
-    uint64_t u[2];          /* canonical k-mer of u, [0]=low word (last 32 bases), [1]=high word */
-    uint64_t v[2];
+    uint64_t u[4];          /* canonical k-mer of u, Kmer<k>'s words: [0] = the last 32 bases, [1] the
+                               32 before them, ...; words past ceil(k/32) are 0 */
+    uint64_t v[4];
     uint64_t label_off;     /* offset of the label in cfg_results.lmtig_text */
     uint32_t label_len;
     uint16_t g;             /* subgraph */
@@ -105,7 +112,7 @@ typedef struct cfg_results {
 
 /* One vertex state (debug / parity). */
 typedef struct cfg_state {
-    uint64_t key[2];        /* canonical k-mer, [0]=low word */
+    uint64_t key[4];        /* canonical k-mer, words as in cfg_lmtig::u */
     uint32_t ef;            /* packed 4-bit edge frequencies (front nibbles 0-3, back 4-7), saturated at 15 */
     uint16_t g;
     uint8_t  status;        /* bit0 visited, bit1 disc front, bit2 disc back */

@@ -92,40 +92,48 @@ static void km1_min_hashes(const unsigned char* s, uint64_t n, uint32_t k, uint3
 }
 
 // ---------------------------------------------------------------------------
-// Kmer<k>: kmer_data[0] holds the last 32 bases, last base in bits 1:0
-// (include/Kmer.hpp:45-54); words compare high to low (:509-521).
+// Kmer<k>: kmer_data[0] holds the last 32 bases, last base in bits 1:0, and word j the
+// 32 before word j-1's (include/Kmer.hpp:45-54); words compare high to low (:509-521).
+// Four words hold any k <= 127 (INSTANCE_COUNT 64, include/globals.hpp:16-22); words
+// past ceil(k/32) stay 0.
+constexpr int KW = 4;
 struct Kmer {
-    uint64_t w[2];  // w[1] high (first k-32 bases when k > 32), w[0] low
-    bool operator==(const Kmer& o) const { return w[0] == o.w[0] && w[1] == o.w[1]; }
-    bool operator<(const Kmer& o) const { return w[1] != o.w[1] ? w[1] < o.w[1] : w[0] < o.w[0]; }
+    uint64_t w[KW];  // w[0] low ... w[KW-1] high
+    bool operator==(const Kmer& o) const { return std::memcmp(w, o.w, sizeof w) == 0; }
+    bool operator<(const Kmer& o) const {
+        for (int j = KW - 1; j > 0; --j)
+            if (w[j] != o.w[j]) return w[j] < o.w[j];
+        return w[0] < o.w[0];
+    }
 };
 
 struct KCodec {
     uint32_t k;
-    uint64_t m0, m1;  // masks of the two words
+    uint64_t m[KW];  // the bits each word holds
     explicit KCodec(uint32_t k_) : k(k_) {
-        if (k <= 32) { m0 = (k == 32) ? ~0ull : ((1ull << (2 * k)) - 1); m1 = 0; }
-        else { m0 = ~0ull; m1 = (1ull << (2 * (k - 32))) - 1; }
+        for (int j = 0; j < KW; ++j) {
+            const int left = 2 * (int)k - 64 * j;
+            m[j] = left >= 64 ? ~0ull : left <= 0 ? 0ull : ((1ull << left) - 1);
+        }
     }
     // roll_to_next_kmer: shift one base in at the end -- include/Kmer.hpp:610-621
     void push_back(Kmer& x, uint8_t b) const {
-        x.w[1] = ((x.w[1] << 2) | (x.w[0] >> 62)) & m1;
-        x.w[0] = ((x.w[0] << 2) | b) & m0;
+        for (int j = KW - 1; j > 0; --j) x.w[j] = ((x.w[j] << 2) | (x.w[j - 1] >> 62)) & m[j];
+        x.w[0] = ((x.w[0] << 2) | b) & m[0];
     }
     // reverse-complement roll: shift one complemented base in at the front
     void push_front(Kmer& x, uint8_t b) const {
         const uint32_t pos = 2 * (k - 1);
-        x.w[0] = (x.w[0] >> 2) | (x.w[1] << 62);
-        x.w[1] >>= 2;
-        if (k <= 32) { x.w[1] = 0; x.w[0] |= (uint64_t)b << pos; x.w[0] &= m0; }
-        else x.w[1] |= (uint64_t)b << (pos - 64);
+        for (int j = 0; j < KW - 1; ++j) x.w[j] = (x.w[j] >> 2) | (x.w[j + 1] << 62);
+        x.w[KW - 1] >>= 2;
+        x.w[pos / 64] |= (uint64_t)b << (pos % 64);
     }
     uint8_t base_at(const Kmer& x, uint32_t i) const {  // i-th base from the start
         const uint32_t bitpos = 2 * (k - 1 - i);
-        return bitpos >= 64 ? (uint8_t)((x.w[1] >> (bitpos - 64)) & 3) : (uint8_t)((x.w[0] >> bitpos) & 3);
+        return (uint8_t)((x.w[bitpos / 64] >> (bitpos % 64)) & 3);
     }
     Kmer rc(const Kmer& x) const {
-        Kmer r{{0, 0}};
+        Kmer r{};
         for (uint32_t i = 0; i < k; ++i) push_back(r, (uint8_t)(3 - base_at(x, k - 1 - i)));
         return r;
     }
@@ -193,7 +201,8 @@ struct OMap {
     std::vector<int64_t> idx;
     uint64_t mask = 0;
     static uint64_t h(const Kmer& x) {
-        uint64_t z = x.w[0] * 0x9E3779B97F4A7C15ull ^ (x.w[1] + 0x632BE59BD9B4E019ull);
+        uint64_t z = x.w[0] * 0x9E3779B97F4A7C15ull ^ (x.w[1] + 0x632BE59BD9B4E019ull) ^ (x.w[2] * 0xC2B2AE3D27D4EB4Full) ^
+                     (x.w[3] * 0x165667B19E3779F9ull);
         z ^= z >> 31; z *= 0xBF58476D1CE4E5B9ull; z ^= z >> 29;
         return z;
     }
@@ -284,10 +293,10 @@ struct Worker {
             const unsigned char* lab = (const unsigned char*)in.data() + r.src;
             const uint32_t len = r.len;
             o.n_inst += len - (k - 1);
-            Kmer x{{0, 0}};
+            Kmer x{};
             for (uint32_t i = 0; i < k; ++i) kc.push_back(x, map_base(lab[i]));
             DVertex v; dv_init(kc, v, x);
-            Kmer pred_v{{0, 0}};
+            Kmer pred_v{};
             for (uint32_t idx = 0;; ++idx) {
                 const bool canon = v.canon_fw;
                 const uint8_t pred = idx == 0 ? E : map_base(lab[idx - 1]);
@@ -405,7 +414,7 @@ struct Worker {
     }
 
     Kmer phi_kmer() const {  // all-T k-mer, include/Discontinuity_Graph.hpp:44-49
-        Kmer x{{0, 0}};
+        Kmer x{};
         for (uint32_t i = 0; i < k; ++i) kc.push_back(x, T);
         return x;
     }
@@ -430,7 +439,7 @@ struct orc_ctx {
 };
 
 static bool valid(const orc_params* p) {
-    if (!p || p->k < 3 || p->k > 63 || (p->k % 2) == 0) return false;
+    if (!p || p->k < 3 || p->k > 127 || (p->k % 2) == 0) return false;
     if (p->l < 1 || p->l > 32 || p->l > p->k - 1) return false;
     if (p->cutoff < 1 || p->cutoff > 15) return false;
     if (p->graph_count == 0 || (p->graph_count & (p->graph_count - 1))) return false;
@@ -553,7 +562,7 @@ int orc_run(orc_ctx* c, const char* seq, const uint64_t* rec_off, uint64_t n_rec
         SubOut& o = outs[g];
         for (size_t i = 0; i < o.vkeys.size(); ++i) {
             c->vtx_g.push_back(g);
-            c->vtx_key.push_back(o.vkeys[i].w[1]); c->vtx_key.push_back(o.vkeys[i].w[0]);
+            for (int j = KW - 1; j >= 0; --j) c->vtx_key.push_back(o.vkeys[i].w[j]);   // highest word first
             c->vtx_ef.push_back(o.vstates[i].ef); c->vtx_status.push_back(o.vstates[i].st);
         }
         c->fasta += o.fasta;
@@ -562,8 +571,8 @@ int orc_run(orc_ctx* c, const char* seq, const uint64_t* rec_off, uint64_t n_rec
         for (size_t i = 0; i < o.lm_len.size(); ++i) {
             off += o.lm_len[i];
             c->lm_off.push_back(off);
-            c->lm_u.push_back(o.lm_u[i].w[1]); c->lm_u.push_back(o.lm_u[i].w[0]);
-            c->lm_v.push_back(o.lm_v[i].w[1]); c->lm_v.push_back(o.lm_v[i].w[0]);
+            for (int j = KW - 1; j >= 0; --j) c->lm_u.push_back(o.lm_u[i].w[j]);
+            for (int j = KW - 1; j >= 0; --j) c->lm_v.push_back(o.lm_v[i].w[j]);
             c->lm_flags.push_back(o.lm_flags[i]);
             c->lm_g.push_back(g);
         }

@@ -29,7 +29,7 @@ extern "C" {
 #endif
 
 typedef struct orc_params {
-    uint32_t k;            /* odd, 3..63 */
+    uint32_t k;            /* odd, 3..127 */
     uint32_t l;            /* minimizer length, 1..min(k-1, 32) */
     uint32_t cutoff;       /* edge-frequency threshold, 1..15 */
     uint32_t graph_count;  /* power of two; 16384 in the reference, 1 for the global oracle */
@@ -56,7 +56,7 @@ typedef struct orc_result {
 
     /* vertex states, per subgraph in insertion order */
     const uint32_t* vtx_g;
-    const uint64_t* vtx_key;     /* 2 words per vertex: [high, low] of the canonical k-mer */
+    const uint64_t* vtx_key;     /* 4 words per vertex: the canonical k-mer's words, highest first */
     const uint32_t* vtx_ef;      /* packed 4-bit edge frequencies, front bits 0-15, back 16-31 */
     const uint8_t*  vtx_status;  /* bit0 visited, bit1 disc-front, bit2 disc-back */
 
@@ -67,8 +67,8 @@ typedef struct orc_result {
     /* lm-tigs: labels and discontinuity edges */
     const char*     lm_text;
     const uint64_t* lm_off;      /* n_lmtig + 1 offsets into lm_text */
-    const uint64_t* lm_u;        /* 2 words per lm-tig */
-    const uint64_t* lm_v;        /* 2 words per lm-tig */
+    const uint64_t* lm_u;        /* 4 words per lm-tig, highest first */
+    const uint64_t* lm_v;        /* 4 words per lm-tig, highest first */
     const uint8_t*  lm_flags;    /* bit0 s_u==back, bit1 s_v==back, bit2 u_is_phi, bit3 v_is_phi */
     const uint32_t* lm_g;
 } orc_result;

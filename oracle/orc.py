@@ -64,12 +64,15 @@ def load():
     return _lib
 
 
-def key_label(hi, lo, k):
+KW = 4   # words per k-mer in the oracle's outputs, highest first
+
+
+def key_label(words, k):
+    """A k-mer's words, highest first (KW of them) -> ACGT string."""
     out = []
     for i in range(k):
         bp = 2 * (k - 1 - i)
-        b = (hi >> (bp - 64)) & 3 if bp >= 64 else (lo >> bp) & 3
-        out.append("ACGT"[b])
+        out.append("ACGT"[(words[KW - 1 - (bp >> 6)] >> (bp & 63)) & 3])
     return "".join(out)
 
 
@@ -111,15 +114,15 @@ class OracleRun:
                 return
             self.states = {}
             for i in range(r.n_vertices):
-                lab = key_label(r.vtx_key[2 * i], r.vtx_key[2 * i + 1], k)
+                lab = key_label(r.vtx_key[KW * i:KW * i + KW], k)
                 self.states[(r.vtx_g[i], lab)] = (r.vtx_ef[i], r.vtx_status[i])
             self.fasta = ctypes.string_at(r.fasta, r.fasta_bytes) if r.fasta_bytes else b""
             self.lmtigs = collections.Counter()
             if r.n_lmtig:
                 txt = ctypes.string_at(r.lm_text, r.lm_off[r.n_lmtig]).decode()
                 for i in range(r.n_lmtig):
-                    u = key_label(r.lm_u[2 * i], r.lm_u[2 * i + 1], k)
-                    v = key_label(r.lm_v[2 * i], r.lm_v[2 * i + 1], k)
+                    u = key_label(r.lm_u[KW * i:KW * i + KW], k)
+                    v = key_label(r.lm_v[KW * i:KW * i + KW], k)
                     self.lmtigs[(r.lm_g[i], txt[r.lm_off[i]:r.lm_off[i + 1]], u, v, r.lm_flags[i])] += 1
         finally:
             lib.orc_destroy(ctx)
@@ -158,9 +161,10 @@ def fasta_seq_hashes(fasta):
 
 class OracleArrays:
     """One oracle run with its outputs as numpy arrays (no per-item Python objects):
-    records (g, len, flags, src) sorted, states (g, hi, lo, ef, status) sorted,
-    trivial-unitig sequence hashes sorted, lm-tigs (g, u_hi, u_lo, v_hi, v_lo, flags,
-    label hash) sorted.  src is the record's start in the concatenated input text."""
+    records (g, len, flags, src) sorted, states (g, k3, k2, hi, lo, ef, status) sorted,
+    trivial-unitig sequence hashes sorted, lm-tigs (g, u words, v words, flags, label hash)
+    sorted -- k-mer words from the highest, the field names of STATE_KEY and LMTIG_KEY.
+    src is the record's start in the concatenated input text."""
 
     def __init__(self, data, offsets, n_rec, k, l, cutoff, graph_count, threads=8):
         import numpy as np
@@ -182,19 +186,22 @@ class OracleArrays:
             rec["g"], rec["len"] = arr(r.rec_g, nr, np.uint32), arr(r.rec_len, nr, np.uint8)
             rec["flags"], rec["src"] = arr(r.rec_flags, nr, np.uint8), arr(r.rec_src, nr, np.uint64)
             self.records = sort_rows(rec, ["g", "src", "len", "flags"])
-            st = np.zeros(nv, dtype=[("g", "<u4"), ("hi", "<u8"), ("lo", "<u8"), ("ef", "<u4"), ("status", "u1")])
-            key = arr(r.vtx_key, 2 * nv, np.uint64)
-            st["g"], st["hi"], st["lo"] = arr(r.vtx_g, nv, np.uint32), key[0::2], key[1::2]
+            st = np.zeros(nv, dtype=STATE_KEY)
+            key = arr(r.vtx_key, KW * nv, np.uint64)
+            st["g"] = arr(r.vtx_g, nv, np.uint32)
+            for j, f in enumerate(("k3", "k2", "hi", "lo")):
+                st[f] = key[j::KW]
             st["ef"], st["status"] = arr(r.vtx_ef, nv, np.uint32), arr(r.vtx_status, nv, np.uint8)
-            self.states = sort_rows(st, ["g", "hi", "lo"])
+            self.states = sort_rows(st, ["g", "k3", "k2", "hi", "lo"])
             self.fasta = ctypes.string_at(r.fasta, r.fasta_bytes) if r.fasta_bytes else b""
             self.trivial = fasta_seq_hashes(self.fasta)
             lm = np.zeros(nl, dtype=LMTIG_KEY)
             if nl:
                 off = arr(r.lm_off, nl + 1, np.uint64)
-                u, v = arr(r.lm_u, 2 * nl, np.uint64), arr(r.lm_v, 2 * nl, np.uint64)
+                u, v = arr(r.lm_u, KW * nl, np.uint64), arr(r.lm_v, KW * nl, np.uint64)
                 lm["g"], lm["flags"] = arr(r.lm_g, nl, np.uint32), arr(r.lm_flags, nl, np.uint8)
-                lm["u_hi"], lm["u_lo"], lm["v_hi"], lm["v_lo"] = u[0::2], u[1::2], v[0::2], v[1::2]
+                for j, f in enumerate(("3", "2", "hi", "lo")):
+                    lm["u_" + f], lm["v_" + f] = u[j::KW], v[j::KW]
                 lm["label"] = hash_spans(r.lm_text, off[:-1], np.diff(off))
                 self.lm_text = ctypes.string_at(r.lm_text, int(off[-1]))
                 self.lm_off = off
@@ -208,9 +215,11 @@ class OracleArrays:
             lib.orc_destroy(ctx)
 
 
-# an lm-tig as a comparison key: subgraph, discontinuity vertices (k-mer words), flags, label hash
-LMTIG_KEY = [("g", "<u4"), ("u_hi", "<u8"), ("u_lo", "<u8"), ("v_hi", "<u8"), ("v_lo", "<u8"), ("flags", "u1"),
-             ("label", "<u8")]
+# a vertex state and an lm-tig as comparison keys (k-mer words from the highest; the
+# binding's cfgpu.STATE_KEY / LMTIG_KEY are the same)
+STATE_KEY = [("g", "<u4"), ("k3", "<u8"), ("k2", "<u8"), ("hi", "<u8"), ("lo", "<u8"), ("ef", "<u4"), ("status", "u1")]
+LMTIG_KEY = [("g", "<u4"), ("u_3", "<u8"), ("u_2", "<u8"), ("u_hi", "<u8"), ("u_lo", "<u8"), ("v_3", "<u8"), ("v_2", "<u8"),
+             ("v_hi", "<u8"), ("v_lo", "<u8"), ("flags", "u1"), ("label", "<u8")]
 
 
 def timed_run(data, offsets, n_rec, k, l, cutoff, graph_count=16384, threads=1):

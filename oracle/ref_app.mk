@@ -14,7 +14,7 @@ $(error REF=<reference tree> is required)
 endif
 CXX      ?= g++
 OUT      := _ref
-KS       := 31 63
+KS       := 31 63 95 127
 BASE     := -std=c++17 -O3 -w -DL1_CACHE_LINE_SIZE=64 -DFMT_HEADER_ONLY -pthread -include cstdint \
             -include ref_shim/flushing_ofstream.hpp
 INC      := -Iref_shim_app -Iref_shim -I$(REF)/include -I$(REF)/include/RabbitFX -I$(REF)/src

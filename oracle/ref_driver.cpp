@@ -270,6 +270,7 @@ int main(int argc, char** argv) {
             case 5: mode_min<4>(l); break;   case 9: mode_min<8>(l); break;
             case 15: mode_min<14>(l); break; case 23: mode_min<22>(l); break;
             case 31: mode_min<30>(l); break; case 63: mode_min<62>(l); break;
+            case 95: mode_min<94>(l); break; case 127: mode_min<126>(l); break;
             default: return 3;
         }
         return 0;
@@ -280,6 +281,7 @@ int main(int argc, char** argv) {
             case 5: return run_k<5>(argc, argv);   case 9: return run_k<9>(argc, argv);
             case 15: return run_k<15>(argc, argv); case 23: return run_k<23>(argc, argv);
             case 31: return run_k<31>(argc, argv); case 63: return run_k<63>(argc, argv);
+            case 95: return run_k<95>(argc, argv); case 127: return run_k<127>(argc, argv);
             default: return 3;
         }
     }

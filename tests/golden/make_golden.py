@@ -76,6 +76,16 @@ def main():
         out = drv(["min", str(k), str(l)], "\n".join(seqs) + "\n").splitlines()
         for s, line in zip(seqs, out):
             mins.append({"k": k, "l": l, "seq": s, "hash": [int(v) for v in line.split()]})
+    # k > 63 (the reference built with INSTANCE_COUNT 64), from a second generator so the
+    # cases above stay as they were
+    rng2 = random.Random(2026)
+    for k, l in ((95, 20), (95, 1), (127, 20), (127, 32)):
+        seqs = ["".join(rng2.choice("ACGT") for _ in range(rng2.randrange(k - 1, 400))) for _ in range(4)]
+        seqs.append("A" * 200)
+        seqs.append("AC" * 100)
+        out = drv(["min", str(k), str(l)], "\n".join(seqs) + "\n").splitlines()
+        for s, line in zip(seqs, out):
+            mins.append({"k": k, "l": l, "seq": s, "hash": [int(v) for v in line.split()]})
     json.dump(mins, open(os.path.join(HERE, "minhash.json"), "w"))
 
     states = []
@@ -115,6 +125,21 @@ def main():
         u = rseq(k)
         recs.append(rseq(20) + u + u[::-1].translate(str.maketrans("ACGT", "TGCA")) + rseq(20))
         recs.append(rseq(3 * k) * 3)
+        case = pipeline(recs, k, l, c, G)
+        case["name"] = f"seeded k={k}"
+        cases.append(case)
+    def rseq2(n):
+        return "".join(rng2.choice("ACGT") for _ in range(n))
+
+    for k, l, c, G in ((95, 20, 1, 64), (127, 20, 1, 64), (127, 32, 2, 16)):
+        recs = [rseq2(rng2.randrange(k + 1, 500)) for _ in range(3)]
+        recs.append("A" * (2 * k) + rseq2(30) + "C" * (k + 3))
+        u = rseq2(k)
+        recs.append(rseq2(20) + u + u[::-1].translate(str.maketrans("ACGT", "TGCA")) + rseq2(20))
+        recs.append(rseq2(3 * k) * 3)
+        if c > 1:   # read-like copies so that edges pass the cutoff
+            g = rseq2(600)
+            recs += [g[i:i + 200] for i in range(0, 400, 41)] * 2
         case = pipeline(recs, k, l, c, G)
         case["name"] = f"seeded k={k}"
         cases.append(case)

@@ -35,7 +35,7 @@ def test_library_exports_every_declared_symbol():
 def test_create_rejects_bad_params():
     lib = cfgpu.load()
     ctx = ctypes.c_void_p()
-    for k, l, c, G in ((30, 20, 1, 16384), (65, 20, 1, 16384), (31, 31, 1, 16384), (31, 20, 0, 16384),
+    for k, l, c, G in ((30, 20, 1, 16384), (129, 20, 1, 16384), (31, 31, 1, 16384), (31, 20, 0, 16384),
                        (31, 20, 16, 16384), (31, 20, 1, 1000), (31, 20, 1, 1 << 21)):
         p = cfgpu.Params(k, l, c, G, 0, 0)
         assert lib.cfg_create(0, ctypes.byref(p), ctypes.byref(ctx)) == 1

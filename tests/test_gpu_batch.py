@@ -92,6 +92,13 @@ def test_batch_small_graph_count_and_k63():
     check_batch(63, 20, 1, 4, make_jobs(rng, 63, 3))
 
 
+def test_batch_wide_k():
+    """k = 95 and 127 (three and four key words) in the batched form."""
+    rng = np.random.default_rng(109)
+    check_batch(95, 20, 1, 16384, make_jobs(rng, 95, 5))
+    check_batch(127, 20, 1, 64, make_jobs(rng, 127, 4))
+
+
 def test_batch_redoes_overflowing_jobs():
     rng = np.random.default_rng(104)
     jobs = [[synth.random_seq(rng, 60_000)], [synth.random_seq(rng, 500)], [synth.random_seq(rng, 80_000)]]
@@ -151,9 +158,10 @@ def test_batch_device_input_runs_plain():
         p.close()
 
 
-@pytest.mark.parametrize("k,c,G,load", [(31, 1, 16384, 0), (31, 2, 16384, 0), (63, 1, 64, 0), (31, 1, 64, 10)])
+@pytest.mark.parametrize("k,c,G,load", [(31, 1, 16384, 0), (31, 2, 16384, 0), (63, 1, 64, 0), (31, 1, 64, 10),
+                                        (127, 1, 16384, 0)])
 def test_batch_unitigs_equal_plain(k, c, G, load):
-    """cfg_batch_unitigs: every job's final unitigs (joined on the device, cycles and
+    """cfg_batch_unitigs: every job's final unitigs (joined on the device, cycles included;
     redone jobs on the host) are those cfg_unitigs gives for the job run alone."""
     rng = np.random.default_rng(108 + k + c + G)
     jobs = make_jobs(rng, k, 7)

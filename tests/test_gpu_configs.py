@@ -110,8 +110,8 @@ def oracle_final_unitigs(o, k):
     nl = len(o.lm_g)
     arr = np.zeros(max(nl, 1), dtype=cfgpu.LMTIG_DTYPE)
     if nl:
-        arr["u_hi"][:nl], arr["u_lo"][:nl] = o.lm_u[0::2], o.lm_u[1::2]
-        arr["v_hi"][:nl], arr["v_lo"][:nl] = o.lm_v[0::2], o.lm_v[1::2]
+        for j, f in enumerate(("3", "2", "hi", "lo")):   # the oracle's words come highest first
+            arr["u_" + f][:nl], arr["v_" + f][:nl] = o.lm_u[j::orc.KW], o.lm_v[j::orc.KW]
         arr["label_off"][:nl], arr["label_len"][:nl] = o.lm_off[:-1], np.diff(o.lm_off)
         arr["g"][:nl], arr["flags"][:nl] = o.lm_g, o.lm_flags
     text = ctypes.create_string_buffer(o.lm_text + b"\0")
@@ -165,6 +165,17 @@ def test_config3_k63_30mbp():
     got = gpu_arrays(d, 63, 20, 1, 16384, load_pct=100)
     assert_equal_to_oracle(got, o)
     assert np.array_equal(got["unitigs"], oracle_final_unitigs(o, 63))
+
+
+@pytest.mark.parametrize("k", [95, 127])
+def test_config3_shape_wide_k(k):
+    """Config 3's generator at 8 Mbp with k = 95 and 127 (three and four key words): the
+    tandem-repeat skew through one-CTA and arena tables, bit-exact, and final unitigs."""
+    d = config3_shape(8_000_000, 7, 20)
+    o = orc.OracleArrays(*d, k, 20, 1, 16384)
+    got = gpu_arrays(d, k, 20, 1, 16384, load_pct=100)
+    assert_equal_to_oracle(got, o)
+    assert np.array_equal(got["unitigs"], oracle_final_unitigs(o, k))
 
 
 def reference_build(k, data_offsets, tmp_path, read):
@@ -234,3 +245,12 @@ def test_reference_build_equals_gpu_config2_sample(tmp_path):
     d = config2_reads(200_000)
     want = canonical_hashes(reference_build(31, d, tmp_path, read=True))
     assert np.array_equal(canonical_hashes(gpu_unitig_fasta(d, 31, 20, 2, 131072, 15)), want)
+
+
+@pytest.mark.parametrize("k", [95, 127])
+def test_reference_build_equals_gpu_wide_k(tmp_path, k):
+    """k = 95 and 127 on 3 Mbp of config 3's generator: the reference's own build (compiled
+    with INSTANCE_COUNT 64) and the GPU write the same maximal unitigs."""
+    d = config3_shape(3_000_000, 9, 20)
+    want = canonical_hashes(reference_build(k, d, tmp_path, read=False))
+    assert np.array_equal(canonical_hashes(gpu_unitig_fasta(d, k, 20, 1, 65536, 100)), want)

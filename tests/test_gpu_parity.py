@@ -66,6 +66,15 @@ CASES = [  # k, l, cutoff, G, n, seed
     (33, 15, 1, 1024, 10_000, 11),
     (31, 30, 1, 16384, 10_000, 12),
     (31, 1, 1, 16384, 10_000, 13),
+    # k > 63: three and four key words (the reference built with INSTANCE_COUNT 64)
+    (95, 20, 1, 16384, 40_000, 14),
+    (95, 20, 1, 4, 12_000, 15),
+    (127, 20, 1, 16384, 40_000, 16),
+    (127, 32, 2, 64, 20_000, 17),
+    (65, 20, 1, 1024, 10_000, 18),
+    (97, 1, 1, 256, 10_000, 19),     # window of 96 l-mers: the second block starts a chunk back
+    (101, 4, 1, 256, 10_000, 20),    # 97: two chunks back
+    (127, 1, 1, 256, 10_000, 21),    # 126, the widest window
 ]
 
 
@@ -100,7 +109,7 @@ def test_homopolymer_and_cycles():
             compare(recs, k, l, 1, G)
 
 
-@pytest.mark.parametrize("k", [31, 63])
+@pytest.mark.parametrize("k", [31, 63, 95, 127])
 @pytest.mark.parametrize("load_pct", [1500, 4500, 40000])
 def test_table_modes(k, load_pct):
     """Oversized table requests route subgraphs to one-CTA, cluster (DSMEM; k <= 31 only) and
@@ -118,7 +127,8 @@ def test_small_table_retry():
     assert counts.n_retries > 0
 
 
-@pytest.mark.parametrize("k,l,c,seed", [(31, 20, 1, 31), (31, 20, 2, 32), (63, 20, 1, 33), (15, 7, 1, 34)])
+@pytest.mark.parametrize("k,l,c,seed", [(31, 20, 1, 31), (31, 20, 2, 32), (63, 20, 1, 33), (15, 7, 1, 34),
+                                        (95, 20, 1, 35), (127, 20, 2, 36)])
 def test_final_unitigs_equal_global_oracle(k, l, c, seed):
     """GPU lm-tigs stitched on the host plus GPU trivial unitigs == the global maximal unitigs."""
     rng = np.random.default_rng(seed)
@@ -142,7 +152,8 @@ def test_final_unitigs_equal_global_oracle(k, l, c, seed):
 
 
 @pytest.mark.parametrize("k,l,c,G,seed", [(31, 20, 1, 16384, 41), (31, 20, 2, 16384, 42), (63, 20, 1, 16384, 43),
-                                          (15, 7, 1, 64, 44), (31, 20, 1, 4, 45), (9, 4, 1, 16, 46)])
+                                          (15, 7, 1, 64, 44), (31, 20, 1, 4, 45), (9, 4, 1, 16, 46),
+                                          (95, 20, 1, 16384, 51), (127, 20, 1, 64, 52), (127, 20, 2, 16384, 53)])
 def test_device_unitigs(k, l, c, G, seed):
     """cfg_unitigs (lm-tigs joined on the device) == host collation == the global maximal unitigs."""
     rng = np.random.default_rng(seed)

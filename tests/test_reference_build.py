@@ -5,7 +5,7 @@ the discontinuity-graph phases -- from its sources into oracle/_ref/cuttlefish_r
 (one binary per k).  Its <o>.fa must hold exactly the global maximal unitigs the
 oracle computes (the one-subgraph run), so the oracle -- and through the GPU parity
 tests the CUDA path -- is pinned to the reference end to end, not only to its classes.
-Each run pays the reference's fixed start-up (its 16384 subgraph buckets): two cases.
+Each run pays the reference's fixed start-up (its 16384 subgraph buckets): a few cases.
 """
 import os
 import subprocess
@@ -71,3 +71,19 @@ def test_reference_build_k63_tandem_equals_oracle(tmp_path):
     recs = [bytes(g).decode()]
     got = unitig_set(run_reference(63, recs, tmp_path))
     assert got == unitig_set(orc.OracleRun(recs, 63, 20, 1, 1).fasta)
+
+
+@pytest.mark.parametrize("k", [95, 127])
+def test_reference_build_wide_k_equals_oracle(tmp_path, k):
+    """k > 63: the reference built with INSTANCE_COUNT 64 (Kmer<k> of three and four words)."""
+    rng = np.random.default_rng(303 + k)
+    g = bytearray(synth.genome_with_repeats(rng, 150_000, n_copies=15, n_pal=10).encode())
+    for _ in range(20):                          # tandem repeats of 2-50 bp units
+        U, L = int(rng.integers(2, 51)), int(rng.integers(300, 2000))
+        u = synth.random_seq(rng, U).encode()
+        b = int(rng.integers(0, len(g) - L))
+        g[b:b + L] = (u * (L // U + 1))[:L]
+    s = synth.random_seq(rng, 1_500)
+    recs = [bytes(g).decode(), s + s[:k]]        # and a circular molecule
+    got = unitig_set(run_reference(k, recs, tmp_path))
+    assert got == unitig_set(orc.OracleRun(recs, k, 20, 1, 1).fasta)
