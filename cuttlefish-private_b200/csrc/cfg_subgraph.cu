@@ -340,6 +340,10 @@ __device__ __forceinline__ void sink_for(const SubgraphArgs& a, uint32_t b, Sink
 
 struct Block {   // per-CTA shared bookkeeping (in CLUSTER mode the flags of rank 0 are the cluster's)
     uint32_t inserted, overflow, wl_n, covered;   // covered: vertices of the paths and one-k-mer cycles emitted
+    // work-list counters: slots the build claimed, W1's compacted slots (when that list
+    // overflowed), path ends W1 found, W3's unvisited vertices
+    uint32_t fresh_n, w1_n, end_n, cyc_n;
+    uint32_t dd_over;   // the record merge's table filled up
     unsigned long long vertices, isolated, phantom, trivial, icc, lmtig;
     Sink sk;
     unsigned long long rs[3][32];   // reserve_block: per-warp totals (<= 1024 threads), then their offsets
@@ -764,12 +768,12 @@ __device__ bool dedup_records(const SubgraphArgs& a, Block& B, uint32_t q0, uint
     for (uint32_t e = tid; e < D; e += nt) {
         lkeys[4 * e] = EMPTY; lkeys[4 * e + 1] = EMPTY; lkeys[4 * e + 2] = ~0ull; lkeys[4 * e + 3] = 0;
     }
-    if (tid == 0) { B.overflow = 0; B.wl_n = 0; }
+    if (tid == 0) { B.dd_over = 0; B.wl_n = 0; }
     __syncthreads();
     const uint32_t base = smem_addr(lkeys);
     const uint32_t bound = D > 256 ? D / 4 : D;
     for (uint32_t r = q0 + tid; r < q1; r += nt) {
-        if (*(volatile uint32_t*)&B.overflow) break;
+        if (*(volatile uint32_t*)&B.dd_over) break;
         const uint64_t rec = a.recs[r];
         const uint32_t len = rec_len(rec), pos = rec_pos(rec);
         const RecWords<1> rw(a.packed, pos, true);
@@ -792,10 +796,10 @@ __device__ bool dedup_records(const SubgraphArgs& a, Block& B, uint32_t q0, uint
             }
             if (++h == D) h = 0;
         }
-        if (!done) { atomicOr(&B.overflow, 1u); break; }
+        if (!done) { atomicOr(&B.dd_over, 1u); break; }
     }
     __syncthreads();
-    if (*(volatile uint32_t*)&B.overflow) return false;
+    if (*(volatile uint32_t*)&B.dd_over) return false;   // its own flag: the caller resets B.overflow next
     compact_to(D, wl, &B.wl_n, [&](uint32_t e) { return lkeys[4 * e + 1] != EMPTY; }, [&](uint32_t e) {
         const uint32_t c = (uint32_t)lkeys[4 * e + 3];
         return ((uint32_t)lkeys[4 * e + 2] & 0xFFFFFu) | ((c < 15u ? c : 15u) << 20);
@@ -824,10 +828,16 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
     if constexpr (W == 1 && MODE == LOCAL) {
         if (a.dedup && n_items >= 64 && n_items < (1u << 20) && dedup_records(a, B, q0, q1, per, lkeys, wl)) {
             from_list = true;
-            n_items = B.wl_n;
-            __syncthreads();   // every thread has read the count before it is reset below
+            n_items = B.wl_n;   // only the merge writes this count
         }
     }
+    // One-table modes keep two lists in wl, one growing from each end: the build appends
+    // the slots it claims at the top (the merged records, if any, hold the bottom), and
+    // W1, reading that list, appends the path ends at the bottom -- no pass over every
+    // slot to compact them.  A list that would run into the other falls back to a
+    // compaction pass.  Cluster tables compact per CTA as before.
+    constexpr bool LISTS = MODE != CLUSTER;
+    const uint32_t cap_fresh = per - (from_list ? n_items : 0u);
 
     for (uint32_t s = tid; s < per; s += nt) {
         if constexpr (W == 1) lkeys[2 * s] = EMPTY;
@@ -837,7 +847,8 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         lmeta[s] = 0;
     }
     if (tid == 0) {
-        B.inserted = 0; B.overflow = 0; B.wl_n = 0; B.covered = 0;
+        B.inserted = 0; B.overflow = 0; B.covered = 0;
+        B.fresh_n = 0; B.w1_n = 0; B.end_n = 0; B.cyc_n = 0;
         B.vertices = B.isolated = B.phantom = B.trivial = B.icc = B.lmtig = 0;
         sink_for(a, g, B.sk);
     }
@@ -850,7 +861,8 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
     // edges from its predecessor / successor bases, the self-loop rule against the
     // previous k-mer's canonical form, and the record's entrance / exit marks.
     auto insert = [&](const Kmer<W>& fw, const Kmer<W>& rc, const Kmer<W>& pred_can, uint32_t idx, uint32_t pred,
-                      uint32_t succ, uint32_t p, bool l_mark, bool r_mark, uint32_t m) -> bool {
+                      uint32_t succ, uint32_t p, bool l_mark, bool r_mark, uint32_t m, uint32_t& slot_out,
+                      bool& fresh_out) -> bool {
         const bool canon = fw < rc;
         const Kmer<W> can = canon ? fw : rc;
         uint32_t front = canon ? pred : compb(succ);
@@ -869,6 +881,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         }
         if (s == NONE) { atomicOr(&B.overflow, 1u); return false; }
         n_fresh += fresh;
+        slot_out = s; fresh_out = fresh;
         uint32_t disc = 0;
         if (l_mark) disc |= canon ? M_DISC_F : M_DISC_B;      // entrance side
         if (r_mark) disc |= canon ? M_DISC_B : M_DISC_F;      // exit side
@@ -913,7 +926,8 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
                 const uint32_t mj = __shfl_sync(FULL, mult, j);
                 const RecWords<W> xw = rw.from_lane(j);
                 const uint32_t t = t0 + lane;
-                bool ok = true;
+                bool ok = true, fr = false;
+                uint32_t fs = 0;
                 if (t < total) {
                     const uint32_t idx = t - Pj, len = rec_len(rj);
                     Kmer<W> fw;
@@ -928,7 +942,17 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
                         pc = pf < pr ? pf : pr;
                     }
                     ok = insert(fw, rc, pc, idx, pred, succ, rec_pos(rj) + idx, idx == 0 && rec_ld(rj),
-                                idx + k == len && rec_rd(rj), mj);
+                                idx + k == len && rec_rd(rj), mj, fs, fr);
+                }
+                if constexpr (LISTS) {   // the claimed slots, at the top of wl (one atomic per warp and round)
+                    const uint32_t fm = __ballot_sync(FULL, fr);
+                    if (fm) {
+                        uint32_t b0 = 0;
+                        if (lane == 0) b0 = atomicAdd(&B.fresh_n, (uint32_t)__popc(fm));
+                        b0 = __shfl_sync(FULL, b0, 0);
+                        const uint32_t jx = b0 + __popc(fm & lane_lt());
+                        if (fr && jx < cap_fresh) wl[per - 1 - jx] = fs;
+                    }
                 }
                 // a failed insert (table full) stops the build: warp-uniform, between rounds
                 if (__any_sync(FULL, !ok || *(volatile uint32_t*)&B.overflow)) { stop = true; break; }
@@ -942,12 +966,17 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
     for (int d = 16; d; d >>= 1) n_fresh += __shfl_down_sync(0xffffffffu, n_fresh, d);
     if ((tid & 31) == 0 && n_fresh) atomicAdd(&B.inserted, n_fresh);
     __syncthreads();
-    if (tid == 0 && B.inserted > limit) B.overflow = 1;
-    // one CTA's overflow is the whole cluster's
-    __syncthreads();
-    if (tid == 0 && B.overflow && Bc != &B) atomicOr(&Bc->overflow, 1u);
-    tsync<MODE>();
-    const bool overflow = *(volatile uint32_t*)&Bc->overflow;
+    bool overflow;
+    if constexpr (MODE == CLUSTER) {
+        if (tid == 0 && B.inserted > limit) B.overflow = 1;
+        // one CTA's overflow is the whole cluster's
+        __syncthreads();
+        if (tid == 0 && B.overflow && Bc != &B) atomicOr(&Bc->overflow, 1u);
+        tsync<MODE>();
+        overflow = *(volatile uint32_t*)&Bc->overflow;
+    } else {   // one table: every thread reads the build's final counts
+        overflow = *(volatile uint32_t*)&B.overflow || *(volatile uint32_t*)&B.inserted > limit;
+    }
     if (overflow) {
         if (rank == 0 && tid == 0) {
             const unsigned long long i = atomicAdd(&a.cnt->retry_count, 1ull);
@@ -959,12 +988,23 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
 
     clk[1] = clock64();
     // ---------------- W1: termination of every side ----------------
-    compact(per, wl, &B.wl_n, [&](uint32_t ls) { return !local_empty<W>(lkeys, ls); });
-    __syncthreads();
+    // its list: the slots the build claimed (top of wl), else a compaction (bottom)
+    const uint32_t n_claimed = LISTS ? *(volatile uint32_t*)&B.fresh_n : 0u;
+    const bool l1_top = LISTS && n_claimed <= cap_fresh;
+    if (!l1_top) {
+        compact(per, wl, &B.w1_n, [&](uint32_t ls) { return !local_empty<W>(lkeys, ls); });
+        __syncthreads();
+    }
+    const uint32_t n1 = l1_top ? n_claimed : *(volatile uint32_t*)&B.w1_n;
+    const uint32_t cap_end = per - n1;   // path ends go to the other end of wl
     const bool links = MODE == LOCAL && per <= LINK_SLOTS;
     uint32_t n_vert = 0, n_iso = 0, n_phantom = 0;   // this thread's vertices (summed once per warp)
-    for (uint32_t i = tid, nw = B.wl_n; i < nw; i += nt) {
-        const uint32_t ls = wl[i];
+    for (uint32_t base = 0; base < n1; base += nt) {   // uniform over the CTA: warps append path ends together
+      const uint32_t i = base + tid;
+      bool is_end = false;
+      uint32_t ls = 0;
+      if (i < n1) do {
+        ls = wl[l1_top ? per - 1 - i : i];
         const uint32_t s = base_slot + ls;
         const uint32_t ef = st_ef(lst[sti<W>(ls)]);
         uint32_t meta = lmeta[ls];
@@ -974,7 +1014,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
             ++n_iso;
             if (meta & (M_DISC_F | M_DISC_B)) ++n_phantom;
             lmeta[ls] = meta | M_ISO;
-            continue;
+            break;
         }
         const Kmer<W> x = T.key(s);
         const Kmer<W> xr = ops.rc(x);
@@ -999,6 +1039,18 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
             meta |= side_bits(link ? link : term << 1, side);
         }
         lmeta[ls] = meta;
+        is_end = term_of(meta, FRONT) != T_OK || term_of(meta, BACK) != T_OK;
+      } while (false);
+      if constexpr (LISTS) {
+        const uint32_t em = __ballot_sync(FULL, is_end);
+        if (em) {
+            uint32_t b0 = 0;
+            if ((tid & 31) == 0) b0 = atomicAdd(&B.end_n, (uint32_t)__popc(em));
+            b0 = __shfl_sync(FULL, b0, 0);
+            const uint32_t jx = b0 + __popc(em & lane_lt());
+            if (is_end && jx < cap_end) wl[l1_top ? jx : per - 1 - jx] = ls;
+        }
+      }
     }
     for (int d = 16; d; d >>= 1) {
         n_vert += __shfl_down_sync(0xffffffffu, n_vert, d);
@@ -1014,15 +1066,22 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
 
     clk[2] = clock64();
     // ---------------- W2: paths, walked from their ends ----------------
-    if (tid == 0) B.wl_n = 0;
-    __syncthreads();
-    compact(per, wl, &B.wl_n, [&](uint32_t ls) {
-        if (local_empty<W>(lkeys, ls)) return false;
-        const uint32_t m = lmeta[ls];
-        return !(m & M_ISO) && (term_of(m, FRONT) != T_OK || term_of(m, BACK) != T_OK);
-    });
-    __syncthreads();
-    const uint32_t nw2 = B.wl_n;
+    // its list: the path ends W1 found, else a compaction (bottom of wl)
+    const uint32_t n_ends = *(volatile uint32_t*)&B.end_n;
+    const bool ends_listed = LISTS && n_ends <= cap_end;
+    const bool ends_top = ends_listed && !l1_top;
+    if (!ends_listed) {
+        __syncthreads();   // every thread has read the count
+        if (tid == 0) B.end_n = 0;
+        __syncthreads();
+        compact(per, wl, &B.end_n, [&](uint32_t ls) {
+            if (local_empty<W>(lkeys, ls)) return false;
+            const uint32_t m = lmeta[ls];
+            return !(m & M_ISO) && (term_of(m, FRONT) != T_OK || term_of(m, BACK) != T_OK);
+        });
+        __syncthreads();
+    }
+    const uint32_t nw2 = ends_listed ? n_ends : *(volatile uint32_t*)&B.end_n;
     uint32_t n_cov = 0;   // vertices of what this thread emitted
     for (uint32_t base = 0; base < nw2; base += nt) {   // uniform over the CTA: warps reserve output together
         const uint32_t i = base + tid;
@@ -1036,7 +1095,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         EndInfo st{0, 0, true}, en{0, 0, true};
         bool best_canon = true;
         if (i < nw2) {
-            const uint32_t ls = wl[i];
+            const uint32_t ls = wl[ends_top ? per - 1 - i : i];
             s = base_slot + ls;
             e = s;
             const uint32_t meta = lmeta[ls];
@@ -1148,14 +1207,12 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
     // Every path is emitted once, with its vertices counted: when they cover every vertex
     // with an edge, no isolated cycle is left (one CTA's table; a cluster's paths span CTAs)
     const bool no_cycles = MODE != CLUSTER && B.covered == B.vertices - B.isolated;
-    if (tid == 0) B.wl_n = 0;
-    __syncthreads();
     if (!no_cycles) {
-        compact(per, wl, &B.wl_n, [&](uint32_t ls) {
+        compact(per, wl, &B.cyc_n, [&](uint32_t ls) {
             return !local_empty<W>(lkeys, ls) && !(lmeta[ls] & (M_ISO | M_VISITED));
         });
         __syncthreads();
-        const uint32_t nw3 = B.wl_n;
+        const uint32_t nw3 = B.cyc_n;
         for (uint32_t base = 0; base < nw3; base += nt) {
             const uint32_t i = base + tid;
             bool emit = false;
