@@ -118,12 +118,11 @@ struct UnitigInput {
 };
 // ... the buffers it works in ...
 struct UnitigBuffers {
-    DevBuf b_lm, b_label, b_tab, b_partner, b_X0, b_X1, b_fin, b_off, b_words, b_out, b_job, b_flip, b_sx, b_sw, b_len, b_ends;
+    DevBuf b_label, b_tab, b_partner, b_X0, b_X1, b_fin, b_off, b_words, b_out, b_job, b_flip, b_sx, b_sw, b_len, b_ends;
     ulonglong2* ends = nullptr;   // both ends of each gathered lm-tig, packed for the pairing pass
     uint32_t end_words = 2;       // 64-bit words per end there: 2 for k <= 63, 4 beyond (set from k)
-    uint32_t* len = nullptr;   // each gathered lm-tig's label length (the kernels that need only it read 4 bytes, not 48)
+    uint32_t* len = nullptr;   // each gathered lm-tig's label length (the kernels after the gather read 4 bytes, not a record)
     uint8_t* flipb = nullptr;  // per lm-tig heading its chain's walked list: flip it
-    LmtigOut* lm = nullptr;
     uint32_t* job = nullptr;   // batch: each gathered lm-tig's job
     const char** label = nullptr;
     void* tab = nullptr;
@@ -143,7 +142,7 @@ struct UnitigBuffers {
         return true;
     }
     void release() {
-        DevBuf* all[] = {&b_lm, &b_label, &b_tab, &b_partner, &b_X0, &b_X1, &b_fin, &b_off, &b_words, &b_out, &b_job,
+        DevBuf* all[] = {&b_label, &b_tab, &b_partner, &b_X0, &b_X1, &b_fin, &b_off, &b_words, &b_out, &b_job,
                          &b_flip, &b_sx, &b_sw, &b_len, &b_ends};
         for (DevBuf* b : all) b->release();
     }

@@ -107,14 +107,13 @@ template <int EW> struct EndKey {
 // 0: gather the striped lm-tigs into one array with their label addresses.
 __global__ void k_ut_gather(const LmtigOut* lm, uint64_t lm_slice, const char* text, uint64_t text_slice,
                             const unsigned long long* __restrict__ lm_base, const unsigned long long* __restrict__ text_base,
-                            const unsigned long long* __restrict__ stripe_cur, uint32_t stripes, LmtigOut* out,
+                            const unsigned long long* __restrict__ stripe_cur, uint32_t stripes,
                             const char** label, uint32_t* lens, ulonglong2* ends, uint32_t ew) {
     for (uint32_t st = blockIdx.y; st < stripes; st += gridDim.y) {
         const unsigned long long n = stripe_cur[st * JOB_CUR_STRIDE + 2];
         for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
             const LmtigOut m = lm[st * lm_slice + i];
             const uint64_t g = lm_base[st] + i;
-            out[g] = m;
             lens[g] = m.label_len;
             put_ends(ends, g, m, ew);
             label[g] = text + st * text_slice + (m.label_off - text_base[st]);
@@ -125,7 +124,7 @@ __global__ void k_ut_gather(const LmtigOut* lm, uint64_t lm_slice, const char* t
 // 0 (batch): gather every job's lm-tigs from its regions; the job rides along.
 __global__ void k_ut_gather_jobs(const LmtigOut* lm, const char* text, const JobOut* __restrict__ jobs, uint32_t n_jobs,
                                  const unsigned long long* __restrict__ job_n, const unsigned long long* __restrict__ job_lm_base,
-                                 LmtigOut* out, const char** label, uint32_t* out_job, uint32_t* lens,
+                                 const char** label, uint32_t* out_job, uint32_t* lens,
                                  ulonglong2* ends, uint32_t ew) {
     for (uint32_t j = blockIdx.y; j < n_jobs; j += gridDim.y) {
         const unsigned long long n = job_n[j];
@@ -133,7 +132,6 @@ __global__ void k_ut_gather_jobs(const LmtigOut* lm, const char* text, const Job
         for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
             const LmtigOut m = lm[J.lm_off + i];
             const uint64_t g = job_lm_base[j] + i;
-            out[g] = m;
             lens[g] = m.label_len;
             put_ends(ends, g, m, ew);
             label[g] = text + J.lm_text_off + m.label_off;
@@ -537,7 +535,7 @@ __global__ void k_cy_number(uint32_t* fin, uint64_t n, uint32_t* cyc_lm, unsigne
 }
 
 struct CyArgs {
-    const LmtigOut* lm; const char* const* label; const uint32_t* partner; const uint32_t* fin;
+    const uint32_t* len; const char* const* label; const uint32_t* partner; const uint32_t* fin;
     const uint32_t* cyc_lm; uint64_t m2;    // entries: 2 x cycle lm-tigs
     const uint32_t* job;                    // batch: each gathered lm-tig's job (nullptr: one job)
     uint32_t* rec_job;                      // per cycle record (in head order): its job
@@ -557,7 +555,7 @@ __global__ void k_cy_init(CyArgs a) {
         else nx = 2 * (a.fin[y >> 1] & ~CYC) + (y & 1);
         a.succ[X] = nx; a.jmp0[X] = nx;
         a.mn0[X] = 2 * i + d;
-        const uint32_t len = a.lm[i].label_len;
+        const uint32_t len = a.len[i];
         a.w[X] = len >= a.k ? len - a.k : 0;
     }
 }
@@ -623,7 +621,7 @@ __global__ void k_cy_text(CyArgs a, const unsigned long long* __restrict__ scr_o
     for (uint64_t X = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; X < a.m2; X += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t H = a.head[X];
         if (H == NONE) continue;
-        const uint32_t i = a.cyc_lm[X >> 1], len = a.lm[i].label_len;
+        const uint32_t i = a.cyc_lm[X >> 1], len = a.len[i];
         const char* lab = a.label[i];
         char* dst = scr + scr_off[H] + a.pos[X];
         const uint64_t wx = a.w[X];
@@ -728,7 +726,7 @@ bool UnitigBuffers::ensure(uint64_t n) {
     // pairing it holds the splitters' second ranking buffer (up to 2n records)
     const uint64_t t = 4 * n + 64;
     const uint64_t n2 = 2 * n + 2;
-    if (!b_lm.ensure(sizeof(LmtigOut) * (n + 1)) || !b_label.ensure(8 * (n + 1)) || !b_tab.ensure(sizeof(EndSlot) * t) ||
+    if (!b_label.ensure(8 * (n + 1)) || !b_tab.ensure(sizeof(EndSlot) * t) ||
         !b_partner.ensure(4 * n2) || !b_X0.ensure(sizeof(RankRec) * n2) || !b_X1.ensure(sizeof(RankRec) * n2) ||
         !b_fin.ensure(4 * (n + 1)) || !b_sx.ensure(4 * n2) || !b_sw.ensure(4 * n2) ||
         !b_off.ensure(8 * n2) || !b_words.ensure(64) || !b_job.ensure(4 * (n + 1)) || !b_flip.ensure(n + 1) ||
@@ -738,7 +736,7 @@ bool UnitigBuffers::ensure(uint64_t n) {
     ends = b_ends.as<ulonglong2>();
     job = b_job.as<uint32_t>();
     flipb = b_flip.as<uint8_t>();
-    lm = b_lm.as<LmtigOut>(); label = (const char**)b_label.p; tab = b_tab.p; tab_n = t;
+    label = (const char**)b_label.p; tab = b_tab.p; tab_n = t;
     partner = b_partner.as<uint32_t>(); X[0] = b_X0.p; X[1] = b_X1.p;
     fin = b_fin.as<uint32_t>(); out_off = b_off.as<unsigned long long>();
     sx = b_sx.as<uint32_t>();
@@ -763,7 +761,7 @@ int collate_cycles_on_device(UnitigBuffers& ub, uint64_t n, uint64_t m, uint32_t
     auto take = [&](size_t bytes) { unsigned char* q = p; p += (bytes + 15) & ~(size_t)15; return q; };
     unsigned long long* cur = (unsigned long long*)take(32);
     CyArgs a{};
-    a.lm = ub.lm; a.label = ub.label; a.partner = ub.partner; a.fin = ub.fin; a.m2 = m2; a.k = k; a.err = err;
+    a.len = ub.len; a.label = ub.label; a.partner = ub.partner; a.fin = ub.fin; a.m2 = m2; a.k = k; a.err = err;
     a.w = (unsigned long long*)take(8 * m2); a.acc0 = (unsigned long long*)take(8 * m2);
     a.acc1 = (unsigned long long*)take(8 * m2); a.pos = (unsigned long long*)take(8 * m2);
     unsigned long long* T_of = (unsigned long long*)take(8 * m2);
@@ -835,10 +833,10 @@ int collate_device(const UnitigInput& in, UnitigBuffers& ub, cudaStream_t s, Uni
     const uint32_t* job = in.jobs ? ub.job : nullptr;
     if (in.jobs)
         k_ut_gather_jobs<<<dim3(16, std::min<uint32_t>(in.n_jobs, 65535)), 256, 0, s>>>(
-            in.job_lm, in.job_text, in.jobs, in.n_jobs, in.job_n, in.job_lm_base, ub.lm, ub.label, ub.job, ub.len, ub.ends, ub.end_words);
+            in.job_lm, in.job_text, in.jobs, in.n_jobs, in.job_n, in.job_lm_base, ub.label, ub.job, ub.len, ub.ends, ub.end_words);
     else
         k_ut_gather<<<dim3(64, in.stripes), 256, 0, s>>>(in.lm, in.lm_slice, in.text, in.text_slice, in.lm_base, in.text_base,
-                                                         in.stripe_cur, in.stripes, ub.lm, ub.label, ub.len, ub.ends, ub.end_words);
+                                                         in.stripe_cur, in.stripes, ub.label, ub.len, ub.ends, ub.end_words);
     if (cudaMemsetAsync(ub.tab, 0xff, sizeof(EndSlot) * ub.tab_n, s) != cudaSuccess ||
         cudaMemsetAsync(ub.partner, 0xff, 4 * 2 * n, s) != cudaSuccess)
         return CFG_ERR_CUDA;
