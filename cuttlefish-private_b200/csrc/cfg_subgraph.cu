@@ -41,7 +41,7 @@ namespace {
 
 constexpr uint32_t NONE = 0xffffffffu;
 constexpr uint64_t EMPTY = ~0ull;
-constexpr uint64_t BUSY = ~1ull;   // a two-word key's high word while its low word is written
+constexpr uint64_t BUSY = ~1ull;   // a three- or four-word key's highest word while the others are written
 constexpr uint64_t ST_INIT = 0xffffffff00000000ull;   // a new slot's state: no edges, first occurrence "none"
 // walk termination kinds (Walk_Termination, include/Subgraph.hpp:362-369)
 constexpr uint32_t T_OK = 0, T_BRANCHED = 1, T_CROSSED = 2, T_DEAD = 3, T_EXIT = 4;
@@ -198,6 +198,11 @@ struct Tab {
                 M::ld2(a, top, stv);   // key and state together
                 if (top == EMPTY) return NONE;
                 if (top == x.lo) return b + h;
+            } else if constexpr (W == 2) {
+                uint64_t lo, hi;
+                M::ld2(a, lo, hi);     // the whole key in one read (the table no longer changes)
+                if (hi == EMPTY) return NONE;
+                if (hi == x.hi && lo == x.lo) { stv = ld_st(b + h); return b + h; }
             } else {
                 const uint64_t top = M::ld64(a + 8 * (W - 1));
                 if (top == EMPTY) return NONE;
@@ -232,6 +237,19 @@ struct Tab {
                     if (old == EMPTY) { fresh = true; seen = ST_INIT; return b + h; }
                     if (old == x.lo) { seen = stv; return b + h; }
                 }
+            } else if constexpr (W == 2) {
+                // two-word key: one 16-byte CAS claims a free slot (both words EMPTY) with the
+                // whole key, so no reader waits on half of one.  A plain 16-byte read showing an
+                // EMPTY word may have caught a claim in progress (a real key's high word holds
+                // k - 32 <= 31 bases and is never EMPTY; its low word may be all ones), so such a
+                // slot is read again atomically by the same CAS, which fails on a taken slot.
+                uint64_t lo, hi;
+                M::ld2(a, lo, hi);
+                if (hi == EMPTY || lo == EMPTY) {
+                    M::cas128(a, EMPTY, EMPTY, x.lo, x.hi, lo, hi);
+                    if (lo == EMPTY && hi == EMPTY) { fresh = true; seen = ST_INIT; return b + h; }
+                }
+                if (lo == x.lo && hi == x.hi) { seen = M::ld64(sa(b + h)); return b + h; }
             } else {
                 // multi-word key: claim the highest word with a 64-bit CAS (EMPTY -> BUSY),
                 // write the others, then publish the highest; readers wait (bounded) on BUSY
@@ -530,10 +548,13 @@ struct WordWriter {
     }
 };
 
-// Writes the label of the path of n vertices that starts at v (in walk direction).
+// Writes the label of the path of n vertices that starts at v (in walk direction).  With
+// links (one-CTA tables of at most LINK_SLOTS slots) every step follows the link W1 stored
+// for the side it leaves by -- every side inside a path or an isolated cycle has one -- and
+// appends the base of the side's single edge, with no table lookup.
 template <int W, int MODE>
 __device__ void write_path(const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t fth, DV<W> v, int side, uint32_t n,
-                           char* dst, bool rev, bool mark) {
+                           char* dst, bool rev, bool mark, bool links = false) {
     const uint32_t k = ops.k, L = n + k - 1;
     WordWriter ww;
     auto put = [&](uint32_t i, uint32_t b) {
@@ -544,8 +565,20 @@ __device__ void write_path(const Tab<W, MODE>& T, const KOps<W>& ops, uint32_t f
     if (mark) T.or_meta(v.slot, M_VISITED);
     for (uint32_t t = 1; t < n; ++t) {
         int s_in;
-        if (!step(T, ops, fth, v, side, s_in)) break;
-        if (dst) put(k - 1 + t, ops.last_base(v.d));
+        uint32_t b;
+        if (links) {
+            const uint32_t f = side_field(T.ld_meta(v.slot), side);
+            if (!(f & 1)) break;
+            const uint32_t e = ef_edge_at(st_ef(v.st), side, fth);
+            b = side == BACK ? e : 3 - e;
+            v.slot = (f >> 1) & (LINK_SLOTS - 1);
+            s_in = (int)(f >> 13);
+            v.st = T.ld_st(v.slot);
+        } else {
+            if (!step(T, ops, fth, v, side, s_in)) break;
+            b = ops.last_base(v.d);
+        }
+        if (dst) put(k - 1 + t, b);
         if (mark) T.or_meta(v.slot, M_VISITED);
         side = 1 - s_in;
     }
@@ -713,7 +746,7 @@ __device__ void write_emitted_path(const SubgraphArgs& a, const Tab<W, MODE>& T,
                                    int side0, uint32_t n, const DV<W>& vlast, EndInfo st, EndInfo en, bool seed_canon,
                                    Block& B, bool lm, unsigned long long fo, unsigned long long idx,
                                    unsigned long long off, bool buffered, unsigned long long steps0,
-                                   unsigned long long steps1, const Kmer<W>& first, uint32_t skip) {
+                                   unsigned long long steps1, const Kmer<W>& first, uint32_t skip, bool links) {
     const uint32_t k = ops.k, fth = a.fth;
     const uint32_t L = n + k - 1;
     if (!lm) {
@@ -721,7 +754,7 @@ __device__ void write_emitted_path(const SubgraphArgs& a, const Tab<W, MODE>& T,
         const bool rev = vlast.r < v0.d;   // rc(last k-mer) < first k-mer
         char* p = fasta_at(B.sk, fo, L);
         if (buffered) write_buffered(ops, first, steps0, steps1, skip, L, p, rev);
-        else write_path(T, ops, fth, v0, side0, n, p, rev, true);
+        else write_path(T, ops, fth, v0, side0, n, p, rev, true, links);
         atomicAdd(&B.trivial, 1ull);
         return;
     }
@@ -735,7 +768,7 @@ __device__ void write_emitted_path(const SubgraphArgs& a, const Tab<W, MODE>& T,
     const bool fits = idx < sk.lm_cap && off + L <= sk.lm_text_cap;
     if (!fits) atomicOr(sk.oflow, DERR_OUT_OVERFLOW);
     if (buffered) write_buffered(ops, first, steps0, steps1, skip, L, fits ? sk.lm_text + off : nullptr, rev);
-    else write_path(T, ops, fth, v0, side0, n, fits ? sk.lm_text + off : nullptr, rev, true);
+    else write_path(T, ops, fth, v0, side0, n, fits ? sk.lm_text + off : nullptr, rev, true, links);
     if (!fits) return;
     LmtigOut o;
     const Kmer<W> phi = phi_kmer(ops);
@@ -1192,7 +1225,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
         if (path) {
             const bool buffered = W <= 2 && walked > 0 && walked - 1 <= STEP_BUF;
             write_emitted_path(a, T, ops, vs, sd0, n2, ve, st, en, best_canon, B, lm, fo, r.lm_idx, r.lm_off,
-                               buffered, steps0, steps1, first, kc0 ? 1u : 0u);
+                               buffered, steps0, steps1, first, kc0 ? 1u : 0u, links);
         }
         if (mark0) T.or_meta(s, M_VISITED);
         if (mark1) T.or_meta(e, M_VISITED);
@@ -1241,7 +1274,7 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
                 // Character_Buffer::rotate_append_cycle (include/Character_Buffer.hpp:166-175): start at the
                 // minimum vertex in its canonical orientation
                 char* p = fasta_at(B.sk, r.fa, n + k - 1);
-                write_path(T, ops, fth, v0, BACK, n, p, false, true);
+                write_path(T, ops, fth, v0, BACK, n, p, false, true, links);
                 atomicAdd(&B.trivial, 1ull); atomicAdd(&B.icc, 1ull);
             }
         }
