@@ -107,8 +107,8 @@ __device__ void sweep_fragment(const PartitionArgs& a, const uint8_t* mod_w, uin
     const uint32_t start = j0 == 0 ? 0 : j0 - 1;   // position j0-1 only primes the change test
     const uint32_t dq = w - (1u << E);
     // hash of l-mer q, or "none" (all ones, above every hash) outside the fragment
-    auto hash_at = [&](int64_t q) -> uint64_t {
-        return (q >= 0 && q < (int64_t)n_lmers) ? lmer_hash_at(a, F0 + (uint64_t)q, l) : ~0ull;
+    auto hash_at = [&](int64_t q) -> uint64_t {   // a negative q wraps above every l-mer count: one compare
+        return (uint64_t)q < (uint64_t)n_lmers ? lmer_hash_at(a, F0 + (uint64_t)q, l) : ~0ull;
     };
     uint64_t lv[E + 1], pv[E + 1];   // this chunk's / the previous chunk's level values
     uint64_t ppE = ~0ull;            // level E two chunks back (E = 6 only)

@@ -923,11 +923,16 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
     };
     // Each warp takes 32 items (records, or distinct records with their multiplicity) at
     // a time; lane i loads item i's record and its bases once (<= 2 words for k <= 31, <= 4
-    // for k <= 63).  The records' k-mer instances are then dealt out 32 per round, so every
-    // lane has work whatever the record lengths: the lane of instance t finds its record
-    // from the bit mask of the records starting in the round and takes that record's words
-    // (and multiplicity) from its owner lane by shuffles.
+    // for k <= 63).  The records' k-mer instances are then dealt out in runs of up to RUN
+    // consecutive instances of one record, 32 runs per round, so every lane has work
+    // whatever the record lengths: the lane of run t finds its record from the bit mask of
+    // the records starting in the round and takes that record's words (and multiplicity)
+    // from its owner lane by shuffles.  A run's first k-mer is cut from the record's words;
+    // each next one rolls in one base (its reverse complement, predecessor base and the
+    // previous canonical k-mer come from the instance before).  k <= 31 deals single
+    // instances: its records are short (<= 61 bases), and runs left lanes idle there.
     {
+        constexpr uint32_t RUN = W == 1 ? 1 : 4;
         const uint32_t lane = tid & 31, nwarps = nt >> 5;
         const uint32_t le_mask = lane_lt() | (1u << lane);
         bool stop = false;
@@ -938,13 +943,14 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
             const uint64_t rec = has ? a.recs[q0 + (from_list ? item & 0xFFFFFu : item)] : 0ull;
             const uint32_t mult = from_list ? item >> 20 : 1u;
             const uint32_t ninst = has ? rec_len(rec) - k + 1 : 0u;
-            uint32_t incl = ninst;
+            const uint32_t nrun = (ninst + RUN - 1) / RUN;
+            uint32_t incl = nrun;
 #pragma unroll
             for (int d = 1; d < 32; d <<= 1) {
                 const uint32_t y = __shfl_up_sync(FULL, incl, d);
                 if (lane >= (uint32_t)d) incl += y;
             }
-            const uint32_t P = incl - ninst;                      // first instance of record `lane`
+            const uint32_t P = incl - nrun;                       // first run of record `lane`
             const uint32_t total = __shfl_sync(FULL, incl, 31);
             const RecWords<W> rw(a.packed, has ? rec_pos(rec) : 0u, has, has ? rec_len(rec) : 0u);
             uint32_t started = 0;                                 // records started before the round
@@ -952,39 +958,55 @@ __device__ void run_subgraph(const SubgraphArgs& a, const Tab<W, MODE>& T, Block
                 const uint32_t bit = (has && P >= t0 && P < t0 + 32) ? 1u << (P - t0) : 0u;
                 const uint32_t smask = __reduce_or_sync(FULL, bit);
                 const uint32_t jj = started + __popc(smask & le_mask);
-                const uint32_t j = jj ? min(jj - 1, 31u) : 0u;   // the record of instance t0 + lane
+                const uint32_t j = jj ? min(jj - 1, 31u) : 0u;   // the record of run t0 + lane
                 started += __popc(smask);
                 const uint64_t rj = __shfl_sync(FULL, rec, j);
                 const uint32_t Pj = __shfl_sync(FULL, P, j);
                 const uint32_t mj = __shfl_sync(FULL, mult, j);
                 const RecWords<W> xw = rw.from_lane(j);
                 const uint32_t t = t0 + lane;
-                bool ok = true, fr = false;
-                uint32_t fs = 0;
-                if (t < total) {
-                    const uint32_t idx = t - Pj, len = rec_len(rj);
-                    Kmer<W> fw;
-                    uint32_t pred, succ;
-                    xw.kmer_at(k, idx, len, fw, pred, succ);
-                    const Kmer<W> rc = ops.rc(fw);
-                    Kmer<W> pc = fw;
-                    if (idx > 0) {   // the previous k-mer and its reverse complement, from fw and rc
+                const uint32_t len = rec_len(rj);
+                const uint32_t idx0 = t < total ? (t - Pj) * RUN : 0u;
+                const uint32_t cnt = t < total ? min(RUN, len - k + 1 - idx0) : 0u;
+                bool ok = true;
+                Kmer<W> fw{}, rc{}, pc{};
+                uint32_t pred = 0, succ = 0;
+                if (cnt) {
+                    xw.kmer_at(k, idx0, len, fw, pred, succ);
+                    rc = ops.rc(fw);
+                    pc = fw;
+                    if (idx0 > 0) {   // the previous k-mer and its reverse complement, from fw and rc
                         Kmer<W> pf = fw, pr = rc;
                         ops.push_front(pf, pred);
                         ops.push_back(pr, 3 - pred);
                         pc = pf < pr ? pf : pr;
                     }
-                    ok = insert(fw, rc, pc, idx, pred, succ, rec_pos(rj) + idx, idx == 0 && rec_ld(rj),
-                                idx + k == len && rec_rd(rj), mj, fs, fr);
                 }
-                if constexpr (LISTS) {   // the claimed slots, at the top of wl (one atomic per warp and round)
-                    const uint32_t fm = __ballot_sync(FULL, fr);
-                    if (fm) {
-                        uint32_t b0 = 0;
-                        if (lane == 0) b0 = atomicAdd(&B.fresh_n, (uint32_t)__popc(fm));
-                        b0 = __shfl_sync(FULL, b0, 0);
-                        const uint32_t jx = b0 + __popc(fm & lane_lt());
-                        if (fr && jx < cap_fresh) wl[per - 1 - jx] = fs;
+#pragma unroll 1
+                for (uint32_t r = 0; r < RUN; ++r) {   // uniform over the warp
+                    bool fr = false;
+                    uint32_t fs = 0;
+                    if (r < cnt && ok) {
+                        const uint32_t idx = idx0 + r;
+                        if (r > 0) {   // roll in the base after the previous k-mer
+                            pc = fw < rc ? fw : rc;
+                            pred = ops.first_base(fw);
+                            ops.push_back(fw, succ);
+                            ops.push_front(rc, 3 - succ);
+                            succ = idx + k == len ? BASE_E : xw.base(idx + k);
+                        }
+                        ok = insert(fw, rc, pc, idx, pred, succ, rec_pos(rj) + idx, idx == 0 && rec_ld(rj),
+                                    idx + k == len && rec_rd(rj), mj, fs, fr);
+                    }
+                    if constexpr (LISTS) {   // the claimed slots, at the top of wl (one atomic per warp and step)
+                        const uint32_t fm = __ballot_sync(FULL, fr);
+                        if (fm) {
+                            uint32_t b0 = 0;
+                            if (lane == 0) b0 = atomicAdd(&B.fresh_n, (uint32_t)__popc(fm));
+                            b0 = __shfl_sync(FULL, b0, 0);
+                            const uint32_t jx = b0 + __popc(fm & lane_lt());
+                            if (fr && jx < cap_fresh) wl[per - 1 - jx] = fs;
+                        }
                     }
                 }
                 // a failed insert (table full) stops the build: warp-uniform, between rounds
