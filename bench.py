@@ -40,6 +40,8 @@ WORKLOADS = {
     "reads30x": (31, 20, 2, 15, "10M x 150 bp reads, 30x of a 50 Mbp genome with 2% repeats, 0.5% errors, both strands"),
     "ref5m": (31, 20, 1, 100, "one 5 Mbp record with 200 repeat copies (1% divergence) and 50 palindromes"),
     "ref500m": (63, 20, 1, 100, "500 Mbp in 20 records, 10% tandem + 5% interspersed repeats"),
+    # not a benchmark configuration: the ref500m sequence at the widest k (four-word k-mers)
+    "ref500m_k127": (127, 20, 1, 100, "the ref500m sequence (500 Mbp, 20 records) at k = 127"),
 }
 
 
@@ -98,7 +100,7 @@ def make_workload(name, n_reads=10_000_000):
         g = ctypes.create_string_buffer(n)
         lib.cfs_ref5m(g)
         return g, (ctypes.c_uint64 * 2)(0, n), 1
-    if name == "ref500m":
+    if name in ("ref500m", "ref500m_k127"):
         n = lib.cfs_ref500m_len()
         g = ctypes.create_string_buffer(n)
         cuts = (ctypes.c_uint64 * 21)()
@@ -381,7 +383,7 @@ def bench_serve(args, local, world):
         return lat, done, dev / 1e3
 
     srv = cfgpu.Server(device=local if world > 1 else 0, slots=4, batch_max_bases=64_000_000,
-                       small_job_bases=4_000_000, large_job_bases=64 << 20, large_slots=2)
+                       small_job_bases=4_000_000, large_job_bases=64 << 20, large_slots=args.serve_large_slots)
 
     def run_server(arr):
         start = time.perf_counter()
@@ -458,7 +460,7 @@ def bench_serve(args, local, world):
         "pool_jobs": len(jobs), "pool_bases": pool_bases, "arrivals_per_rate": args.serve_arrivals,
         "plain_service_jobs_per_s": mu, "plain_sequential_bases_per_s": pool_bases / seq_s,
         "server": {"slots": 4, "batch_max_bases": 64_000_000, "small_job_bases": 4_000_000,
-                   "large_job_bases": 64 << 20, "large_slots": 2,
+                   "large_job_bases": 64 << 20, "large_slots": args.serve_large_slots,
                    "batches": int(st.batches), "batched_jobs": int(st.batched_jobs),
                    "max_running": int(st.max_running), "max_running_large": int(st.max_running_large),
                    "hbm_budget": int(st.hbm_budget), "contexts_created": int(st.contexts_created),
@@ -888,6 +890,7 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=2)
     ap.add_argument("--serve-jobs", type=int, default=16, help="generated jobs of the serving pool (0: skip serving)")
     ap.add_argument("--serve-arrivals", type=int, default=240, help="arrivals per rate, each a job of the pool")
+    ap.add_argument("--serve-large-slots", type=int, default=2, help="jobs above 64 M bases the server runs at once")
     ap.add_argument("--serve-load", type=float, nargs="+", default=[0.5, 1.0, 2.0],
                     help="arrival rates as multiples of the plain path's service rate")
     args = ap.parse_args()

@@ -17,10 +17,10 @@ import synth
 pytestmark = pytest.mark.gpu
 
 
-def gpu_run(records, k, l, c, G, load_pct=0, extra_flags=0):
+def gpu_run(records, k, l, c, G, load_pct=0, extra_flags=0, slots_per_thread=0):
     packed = cfgpu.PackedInput(records, k)
     flags = cfgpu.CFG_FLAG_DUMP_STATES | cfgpu.CFG_FLAG_DUMP_RECORDS | extra_flags
-    with cfgpu.Compactor(k, l, c, G, flags=flags, table_load_pct=load_pct) as cx:
+    with cfgpu.Compactor(k, l, c, G, flags=flags, table_load_pct=load_pct, slots_per_thread=slots_per_thread) as cx:
         cx.submit(packed)
         cx.run()
         counts, fasta, lms = cx.fetch()
@@ -37,9 +37,9 @@ def gpu_run(records, k, l, c, G, load_pct=0, extra_flags=0):
     return counts, rec_ms, st, orc.fasta_multiset(fasta), lm
 
 
-def compare(records, k, l, c, G, load_pct=0, extra_flags=0):
+def compare(records, k, l, c, G, load_pct=0, extra_flags=0, slots_per_thread=0):
     o = orc.OracleRun(records, k, l, c, G)
-    counts, rec_ms, st, fa, lm = gpu_run(records, k, l, c, G, load_pct, extra_flags)
+    counts, rec_ms, st, fa, lm = gpu_run(records, k, l, c, G, load_pct, extra_flags, slots_per_thread)
     assert counts.n_records == o.counts["n_records"]
     assert counts.n_instances == o.counts["n_instances"]
     assert rec_ms == o.records, "weak super k-mer records differ"
@@ -117,6 +117,15 @@ def test_table_modes(k, load_pct):
     rng = np.random.default_rng(24 + load_pct)
     recs = [synth.adversarial(rng, 20_000, k) for _ in range(2)]
     compare(recs, k, 20, 1, 64, load_pct=load_pct)
+
+
+@pytest.mark.parametrize("k", [31, 63])
+@pytest.mark.parametrize("spt", [2, 8, 16])
+def test_slots_per_thread(k, spt):
+    """The launch knob slots_per_thread changes only the CTA size of one-CTA tables."""
+    rng = np.random.default_rng(25 + spt)
+    recs = [synth.adversarial(rng, 20_000, k) for _ in range(2)]
+    compare(recs, k, 20, 1, 64, slots_per_thread=spt)
 
 
 def test_small_table_retry():
