@@ -55,9 +55,10 @@ struct HostBuf {
 // Device buffers of the text parser (cfg_parse.cu): per-chunk scan words, break
 // ranks, the fragment table and the packed stream it produces.
 struct ParseBuffers {
-    DevBuf cf, cb, ck, br, fo, pn, pbb, foff, flen, tot, pk, tf;
+    DevBuf cf, cb, ck, br, fo, pn, pbb, foff, flen, tot, pk, tf, tp;
     uint32_t* chunk_f = nullptr;
     uint16_t* thread_f = nullptr;   // per thread of every chunk: the chunk's function before its bytes
+    uint32_t* thread_pre = nullptr; // per thread of every chunk: the chunk's bases and breaks before its bytes
     unsigned long long *chunk_b = nullptr, *chunk_k = nullptr, *brk_rank = nullptr, *frag_out = nullptr;
     uint32_t* part_n = nullptr;
     unsigned long long *part_b = nullptr, *totals = nullptr;
@@ -66,9 +67,11 @@ struct ParseBuffers {
     uint64_t* packed = nullptr;
     uint64_t n_frags = 0, n_bases = 0;
     bool ensure_chunks(uint64_t n) {
-        if (!cf.ensure(4 * n) || !cb.ensure(8 * n) || !ck.ensure(8 * n) || !tf.ensure(2 * 256 * n)) return false;
+        if (!cf.ensure(4 * n) || !cb.ensure(8 * n) || !ck.ensure(8 * n) || !tf.ensure(2 * 256 * n) || !tp.ensure(4 * 256 * n))
+            return false;
         chunk_f = cf.as<uint32_t>(); chunk_b = cb.as<unsigned long long>(); chunk_k = ck.as<unsigned long long>();
         thread_f = tf.as<uint16_t>();
+        thread_pre = tp.as<uint32_t>();
         return true;
     }
     bool ensure_frags(uint64_t n) {
@@ -87,7 +90,7 @@ struct ParseBuffers {
         return true;
     }
     void release() {
-        DevBuf* all[] = {&cf, &cb, &ck, &br, &fo, &pn, &pbb, &foff, &flen, &tot, &pk, &tf};
+        DevBuf* all[] = {&cf, &cb, &ck, &br, &fo, &pn, &pbb, &foff, &flen, &tot, &pk, &tf, &tp};
         for (DevBuf* b : all) b->release();
     }
 };

@@ -14,12 +14,16 @@
 // (a scan), so every chunk runs independently:
 //   A  transfer function of every chunk (and of every thread's bytes before it, kept
 //      for C, E and G)                              B  scan: each chunk's start state
-//   C  bases and breaks of every chunk             D  scan: each chunk's offsets
+//   C  bases and breaks of every chunk (and of every thread's bytes before it in its
+//      chunk, kept for E and G)                     D  scan: each chunk's offsets
 //   E  the base rank of every break                F  fragments: lengths, keep, offsets
 //   G  bases written 2 bits each into the packed stream.
+// E and G visit only the threads with breaks, or bases, to place; what one thread does
+// with its 16 bytes is in cfg_parse_thread.cuh.
 #include "cuttlefish_gpu.h"
 #include "cfg_host.h"
 #include "cfg_internal.h"
+#include "cfg_parse_thread.cuh"
 
 #include <algorithm>
 
@@ -27,85 +31,7 @@ namespace cfg {
 
 namespace {
 
-constexpr uint32_t CHUNK = 4096, TPB = 256, BPT = CHUNK / TPB;   // bytes per thread: 16
-enum : uint32_t { C_NL = 0, C_GT = 1, C_BASE = 2, C_CR = 3, C_OTHER = 4, NCLASS = 5 };
-enum : uint32_t { E_SKIP = 0, E_BASE = 1, E_BREAK = 2 };
-
-// Up to 8 states; a transfer function packs the image of each state in 3 bits.
-struct Fsm {
-    uint8_t next[8][NCLASS];
-    uint8_t emit[8][NCLASS];
-    uint32_t n, start;
-};
-
-// The tables of an FSM of at most 5 states packed into registers: entry (class c, state s)
-// at index i = 5 c + s, its next state in 3 bits (bits 3i.. of nx_lo for i < 21, of nx_hi
-// above) and its emission in 2 bits of em.  A lookup is a few shifts on values every
-// thread holds, where an indexed table (in the kernel's parameters or in memory) would
-// serialise the warp's lanes over their distinct (state, class) pairs.
-struct FsmBits {
-    unsigned long long nx_lo, nx_hi, em;
-    // class c's whole next-state map as a transfer function (3 bits per state): bits 15c..
-    // of cf_lo for c < 4, cf_hi for c = 4; idem bit c: that map is idempotent (a run of
-    // class-c bytes acts as one)
-    unsigned long long cf_lo;
-    uint32_t cf_hi, idem;
-    uint32_t n, start;
-};
-__device__ __forceinline__ uint32_t fsm_next(const FsmBits& f, uint32_t st, uint32_t cl) {
-    const uint32_t i = 5 * cl + st;
-    return i < 21 ? (uint32_t)(f.nx_lo >> (3 * i)) & 7u : (uint32_t)(f.nx_hi >> (3 * (i - 21))) & 7u;
-}
-__device__ __forceinline__ uint32_t fsm_emit(const FsmBits& f, uint32_t st, uint32_t cl) {
-    return (uint32_t)(f.em >> (2 * (5 * cl + st))) & 3u;
-}
-FsmBits pack_fsm(const Fsm& m) {
-    FsmBits b{};
-    b.n = m.n; b.start = m.start;
-    for (uint32_t c = 0; c < NCLASS; ++c) {
-        uint32_t F = 0;
-        bool idem = true;
-        for (uint32_t st = 0; st < m.n; ++st) {
-            const uint32_t i = 5 * c + st;
-            if (i < 21) b.nx_lo |= (unsigned long long)m.next[st][c] << (3 * i);
-            else b.nx_hi |= (unsigned long long)m.next[st][c] << (3 * (i - 21));
-            b.em |= (unsigned long long)m.emit[st][c] << (2 * i);
-            F |= (uint32_t)m.next[st][c] << (3 * st);
-            idem = idem && m.next[m.next[st][c]][c] == m.next[st][c];
-        }
-        if (c < 4) b.cf_lo |= (unsigned long long)F << (15 * c); else b.cf_hi = F;
-        if (idem) b.idem |= 1u << c;
-    }
-    return b;
-}
-__device__ __forceinline__ uint32_t class_fn(const FsmBits& f, uint32_t cl) {
-    return cl < 4 ? (uint32_t)(f.cf_lo >> (15 * cl)) & 0x7FFFu : f.cf_hi;
-}
-
-__device__ __forceinline__ uint32_t byte_class(uint32_t c) {
-    if (c == '\n') return C_NL;
-    if (c == '>') return C_GT;
-    if (c == '\r') return C_CR;
-    const uint32_t u = c & 0xDF;
-    return (u == 'A' || u == 'C' || u == 'G' || u == 'T') ? C_BASE : C_OTHER;
-}
-__device__ __forceinline__ uint32_t base_code(uint32_t c) {   // A0 C1 G2 T3 (case-insensitive)
-    const uint32_t u = c & 0xDF;
-    return u == 'A' ? 0 : u == 'C' ? 1 : u == 'G' ? 2 : 3;
-}
-__host__ __device__ __forceinline__ uint32_t f_at(uint32_t f, uint32_t s) { return (f >> (3 * s)) & 7; }
-__host__ __device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
-// first f, then g
-__host__ __device__ __forceinline__ uint32_t compose(uint32_t f, uint32_t g, uint32_t n) {
-    uint32_t h = 0;
-    for (uint32_t s = 0; s < n; ++s) h |= f_at(g, f_at(f, s)) << (3 * s);
-    return h;
-}
-__host__ __device__ __forceinline__ uint32_t identity(uint32_t n) {
-    uint32_t h = 0;
-    for (uint32_t s = 0; s < n; ++s) h |= s << (3 * s);
-    return h;
-}
+using namespace parse;
 
 struct ParseArgs {
     const uint8_t* text;
@@ -113,6 +39,7 @@ struct ParseArgs {
     FsmBits fsm;
     uint32_t* chunk_f;             // A: transfer function; B: start state
     uint16_t* thread_f;            // A: per thread, the chunk's function before the thread's bytes
+    uint32_t* thread_pre;          // C: per thread, the chunk's bases and breaks before the thread's bytes
     unsigned long long* chunk_b;   // C: bases; D: bases before the chunk
     unsigned long long* chunk_k;   // C: breaks; D: breaks before the chunk
     unsigned long long* brk_rank;  // E: bases before break i (NB + 1 entries)
@@ -120,32 +47,24 @@ struct ParseArgs {
     const unsigned long long* frag_out;   // F: output start of fragment i, ~0 if dropped
 };
 
-// The bytes of thread t of a chunk, as 16 values (zero past the end).
-__device__ __forceinline__ void load_bytes(const ParseArgs& a, uint64_t chunk, uint8_t (&v)[BPT]) {
+// The bytes of thread t of a chunk (zero past the end).
+__device__ __forceinline__ Group load_group(const ParseArgs& a, uint64_t chunk) {
     const uint64_t p = chunk * CHUNK + (uint64_t)threadIdx.x * BPT;
+    Group g;
     if (p + BPT <= a.bytes) {
         const uint4 w = *(const uint4*)(a.text + p);
-        const uint32_t x[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-        for (int i = 0; i < BPT; ++i) v[i] = (uint8_t)(x[i >> 2] >> (8 * (i & 3)));
+        g.w[0] = w.x; g.w[1] = w.y; g.w[2] = w.z; g.w[3] = w.w;
     } else {
 #pragma unroll
-        for (int i = 0; i < BPT; ++i) v[i] = p + i < a.bytes ? a.text[p + i] : 0;
-    }
-}
-
-// The transfer function of a thread's bytes: the class maps composed in byte order, a run
-// of one idempotent class composed once (text is mostly runs of bases or quality letters).
-__device__ __forceinline__ uint32_t thread_transfer(const ParseArgs& a, const uint8_t (&v)[BPT], uint32_t nb) {
-    uint32_t f = identity(a.fsm.n), prev = NCLASS;
+        for (int j = 0; j < 4; ++j) {
+            uint32_t x = 0;
 #pragma unroll
-    for (int i = 0; i < BPT; ++i) {
-        if ((uint32_t)i >= nb) break;
-        const uint32_t cl = byte_class(v[i]);
-        if (cl != prev || !((a.fsm.idem >> cl) & 1)) f = compose(f, class_fn(a.fsm, cl), a.fsm.n);
-        prev = cl;
+            for (int i = 0; i < 4; ++i)
+                if (p + 4 * j + i < a.bytes) x |= (uint32_t)a.text[p + 4 * j + i] << (8 * i);
+            g.w[j] = x;
+        }
     }
-    return f;
+    return g;
 }
 
 // Exclusive scan of transfer functions over the CTA (in thread order).
@@ -182,9 +101,8 @@ __device__ __forceinline__ uint32_t bytes_of_thread(const ParseArgs& a, uint64_t
 __global__ void __launch_bounds__(TPB) k_parse_transfer(ParseArgs a) {
     __shared__ uint32_t sh[TPB / 32 + 1];
     for (uint64_t c = blockIdx.x; c < a.n_chunks; c += gridDim.x) {
-        uint8_t v[BPT];
-        load_bytes(a, c, v);
-        const uint32_t f = thread_transfer(a, v, bytes_of_thread(a, c));
+        const Group g = load_group(a, c);
+        const uint32_t f = thread_transfer(a.fsm, g, bytes_of_thread(a, c));
         const uint32_t ex = block_scan_f(f, a.fsm.n, sh);
         a.thread_f[c * TPB + threadIdx.x] = (uint16_t)ex;
         if (threadIdx.x == 0) a.chunk_f[c] = sh[TPB / 32];
@@ -215,26 +133,9 @@ __global__ void __launch_bounds__(1024) k_parse_states(ParseArgs a) {
     }
 }
 
-// Each thread's start state and its class counts, from the chunk's start state.
-struct ThreadPos { uint32_t state; uint8_t v[BPT]; uint32_t nb; };
-
-__device__ __forceinline__ void thread_start(const ParseArgs& a, uint64_t c, ThreadPos& tp, uint32_t*) {
-    load_bytes(a, c, tp.v);
-    tp.nb = bytes_of_thread(a, c);
-    tp.state = f_at(a.thread_f[c * TPB + threadIdx.x], a.chunk_f[c]);   // pass A's prefix from B's start state
-}
-
-__device__ __forceinline__ void thread_counts(const ParseArgs& a, const ThreadPos& tp, uint32_t& nb, uint32_t& nk) {
-    uint32_t st = tp.state;
-    nb = nk = 0;
-#pragma unroll
-    for (int i = 0; i < BPT; ++i) {
-        if ((uint32_t)i >= tp.nb) break;
-        const uint32_t cl = byte_class(tp.v[i]);
-        const uint32_t e = fsm_emit(a.fsm, st, cl);
-        nb += e == E_BASE; nk += e == E_BREAK;
-        st = fsm_next(a.fsm, st, cl);
-    }
+// A thread's start state: pass A's prefix from B's start state of the chunk.
+__device__ __forceinline__ uint32_t thread_state(const ParseArgs& a, uint64_t c) {
+    return f_at(a.thread_f[c * TPB + threadIdx.x], a.chunk_f[c]);
 }
 
 __device__ __forceinline__ void block_sum2(uint32_t& x, uint32_t& y, uint32_t* sh, uint32_t& ex_x, uint32_t& ex_y,
@@ -262,15 +163,15 @@ __device__ __forceinline__ void block_sum2(uint32_t& x, uint32_t& y, uint32_t* s
     __syncthreads();
 }
 
-// C: bases and breaks of every chunk.
+// C: bases and breaks of every chunk, and of every thread's bytes before it in its chunk.
 __global__ void __launch_bounds__(TPB) k_parse_counts(ParseArgs a) {
     __shared__ uint32_t sh[32];
     for (uint64_t c = blockIdx.x; c < a.n_chunks; c += gridDim.x) {
-        ThreadPos tp;
-        thread_start(a, c, tp, sh);
+        const Group g = load_group(a, c);
         uint32_t nb, nk, eb, ek, tb, tk;
-        thread_counts(a, tp, nb, nk);
+        thread_counts(a.fsm, thread_state(a, c), g, bytes_of_thread(a, c), nb, nk);
         block_sum2(nb, nk, sh, eb, ek, tb, tk);
+        a.thread_pre[c * TPB + threadIdx.x] = pre_pack(eb, ek);
         if (threadIdx.x == 0) { a.chunk_b[c] = tb; a.chunk_k[c] = tk; }
     }
 }
@@ -302,27 +203,17 @@ __global__ void __launch_bounds__(1024) k_parse_offsets(ParseArgs a) {
     }
 }
 
+__device__ __forceinline__ ThreadSpan thread_span(const ParseArgs& a, uint64_t c) {
+    return parse::thread_span(a.thread_pre, a.chunk_b, a.chunk_k, c, threadIdx.x);
+}
+
 // E: for every break, the number of bases before it; break NB (after the text) closes
-// the last fragment.
+// the last fragment.  Only threads whose bytes emit a break read them.
 __global__ void __launch_bounds__(TPB) k_parse_breaks(ParseArgs a) {
-    __shared__ uint32_t sh[32];
     for (uint64_t c = blockIdx.x; c < a.n_chunks; c += gridDim.x) {
-        ThreadPos tp;
-        thread_start(a, c, tp, sh);
-        uint32_t nb, nk, eb, ek, tb, tk;
-        thread_counts(a, tp, nb, nk);
-        block_sum2(nb, nk, sh, eb, ek, tb, tk);
-        unsigned long long r = a.chunk_b[c] + eb, kk = a.chunk_k[c] + ek;
-        uint32_t st = tp.state;
-#pragma unroll
-        for (int i = 0; i < BPT; ++i) {
-            if ((uint32_t)i >= tp.nb) break;
-            const uint32_t cl = byte_class(tp.v[i]);
-            const uint32_t e = fsm_emit(a.fsm, st, cl);
-            if (e == E_BASE) ++r;
-            else if (e == E_BREAK) a.brk_rank[kk++] = r;
-            st = fsm_next(a.fsm, st, cl);
-        }
+        const ThreadSpan sp = thread_span(a, c);
+        if (sp.nk == 0) continue;
+        thread_breaks(a.fsm, thread_state(a, c), load_group(a, c), bytes_of_thread(a, c), sp.r, sp.kk, a.brk_rank);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) a.brk_rank[a.chunk_k[a.n_chunks]] = a.chunk_b[a.n_chunks];
 }
@@ -430,77 +321,21 @@ __global__ void __launch_bounds__(1024) k_frag_write(FragArgs f) {
     }
 }
 
-// G: every kept base to its place in the packed stream (MSB-first, 32 per word).
+struct AtomicOr64 {
+    __device__ __forceinline__ void operator()(uint64_t* w, uint64_t bits) const {
+        atomicOr((unsigned long long*)w, (unsigned long long)bits);
+    }
+};
+
+// G: every kept base to its place in the packed stream (MSB-first, 32 per word).  Only
+// threads whose bytes emit a base read them.
 __global__ void __launch_bounds__(TPB) k_parse_pack(ParseArgs a) {
-    __shared__ uint32_t sh[32];
     for (uint64_t c = blockIdx.x; c < a.n_chunks; c += gridDim.x) {
-        ThreadPos tp;
-        thread_start(a, c, tp, sh);
-        uint32_t nb, nk, eb, ek, tb, tk;
-        thread_counts(a, tp, nb, nk);
-        block_sum2(nb, nk, sh, eb, ek, tb, tk);
-        unsigned long long r = a.chunk_b[c] + eb, kk = a.chunk_k[c] + ek;
-        uint32_t st = tp.state;
-        uint64_t word = ~0ull, acc = 0;
-#pragma unroll
-        for (int i = 0; i < BPT; ++i) {
-            if ((uint32_t)i >= tp.nb) break;
-            const uint32_t ch = tp.v[i], cl = byte_class(ch);
-            const uint32_t e = fsm_emit(a.fsm, st, cl);
-            if (e == E_BASE) {
-                const unsigned long long o = a.frag_out[kk];
-                if (o != ~0ull) {
-                    const unsigned long long q = o + (r - (kk ? a.brk_rank[kk - 1] : 0ull));
-                    const uint64_t w = q >> 5;
-                    if (w != word) {
-                        if (word != ~0ull) atomicOr((unsigned long long*)a.packed + word, (unsigned long long)acc);
-                        word = w; acc = 0;
-                    }
-                    acc |= (uint64_t)base_code(ch) << (62 - 2 * (q & 31));
-                }
-                ++r;
-            } else if (e == E_BREAK) {
-                ++kk;
-            }
-            st = fsm_next(a.fsm, st, cl);
-        }
-        if (word != ~0ull) atomicOr((unsigned long long*)a.packed + word, (unsigned long long)acc);
+        const ThreadSpan sp = thread_span(a, c);
+        if (sp.nb == 0) continue;
+        thread_pack(a.fsm, thread_state(a, c), load_group(a, c), bytes_of_thread(a, c), sp.r, sp.kk, sp.nb, sp.nk,
+                    a.frag_out, a.brk_rank, a.packed, AtomicOr64{});
     }
-}
-
-Fsm fasta_fsm() {
-    // states: 0 line start before any record, 1 inside such a line, 2 header,
-    // 3 line start inside a record, 4 sequence line
-    Fsm m{};
-    m.n = 5; m.start = 0;
-    auto set = [&](uint32_t s, uint32_t c, uint32_t nx, uint32_t e) { m.next[s][c] = (uint8_t)nx; m.emit[s][c] = (uint8_t)e; };
-    for (uint32_t c = 0; c < NCLASS; ++c) {
-        set(0, c, 1, E_SKIP); set(1, c, 1, E_SKIP); set(2, c, 2, E_SKIP);
-        set(3, c, 4, E_BREAK); set(4, c, 4, E_BREAK);
-    }
-    set(0, C_NL, 0, E_SKIP); set(0, C_CR, 0, E_SKIP); set(0, C_GT, 2, E_BREAK);
-    set(1, C_NL, 0, E_SKIP);
-    set(2, C_NL, 3, E_SKIP);
-    set(3, C_NL, 3, E_SKIP); set(3, C_GT, 2, E_BREAK); set(3, C_BASE, 4, E_BASE);
-    set(4, C_NL, 3, E_SKIP); set(4, C_BASE, 4, E_BASE);
-    return m;
-}
-
-Fsm fastq_fsm() {
-    // states: 0 before a record (blank lines skipped), 1 header line, 2 sequence line,
-    // 3 '+' line, 4 quality line
-    Fsm m{};
-    m.n = 5; m.start = 0;
-    auto set = [&](uint32_t s, uint32_t c, uint32_t nx, uint32_t e) { m.next[s][c] = (uint8_t)nx; m.emit[s][c] = (uint8_t)e; };
-    for (uint32_t c = 0; c < NCLASS; ++c) {
-        set(0, c, 1, E_SKIP); set(1, c, 1, E_SKIP); set(2, c, 2, E_BREAK); set(3, c, 3, E_SKIP); set(4, c, 4, E_SKIP);
-    }
-    set(0, C_NL, 0, E_SKIP); set(0, C_CR, 0, E_SKIP);
-    set(1, C_NL, 2, E_SKIP);
-    set(2, C_NL, 3, E_BREAK); set(2, C_BASE, 2, E_BASE);
-    set(3, C_NL, 4, E_SKIP);
-    set(4, C_NL, 0, E_SKIP);
-    return m;
 }
 
 }  // namespace
@@ -513,6 +348,7 @@ int parse_text_device(const uint8_t* d_text, uint64_t bytes, int fastq, uint32_t
     const uint64_t nc = a.n_chunks;
     if (!pb.ensure_chunks(nc + 1)) return CFG_ERR_OOM;
     a.chunk_f = pb.chunk_f; a.chunk_b = pb.chunk_b; a.chunk_k = pb.chunk_k; a.thread_f = pb.thread_f;
+    a.thread_pre = pb.thread_pre;
     const unsigned grid = (unsigned)std::min<uint64_t>(std::max<uint64_t>(nc, 1), 148ull * 16);
     if (nc) {
         k_parse_transfer<<<grid, TPB, 0, s>>>(a);
