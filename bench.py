@@ -598,6 +598,30 @@ def bench_workload(args, name, pg, rank, local, world, with_cpu):
         text_times.append(time.perf_counter() - t0)
         if tb != fin_bytes:
             raise RuntimeError("unitigs from the text path differ in size from the packed path's")
+    # where the text path's time goes: cfg_submit_text alone (H2D of the text + device
+    # parse) beside a plain copy of the same pinned buffer; informational, never fatal
+    text_split = None
+    try:
+        import torch
+        dev_copy = torch.empty(text_bytes, dtype=torch.uint8, device=f"cuda:{local if world > 1 else 0}")
+        copy_ms, submit_ms = [], []
+        for rep in range(4):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            dev_copy.copy_(text, non_blocking=True)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            cx.submit_text_ptr(text.data_ptr(), text_bytes)
+            torch.cuda.synchronize()
+            t2 = time.perf_counter()
+            if rep:
+                copy_ms.append(1e3 * (t1 - t0)); submit_ms.append(1e3 * (t2 - t1))
+        del dev_copy
+        text_split = {"submit_text_ms": statistics.median(submit_ms), "plain_copy_ms": statistics.median(copy_ms),
+                      "parse_ms": statistics.median(submit_ms) - statistics.median(copy_ms),
+                      "note": "host wall time with device syncs; parse_ms = cfg_submit_text - a plain H2D of the text"}
+    except Exception as ex:   # the line is printed regardless
+        text_split = {"error": f"{type(ex).__name__}: {ex}"}
     del text
     text_s_max = allreduce_max(pg, local, sum(text_times))
 
@@ -660,7 +684,8 @@ def bench_workload(args, name, pg, rank, local, world, with_cpu):
                      "h2d_bytes_per_step": text_bytes, "d2h_bytes_per_step": d2h,
                      "ms_per_step": 1e3 * text_s_max / args.steps,
                      "input": "FASTQ text (@, sequence, +, quality lines)" if name == "reads30x" else
-                              "FASTA text (one line per record)"},
+                              "FASTA text (one line per record)",
+                     "split": text_split},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": "k_subgraph (construct + walk, all launches of a run)",
                      "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
