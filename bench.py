@@ -617,9 +617,12 @@ def bench_workload(args, name, pg, rank, local, world, with_cpu):
             if rep:
                 copy_ms.append(1e3 * (t1 - t0)); submit_ms.append(1e3 * (t2 - t1))
         del dev_copy
+        dev_copy_ms, dev_parse_ms = cx.text_timings()   # CUDA events of the last submit
         text_split = {"submit_text_ms": statistics.median(submit_ms), "plain_copy_ms": statistics.median(copy_ms),
-                      "parse_ms": statistics.median(submit_ms) - statistics.median(copy_ms),
-                      "note": "host wall time with device syncs; parse_ms = cfg_submit_text - a plain H2D of the text"}
+                      "device_copy_ms": dev_copy_ms, "device_parse_ms": dev_parse_ms,
+                      "note": "submit_text_ms and plain_copy_ms (torch's copy of the same pinned text): host wall "
+                              "time around device syncs, medians of 3; device_*: CUDA events of the library's "
+                              "own copy and parse in the last cfg_submit_text"}
     except Exception as ex:   # the line is printed regardless
         text_split = {"error": f"{type(ex).__name__}: {ex}"}
     del text

@@ -37,6 +37,9 @@ struct cfg_ctx {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t piece_ev[MAX_PIECES] = {}, idle_ev = nullptr;
     ParseBuffers parse;
+    // cfg_submit_text: events before and after the text's copy and after the parse
+    cudaEvent_t text_ev[3] = {};
+    bool text_timed = false;
     const uint64_t* d_packed = nullptr; const uint64_t* d_frag_off = nullptr; const uint32_t* d_frag_len = nullptr;
     uint64_t n_bases = 0, n_frags = 0;
     bool have_input = false, have_run = false;
@@ -432,6 +435,8 @@ int cfg_create(int device, const cfg_params* params, cfg_ctx** out) {
     for (auto& e : c->piece_ev)
         if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) { cfg_destroy(c); return CFG_ERR_CUDA; }
     if (cudaEventCreateWithFlags(&c->idle_ev, cudaEventDisableTiming) != cudaSuccess) { cfg_destroy(c); return CFG_ERR_CUDA; }
+    for (auto& e : c->text_ev)
+        if (cudaEventCreate(&e) != cudaSuccess) { cfg_destroy(c); return CFG_ERR_CUDA; }
     *out = c;
     return CFG_OK;
 }
@@ -527,15 +532,30 @@ int cfg_submit_text(cfg_ctx* c, const char* text, uint64_t bytes) {
     while (i < bytes && (text[i] == '\n' || text[i] == '\r')) ++i;
     const int fastq = i < bytes && text[i] == '@';
     if (!c->text.ensure(bytes + 16)) return fail(c, CFG_ERR_OOM, "text buffer");
+    c->text_timed = false;
+    CK(cudaEventRecord(c->text_ev[0], c->stream));
     if (bytes) CK(cudaMemcpyAsync(c->text.p, text, bytes, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaEventRecord(c->text_ev[1], c->stream));
     c->pieces.clear();
     const int rc = parse_text_device(c->text.as<uint8_t>(), bytes, fastq, c->p.k, c->parse, c->stream);
     if (rc == CFG_ERR_OOM) return fail(c, rc, "parse buffers");
     if (rc == CFG_ERR_BAD_INPUT) return fail(c, rc, "a job must hold fewer than 2^32 bases");
     if (rc) return fail(c, rc, std::string("text parse: ") + cudaGetErrorString(cudaGetLastError()));
+    CK(cudaEventRecord(c->text_ev[2], c->stream));
+    c->text_timed = true;
     c->d_packed = c->parse.packed; c->d_frag_off = c->parse.frag_off; c->d_frag_len = c->parse.frag_len;
     c->n_bases = c->parse.n_bases; c->n_frags = c->parse.n_frags;
     c->have_input = true; c->have_run = false;
+    return CFG_OK;
+}
+
+int cfg_text_timings(cfg_ctx* c, float out_ms[2]) {
+    if (!c || !out_ms) return CFG_ERR_BAD_INPUT;
+    if (!c->text_timed) return fail(c, CFG_ERR_STATE, "no completed cfg_submit_text");
+    CK(cudaSetDevice(c->device));
+    CK(cudaEventSynchronize(c->text_ev[2]));
+    CK(cudaEventElapsedTime(&out_ms[0], c->text_ev[0], c->text_ev[1]));
+    CK(cudaEventElapsedTime(&out_ms[1], c->text_ev[1], c->text_ev[2]));
     return CFG_OK;
 }
 
@@ -763,6 +783,7 @@ void cfg_destroy(cfg_ctx* c) {
     for (auto& e : c->ev) if (e) cudaEventDestroy(e);
     for (auto& e : c->piece_ev) if (e) cudaEventDestroy(e);
     if (c->idle_ev) cudaEventDestroy(c->idle_ev);
+    for (auto& e : c->text_ev) if (e) cudaEventDestroy(e);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;

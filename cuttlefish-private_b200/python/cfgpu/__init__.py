@@ -112,6 +112,7 @@ SIGNATURES = {
     "cfg_dump_states": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(StateDump)]),
     "cfg_dump_records": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(RecordDump)]),
     "cfg_last_timings": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
+    "cfg_text_timings": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
     "cfg_last_phase_cycles": (ctypes.c_int, [ctypes.c_void_p, U64P]),
     "cfg_last_error_string": (ctypes.c_char_p, [ctypes.c_void_p]),
     "cfg_destroy": (None, [ctypes.c_void_p]),
@@ -300,6 +301,12 @@ class Compactor:
     def timings(self):
         t = (ctypes.c_float * 4)()
         _check(self.lib, self.ctx, self.lib.cfg_last_timings(self.ctx, t), "cfg_last_timings")
+        return list(t)
+
+    def text_timings(self):
+        """cfg_text_timings: device ms of the last cfg_submit_text's copy and of its parse."""
+        t = (ctypes.c_float * 2)()
+        _check(self.lib, self.ctx, self.lib.cfg_text_timings(self.ctx, t), "cfg_text_timings")
         return list(t)
 
     def phase_cycles(self):

@@ -161,6 +161,13 @@ int cfg_submit_packed_device(cfg_ctx* ctx, const uint64_t* d_packed, uint64_t n_
  * 265-297) and the fragment scan (src/Graph_Partitioner.cpp:461-501). */
 int cfg_submit_text(cfg_ctx* ctx, const char* text, uint64_t bytes);
 
+/* Device time of the last successful cfg_submit_text, in milliseconds, from CUDA events
+ * on the context's stream: [0] the copy of the text to the device, [1] the parse (every
+ * pass, with its two waits for counts on the host).  Waits for the parse to finish.
+ * No counterpart in the reference (its reader is timed inside its splitting phase,
+ * src/dBG_Contractor.cpp:58). */
+int cfg_text_timings(cfg_ctx* ctx, float out_ms[2]);
+
 /* The submitted input's size, and a copy of it in cfg_submit_packed's layout
  * (words: (n_bases+31)/32 entries; any pointer may be NULL). */
 int cfg_input_counts(cfg_ctx* ctx, uint64_t* n_bases, uint64_t* n_frags);

@@ -88,3 +88,9 @@ def test_server_rejects_bad_config():
     cfg = cfgpu.ServerConfig(65, 0, 0, 0, 0)
     assert lib.cfg_server_create(0, ctypes.byref(cfg), ctypes.byref(s)) == 1
     assert lib.cfg_server_submit(None, None, None, None) == 1
+
+
+def test_text_timings_needs_a_context():
+    lib = cfgpu.load()
+    out = (ctypes.c_float * 2)()
+    assert lib.cfg_text_timings(None, out) == 1   # CFG_ERR_BAD_INPUT, before touching the device

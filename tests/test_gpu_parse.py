@@ -133,3 +133,16 @@ def test_edge_texts():
 def test_large_multichunk_fastq():
     rng = np.random.default_rng(320)
     check(fastq_text(rng, 31, 40_000), 31)
+
+
+def test_text_timings():
+    """cfg_text_timings: device times of the last cfg_submit_text's copy and parse (none
+    before a text was submitted)."""
+    rng = np.random.default_rng(321)
+    text = fastq_text(rng, 31, 5_000)
+    with cfgpu.Compactor(31, 20, 1, 16384) as cx:
+        with pytest.raises(cfgpu.CfgError):
+            cx.text_timings()
+        cx.submit_text(text)
+        copy_ms, parse_ms = cx.text_timings()
+        assert 0.0 <= copy_ms < 60_000 and 0.0 < parse_ms < 60_000
