@@ -3,7 +3,10 @@ over every (chunk, thread) of a text by tests/parse_emul, give exactly the packe
 and fragment table of the CLI's host parser followed by cfg_pack_records -- the same
 comparison tests/test_gpu_parse.py makes on the GPU.  The word-wise steps (byte classes
 by word compares, counts, transfer functions, 2-bit codes) are also checked against the
-byte-by-byte walk of the parser's state machines on random 16-byte groups."""
+byte-by-byte walk of the parser's state machines on random 16-byte groups, and the
+unitigs of the fragments it finds in the edge-case texts of
+tests/test_gpu_parse_reference.py are those of the reference's own build (when
+oracle/_ref holds it)."""
 import ctypes
 import os
 import subprocess
@@ -113,3 +116,33 @@ def test_fasta_long_lines_and_crlf(emul):
 def test_large_multichunk_fastq(emul):
     rng = np.random.default_rng(320)
     check(emul, fastq_text(rng, 31, 40_000), 31)
+
+
+def fragments(words, frag_off, frag_len):
+    """The fragment strings of a packed stream (2 bits per base, MSB-first, 32 per word)."""
+    w = np.array(words, dtype=np.uint64)
+    codes = ((w[:, None] >> (np.uint64(62) - np.uint64(2) * np.arange(32, dtype=np.uint64))) & np.uint64(3)).ravel()
+    text = np.frombuffer(b"ACGT", dtype=np.uint8)[codes.astype(np.int64)].tobytes().decode()
+    return [text[o:o + n] for o, n in zip(frag_off, frag_len)]
+
+
+@pytest.mark.parametrize("case", ["fasta", "fasta_crlf", "fasta_empty_records", "fastq", "fastq_crlf"])
+def test_per_thread_parse_matches_reference_reader(emul, case, tmp_path):
+    """The texts of tests/test_gpu_parse_reference.py (CRLF, lowercase, N runs and IUPAC
+    codes, uneven lines, empty records, quality lines starting with '@' or '+'), parsed by
+    the device parser's per-thread code on the CPU: the global maximal unitigs of its
+    fragments (the oracle at one subgraph) are exactly those of the reference's own
+    `cuttlefish build` on the same file."""
+    import orc
+    import test_gpu_parse_reference as ref
+    rng = np.random.default_rng(sum(case.encode()))
+    if case.startswith("fasta"):
+        text = ref.fasta(rng, crlf=case.endswith("crlf"), empty_records=case.endswith("records"))
+    else:
+        text = ref.fastq(rng, crlf=case.endswith("crlf"))
+    want = ref.reference_unitigs(text, case.startswith("fastq"), tmp_path)
+    n_bases, words, fo, fl = parse(emul, text, ref.K)
+    frags = fragments(words, fo, fl)
+    assert sum(len(f) for f in frags) == n_bases
+    got = ref.unitig_set(orc.OracleRun(frags, ref.K, 20, 1, 1).fasta)
+    assert got == want
