@@ -139,6 +139,12 @@ int parse_emul(const uint8_t* text, uint64_t bytes, int fastq, uint32_t k, uint6
 
 void parse_emul_free(void* p) { std::free(p); }
 
+// The word-wise flags of a machine: loop_mask, gt_other, bo_idem.
+void parse_emul_fsm_flags(int fastq, uint32_t out[3]) {
+    const FsmBits f = pack_fsm(fastq ? fastq_fsm() : fasta_fsm());
+    out[0] = f.loop_mask; out[1] = f.gt_other; out[2] = f.bo_idem;
+}
+
 // Random groups (bytes drawn mostly from letters, quality and delimiter characters): the
 // word-wise counts and transfer functions against the byte-by-byte walk in every state of
 // both machines, and the 2-bit codes of all-letter groups against base_code.  Returns

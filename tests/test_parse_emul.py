@@ -146,3 +146,15 @@ def test_per_thread_parse_matches_reference_reader(emul, case, tmp_path):
     assert sum(len(f) for f in frags) == n_bases
     got = ref.unitig_set(orc.OracleRun(frags, ref.K, 20, 1, 1).fasta)
     assert got == want
+
+
+def test_word_wise_states_of_each_machine(emul):
+    """Which groups may skip the byte walk: FASTQ loops on bases and other bytes inside its
+    header, sequence, '+' and quality lines (states 1-4) and reads '>' as an other byte;
+    FASTA loops inside a pre-record line, a header and a sequence line (states 1, 2, 4),
+    where '>' starts a record.  Bases and other bytes share one idempotent map in both."""
+    out = (ctypes.c_uint32 * 3)()
+    emul.parse_emul_fsm_flags(1, out)
+    assert list(out) == [0b11110, 1, 1]
+    emul.parse_emul_fsm_flags(0, out)
+    assert list(out) == [0b10110, 0, 1]
